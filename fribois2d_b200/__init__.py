@@ -1,0 +1,282 @@
+"""B200-native FRiBoIS2D fluid time step.
+
+The product is the native library ``libfribois2d.so`` (CUDA, sm_100a) behind
+the C ABI in ``include/fribois2d.h``.  This module is a thin ctypes binding
+that mirrors the reference's driver-level interface (src/main.F90:51-97):
+
+* ``Solver(input_dir)``      -- read_genin + fluid_pre + read_rigid + rigid_pre
+* ``Solver.fluid_tsch(ns)``  -- fluid_tsch(ns, 'a')  (src/fluid_tsch.F90:4)
+* ``Solver.rigid(ns)``       -- rigid(ns, 'a', 0)    (src/rigid.F90:4), time += dt
+* ``Solver.advance(ns0, n)`` -- n iterations of the main loop body, CUDA graph
+
+Errors are raised as :class:`FBError` carrying the library's status code,
+where the reference would call stopcase/MPI_ABORT.  There is no CPU
+fallback: if the native library cannot be loaded, import-time use fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfribois2d.so")
+
+FB_OK = 0
+STATUS = {0: "FB_OK", 1: "FB_ERR_CFL", 2: "FB_ERR_MLS", 3: "FB_ERR_MARKER_OUT",
+          4: "FB_ERR_INPUT", 5: "FB_ERR_CUDA", 6: "FB_ERR_STATE", 7: "FB_ERR_UNSUPPORTED",
+          8: "FB_ERR_NUMERIC"}
+FB_ERR_CFL, FB_ERR_MLS, FB_ERR_MARKER_OUT, FB_ERR_INPUT = 1, 2, 3, 4
+FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC = 5, 6, 7, 8
+
+# array ids (include/fribois2d.h)
+IDS = dict(q2=0, q3=1, pr=2, dph=3, rhs2=7, rhs3=8, ru2=9, ru3=10, qb2s=20, qb2n=21, dqb2s=22,
+           dqb2n=23, qb3s=24, qb3n=25, dqb3s=26, dqb3n=27, dq2x2o=28, dq3x2o=29, rc=40, rm=41,
+           zz=42, zm=43, udx2c=48, udx2m=49, udx3c=50, udx3m=51, amphj=64, acphj=65, apphj=66,
+           amphk=67, acphk=68, apphk=69, wr=80, zmm=81, zmmt=82, lmcc=90, lmvel=91, lmacc=92,
+           lmnor=93, lmA=94, vert=95, phi=96, cl=97, press=98, tau=99, bcerrv=100, bcerrw=101,
+           rigid=110, scalars=111, forces=112)
+IIDS = dict(lmind=0, eulins=1)
+FIELDS = ("q2", "q3", "pr", "dph", "rhs2", "rhs3", "ru2", "ru3")
+BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", "dq2x2o", "dq3x2o")
+STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
+              phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17)
+HIST_COLS = 21
+HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
+              "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm")
+SCALAR_NAMES = ("time", "dt", "dt_o", "beta", "al", "ga", "ro", "cflm", "q3avg", "nbcv", "nbcw",
+                "ddmin", "pravg")
+
+
+class FBError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = code
+        super().__init__(f"{where}: {STATUS.get(code, code)} ({_status_string(code)})")
+
+
+_LIB = None
+
+
+def _status_string(code: int) -> str:
+    try:
+        return lib().fb_status_string(code).decode()
+    except Exception:  # pragma: no cover - library missing
+        return "?"
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library (never a fallback: raises if it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"native library missing: {LIB_PATH} (run python -m fribois2d_b200.build)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp, dp, ip, i64 = ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int32), ctypes.c_int64
+    sig = {
+        "fb_create": ([ctypes.c_char_p, ctypes.c_int, P(vp)], ctypes.c_int),
+        "fb_destroy": ([vp], ctypes.c_int),
+        "fb_fluid_tsch": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_rigid": ([vp, ctypes.c_int, dp], ctypes.c_int),
+        "fb_advance": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
+        "fb_get_loads": ([vp, dp, dp], ctypes.c_int),
+        "fb_set_markers": ([vp, dp, dp, dp, dp], ctypes.c_int),
+        "fb_get_dims": ([vp, ip], ctypes.c_int),
+        "fb_get_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
+        "fb_set_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
+        "fb_get_iarray": ([vp, ctypes.c_int, ip, i64], ctypes.c_int),
+        "fb_synchronize": ([vp], ctypes.c_int),
+        "fb_set_substep": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "fb_stage": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "fb_last_advance_ms": ([vp, dp], ctypes.c_int),
+        "fb_host_create": ([ctypes.c_char_p, P(vp)], ctypes.c_int),
+        "fb_host_destroy": ([vp], ctypes.c_int),
+        "fb_host_dims": ([vp, ip], ctypes.c_int),
+        "fb_host_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
+        "fb_eigen_tridiag": ([ctypes.c_int, dp, dp, dp, dp, dp, dp], ctypes.c_int),
+        "fb_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "fb_version": ([], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(code: int, where: str) -> None:
+    if code != FB_OK:
+        raise FBError(code, where)
+
+
+class HostSetup:
+    """Host-only set-up of a case (parsing, metrics, eigen data); no GPU."""
+
+    def __init__(self, input_dir: str):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _check(self._lib.fb_host_create(input_dir.encode(), ctypes.byref(h)), "fb_host_create")
+        self.h = h
+        dims = (ctypes.c_int32 * 8)()
+        _check(self._lib.fb_host_dims(self.h, dims), "fb_host_dims")
+        self.n2, self.n3, self.nlm, self.nsst, self.idtv, self.ibact, self.wfun, self.forst = list(dims)
+        self.n2m, self.n3m = self.n2 - 1, self.n3 - 1
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._lib.fb_host_destroy(self.h)
+            self.h = None
+
+    def array(self, name: str) -> np.ndarray:
+        n = {"rc": self.n2, "rm": self.n2, "udx2c": self.n2, "udx2m": self.n2, "amphj": self.n2,
+             "acphj": self.n2, "apphj": self.n2, "zz": self.n3, "zm": self.n3, "udx3c": self.n3,
+             "udx3m": self.n3, "amphk": self.n3, "acphk": self.n3, "apphk": self.n3,
+             "wr": self.n3m, "zmm": self.n3m ** 2, "zmmt": self.n3m ** 2, "lmcc": 2 * self.nlm,
+             "lmvel": 2 * self.nlm, "lmacc": 2 * self.nlm, "lmnor": 2 * self.nlm,
+             "lmA": self.nlm, "vert": 2 * (self.nlm + 1), "rigid": 18}[name]
+        out = np.zeros(n, dtype=np.float64)
+        _check(self._lib.fb_host_array(self.h, IDS[name], _dp(out), n), f"fb_host_array({name})")
+        if name in ("zmm", "zmmt"):
+            return out.reshape(self.n3m, self.n3m, order="F")
+        return out
+
+
+def eigen_tridiag(am: np.ndarray, ac: np.ndarray, ap: np.ndarray):
+    """Eigen-decomposition of a tridiagonal operator with positive off-diagonal
+    products (the z Poisson operator of src/phini.F90:59-65)."""
+    n = len(ac)
+    am = np.ascontiguousarray(am, dtype=np.float64)
+    ac = np.ascontiguousarray(ac, dtype=np.float64)
+    ap = np.ascontiguousarray(ap, dtype=np.float64)
+    wr = np.zeros(n)
+    zmm = np.zeros(n * n)
+    zmmt = np.zeros(n * n)
+    _check(lib().fb_eigen_tridiag(n, _dp(am), _dp(ac), _dp(ap), _dp(wr), _dp(zmm), _dp(zmmt)),
+           "fb_eigen_tridiag")
+    return wr, zmm.reshape(n, n, order="F"), zmmt.reshape(n, n, order="F")
+
+
+class Solver:
+    """One FRiBoIS2D case on one GPU (the drop-in for src/main.F90's loop)."""
+
+    def __init__(self, input_dir: str, device: int = 0):
+        self._lib = lib()
+        c = ctypes.c_void_p()
+        _check(self._lib.fb_create(input_dir.encode(), int(device), ctypes.byref(c)), "fb_create")
+        self.ctx = c
+        dims = (ctypes.c_int32 * 8)()
+        _check(self._lib.fb_get_dims(self.ctx, dims), "fb_get_dims")
+        self.n2, self.n3, self.nlm, self.nsst, self.pitch, self.ldh = list(dims)[:6]
+        self.n2m, self.n3m = self.n2 - 1, self.n3 - 1
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self._lib.fb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- reference entry points
+    def fluid_tsch(self, ns: int) -> None:
+        _check(self._lib.fb_fluid_tsch(self.ctx, int(ns)), "fb_fluid_tsch")
+
+    def rigid(self, ns: int) -> np.ndarray:
+        row = np.zeros(8)
+        _check(self._lib.fb_rigid(self.ctx, int(ns), _dp(row)), "fb_rigid")
+        return row
+
+    def advance(self, ns0: int, nsteps: int, history: bool = True) -> Optional[np.ndarray]:
+        hist = np.zeros((nsteps, HIST_COLS)) if history else None
+        ptr = _dp(hist) if history else ctypes.POINTER(ctypes.c_double)()
+        _check(self._lib.fb_advance(self.ctx, int(ns0), int(nsteps), ptr), "fb_advance")
+        return hist
+
+    def last_advance_ms(self) -> float:
+        ms = ctypes.c_double()
+        _check(self._lib.fb_last_advance_ms(self.ctx, ctypes.byref(ms)), "fb_last_advance_ms")
+        return ms.value
+
+    def get_loads(self):
+        p = np.zeros(self.nlm)
+        t = np.zeros(2 * self.nlm)
+        _check(self._lib.fb_get_loads(self.ctx, _dp(p), _dp(t)), "fb_get_loads")
+        return p, t.reshape(self.nlm, 2)
+
+    def set_markers(self, lmcc=None, lmvel=None, lmacc=None, lmnor=None) -> None:
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (lmcc, lmvel, lmacc, lmnor)]
+        ptrs = [ctypes.POINTER(ctypes.c_double)() if a is None else _dp(a) for a in arrs]
+        _check(self._lib.fb_set_markers(self.ctx, *ptrs), "fb_set_markers")
+
+    # ---- stages (one reference subroutine each)
+    def set_substep(self, ns: int, n: int) -> None:
+        _check(self._lib.fb_set_substep(self.ctx, int(ns), int(n)), "fb_set_substep")
+
+    def stage(self, name: str, n: int = 1) -> int:
+        return self._lib.fb_stage(self.ctx, STAGES[name], int(n))
+
+    # ---- state
+    def _count(self, name: str) -> int:
+        if name in FIELDS:
+            return (self.n3 + 1) * self.n2
+        if name in BOUNDARY or name in ("rc", "rm", "udx2c", "udx2m", "amphj", "acphj", "apphj"):
+            return self.n2
+        if name in ("zz", "zm", "udx3c", "udx3m", "amphk", "acphk", "apphk"):
+            return self.n3
+        return {"wr": self.n3m, "zmm": self.n3m ** 2, "zmmt": self.n3m ** 2,
+                "lmcc": 2 * self.nlm, "lmvel": 2 * self.nlm, "lmacc": 2 * self.nlm,
+                "lmnor": 2 * self.nlm, "lmA": self.nlm, "vert": 2 * (self.nlm + 1),
+                "phi": 18 * self.nlm, "cl": 2 * self.nlm, "press": self.nlm, "tau": 2 * self.nlm,
+                "bcerrv": self.nlm, "bcerrw": self.nlm, "rigid": 18, "scalars": 13,
+                "forces": 8}[name]
+
+    def get(self, name: str) -> np.ndarray:
+        """Copy of a device array; fields come back as ``(n3+1, n2)``: row k, column j-1."""
+        n = self._count(name)
+        out = np.zeros(n)
+        _check(self._lib.fb_get_array(self.ctx, IDS[name], _dp(out), n), f"fb_get_array({name})")
+        if name in FIELDS:
+            return out.reshape(self.n3 + 1, self.n2)
+        if name in ("zmm", "zmmt"):
+            return out.reshape(self.n3m, self.n3m, order="F")
+        return out
+
+    def set(self, name: str, value: np.ndarray) -> None:
+        a = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+        n = self._count(name)
+        if a.size != n:
+            raise ValueError(f"{name}: expected {n} values, got {a.size}")
+        _check(self._lib.fb_set_array(self.ctx, IDS[name], _dp(a), n), f"fb_set_array({name})")
+
+    def geti(self, name: str) -> np.ndarray:
+        n = {"lmind": 4 * self.nlm, "eulins": 36 * self.nlm}[name]
+        out = np.zeros(n, dtype=np.int32)
+        _check(self._lib.fb_get_iarray(self.ctx, IIDS[name], out.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_int32)), n), f"fb_get_iarray({name})")
+        return out
+
+    def scalars(self) -> dict:
+        s = self.get("scalars")
+        return {k: float(s[i]) for i, k in enumerate(SCALAR_NAMES)}
+
+    def synchronize(self) -> None:
+        _check(self._lib.fb_synchronize(self.ctx), "fb_synchronize")
+
+
+def version() -> str:
+    return lib().fb_version().decode()

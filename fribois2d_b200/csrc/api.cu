@@ -1,0 +1,993 @@
+// C ABI of the B200-native FRiBoIS2D fluid time step (include/fribois2d.h):
+// context set-up, device memory, substep orchestration, CUDA-graph replay.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fribois2d.h"
+#include "device.cuh"
+#include "host.h"
+#include "kernels.h"
+
+using fb::Dev;
+using fb::SubDev;
+using fb::TriDev;
+
+struct fb_host {
+    fb::HostCase hc;
+};
+
+struct fb_ctx {
+    fb::HostCase hc;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t blas = nullptr;
+    Dev d{};
+    SubDev sub[3]{};
+    double usdtal[3] = {0, 0, 0};
+    std::vector<void *> allocs;
+    void *sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int sort_bits = 32;
+    int hist_cap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    double *zmm = nullptr, *zmmt = nullptr;  // Poisson eigenvectors and inverse
+    // host copies of the scalar state the reference keeps in modules
+    double dt = 0, dt_o = 0, beta = 0, al = 0, ga = 0, ro = 0;
+    int cur_ns = 0, cur_n = 1;
+    std::string err;
+};
+
+namespace {
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            std::fprintf(stderr, "fribois2d: %s failed: %s (%s:%d)\n", #call,            \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+            return FB_ERR_CUDA;                                                          \
+        }                                                                                \
+    } while (0)
+#define CB(call)                                                                         \
+    do {                                                                                 \
+        cublasStatus_t s_ = (call);                                                      \
+        if (s_ != CUBLAS_STATUS_SUCCESS) {                                               \
+            std::fprintf(stderr, "fribois2d: %s failed: %d (%s:%d)\n", #call,            \
+                         static_cast<int>(s_), __FILE__, __LINE__);                      \
+            return FB_ERR_CUDA;                                                          \
+        }                                                                                \
+    } while (0)
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+template <class T>
+int dnew(fb_ctx *c, T **p, size_t n) {
+    void *q = nullptr;
+    CK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
+    CK(cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T)));
+    c->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return FB_OK;
+}
+
+template <class T>
+int dup(fb_ctx *c, T **p, const std::vector<T> &v) {
+    int st = dnew(c, p, v.size());
+    if (st) return st;
+    if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return FB_OK;
+}
+
+// tridiagonal system (lower(2:n), diag, upper(1:n-1)) -> device factors
+int upload_tri(fb_ctx *c, TriDev &t, const std::vector<double> &lo, const std::vector<double> &di,
+               const std::vector<double> &up) {
+    fb::TriLU f = fb::factor(lo, di, up);
+    if (f.info != 0) return FB_ERR_NUMERIC;
+    std::vector<double> dinv(f.d.size());
+    for (size_t i = 0; i < f.d.size(); ++i) dinv[i] = 1.0 / f.d[i];
+    t.n = f.n;
+    t.pivoted = f.pivoted ? 1 : 0;
+    double *p;
+    int *ip;
+    int st;
+    if ((st = dup(c, &p, f.dl))) return st;
+    t.dl = p;
+    if ((st = dup(c, &p, dinv))) return st;
+    t.dinv = p;
+    if ((st = dup(c, &p, f.du))) return st;
+    t.du = p;
+    if ((st = dup(c, &p, f.du2))) return st;
+    t.du2 = p;
+    if ((st = dup(c, &ip, f.ipiv))) return st;
+    t.ipiv = ip;
+    return FB_OK;
+}
+
+// solve_fluid.F90: the four Helmholtz systems of one substep, normalised to
+// a unit diagonal exactly as the reference builds them before DGTTRF.
+int build_substep(fb_ctx *c, int n, double al) {
+    const fb::Grid &g = c->hc.grid;
+    SubDev &s = c->sub[n];
+    const int n2 = g.n2, n3 = g.n3, n2m = g.n2m, n3m = g.n3m;
+    s.al = al;
+    s.beta = c->dt / g.ren * 0.5;
+    s.betadx = s.beta * al;
+    const double betadx = s.betadx;
+    std::vector<double> b(static_cast<size_t>(std::max(n2, n3)) + 2, 0.0);
+    int st;
+    double *p;
+    {   // solq2j (solve_fluid.F90:126-153)
+        std::vector<double> am(n2 + 1, 0.0), ap(n2 + 1, 0.0), lo, di(n2, 1.0), up;
+        std::fill(b.begin(), b.end(), 0.0);
+        for (int jc = 2; jc <= n2m; ++jc) {
+            double acjl_b = 1.0 / (1.0 - betadx * g.ac2j[jc]);
+            ap[jc] = -betadx * g.ap2j[jc] * acjl_b;
+            am[jc] = -betadx * g.am2j[jc] * acjl_b;
+            b[jc] = acjl_b;
+        }
+        for (int j = 2; j <= n2; ++j) lo.push_back(am[j]);
+        for (int j = 1; j <= n2 - 1; ++j) up.push_back(ap[j]);
+        if ((st = upload_tri(c, s.y2, lo, di, up))) return st;
+        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
+        s.by2 = p;
+    }
+    {   // solq2k (solve_fluid.F90:185-212)
+        std::vector<double> am(n3m + 1, 0.0), ap(n3m + 1, 0.0), lo, di(n3m, 1.0), up;
+        std::fill(b.begin(), b.end(), 0.0);
+        for (int kc = 1; kc <= n3m; ++kc) {
+            double ackl_b = 1.0 / (1.0 - g.ac3sk[kc] * betadx);
+            am[kc] = -g.am3sk[kc] * betadx * ackl_b;
+            ap[kc] = -g.ap3sk[kc] * betadx * ackl_b;
+            b[kc] = ackl_b;
+        }
+        for (int k = 2; k <= n3m; ++k) lo.push_back(am[k]);
+        for (int k = 1; k <= n3m - 1; ++k) up.push_back(ap[k]);
+        if ((st = upload_tri(c, s.z2, lo, di, up))) return st;
+        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
+        s.bz2 = p;
+        s.ugkks = 1.0 / (g.g3rm[1] * g.g3rc[1]) * g.dx3q * 2.0 * betadx;
+        s.ugkkn = 1.0 / (g.g3rm[n3m] * g.g3rc[n3]) * g.dx3q * 2.0 * betadx;
+    }
+    {   // solq3j (solve_fluid.F90:77-97)
+        std::vector<double> am(n2m + 1, 0.0), ap(n2m + 1, 0.0), lo, di(n2m, 1.0), up;
+        std::fill(b.begin(), b.end(), 0.0);
+        for (int jc = 1; jc <= n2m; ++jc) {
+            double acjl_b = 1.0 / (1.0 - betadx * g.ac3j[jc]);
+            ap[jc] = -betadx * g.ap3j[jc] * acjl_b;
+            am[jc] = -betadx * g.am3j[jc] * acjl_b;
+            b[jc] = acjl_b;
+        }
+        for (int j = 2; j <= n2m; ++j) lo.push_back(am[j]);
+        for (int j = 1; j <= n2m - 1; ++j) up.push_back(ap[j]);
+        if ((st = upload_tri(c, s.y3, lo, di, up))) return st;
+        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
+        s.by3 = p;
+    }
+    {   // solq3k (solve_fluid.F90:260-288)
+        std::vector<double> am(n3 + 1, 0.0), ap(n3 + 1, 0.0), lo, di(n3, 1.0), up;
+        std::fill(b.begin(), b.end(), 0.0);
+        for (int kc = 2; kc <= n3m; ++kc) {
+            double ackl_b = 1.0 / (1.0 - g.ac3sk[kc] * betadx);
+            am[kc] = -g.am3sk[kc] * betadx * ackl_b;
+            ap[kc] = -g.ap3sk[kc] * betadx * ackl_b;
+            b[kc] = ackl_b;
+        }
+        for (int k = 2; k <= n3; ++k) lo.push_back(am[k]);
+        for (int k = 1; k <= n3 - 1; ++k) up.push_back(ap[k]);
+        if ((st = upload_tri(c, s.z3, lo, di, up))) return st;
+        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
+        s.bz3 = p;
+    }
+    c->usdtal[n] = 1.0 / (c->dt * al);
+    return FB_OK;
+}
+
+// phcalc_outflow.F90:34-52: per-mode y systems, factorised once
+int build_poisson(fb_ctx *c) {
+    const fb::Grid &g = c->hc.grid;
+    const int n2m = g.n2m, n3m = g.n3m, ldh = c->d.ldh;
+    const size_t tot = static_cast<size_t>(n3m) * ldh;
+    std::vector<double> pb(tot, 0.0), pdl(tot, 0.0), pdinv(tot, 0.0), pdu(tot, 0.0), pdu2(tot, 0.0);
+    std::vector<int> pipiv(tot, 0), ppiv(static_cast<size_t>(n3m), 0);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+    for (int m = 0; m < n3m; ++m) {
+        const double wrk = c->hc.wr[static_cast<size_t>(m)];
+        std::vector<double> lo(static_cast<size_t>(n2m), 0.0), di(static_cast<size_t>(n2m), 1.0),
+            up(static_cast<size_t>(n2m), 0.0), du2(static_cast<size_t>(n2m), 0.0);
+        std::vector<int> ip(static_cast<size_t>(n2m), 0);
+        const size_t o = static_cast<size_t>(m) * ldh;
+        for (int j = 1; j <= n2m; ++j) {
+            double acphT_b = 1.0 / (g.acphj[j] + wrk);
+            pb[o + j - 1] = acphT_b;
+            if (j >= 2) lo[static_cast<size_t>(j - 2)] = g.amphj[j] * acphT_b;
+            if (j <= n2m - 1) up[static_cast<size_t>(j - 1)] = g.apphj[j] * acphT_b;
+        }
+        if (fb::dgttrf(n2m, lo.data(), di.data(), up.data(), du2.data(), ip.data()) != 0) ++bad;
+        for (int j = 0; j < n2m; ++j) {
+            pdinv[o + j] = 1.0 / di[static_cast<size_t>(j)];
+            pipiv[o + j] = ip[static_cast<size_t>(j)];
+            if (ip[static_cast<size_t>(j)] != j + 1) ppiv[static_cast<size_t>(m)] = 1;
+            if (j < n2m - 1) {
+                pdl[o + j] = lo[static_cast<size_t>(j)];
+                pdu[o + j] = up[static_cast<size_t>(j)];
+            }
+            if (j < n2m - 2) pdu2[o + j] = du2[static_cast<size_t>(j)];
+        }
+    }
+    if (bad) return FB_ERR_NUMERIC;
+    int st;
+    double *p;
+    int *ip;
+    Dev &d = c->d;
+    if ((st = dup(c, &p, pb))) return st;
+    d.pb = p;
+    if ((st = dup(c, &p, pdl))) return st;
+    d.pdl = p;
+    if ((st = dup(c, &p, pdinv))) return st;
+    d.pdinv = p;
+    if ((st = dup(c, &p, pdu))) return st;
+    d.pdu = p;
+    if ((st = dup(c, &p, pdu2))) return st;
+    d.pdu2 = p;
+    if ((st = dup(c, &ip, pipiv))) return st;
+    d.pipiv = ip;
+    if ((st = dup(c, &ip, ppiv))) return st;
+    d.ppiv = ip;
+    return FB_OK;
+}
+
+int create_impl(const char *dir, int device, fb_ctx *c) {
+    std::string err = fb::setup_case(dir, c->hc);
+    if (!err.empty()) {
+        c->err = err;
+        std::fprintf(stderr, "fribois2d: %s\n", err.c_str());
+        return FB_ERR_INPUT;
+    }
+    const fb::Deck &dk = c->hc.deck;
+    const fb::Grid &g = c->hc.grid;
+    if (!dk.idtv) {
+        std::fprintf(stderr, "fribois2d: variable time step (idtv = .false.) is not supported on the device path\n");
+        return FB_ERR_UNSUPPORTED;
+    }
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    CB(cublasCreate(&c->blas));
+    CB(cublasSetStream(c->blas, c->stream));
+    CB(cublasSetPointerMode(c->blas, CUBLAS_POINTER_MODE_HOST));
+    {   // a fixed workspace keeps cuBLAS from allocating inside graph capture
+        void *ws = nullptr;
+        CK(cudaMalloc(&ws, 32u << 20));
+        c->allocs.push_back(ws);
+        CB(cublasSetWorkspace(c->blas, ws, 32u << 20));
+    }
+
+    Dev &d = c->d;
+    d.n2 = g.n2;
+    d.n3 = g.n3;
+    d.n2m = g.n2m;
+    d.n3m = g.n3m;
+    d.P = round_up(g.n2, 32);
+    d.NK = g.n3 + 1;
+    d.ldh = round_up(g.n2m, 32);
+    d.nlm = dk.ibact ? dk.nlm : 0;
+    d.nsst = dk.nsst;
+    d.wfun = dk.wfun;
+    d.dx2 = g.dx2;
+    d.dx3 = g.dx3;
+    d.dx2q = g.dx2q;
+    d.dx3q = g.dx3q;
+    d.ren = g.ren;
+    d.visc = dk.visc;
+    d.dt = dk.dt;
+    d.cou = dk.cou;
+    d.q3uw = dk.q3uw;
+    d.q3lw = dk.q3lw;
+    d.rext2 = dk.rext2;
+    d.alx3 = dk.alx3;
+    d.radiusSD = dk.radiusSD;
+    d.kprobe = dk.kprobe;
+    d.ddmin = g.ddmin;
+    d.cfllim = dk.cfllim;
+    {   // iobcs.F90:54-59: the outflow section area (constant)
+        double area = 0.0;
+        for (int j = 1; j <= g.n2m; ++j) area = area + g.g2rm[j] / g.dx2;
+        d.area_out = area;
+    }
+    c->dt = dk.dt;
+    c->dt_o = dk.dt;
+    int st;
+    double *p;
+    int *ip;
+#define UP1(name)                                           \
+    if ((st = dup(c, &p, g.name))) return st;               \
+    d.name = p;
+#define UPI(name)                                           \
+    if ((st = dup(c, &ip, g.name))) return st;              \
+    d.name = ip;
+    UP1(rc) UP1(rm) UP1(zz) UP1(zm) UP1(g2rc) UP1(g2rm) UP1(g3rc) UP1(g3rm)
+    UP1(udx2c) UP1(udx2m) UP1(udx3c) UP1(udx3m)
+    UPI(jmv) UPI(jpv) UPI(kmv) UPI(kpv)
+    UP1(am2j) UP1(ac2j) UP1(ap2j) UP1(am3j) UP1(ac3j) UP1(ap3j)
+    UP1(am3ck) UP1(ac3ck) UP1(ap3ck) UP1(am3sk) UP1(ac3sk) UP1(ap3sk)
+    UP1(amphj) UP1(acphj) UP1(apphj) UP1(amphk) UP1(acphk) UP1(apphk)
+#undef UP1
+#undef UPI
+
+    const size_t nf = static_cast<size_t>(d.NK) * d.P;
+    double **fields[] = {&d.q2, &d.q3, &d.pr, &d.dph, &d.rhs2, &d.rhs3, &d.ru2, &d.ru3};
+    for (double **f : fields)
+        if ((st = dnew(c, f, nf))) return st;
+    if ((st = dnew(c, &d.hmn, static_cast<size_t>(d.n3m) * d.ldh))) return st;
+    {   // inqpr (initial_sol.F90:268-296): q2 = 0, q3 = velin = 1, pr = 0
+        std::vector<double> one(nf, 0.0);
+        for (int k = 0; k <= g.n3; ++k)
+            for (int j = 1; j <= g.n2; ++j) one[fb::fidx(d, j, k)] = 1.0;
+        CK(cudaMemcpy(d.q3, one.data(), nf * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    double **bnd[] = {&d.qb2s, &d.qb2n, &d.dqb2s, &d.dqb2n, &d.qb3s, &d.qb3n, &d.dqb3s, &d.dqb3n, &d.dq2x2o, &d.dq3x2o};
+    for (double **b : bnd)
+        if ((st = dnew(c, b, static_cast<size_t>(g.n2) + 2))) return st;
+    {
+        std::vector<double> v(static_cast<size_t>(g.n2) + 2, 0.0);
+        for (int j = 1; j <= g.n2m; ++j) v[j] = 1.0;
+        CK(cudaMemcpy(d.qb3s, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.qb3n, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    const size_t nlm = static_cast<size_t>(std::max(d.nlm, 1));
+    if ((st = dup(c, &d.lmcc, c->hc.lmcc))) return st;
+    if ((st = dup(c, &d.lmvel, c->hc.lmvel))) return st;
+    if ((st = dup(c, &d.lmacc, c->hc.lmacc))) return st;
+    if ((st = dup(c, &d.lmnor, c->hc.lmnor))) return st;
+    if ((st = dup(c, &d.lmA, c->hc.lmA))) return st;
+    if ((st = dup(c, &d.vert, c->hc.vert))) return st;
+    if ((st = dnew(c, &d.lmind, nlm * 4))) return st;
+    if ((st = dnew(c, &d.eulins, nlm * 2 * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.phi, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.cl, nlm * 2))) return st;
+    if ((st = dnew(c, &d.contrib, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.skey_in, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.sval_in, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.skey, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.sval, nlm * 2 * fb::kSD))) return st;
+    if ((st = dnew(c, &d.probe, nlm * 24))) return st;
+    if ((st = dnew(c, &d.press, nlm))) return st;
+    if ((st = dnew(c, &d.tau, nlm * 2))) return st;
+    if ((st = dnew(c, &d.bcerrv, nlm))) return st;
+    if ((st = dnew(c, &d.bcerrw, nlm))) return st;
+    if ((st = dnew(c, &d.rigid, 18))) return st;
+    CK(cudaMemcpy(d.rigid, c->hc.rigid, 18 * sizeof(double), cudaMemcpyHostToDevice));
+    if ((st = dnew(c, &d.forces, 8))) return st;
+    if ((st = dnew(c, &d.scal, fb::S_COUNT))) return st;
+    c->hist_cap = 4096;
+    if ((st = dnew(c, &d.hist, static_cast<size_t>(c->hist_cap) * FB_HIST_COLS))) return st;
+    if ((st = dnew(c, &d.red, static_cast<size_t>(3) * fb::kRedSlot))) return st;
+    if ((st = dnew(c, &d.count, 4))) return st;
+    if ((st = dnew(c, &d.status, 1))) return st;
+    const size_t gridblocks = static_cast<size_t>((d.n2m + 31) / 32) * ((d.n3m + 7) / 8);
+    if (gridblocks > static_cast<size_t>(fb::kRedSlot)) return FB_ERR_UNSUPPORTED;
+    d.rbden = dk.rbden;
+    d.rba0 = dk.rba[0];
+    d.rba1 = dk.rba[1];
+    d.cmposi0 = dk.cmposi[0];
+    d.cmposi1 = dk.cmposi[1];
+    d.cmroti = dk.cmroti;
+    d.rbgravF0 = dk.rbgravF[0];
+    d.rbgravF1 = dk.rbgravF[1];
+    d.rrr = dk.rrr;
+    for (int i = 0; i < 3; ++i) {
+        d.kk[i] = dk.kk[i];
+        d.kk3[i] = dk.kk3[i];
+        d.cc[i] = dk.cc[i];
+        d.rbmcon[i] = dk.rbmcon[i];
+    }
+    for (int i = 0; i < 9; ++i) d.kinori[i] = c->hc.kinori[i];
+    d.rtcoup = dk.rtcoup ? 1 : 0;
+
+    for (int n = 0; n < dk.nsst; ++n) {
+        double al = (dk.nsst == 3) ? c->hc.alm[n] : 1.0;
+        if ((st = build_substep(c, n, al))) return st;
+    }
+    c->beta = c->dt / g.ren * 0.5;
+    if ((st = build_poisson(c))) return st;
+    if ((st = dup(c, &c->zmm, c->hc.zmm))) return st;
+    if ((st = dup(c, &c->zmmt, c->hc.zmmt))) return st;
+    c->sort_bits = 1;
+    while ((static_cast<uint64_t>(1) << c->sort_bits) < static_cast<uint64_t>(2) * nf + 1) ++c->sort_bits;
+    if (d.nlm) {
+        int nitems = 2 * d.nlm * fb::kSD;
+        cub::DeviceRadixSort::SortPairs(nullptr, c->sort_tmp_bytes, d.skey_in, d.skey, d.sval_in, d.sval,
+                                        nitems, 0, c->sort_bits, c->stream);
+        CK(cudaMalloc(&c->sort_tmp, std::max<size_t>(c->sort_tmp_bytes, 16)));
+        c->allocs.push_back(c->sort_tmp);
+    }
+    CK(cudaDeviceSynchronize());
+    return FB_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// substep coefficients (fluid_tsch.F90:64-77)
+void coefs(const fb_ctx *c, int ns, int n, double &al, double &ga, double &ro) {
+    if (c->hc.deck.nsst == 3) {
+        al = c->hc.alm[n - 1];
+        ga = c->hc.gam[n - 1];
+        ro = c->hc.rom[n - 1];
+    } else {
+        if (ns == 0) {
+            ga = 1.0;
+            ro = 0.0;
+        } else {
+            ga = 1.0 + 0.5 * c->dt / c->dt_o;
+            ro = -0.5 * c->dt / c->dt_o;
+        }
+        al = ga + ro;
+    }
+}
+
+int gemm_fwd(fb_ctx *c) {   // phcalc_outflow.F90:31, hmn = dph * zmmt^T
+    const Dev &d = c->d;
+    const double one = 1.0, zero = 0.0;
+    CB(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, d.dph + d.P, d.P,
+                   c->zmmt, d.n3m, &zero, d.hmn, d.ldh));
+    return FB_OK;
+}
+
+int gemm_bwd(fb_ctx *c) {   // phcalc_outflow.F90:61,65-69, dph = vmn * zmm^T
+    const Dev &d = c->d;
+    const double one = 1.0, zero = 0.0;
+    CB(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, d.hmn, d.ldh, c->zmm,
+                   d.n3m, &zero, d.dph + d.P, d.P));
+    return FB_OK;
+}
+
+int run_sort(fb_ctx *c) {
+    const Dev &d = c->d;
+    const int nitems = 2 * d.nlm * fb::kSD;
+    size_t bytes = c->sort_tmp_bytes;
+    if (cub::DeviceRadixSort::SortPairs(c->sort_tmp, bytes, d.skey_in, d.skey, d.sval_in, d.sval, nitems, 0,
+                                        c->sort_bits, c->stream) != cudaSuccess)
+        return FB_ERR_CUDA;
+    return FB_OK;
+}
+
+int stage_impl(fb_ctx *c, int stage, int ns, int n) {
+    double al, ga, ro;
+    coefs(c, ns, n, al, ga, ro);
+    c->al = al;
+    c->ga = ga;
+    c->ro = ro;
+    const Dev &d = c->d;
+    const SubDev &s = c->sub[n - 1];
+    cudaStream_t st = c->stream;
+    int r = FB_OK;
+    switch (stage) {
+    case FB_ST_CFL: fb::launch_cfl(d, st); break;
+    case FB_ST_BOUCDQ: fb::launch_boucdq(d, ga, ro, st); break;
+    case FB_ST_NL_RHS: fb::launch_nl_rhs(d, al, ga, ro, st); break;
+    case FB_ST_LGRDIST: fb::launch_lgrdist(d, st); break;
+    case FB_ST_FORCING:
+        if (!d.nlm) break;
+        if (n == 1) {
+            fb::launch_mls_setup(d, st);
+            if ((r = run_sort(c))) return r;
+        }
+        fb::launch_mls_interp(d, st);
+        fb::launch_mls_spread(d, st);
+        break;
+    case FB_ST_HELSOLVE: fb::launch_helsolve(d, s, st); break;
+    case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
+    case FB_ST_PHCALC:
+        if ((r = gemm_fwd(c))) return r;
+        fb::launch_tri_poisson(d, st);
+        if ((r = gemm_bwd(c))) return r;
+        break;
+    case FB_ST_UPDVP: fb::launch_updvp_prcalc(d, al, al * c->beta, st); break;
+    case FB_ST_PRSUBMEAN: fb::launch_submean_boucqt(d, st); break;
+    case FB_ST_CHECKBCS:
+    case FB_ST_LOADS: fb::launch_loads(d, st); break;
+    case FB_ST_RIGID: fb::launch_rigid(d, c->hist_cap, st); break;
+    default: return FB_ERR_STATE;
+    }
+    if (cudaGetLastError() != cudaSuccess) return FB_ERR_CUDA;
+    return FB_OK;
+}
+
+// fluid_tsch.F90:30-182 enqueued on the context stream (no host sync)
+int enqueue_fluid(fb_ctx *c, int ns) {
+    const Dev &d = c->d;
+    int r;
+    if ((r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
+    c->beta = c->dt / c->hc.grid.ren * 0.5;
+    for (int n = 1; n <= d.nsst; ++n) {
+        if ((r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_NL_RHS, ns, n))) return r;
+        if (d.nlm) {
+            if (n == 1 && (r = stage_impl(c, FB_ST_LGRDIST, ns, n))) return r;
+            if ((r = stage_impl(c, FB_ST_FORCING, ns, n))) return r;
+        }
+        if ((r = stage_impl(c, FB_ST_HELSOLVE, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_PHCALC, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_UPDVP, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_PRSUBMEAN, ns, n))) return r;
+    }
+    if (d.nlm && c->hc.deck.cbody && (r = stage_impl(c, FB_ST_LOADS, ns, 1))) return r;
+    return FB_OK;
+}
+
+int enqueue_step(fb_ctx *c, int ns) {
+    int r = enqueue_fluid(c, ns);
+    if (r) return r;
+    if (c->d.nlm) return stage_impl(c, FB_ST_RIGID, ns, 1);
+    return FB_OK;
+}
+
+int read_status(fb_ctx *c, int *status) {
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(status, c->d.status, sizeof(int), cudaMemcpyDeviceToHost));
+    return FB_OK;
+}
+
+// advances the host clock the way main.F90:92,96 does
+void host_clock(fb_ctx *c, int nsteps) {
+    for (int i = 0; i < nsteps; ++i) c->dt_o = c->dt;
+}
+
+int capture_step(fb_ctx *c) {
+    if (c->graph_exec) return FB_OK;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int r = enqueue_step(c, 1);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return FB_ERR_CUDA;
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->graph_exec, g, 0));
+    return FB_OK;
+}
+
+// field (j, k) <-> host (k, j) dense copies
+int field_ptr(fb_ctx *c, int id, double **p) {
+    Dev &d = c->d;
+    switch (id) {
+    case FB_Q2: *p = d.q2; return FB_OK;
+    case FB_Q3: *p = d.q3; return FB_OK;
+    case FB_PR: *p = d.pr; return FB_OK;
+    case FB_DPH: *p = d.dph; return FB_OK;
+    case FB_RHS2: *p = d.rhs2; return FB_OK;
+    case FB_RHS3: *p = d.rhs3; return FB_OK;
+    case FB_RU2: *p = d.ru2; return FB_OK;
+    case FB_RU3: *p = d.ru3; return FB_OK;
+    }
+    return FB_ERR_STATE;
+}
+
+// 1-based device vectors and plain marker arrays
+int vec_ptr(fb_ctx *c, int id, double **p, int64_t *n, bool *one_based) {
+    Dev &d = c->d;
+    const int64_t n2 = d.n2, n3 = d.n3, nlm = d.nlm, n3m = d.n3m;
+    *one_based = true;
+    switch (id) {
+    case FB_QB2S: *p = d.qb2s; *n = n2; return FB_OK;
+    case FB_QB2N: *p = d.qb2n; *n = n2; return FB_OK;
+    case FB_DQB2S: *p = d.dqb2s; *n = n2; return FB_OK;
+    case FB_DQB2N: *p = d.dqb2n; *n = n2; return FB_OK;
+    case FB_QB3S: *p = d.qb3s; *n = n2; return FB_OK;
+    case FB_QB3N: *p = d.qb3n; *n = n2; return FB_OK;
+    case FB_DQB3S: *p = d.dqb3s; *n = n2; return FB_OK;
+    case FB_DQB3N: *p = d.dqb3n; *n = n2; return FB_OK;
+    case FB_DQ2X2O: *p = d.dq2x2o; *n = n2; return FB_OK;
+    case FB_DQ3X2O: *p = d.dq3x2o; *n = n2; return FB_OK;
+    case FB_RC: *p = const_cast<double *>(d.rc); *n = n2; return FB_OK;
+    case FB_RM: *p = const_cast<double *>(d.rm); *n = n2; return FB_OK;
+    case FB_ZZ: *p = const_cast<double *>(d.zz); *n = n3; return FB_OK;
+    case FB_ZM: *p = const_cast<double *>(d.zm); *n = n3; return FB_OK;
+    case FB_UDX2C: *p = const_cast<double *>(d.udx2c); *n = n2; return FB_OK;
+    case FB_UDX2M: *p = const_cast<double *>(d.udx2m); *n = n2; return FB_OK;
+    case FB_UDX3C: *p = const_cast<double *>(d.udx3c); *n = n3; return FB_OK;
+    case FB_UDX3M: *p = const_cast<double *>(d.udx3m); *n = n3; return FB_OK;
+    case FB_AMPHJ: *p = const_cast<double *>(d.amphj); *n = n2; return FB_OK;
+    case FB_ACPHJ: *p = const_cast<double *>(d.acphj); *n = n2; return FB_OK;
+    case FB_APPHJ: *p = const_cast<double *>(d.apphj); *n = n2; return FB_OK;
+    case FB_AMPHK: *p = const_cast<double *>(d.amphk); *n = n3; return FB_OK;
+    case FB_ACPHK: *p = const_cast<double *>(d.acphk); *n = n3; return FB_OK;
+    case FB_APPHK: *p = const_cast<double *>(d.apphk); *n = n3; return FB_OK;
+    }
+    *one_based = false;
+    switch (id) {
+    case FB_ZMM: *p = c->zmm; *n = n3m * n3m; return FB_OK;
+    case FB_ZMMT: *p = c->zmmt; *n = n3m * n3m; return FB_OK;
+    case FB_LMCC: *p = d.lmcc; *n = 2 * nlm; return FB_OK;
+    case FB_LMVEL: *p = d.lmvel; *n = 2 * nlm; return FB_OK;
+    case FB_LMACC: *p = d.lmacc; *n = 2 * nlm; return FB_OK;
+    case FB_LMNOR: *p = d.lmnor; *n = 2 * nlm; return FB_OK;
+    case FB_LMA: *p = d.lmA; *n = nlm; return FB_OK;
+    case FB_VERT: *p = d.vert; *n = 2 * (nlm + 1); return FB_OK;
+    case FB_PHI: *p = d.phi; *n = 18 * nlm; return FB_OK;
+    case FB_CL: *p = d.cl; *n = 2 * nlm; return FB_OK;
+    case FB_PRESS: *p = d.press; *n = nlm; return FB_OK;
+    case FB_TAU: *p = d.tau; *n = 2 * nlm; return FB_OK;
+    case FB_BCERRV: *p = d.bcerrv; *n = nlm; return FB_OK;
+    case FB_BCERRW: *p = d.bcerrw; *n = nlm; return FB_OK;
+    case FB_RIGID: *p = d.rigid; *n = 18; return FB_OK;
+    case FB_FORCES: *p = d.forces; *n = 8; return FB_OK;
+    }
+    return FB_ERR_STATE;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+const char *fb_version(void) { return "fribois2d_b200 0.1 (sm_100a)"; }
+
+const char *fb_status_string(int status) {
+    switch (status) {
+    case FB_OK: return "ok";
+    case FB_ERR_CFL: return "CFL number above cfllim (fluid_tsch.F90:51-54)";
+    case FB_ERR_MLS: return "MLS partition of unity violated (MLSint.F90:157-163)";
+    case FB_ERR_MARKER_OUT: return "Lagrangian marker outside the grid (lgrdistribution.F90:217-221)";
+    case FB_ERR_INPUT: return "malformed or missing input deck";
+    case FB_ERR_CUDA: return "CUDA runtime or cuBLAS failure";
+    case FB_ERR_STATE: return "invalid argument for this context";
+    case FB_ERR_UNSUPPORTED: return "deck option not supported on the device path";
+    case FB_ERR_NUMERIC: return "singular set-up system or non-finite value";
+    }
+    return "unknown status";
+}
+
+int fb_create(const char *input_dir, int device, fb_ctx **out) {
+    if (!input_dir || !out) return FB_ERR_STATE;
+    *out = nullptr;
+    fb_ctx *c = new (std::nothrow) fb_ctx();
+    if (!c) return FB_ERR_STATE;
+    int r = create_impl(input_dir, device, c);
+    if (r) {
+        fb_destroy(c);
+        return r;
+    }
+    *out = c;
+    return FB_OK;
+}
+
+int fb_destroy(fb_ctx *c) {
+    if (!c) return FB_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    for (void *p : c->allocs)
+        if (p) cudaFree(p);
+    if (c->blas) cublasDestroy(c->blas);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return FB_OK;
+}
+
+int fb_fluid_tsch(fb_ctx *c, int ns) {
+    if (!c) return FB_ERR_STATE;
+    int r = enqueue_fluid(c, ns);
+    if (r) return r;
+    int status = 0;
+    if ((r = read_status(c, &status))) return r;
+    return status;
+}
+
+int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
+    if (!c) return FB_ERR_STATE;
+    int r = stage_impl(c, FB_ST_RIGID, ns, 1);
+    if (r) return r;
+    if (forcecomp) CK(cudaMemcpyAsync(forcecomp, c->d.forces, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    int status = 0;
+    if ((r = read_status(c, &status))) return r;
+    host_clock(c, 1);
+    return status;
+}
+
+int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
+    if (!c || nsteps < 0) return FB_ERR_STATE;
+    if (!c->d.nlm) return FB_ERR_UNSUPPORTED;
+    int r, status = 0, done = 0;
+    // the first Adams-Bashforth step has its own coefficients: run it eagerly
+    if (c->hc.deck.nsst == 1 && ns0 == 0 && nsteps > 0) {
+        CK(cudaEventRecord(c->ev0, c->stream));
+        if ((r = enqueue_step(c, 0))) return r;
+        CK(cudaEventRecord(c->ev1, c->stream));
+        if ((r = read_status(c, &status))) return r;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        c->last_ms = ms;
+        if (hist) {
+            double row0;
+            CK(cudaMemcpy(&row0, c->d.scal + fb::S_STEP, sizeof(double), cudaMemcpyDeviceToHost));
+            int row = (static_cast<int>(row0) - 1 + c->hist_cap) % c->hist_cap;
+            CK(cudaMemcpy(hist, c->d.hist + static_cast<size_t>(row) * FB_HIST_COLS, FB_HIST_COLS * sizeof(double),
+                          cudaMemcpyDeviceToHost));
+        }
+        host_clock(c, 1);
+        if (status) return status;
+        done = 1;
+    } else {
+        c->last_ms = 0.0;
+    }
+    if ((r = capture_step(c))) return r;
+    while (done < nsteps) {
+        const int chunk = std::min(nsteps - done, c->hist_cap);
+        double row0;
+        CK(cudaMemcpyAsync(&row0, c->d.scal + fb::S_STEP, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->ev0, c->stream));
+        for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(c->graph_exec, c->stream));
+        CK(cudaEventRecord(c->ev1, c->stream));
+        if ((r = read_status(c, &status))) return r;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->last_ms += ms;
+        if (hist) {
+            for (int i = 0; i < chunk; ++i) {
+                int row = (static_cast<int>(row0) + i) % c->hist_cap;
+                CK(cudaMemcpy(hist + static_cast<size_t>(done + i) * FB_HIST_COLS,
+                              c->d.hist + static_cast<size_t>(row) * FB_HIST_COLS, FB_HIST_COLS * sizeof(double),
+                              cudaMemcpyDeviceToHost));
+            }
+        }
+        host_clock(c, chunk);
+        done += chunk;
+        if (status) return status;
+    }
+    return FB_OK;
+}
+
+int fb_get_loads(fb_ctx *c, double *press, double *tau) {
+    if (!c) return FB_ERR_STATE;
+    const size_t nlm = static_cast<size_t>(c->d.nlm);
+    if (press) CK(cudaMemcpyAsync(press, c->d.press, nlm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (tau) CK(cudaMemcpyAsync(tau, c->d.tau, 2 * nlm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FB_OK;
+}
+
+int fb_set_markers(fb_ctx *c, const double *lmcc, const double *lmvel, const double *lmacc, const double *lmnor) {
+    if (!c) return FB_ERR_STATE;
+    const size_t b = 2 * static_cast<size_t>(c->d.nlm) * sizeof(double);
+    if (lmcc) CK(cudaMemcpyAsync(c->d.lmcc, lmcc, b, cudaMemcpyHostToDevice, c->stream));
+    if (lmvel) CK(cudaMemcpyAsync(c->d.lmvel, lmvel, b, cudaMemcpyHostToDevice, c->stream));
+    if (lmacc) CK(cudaMemcpyAsync(c->d.lmacc, lmacc, b, cudaMemcpyHostToDevice, c->stream));
+    if (lmnor) CK(cudaMemcpyAsync(c->d.lmnor, lmnor, b, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FB_OK;
+}
+
+int fb_get_dims(fb_ctx *c, int32_t dims[8]) {
+    if (!c || !dims) return FB_ERR_STATE;
+    dims[0] = c->d.n2;
+    dims[1] = c->d.n3;
+    dims[2] = c->d.nlm;
+    dims[3] = c->d.nsst;
+    dims[4] = c->d.P;
+    dims[5] = c->d.ldh;
+    dims[6] = c->sub[0].y2.pivoted | (c->sub[0].z3.pivoted << 1);
+    dims[7] = 0;
+    return FB_OK;
+}
+
+int fb_get_array(fb_ctx *c, int id, double *host, int64_t n) {
+    if (!c || !host) return FB_ERR_STATE;
+    Dev &d = c->d;
+    double *p = nullptr;
+    CK(cudaStreamSynchronize(c->stream));
+    if (field_ptr(c, id, &p) == FB_OK) {
+        if (n != static_cast<int64_t>(d.NK) * d.n2) return FB_ERR_STATE;
+        CK(cudaMemcpy2D(host, d.n2 * sizeof(double), p, d.P * sizeof(double), d.n2 * sizeof(double), d.NK,
+                        cudaMemcpyDeviceToHost));
+        return FB_OK;
+    }
+    if (id == FB_SCALARS) {
+        if (n != 13) return FB_ERR_STATE;
+        double s[fb::S_COUNT];
+        CK(cudaMemcpy(s, d.scal, sizeof(s), cudaMemcpyDeviceToHost));
+        const double v[13] = {s[fb::S_TIME], c->dt, c->dt_o, c->beta, c->al, c->ga, c->ro, s[fb::S_CFLM],
+                              s[fb::S_Q3AVG], s[fb::S_NBCV], s[fb::S_NBCW], d.ddmin, s[fb::S_PRAVG]};
+        std::memcpy(host, v, sizeof(v));
+        return FB_OK;
+    }
+    if (id == FB_WR) {
+        if (n != d.n3m) return FB_ERR_STATE;
+        std::memcpy(host, c->hc.wr.data(), static_cast<size_t>(n) * sizeof(double));
+        return FB_OK;
+    }
+    int64_t cnt = 0;
+    bool one_based = false;
+    if (vec_ptr(c, id, &p, &cnt, &one_based) != FB_OK || n != cnt) return FB_ERR_STATE;
+    CK(cudaMemcpy(host, p + (one_based ? 1 : 0), static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost));
+    return FB_OK;
+}
+
+int fb_set_array(fb_ctx *c, int id, const double *host, int64_t n) {
+    if (!c || !host) return FB_ERR_STATE;
+    Dev &d = c->d;
+    double *p = nullptr;
+    CK(cudaStreamSynchronize(c->stream));
+    if (field_ptr(c, id, &p) == FB_OK) {
+        if (n != static_cast<int64_t>(d.NK) * d.n2) return FB_ERR_STATE;
+        CK(cudaMemcpy2D(p, d.P * sizeof(double), host, d.n2 * sizeof(double), d.n2 * sizeof(double), d.NK,
+                        cudaMemcpyHostToDevice));
+        return FB_OK;
+    }
+    if (id == FB_WR || id == FB_ZMM || id == FB_ZMMT) return FB_ERR_STATE;  // set-up data is immutable
+    int64_t cnt = 0;
+    bool one_based = false;
+    if (vec_ptr(c, id, &p, &cnt, &one_based) != FB_OK || n != cnt) return FB_ERR_STATE;
+    if (one_based && id >= FB_RC) return FB_ERR_STATE;  // grid data is immutable
+    CK(cudaMemcpy(p + (one_based ? 1 : 0), host, static_cast<size_t>(n) * sizeof(double), cudaMemcpyHostToDevice));
+    return FB_OK;
+}
+
+int fb_get_iarray(fb_ctx *c, int id, int32_t *host, int64_t n) {
+    if (!c || !host) return FB_ERR_STATE;
+    CK(cudaStreamSynchronize(c->stream));
+    const int64_t nlm = c->d.nlm;
+    if (id == FB_LMIND && n == 4 * nlm) {
+        CK(cudaMemcpy(host, c->d.lmind, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost));
+        return FB_OK;
+    }
+    if (id == FB_EULINS && n == 36 * nlm) {
+        CK(cudaMemcpy(host, c->d.eulins, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost));
+        return FB_OK;
+    }
+    return FB_ERR_STATE;
+}
+
+int fb_synchronize(fb_ctx *c) {
+    if (!c) return FB_ERR_STATE;
+    int status = 0;
+    int r = read_status(c, &status);
+    return r ? r : status;
+}
+
+int fb_set_substep(fb_ctx *c, int ns, int n) {
+    if (!c || n < 1 || n > c->d.nsst) return FB_ERR_STATE;
+    c->cur_ns = ns;
+    c->cur_n = n;
+    double al, ga, ro;
+    coefs(c, ns, n, al, ga, ro);
+    c->al = al;
+    c->ga = ga;
+    c->ro = ro;
+    c->beta = c->dt / c->hc.grid.ren * 0.5;
+    return FB_OK;
+}
+
+int fb_stage(fb_ctx *c, int stage, int n) {
+    if (!c || n < 1 || n > c->d.nsst) return FB_ERR_STATE;
+    int r = stage_impl(c, stage, c->cur_ns, n);
+    if (r) return r;
+    int status = 0;
+    if ((r = read_status(c, &status))) return r;
+    return status;
+}
+
+int fb_last_advance_ms(fb_ctx *c, double *ms) {
+    if (!c || !ms) return FB_ERR_STATE;
+    *ms = c->last_ms;
+    return FB_OK;
+}
+
+// ---- host-only set-up -------------------------------------------------------
+
+int fb_host_create(const char *input_dir, fb_host **out) {
+    if (!input_dir || !out) return FB_ERR_STATE;
+    fb_host *h = new (std::nothrow) fb_host();
+    if (!h) return FB_ERR_STATE;
+    std::string err = fb::setup_case(input_dir, h->hc);
+    if (!err.empty()) {
+        std::fprintf(stderr, "fribois2d: %s\n", err.c_str());
+        delete h;
+        *out = nullptr;
+        return FB_ERR_INPUT;
+    }
+    *out = h;
+    return FB_OK;
+}
+
+int fb_host_destroy(fb_host *h) {
+    delete h;
+    return FB_OK;
+}
+
+int fb_host_dims(fb_host *h, int32_t dims[8]) {
+    if (!h || !dims) return FB_ERR_STATE;
+    const fb::HostCase &hc = h->hc;
+    dims[0] = hc.grid.n2;
+    dims[1] = hc.grid.n3;
+    dims[2] = hc.deck.nlm;
+    dims[3] = hc.deck.nsst;
+    dims[4] = hc.deck.idtv ? 1 : 0;
+    dims[5] = hc.deck.ibact ? 1 : 0;
+    dims[6] = hc.deck.wfun;
+    dims[7] = hc.deck.forst;
+    return FB_OK;
+}
+
+int fb_host_array(fb_host *h, int id, double *out, int64_t n) {
+    if (!h || !out) return FB_ERR_STATE;
+    const fb::HostCase &hc = h->hc;
+    const fb::Grid &g = hc.grid;
+    const std::vector<double> *v = nullptr;
+    bool one_based = true;
+    switch (id) {
+    case FB_RC: v = &g.rc; break;
+    case FB_RM: v = &g.rm; break;
+    case FB_ZZ: v = &g.zz; break;
+    case FB_ZM: v = &g.zm; break;
+    case FB_UDX2C: v = &g.udx2c; break;
+    case FB_UDX2M: v = &g.udx2m; break;
+    case FB_UDX3C: v = &g.udx3c; break;
+    case FB_UDX3M: v = &g.udx3m; break;
+    case FB_AMPHJ: v = &g.amphj; break;
+    case FB_ACPHJ: v = &g.acphj; break;
+    case FB_APPHJ: v = &g.apphj; break;
+    case FB_AMPHK: v = &g.amphk; break;
+    case FB_ACPHK: v = &g.acphk; break;
+    case FB_APPHK: v = &g.apphk; break;
+    default: one_based = false;
+    }
+    if (one_based) {
+        const int64_t cnt = static_cast<int64_t>(v->size()) - 2;
+        if (n != cnt) return FB_ERR_STATE;
+        std::memcpy(out, v->data() + 1, static_cast<size_t>(n) * sizeof(double));
+        return FB_OK;
+    }
+    switch (id) {
+    case FB_WR: v = &hc.wr; break;
+    case FB_ZMM: v = &hc.zmm; break;
+    case FB_ZMMT: v = &hc.zmmt; break;
+    case FB_LMCC: v = &hc.lmcc; break;
+    case FB_LMVEL: v = &hc.lmvel; break;
+    case FB_LMACC: v = &hc.lmacc; break;
+    case FB_LMNOR: v = &hc.lmnor; break;
+    case FB_LMA: v = &hc.lmA; break;
+    case FB_VERT: v = &hc.vert; break;
+    case FB_RIGID:
+        if (n != 18) return FB_ERR_STATE;
+        std::memcpy(out, hc.rigid, sizeof(hc.rigid));
+        return FB_OK;
+    default: return FB_ERR_STATE;
+    }
+    if (n != static_cast<int64_t>(v->size())) return FB_ERR_STATE;
+    std::memcpy(out, v->data(), static_cast<size_t>(n) * sizeof(double));
+    return FB_OK;
+}
+
+int fb_eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr, double *zmm,
+                     double *zmmt) {
+    if (n < 1 || !am || !ac || !ap || !wr || !zmm || !zmmt) return FB_ERR_STATE;
+    return fb::eigen_tridiag(n, am, ac, ap, wr, zmm, zmmt) ? FB_ERR_NUMERIC : FB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1145 @@
+// CUDA kernels of the FRiBoIS2D fluid time step (sm_100a, FP64).
+//
+// This translation unit is compiled with -fmad=false: every expression keeps
+// the reference's left-to-right evaluation without fused multiply-adds, so
+// the stencil stages reproduce the CPU restatement bit for bit.  Each kernel
+// cites the reference routine it implements.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "device.cuh"
+#include "kernels.h"
+#include "../../include/fribois2d.h"
+
+namespace fb {
+
+#define Fv(a, j, k) (a)[fidx(d, (j), (k))]
+
+// ------------------------------------------------------------ helpers
+
+__device__ __forceinline__ void raise_status(const Dev &d, int code) {
+    atomicCAS(d.status, 0, code);
+}
+
+// fixed-shape tree reduction over a block (blockDim.x * blockDim.y <= 1024)
+template <bool kMax>
+__device__ double block_reduce(double v, double *sh) {
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int n = blockDim.x * blockDim.y;
+    sh[t] = v;
+    __syncthreads();
+    for (int s = 512; s > 0; s >>= 1) {
+        if (t < s && t + s < n) sh[t] = kMax ? fmax(sh[t], sh[t + s]) : sh[t] + sh[t + s];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Grid-wide deterministic reduction: every block deposits its partial,
+// the last block to arrive combines them in block order.  Returns true in
+// the last block (all its threads), with *out set there.
+template <bool kMax>
+__device__ bool grid_reduce(const Dev &d, double v, int slot, double *out, double *sh) {
+    const int nb = gridDim.x * gridDim.y;
+    const int b = blockIdx.x + blockIdx.y * gridDim.x;
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nt = blockDim.x * blockDim.y;
+    __shared__ bool last;
+    double part = block_reduce<kMax>(v, sh);
+    double *red = d.red + static_cast<size_t>(slot) * kRedSlot;
+    if (t == 0) {
+        red[b] = part;
+        __threadfence();
+        unsigned prev = atomicAdd(d.count + slot, 1u);
+        last = (prev == static_cast<unsigned>(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double acc = kMax ? -INFINITY : 0.0;
+    for (int i = t; i < nb; i += nt) {
+        double x = __ldcg(red + i);
+        acc = kMax ? fmax(acc, x) : acc + x;
+    }
+    double r = block_reduce<kMax>(acc, sh);
+    if (t == 0) d.count[slot] = 0u;
+    *out = r;
+    return true;
+}
+
+// ------------------------------------------------------------ cfl
+
+// cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
+// Both reductions (max for the CFL number, sum for the mean w) share one
+// last-block pass so that a single block finalises them.
+__global__ void k_cfl(Dev d) {
+    __shared__ double sh[1024];
+    __shared__ bool last;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int t = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
+    const int b = blockIdx.x + blockIdx.y * gridDim.x, nb = gridDim.x * gridDim.y;
+    double qcf = 1.0e-8, q3a = 0.0;
+    if (j <= d.n2m && k <= d.n3m) {
+        const int jp = j + 1, kp = k + 1;
+        const double udx2 = d.udx2m[j], udx3 = d.udx3m[k];
+        qcf = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
+               fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
+        q3a = Fv(d.q3, j, k) * (d.zz[kp] - d.zz[k]) * (d.rc[jp] - d.rc[j]);
+    }
+    const double pm = block_reduce<true>(qcf, sh);
+    const double ps = block_reduce<false>(q3a, sh);
+    double *rm = d.red, *rs = d.red + kRedSlot;
+    if (t == 0) {
+        rm[b] = pm;
+        rs[b] = ps;
+        __threadfence();
+        last = (atomicAdd(d.count, 1u) == static_cast<unsigned>(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double am = 1.0e-8, as = 0.0;
+    for (int i = t; i < nb; i += nt) {
+        am = fmax(am, __ldcg(rm + i));
+        as = as + __ldcg(rs + i);
+    }
+    am = block_reduce<true>(am, sh);
+    as = block_reduce<false>(as, sh);
+    if (t == 0) {
+        d.count[0] = 0u;
+        const double cflm = am * d.dt;
+        d.scal[S_CFLM] = cflm;
+        d.scal[S_Q3AVG] = as / (d.rext2 * d.alx3);
+        if (cflm > d.cfllim || !(cflm == cflm)) raise_status(d, FB_ERR_CFL);
+    }
+}
+
+// ------------------------------------------------------------ boundaries
+
+// iobcs.F90:5-77 (boucdq): radiative outflow increments + mass-flux correction
+__global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
+    __shared__ double sh[1024];
+    const int n3 = d.n3, n3m = d.n3m;
+    double qout = 0.0;
+    for (int j = threadIdx.x + 1; j <= d.n2; j += blockDim.x) {
+        d.dqb2s[j] = 0.0;
+        d.dqb3s[j] = 0.0;
+    }
+    for (int j = threadIdx.x + 1; j <= d.n2m; j += blockDim.x) {
+        double dq2x2 = (d.qb2n[j] - Fv(d.q2, j, n3m)) * 2.0 * d.udx3c[n3];
+        double dqb2n = -d.dt * (ga * dq2x2 + ro * d.dq2x2o[j]) * d.cou;
+        double dq3x2 = (d.qb3n[j] - Fv(d.q3, j, n3m)) * d.udx3c[n3];
+        double dqb3n = -d.dt * (ga * dq3x2 + ro * d.dq3x2o[j]) * d.cou;
+        d.dqb2n[j] = dqb2n;
+        d.dqb3n[j] = dqb3n;
+        d.dq2x2o[j] = dq2x2;
+        d.dq3x2o[j] = dq3x2;
+        qout = qout + dqb3n * (d.g2rm[j] / d.dx2);
+    }
+    double q = block_reduce<false>(qout, sh);
+    const double cor = (0.0 - q) / d.area_out;
+    __syncthreads();
+    for (int j = threadIdx.x + 1; j <= d.n2m; j += blockDim.x) d.dqb3n[j] = d.dqb3n[j] + cor;
+}
+
+// ------------------------------------------------------------ explicit terms
+
+// HDNL.F90:5-171 (hdnl2, hdnl3) fused with INVTR.F90:4-280 (invtr2, invtr3).
+// The convective terms stay in registers; ru2/ru3 receive them as the
+// reference's invtr does (ru2 = dph, ru3 = qcap).  q2f/q3f are not stored:
+// the forcing stage forms q + rhs at the few support nodes it reads.
+__global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
+    const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int n2m = d.n2m, n3m = d.n3m;
+    if (jc > n2m || kc > n3m) return;
+    const double dt = d.dt, alre = al / d.ren;
+    const double *q2 = d.q2, *q3 = d.q3, *pr = d.pr;
+
+    // ---- v momentum at (jc, kc), jc = 2..n2m
+    if (jc >= 2) {
+        const int jm = jc - 1, jp = jc + 1;
+        double h22 = ((Fv(q2, jp, kc) + Fv(q2, jc, kc)) * (Fv(q2, jp, kc) + Fv(q2, jc, kc)) -
+                      (Fv(q2, jm, kc) + Fv(q2, jc, kc)) * (Fv(q2, jm, kc) + Fv(q2, jc, kc))) *
+                     d.udx2c[jc] * 0.25;
+        double dph = -h22;
+        const int jmv = d.jmv[jc];
+        if (kc >= 2 && kc <= n3m - 1) {
+            const int kmm = d.kmv[kc], kpp = d.kpv[kc], kp = kc + 1;
+            double h23 = ((Fv(q3, jc, kp) + Fv(q3, jmv, kp)) * (Fv(q2, jc, kpp) + Fv(q2, jc, kc)) -
+                          (Fv(q3, jc, kc) + Fv(q3, jmv, kc)) * (Fv(q2, jc, kc) + Fv(q2, jc, kmm))) *
+                         d.udx3m[kc] * 0.25;
+            dph = dph - h23;
+        } else if (kc == n3m) {
+            const int kmm = kc - 1;
+            double h23 = (d.qb2n[jc] * (d.qb3n[jc] + d.qb3n[jmv]) -
+                          (Fv(q3, jc, kc) + Fv(q3, jmv, kc)) * (Fv(q2, jc, kc) + Fv(q2, jc, kmm)) * 0.5) *
+                         d.udx3m[kc] * 0.5;
+            dph = dph - h23;
+        }
+        if (kc == 1) {
+            const int kp = kc + 1;
+            double h23 = ((Fv(q3, jc, kp) + Fv(q3, jmv, kp)) * (Fv(q2, jc, kc) + Fv(q2, jc, kp)) * 0.5 -
+                          d.qb2s[jc] * (d.qb3s[jc] + d.qb3s[jmv])) *
+                         d.udx3m[kc] * 0.5;
+            dph = dph - h23;
+        }
+        const double ammj = d.am2j[jc], accj = d.ac2j[jc], appj = d.ap2j[jc];
+        const double d22q2 = Fv(q2, jp, kc) * appj + Fv(q2, jc, kc) * accj + Fv(q2, jm, kc) * ammj;
+        double d33q2, dpx22;
+        if (kc >= 2 && kc <= n3m - 1) {
+            const int km = d.kmv[kc], kp = d.kpv[kc];
+            d33q2 = Fv(q2, jc, kp) * d.ap3sk[kc] + Fv(q2, jc, kc) * d.ac3sk[kc] + Fv(q2, jc, km) * d.am3sk[kc];
+            const double udx2 = al * d.udx2c[jc];
+            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * udx2;
+        } else if (kc == 1) {
+            const int kp = kc + 1;
+            const double codea = d.dx3q / (d.g3rc[kp] * d.g3rm[kc]);
+            const double codeb = d.dx3q / (d.g3rc[kc] * d.g3rm[kc]);
+            d33q2 = ((Fv(q2, jc, kp) - Fv(q2, jc, kc)) * codea - (Fv(q2, jc, kc) - d.qb2s[jc]) * codeb * 2.0);
+            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * d.udx2c[jc] * al;
+        } else {
+            const int km = kc - 1, kp = kc + 1;
+            const double codea = d.dx3q / (d.g3rc[kp] * d.g3rm[kc]);
+            const double codeb = d.dx3q / (d.g3rc[kc] * d.g3rm[kc]);
+            d33q2 = ((d.qb2n[jc] - Fv(q2, jc, kc)) * codea * 2.0 - (Fv(q2, jc, kc) - Fv(q2, jc, km)) * codeb);
+            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * d.udx2c[jc] * al;
+        }
+        const double dcq2 = d22q2 + d33q2;
+        const size_t i = fidx(d, jc, kc);
+        d.rhs2[i] = (ga * dph + ro * d.ru2[i] + alre * dcq2 - dpx22) * dt;
+        d.ru2[i] = dph;
+    }
+
+    // ---- w momentum at (jc, kc), kc = 2..n3m
+    if (kc >= 2) {
+        double qcap = 0.0;  // hdnl3 never writes kc = n3m (HDNL.F90:143)
+        if (kc <= n3m - 1) {
+            const int kmm = kc - 1, km = d.kmv[kc], kp = kc + 1;
+            const int jmm = d.jmv[jc], jpp = d.jpv[jc], jp = jc + 1;
+            double h32 = (((Fv(q2, jp, kc) + Fv(q2, jp, km)) * (Fv(q3, jpp, kc) + Fv(q3, jc, kc))) -
+                          ((Fv(q2, jc, kc) + Fv(q2, jc, km)) * (Fv(q3, jc, kc) + Fv(q3, jmm, kc)))) *
+                         d.udx2m[jc] * 0.25;
+            double h33 = ((Fv(q3, jc, kp) + Fv(q3, jc, kc)) * (Fv(q3, jc, kp) + Fv(q3, jc, kc)) -
+                          (Fv(q3, jc, kc) + Fv(q3, jc, kmm)) * (Fv(q3, jc, kc) + Fv(q3, jc, kmm))) *
+                         d.udx3c[kc] * 0.25;
+            qcap = -(h32 + h33);
+        }
+        const int km = kc - 1, kp = kc + 1;
+        const double udx3 = al * d.udx3c[kc];
+        const double ammj = d.am3j[jc], accj = d.ac3j[jc], appj = d.ap3j[jc];
+        double dq32;
+        if (jc == 1) {
+            dq32 = Fv(q3, jc + 1, kc) * appj + Fv(q3, jc, kc) * accj + d.q3lw * ammj;
+        } else if (jc == n2m) {
+            dq32 = d.q3uw * appj + Fv(q3, jc, kc) * accj + Fv(q3, jc - 1, kc) * ammj;
+        } else {
+            dq32 = Fv(q3, d.jpv[jc], kc) * appj + Fv(q3, jc, kc) * accj + Fv(q3, d.jmv[jc], kc) * ammj;
+        }
+        const double dq33 = Fv(q3, jc, kp) * d.ap3ck[kc] + Fv(q3, jc, kc) * d.ac3ck[kc] + Fv(q3, jc, km) * d.am3ck[kc];
+        const double dcq3 = dq32 + dq33;
+        const double dpx33 = (Fv(pr, jc, kc) - Fv(pr, jc, km)) * udx3;
+        const size_t i = fidx(d, jc, kc);
+        d.rhs3[i] = (ga * qcap + ro * d.ru3[i] + alre * dcq3 - dpx33) * dt;
+        d.ru3[i] = qcap;
+    }
+}
+
+// ------------------------------------------------------------ MLS forcing
+
+__device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
+    // first index of min |a(i) - x| over a(lo..hi), a strictly increasing
+    int l = lo, h = hi;
+    if (x <= a[lo]) return lo;
+    if (x >= a[hi]) return hi;
+    while (h - l > 1) {
+        int m = (l + h) >> 1;
+        if (a[m] <= x) l = m;
+        else h = m;
+    }
+    double dl = fabs(a[l] - x), dh = fabs(a[h] - x);
+    return (dh < dl) ? h : l;
+}
+
+// lgrdistribution.F90:189-267: nearest nodes per marker and direction
+__global__ void k_lgrdist(Dev d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nlm) return;
+    const double y = d.lmcc[2 * i], z = d.lmcc[2 * i + 1];
+    if (y > d.rext2 || y < 0.0 || z > d.alx3 || z < 0.0 || !(y == y) || !(z == z)) {
+        raise_status(d, FB_ERR_MARKER_OUT);
+        for (int c = 0; c < 4; ++c) d.lmind[4 * i + c] = -1;
+        return;
+    }
+    int ind;
+    d.lmind[4 * i + 0] = nearest_sorted(d.rc, 1, d.n2, y);
+    if (z < d.zm[1] && z > 0.0) ind = 1;
+    else if (z > d.zm[d.n3m] && z < d.alx3) ind = d.n3m;
+    else ind = nearest_sorted(d.zm, 1, d.n3, z);
+    d.lmind[4 * i + 1] = ind;
+    if (y < d.rm[1] && y > 0.0) ind = 1;
+    else if (y > d.rm[d.n2m] && y < d.rext2) ind = d.n2m;
+    else ind = nearest_sorted(d.rm, 1, d.n2, y);
+    d.lmind[4 * i + 2] = ind;
+    d.lmind[4 * i + 3] = nearest_sorted(d.zz, 1, d.n3, z);
+}
+
+// MLSint.F90:4-104 (MLS_SD_ind): 3x3 support moved inside the field.
+// Returns false when a support node lacks its right neighbour on an axis.
+__device__ bool sd_ind(const Dev &d, int idir, int i0, int k0, double sdc[2][kSD], double sdd[2][kSD],
+                       int eul[2][kSD]) {
+    const double *y, *z;
+    int dimy, dimz;
+    if (idir == 1) {
+        y = d.rc; dimy = d.n2; z = d.zm; dimz = d.n3m;
+    } else if (idir == 2) {
+        y = d.rm; dimy = d.n2m; z = d.zz; dimz = d.n3;
+    } else {
+        y = d.rm; dimy = d.n2m; z = d.zm; dimz = d.n3m;
+    }
+    const int sj = (i0 == 1) ? 1 : (i0 == d.n2m ? -1 : 0);
+    const int sk = (k0 == 1) ? 1 : (k0 == d.n3m ? -1 : 0);
+    int m = 0;
+    for (int j = 1; j <= 3; ++j)
+        for (int k = 1; k <= 3; ++k) {
+            const int ej = i0 + (j + sj) - 2, ek = k0 + (k + sk) - 2;
+            if (ej < 1 || ej + 1 > dimy || ek < 1 || ek + 1 > dimz) return false;
+            sdc[0][m] = y[ej];
+            sdd[0][m] = y[ej + 1] - y[ej];
+            sdc[1][m] = z[ek];
+            sdd[1][m] = z[ek + 1] - z[ek];
+            eul[0][m] = ej;
+            eul[1][m] = ek;
+            ++m;
+        }
+    return true;
+}
+
+// utils_math.f90:637-725 (GEsolve), n = 3, scaled partial pivoting
+__device__ bool gesolve3(const double ai[3][3], const double bi[3], double x[3]) {
+    double a[3][3], b[3], s[3];
+    for (int i = 0; i < 3; ++i) {
+        b[i] = bi[i];
+        for (int j = 0; j < 3; ++j) a[i][j] = ai[i][j];
+    }
+    for (int k = 0; k < 2; ++k) {
+        for (int i = k; i < 3; ++i) {
+            s[i] = 0.0;
+            for (int j = k; j < 3; ++j) s[i] = fmax(s[i], fabs(a[i][j]));
+        }
+        double pivot = fabs(a[k][k] / s[k]);
+        int l = k;
+        for (int j = k + 1; j < 3; ++j) {
+            double q = fabs(a[j][k] / s[j]);
+            if (q > pivot) {
+                pivot = q;
+                l = j;
+            }
+        }
+        if (pivot == 0.0) return false;
+        if (l != k) {
+            for (int j = k; j < 3; ++j) {
+                double t = a[k][j];
+                a[k][j] = a[l][j];
+                a[l][j] = t;
+            }
+            double t = b[k];
+            b[k] = b[l];
+            b[l] = t;
+        }
+        for (int i = k + 1; i < 3; ++i) {
+            double c = a[i][k] / a[k][k];
+            a[i][k] = 0.0;
+            b[i] = b[i] - c * b[k];
+            for (int j = k + 1; j < 3; ++j) a[i][j] = a[i][j] - c * a[k][j];
+        }
+    }
+    x[2] = b[2] / a[2][2];
+    for (int i = 1; i >= 0; --i) {
+        double c = 0.0;
+        for (int j = i + 1; j < 3; ++j) c = c + a[i][j] * x[j];
+        x[i] = (b[i] - c) / a[i][i];
+    }
+    return true;
+}
+
+// MLSint.F90:406-486 (one axis of the weight function) and its derivative
+// MLSint.F90:492-593
+__device__ void wkernel(int wfun, double difc, double sdds, double &wc, double &dw) {
+    double drdc = (fabs(difc) <= 1.0e-20) ? 0.0 : (difc / fabs(difc)) / sdds;
+    double rc = fabs(difc) / sdds;
+    double rc2 = rc * rc, rc3 = rc * rc * rc, rc4 = rc * rc * rc * rc;
+    wc = 0.0;
+    dw = 0.0;
+    if (wfun == 1) {
+        if (rc > 1.0) {
+        } else if (rc <= 0.5) {
+            wc = (2.0 / 3.0) - 4.0 * rc2 + 4.0 * rc3;
+            dw = (-8.0 * rc + 12.0 * rc2) * drdc;
+        } else {
+            wc = (4.0 / 3.0) - 4.0 * rc + 4.0 * rc2 - (4.0 / 3.0) * rc3;
+            dw = (-4.0 + 8.0 * rc - 4.0 * rc2) * drdc;
+        }
+    } else if (wfun == 2) {
+        if (rc <= 1.0) {
+            double e = exp(-((rc / 0.3) * (rc / 0.3)));
+            wc = e;
+            dw = (-1.0 / (0.3 * 0.3) * 2.0 * rc * e) * drdc;
+        }
+    } else if (wfun == 3) {
+        if (rc <= 1.0) {
+            wc = 1.0 - 6.0 * rc2 + 8.0 * rc3 - 3.0 * rc4;
+            dw = -12.0 * rc + 24.0 * rc2 - 12.0 * rc3;
+        }
+    } else if (wfun == 4) {
+        if (rc > 1.0) {
+        } else if (rc < 0.5) {
+            wc = 1.0 / 3.0 * (1.0 + sqrt(-3.0 * rc2 + 1.0));
+            dw = -rc * pow(-3.0 * rc2 - 1.0, -0.5);
+        } else {
+            wc = 1.0 / 6.0 * (5.0 - 3.0 * rc - sqrt(-3.0 * ((1.0 - rc) * (1.0 - rc)) + 1.0));
+            dw = -(1.0 - rc) / (2.0 * sqrt(1.0 - 3.0 * ((1.0 - rc) * (1.0 - rc)))) - 0.5;
+        }
+    }
+}
+
+// Marker set-up at substep 1: MLS_SD_ind + MLS_SF + momentum coefficient cl
+// (forcing_MLS.F90:57-94, MLSint.F90:115-166, compute_AB :284-338), and the
+// spreading keys.  One thread per (marker, direction).
+__global__ void k_mls_setup(Dev d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * d.nlm) return;
+    const int n = t >> 1, idir = (t & 1) + 1;
+    double *phi = d.phi + static_cast<size_t>(t) * kSD;
+    int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+    uint32_t *key = d.skey_in + static_cast<size_t>(t) * kSD;
+    uint32_t *val = d.sval_in + static_cast<size_t>(t) * kSD;
+    for (int m = 0; m < kSD; ++m) {
+        phi[m] = 0.0;
+        key[m] = 0xFFFFFFFFu;
+        val[m] = static_cast<uint32_t>(t * kSD + m);
+    }
+    d.cl[t] = 0.0;
+    if (*d.status) return;
+    const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
+    if (!(d.zz[1] < pos[1] && pos[1] < d.zz[d.n3])) return;
+    const int i0 = d.lmind[4 * n + 2 * (idir - 1)], k0 = d.lmind[4 * n + 2 * (idir - 1) + 1];
+    double sdc[2][kSD], sdd[2][kSD];
+    int eul[2][kSD];
+    if (i0 < 1 || k0 < 1 || !sd_ind(d, idir, i0, k0, sdc, sdd, eul)) {
+        raise_status(d, FB_ERR_MARKER_OUT);
+        return;
+    }
+    double w[kSD];
+    for (int i = 0; i < kSD; ++i) {
+        double wc0, wc1, dw;
+        wkernel(d.wfun, pos[0] - sdc[0][i], d.radiusSD * sdd[0][i], wc0, dw);
+        wkernel(d.wfun, pos[1] - sdc[1][i], d.radiusSD * sdd[1][i], wc1, dw);
+        w[i] = wc0 * wc1;
+    }
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int i = 0; i < kSD; ++i) {
+        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) A[a][b] = A[a][b] + w[i] * (pk[a] * pk[b]);
+    }
+    const double gps[3] = {1.0, pos[0], pos[1]};
+    double ptA[3];
+    gesolve3(A, gps, ptA);
+    double ph[kSD], sumphi = 0.0;
+    for (int m = 0; m < kSD; ++m) {
+        const double B0 = 1.0 * w[m], B1 = sdc[0][m] * w[m], B2 = sdc[1][m] * w[m];
+        double acc = 0.0;
+        acc = acc + ptA[0] * B0;
+        acc = acc + ptA[1] * B1;
+        acc = acc + ptA[2] * B2;
+        ph[m] = acc;
+    }
+    for (int m = 0; m < kSD; ++m) sumphi = sumphi + ph[m];
+    if (!(fabs(1.0 - fabs(sumphi)) <= 1.0e-10)) raise_status(d, FB_ERR_MLS);
+    double dvel = 0.0, lgr_h = 0.0;
+    for (int m = 0; m < kSD; ++m) {
+        const double vol = sdd[0][m] * sdd[1][m];
+        dvel = dvel + ph[m] * vol;
+        lgr_h = lgr_h + 1.0 / 2.0 * ph[m] * (sdd[0][m] + sdd[1][m]);
+    }
+    d.cl[t] = d.lmA[n] * lgr_h / dvel;
+    const uint32_t base = (idir == 1) ? 0u : static_cast<uint32_t>(d.NK) * static_cast<uint32_t>(d.P);
+    for (int m = 0; m < kSD; ++m) {
+        phi[m] = ph[m];
+        eu[m] = eul[0][m];
+        eu[kSD + m] = eul[1][m];
+        const int j = eul[0][m], k = eul[1][m];
+        // cells helsolve reads: v at j = 2..n2m, k = 1..n3m; w at j = 1..n2m, k = 2..n3m
+        const bool used = (idir == 1) ? (j >= 2 && j <= d.n2m && k >= 1 && k <= d.n3m)
+                                      : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
+        if (used) key[m] = base + static_cast<uint32_t>(fidx(d, j, k));
+    }
+}
+
+// interp_spread (forcing_MLS.F90:135-182), interpolation half: the
+// provisional velocity q* = q + rhs (INVTR.F90:147,275) at the support,
+// direct forcing F = (V - u*)/dt and the per-node contributions cl*phi*F.
+__global__ void k_mls_interp(Dev d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * d.nlm) return;
+    if (*d.status) return;
+    const int n = t >> 1, idir = (t & 1) + 1;
+    const double pos2 = d.lmcc[2 * n + 1];
+    double *c = d.contrib + static_cast<size_t>(t) * kSD;
+    if (!(d.zz[1] < pos2 && pos2 < d.zz[d.n3])) {
+        for (int m = 0; m < kSD; ++m) c[m] = 0.0;
+        return;
+    }
+    const double *phi = d.phi + static_cast<size_t>(t) * kSD;
+    const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+    const double *q = (idir == 1) ? d.q2 : d.q3;
+    const double *r = (idir == 1) ? d.rhs2 : d.rhs3;
+    double u = 0.0;
+    for (int m = 0; m < kSD; ++m) {
+        const int j = eu[m], k = eu[kSD + m];
+        // q2f/q3f are written only where invtr2/invtr3 write them; elsewhere
+        // the reference reads storage that was never set (zero here)
+        const bool written = (idir == 1) ? (j >= 2 && j <= d.n2m && k >= 1 && k <= d.n3m)
+                                         : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
+        double qf = 0.0;
+        if (written) {
+            const size_t i = fidx(d, j, k);
+            qf = q[i] + r[i];
+        }
+        u = u + phi[m] * qf;
+    }
+    const double f = (d.lmvel[2 * n + idir - 1] - u) / d.dt;
+    const double clv = d.cl[t];
+    for (int m = 0; m < kSD; ++m) c[m] = clv * phi[m] * f;
+}
+
+// interp_spread, spreading half, without atomics: contributions sorted by
+// target cell (stable, so each cell keeps the reference's marker order) are
+// summed by the segment head, then helsolve.F90:22,47 adds fe*dt to rhs.
+__global__ void k_mls_spread(Dev d, int nitems) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    if (*d.status) return;
+    const uint32_t key = d.skey[i];
+    if (key == 0xFFFFFFFFu) return;
+    if (i > 0 && d.skey[i - 1] == key) return;
+    double fe = 0.0;
+    for (int t = i; t < nitems && d.skey[t] == key; ++t) fe = fe + d.contrib[d.sval[t]];
+    const uint32_t plane = static_cast<uint32_t>(d.NK) * static_cast<uint32_t>(d.P);
+    double *r = (key >= plane) ? d.rhs3 : d.rhs2;
+    const uint32_t cell = (key >= plane) ? key - plane : key;
+    r[cell] = r[cell] + fe * d.dt;
+}
+
+// ------------------------------------------------------------ tridiagonal
+
+// DGTTS2 (LAPACK) for one line with precomputed DGTTRF factors; b strided.
+// The pivots are stored as reciprocals, so the back substitution multiplies.
+__device__ __forceinline__ void gtts2(const TriDev &f, size_t off, double *b, size_t s) {
+    const int n = f.n;
+    const double *dl = f.dl + off, *dinv = f.dinv + off, *du = f.du + off, *du2 = f.du2 + off;
+    if (!f.pivoted) {
+        double prev = b[0];
+        for (int i = 0; i < n - 1; ++i) {
+            double cur = b[(i + 1) * s] - dl[i] * prev;
+            b[(i + 1) * s] = cur;
+            prev = cur;
+        }
+        double x1 = b[(n - 1) * s] * dinv[n - 1];
+        b[(n - 1) * s] = x1;
+        for (int i = n - 2; i >= 0; --i) {
+            double x0 = (b[i * s] - du[i] * x1) * dinv[i];
+            b[i * s] = x0;
+            x1 = x0;
+        }
+    } else {
+        const int *ipiv = f.ipiv + off;
+        for (int i = 0; i < n - 1; ++i) {
+            if (ipiv[i] == i + 1) {
+                b[(i + 1) * s] = b[(i + 1) * s] - dl[i] * b[i * s];
+            } else {
+                double temp = b[i * s] - dl[i] * b[(i + 1) * s];
+                b[i * s] = b[(i + 1) * s];
+                b[(i + 1) * s] = temp;
+            }
+        }
+        b[(n - 1) * s] = b[(n - 1) * s] * dinv[n - 1];
+        if (n > 1) b[(n - 2) * s] = (b[(n - 2) * s] - du[n - 2] * b[(n - 1) * s]) * dinv[n - 2];
+        for (int i = n - 3; i >= 0; --i)
+            b[i * s] = (b[i * s] - du[i] * b[(i + 1) * s] - du2[i] * b[(i + 2) * s]) * dinv[i];
+    }
+}
+
+// solve_fluid.F90:110-160 (solq2j): v, y lines of n2 unknowns, k = 1..n3m
+__global__ void k_tri_y2(Dev d, SubDev s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (k > d.n3m) return;
+    double *b = d.rhs2 + fidx(d, 1, k);
+    b[0] = 0.0;
+    for (int j = 2; j <= d.n2m; ++j) b[j - 1] = b[j - 1] * s.by2[j];
+    b[d.n2 - 1] = 0.0;
+    gtts2(s.y2, 0, b, 1);
+}
+
+// solve_fluid.F90:164-229 (solq2k) then helsolve.F90:32-33: v, z lines of
+// n3m unknowns with the inflow/outflow terms, q2 += x, wall columns zeroed
+__global__ void k_tri_z2(Dev d, SubDev s) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (j > d.n2m) return;
+    if (j == 1) {
+        for (int k = 0; k <= d.n3; ++k) {
+            Fv(d.q2, 1, k) = 0.0;
+            Fv(d.q2, d.n2, k) = 0.0;
+        }
+        return;
+    }
+    double *b = d.rhs2 + fidx(d, j, 1);
+    const size_t P = static_cast<size_t>(d.P);
+    for (int k = 1; k <= d.n3m; ++k) b[(k - 1) * P] = b[(k - 1) * P] * s.bz2[k];
+    b[0] = b[0] + d.dqb2s[j] * s.ugkks;
+    b[(d.n3m - 1) * P] = b[(d.n3m - 1) * P] + d.dqb2n[j] * s.ugkkn;
+    gtts2(s.z2, 0, b, P);
+    for (int k = 1; k <= d.n3m; ++k) Fv(d.q2, j, k) = Fv(d.q2, j, k) + b[(k - 1) * P];
+}
+
+// solve_fluid.F90:61-104 (solq3j): w, y lines of n2m unknowns, k = 2..n3m
+// (the k = 1 line of the reference is overwritten by solq3k and skipped)
+__global__ void k_tri_y3(Dev d, SubDev s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    if (k > d.n3m) return;
+    double *b = d.rhs3 + fidx(d, 1, k);
+    for (int j = 1; j <= d.n2m; ++j) b[j - 1] = b[j - 1] * s.by3[j];
+    gtts2(s.y3, 0, b, 1);
+}
+
+// solve_fluid.F90:233-312 (solq3k): w, z lines of n3 unknowns with
+// Dirichlet end rows, q3 += x, outflow row advanced by dqb3n
+__global__ void k_tri_z3(Dev d, SubDev s) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (j > d.n2m) return;
+    double *b = d.rhs3 + fidx(d, j, 1);
+    const size_t P = static_cast<size_t>(d.P);
+    b[0] = d.dqb3s[j];
+    for (int k = 2; k <= d.n3m; ++k) b[(k - 1) * P] = b[(k - 1) * P] * s.bz3[k];
+    b[(d.n3 - 1) * P] = d.dqb3n[j];
+    gtts2(s.z3, 0, b, P);
+    for (int k = 1; k <= d.n3m; ++k) Fv(d.q3, j, k) = Fv(d.q3, j, k) + b[(k - 1) * P];
+    Fv(d.q3, j, d.n3) = Fv(d.q3, j, d.n3) + d.dqb3n[j];
+}
+
+// ------------------------------------------------------------ Poisson
+
+// divergence.F90:88-115 (divg)
+__global__ void k_divg(Dev d, double usdtal) {
+    const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (jc > d.n2m || kc > d.n3m) return;
+    const double dqcap = (Fv(d.q2, jc + 1, kc) - Fv(d.q2, jc, kc)) * d.udx2m[jc] +
+                         (Fv(d.q3, jc, kc + 1) - Fv(d.q3, jc, kc)) * d.udx3m[kc];
+    Fv(d.dph, jc, kc) = dqcap * usdtal;
+}
+
+// phcalc_outflow.F90:33-56: per z-mode tridiagonal in y, factors precomputed
+__global__ void k_tri_poisson(Dev d) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;  // mode k - 1
+    if (m >= d.n3m) return;
+    const size_t off = static_cast<size_t>(m) * static_cast<size_t>(d.ldh);
+    double *b = d.hmn + off;
+    const double *pb = d.pb + off;
+    for (int j = 0; j < d.n2m; ++j) b[j] = b[j] * pb[j];
+    TriDev f{d.n2m, d.ppiv[m], d.pdl, d.pdinv, d.pdu, d.pdu2, d.pipiv};
+    gtts2(f, off, b, 1);
+}
+
+// updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
+// partial sums of pr_submean (updvp.F90:320-333)
+__global__ void k_updvp_prcalc(Dev d, double al, double be) {
+    __shared__ double sh[1024];
+    const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    double part = 0.0;
+    if (jc <= d.n2m && kc <= d.n3m) {
+        const double *dph = d.dph;
+        const int jm = d.jmv[jc], jp = d.jpv[jc];
+        const double usujm = al * d.dt * d.udx2c[jc];
+        const double locdph = Fv(dph, jc, kc);
+        Fv(d.q2, jc, kc) = Fv(d.q2, jc, kc) - (locdph - Fv(dph, jm, kc)) * usujm;
+        if (kc >= 2) {
+            const double usukm = al * d.dt * d.udx3c[kc];
+            Fv(d.q3, jc, kc) = Fv(d.q3, jc, kc) - (Fv(dph, jc, kc) - Fv(dph, jc, kc - 1)) * usukm;
+        }
+        const int kp = d.kpv[kc], km = d.kmv[kc];
+        const double p = Fv(d.pr, jc, kc) + Fv(dph, jc, kc) -
+                         be * ((Fv(dph, jp, kc) * d.apphj[jc] + Fv(dph, jc, kc) * d.acphj[jc] +
+                                Fv(dph, jm, kc) * d.amphj[jc]) +
+                               (Fv(dph, jc, kp) * d.apphk[kc] + Fv(dph, jc, kc) * d.acphk[kc] +
+                                Fv(dph, jc, km) * d.amphk[kc]));
+        Fv(d.pr, jc, kc) = p;
+        part = p * (d.zz[kc + 1] - d.zz[kc]) * (d.rc[jc + 1] - d.rc[jc]);
+    }
+    double tot;
+    if (grid_reduce<false>(d, part, 2, &tot, sh)) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) d.scal[S_PRAVG] = tot / (d.rext2 * d.alx3);
+    }
+}
+
+// pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
+__global__ void k_submean_boucqt(Dev d) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const double pravg = d.scal[S_PRAVG];
+    if (j <= d.n2 && k <= d.n3) Fv(d.pr, j, k) = Fv(d.pr, j, k) - pravg;
+    if (blockIdx.y == 0 && threadIdx.y == 0 && j <= d.n2m) {
+        d.qb2s[j] = d.qb2s[j] + d.dqb2s[j];
+        d.qb3s[j] = d.qb3s[j] + d.dqb3s[j];
+        d.qb2n[j] = d.qb2n[j] + d.dqb2n[j];
+        d.qb3n[j] = d.qb3n[j] + d.dqb3n[j];
+    }
+}
+
+// ------------------------------------------------------------ loads
+
+// loads_transfer.F90:238-281 (probeind)
+__device__ bool probeind(const Dev &d, int idir, int mj, int mk, const double pp[2], int &ij, int &ik) {
+    const int off = 5;
+    const int js = mj - off, je = mj + off, ks = mk - off, ke = mk + off;
+    if (js < 1 || je > d.n2 || ks < 1 || ke > d.n3) return false;
+    const double *ya = (idir == 1) ? d.rc : d.rm;
+    const double *za = (idir == 2) ? d.zz : d.zm;
+    int b = js;
+    double bv = fabs(ya[js] - pp[0]);
+    for (int i = js + 1; i <= je; ++i) {
+        double v = fabs(ya[i] - pp[0]);
+        if (v < bv) bv = v, b = i;
+    }
+    ij = b;
+    b = ks;
+    bv = fabs(za[ks] - pp[1]);
+    for (int i = ks + 1; i <= ke; ++i) {
+        double v = fabs(za[i] - pp[1]);
+        if (v < bv) bv = v, b = i;
+    }
+    ik = b;
+    return true;
+}
+
+// MLSint.F90:173-258 (MLS_SF_d) with compute_AB_d :342-402
+__device__ bool mls_sf_d(const Dev &d, const double pos[2], const double sdc[2][kSD],
+                         const double sdd[2][kSD], double phid[3][kSD]) {
+    double w[kSD][3];
+    for (int i = 0; i < kSD; ++i) {
+        double wc[2], dw[2];
+        for (int k = 0; k < 2; ++k) wkernel(d.wfun, pos[k] - sdc[k][i], d.radiusSD * sdd[k][i], wc[k], dw[k]);
+        w[i][0] = wc[0] * wc[1];
+        w[i][1] = wc[1] * dw[0];
+        w[i][2] = wc[0] * dw[1];
+    }
+    double A[3][3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            for (int l = 0; l < 3; ++l) A[a][b][l] = 0.0;
+    for (int i = 0; i < kSD; ++i) {
+        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                const double pp = pk[a] * pk[b];
+                for (int l = 0; l < 3; ++l) A[a][b][l] = A[a][b][l] + w[i][l] * pp;
+            }
+    }
+    double Aa[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) Aa[a][b] = A[a][b][0];
+    double gam[3][3];
+    const double gps[3] = {1.0, pos[0], pos[1]};
+    double g0[3];
+    gesolve3(Aa, gps, g0);
+    for (int l = 1; l <= 2; ++l) {
+        double C[3], gx[3];
+        for (int a = 0; a < 3; ++a) {
+            double acc = 0.0;
+            for (int b = 0; b < 3; ++b) acc = acc + A[a][b][l] * g0[b];
+            const double gpl = (a == l) ? 1.0 : 0.0;
+            C[a] = gpl - acc;
+        }
+        gesolve3(Aa, C, gx);
+        for (int a = 0; a < 3; ++a) gam[a][l] = gx[a];
+    }
+    for (int a = 0; a < 3; ++a) gam[a][0] = g0[a];
+    double sumphi = 0.0;
+    for (int i = 0; i < kSD; ++i) {
+        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            const double B0 = pk[a] * w[i][0], B1 = pk[a] * w[i][1], B2 = pk[a] * w[i][2];
+            p0 = p0 + gam[a][0] * B0;
+            p1 = p1 + gam[a][1] * B0 + gam[a][0] * B1;
+            p2 = p2 + gam[a][2] * B0 + gam[a][0] * B2;
+        }
+        phid[0][i] = p0;
+        phid[1][i] = p1;
+        phid[2][i] = p2;
+        sumphi = sumphi + p0;
+    }
+    return fabs(1.0 - fabs(sumphi)) <= 1.0e-10;
+}
+
+// getpbup (loads_transfer.F90:285-357) for one quantity
+__device__ void getpbup_one(const Dev &d, const double *f, const int eul[2][kSD], const double ph[3][kSD],
+                            double out[7]) {
+    for (int i = 0; i < 7; ++i) out[i] = 0.0;
+    for (int n = 0; n < kSD; ++n) {
+        const int cyk = eul[0][n], czk = eul[1][n];
+        const double f0 = Fv(f, cyk, czk);
+        const double uk1 = (f0 - Fv(f, cyk - 1, czk)) * d.dx2 / d.g2rc[cyk];
+        const double uk2 = (f0 - Fv(f, cyk, czk - 1)) * d.dx3 / d.g3rc[czk];
+        for (int i = 0; i < 3; ++i) out[i] = out[i] + ph[i][n] * f0;
+        out[3] = out[3] + ph[1][n] * uk1;
+        out[4] = out[4] + ph[1][n] * uk2;
+        out[5] = out[5] + ph[2][n] * uk1;
+        out[6] = out[6] + ph[2][n] * uk2;
+    }
+}
+
+// loads_transfer_c (loads_transfer.F90:143-185), per-marker part: probe
+// interpolation of v, w, p with first and second derivatives, and the
+// marker's own tangent; plus checkbcs (ckbcs.F90:29-60).
+__global__ void k_loads_probe(Dev d) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= d.nlm) return;
+    double *pb = d.probe + static_cast<size_t>(n) * 24;
+    pb[23] = -1.0;  // skipped
+    d.bcerrv[n] = 0.0;
+    d.bcerrw[n] = 0.0;
+    if (*d.status) return;
+    const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
+    if (!(d.zz[1] < pos[1] && pos[1] < d.zz[d.n3])) return;
+    // checkbcs with the substep-1 weights (phipred) and the final velocity
+    for (int idir = 1; idir <= 2; ++idir) {
+        const int t = 2 * n + idir - 1;
+        const double *phi = d.phi + static_cast<size_t>(t) * kSD;
+        const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+        const double *q = (idir == 1) ? d.q2 : d.q3;
+        double u = 0.0;
+        for (int m = 0; m < kSD; ++m) u = u + phi[m] * q[fidx(d, eu[m], eu[kSD + m])];
+        if (idir == 1) d.bcerrv[n] = d.lmvel[2 * n] - u;
+        else d.bcerrw[n] = d.lmvel[2 * n + 1] - u;
+    }
+    const double hpr = d.ddmin * d.kprobe;
+    const double probe[2] = {pos[0] + d.lmnor[2 * n] * hpr, pos[1] + d.lmnor[2 * n + 1] * hpr};
+    double res[3][7];
+    for (int idir = 1; idir <= 3; ++idir) {
+        int mj, mk;
+        if (idir == 3) {
+            mj = d.lmind[4 * n + 2];
+            mk = d.lmind[4 * n + 1];
+        } else {
+            mj = d.lmind[4 * n + 2 * (idir - 1)];
+            mk = d.lmind[4 * n + 2 * (idir - 1) + 1];
+        }
+        int ij, ik;
+        double sdc[2][kSD], sdd[2][kSD], ph[3][kSD];
+        int eul[2][kSD];
+        if (!probeind(d, idir, mj, mk, probe, ij, ik) || !sd_ind(d, idir, ij, ik, sdc, sdd, eul) ||
+            eul[0][0] < 2) {
+            raise_status(d, FB_ERR_MARKER_OUT);
+            return;
+        }
+        if (!mls_sf_d(d, probe, sdc, sdd, ph)) raise_status(d, FB_ERR_MLS);
+        const double *f = (idir == 1) ? d.q2 : (idir == 2 ? d.q3 : d.pr);
+        getpbup_one(d, f, eul, ph, res[idir - 1]);
+    }
+    for (int i = 0; i < 7; ++i) {
+        pb[i] = res[0][i];
+        pb[7 + i] = res[1][i];
+        pb[14 + i] = res[2][i];
+    }
+    const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
+    const double vel0 = res[0][0], vel1 = res[1][0];
+    const double veln_md = vel0 * nory + vel1 * norz;
+    const double velt0 = vel0 - veln_md * nory, velt1 = vel1 - veln_md * norz;
+    const double velt_md = sqrt(velt0 * velt0 + velt1 * velt1);
+    if (velt_md != 0.0) {
+        pb[21] = velt0 / sqrt(velt0 * velt0 + velt1 * velt1);
+        pb[22] = velt1 / sqrt(velt0 * velt0 + velt1 * velt1);
+        pb[23] = 1.0;
+    } else {
+        pb[23] = 0.0;
+    }
+}
+
+// loads_transfer_c (loads_transfer.F90:187-214): the tangent carries over
+// from the previous marker when the probe's tangential velocity vanishes;
+// pressure extrapolation (Wang et al. 2019 eq. 20) and wall shear (eq. 26).
+// Also the L2 norms of checkbcs (ckbcs.F90:76-81).  Single block.
+__global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
+    __shared__ double sh[1024];
+    const double hpr = d.ddmin * d.kprobe, visc = d.visc;
+    double sv = 0.0, sw = 0.0;
+    if (*d.status == 0) {
+        for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
+            const double *pb = d.probe + static_cast<size_t>(n) * 24;
+            d.press[n] = 0.0;
+            d.tau[2 * n] = 0.0;
+            d.tau[2 * n + 1] = 0.0;
+            if (pb[23] < 0.0) continue;
+            double tany = 0.0, tanz = 0.0;
+            for (int m = n; m >= 0; --m) {
+                const double *pm = d.probe + static_cast<size_t>(m) * 24;
+                if (pm[23] > 0.5) {
+                    tany = pm[21];
+                    tanz = pm[22];
+                    break;
+                }
+            }
+            const double *ucy = pb, *ucz = pb + 7, *pc = pb + 14;
+            const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
+            double dpdnw = d.lmacc[2 * n] * nory + d.lmacc[2 * n + 1] * norz;
+            dpdnw = -1.0 * dpdnw;
+            const double dpdne = pc[1] * nory + pc[2] * norz;
+            d.press[n] = pc[0] - 0.5 * (dpdnw + dpdne) * hpr;
+            const double ducdn = (ucy[1] * tany * nory + ucy[2] * tany * norz + ucz[1] * tanz * nory +
+                                  ucz[2] * tanz * norz);
+            const double d3ucdn3 = (pc[3] * nory * nory + pc[4] * nory * norz + pc[5] * norz * nory +
+                                    pc[6] * norz * norz) * 1.0 / visc;
+            const double d2ucdn2 = (ucy[3] * tany * nory * nory + ucy[4] * tany * nory * norz +
+                                    ucy[5] * tany * norz * nory + ucy[6] * tany * norz * norz +
+                                    ucz[3] * tanz * nory * nory + ucz[4] * tanz * nory * norz +
+                                    ucz[5] * tanz * norz * nory + ucz[6] * tanz * norz * norz);
+            const double ducdnm = ducdn - d2ucdn2 * hpr - 0.5 * d3ucdn3 * (hpr * hpr);
+            d.tau[2 * n] = visc * ducdnm * tany;
+            d.tau[2 * n + 1] = visc * ducdnm * tanz;
+        }
+    }
+    for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
+        sv = sv + d.bcerrv[n] * d.bcerrv[n];
+        sw = sw + d.bcerrw[n] * d.bcerrw[n];
+    }
+    const double tv = block_reduce<false>(sv, sh);
+    const double tw = block_reduce<false>(sw, sh);
+    if (threadIdx.x == 0) {
+        d.scal[S_NBCV] = sqrt(tv) / static_cast<double>(d.nlm);
+        d.scal[S_NBCW] = sqrt(tw) / static_cast<double>(d.nlm);
+    }
+}
+
+// ------------------------------------------------------------ rigid body
+
+// rigid.F90:341-369 (modfn) for the uncoupled 3-DOF system
+__device__ void modfn(double K[6], const double t[6], const double FF[6], const double Mi[3], const Dev &d) {
+    for (int i = 0; i < 3; ++i) {
+        const double cube = t[i] * t[i] * t[i];
+        const double lin = -d.kk[i] * t[i] + -d.cc[i] * t[i + 3];
+        const double rhs = lin + -d.kk3[i] * cube + FF[i + 3];
+        K[i] = t[i + 3];
+        K[i + 3] = Mi[i] * rhs;
+    }
+}
+
+// rigid.F90:4-138 (rigid) with int_stress :373-464, kinem_RK4 :165-228 /
+// kinem_RK4i :233-299, get_rotmat :142-161, createnorm :468-495; then the
+// clock update of main.F90:92 and one history row.  Single block.
+__global__ void __launch_bounds__(1024) k_rigid(Dev d, int hist_rows) {
+    __shared__ double sh[1024];
+    __shared__ double cm[18];
+    __shared__ double rot[4];
+    const int tid = threadIdx.x, nt = blockDim.x, nlm = d.nlm;
+    double *R = d.rigid;
+    double fyp = 0.0, fzp = 0.0, fyv = 0.0, fzv = 0.0, mom = 0.0;
+    for (int i = tid; i < nlm; i += nt) {
+        const double p = d.press[i], A = d.lmA[i];
+        const double Fp1 = -p * d.lmnor[2 * i] * A, Fp2 = -p * d.lmnor[2 * i + 1] * A;
+        const double Fv1 = d.tau[2 * i] * A, Fv2 = d.tau[2 * i + 1] * A;
+        fyp = fyp + Fp1;
+        fzp = fzp + Fp2;
+        fyv = fyv + Fv1;
+        fzv = fzv + Fv2;
+        const double r1 = d.lmcc[2 * i] - R[0], r2 = d.lmcc[2 * i + 1] - R[1];
+        mom = mom + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
+    }
+    fyp = block_reduce<false>(fyp, sh);
+    fzp = block_reduce<false>(fzp, sh);
+    fyv = block_reduce<false>(fyv, sh);
+    fzv = block_reduce<false>(fzv, sh);
+    mom = block_reduce<false>(mom, sh);
+    if (tid == 0) {
+        const double time = d.scal[S_TIME], dt = d.dt;
+        const double fy = fyp + fyv, fz = fzp + fzv;
+        const double g0 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF0;
+        const double g1 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF1;
+        const double Fy = fy + g0, Fz = fz + g1, M = mom;
+        d.forces[0] = time;
+        d.forces[1] = Fy;
+        d.forces[2] = Fz;
+        d.forces[3] = M;
+        d.forces[4] = fyp;
+        d.forces[5] = fzp;
+        d.forces[6] = fyv;
+        d.forces[7] = fzv;
+        // explicit RK4 with loads frozen over the stages
+        const double csp[3] = {d.cmposi0, d.cmposi1, d.cmroti};
+        double xo[6], FF[6] = {0.0, 0.0, 0.0, 0.0, Fz, M}, Mi[3];
+        for (int i = 0; i < 3; ++i) xo[i] = R[i] - csp[i];
+        for (int i = 0; i < 3; ++i) xo[i + 3] = R[3 + i];
+        if (d.rtcoup) {
+            FF[3] = Fy + M / d.rrr;
+            Mi[0] = 1.0 / ((d.rba1 / (d.rrr * d.rrr) + d.rba0) * d.rbden);
+        } else {
+            FF[3] = Fy;
+            Mi[0] = 1.0 / (d.rba0 * d.rbden);
+        }
+        Mi[1] = 1.0 / (d.rba0 * d.rbden);
+        Mi[2] = 1.0 / (d.rba1 * d.rbden);
+        double K1[6], K2[6], K3[6], K4[6], t1[6], xn[6];
+        modfn(K1, xo, FF, Mi, d);
+        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K1[i] * dt / 2.0;
+        modfn(K2, t1, FF, Mi, d);
+        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K2[i] * dt / 2.0;
+        modfn(K3, t1, FF, Mi, d);
+        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K3[i] * dt;
+        modfn(K4, t1, FF, Mi, d);
+        for (int i = 0; i < 6; ++i) xn[i] = xo[i] + dt * (K1[i] / 6.0 + K2[i] / 3.0 + K3[i] / 3.0 + K4[i] / 6.0);
+        double *P1 = R + 9, *V1 = R + 12, *A1 = R + 15;
+        if (!d.rtcoup) {
+            for (int i = 0; i < 3; ++i) {
+                P1[i] = csp[i] + xn[i];
+                V1[i] = xn[3 + i];
+                A1[i] = (V1[i] - R[3 + i]) / dt;
+            }
+        } else {
+            P1[0] = csp[0] + xn[0];
+            V1[0] = xn[3];
+            A1[0] = (V1[0] - R[3]) / dt;
+            P1[1] = csp[1];
+            V1[1] = 0.0;
+            A1[1] = 0.0;
+            P1[2] = csp[2] + xn[0] / d.rrr;
+            V1[2] = V1[0] / d.rrr;
+            A1[2] = A1[2] / d.rrr;  // as rigid.F90:296 (incoming value / rr)
+        }
+        for (int i = 0; i < 3; ++i)
+            if (d.rbmcon[i] == 1) {
+                P1[i] = d.kinori[i];
+                V1[i] = d.kinori[3 + i];
+                A1[i] = d.kinori[6 + i];
+            }
+        const double cmrot = P1[2] - R[2];
+        rot[0] = cos(cmrot);
+        rot[1] = -sin(cmrot);
+        rot[2] = sin(cmrot);
+        rot[3] = cos(cmrot);
+        for (int i = 0; i < 18; ++i) cm[i] = R[i];
+    }
+    __syncthreads();
+    const double *P0 = cm, *P1 = cm + 9, *V1 = cm + 12, *A1 = cm + 15;
+    for (int i = tid; i < nlm; i += nt) {
+        const double rho0 = d.lmcc[2 * i] - P0[0], rho1 = d.lmcc[2 * i + 1] - P0[1];
+        const double c10 = -V1[2] * rho1, c11 = V1[2] * rho0;
+        const double c20 = -A1[2] * rho1, c21 = A1[2] * rho0;
+        const double c30 = -V1[2] * c11, c31 = V1[2] * c10;
+        d.lmcc[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
+        d.lmcc[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
+        d.lmvel[2 * i] = V1[0] + c10;
+        d.lmvel[2 * i + 1] = V1[1] + c11;
+        d.lmacc[2 * i] = A1[0] + c20 + c30;
+        d.lmacc[2 * i + 1] = A1[1] + c21 + c31;
+    }
+    // vertices rotate about the updated centre (rigid.F90:110-121)
+    for (int i = tid; i <= nlm; i += nt) {
+        const double rho0 = d.vert[2 * i] - P1[0], rho1 = d.vert[2 * i + 1] - P1[1];
+        d.vert[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
+        d.vert[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
+    }
+    __syncthreads();
+    for (int i = tid; i < nlm; i += nt) {
+        const double *a = d.vert + 2 * i, *b = d.vert + 2 * i + 2;
+        const double v1[3] = {0.0 - 0.0, b[0] - a[0], b[1] - a[1]};
+        const double v2[3] = {-1.0 - 0.0, (a[0] + b[0]) * 0.5 - a[0], (a[1] + b[1]) * 0.5 - a[1]};
+        const double c0 = v1[1] * v2[2] - v1[2] * v2[1];
+        const double c1 = v1[2] * v2[0] - v1[0] * v2[2];
+        const double c2 = v1[0] * v2[1] - v1[1] * v2[0];
+        const double den = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+        d.lmnor[2 * i] = c1 / den;
+        d.lmnor[2 * i + 1] = c2 / den;
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 9; ++i) R[i] = cm[9 + i];
+        const double t0 = d.scal[S_TIME];
+        const double t1 = t0 + d.dt;
+        d.scal[S_TIME] = t1;
+        const int row = static_cast<int>(d.scal[S_STEP]);
+        if (hist_rows > 0) {
+            double *h = d.hist + static_cast<size_t>(row % hist_rows) * FB_HIST_COLS;
+            for (int i = 0; i < 8; ++i) h[i] = d.forces[i];
+            h[8] = t1;
+            for (int i = 0; i < 9; ++i) h[9 + i] = cm[9 + i];
+            h[18] = d.scal[S_NBCV];
+            h[19] = d.scal[S_NBCW];
+            h[20] = d.scal[S_CFLM];
+        }
+        d.scal[S_STEP] = static_cast<double>(row + 1);
+    }
+}
+
+// ------------------------------------------------------------ launchers
+
+namespace {
+inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
+}  // namespace
+
+void launch_cfl(const Dev &d, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_cfl<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d);
+}
+void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { k_boucdq<<<1, 1024, 0, s>>>(d, ga, ro); }
+void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_nl_rhs<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, al, ga, ro);
+}
+void launch_lgrdist(const Dev &d, cudaStream_t s) {
+    if (d.nlm) k_lgrdist<<<(d.nlm + 127) / 128, 128, 0, s>>>(d);
+}
+void launch_mls_setup(const Dev &d, cudaStream_t s) {
+    if (d.nlm) k_mls_setup<<<(2 * d.nlm + 127) / 128, 128, 0, s>>>(d);
+}
+void launch_mls_interp(const Dev &d, cudaStream_t s) {
+    if (d.nlm) k_mls_interp<<<(2 * d.nlm + 127) / 128, 128, 0, s>>>(d);
+}
+void launch_mls_spread(const Dev &d, cudaStream_t s) {
+    const int n = 2 * d.nlm * kSD;
+    if (n) k_mls_spread<<<(n + 255) / 256, 256, 0, s>>>(d, n);
+}
+void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s) {
+    k_tri_y2<<<(d.n3m + 63) / 64, 64, 0, s>>>(d, sd);
+    k_tri_z2<<<(d.n2m + 63) / 64, 64, 0, s>>>(d, sd);
+    k_tri_y3<<<(d.n3m + 63) / 64, 64, 0, s>>>(d, sd);
+    k_tri_z3<<<(d.n2m + 63) / 64, 64, 0, s>>>(d, sd);
+}
+void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_divg<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, usdtal);
+}
+void launch_tri_poisson(const Dev &d, cudaStream_t s) { k_tri_poisson<<<(d.n3m + 63) / 64, 64, 0, s>>>(d); }
+void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_updvp_prcalc<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, al, be);
+}
+void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_submean_boucqt<<<grid2(d.n2, d.n3 + 1, b), b, 0, s>>>(d);
+}
+void launch_loads(const Dev &d, cudaStream_t s) {
+    if (!d.nlm) return;
+    k_loads_probe<<<(d.nlm + 127) / 128, 128, 0, s>>>(d);
+    k_loads_finish<<<1, 1024, 0, s>>>(d);
+}
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s) {
+    if (d.nlm) k_rigid<<<1, 1024, 0, s>>>(d, hist_rows);
+}
+
+}  // namespace fb

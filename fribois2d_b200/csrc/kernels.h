@@ -1,0 +1,27 @@
+// Kernel launchers of the fluid time step (definitions in kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace fb {
+
+constexpr int kRedSlot = 65536;  // block partials per reduction slot
+
+void launch_cfl(const Dev &d, cudaStream_t s);
+void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s);
+void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s);
+void launch_lgrdist(const Dev &d, cudaStream_t s);
+void launch_mls_setup(const Dev &d, cudaStream_t s);
+void launch_mls_interp(const Dev &d, cudaStream_t s);
+void launch_mls_spread(const Dev &d, cudaStream_t s);
+void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
+void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
+void launch_tri_poisson(const Dev &d, cudaStream_t s);
+void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s);
+void launch_submean_boucqt(const Dev &d, cudaStream_t s);
+void launch_loads(const Dev &d, cudaStream_t s);
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s);
+
+}  // namespace fb

@@ -1,0 +1,188 @@
+/*
+ * fribois2d.h -- C ABI of the B200-native FRiBoIS2D fluid time step.
+ *
+ * The reference (AleNit/FRiBoIS2D, Fortran 90 + MPI) has no plugin or FFI
+ * boundary: its driver calls module subroutines on global state
+ * (src/main.F90:51-97).  This header is the boundary a Fortran host binds
+ * with ISO_C_BINDING (`bind(C)` interfaces) to replace
+ * those subroutines with one GPU.  Conventions:
+ *
+ *  - every function returns an int status (FB_OK = 0); the reference aborts
+ *    through stopcase/MPI_ABORT (src/stopcase.F90:4-31) instead;
+ *  - arrays crossing the boundary are plain host `double*` / `int*` with an
+ *    element count; fields are the reference's column-major A(j,k), j = 1..n2
+ *    contiguous, k = 0..n3 (the k = 0 ghost row of the reference is kept),
+ *    i.e. (n3+1) * n2 doubles;
+ *  - all device memory is owned by the opaque context; one host thread per
+ *    context; calls are synchronous unless stated otherwise.
+ */
+#ifndef FRIBOIS2D_H
+#define FRIBOIS2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace stopcase calls) ----------------------------- */
+#define FB_OK 0
+#define FB_ERR_CFL 1          /* fluid_tsch.F90:43-55: CFL above cfllim / dt too small */
+#define FB_ERR_MLS 2          /* MLSint.F90:157-163: MLS partition of unity violated */
+#define FB_ERR_MARKER_OUT 3   /* lgrdistribution.F90:217-221: marker leaves the grid */
+#define FB_ERR_INPUT 4        /* utils_proc.F90:174-219: malformed or missing input */
+#define FB_ERR_CUDA 5         /* CUDA runtime / cuBLAS failure */
+#define FB_ERR_STATE 6        /* bad argument for this context (id, size, order) */
+#define FB_ERR_UNSUPPORTED 7  /* deck option not implemented on the device path */
+#define FB_ERR_NUMERIC 8      /* a NaN/Inf or a singular set-up system was detected */
+
+typedef struct fb_ctx fb_ctx;     /* device context: one case on one GPU */
+typedef struct fb_host fb_host;   /* host-side set-up of one case (no GPU) */
+
+/* ---- array ids for fb_get_array / fb_set_array / fb_host_array --------- */
+/* fields, (n3+1) x n2 doubles, k = 0..n3 */
+#define FB_Q2 0      /* v at (rc_j, zm_k)   declarations.F90:148 */
+#define FB_Q3 1      /* w at (rm_j, zz_k)   */
+#define FB_PR 2      /* pressure at (rm_j, zm_k) */
+#define FB_DPH 3     /* pressure correction phi (after phcalc) or divergence (after divg) */
+#define FB_RHS2 7    /* explicit v right-hand side (after invtr2; forcing added in place) */
+#define FB_RHS3 8
+#define FB_RU2 9     /* previous convective term of v (= hdnl2 output) */
+#define FB_RU3 10    /* previous convective term of w (= hdnl3 output) */
+/* inflow / outflow boundary arrays, n2 doubles (index j-1) */
+#define FB_QB2S 20
+#define FB_QB2N 21
+#define FB_DQB2S 22
+#define FB_DQB2N 23
+#define FB_QB3S 24
+#define FB_QB3N 25
+#define FB_DQB3S 26
+#define FB_DQB3N 27
+#define FB_DQ2X2O 28
+#define FB_DQ3X2O 29
+/* 1-D grid data, n2 or n3 doubles (index j-1 / k-1) */
+#define FB_RC 40
+#define FB_RM 41
+#define FB_ZZ 42
+#define FB_ZM 43
+#define FB_UDX2C 48
+#define FB_UDX2M 49
+#define FB_UDX3C 50
+#define FB_UDX3M 51
+#define FB_AMPHJ 64
+#define FB_ACPHJ 65
+#define FB_APPHJ 66
+#define FB_AMPHK 67
+#define FB_ACPHK 68
+#define FB_APPHK 69
+/* Poisson eigen data: wr (n3m), zmm and zmmt (n3m*n3m, column-major) */
+#define FB_WR 80
+#define FB_ZMM 81
+#define FB_ZMMT 82
+/* markers: nlm x 2 row-major (y, z) unless stated */
+#define FB_LMCC 90
+#define FB_LMVEL 91
+#define FB_LMACC 92
+#define FB_LMNOR 93
+#define FB_LMA 94    /* nlm */
+#define FB_VERT 95   /* (nlm+1) x 2 */
+#define FB_PHI 96    /* nlm x 2 x 9: MLS transfer weights, (marker, direction, support node) */
+#define FB_CL 97     /* nlm x 2 */
+#define FB_PRESS 98  /* nlm: wall pressure from loads_transfer_c */
+#define FB_TAU 99    /* nlm x 2: wall shear stress */
+#define FB_BCERRV 100
+#define FB_BCERRW 101
+#define FB_RIGID 110   /* 18: cmp_n, cmv_n, cma_n, cmp_np1, cmv_np1, cma_np1 */
+#define FB_SCALARS 111 /* 13: time, dt, dt_o, beta, al, ga, ro, cflm, q3avg, nbcv, nbcw, ddmin, pravg */
+#define FB_FORCES 112  /* 8: forcecomp.out row: time, Fy, Fz, M, Fyp, Fzp, Fyv, Fzv */
+/* integer arrays for fb_get_iarray */
+#define FB_LMIND 0     /* nlm x 2 x 2: nearest node per marker and direction */
+#define FB_EULINS 1    /* nlm x 2 x 2 x 9: MLS support node indices (j, k) */
+
+/* ---- history rows written by fb_advance -------------------------------- */
+/* one row per step: forcecomp.out (rigid.F90:432) then rbkin.out (ttime.F90:146)
+ *  [0] time (start of step)  [1] Fy  [2] Fz  [3] M  [4] Fyp [5] Fzp [6] Fyv [7] Fzv
+ *  [8] time (end of step) [9..11] cmp_np1 [12..14] cmv_np1 [15..17] cma_np1
+ *  [18] nbcv [19] nbcw [20] cflm */
+#define FB_HIST_COLS 21
+
+/* ---- stage ids for fb_stage: one per reference subroutine --------------- */
+#define FB_ST_CFL 0        /* cfl.F90 (fluid_tsch.F90:211-258) */
+#define FB_ST_BOUCDQ 1     /* iobcs.F90:5-77 */
+#define FB_ST_NL_RHS 2     /* HDNL.F90:5-171 + INVTR.F90:4-280, fused */
+#define FB_ST_LGRDIST 6    /* lgrdistribution.F90:189-267 */
+#define FB_ST_FORCING 7    /* forcing_MLS.F90:5-182 (forcing added to rhs2/rhs3) */
+#define FB_ST_HELSOLVE 8   /* helsolve.F90:4-56 + solve_fluid.F90:4-255 */
+#define FB_ST_DIVG 9       /* divergence.F90:88-115 */
+#define FB_ST_PHCALC 10    /* phcalc_outflow.F90:4-71 */
+#define FB_ST_UPDVP 11     /* updvp.F90:5-105 (updvp + prcalc, fused) */
+#define FB_ST_PRSUBMEAN 13 /* updvp.F90:112-144 + iobcs.F90:81-108 (boucqt), fused */
+#define FB_ST_CHECKBCS 15  /* ckbcs.F90:5-86 */
+#define FB_ST_LOADS 16     /* loads_transfer.F90:93-281 */
+#define FB_ST_RIGID 17     /* rigid.F90:4-138 on the device */
+
+/* ---- set-up -------------------------------------------------------------
+ * Replaces read_genin + fluid_pre + read_rigid + allocate_mls_local +
+ * rigid_pre (main.F90:51-62; utils_proc.F90:45-222,519-578; fluid_pre.F90;
+ * indic.F90; cordin.F90; coetar.F90; phini.F90; initial_sol.F90:251-299;
+ * rigid_pre.F90).  Reads input_dir/{global,fluid,rigid}_par.in,
+ * ycoord.dat, zcoord.dat, lmdata.in.  The state starts as inqpr leaves it. */
+int fb_create(const char *input_dir, int device, fb_ctx **out);
+int fb_destroy(fb_ctx *ctx);
+
+/* One fluid time step: fluid_tsch(ns, str) (fluid_tsch.F90:4-204),
+ * including checkbcs and loads_transfer_c.  Leaves press/tau for fb_rigid. */
+int fb_fluid_tsch(fb_ctx *ctx, int ns);
+
+/* rigid(ns, str, nk) (rigid.F90:4-138) on the device state; writes the
+ * forcecomp.out row (8 doubles, see FB_FORCES) when forcecomp != NULL.
+ * Then advances time by dt as main.F90:92 does. */
+int fb_rigid(fb_ctx *ctx, int ns, double *forcecomp);
+
+/* nsteps iterations of the reference main loop body (main.F90:85-97:
+ * fluid_tsch, rigid, time += dt) starting at step index ns0, replayed from a
+ * captured CUDA graph; hist (nsteps x FB_HIST_COLS, may be NULL) receives the
+ * per-step history rows.  Status errors found on the device stop the call and
+ * are returned after the step that raised them. */
+int fb_advance(fb_ctx *ctx, int ns0, int nsteps, double *hist);
+
+/* Marker-side coupling for a host rigid-body solver (the reference's own
+ * rigid.F90 kept on the host): fb_get_loads copies press (nlm) and tau
+ * (nlm x 2) to the host; fb_set_markers uploads lmcc, lmvel, lmacc, lmnor
+ * (each nlm x 2, any may be NULL to keep the device copy). */
+int fb_get_loads(fb_ctx *ctx, double *press, double *tau);
+int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const double *lmacc,
+                   const double *lmnor);
+
+/* ---- state access --------------------------------------------------------- */
+int fb_get_dims(fb_ctx *ctx, int32_t dims[8]); /* n2, n3, nlm, nsst, ... */
+int fb_get_array(fb_ctx *ctx, int id, double *host, int64_t n);
+int fb_set_array(fb_ctx *ctx, int id, const double *host, int64_t n);
+int fb_get_iarray(fb_ctx *ctx, int id, int32_t *host, int64_t n);
+int fb_synchronize(fb_ctx *ctx);
+
+/* ---- stage entry points (parity tests; one reference subroutine each) ---- */
+int fb_set_substep(fb_ctx *ctx, int ns, int n);
+int fb_stage(fb_ctx *ctx, int stage, int n);
+
+/* ---- timing: device time of the last fb_advance, and per-kernel totals --- */
+int fb_last_advance_ms(fb_ctx *ctx, double *ms);
+
+/* ---- host-only set-up (no GPU touched; usable on a CPU-only machine) ----- */
+int fb_host_create(const char *input_dir, fb_host **out);
+int fb_host_destroy(fb_host *h);
+int fb_host_dims(fb_host *h, int32_t dims[8]);
+int fb_host_array(fb_host *h, int id, double *out, int64_t n);
+/* Symmetric-tridiagonal eigen-decomposition replacing phini's DGEEV+DGESV:
+ * am/ac/ap are the z operator's sub/diag/super diagonals (n, 0-based rows);
+ * writes wr (n), zmm and zmmt (n*n column-major). */
+int fb_eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr,
+                     double *zmm, double *zmmt);
+
+const char *fb_status_string(int status);
+const char *fb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
