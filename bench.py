@@ -1,0 +1,374 @@
+"""Benchmark: cell-steps/s of the FRiBoIS2D fluid time step on B200.
+
+One step is one full time step of the reference's main loop (three RK3
+substeps of fluid_tsch, loads, rigid-body update; src/main.F90:85-97).
+Workload: the rotational-galloping rectangle on 1024 (z) x 768 (y) cells,
+1200 markers, plain FP64 (synthetic deck written by fribois2d_b200.case).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs one independent replica per GPU (the single-case path does not
+shard); launch with torch.distributed.run.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s (plain FP64 fluid time step, galloping rectangle 1024x768)"
+UNIT = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config3"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_case(name):
+    from fribois2d_b200 import case as cases
+    return cases.CONFIGS[name]()
+
+
+def write_deck(c, rank=0):
+    root = tempfile.mkdtemp(prefix=f"fbbench{rank}_")
+    return c.write(os.path.join(root, c.name))
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_run(case_name, seconds, max_steps):
+    """The oracle (a C restatement of the reference's CPU path) on the host
+    cores with all threads; returns (cell-steps/s, steps timed, threads)."""
+    import oracle
+    c = make_case(case_name)
+    path = write_deck(c, 99)
+    threads = os.cpu_count() or 1
+    o = oracle.Oracle(oracle.parse_deck(path), threads=threads)
+    o.add_v_perturbation(c.v_perturbation())
+    st = o.step(0)  # warm-up step (first touch of every array)
+    if st:
+        raise RuntimeError(f"oracle status {st}")
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        if o.step(steps + 1):
+            raise RuntimeError("oracle failed")
+        steps += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return c.cells * steps / dt, steps, threads, dt
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    try:
+        import oracle
+        oracle.build()
+        value, steps, threads, secs = cpu_run(args.config, seconds=max(30.0, 3.0 * args.cpu_seconds),
+                                              max_steps=max(1, args.steps))
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle failed: {e}"}))
+        return
+    c = make_case(args.config)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": c.name, "cells": c.cells, "markers": c.nlm, "host": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} full time steps of {c.name} (bounded by time budget)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ device arm
+
+def fp64_gemm_peak(torch, dev):
+    """cuBLAS DGEMM throughput measured in this run (the FP64 denominator;
+    the driver's measured peaks cover copy bandwidth and bf16 only)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = math.inf
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def kernel_table(fb, path, c):
+    """Average device time of every kernel of one step, timed live with CUDA
+    events on the launching stream, on a scratch context."""
+    s = fb.Solver(path)
+    s.advance(0, 2)
+    s.set_substep(1, 1)
+    cells = c.cells
+    B = 8.0 * cells
+    n2m, n3m = c.n2m, c.n3m
+    # (name, stage, launches per step, algorithmic bytes or flops per launch, bound)
+    rows = [
+        ("cfl", "cfl", 1, 2 * B, "hbm"),
+        ("boucdq", "boucdq", 3, 8.0 * 8 * n2m, "hbm"),
+        ("nl_rhs", "nl_rhs", 3, 9 * B, "hbm"),
+        ("helsolve(4 line-solve kernels)", "helsolve", 3, 10 * B, "hbm"),
+        ("divg", "divg", 3, 3 * B, "hbm"),
+        ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+        ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
+        ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+        ("updvp_prcalc", "updvp", 3, 7 * B, "hbm"),
+        ("submean_boucqt", "pr_submean", 3, 2 * B, "hbm"),
+        ("forcing(interp+spread)", "forcing", 2, 0.0, "latency"),
+        ("loads", "loads", 1, 0.0, "latency"),
+    ]
+    out = []
+    for name, st, per_step, work, bound in rows:
+        ms = s.time_stage(st, 2 if st == "forcing" else 1, reps=20)
+        out.append({"kernel": name, "ms": ms, "per_step": per_step, "work": work, "bound": bound})
+    s.close()
+    return out
+
+
+def device_arm(args, rank, world, local):
+    import torch
+    import fribois2d_b200 as fb
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+        dist = dist_mod
+    c = make_case(args.config)
+    path = write_deck(c, rank)
+    s = fb.Solver(path, device=local)
+    pert = c.v_perturbation()
+    q2 = s.get("q2")
+    q2[1:c.n3m + 1] += pert
+    s.set("q2", q2)
+    W, K = max(3, args.warmup), max(1, args.steps)
+    s.advance(0, W)
+    per_step_kernels = s.kernel_count()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    t_wall0 = time.perf_counter()
+    dev_ms = 0.0
+    for i in range(K):
+        flush.zero_()                     # L2 flushed between timed steps
+        s.advance(W + i, 1, history=False)  # device-timed (events on the step's stream)
+        dev_ms += s.last_advance_ms()
+    barrier()
+    wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms_max = float(t.item())
+    value = world * c.cells * K / (dev_ms_max * 1e-3)
+
+    # end to end through the C ABI with host buffers (loose FSI coupling as
+    # the reference runs it: markers in, fluid step, rigid step, state out)
+    e2e = None
+    if not args.no_e2e:
+        nlm = c.nlm
+        pin = [torch.empty(2 * nlm, dtype=torch.float64).pin_memory() for _ in range(4)]
+        fc = torch.empty(8, dtype=torch.float64).pin_memory()
+        for buf, name in zip(pin, ("lmcc", "lmvel", "lmacc", "lmnor")):
+            buf.copy_(torch.from_numpy(s.get(name)))
+        L = fb.lib()
+        ptr = [ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_double)) for b in pin]
+        fptr = ctypes.cast(fc.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        ids = (fb.IDS["lmcc"], fb.IDS["lmvel"], fb.IDS["lmacc"], fb.IDS["lmnor"])
+        ns0 = W + K
+        Ke = max(3, min(K, 20))
+        barrier()
+        te0 = time.perf_counter()
+        for i in range(Ke):
+            ns = ns0 + i
+            assert L.fb_set_markers(s.ctx, *ptr) == 0
+            assert L.fb_fluid_tsch(s.ctx, ns) == 0
+            assert L.fb_rigid(s.ctx, ns, fptr) == 0
+            for b, idx in zip(ptr, ids):
+                assert L.fb_get_array(s.ctx, idx, b, 2 * nlm) == 0
+        barrier()
+        te = time.perf_counter() - te0
+        tt = torch.tensor([te], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * c.cells * Ke / float(tt.item()), "unit": UNIT,
+               "h2d_bytes_per_step": 4 * 2 * nlm * 8, "d2h_bytes_per_step": 4 * 2 * nlm * 8 + 8 * 8,
+               "steps": Ke, "timing": "host wall clock, per-step synchronous C-ABI calls"}
+
+    result = None
+    if rank == 0:
+        table = kernel_table(fb, path, c)
+        peak_fp64 = fp64_gemm_peak(torch, dev)
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except OSError:
+            pass
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        hbm_src = "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "of fallback 6.65 TB/s"
+        step_ms = dev_ms_max / K
+        for r in table:
+            r["share"] = r["ms"] * r["per_step"] / step_ms
+        dom = max((r for r in table if r["bound"] in ("hbm", "tensor")), key=lambda r: r["ms"] * r["per_step"])
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+                tr = json.load(f).get(c.name, {})
+            traffic = tr.get(dom["kernel"])
+        except (OSError, ValueError):
+            pass
+        if dom["bound"] == "tensor":
+            achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e12
+            roof = {"kernel": dom["kernel"], "bound": "tensor", "achieved": achieved, "peak": peak_fp64,
+                    "unit": "TFLOP/s", "frac": achieved / peak_fp64, "traffic": traffic,
+                    "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
+                    "work_per_launch": f"2*n2m*n3m^2 = {dom['work']:.4g} flop"}
+        else:
+            achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e9
+            roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                    "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": hbm_src}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, steps, threads, secs = cpu_run(args.config, seconds=args.cpu_seconds, max_steps=1000)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{steps} full time steps of {c.name} on the oracle ({secs:.1f} s)"}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": c.name, "cells": c.cells, "markers": c.nlm, "dt": c.params.dt,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single case",
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": per_step_kernels * K, "clocks": clk,
+            "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()} for r in table],
+            "wall_s": wall,
+        }
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    device_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -42,7 +42,8 @@ IIDS = dict(lmind=0, eulins=1)
 FIELDS = ("q2", "q3", "pr", "dph", "rhs2", "rhs3", "ru2", "ru3")
 BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", "dq2x2o", "dq3x2o")
 STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
-              phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17)
+              phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17,
+              gemm_fwd=100, poisson_tri=101, gemm_bwd=102)
 HIST_COLS = 21
 HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
               "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm")
@@ -92,6 +93,8 @@ def lib() -> ctypes.CDLL:
         "fb_set_substep": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "fb_stage": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "fb_last_advance_ms": ([vp, dp], ctypes.c_int),
+        "fb_time_stage": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
+        "fb_kernel_count": ([vp, ip], ctypes.c_int),
         "fb_host_create": ([ctypes.c_char_p, P(vp)], ctypes.c_int),
         "fb_host_destroy": ([vp], ctypes.c_int),
         "fb_host_dims": ([vp, ip], ctypes.c_int),
@@ -210,6 +213,18 @@ class Solver:
         ms = ctypes.c_double()
         _check(self._lib.fb_last_advance_ms(self.ctx, ctypes.byref(ms)), "fb_last_advance_ms")
         return ms.value
+
+    def time_stage(self, name: str, n: int = 1, reps: int = 20) -> float:
+        """Average device ms of one launch of a stage (overwrites the state)."""
+        ms = ctypes.c_double()
+        _check(self._lib.fb_time_stage(self.ctx, STAGES[name], int(n), int(reps), ctypes.byref(ms)),
+               f"fb_time_stage({name})")
+        return ms.value
+
+    def kernel_count(self) -> int:
+        v = ctypes.c_int32()
+        _check(self._lib.fb_kernel_count(self.ctx, ctypes.byref(v)), "fb_kernel_count")
+        return v.value
 
     def get_loads(self):
         p = np.zeros(self.nlm)

@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-ffp-c
 UNITS = [
     ("host.cpp", ["-fmad=false"]),
     ("kernels.cu", ["-fmad=false"]),
+    ("tri.cu", []),
     ("api.cu", ["-fmad=false"]),
 ]
 

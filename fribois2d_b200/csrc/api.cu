@@ -18,6 +18,7 @@
 #include "device.cuh"
 #include "host.h"
 #include "kernels.h"
+#include "tri.h"
 
 using fb::Dev;
 using fb::SubDev;
@@ -45,6 +46,9 @@ struct fb_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     double *zmm = nullptr, *zmmt = nullptr;  // Poisson eigenvectors and inverse
+    int null_mode = -1;
+    int own_launches = 0;     // own kernels enqueued (counted while capturing)
+    int step_kernels = 0;     // own kernels per captured step
     // host copies of the scalar state the reference keeps in modules
     double dt = 0, dt_o = 0, beta = 0, al = 0, ga = 0, ro = 0;
     int cur_ns = 0, cur_n = 1;
@@ -93,12 +97,27 @@ int dup(fb_ctx *c, T **p, const std::vector<T> &v) {
 }
 
 // tridiagonal system (lower(2:n), diag, upper(1:n-1)) -> device factors
-int upload_tri(fb_ctx *c, TriDev &t, const std::vector<double> &lo, const std::vector<double> &di,
-               const std::vector<double> &up) {
+int upload_tri(fb_ctx *c, TriDev &t, fb::ScanSys &sc, const std::vector<double> &lo,
+               const std::vector<double> &di, const std::vector<double> &up) {
     fb::TriLU f = fb::factor(lo, di, up);
     if (f.info != 0) return FB_ERR_NUMERIC;
     std::vector<double> dinv(f.d.size());
     for (size_t i = 0; i < f.d.size(); ++i) dinv[i] = 1.0 / f.d[i];
+    {   // recurrence form of DGTTS2 without interchanges (tri.cu)
+        const int n = f.n;
+        std::vector<double> a(static_cast<size_t>(n), 0.0), e(static_cast<size_t>(n), 0.0);
+        for (int i = 1; i < n; ++i) a[static_cast<size_t>(i)] = -f.dl[static_cast<size_t>(i - 1)];
+        for (int i = 0; i + 1 < n; ++i)
+            e[static_cast<size_t>(i)] = -f.du[static_cast<size_t>(i)] * dinv[static_cast<size_t>(i)];
+        double *q;
+        int st2;
+        if ((st2 = dup(c, &q, a))) return st2;
+        sc.a = q;
+        if ((st2 = dup(c, &q, e))) return st2;
+        sc.e = q;
+        if ((st2 = dup(c, &q, dinv))) return st2;
+        sc.g = q;
+    }
     t.n = f.n;
     t.pivoted = f.pivoted ? 1 : 0;
     double *p;
@@ -141,7 +160,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int j = 2; j <= n2; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2 - 1; ++j) up.push_back(ap[j]);
-        if ((st = upload_tri(c, s.y2, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.y2, s.sy2, lo, di, up))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
         s.by2 = p;
     }
@@ -156,7 +175,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int k = 2; k <= n3m; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3m - 1; ++k) up.push_back(ap[k]);
-        if ((st = upload_tri(c, s.z2, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.z2, s.sz2, lo, di, up))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
         s.bz2 = p;
         s.ugkks = 1.0 / (g.g3rm[1] * g.g3rc[1]) * g.dx3q * 2.0 * betadx;
@@ -173,7 +192,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int j = 2; j <= n2m; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2m - 1; ++j) up.push_back(ap[j]);
-        if ((st = upload_tri(c, s.y3, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.y3, s.sy3, lo, di, up))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
         s.by3 = p;
     }
@@ -188,66 +207,62 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int k = 2; k <= n3; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3 - 1; ++k) up.push_back(ap[k]);
-        if ((st = upload_tri(c, s.z3, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.z3, s.sz3, lo, di, up))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
         s.bz3 = p;
     }
     c->usdtal[n] = 1.0 / (c->dt * al);
+    s.scan_ok = !(s.y2.pivoted || s.z2.pivoted || s.y3.pivoted || s.z3.pivoted);
     return FB_OK;
 }
 
-// phcalc_outflow.F90:34-52: per-mode y systems, factorised once
+// phcalc_outflow.F90:34-56: one y system per z mode, (A_y + wr(k) I) x = h.
+// The reference divides each row by its diagonal before DGTTRF; the same
+// solution is obtained here from the LU of the unscaled system, of which only
+// the reciprocal pivots depend on the mode (multipliers are rebuilt on the
+// device from amphj/apphj).  The Neumann null mode (wr = 0 up to round-off)
+// is singular: the reference's answer there is fixed only up to an arbitrary
+// constant, which updvp differentiates away and pr_submean removes, so its
+// last unknown is pinned to zero instead of dividing by a round-off pivot.
 int build_poisson(fb_ctx *c) {
     const fb::Grid &g = c->hc.grid;
     const int n2m = g.n2m, n3m = g.n3m, ldh = c->d.ldh;
-    const size_t tot = static_cast<size_t>(n3m) * ldh;
-    std::vector<double> pb(tot, 0.0), pdl(tot, 0.0), pdinv(tot, 0.0), pdu(tot, 0.0), pdu2(tot, 0.0);
-    std::vector<int> pipiv(tot, 0), ppiv(static_cast<size_t>(n3m), 0);
+    std::vector<double> pg(static_cast<size_t>(n3m) * ldh, 0.0);
+    double wmax = 0.0;
+    int k0 = 0;
+    for (int m = 0; m < n3m; ++m) {
+        wmax = std::max(wmax, std::fabs(c->hc.wr[static_cast<size_t>(m)]));
+        if (std::fabs(c->hc.wr[static_cast<size_t>(m)]) < std::fabs(c->hc.wr[static_cast<size_t>(k0)])) k0 = m;
+    }
+    int nnull = 0;
+    for (int m = 0; m < n3m; ++m)
+        if (std::fabs(c->hc.wr[static_cast<size_t>(m)]) < 1e-9 * wmax) ++nnull;
+    if (nnull != 1) return FB_ERR_NUMERIC;
+    c->null_mode = k0;
     int bad = 0;
 #pragma omp parallel for schedule(static) reduction(+ : bad)
     for (int m = 0; m < n3m; ++m) {
         const double wrk = c->hc.wr[static_cast<size_t>(m)];
-        std::vector<double> lo(static_cast<size_t>(n2m), 0.0), di(static_cast<size_t>(n2m), 1.0),
-            up(static_cast<size_t>(n2m), 0.0), du2(static_cast<size_t>(n2m), 0.0);
-        std::vector<int> ip(static_cast<size_t>(n2m), 0);
-        const size_t o = static_cast<size_t>(m) * ldh;
-        for (int j = 1; j <= n2m; ++j) {
-            double acphT_b = 1.0 / (g.acphj[j] + wrk);
-            pb[o + j - 1] = acphT_b;
-            if (j >= 2) lo[static_cast<size_t>(j - 2)] = g.amphj[j] * acphT_b;
-            if (j <= n2m - 1) up[static_cast<size_t>(j - 1)] = g.apphj[j] * acphT_b;
-        }
-        if (fb::dgttrf(n2m, lo.data(), di.data(), up.data(), du2.data(), ip.data()) != 0) ++bad;
-        for (int j = 0; j < n2m; ++j) {
-            pdinv[o + j] = 1.0 / di[static_cast<size_t>(j)];
-            pipiv[o + j] = ip[static_cast<size_t>(j)];
-            if (ip[static_cast<size_t>(j)] != j + 1) ppiv[static_cast<size_t>(m)] = 1;
-            if (j < n2m - 1) {
-                pdl[o + j] = lo[static_cast<size_t>(j)];
-                pdu[o + j] = up[static_cast<size_t>(j)];
+        double *gm = pg.data() + static_cast<size_t>(m) * ldh;
+        double dprev = g.acphj[1] + wrk;
+        gm[0] = 1.0 / dprev;
+        for (int i = 1; i < n2m; ++i) {
+            const double l = g.amphj[i + 1] / dprev;
+            const double di = (g.acphj[i + 1] + wrk) - l * g.apphj[i];
+            if (m == k0 && i == n2m - 1) {
+                gm[i] = 0.0;  // gauge of the null mode
+                break;
             }
-            if (j < n2m - 2) pdu2[o + j] = du2[static_cast<size_t>(j)];
+            if (!(std::fabs(di) > 0.0) || !std::isfinite(di)) ++bad;
+            gm[i] = 1.0 / di;
+            dprev = di;
         }
     }
     if (bad) return FB_ERR_NUMERIC;
-    int st;
     double *p;
-    int *ip;
-    Dev &d = c->d;
-    if ((st = dup(c, &p, pb))) return st;
-    d.pb = p;
-    if ((st = dup(c, &p, pdl))) return st;
-    d.pdl = p;
-    if ((st = dup(c, &p, pdinv))) return st;
-    d.pdinv = p;
-    if ((st = dup(c, &p, pdu))) return st;
-    d.pdu = p;
-    if ((st = dup(c, &p, pdu2))) return st;
-    d.pdu2 = p;
-    if ((st = dup(c, &ip, pipiv))) return st;
-    d.pipiv = ip;
-    if ((st = dup(c, &ip, ppiv))) return st;
-    d.ppiv = ip;
+    int st;
+    if ((st = dup(c, &p, pg))) return st;
+    c->d.pg = p;
     return FB_OK;
 }
 
@@ -266,6 +281,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     }
     c->device = device;
     CK(cudaSetDevice(device));
+    CK(fb::scan_configure());
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -480,6 +496,8 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     const SubDev &s = c->sub[n - 1];
     cudaStream_t st = c->stream;
     int r = FB_OK;
+    static const int kOwn[18] = {1, 1, 1, 0, 0, 0, 1, 2, 4, 1, 1, 1, 0, 1, 0, 2, 2, 1};
+    if (stage >= 0 && stage < 18) c->own_launches += kOwn[stage] + ((stage == FB_ST_FORCING && n == 1) ? 1 : 0);
     switch (stage) {
     case FB_ST_CFL: fb::launch_cfl(d, st); break;
     case FB_ST_BOUCDQ: fb::launch_boucdq(d, ga, ro, st); break;
@@ -494,11 +512,14 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         fb::launch_mls_interp(d, st);
         fb::launch_mls_spread(d, st);
         break;
-    case FB_ST_HELSOLVE: fb::launch_helsolve(d, s, st); break;
+    case FB_ST_HELSOLVE:
+        if (s.scan_ok) fb::launch_scan_helsolve(d, s, st);
+        else fb::launch_helsolve(d, s, st);
+        break;
     case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
     case FB_ST_PHCALC:
         if ((r = gemm_fwd(c))) return r;
-        fb::launch_tri_poisson(d, st);
+        fb::launch_scan_poisson(d, st);
         if ((r = gemm_bwd(c))) return r;
         break;
     case FB_ST_UPDVP: fb::launch_updvp_prcalc(d, al, al * c->beta, st); break;
@@ -506,6 +527,9 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_ST_CHECKBCS:
     case FB_ST_LOADS: fb::launch_loads(d, st); break;
     case FB_ST_RIGID: fb::launch_rigid(d, c->hist_cap, st); break;
+    case FB_TK_GEMM_FWD: return gemm_fwd(c);
+    case FB_TK_POISSON_TRI: fb::launch_scan_poisson(d, st); break;
+    case FB_TK_GEMM_BWD: return gemm_bwd(c);
     default: return FB_ERR_STATE;
     }
     if (cudaGetLastError() != cudaSuccess) return FB_ERR_CUDA;
@@ -543,8 +567,8 @@ int enqueue_step(fb_ctx *c, int ns) {
 }
 
 int read_status(fb_ctx *c, int *status) {
+    CK(cudaMemcpyAsync(status, c->d.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    CK(cudaMemcpy(status, c->d.status, sizeof(int), cudaMemcpyDeviceToHost));
     return FB_OK;
 }
 
@@ -556,7 +580,9 @@ void host_clock(fb_ctx *c, int nsteps) {
 int capture_step(fb_ctx *c) {
     if (c->graph_exec) return FB_OK;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->own_launches = 0;
     int r = enqueue_step(c, 1);
+    c->step_kernels = c->own_launches;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (r) {
@@ -803,14 +829,16 @@ int fb_get_array(fb_ctx *c, int id, double *host, int64_t n) {
     CK(cudaStreamSynchronize(c->stream));
     if (field_ptr(c, id, &p) == FB_OK) {
         if (n != static_cast<int64_t>(d.NK) * d.n2) return FB_ERR_STATE;
-        CK(cudaMemcpy2D(host, d.n2 * sizeof(double), p, d.P * sizeof(double), d.n2 * sizeof(double), d.NK,
-                        cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy2DAsync(host, d.n2 * sizeof(double), p, d.P * sizeof(double), d.n2 * sizeof(double), d.NK,
+                             cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         return FB_OK;
     }
     if (id == FB_SCALARS) {
         if (n != 13) return FB_ERR_STATE;
         double s[fb::S_COUNT];
-        CK(cudaMemcpy(s, d.scal, sizeof(s), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(s, d.scal, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         const double v[13] = {s[fb::S_TIME], c->dt, c->dt_o, c->beta, c->al, c->ga, c->ro, s[fb::S_CFLM],
                               s[fb::S_Q3AVG], s[fb::S_NBCV], s[fb::S_NBCW], d.ddmin, s[fb::S_PRAVG]};
         std::memcpy(host, v, sizeof(v));
@@ -824,7 +852,9 @@ int fb_get_array(fb_ctx *c, int id, double *host, int64_t n) {
     int64_t cnt = 0;
     bool one_based = false;
     if (vec_ptr(c, id, &p, &cnt, &one_based) != FB_OK || n != cnt) return FB_ERR_STATE;
-    CK(cudaMemcpy(host, p + (one_based ? 1 : 0), static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(host, p + (one_based ? 1 : 0), static_cast<size_t>(n) * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return FB_OK;
 }
 
@@ -835,8 +865,9 @@ int fb_set_array(fb_ctx *c, int id, const double *host, int64_t n) {
     CK(cudaStreamSynchronize(c->stream));
     if (field_ptr(c, id, &p) == FB_OK) {
         if (n != static_cast<int64_t>(d.NK) * d.n2) return FB_ERR_STATE;
-        CK(cudaMemcpy2D(p, d.P * sizeof(double), host, d.n2 * sizeof(double), d.n2 * sizeof(double), d.NK,
-                        cudaMemcpyHostToDevice));
+        CK(cudaMemcpy2DAsync(p, d.P * sizeof(double), host, d.n2 * sizeof(double), d.n2 * sizeof(double), d.NK,
+                             cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         return FB_OK;
     }
     if (id == FB_WR || id == FB_ZMM || id == FB_ZMMT) return FB_ERR_STATE;  // set-up data is immutable
@@ -844,7 +875,9 @@ int fb_set_array(fb_ctx *c, int id, const double *host, int64_t n) {
     bool one_based = false;
     if (vec_ptr(c, id, &p, &cnt, &one_based) != FB_OK || n != cnt) return FB_ERR_STATE;
     if (one_based && id >= FB_RC) return FB_ERR_STATE;  // grid data is immutable
-    CK(cudaMemcpy(p + (one_based ? 1 : 0), host, static_cast<size_t>(n) * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(p + (one_based ? 1 : 0), host, static_cast<size_t>(n) * sizeof(double),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return FB_OK;
 }
 
@@ -853,11 +886,13 @@ int fb_get_iarray(fb_ctx *c, int id, int32_t *host, int64_t n) {
     CK(cudaStreamSynchronize(c->stream));
     const int64_t nlm = c->d.nlm;
     if (id == FB_LMIND && n == 4 * nlm) {
-        CK(cudaMemcpy(host, c->d.lmind, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(host, c->d.lmind, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         return FB_OK;
     }
     if (id == FB_EULINS && n == 36 * nlm) {
-        CK(cudaMemcpy(host, c->d.eulins, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(host, c->d.eulins, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         return FB_OK;
     }
     return FB_ERR_STATE;
@@ -890,6 +925,31 @@ int fb_stage(fb_ctx *c, int stage, int n) {
     int status = 0;
     if ((r = read_status(c, &status))) return r;
     return status;
+}
+
+int fb_time_stage(fb_ctx *c, int stage, int n, int reps, double *ms) {
+    if (!c || !ms || reps < 1 || n < 1 || n > c->d.nsst) return FB_ERR_STATE;
+    int r = stage_impl(c, stage, c->cur_ns, n);
+    if (r) return r;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int i = 0; i < reps; ++i)
+        if ((r = stage_impl(c, stage, c->cur_ns, n))) return r;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+    *ms = static_cast<double>(t) / reps;
+    CK(cudaMemsetAsync(c->d.status, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FB_OK;
+}
+
+int fb_kernel_count(fb_ctx *c, int32_t *per_step) {
+    if (!c || !per_step) return FB_ERR_STATE;
+    int r = capture_step(c);
+    if (r) return r;
+    *per_step = c->step_kernels;
+    return FB_OK;
 }
 
 int fb_last_advance_ms(fb_ctx *c, double *ms) {

@@ -18,10 +18,16 @@ struct TriDev {          // factors of one tridiagonal system (DGTTRF output)
     const int *ipiv;     // 1-based pivot rows as LAPACK returns them
 };
 
+struct ScanSys {         // LU substitution as two recurrences (tri.cu)
+    const double *a, *e, *g;  // y(i) = a(i) y(i-1) + b(i);  x(i) = e(i) x(i+1) + g(i) y(i)
+};
+
 struct SubDev {          // substep constants (fluid_tsch.F90:64-77)
     double al, ga, ro, beta, betadx, usdtal, ugkks, ugkkn;
     const double *by2, *bz2, *by3, *bz3;  // row normalisers 1/(1 - betadx*ac), 1-based
     TriDev y2, z2, y3, z3;                // solq2j, solq2k, solq3j, solq3k systems
+    ScanSys sy2, sz2, sy3, sz3;           // the same systems for the scan solver
+    int scan_ok;                          // 0 if a system needed row interchanges
 };
 
 struct Dev {
@@ -34,9 +40,8 @@ struct Dev {
     const double *am2j, *ac2j, *ap2j, *am3j, *ac3j, *ap3j;
     const double *am3ck, *ac3ck, *ap3ck, *am3sk, *ac3sk, *ap3sk;
     const double *amphj, *acphj, *apphj, *amphk, *acphk, *apphk;
-    // Poisson per-mode data, [k][j] with row pitch ldh
-    const double *pb, *pdl, *pdinv, *pdu, *pdu2;
-    const int *pipiv, *ppiv;
+    // Poisson: reciprocal pivots of each mode's y system, [mode][j] pitch ldh
+    const double *pg;
     // fields
     double *q2, *q3, *pr, *dph, *rhs2, *rhs3, *ru2, *ru3, *hmn;
     // inflow / outflow (1-based)

@@ -645,18 +645,6 @@ __global__ void k_divg(Dev d, double usdtal) {
     Fv(d.dph, jc, kc) = dqcap * usdtal;
 }
 
-// phcalc_outflow.F90:33-56: per z-mode tridiagonal in y, factors precomputed
-__global__ void k_tri_poisson(Dev d) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;  // mode k - 1
-    if (m >= d.n3m) return;
-    const size_t off = static_cast<size_t>(m) * static_cast<size_t>(d.ldh);
-    double *b = d.hmn + off;
-    const double *pb = d.pb + off;
-    for (int j = 0; j < d.n2m; ++j) b[j] = b[j] * pb[j];
-    TriDev f{d.n2m, d.ppiv[m], d.pdl, d.pdinv, d.pdu, d.pdu2, d.pipiv};
-    gtts2(f, off, b, 1);
-}
-
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
 // partial sums of pr_submean (updvp.F90:320-333)
 __global__ void k_updvp_prcalc(Dev d, double al, double be) {
@@ -1124,7 +1112,6 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     dim3 b(32, 8);
     k_divg<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, usdtal);
 }
-void launch_tri_poisson(const Dev &d, cudaStream_t s) { k_tri_poisson<<<(d.n3m + 63) / 64, 64, 0, s>>>(d); }
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
     dim3 b(32, 8);
     k_updvp_prcalc<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, al, be);

@@ -18,7 +18,6 @@ void launch_mls_interp(const Dev &d, cudaStream_t s);
 void launch_mls_spread(const Dev &d, cudaStream_t s);
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
 void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
-void launch_tri_poisson(const Dev &d, cudaStream_t s);
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s);
 void launch_loads(const Dev &d, cudaStream_t s);

@@ -1,0 +1,17 @@
+// Batched tridiagonal line solves (definitions in tri.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace fb {
+
+constexpr int kYLines = 8;  // contiguous lines per block (one warp each)
+constexpr int kZLines = 4;  // strided lines per block (one warp each)
+
+cudaError_t scan_configure();
+void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
+void launch_scan_poisson(const Dev &d, cudaStream_t st);
+
+}  // namespace fb

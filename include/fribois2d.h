@@ -167,6 +167,16 @@ int fb_stage(fb_ctx *ctx, int stage, int n);
 
 /* ---- timing: device time of the last fb_advance, and per-kernel totals --- */
 int fb_last_advance_ms(fb_ctx *ctx, double *ms);
+/* Average device time (CUDA events on the context stream) of one launch of
+ * a stage or of one of its kernels, over reps launches after one warm-up.
+ * It overwrites the state: use a context dedicated to measurement. */
+#define FB_TK_GEMM_FWD 100   /* phcalc_outflow.F90:31 eigen transform (cuBLAS DGEMM) */
+#define FB_TK_POISSON_TRI 101 /* phcalc_outflow.F90:34-56 per-mode y solves */
+#define FB_TK_GEMM_BWD 102   /* phcalc_outflow.F90:61 back transform */
+int fb_time_stage(fb_ctx *ctx, int stage, int n, int reps, double *ms);
+/* Number of this library's own kernels one captured time step launches
+ * (library kernels of cuBLAS and CUB are not counted). */
+int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
 
 /* ---- host-only set-up (no GPU touched; usable on a CPU-only machine) ----- */
 int fb_host_create(const char *input_dir, fb_host **out);
