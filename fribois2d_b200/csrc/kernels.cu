@@ -794,24 +794,27 @@ __device__ void getpbup_one(const Dev &d, const double *f, const int eul[2][kSD]
     }
 }
 
-// loads_transfer_c (loads_transfer.F90:143-185), per-marker part: probe
-// interpolation of v, w, p with first and second derivatives, and the
-// marker's own tangent; plus checkbcs (ckbcs.F90:29-60).
+// loads_transfer_c (loads_transfer.F90:143-185), per-marker part: the
+// probe interpolation of v, w or p with first and second derivatives (one
+// thread per marker and quantity); the v and w threads also form checkbcs
+// (ckbcs.F90:29-60) with the substep-1 weights.
 __global__ void k_loads_probe(Dev d) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= d.nlm) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * d.nlm) return;
+    const int n = t / 3, idir = t % 3 + 1;
     double *pb = d.probe + static_cast<size_t>(n) * 24;
-    pb[23] = -1.0;  // skipped
-    d.bcerrv[n] = 0.0;
-    d.bcerrw[n] = 0.0;
-    if (*d.status) return;
     const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
-    if (!(d.zz[1] < pos[1] && pos[1] < d.zz[d.n3])) return;
-    // checkbcs with the substep-1 weights (phipred) and the final velocity
-    for (int idir = 1; idir <= 2; ++idir) {
-        const int t = 2 * n + idir - 1;
-        const double *phi = d.phi + static_cast<size_t>(t) * kSD;
-        const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+    const bool inside = (d.zz[1] < pos[1] && pos[1] < d.zz[d.n3]);
+    if (idir == 1) {
+        pb[23] = inside ? 0.0 : -1.0;
+        d.bcerrv[n] = 0.0;
+    }
+    if (idir == 2) d.bcerrw[n] = 0.0;
+    if (*d.status || !inside) return;
+    if (idir <= 2) {
+        const int tt = 2 * n + idir - 1;
+        const double *phi = d.phi + static_cast<size_t>(tt) * kSD;
+        const int *eu = d.eulins + static_cast<size_t>(tt) * 2 * kSD;
         const double *q = (idir == 1) ? d.q2 : d.q3;
         double u = 0.0;
         for (int m = 0; m < kSD; ++m) u = u + phi[m] * q[fidx(d, eu[m], eu[kSD + m])];
@@ -820,45 +823,25 @@ __global__ void k_loads_probe(Dev d) {
     }
     const double hpr = d.ddmin * d.kprobe;
     const double probe[2] = {pos[0] + d.lmnor[2 * n] * hpr, pos[1] + d.lmnor[2 * n + 1] * hpr};
-    double res[3][7];
-    for (int idir = 1; idir <= 3; ++idir) {
-        int mj, mk;
-        if (idir == 3) {
-            mj = d.lmind[4 * n + 2];
-            mk = d.lmind[4 * n + 1];
-        } else {
-            mj = d.lmind[4 * n + 2 * (idir - 1)];
-            mk = d.lmind[4 * n + 2 * (idir - 1) + 1];
-        }
-        int ij, ik;
-        double sdc[2][kSD], sdd[2][kSD], ph[3][kSD];
-        int eul[2][kSD];
-        if (!probeind(d, idir, mj, mk, probe, ij, ik) || !sd_ind(d, idir, ij, ik, sdc, sdd, eul) ||
-            eul[0][0] < 2) {
-            raise_status(d, FB_ERR_MARKER_OUT);
-            return;
-        }
-        if (!mls_sf_d(d, probe, sdc, sdd, ph)) raise_status(d, FB_ERR_MLS);
-        const double *f = (idir == 1) ? d.q2 : (idir == 2 ? d.q3 : d.pr);
-        getpbup_one(d, f, eul, ph, res[idir - 1]);
-    }
-    for (int i = 0; i < 7; ++i) {
-        pb[i] = res[0][i];
-        pb[7 + i] = res[1][i];
-        pb[14 + i] = res[2][i];
-    }
-    const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
-    const double vel0 = res[0][0], vel1 = res[1][0];
-    const double veln_md = vel0 * nory + vel1 * norz;
-    const double velt0 = vel0 - veln_md * nory, velt1 = vel1 - veln_md * norz;
-    const double velt_md = sqrt(velt0 * velt0 + velt1 * velt1);
-    if (velt_md != 0.0) {
-        pb[21] = velt0 / sqrt(velt0 * velt0 + velt1 * velt1);
-        pb[22] = velt1 / sqrt(velt0 * velt0 + velt1 * velt1);
-        pb[23] = 1.0;
+    int mj, mk;
+    if (idir == 3) {
+        mj = d.lmind[4 * n + 2];
+        mk = d.lmind[4 * n + 1];
     } else {
-        pb[23] = 0.0;
+        mj = d.lmind[4 * n + 2 * (idir - 1)];
+        mk = d.lmind[4 * n + 2 * (idir - 1) + 1];
     }
+    int ij, ik;
+    double sdc[2][kSD], sdd[2][kSD], ph[3][kSD], res[7];
+    int eul[2][kSD];
+    if (!probeind(d, idir, mj, mk, probe, ij, ik) || !sd_ind(d, idir, ij, ik, sdc, sdd, eul) || eul[0][0] < 2) {
+        raise_status(d, FB_ERR_MARKER_OUT);
+        return;
+    }
+    if (!mls_sf_d(d, probe, sdc, sdd, ph)) raise_status(d, FB_ERR_MLS);
+    const double *f = (idir == 1) ? d.q2 : (idir == 2 ? d.q3 : d.pr);
+    getpbup_one(d, f, eul, ph, res);
+    for (int i = 0; i < 7; ++i) pb[7 * (idir - 1) + i] = res[i];
 }
 
 // loads_transfer_c (loads_transfer.F90:187-214): the tangent carries over
@@ -869,7 +852,27 @@ __global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
     __shared__ double sh[1024];
     const double hpr = d.ddmin * d.kprobe, visc = d.visc;
     double sv = 0.0, sw = 0.0;
-    if (*d.status == 0) {
+    const bool ok = (*d.status == 0);
+    if (ok) {   // the probe's own tangent (loads_transfer.F90:177-185)
+        for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
+            double *pb = d.probe + static_cast<size_t>(n) * 24;
+            if (pb[23] < 0.0) continue;
+            const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
+            const double vel0 = pb[0], vel1 = pb[7];
+            const double veln_md = vel0 * nory + vel1 * norz;
+            const double velt0 = vel0 - veln_md * nory, velt1 = vel1 - veln_md * norz;
+            const double velt_md = sqrt(velt0 * velt0 + velt1 * velt1);
+            if (velt_md != 0.0) {
+                pb[21] = velt0 / sqrt(velt0 * velt0 + velt1 * velt1);
+                pb[22] = velt1 / sqrt(velt0 * velt0 + velt1 * velt1);
+                pb[23] = 1.0;
+            } else {
+                pb[23] = 0.0;
+            }
+        }
+    }
+    __syncthreads();
+    if (ok) {
         for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
             const double *pb = d.probe + static_cast<size_t>(n) * 24;
             d.press[n] = 0.0;
@@ -1093,10 +1096,10 @@ void launch_lgrdist(const Dev &d, cudaStream_t s) {
     if (d.nlm) k_lgrdist<<<(d.nlm + 127) / 128, 128, 0, s>>>(d);
 }
 void launch_mls_setup(const Dev &d, cudaStream_t s) {
-    if (d.nlm) k_mls_setup<<<(2 * d.nlm + 127) / 128, 128, 0, s>>>(d);
+    if (d.nlm) k_mls_setup<<<(2 * d.nlm + 63) / 64, 64, 0, s>>>(d);
 }
 void launch_mls_interp(const Dev &d, cudaStream_t s) {
-    if (d.nlm) k_mls_interp<<<(2 * d.nlm + 127) / 128, 128, 0, s>>>(d);
+    if (d.nlm) k_mls_interp<<<(2 * d.nlm + 63) / 64, 64, 0, s>>>(d);
 }
 void launch_mls_spread(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;
@@ -1122,7 +1125,7 @@ void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
 }
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
-    k_loads_probe<<<(d.nlm + 127) / 128, 128, 0, s>>>(d);
+    k_loads_probe<<<(3 * d.nlm + 63) / 64, 64, 0, s>>>(d);
     k_loads_finish<<<1, 1024, 0, s>>>(d);
 }
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s) {

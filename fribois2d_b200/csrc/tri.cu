@@ -7,10 +7,17 @@
 // substitution,
 //     forward   y(i) = a(i) y(i-1) + b(i),        a(0)   = 0
 //     backward  x(i) = e(i) x(i+1) + g(i) y(i),   e(n-1) = 0
-// Each line is staged in shared memory with coalesced loads and solved by
-// one warp: every lane owns a contiguous chunk, composes its chunk's affine
-// map, a 5-step shuffle scan gives each lane its incoming value, and the
-// lane then applies its chunk.  Depth is O(n/32 + log 32) instead of O(n).
+// A line is cut into contiguous chunks held in registers by consecutive
+// threads.  Each thread composes the affine map of its chunk, a scan over
+// the chunks (warp shuffles, plus shared memory across warps for long
+// lines) gives every chunk its incoming value, and the chunk is applied.
+// Depth is O(n/chunks + log chunks); every element is loaded and stored
+// once, with all of a thread's loads independent and in flight together.
+//
+// Lines along y are contiguous in memory: one warp per line, staged through
+// shared memory so that global accesses are coalesced.  Lines along z are
+// strided: four neighbouring lines share each 32-byte sector, so a block
+// interleaves four lines over its lanes and splits k among its warps.
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -24,37 +31,76 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// y-direction coefficient sets: 1-D arrays shared by all lines
-struct CoefShared {
+struct CoefShared {      // y or z systems: 1-D factors shared by all lines
     const double *a, *e, *g;
     __device__ double A(int i) const { return __ldg(a + i); }
     __device__ double E(int i) const { return __ldg(e + i); }
     __device__ double G(int i) const { return __ldg(g + i); }
 };
 
-// Poisson mode: only the reciprocal pivots depend on the mode; the
-// multipliers follow from the operator's off-diagonals (1-based arrays)
-struct CoefMode {
-    const double *g;       // this mode's 1/d(i), i = 0..n-1
-    const double *amphj, *apphj;
+struct CoefMode {        // Poisson mode: reciprocal pivots per mode, 1-based off-diagonals
+    const double *g, *amphj, *apphj;
     int n;
     __device__ double A(int i) const { return i == 0 ? 0.0 : -(__ldg(amphj + i + 1) * __ldg(g + i - 1)); }
     __device__ double E(int i) const { return i == n - 1 ? 0.0 : -(__ldg(apphj + i + 1) * __ldg(g + i)); }
     __device__ double G(int i) const { return __ldg(g + i); }
 };
 
-template <class Co>
-__device__ __forceinline__ void warp_solve(double *v, int n, const Co &co) {
+// composite affine map of a chunk, forward order
+template <int M, class Co>
+__device__ __forceinline__ void fwd_compose(const double (&v)[M], int i0, int cnt, const Co &co, double &A,
+                                            double &C) {
+    A = 1.0;
+    C = 0.0;
+#pragma unroll
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) {
+            const double a = co.A(i0 + t);
+            C = fma(a, C, v[t]);
+            A *= a;
+        }
+}
+
+template <int M, class Co>
+__device__ __forceinline__ void fwd_apply(double (&v)[M], int i0, int cnt, const Co &co, double y) {
+#pragma unroll
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) {
+            y = fma(co.A(i0 + t), y, v[t]);
+            v[t] = y;
+        }
+}
+
+template <int M, class Co>
+__device__ __forceinline__ void bwd_compose(const double (&v)[M], int i0, int cnt, const Co &co, double &A,
+                                            double &C) {
+    A = 1.0;
+    C = 0.0;
+#pragma unroll
+    for (int t = M - 1; t >= 0; --t)
+        if (t < cnt) {
+            const double e = co.E(i0 + t);
+            C = fma(e, C, co.G(i0 + t) * v[t]);
+            A *= e;
+        }
+}
+
+template <int M, class Co>
+__device__ __forceinline__ void bwd_apply(double (&v)[M], int i0, int cnt, const Co &co, double x) {
+#pragma unroll
+    for (int t = M - 1; t >= 0; --t)
+        if (t < cnt) {
+            x = fma(co.E(i0 + t), x, co.G(i0 + t) * v[t]);
+            v[t] = x;
+        }
+}
+
+// one warp = one line of n unknowns, chunk of m = ceil(n/32) per lane
+template <int M, class Co>
+__device__ __forceinline__ void warp_line(double (&v)[M], int i0, int cnt, const Co &co) {
     const int lane = threadIdx.x & 31;
-    const int m = (n + 31) >> 5;
-    const int i0 = min(lane * m, n), i1 = min(i0 + m, n);
-    // forward substitution
-    double A = 1.0, C = 0.0;
-    for (int i = i0; i < i1; ++i) {
-        const double a = co.A(i);
-        C = fma(a, C, v[i]);
-        A *= a;
-    }
+    double A, C;
+    fwd_compose(v, i0, cnt, co, A, C);
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
         const double Ao = __shfl_up_sync(kFull, A, dd), Co_ = __shfl_up_sync(kFull, C, dd);
@@ -65,18 +111,8 @@ __device__ __forceinline__ void warp_solve(double *v, int n, const Co &co) {
     }
     double y = __shfl_up_sync(kFull, C, 1);
     if (lane == 0) y = 0.0;
-    for (int i = i0; i < i1; ++i) {
-        y = fma(co.A(i), y, v[i]);
-        v[i] = y;
-    }
-    // back substitution
-    A = 1.0;
-    C = 0.0;
-    for (int i = i1 - 1; i >= i0; --i) {
-        const double e = co.E(i);
-        C = fma(e, C, co.G(i) * v[i]);
-        A *= e;
-    }
+    fwd_apply(v, i0, cnt, co, y);
+    bwd_compose(v, i0, cnt, co, A, C);
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
         const double Ao = __shfl_down_sync(kFull, A, dd), Co_ = __shfl_down_sync(kFull, C, dd);
@@ -87,174 +123,242 @@ __device__ __forceinline__ void warp_solve(double *v, int n, const Co &co) {
     }
     double x = __shfl_down_sync(kFull, C, 1);
     if (lane == 31) x = 0.0;
-    for (int i = i1 - 1; i >= i0; --i) {
-        x = fma(co.E(i), x, co.G(i) * v[i]);
-        v[i] = x;
-    }
+    bwd_apply(v, i0, cnt, co, x);
 }
 
-inline __device__ int odd_ld(int n) { return n | 1; }
+// kZLines lines interleaved over the lanes (line = lane % 4), chunks over
+// lane/4 and the block's warps; shA/shC hold one composite per (warp, line)
+template <int M, class Co>
+__device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, const Co &co, double *shA,
+                                            double *shC) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
+    const int l = lane & (kZLines - 1), sub = lane / kZLines;
+    constexpr int kSub = 32 / kZLines;
+    double A, C, Ao, Co_;
+    // ---- forward
+    fwd_compose(v, i0, cnt, co, A, C);
+#pragma unroll
+    for (int dd = kZLines; dd < 32; dd <<= 1) {
+        Ao = __shfl_up_sync(kFull, A, dd);
+        Co_ = __shfl_up_sync(kFull, C, dd);
+        if (lane >= dd) {
+            C = fma(A, Co_, C);
+            A *= Ao;
+        }
+    }
+    if (sub == kSub - 1) {
+        shA[w * kZLines + l] = A;
+        shC[w * kZLines + l] = C;
+    }
+    double Aex = __shfl_up_sync(kFull, A, kZLines), Cex = __shfl_up_sync(kFull, C, kZLines);
+    if (sub == 0) {
+        Aex = 1.0;
+        Cex = 0.0;
+    }
+    __syncthreads();
+    double PC = 0.0;
+    for (int q = 0; q < w; ++q) PC = fma(shA[q * kZLines + l], PC, shC[q * kZLines + l]);
+    fwd_apply(v, i0, cnt, co, fma(Aex, PC, Cex));
+    __syncthreads();
+    // ---- backward
+    bwd_compose(v, i0, cnt, co, A, C);
+#pragma unroll
+    for (int dd = kZLines; dd < 32; dd <<= 1) {
+        Ao = __shfl_down_sync(kFull, A, dd);
+        Co_ = __shfl_down_sync(kFull, C, dd);
+        if (lane + dd < 32) {
+            C = fma(A, Co_, C);
+            A *= Ao;
+        }
+    }
+    if (sub == 0) {
+        shA[w * kZLines + l] = A;
+        shC[w * kZLines + l] = C;
+    }
+    Aex = __shfl_down_sync(kFull, A, kZLines);
+    Cex = __shfl_down_sync(kFull, C, kZLines);
+    if (sub == kSub - 1) {
+        Aex = 1.0;
+        Cex = 0.0;
+    }
+    __syncthreads();
+    double SC = 0.0;
+    for (int q = W - 1; q > w; --q) SC = fma(shA[q * kZLines + l], SC, shC[q * kZLines + l]);
+    bwd_apply(v, i0, cnt, co, fma(Aex, SC, Cex));
+}
 
 }  // namespace
 
-// solq2j (solve_fluid.F90:135-157): lines k = 1..n3m of n2 unknowns, rows 1
-// and n2 identity with zero right-hand side; result stays in rhs2.
-__global__ void __launch_bounds__(kYLines * 32) k_scan_y2(Dev d, ScanSys s, const double *by) {
-    extern __shared__ double sm[];
-    const int n = d.n2, ld = odd_ld(n);
-    const int k0 = blockIdx.x * kYLines + 1;
-    for (int l = 0; l < kYLines; ++l) {
-        const int k = k0 + l;
-        if (k > d.n3m) break;
-        const double *row = d.rhs2 + fidx(d, 1, k);
-        for (int j = threadIdx.x + 1; j <= n; j += blockDim.x)
-            sm[l * ld + j - 1] = (j >= 2 && j <= d.n2m) ? row[j - 1] * by[j] : 0.0;
-    }
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    if (k0 + w <= d.n3m) warp_solve(sm + w * ld, n, CoefShared{s.a, s.e, s.g});
-    __syncthreads();
-    for (int l = 0; l < kYLines; ++l) {
-        const int k = k0 + l;
-        if (k > d.n3m) break;
-        double *row = d.rhs2 + fidx(d, 1, k);
-        for (int j = threadIdx.x; j < n; j += blockDim.x) row[j] = sm[l * ld + j];
-    }
-}
+// ---------------------------------------------------------------- y lines
 
-// solq3j (solve_fluid.F90:79-101): lines k = 2..n3m of n2m unknowns
-__global__ void __launch_bounds__(kYLines * 32) k_scan_y3(Dev d, ScanSys s, const double *by) {
+// Rows of a k-major field staged through shared memory: load row (scaled),
+// solve with a warp per line, write back.  kind: 0 = solq2j, 1 = solq3j,
+// 2 = Poisson mode (rows of hmn).
+template <int M, int kKind>
+__global__ void __launch_bounds__(kYLines * 32) k_ylines(Dev d, ScanSys s, const double *by) {
     extern __shared__ double sm[];
-    const int n = d.n2m, ld = odd_ld(n);
-    const int k0 = blockIdx.x * kYLines + 2;
+    int n, first, last;
+    if (kKind == 0) n = d.n2, first = 1, last = d.n3m;
+    else if (kKind == 1) n = d.n2m, first = 2, last = d.n3m;
+    else n = d.n2m, first = 0, last = d.n3m - 1;
+    const int ld = n + 1;
+    const int r0 = first + blockIdx.x * kYLines;
+    const int nt = blockDim.x, tid = threadIdx.x;
+    // coalesced staging of the block's rows
     for (int l = 0; l < kYLines; ++l) {
-        const int k = k0 + l;
-        if (k > d.n3m) break;
-        const double *row = d.rhs3 + fidx(d, 1, k);
-        for (int j = threadIdx.x + 1; j <= n; j += blockDim.x) sm[l * ld + j - 1] = row[j - 1] * by[j];
-    }
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    if (k0 + w <= d.n3m) warp_solve(sm + w * ld, n, CoefShared{s.a, s.e, s.g});
-    __syncthreads();
-    for (int l = 0; l < kYLines; ++l) {
-        const int k = k0 + l;
-        if (k > d.n3m) break;
-        double *row = d.rhs3 + fidx(d, 1, k);
-        for (int j = threadIdx.x; j < n; j += blockDim.x) row[j] = sm[l * ld + j];
-    }
-}
-
-// solq2k (solve_fluid.F90:185-224) and helsolve.F90:32-33: lines j of n3m
-// unknowns with the inflow/outflow terms; q2 += x; wall columns zeroed.
-__global__ void __launch_bounds__(kZLines * 32) k_scan_z2(Dev d, ScanSys s, const double *bz, double ugkks,
-                                                          double ugkkn) {
-    extern __shared__ double sm[];
-    const int n = d.n3m, ld = odd_ld(n);
-    const int j0 = blockIdx.x * kZLines + 1;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int t = tid; t < kZLines * n; t += nt) {
-        const int l = t % kZLines, k = t / kZLines + 1, j = j0 + l;
-        double v = 0.0;
-        if (j <= d.n2m) {
-            v = Fv(d.rhs2, j, k) * bz[k];
-            if (k == 1) v = v + d.dqb2s[j] * ugkks;
-            if (k == n) v = v + d.dqb2n[j] * ugkkn;
+        const int r = r0 + l;
+        if (r > last) break;
+        const double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh
+                                         : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
+        double *dst = sm + l * ld;
+#pragma unroll 4
+        for (int i = tid; i < n; i += nt) {
+            double v = __ldcg(row + i);
+            if (kKind == 0) v = (i >= 1 && i <= n - 2) ? v * __ldg(by + i + 1) : 0.0;
+            else if (kKind == 1) v = v * __ldg(by + i + 1);
+            dst[i] = v;
         }
-        sm[l * ld + k - 1] = v;
     }
     __syncthreads();
-    const int w = tid >> 5;
-    if (j0 + w <= d.n2m && j0 + w >= 2) warp_solve(sm + w * ld, n, CoefShared{s.a, s.e, s.g});
-    __syncthreads();
-    for (int t = tid; t < kZLines * n; t += nt) {
-        const int l = t % kZLines, k = t / kZLines + 1, j = j0 + l;
-        if (j >= 2 && j <= d.n2m) Fv(d.q2, j, k) = Fv(d.q2, j, k) + sm[l * ld + k - 1];
+    const int w = tid >> 5, lane = tid & 31, r = r0 + w;
+    const int m = ((n + 31) >> 5) | 1;  // odd chunk: conflict-free 64-bit shared loads
+    const int i0 = min(lane * m, n), cnt = min(m, n - i0);
+    if (r <= last) {
+        double v[M];
+        double *line = sm + w * ld;
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) v[t] = line[i0 + t];
+        if (kKind == 2) {
+            warp_line(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(r) * d.ldh, d.amphj, d.apphj, n});
+        } else {
+            warp_line(v, i0, cnt, CoefShared{s.a, s.e, s.g});
+        }
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) line[i0 + t] = v[t];
     }
-    if (j0 == 1) {
-        for (int k = tid; k <= d.n3; k += nt) {
+    __syncthreads();
+    for (int l = 0; l < kYLines; ++l) {
+        const int rr = r0 + l;
+        if (rr > last) break;
+        double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(rr) * d.ldh
+                                   : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, rr);
+        const double *src = sm + l * ld;
+#pragma unroll 4
+        for (int i = tid; i < n; i += nt) row[i] = src[i];
+    }
+}
+
+// ---------------------------------------------------------------- z lines
+
+// kind 0 = solq2k (+ helsolve wall columns), 1 = solq3k.  Lines j0..j0+3.
+template <int M, int kKind>
+__global__ void __launch_bounds__(256) k_zlines(Dev d, ScanSys s, const double *bz, double ugkks, double ugkkn) {
+    __shared__ double shA[16 * kZLines], shC[16 * kZLines];
+    const int n = (kKind == 0) ? d.n3m : d.n3;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
+    const int l = lane & (kZLines - 1);
+    const int c = w * (32 / kZLines) + lane / kZLines;  // chunk index within the line
+    const int nc = W * (32 / kZLines);
+    const int m = (n + nc - 1) / nc;
+    const int i0 = min(c * m, n), cnt = min(m, n - i0);
+    const int j0 = blockIdx.x * kZLines + 1, j = j0 + l;
+    const bool live = (j <= d.n2m) && (kKind == 1 || j >= 2);
+    double v[M];
+    // gather this thread's chunk: row k = i + 1 of column j
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+        if (t < cnt) {
+            const int k = i0 + t + 1;
+            double x = 0.0;
+            if (live) {
+                if (kKind == 0) {
+                    x = __ldcg(&Fv(d.rhs2, j, k)) * __ldg(bz + k);
+                    if (k == 1) x = x + d.dqb2s[j] * ugkks;
+                    if (k == n) x = x + d.dqb2n[j] * ugkkn;
+                } else {
+                    if (k == 1) x = d.dqb3s[j];
+                    else if (k == n) x = d.dqb3n[j];
+                    else x = __ldcg(&Fv(d.rhs3, j, k)) * __ldg(bz + k);
+                }
+            }
+            v[t] = x;
+        }
+    }
+    block_lines(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shA, shC);
+    if (live) {
+        double *q = (kKind == 0) ? d.q2 : d.q3;
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            if (t < cnt) {
+                const int k = i0 + t + 1;
+                const size_t ix = fidx(d, j, k);
+                if (kKind == 1 && k == n) q[ix] = q[ix] + d.dqb3n[j];
+                else q[ix] = q[ix] + v[t];
+            }
+        }
+    }
+    if (kKind == 0 && j0 == 1) {
+        for (int k = threadIdx.x; k <= d.n3; k += blockDim.x) {
             Fv(d.q2, 1, k) = 0.0;
             Fv(d.q2, d.n2, k) = 0.0;
         }
     }
 }
 
-// solq3k (solve_fluid.F90:262-307): lines j of n3 unknowns with Dirichlet
-// end rows; q3 += x, the outflow row advanced by dqb3n.
-__global__ void __launch_bounds__(kZLines * 32) k_scan_z3(Dev d, ScanSys s, const double *bz) {
-    extern __shared__ double sm[];
-    const int n = d.n3, ld = odd_ld(n);
-    const int j0 = blockIdx.x * kZLines + 1;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int t = tid; t < kZLines * n; t += nt) {
-        const int l = t % kZLines, k = t / kZLines + 1, j = j0 + l;
-        double v = 0.0;
-        if (j <= d.n2m) {
-            if (k == 1) v = d.dqb3s[j];
-            else if (k == n) v = d.dqb3n[j];
-            else v = Fv(d.rhs3, j, k) * bz[k];
-        }
-        sm[l * ld + k - 1] = v;
-    }
-    __syncthreads();
-    const int w = tid >> 5;
-    if (j0 + w <= d.n2m) warp_solve(sm + w * ld, n, CoefShared{s.a, s.e, s.g});
-    __syncthreads();
-    for (int t = tid; t < kZLines * n; t += nt) {
-        const int l = t % kZLines, k = t / kZLines + 1, j = j0 + l;
-        if (j > d.n2m) continue;
-        if (k < n) Fv(d.q3, j, k) = Fv(d.q3, j, k) + sm[l * ld + k - 1];
-        else Fv(d.q3, j, k) = Fv(d.q3, j, k) + d.dqb3n[j];
-    }
+// ---------------------------------------------------------------- dispatch
+
+namespace {
+
+template <int kKind>
+void ylaunch(const Dev &d, const ScanSys &s, const double *by, int n, int lines, cudaStream_t st) {
+    const int m = ((n + 31) / 32) | 1;
+    const int blocks = (lines + kYLines - 1) / kYLines;
+    const size_t smem = static_cast<size_t>(kYLines) * (n + 1) * sizeof(double);
+    if (m <= 17) k_ylines<17, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
+    else if (m <= 33) k_ylines<33, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
+    else k_ylines<65, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
 }
 
-// phcalc_outflow.F90:34-56: one y system per z mode, in place in hmn
-__global__ void __launch_bounds__(kYLines * 32) k_scan_poisson(Dev d) {
-    extern __shared__ double sm[];
-    const int n = d.n2m, ld = odd_ld(n);
-    const int m0 = blockIdx.x * kYLines;
-    for (int l = 0; l < kYLines; ++l) {
-        const int m = m0 + l;
-        if (m >= d.n3m) break;
-        const double *row = d.hmn + static_cast<size_t>(m) * d.ldh;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) sm[l * ld + j] = row[j];
-    }
-    __syncthreads();
-    const int w = threadIdx.x >> 5, m = m0 + w;
-    if (m < d.n3m) warp_solve(sm + w * ld, n, CoefMode{d.pg + static_cast<size_t>(m) * d.ldh, d.amphj, d.apphj, n});
-    __syncthreads();
-    for (int l = 0; l < kYLines; ++l) {
-        const int mm = m0 + l;
-        if (mm >= d.n3m) break;
-        double *row = d.hmn + static_cast<size_t>(mm) * d.ldh;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) row[j] = sm[l * ld + j];
-    }
+template <int kKind>
+void zlaunch(const Dev &d, const ScanSys &s, const double *bz, double ugkks, double ugkkn, int n,
+             cudaStream_t st) {
+    const int blocks = (d.n2m + kZLines - 1) / kZLines;
+    const int threads = 256;  // 8 warps -> 64 chunks per line
+    const int m = (n + threads / kZLines - 1) / (threads / kZLines);
+    if (m <= 16) k_zlines<16, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
+    else if (m <= 32) k_zlines<32, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
+    else k_zlines<64, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
 }
 
-size_t scan_smem_y(int n) { return static_cast<size_t>(kYLines) * static_cast<size_t>(n | 1) * sizeof(double); }
-size_t scan_smem_z(int n) { return static_cast<size_t>(kZLines) * static_cast<size_t>(n | 1) * sizeof(double); }
+template <class K>
+cudaError_t allow_smem(K kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+}  // namespace
 
 cudaError_t scan_configure() {
-    const int big = 200 * 1024;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_scan_y2, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_scan_y3, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_scan_z2, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_scan_z3, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_scan_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+#define AL(K)                                  \
+    if ((e = allow_smem(K)) != cudaSuccess) return e;
+    AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>)) AL((k_ylines<65, 0>))
+    AL((k_ylines<17, 1>)) AL((k_ylines<33, 1>)) AL((k_ylines<65, 1>))
+    AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>)) AL((k_ylines<65, 2>))
+#undef AL
     return cudaSuccess;
 }
 
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
-    k_scan_y2<<<(d.n3m + kYLines - 1) / kYLines, kYLines * 32, scan_smem_y(d.n2), st>>>(d, s.sy2, s.by2);
-    k_scan_z2<<<(d.n2m + kZLines - 1) / kZLines, kZLines * 32, scan_smem_z(d.n3m), st>>>(d, s.sz2, s.bz2, s.ugkks,
-                                                                                       s.ugkkn);
-    k_scan_y3<<<(d.n3m - 1 + kYLines - 1) / kYLines, kYLines * 32, scan_smem_y(d.n2m), st>>>(d, s.sy3, s.by3);
-    k_scan_z3<<<(d.n2m + kZLines - 1) / kZLines, kZLines * 32, scan_smem_z(d.n3), st>>>(d, s.sz3, s.bz3);
+    ylaunch<0>(d, s.sy2, s.by2, d.n2, d.n3m, st);
+    zlaunch<0>(d, s.sz2, s.bz2, s.ugkks, s.ugkkn, d.n3m, st);
+    ylaunch<1>(d, s.sy3, s.by3, d.n2m, d.n3m - 1, st);
+    zlaunch<1>(d, s.sz3, s.bz3, 0.0, 0.0, d.n3, st);
 }
 
 void launch_scan_poisson(const Dev &d, cudaStream_t st) {
-    k_scan_poisson<<<(d.n3m + kYLines - 1) / kYLines, kYLines * 32, scan_smem_y(d.n2m), st>>>(d);
+    ylaunch<2>(d, ScanSys{nullptr, nullptr, nullptr}, nullptr, d.n2m, d.n3m, st);
 }
 
 }  // namespace fb
