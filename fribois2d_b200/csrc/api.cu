@@ -279,6 +279,10 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         std::fprintf(stderr, "fribois2d: variable time step (idtv = .false.) is not supported on the device path\n");
         return FB_ERR_UNSUPPORTED;
     }
+    if (g.n3 > 4096 || g.n2 > 2080) {
+        std::fprintf(stderr, "fribois2d: grid larger than the line solvers support (n3 <= 4096, n2 <= 2080)\n");
+        return FB_ERR_UNSUPPORTED;
+    }
     c->device = device;
     CK(cudaSetDevice(device));
     CK(fb::scan_configure());

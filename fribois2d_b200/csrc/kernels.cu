@@ -6,6 +6,7 @@
 // cites the reference routine it implements.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -21,6 +22,39 @@ namespace fb {
 
 __device__ __forceinline__ void raise_status(const Dev &d, int code) {
     atomicCAS(d.status, 0, code);
+}
+
+// indic.F90:276-303 as arithmetic (no dependent index loads)
+__device__ __forceinline__ int jmv_(int jc) { return jc == 1 ? 1 : jc - 1; }
+__device__ __forceinline__ int jpv_(const Dev &d, int jc) { return jc >= d.n2m ? jc : jc + 1; }
+__device__ __forceinline__ int kmv_(int kc) { return kc == 1 ? 1 : kc - 1; }
+__device__ __forceinline__ int kpv_(const Dev &d, int kc) { return kc == d.n3m ? kc : kc + 1; }
+
+template <bool kMax>
+__device__ __forceinline__ double warp_reduce(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, v, o);
+        v = kMax ? fmax(v, x) : v + x;
+    }
+    return v;
+}
+
+// block reduction with shuffles; sh holds 32 doubles; result in every thread
+template <bool kMax>
+__device__ double block_reduce_fast(double v, double *sh) {
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    v = warp_reduce<kMax>(v);
+    if ((t & 31) == 0) sh[t >> 5] = v;
+    __syncthreads();
+    double r = (t < nw) ? sh[t] : (kMax ? -INFINITY : 0.0);
+    if (t < 32) r = warp_reduce<kMax>(r);
+    if (t == 0) sh[0] = r;
+    __syncthreads();
+    r = sh[0];
+    __syncthreads();
+    return r;
 }
 
 // fixed-shape tree reduction over a block (blockDim.x * blockDim.y <= 1024)
@@ -76,23 +110,24 @@ __device__ bool grid_reduce(const Dev &d, double v, int slot, double *out, doubl
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
 // Both reductions (max for the CFL number, sum for the mean w) share one
 // last-block pass so that a single block finalises them.
-__global__ void k_cfl(Dev d) {
-    __shared__ double sh[1024];
+__global__ void __launch_bounds__(256) k_cfl(Dev d) {
+    __shared__ double sh[32];
     __shared__ bool last;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int t = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    const int b = blockIdx.x + blockIdx.y * gridDim.x, nb = gridDim.x * gridDim.y;
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int b = blockIdx.x, nb = gridDim.x;
+    const long cells = static_cast<long>(d.n2m) * d.n3m;
     double qcf = 1.0e-8, q3a = 0.0;
-    if (j <= d.n2m && k <= d.n3m) {
+    for (long idx = static_cast<long>(b) * nt + t; idx < cells; idx += static_cast<long>(nb) * nt) {
+        const int j = static_cast<int>(idx % d.n2m) + 1, k = static_cast<int>(idx / d.n2m) + 1;
         const int jp = j + 1, kp = k + 1;
         const double udx2 = d.udx2m[j], udx3 = d.udx3m[k];
-        qcf = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
-               fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
-        q3a = Fv(d.q3, j, k) * (d.zz[kp] - d.zz[k]) * (d.rc[jp] - d.rc[j]);
+        const double q = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
+                          fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
+        qcf = fmax(qcf, q);
+        q3a = q3a + Fv(d.q3, j, k) * (d.zz[kp] - d.zz[k]) * (d.rc[jp] - d.rc[j]);
     }
-    const double pm = block_reduce<true>(qcf, sh);
-    const double ps = block_reduce<false>(q3a, sh);
+    const double pm = block_reduce_fast<true>(qcf, sh);
+    const double ps = block_reduce_fast<false>(q3a, sh);
     double *rm = d.red, *rs = d.red + kRedSlot;
     if (t == 0) {
         rm[b] = pm;
@@ -108,8 +143,8 @@ __global__ void k_cfl(Dev d) {
         am = fmax(am, __ldcg(rm + i));
         as = as + __ldcg(rs + i);
     }
-    am = block_reduce<true>(am, sh);
-    as = block_reduce<false>(as, sh);
+    am = block_reduce_fast<true>(am, sh);
+    as = block_reduce_fast<false>(as, sh);
     if (t == 0) {
         d.count[0] = 0u;
         const double cflm = am * d.dt;
@@ -168,9 +203,9 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
                       (Fv(q2, jm, kc) + Fv(q2, jc, kc)) * (Fv(q2, jm, kc) + Fv(q2, jc, kc))) *
                      d.udx2c[jc] * 0.25;
         double dph = -h22;
-        const int jmv = d.jmv[jc];
+        const int jmv = jc - 1;  // jmv(jc) for jc >= 2
         if (kc >= 2 && kc <= n3m - 1) {
-            const int kmm = d.kmv[kc], kpp = d.kpv[kc], kp = kc + 1;
+            const int kmm = kc - 1, kpp = kc + 1, kp = kc + 1;  // kmv, kpv in the interior
             double h23 = ((Fv(q3, jc, kp) + Fv(q3, jmv, kp)) * (Fv(q2, jc, kpp) + Fv(q2, jc, kc)) -
                           (Fv(q3, jc, kc) + Fv(q3, jmv, kc)) * (Fv(q2, jc, kc) + Fv(q2, jc, kmm))) *
                          d.udx3m[kc] * 0.25;
@@ -193,7 +228,7 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
         const double d22q2 = Fv(q2, jp, kc) * appj + Fv(q2, jc, kc) * accj + Fv(q2, jm, kc) * ammj;
         double d33q2, dpx22;
         if (kc >= 2 && kc <= n3m - 1) {
-            const int km = d.kmv[kc], kp = d.kpv[kc];
+            const int km = kc - 1, kp = kc + 1;
             d33q2 = Fv(q2, jc, kp) * d.ap3sk[kc] + Fv(q2, jc, kc) * d.ac3sk[kc] + Fv(q2, jc, km) * d.am3sk[kc];
             const double udx2 = al * d.udx2c[jc];
             dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * udx2;
@@ -220,8 +255,8 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
     if (kc >= 2) {
         double qcap = 0.0;  // hdnl3 never writes kc = n3m (HDNL.F90:143)
         if (kc <= n3m - 1) {
-            const int kmm = kc - 1, km = d.kmv[kc], kp = kc + 1;
-            const int jmm = d.jmv[jc], jpp = d.jpv[jc], jp = jc + 1;
+            const int kmm = kc - 1, km = kc - 1, kp = kc + 1;
+            const int jmm = jmv_(jc), jpp = jpv_(d, jc), jp = jc + 1;
             double h32 = (((Fv(q2, jp, kc) + Fv(q2, jp, km)) * (Fv(q3, jpp, kc) + Fv(q3, jc, kc))) -
                           ((Fv(q2, jc, kc) + Fv(q2, jc, km)) * (Fv(q3, jc, kc) + Fv(q3, jmm, kc)))) *
                          d.udx2m[jc] * 0.25;
@@ -239,7 +274,7 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
         } else if (jc == n2m) {
             dq32 = d.q3uw * appj + Fv(q3, jc, kc) * accj + Fv(q3, jc - 1, kc) * ammj;
         } else {
-            dq32 = Fv(q3, d.jpv[jc], kc) * appj + Fv(q3, jc, kc) * accj + Fv(q3, d.jmv[jc], kc) * ammj;
+            dq32 = Fv(q3, jpv_(d, jc), kc) * appj + Fv(q3, jc, kc) * accj + Fv(q3, jmv_(jc), kc) * ammj;
         }
         const double dq33 = Fv(q3, jc, kp) * d.ap3ck[kc] + Fv(q3, jc, kc) * d.ac3ck[kc] + Fv(q3, jc, km) * d.am3ck[kc];
         const double dcq3 = dq32 + dq33;
@@ -647,14 +682,16 @@ __global__ void k_divg(Dev d, double usdtal) {
 
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
 // partial sums of pr_submean (updvp.F90:320-333)
-__global__ void k_updvp_prcalc(Dev d, double al, double be) {
-    __shared__ double sh[1024];
-    const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+__global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double be) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int t = threadIdx.x, nt = blockDim.x, b = blockIdx.x, nb = gridDim.x;
+    const long cells = static_cast<long>(d.n2m) * d.n3m;
+    const double *dph = d.dph;
     double part = 0.0;
-    if (jc <= d.n2m && kc <= d.n3m) {
-        const double *dph = d.dph;
-        const int jm = d.jmv[jc], jp = d.jpv[jc];
+    for (long idx = static_cast<long>(b) * nt + t; idx < cells; idx += static_cast<long>(nb) * nt) {
+        const int jc = static_cast<int>(idx % d.n2m) + 1, kc = static_cast<int>(idx / d.n2m) + 1;
+        const int jm = jmv_(jc), jp = jpv_(d, jc);
         const double usujm = al * d.dt * d.udx2c[jc];
         const double locdph = Fv(dph, jc, kc);
         Fv(d.q2, jc, kc) = Fv(d.q2, jc, kc) - (locdph - Fv(dph, jm, kc)) * usujm;
@@ -662,18 +699,31 @@ __global__ void k_updvp_prcalc(Dev d, double al, double be) {
             const double usukm = al * d.dt * d.udx3c[kc];
             Fv(d.q3, jc, kc) = Fv(d.q3, jc, kc) - (Fv(dph, jc, kc) - Fv(dph, jc, kc - 1)) * usukm;
         }
-        const int kp = d.kpv[kc], km = d.kmv[kc];
+        const int kp = kpv_(d, kc), km = kmv_(kc);
         const double p = Fv(d.pr, jc, kc) + Fv(dph, jc, kc) -
                          be * ((Fv(dph, jp, kc) * d.apphj[jc] + Fv(dph, jc, kc) * d.acphj[jc] +
                                 Fv(dph, jm, kc) * d.amphj[jc]) +
                                (Fv(dph, jc, kp) * d.apphk[kc] + Fv(dph, jc, kc) * d.acphk[kc] +
                                 Fv(dph, jc, km) * d.amphk[kc]));
         Fv(d.pr, jc, kc) = p;
-        part = p * (d.zz[kc + 1] - d.zz[kc]) * (d.rc[jc + 1] - d.rc[jc]);
+        part = part + p * (d.zz[kc + 1] - d.zz[kc]) * (d.rc[jc + 1] - d.rc[jc]);
     }
-    double tot;
-    if (grid_reduce<false>(d, part, 2, &tot, sh)) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) d.scal[S_PRAVG] = tot / (d.rext2 * d.alx3);
+    const double bsum = block_reduce_fast<false>(part, sh);
+    double *red = d.red + 2 * static_cast<size_t>(kRedSlot);
+    if (t == 0) {
+        red[b] = bsum;
+        __threadfence();
+        last = (atomicAdd(d.count + 2, 1u) == static_cast<unsigned>(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int i = t; i < nb; i += nt) acc = acc + __ldcg(red + i);
+    acc = block_reduce_fast<false>(acc, sh);
+    if (t == 0) {
+        d.count[2] = 0u;
+        d.scal[S_PRAVG] = acc / (d.rext2 * d.alx3);
     }
 }
 
@@ -1083,10 +1133,11 @@ namespace {
 inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
 }  // namespace
 
-void launch_cfl(const Dev &d, cudaStream_t s) {
-    dim3 b(32, 8);
-    k_cfl<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d);
+int stride_blocks(const Dev &d) {
+    const long cells = static_cast<long>(d.n2m) * d.n3m;
+    return static_cast<int>(std::min<long>((cells + 255) / 256, 148L * 8));
 }
+void launch_cfl(const Dev &d, cudaStream_t s) { k_cfl<<<stride_blocks(d), 256, 0, s>>>(d); }
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { k_boucdq<<<1, 1024, 0, s>>>(d, ga, ro); }
 void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s) {
     dim3 b(32, 8);
@@ -1116,8 +1167,7 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     k_divg<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, usdtal);
 }
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
-    dim3 b(32, 8);
-    k_updvp_prcalc<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, al, be);
+    k_updvp_prcalc<<<stride_blocks(d), 256, 0, s>>>(d, al, be);
 }
 void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
     dim3 b(32, 8);

@@ -33,74 +33,117 @@ constexpr unsigned kFull = 0xffffffffu;
 
 struct CoefShared {      // y or z systems: 1-D factors shared by all lines
     const double *a, *e, *g;
-    __device__ double A(int i) const { return __ldg(a + i); }
-    __device__ double E(int i) const { return __ldg(e + i); }
-    __device__ double G(int i) const { return __ldg(g + i); }
+    template <int M>
+    __device__ __forceinline__ void loadA(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) c[t] = __ldg(a + i0 + t);
+    }
+    template <int M>
+    __device__ __forceinline__ void loadE(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) c[t] = __ldg(e + i0 + t);
+    }
+    template <int M>
+    __device__ __forceinline__ void loadG(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) c[t] = __ldg(g + i0 + t);
+    }
 };
 
 struct CoefMode {        // Poisson mode: reciprocal pivots per mode, 1-based off-diagonals
     const double *g, *amphj, *apphj;
     int n;
-    __device__ double A(int i) const { return i == 0 ? 0.0 : -(__ldg(amphj + i + 1) * __ldg(g + i - 1)); }
-    __device__ double E(int i) const { return i == n - 1 ? 0.0 : -(__ldg(apphj + i + 1) * __ldg(g + i)); }
-    __device__ double G(int i) const { return __ldg(g + i); }
+    template <int M>
+    __device__ __forceinline__ void loadA(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) {
+                const int i = i0 + t;
+                c[t] = (i == 0) ? 0.0 : -(__ldg(amphj + i + 1) * __ldg(g + i - 1));
+            }
+    }
+    template <int M>
+    __device__ __forceinline__ void loadE(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) {
+                const int i = i0 + t;
+                c[t] = (i == n - 1) ? 0.0 : -(__ldg(apphj + i + 1) * __ldg(g + i));
+            }
+    }
+    template <int M>
+    __device__ __forceinline__ void loadG(double (&c)[M], int i0, int cnt) const {
+#pragma unroll
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) c[t] = __ldg(g + i0 + t);
+    }
 };
 
-// composite affine map of a chunk, forward order
-template <int M, class Co>
-__device__ __forceinline__ void fwd_compose(const double (&v)[M], int i0, int cnt, const Co &co, double &A,
+// The chains below only read registers: the coefficients of a chunk are
+// loaded into c[] before each recurrence starts.
+template <int M>
+__device__ __forceinline__ void fwd_compose(const double (&v)[M], const double (&c)[M], int cnt, double &A,
                                             double &C) {
     A = 1.0;
     C = 0.0;
 #pragma unroll
     for (int t = 0; t < M; ++t)
         if (t < cnt) {
-            const double a = co.A(i0 + t);
-            C = fma(a, C, v[t]);
-            A *= a;
+            C = fma(c[t], C, v[t]);
+            A *= c[t];
         }
 }
 
-template <int M, class Co>
-__device__ __forceinline__ void fwd_apply(double (&v)[M], int i0, int cnt, const Co &co, double y) {
+template <int M>
+__device__ __forceinline__ void fwd_apply(double (&v)[M], const double (&c)[M], int cnt, double y) {
 #pragma unroll
     for (int t = 0; t < M; ++t)
         if (t < cnt) {
-            y = fma(co.A(i0 + t), y, v[t]);
+            y = fma(c[t], y, v[t]);
             v[t] = y;
         }
 }
 
-template <int M, class Co>
-__device__ __forceinline__ void bwd_compose(const double (&v)[M], int i0, int cnt, const Co &co, double &A,
+template <int M>
+__device__ __forceinline__ void bwd_compose(const double (&v)[M], const double (&c)[M], int cnt, double &A,
                                             double &C) {
     A = 1.0;
     C = 0.0;
 #pragma unroll
     for (int t = M - 1; t >= 0; --t)
         if (t < cnt) {
-            const double e = co.E(i0 + t);
-            C = fma(e, C, co.G(i0 + t) * v[t]);
-            A *= e;
+            C = fma(c[t], C, v[t]);
+            A *= c[t];
         }
 }
 
-template <int M, class Co>
-__device__ __forceinline__ void bwd_apply(double (&v)[M], int i0, int cnt, const Co &co, double x) {
+template <int M>
+__device__ __forceinline__ void bwd_apply(double (&v)[M], const double (&c)[M], int cnt, double x) {
 #pragma unroll
     for (int t = M - 1; t >= 0; --t)
         if (t < cnt) {
-            x = fma(co.E(i0 + t), x, co.G(i0 + t) * v[t]);
+            x = fma(c[t], x, v[t]);
             v[t] = x;
         }
 }
 
-// one warp = one line of n unknowns, chunk of m = ceil(n/32) per lane
+template <int M>
+__device__ __forceinline__ void scale(double (&v)[M], const double (&c)[M], int cnt) {
+#pragma unroll
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) v[t] = c[t] * v[t];
+}
+
+// one warp = one line of n unknowns, one contiguous chunk per lane
 template <int M, class Co>
 __device__ __forceinline__ void warp_line(double (&v)[M], int i0, int cnt, const Co &co) {
     const int lane = threadIdx.x & 31;
-    double A, C;
-    fwd_compose(v, i0, cnt, co, A, C);
+    double c[M], A, C;
+    co.loadA(c, i0, cnt);
+    fwd_compose(v, c, cnt, A, C);
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
         const double Ao = __shfl_up_sync(kFull, A, dd), Co_ = __shfl_up_sync(kFull, C, dd);
@@ -111,8 +154,11 @@ __device__ __forceinline__ void warp_line(double (&v)[M], int i0, int cnt, const
     }
     double y = __shfl_up_sync(kFull, C, 1);
     if (lane == 0) y = 0.0;
-    fwd_apply(v, i0, cnt, co, y);
-    bwd_compose(v, i0, cnt, co, A, C);
+    fwd_apply(v, c, cnt, y);
+    co.loadG(c, i0, cnt);
+    scale(v, c, cnt);  // g(i) y(i)
+    co.loadE(c, i0, cnt);
+    bwd_compose(v, c, cnt, A, C);
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
         const double Ao = __shfl_down_sync(kFull, A, dd), Co_ = __shfl_down_sync(kFull, C, dd);
@@ -123,7 +169,7 @@ __device__ __forceinline__ void warp_line(double (&v)[M], int i0, int cnt, const
     }
     double x = __shfl_down_sync(kFull, C, 1);
     if (lane == 31) x = 0.0;
-    bwd_apply(v, i0, cnt, co, x);
+    bwd_apply(v, c, cnt, x);
 }
 
 // kZLines lines interleaved over the lanes (line = lane % 4), chunks over
@@ -134,9 +180,10 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
     const int l = lane & (kZLines - 1), sub = lane / kZLines;
     constexpr int kSub = 32 / kZLines;
-    double A, C, Ao, Co_;
+    double c[M], A, C, Ao, Co_;
     // ---- forward
-    fwd_compose(v, i0, cnt, co, A, C);
+    co.loadA(c, i0, cnt);
+    fwd_compose(v, c, cnt, A, C);
 #pragma unroll
     for (int dd = kZLines; dd < 32; dd <<= 1) {
         Ao = __shfl_up_sync(kFull, A, dd);
@@ -158,10 +205,13 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
     __syncthreads();
     double PC = 0.0;
     for (int q = 0; q < w; ++q) PC = fma(shA[q * kZLines + l], PC, shC[q * kZLines + l]);
-    fwd_apply(v, i0, cnt, co, fma(Aex, PC, Cex));
+    fwd_apply(v, c, cnt, fma(Aex, PC, Cex));
+    co.loadG(c, i0, cnt);
+    scale(v, c, cnt);
+    co.loadE(c, i0, cnt);
     __syncthreads();
     // ---- backward
-    bwd_compose(v, i0, cnt, co, A, C);
+    bwd_compose(v, c, cnt, A, C);
 #pragma unroll
     for (int dd = kZLines; dd < 32; dd <<= 1) {
         Ao = __shfl_down_sync(kFull, A, dd);
@@ -184,7 +234,7 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
     __syncthreads();
     double SC = 0.0;
     for (int q = W - 1; q > w; --q) SC = fma(shA[q * kZLines + l], SC, shC[q * kZLines + l]);
-    bwd_apply(v, i0, cnt, co, fma(Aex, SC, Cex));
+    bwd_apply(v, c, cnt, fma(Aex, SC, Cex));
 }
 
 }  // namespace
@@ -201,60 +251,49 @@ __global__ void __launch_bounds__(kYLines * 32) k_ylines(Dev d, ScanSys s, const
     if (kKind == 0) n = d.n2, first = 1, last = d.n3m;
     else if (kKind == 1) n = d.n2m, first = 2, last = d.n3m;
     else n = d.n2m, first = 0, last = d.n3m - 1;
-    const int ld = n + 1;
-    const int r0 = first + blockIdx.x * kYLines;
-    const int nt = blockDim.x, tid = threadIdx.x;
-    // coalesced staging of the block's rows
-    for (int l = 0; l < kYLines; ++l) {
-        const int r = r0 + l;
-        if (r > last) break;
-        const double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh
-                                         : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
-        double *dst = sm + l * ld;
-#pragma unroll 4
-        for (int i = tid; i < n; i += nt) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = first + blockIdx.x * kYLines + w;
+    if (r > last) return;  // whole warp leaves; no block-level barriers below
+    double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh
+                               : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
+    double *line = sm + w * (n + 1);
+    // coalesced staging: lane-strided loads (independent, so they overlap)
+#pragma unroll
+    for (int it = 0; it < M; ++it) {
+        const int i = lane + 32 * it;
+        if (i < n) {
             double v = __ldcg(row + i);
             if (kKind == 0) v = (i >= 1 && i <= n - 2) ? v * __ldg(by + i + 1) : 0.0;
             else if (kKind == 1) v = v * __ldg(by + i + 1);
-            dst[i] = v;
+            line[i] = v;
         }
     }
-    __syncthreads();
-    const int w = tid >> 5, lane = tid & 31, r = r0 + w;
+    __syncwarp();
     const int m = ((n + 31) >> 5) | 1;  // odd chunk: conflict-free 64-bit shared loads
     const int i0 = min(lane * m, n), cnt = min(m, n - i0);
-    if (r <= last) {
-        double v[M];
-        double *line = sm + w * ld;
+    double v[M];
 #pragma unroll
-        for (int t = 0; t < M; ++t)
-            if (t < cnt) v[t] = line[i0 + t];
-        if (kKind == 2) {
-            warp_line(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(r) * d.ldh, d.amphj, d.apphj, n});
-        } else {
-            warp_line(v, i0, cnt, CoefShared{s.a, s.e, s.g});
-        }
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) v[t] = line[i0 + t];
+    if (kKind == 2) warp_line(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(r) * d.ldh, d.amphj, d.apphj, n});
+    else warp_line(v, i0, cnt, CoefShared{s.a, s.e, s.g});
 #pragma unroll
-        for (int t = 0; t < M; ++t)
-            if (t < cnt) line[i0 + t] = v[t];
-    }
-    __syncthreads();
-    for (int l = 0; l < kYLines; ++l) {
-        const int rr = r0 + l;
-        if (rr > last) break;
-        double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(rr) * d.ldh
-                                   : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, rr);
-        const double *src = sm + l * ld;
-#pragma unroll 4
-        for (int i = tid; i < n; i += nt) row[i] = src[i];
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) line[i0 + t] = v[t];
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < M; ++it) {
+        const int i = lane + 32 * it;
+        if (i < n) row[i] = line[i];
     }
 }
 
 // ---------------------------------------------------------------- z lines
 
 // kind 0 = solq2k (+ helsolve wall columns), 1 = solq3k.  Lines j0..j0+3.
-template <int M, int kKind>
-__global__ void __launch_bounds__(256) k_zlines(Dev d, ScanSys s, const double *bz, double ugkks, double ugkkn) {
+template <int M, int kKind, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, ScanSys s, const double *bz, double ugkks,
+                                                        double ugkkn) {
     __shared__ double shA[16 * kZLines], shC[16 * kZLines];
     const int n = (kKind == 0) ? d.n3m : d.n3;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
@@ -265,39 +304,53 @@ __global__ void __launch_bounds__(256) k_zlines(Dev d, ScanSys s, const double *
     const int i0 = min(c * m, n), cnt = min(m, n - i0);
     const int j0 = blockIdx.x * kZLines + 1, j = j0 + l;
     const bool live = (j <= d.n2m) && (kKind == 1 || j >= 2);
+    const int jj = live ? j : 2;  // a valid column for the (discarded) loads of idle lanes
+    const double *src = (kKind == 0) ? d.rhs2 : d.rhs3;
     double v[M];
-    // gather this thread's chunk: row k = i + 1 of column j
+    // gather this thread's chunk (row k = i + 1 of column j): loads first
 #pragma unroll
-    for (int t = 0; t < M; ++t) {
+    for (int t = 0; t < M; ++t)
+        if (t < cnt) v[t] = __ldcg(src + fidx(d, jj, i0 + t + 1));
+    double *qf = (kKind == 0) ? d.q2 : d.q3;
+    double bs = 0.0, bn = 0.0;
+    if (kKind == 0) {
+        bs = d.dqb2s[jj] * ugkks;
+        bn = d.dqb2n[jj] * ugkkn;
+    } else {
+        bs = d.dqb3s[jj];
+        bn = d.dqb3n[jj];
+    }
+#pragma unroll
+    for (int t = 0; t < M; ++t)
         if (t < cnt) {
             const int k = i0 + t + 1;
             double x = 0.0;
             if (live) {
                 if (kKind == 0) {
-                    x = __ldcg(&Fv(d.rhs2, j, k)) * __ldg(bz + k);
-                    if (k == 1) x = x + d.dqb2s[j] * ugkks;
-                    if (k == n) x = x + d.dqb2n[j] * ugkkn;
+                    x = v[t] * __ldg(bz + k);
+                    if (k == 1) x = x + bs;
+                    if (k == n) x = x + bn;
                 } else {
-                    if (k == 1) x = d.dqb3s[j];
-                    else if (k == n) x = d.dqb3n[j];
-                    else x = __ldcg(&Fv(d.rhs3, j, k)) * __ldg(bz + k);
+                    if (k == 1) x = bs;
+                    else if (k == n) x = bn;
+                    else x = v[t] * __ldg(bz + k);
                 }
             }
             v[t] = x;
         }
-    }
     block_lines(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shA, shC);
     if (live) {
-        double *q = (kKind == 0) ? d.q2 : d.q3;
+        double q[M];
 #pragma unroll
-        for (int t = 0; t < M; ++t) {
+        for (int t = 0; t < M; ++t)
+            if (t < cnt) q[t] = __ldcg(qf + fidx(d, j, i0 + t + 1));
+#pragma unroll
+        for (int t = 0; t < M; ++t)
             if (t < cnt) {
                 const int k = i0 + t + 1;
-                const size_t ix = fidx(d, j, k);
-                if (kKind == 1 && k == n) q[ix] = q[ix] + d.dqb3n[j];
-                else q[ix] = q[ix] + v[t];
+                const double add = (kKind == 1 && k == n) ? bn : v[t];
+                qf[fidx(d, j, k)] = q[t] + add;
             }
-        }
     }
     if (kKind == 0 && j0 == 1) {
         for (int k = threadIdx.x; k <= d.n3; k += blockDim.x) {
@@ -313,6 +366,7 @@ namespace {
 
 template <int kKind>
 void ylaunch(const Dev &d, const ScanSys &s, const double *by, int n, int lines, cudaStream_t st) {
+    // M bounds both the lane chunk, ceil(n/32)|1, and the staging loads per lane
     const int m = ((n + 31) / 32) | 1;
     const int blocks = (lines + kYLines - 1) / kYLines;
     const size_t smem = static_cast<size_t>(kYLines) * (n + 1) * sizeof(double);
@@ -325,11 +379,20 @@ template <int kKind>
 void zlaunch(const Dev &d, const ScanSys &s, const double *bz, double ugkks, double ugkkn, int n,
              cudaStream_t st) {
     const int blocks = (d.n2m + kZLines - 1) / kZLines;
-    const int threads = 256;  // 8 warps -> 64 chunks per line
-    const int m = (n + threads / kZLines - 1) / (threads / kZLines);
-    if (m <= 16) k_zlines<16, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
-    else if (m <= 32) k_zlines<32, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
-    else k_zlines<64, kKind><<<blocks, threads, 0, st>>>(d, s, bz, ugkks, ugkkn);
+    constexpr int kChunksPerWarp = 32 / kZLines;
+    // as many warps as keep every chunk within 16 (then 32, 64) elements
+    int warps = (n + kChunksPerWarp * 16 - 1) / (kChunksPerWarp * 16);
+    if (warps <= 16) {
+        k_zlines<16, kKind, 512><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
+        return;
+    }
+    warps = (n + kChunksPerWarp * 32 - 1) / (kChunksPerWarp * 32);
+    if (warps <= 10) {
+        k_zlines<32, kKind, 320><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
+        return;
+    }
+    warps = (n + kChunksPerWarp * 64 - 1) / (kChunksPerWarp * 64);
+    k_zlines<64, kKind, 256><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
 }
 
 template <class K>

@@ -7,7 +7,7 @@
 
 namespace fb {
 
-constexpr int kYLines = 8;  // contiguous lines per block (one warp each)
+constexpr int kYLines = 4;  // contiguous lines per block (one warp each)
 constexpr int kZLines = 4;  // strided lines per block (one warp each)
 
 cudaError_t scan_configure();
