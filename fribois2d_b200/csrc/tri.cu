@@ -172,6 +172,64 @@ __device__ __forceinline__ void warp_line(double (&v)[M], int i0, int cnt, const
     bwd_apply(v, c, cnt, x);
 }
 
+// G consecutive warps share one line (lane chunks in warp-major order);
+// warps exchange their chunk composites through sh (2 * G doubles per line).
+template <int M, int G, class Co>
+__device__ __forceinline__ void group_line(double (&v)[M], int i0, int cnt, const Co &co, double *sh) {
+    const int lane = threadIdx.x & 31, gw = (threadIdx.x >> 5) % G;
+    double c[M], A, C;
+    co.loadA(c, i0, cnt);
+    fwd_compose(v, c, cnt, A, C);
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+        const double Ao = __shfl_up_sync(kFull, A, dd), Co_ = __shfl_up_sync(kFull, C, dd);
+        if (lane >= dd) {
+            C = fma(A, Co_, C);
+            A *= Ao;
+        }
+    }
+    if (lane == 31) {
+        sh[2 * gw] = A;
+        sh[2 * gw + 1] = C;
+    }
+    double Cex = __shfl_up_sync(kFull, C, 1), Aex = __shfl_up_sync(kFull, A, 1);
+    if (lane == 0) {
+        Aex = 1.0;
+        Cex = 0.0;
+    }
+    __syncthreads();
+    double PC = 0.0;
+    for (int q = 0; q < gw; ++q) PC = fma(sh[2 * q], PC, sh[2 * q + 1]);
+    fwd_apply(v, c, cnt, fma(Aex, PC, Cex));
+    co.loadG(c, i0, cnt);
+    scale(v, c, cnt);
+    co.loadE(c, i0, cnt);
+    __syncthreads();
+    bwd_compose(v, c, cnt, A, C);
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+        const double Ao = __shfl_down_sync(kFull, A, dd), Co_ = __shfl_down_sync(kFull, C, dd);
+        if (lane + dd < 32) {
+            C = fma(A, Co_, C);
+            A *= Ao;
+        }
+    }
+    if (lane == 0) {
+        sh[2 * gw] = A;
+        sh[2 * gw + 1] = C;
+    }
+    Cex = __shfl_down_sync(kFull, C, 1);
+    Aex = __shfl_down_sync(kFull, A, 1);
+    if (lane == 31) {
+        Aex = 1.0;
+        Cex = 0.0;
+    }
+    __syncthreads();
+    double SC = 0.0;
+    for (int q = G - 1; q > gw; --q) SC = fma(sh[2 * q], SC, sh[2 * q + 1]);
+    bwd_apply(v, c, cnt, fma(Aex, SC, Cex));
+}
+
 // kZLines lines interleaved over the lanes (line = lane % 4), chunks over
 // lane/4 and the block's warps; shA/shC hold one composite per (warp, line)
 template <int M, class Co>
@@ -244,57 +302,93 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
 // Rows of a k-major field staged through shared memory: load row (scaled),
 // solve with a warp per line, write back.  kind: 0 = solq2j, 1 = solq3j,
 // 2 = Poisson mode (rows of hmn).
+// kKind 0: the v and w systems of helsolve in one launch (solq2j on rows
+// k = 1..n3m of rhs2, then solq3j on rows k = 2..n3m of rhs3; they are
+// independent).  kKind 2: Poisson modes (rows of hmn).
 template <int M, int kKind>
-__global__ void __launch_bounds__(kYLines * 32) k_ylines(Dev d, ScanSys s, const double *by) {
+__global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSys s2, const double *by2,
+                                                                   ScanSys s3, const double *by3) {
     extern __shared__ double sm[];
-    int n, first, last;
-    if (kKind == 0) n = d.n2, first = 1, last = d.n3m;
-    else if (kKind == 1) n = d.n2m, first = 2, last = d.n3m;
-    else n = d.n2m, first = 0, last = d.n3m - 1;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = first + blockIdx.x * kYLines + w;
-    if (r > last) return;  // whole warp leaves; no block-level barriers below
-    double *row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh
-                               : (kKind == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
-    double *line = sm + w * (n + 1);
-    // coalesced staging: lane-strided loads (independent, so they overlap)
+    __shared__ double shx[kYLines][2 * kYWarps];
+    const int wl = (threadIdx.x >> 5) / kYWarps;       // line slot in the block
+    const int tl = threadIdx.x % (32 * kYWarps);       // thread within the line group
+    int line = blockIdx.x * kYLines + wl;
+    int sys = 0, n, r;
+    if (kKind == 2) {
+        n = d.n2m;
+        r = line;
+        if (r >= d.n3m) r = -1;
+    } else if (line < d.n3m) {
+        sys = 0;
+        n = d.n2;
+        r = line + 1;
+    } else {
+        sys = 1;
+        n = d.n2m;
+        r = line - d.n3m + 2;
+        if (r > d.n3m) r = -1;
+    }
+    const bool live = (r >= 0);
+    if (!live) n = d.n2m;  // idle line slot: still takes part in the block barriers
+    double *row = nullptr;
+    if (live) row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh : (sys == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
+    const double *by = (sys == 0) ? by2 : by3;
+    double *buf = sm + wl * (d.n2 + 1);
+    constexpr int kT = 32 * kYWarps;
+    // coalesced staging: thread-strided loads, all independent
+    if (live) {
 #pragma unroll
-    for (int it = 0; it < M; ++it) {
-        const int i = lane + 32 * it;
-        if (i < n) {
-            double v = __ldcg(row + i);
-            if (kKind == 0) v = (i >= 1 && i <= n - 2) ? v * __ldg(by + i + 1) : 0.0;
-            else if (kKind == 1) v = v * __ldg(by + i + 1);
-            line[i] = v;
+        for (int it = 0; it < M; ++it) {
+            const int i = tl + kT * it;
+            if (i < n) {
+                double v = __ldcg(row + i);
+                if (kKind != 2) {
+                    if (sys == 0) v = (i >= 1 && i <= n - 2) ? v * __ldg(by + i + 1) : 0.0;
+                    else v = v * __ldg(by + i + 1);
+                }
+                buf[i] = v;
+            }
         }
     }
-    __syncwarp();
-    const int m = ((n + 31) >> 5) | 1;  // odd chunk: conflict-free 64-bit shared loads
-    const int i0 = min(lane * m, n), cnt = min(m, n - i0);
+    __syncthreads();
+    const int m = ((n + kT - 1) / kT) | 1;  // odd chunk: conflict-free 64-bit shared loads
+    const int i0 = min(tl * m, n), cnt = live ? min(m, n - i0) : 0;
     double v[M];
 #pragma unroll
     for (int t = 0; t < M; ++t)
-        if (t < cnt) v[t] = line[i0 + t];
-    if (kKind == 2) warp_line(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(r) * d.ldh, d.amphj, d.apphj, n});
-    else warp_line(v, i0, cnt, CoefShared{s.a, s.e, s.g});
+        if (t < cnt) v[t] = buf[i0 + t];
+    if (kKind == 2) {
+        group_line<M, kYWarps>(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(live ? r : 0) * d.ldh, d.amphj, d.apphj, n},
+                               shx[wl]);
+    } else {
+        const ScanSys &s = (sys == 0) ? s2 : s3;
+        group_line<M, kYWarps>(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shx[wl]);
+    }
 #pragma unroll
     for (int t = 0; t < M; ++t)
-        if (t < cnt) line[i0 + t] = v[t];
-    __syncwarp();
+        if (t < cnt) buf[i0 + t] = v[t];
+    __syncthreads();
+    if (live) {
 #pragma unroll
-    for (int it = 0; it < M; ++it) {
-        const int i = lane + 32 * it;
-        if (i < n) row[i] = line[i];
+        for (int it = 0; it < M; ++it) {
+            const int i = tl + kT * it;
+            if (i < n) row[i] = buf[i];
+        }
     }
 }
 
 // ---------------------------------------------------------------- z lines
 
-// kind 0 = solq2k (+ helsolve wall columns), 1 = solq3k.  Lines j0..j0+3.
-template <int M, int kKind, int kMaxThreads>
-__global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, ScanSys s, const double *bz, double ugkks,
-                                                        double ugkkn) {
+// solq2k (+ helsolve wall columns) on blocks [0, nb2) and solq3k on the
+// rest, one launch (the two are independent).  Lines j0..j0+3.
+template <int M, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb2) {
     __shared__ double shA[16 * kZLines], shC[16 * kZLines];
+    const int kKind = (static_cast<int>(blockIdx.x) < nb2) ? 0 : 1;
+    const int blk = (kKind == 0) ? blockIdx.x : blockIdx.x - nb2;
+    const ScanSys &s = (kKind == 0) ? sd.sz2 : sd.sz3;
+    const double *bz = (kKind == 0) ? sd.bz2 : sd.bz3;
+    const double ugkks = sd.ugkks, ugkkn = sd.ugkkn;
     const int n = (kKind == 0) ? d.n3m : d.n3;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
     const int l = lane & (kZLines - 1);
@@ -302,7 +396,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, ScanSys s, const 
     const int nc = W * (32 / kZLines);
     const int m = (n + nc - 1) / nc;
     const int i0 = min(c * m, n), cnt = min(m, n - i0);
-    const int j0 = blockIdx.x * kZLines + 1, j = j0 + l;
+    const int j0 = blk * kZLines + 1, j = j0 + l;
     const bool live = (j <= d.n2m) && (kKind == 1 || j >= 2);
     const int jj = live ? j : 2;  // a valid column for the (discarded) loads of idle lanes
     const double *src = (kKind == 0) ? d.rhs2 : d.rhs3;
@@ -365,34 +459,37 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, ScanSys s, const 
 namespace {
 
 template <int kKind>
-void ylaunch(const Dev &d, const ScanSys &s, const double *by, int n, int lines, cudaStream_t st) {
-    // M bounds both the lane chunk, ceil(n/32)|1, and the staging loads per lane
-    const int m = ((n + 31) / 32) | 1;
+void ylaunch(const Dev &d, const SubDev *sd, cudaStream_t st) {
+    const int lines = (kKind == 2) ? d.n3m : d.n3m + (d.n3m - 1);
     const int blocks = (lines + kYLines - 1) / kYLines;
-    const size_t smem = static_cast<size_t>(kYLines) * (n + 1) * sizeof(double);
-    if (m <= 17) k_ylines<17, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
-    else if (m <= 33) k_ylines<33, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
-    else k_ylines<65, kKind><<<blocks, kYLines * 32, smem, st>>>(d, s, by);
+    const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
+    const size_t smem = static_cast<size_t>(kYLines) * (d.n2 + 1) * sizeof(double);
+    const ScanSys z{nullptr, nullptr, nullptr};
+    const ScanSys s2 = sd ? sd->sy2 : z, s3 = sd ? sd->sy3 : z;
+    const double *b2 = sd ? sd->by2 : nullptr, *b3 = sd ? sd->by3 : nullptr;
+    const int threads = kYLines * kYWarps * 32;
+    if (m <= 9) k_ylines<9, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
+    else if (m <= 17) k_ylines<17, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
+    else k_ylines<33, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
 }
 
-template <int kKind>
-void zlaunch(const Dev &d, const ScanSys &s, const double *bz, double ugkks, double ugkkn, int n,
-             cudaStream_t st) {
-    const int blocks = (d.n2m + kZLines - 1) / kZLines;
+void zlaunch(const Dev &d, const SubDev &sd, cudaStream_t st) {
+    const int nb2 = (d.n2m + kZLines - 1) / kZLines;
+    const int blocks = 2 * nb2;
+    const int n = d.n3;  // the longer of the two systems sets the chunking
     constexpr int kChunksPerWarp = 32 / kZLines;
-    // as many warps as keep every chunk within 16 (then 32, 64) elements
     int warps = (n + kChunksPerWarp * 16 - 1) / (kChunksPerWarp * 16);
     if (warps <= 16) {
-        k_zlines<16, kKind, 512><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
+        k_zlines<16, 512><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
         return;
     }
     warps = (n + kChunksPerWarp * 32 - 1) / (kChunksPerWarp * 32);
     if (warps <= 10) {
-        k_zlines<32, kKind, 320><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
+        k_zlines<32, 320><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
         return;
     }
     warps = (n + kChunksPerWarp * 64 - 1) / (kChunksPerWarp * 64);
-    k_zlines<64, kKind, 256><<<blocks, warps * 32, 0, st>>>(d, s, bz, ugkks, ugkkn);
+    k_zlines<64, 256><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
 }
 
 template <class K>
@@ -406,22 +503,17 @@ cudaError_t scan_configure() {
     cudaError_t e;
 #define AL(K)                                  \
     if ((e = allow_smem(K)) != cudaSuccess) return e;
-    AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>)) AL((k_ylines<65, 0>))
-    AL((k_ylines<17, 1>)) AL((k_ylines<33, 1>)) AL((k_ylines<65, 1>))
-    AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>)) AL((k_ylines<65, 2>))
+    AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
+    AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
 #undef AL
     return cudaSuccess;
 }
 
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
-    ylaunch<0>(d, s.sy2, s.by2, d.n2, d.n3m, st);
-    zlaunch<0>(d, s.sz2, s.bz2, s.ugkks, s.ugkkn, d.n3m, st);
-    ylaunch<1>(d, s.sy3, s.by3, d.n2m, d.n3m - 1, st);
-    zlaunch<1>(d, s.sz3, s.bz3, 0.0, 0.0, d.n3, st);
+    ylaunch<0>(d, &s, st);
+    zlaunch(d, s, st);
 }
 
-void launch_scan_poisson(const Dev &d, cudaStream_t st) {
-    ylaunch<2>(d, ScanSys{nullptr, nullptr, nullptr}, nullptr, d.n2m, d.n3m, st);
-}
+void launch_scan_poisson(const Dev &d, cudaStream_t st) { ylaunch<2>(d, nullptr, st); }
 
 }  // namespace fb

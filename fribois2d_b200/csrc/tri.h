@@ -7,7 +7,8 @@
 
 namespace fb {
 
-constexpr int kYLines = 4;  // contiguous lines per block (one warp each)
+constexpr int kYLines = 2;  // contiguous lines per block
+constexpr int kYWarps = 2;  // warps per contiguous line
 constexpr int kZLines = 4;  // strided lines per block (one warp each)
 
 cudaError_t scan_configure();
