@@ -350,6 +350,7 @@ def device_arm(args, rank, world, local):
                        "l2": "flushed (256 MB write) between timed steps"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": per_step_kernels * K, "clocks": clk,
+            "fp64_gemm_peak_tflops": peak_fp64,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()} for r in table],
             "wall_s": wall,
         }

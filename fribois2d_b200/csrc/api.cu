@@ -3,8 +3,6 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -32,14 +30,13 @@ struct fb_ctx {
     fb::HostCase hc;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;              // marker set-up branch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cublasHandle_t blas = nullptr;
     Dev d{};
     SubDev sub[3]{};
     double usdtal[3] = {0, 0, 0};
     std::vector<void *> allocs;
-    void *sort_tmp = nullptr;
-    size_t sort_tmp_bytes = 0;
-    int sort_bits = 32;
     int hist_cap = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -287,6 +284,9 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     CK(cudaSetDevice(device));
     CK(fb::scan_configure());
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     CB(cublasCreate(&c->blas));
@@ -383,10 +383,11 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = dnew(c, &d.phi, nlm * 2 * fb::kSD))) return st;
     if ((st = dnew(c, &d.cl, nlm * 2))) return st;
     if ((st = dnew(c, &d.contrib, nlm * 2 * fb::kSD))) return st;
-    if ((st = dnew(c, &d.skey_in, nlm * 2 * fb::kSD))) return st;
-    if ((st = dnew(c, &d.sval_in, nlm * 2 * fb::kSD))) return st;
-    if ((st = dnew(c, &d.skey, nlm * 2 * fb::kSD))) return st;
-    if ((st = dnew(c, &d.sval, nlm * 2 * fb::kSD))) return st;
+    d.bcap = 16;
+    if (d.nlm) {
+        if ((st = dnew(c, &d.bcnt, 2 * nf))) return st;
+        if ((st = dnew(c, &d.bucket, 2 * nf * static_cast<size_t>(d.bcap)))) return st;
+    }
     if ((st = dnew(c, &d.probe, nlm * 24))) return st;
     if ((st = dnew(c, &d.press, nlm))) return st;
     if ((st = dnew(c, &d.tau, nlm * 2))) return st;
@@ -429,15 +430,6 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = build_poisson(c))) return st;
     if ((st = dup(c, &c->zmm, c->hc.zmm))) return st;
     if ((st = dup(c, &c->zmmt, c->hc.zmmt))) return st;
-    c->sort_bits = 1;
-    while ((static_cast<uint64_t>(1) << c->sort_bits) < static_cast<uint64_t>(2) * nf + 1) ++c->sort_bits;
-    if (d.nlm) {
-        int nitems = 2 * d.nlm * fb::kSD;
-        cub::DeviceRadixSort::SortPairs(nullptr, c->sort_tmp_bytes, d.skey_in, d.skey, d.sval_in, d.sval,
-                                        nitems, 0, c->sort_bits, c->stream);
-        CK(cudaMalloc(&c->sort_tmp, std::max<size_t>(c->sort_tmp_bytes, 16)));
-        c->allocs.push_back(c->sort_tmp);
-    }
     CK(cudaDeviceSynchronize());
     return FB_OK;
 }
@@ -480,16 +472,6 @@ int gemm_bwd(fb_ctx *c) {   // phcalc_outflow.F90:61,65-69, dph = vmn * zmm^T
     return FB_OK;
 }
 
-int run_sort(fb_ctx *c) {
-    const Dev &d = c->d;
-    const int nitems = 2 * d.nlm * fb::kSD;
-    size_t bytes = c->sort_tmp_bytes;
-    if (cub::DeviceRadixSort::SortPairs(c->sort_tmp, bytes, d.skey_in, d.skey, d.sval_in, d.sval, nitems, 0,
-                                        c->sort_bits, c->stream) != cudaSuccess)
-        return FB_ERR_CUDA;
-    return FB_OK;
-}
-
 int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     double al, ga, ro;
     coefs(c, ns, n, al, ga, ro);
@@ -509,10 +491,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_ST_LGRDIST: fb::launch_lgrdist(d, st); break;
     case FB_ST_FORCING:
         if (!d.nlm) break;
-        if (n == 1) {
-            fb::launch_mls_setup(d, st);
-            if ((r = run_sort(c))) return r;
-        }
+        if (n == 1) fb::launch_mls_setup(d, st);
         fb::launch_mls_interp(d, st);
         fb::launch_mls_spread(d, st);
         break;
@@ -544,14 +523,27 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
 int enqueue_fluid(fb_ctx *c, int ns) {
     const Dev &d = c->d;
     int r;
+    // The marker set-up of substep 1 (lgrdistribution, MLS weights) reads
+    // only marker data: it runs on a side branch while cfl, boucdq and the
+    // explicit terms run on the main stream.
+    if (d.nlm) {
+        CK(cudaEventRecord(c->ev_fork, c->stream));
+        CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+        c->own_launches += 2;
+        fb::launch_lgrdist(d, c->side);
+        fb::launch_mls_setup(d, c->side);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->ev_join, c->side));
+    }
     if ((r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
     c->beta = c->dt / c->hc.grid.ren * 0.5;
     for (int n = 1; n <= d.nsst; ++n) {
         if ((r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
         if ((r = stage_impl(c, FB_ST_NL_RHS, ns, n))) return r;
         if (d.nlm) {
-            if (n == 1 && (r = stage_impl(c, FB_ST_LGRDIST, ns, n))) return r;
-            if ((r = stage_impl(c, FB_ST_FORCING, ns, n))) return r;
+            if (n == 1) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+            // the weights are ready: interpolation and spreading only
+            if ((r = stage_impl(c, FB_ST_FORCING, ns, n == 1 ? 2 : n))) return r;
         }
         if ((r = stage_impl(c, FB_ST_HELSOLVE, ns, n))) return r;
         if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
@@ -715,6 +707,9 @@ int fb_destroy(fb_ctx *c) {
     if (c->blas) cublasDestroy(c->blas);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return FB_OK;
@@ -933,15 +928,30 @@ int fb_stage(fb_ctx *c, int stage, int n) {
 
 int fb_time_stage(fb_ctx *c, int stage, int n, int reps, double *ms) {
     if (!c || !ms || reps < 1 || n < 1 || n > c->d.nsst) return FB_ERR_STATE;
+    // reps launches captured into one graph, so that host launch cost does
+    // not enter the device time of short kernels
     int r = stage_impl(c, stage, c->cur_ns, n);
     if (r) return r;
-    CK(cudaEventRecord(c->ev0, c->stream));
-    for (int i = 0; i < reps; ++i)
-        if ((r = stage_impl(c, stage, c->cur_ns, n))) return r;
-    CK(cudaEventRecord(c->ev1, c->stream));
-    CK(cudaEventSynchronize(c->ev1));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < reps && !r; ++i) r = stage_impl(c, stage, c->cur_ns, n);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return r ? r : FB_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&ge, g, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ge, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ge, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
     float t = 0.f;
-    CK(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, c->ev0, c->ev1);
+    if (ge) cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return FB_ERR_CUDA;
     *ms = static_cast<double>(t) / reps;
     CK(cudaMemsetAsync(c->d.status, 0, sizeof(int), c->stream));
     CK(cudaStreamSynchronize(c->stream));

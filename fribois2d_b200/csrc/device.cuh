@@ -52,7 +52,8 @@ struct Dev {
     int *eulins;             // [marker][dir][2][kSD]
     double *phi, *cl;        // [marker][dir][kSD], [marker][dir]
     double *contrib;         // [marker][dir][kSD] forcing contributions of one substep
-    uint32_t *skey_in, *sval_in, *skey, *sval;  // spreading order (sorted by cell)
+    int *bcnt, *bucket;      // markers per support-box start cell, [dir][cell] and [dir][cell][bcap]
+    int bcap;
     double *probe;           // [marker][24]: ucy(7), ucz(7), pc(7), tan(2), flag
     double *press, *tau, *bcerrv, *bcerrw;
     // rigid body

@@ -57,54 +57,6 @@ __device__ double block_reduce_fast(double v, double *sh) {
     return r;
 }
 
-// fixed-shape tree reduction over a block (blockDim.x * blockDim.y <= 1024)
-template <bool kMax>
-__device__ double block_reduce(double v, double *sh) {
-    const int t = threadIdx.x + threadIdx.y * blockDim.x;
-    const int n = blockDim.x * blockDim.y;
-    sh[t] = v;
-    __syncthreads();
-    for (int s = 512; s > 0; s >>= 1) {
-        if (t < s && t + s < n) sh[t] = kMax ? fmax(sh[t], sh[t + s]) : sh[t] + sh[t + s];
-        __syncthreads();
-    }
-    double r = sh[0];
-    __syncthreads();
-    return r;
-}
-
-// Grid-wide deterministic reduction: every block deposits its partial,
-// the last block to arrive combines them in block order.  Returns true in
-// the last block (all its threads), with *out set there.
-template <bool kMax>
-__device__ bool grid_reduce(const Dev &d, double v, int slot, double *out, double *sh) {
-    const int nb = gridDim.x * gridDim.y;
-    const int b = blockIdx.x + blockIdx.y * gridDim.x;
-    const int t = threadIdx.x + threadIdx.y * blockDim.x;
-    const int nt = blockDim.x * blockDim.y;
-    __shared__ bool last;
-    double part = block_reduce<kMax>(v, sh);
-    double *red = d.red + static_cast<size_t>(slot) * kRedSlot;
-    if (t == 0) {
-        red[b] = part;
-        __threadfence();
-        unsigned prev = atomicAdd(d.count + slot, 1u);
-        last = (prev == static_cast<unsigned>(nb - 1));
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    double acc = kMax ? -INFINITY : 0.0;
-    for (int i = t; i < nb; i += nt) {
-        double x = __ldcg(red + i);
-        acc = kMax ? fmax(acc, x) : acc + x;
-    }
-    double r = block_reduce<kMax>(acc, sh);
-    if (t == 0) d.count[slot] = 0u;
-    *out = r;
-    return true;
-}
-
 // ------------------------------------------------------------ cfl
 
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
@@ -158,7 +110,7 @@ __global__ void __launch_bounds__(256) k_cfl(Dev d) {
 
 // iobcs.F90:5-77 (boucdq): radiative outflow increments + mass-flux correction
 __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
-    __shared__ double sh[1024];
+    __shared__ double sh[32];
     const int n3 = d.n3, n3m = d.n3m;
     double qout = 0.0;
     for (int j = threadIdx.x + 1; j <= d.n2; j += blockDim.x) {
@@ -176,7 +128,7 @@ __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
         d.dq3x2o[j] = dq3x2;
         qout = qout + dqb3n * (d.g2rm[j] / d.dx2);
     }
-    double q = block_reduce<false>(qout, sh);
+    double q = block_reduce_fast<false>(qout, sh);
     const double cor = (0.0 - q) / d.area_out;
     __syncthreads();
     for (int j = threadIdx.x + 1; j <= d.n2m; j += blockDim.x) d.dqb3n[j] = d.dqb3n[j] + cor;
@@ -305,6 +257,14 @@ __device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
 __global__ void k_lgrdist(Dev d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nlm) return;
+    {   // empty the support-box buckets this marker filled at the previous step
+        const size_t nf = static_cast<size_t>(d.NK) * d.P;
+        for (int dir = 0; dir < 2; ++dir) {
+            const int *eu = d.eulins + static_cast<size_t>(2 * i + dir) * 2 * kSD;
+            const int j0 = eu[0], k0 = eu[kSD];
+            if (j0 >= 1 && j0 <= d.n2 && k0 >= 0 && k0 <= d.n3) d.bcnt[dir * nf + fidx(d, j0, k0)] = 0;
+        }
+    }
     const double y = d.lmcc[2 * i], z = d.lmcc[2 * i + 1];
     if (y > d.rext2 || y < 0.0 || z > d.alx3 || z < 0.0 || !(y == y) || !(z == z)) {
         raise_status(d, FB_ERR_MARKER_OUT);
@@ -452,13 +412,7 @@ __global__ void k_mls_setup(Dev d) {
     const int n = t >> 1, idir = (t & 1) + 1;
     double *phi = d.phi + static_cast<size_t>(t) * kSD;
     int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
-    uint32_t *key = d.skey_in + static_cast<size_t>(t) * kSD;
-    uint32_t *val = d.sval_in + static_cast<size_t>(t) * kSD;
-    for (int m = 0; m < kSD; ++m) {
-        phi[m] = 0.0;
-        key[m] = 0xFFFFFFFFu;
-        val[m] = static_cast<uint32_t>(t * kSD + m);
-    }
+    for (int m = 0; m < kSD; ++m) phi[m] = 0.0;
     d.cl[t] = 0.0;
     if (*d.status) return;
     const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
@@ -504,17 +458,16 @@ __global__ void k_mls_setup(Dev d) {
         lgr_h = lgr_h + 1.0 / 2.0 * ph[m] * (sdd[0][m] + sdd[1][m]);
     }
     d.cl[t] = d.lmA[n] * lgr_h / dvel;
-    const uint32_t base = (idir == 1) ? 0u : static_cast<uint32_t>(d.NK) * static_cast<uint32_t>(d.P);
     for (int m = 0; m < kSD; ++m) {
         phi[m] = ph[m];
         eu[m] = eul[0][m];
         eu[kSD + m] = eul[1][m];
-        const int j = eul[0][m], k = eul[1][m];
-        // cells helsolve reads: v at j = 2..n2m, k = 1..n3m; w at j = 1..n2m, k = 2..n3m
-        const bool used = (idir == 1) ? (j >= 2 && j <= d.n2m && k >= 1 && k <= d.n3m)
-                                      : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
-        if (used) key[m] = base + static_cast<uint32_t>(fidx(d, j, k));
     }
+    // register the support box (start cell = node m = 0) for the spreading
+    const size_t cell = static_cast<size_t>(idir - 1) * d.NK * d.P + fidx(d, eul[0][0], eul[1][0]);
+    const int slot = atomicAdd(d.bcnt + cell, 1);
+    if (slot < d.bcap) d.bucket[cell * d.bcap + slot] = n;
+    else raise_status(d, FB_ERR_UNSUPPORTED);
 }
 
 // interp_spread (forcing_MLS.F90:135-182), interpolation half: the
@@ -554,22 +507,60 @@ __global__ void k_mls_interp(Dev d) {
     for (int m = 0; m < kSD; ++m) c[m] = clv * phi[m] * f;
 }
 
-// interp_spread, spreading half, without atomics: contributions sorted by
-// target cell (stable, so each cell keeps the reference's marker order) are
-// summed by the segment head, then helsolve.F90:22,47 adds fe*dt to rhs.
-__global__ void k_mls_spread(Dev d, int nitems) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nitems) return;
+// interp_spread, spreading half, without atomics on the field: the markers
+// whose support box holds a cell are found in the buckets of the 3 x 3
+// possible box start cells; the toucher with the lowest index sums all
+// contributions in increasing marker index (the reference's loop order,
+// forcing_MLS.F90:51-104) and adds fe*dt to rhs (helsolve.F90:22,47).
+__global__ void k_mls_spread(Dev d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= 2 * d.nlm * kSD) return;
     if (*d.status) return;
-    const uint32_t key = d.skey[i];
-    if (key == 0xFFFFFFFFu) return;
-    if (i > 0 && d.skey[i - 1] == key) return;
+    const int t = g / kSD, m = g % kSD, n = t >> 1, dir = t & 1;
+    const double pos2 = d.lmcc[2 * n + 1];
+    if (!(d.zz[1] < pos2 && pos2 < d.zz[d.n3])) return;
+    const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+    const int j = eu[m], k = eu[kSD + m];
+    // cells helsolve reads: v at j = 2..n2m, k = 1..n3m; w at j = 1..n2m, k = 2..n3m
+    const bool used = (dir == 0) ? (j >= 2 && j <= d.n2m && k >= 1 && k <= d.n3m)
+                                 : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
+    if (!used) return;
+    const size_t plane = static_cast<size_t>(dir) * d.NK * d.P;
+    constexpr int kMax = 48;  // touchers of one cell (about 3 x 3 cells of markers)
+    int cand[kMax], slotm[kMax];
+    int nc = 0;
+    for (int dj = 0; dj <= 2; ++dj)
+        for (int dk = 0; dk <= 2; ++dk) {
+            const int sj = j - dj, sk = k - dk;
+            if (sj < 1 || sk < 0) continue;
+            const size_t cell = plane + fidx(d, sj, sk);
+            const int c = min(d.bcnt[cell], d.bcap);
+            for (int q = 0; q < c; ++q) {
+                const int nn = d.bucket[cell * d.bcap + q];
+                if (nn < n) return;  // a lower-index toucher owns this cell
+                if (nc == kMax) {
+                    raise_status(d, FB_ERR_UNSUPPORTED);
+                    return;
+                }
+                cand[nc] = nn;
+                slotm[nc] = dj * 3 + dk;  // position of the cell in that marker's box
+                ++nc;
+            }
+        }
+    // this marker has the lowest index: sum in increasing marker order
     double fe = 0.0;
-    for (int t = i; t < nitems && d.skey[t] == key; ++t) fe = fe + d.contrib[d.sval[t]];
-    const uint32_t plane = static_cast<uint32_t>(d.NK) * static_cast<uint32_t>(d.P);
-    double *r = (key >= plane) ? d.rhs3 : d.rhs2;
-    const uint32_t cell = (key >= plane) ? key - plane : key;
-    r[cell] = r[cell] + fe * d.dt;
+    int last = -1;
+    for (int r = 0; r < nc; ++r) {
+        int best = -1;
+        for (int q = 0; q < nc; ++q)
+            if (cand[q] > last && (best < 0 || cand[q] < cand[best])) best = q;
+        if (best < 0) break;
+        last = cand[best];
+        fe = fe + d.contrib[static_cast<size_t>(2 * cand[best] + dir) * kSD + slotm[best]];
+    }
+    double *r = (dir == 0) ? d.rhs2 : d.rhs3;
+    const size_t i = fidx(d, j, k);
+    r[i] = r[i] + fe * d.dt;
 }
 
 // ------------------------------------------------------------ tridiagonal
@@ -898,8 +889,8 @@ __global__ void k_loads_probe(Dev d) {
 // from the previous marker when the probe's tangential velocity vanishes;
 // pressure extrapolation (Wang et al. 2019 eq. 20) and wall shear (eq. 26).
 // Also the L2 norms of checkbcs (ckbcs.F90:76-81).  Single block.
-__global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
-    __shared__ double sh[1024];
+__global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
+    __shared__ double sh[32];
     const double hpr = d.ddmin * d.kprobe, visc = d.visc;
     double sv = 0.0, sw = 0.0;
     const bool ok = (*d.status == 0);
@@ -961,8 +952,8 @@ __global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
         sv = sv + d.bcerrv[n] * d.bcerrv[n];
         sw = sw + d.bcerrw[n] * d.bcerrw[n];
     }
-    const double tv = block_reduce<false>(sv, sh);
-    const double tw = block_reduce<false>(sw, sh);
+    const double tv = block_reduce_fast<false>(sv, sh);
+    const double tw = block_reduce_fast<false>(sw, sh);
     if (threadIdx.x == 0) {
         d.scal[S_NBCV] = sqrt(tv) / static_cast<double>(d.nlm);
         d.scal[S_NBCW] = sqrt(tw) / static_cast<double>(d.nlm);
@@ -985,8 +976,8 @@ __device__ void modfn(double K[6], const double t[6], const double FF[6], const 
 // rigid.F90:4-138 (rigid) with int_stress :373-464, kinem_RK4 :165-228 /
 // kinem_RK4i :233-299, get_rotmat :142-161, createnorm :468-495; then the
 // clock update of main.F90:92 and one history row.  Single block.
-__global__ void __launch_bounds__(1024) k_rigid(Dev d, int hist_rows) {
-    __shared__ double sh[1024];
+__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
+    __shared__ double sh[32];
     __shared__ double cm[18];
     __shared__ double rot[4];
     const int tid = threadIdx.x, nt = blockDim.x, nlm = d.nlm;
@@ -1003,11 +994,11 @@ __global__ void __launch_bounds__(1024) k_rigid(Dev d, int hist_rows) {
         const double r1 = d.lmcc[2 * i] - R[0], r2 = d.lmcc[2 * i + 1] - R[1];
         mom = mom + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
     }
-    fyp = block_reduce<false>(fyp, sh);
-    fzp = block_reduce<false>(fzp, sh);
-    fyv = block_reduce<false>(fyv, sh);
-    fzv = block_reduce<false>(fzv, sh);
-    mom = block_reduce<false>(mom, sh);
+    fyp = block_reduce_fast<false>(fyp, sh);
+    fzp = block_reduce_fast<false>(fzp, sh);
+    fyv = block_reduce_fast<false>(fyv, sh);
+    fzv = block_reduce_fast<false>(fzv, sh);
+    mom = block_reduce_fast<false>(mom, sh);
     if (tid == 0) {
         const double time = d.scal[S_TIME], dt = d.dt;
         const double fy = fyp + fyv, fz = fzp + fzv;
@@ -1154,7 +1145,7 @@ void launch_mls_interp(const Dev &d, cudaStream_t s) {
 }
 void launch_mls_spread(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;
-    if (n) k_mls_spread<<<(n + 255) / 256, 256, 0, s>>>(d, n);
+    if (n) k_mls_spread<<<(n + 127) / 128, 128, 0, s>>>(d);
 }
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s) {
     k_tri_y2<<<(d.n3m + 63) / 64, 64, 0, s>>>(d, sd);
@@ -1176,10 +1167,10 @@ void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
     k_loads_probe<<<(3 * d.nlm + 63) / 64, 64, 0, s>>>(d);
-    k_loads_finish<<<1, 1024, 0, s>>>(d);
+    k_loads_finish<<<1, 256, 0, s>>>(d);
 }
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s) {
-    if (d.nlm) k_rigid<<<1, 1024, 0, s>>>(d, hist_rows);
+    if (d.nlm) k_rigid<<<1, 256, 0, s>>>(d, hist_rows);
 }
 
 }  // namespace fb
