@@ -387,6 +387,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if (d.nlm) {
         if ((st = dnew(c, &d.bcnt, 2 * nf))) return st;
         if ((st = dnew(c, &d.bucket, 2 * nf * static_cast<size_t>(d.bcap)))) return st;
+        if ((st = dnew(c, &d.chain, nlm * 2 * fb::kSD))) return st;
     }
     if ((st = dnew(c, &d.probe, nlm * 24))) return st;
     if ((st = dnew(c, &d.press, nlm))) return st;
@@ -483,7 +484,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     cudaStream_t st = c->stream;
     int r = FB_OK;
     static const int kOwn[18] = {1, 1, 1, 0, 0, 0, 1, 2, 4, 1, 1, 1, 0, 1, 0, 2, 2, 1};
-    if (stage >= 0 && stage < 18) c->own_launches += kOwn[stage] + ((stage == FB_ST_FORCING && n == 1) ? 1 : 0);
+    if (stage >= 0 && stage < 18) c->own_launches += kOwn[stage] + ((stage == FB_ST_FORCING && n == 1) ? 2 : 0);
     switch (stage) {
     case FB_ST_CFL: fb::launch_cfl(d, st); break;
     case FB_ST_BOUCDQ: fb::launch_boucdq(d, ga, ro, st); break;
@@ -491,7 +492,10 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_ST_LGRDIST: fb::launch_lgrdist(d, st); break;
     case FB_ST_FORCING:
         if (!d.nlm) break;
-        if (n == 1) fb::launch_mls_setup(d, st);
+        if (n == 1) {
+            fb::launch_mls_setup(d, st);
+            fb::launch_spread_chains(d, st);
+        }
         fb::launch_mls_interp(d, st);
         fb::launch_mls_spread(d, st);
         break;
@@ -529,9 +533,10 @@ int enqueue_fluid(fb_ctx *c, int ns) {
     if (d.nlm) {
         CK(cudaEventRecord(c->ev_fork, c->stream));
         CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-        c->own_launches += 2;
+        c->own_launches += 3;
         fb::launch_lgrdist(d, c->side);
         fb::launch_mls_setup(d, c->side);
+        fb::launch_spread_chains(d, c->side);
         CK(cudaGetLastError());
         CK(cudaEventRecord(c->ev_join, c->side));
     }

@@ -54,6 +54,8 @@ struct Dev {
     double *contrib;         // [marker][dir][kSD] forcing contributions of one substep
     int *bcnt, *bucket;      // markers per support-box start cell, [dir][cell] and [dir][cell][bcap]
     int bcap;
+    int *chain;              // per contribution slot: next slot of the same cell in marker
+                             // order (>= 0), -1 at the end; -2 if the slot is not a chain head
     double *probe;           // [marker][24]: ucy(7), ucz(7), pc(7), tan(2), flag
     double *press, *tau, *bcerrv, *bcerrw;
     // rigid body

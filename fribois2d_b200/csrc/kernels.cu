@@ -507,14 +507,17 @@ __global__ void k_mls_interp(Dev d) {
     for (int m = 0; m < kSD; ++m) c[m] = clv * phi[m] * f;
 }
 
-// interp_spread, spreading half, without atomics on the field: the markers
-// whose support box holds a cell are found in the buckets of the 3 x 3
-// possible box start cells; the toucher with the lowest index sums all
-// contributions in increasing marker index (the reference's loop order,
-// forcing_MLS.F90:51-104) and adds fe*dt to rhs (helsolve.F90:22,47).
-__global__ void k_mls_spread(Dev d) {
+// interp_spread, spreading half, without atomics on the field.  Once per
+// step (the supports are fixed for the three substeps) every cell's touchers
+// are found in the buckets of the 3 x 3 possible box start cells and chained
+// in increasing marker index (the reference's loop order,
+// forcing_MLS.F90:51-104); the head of each chain is the lowest-index
+// toucher.  Every substep the heads then add their chain's sum fe*dt to rhs
+// (helsolve.F90:22,47).
+__global__ void k_spread_chains(Dev d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
+    d.chain[g] = -2;
     if (*d.status) return;
     const int t = g / kSD, m = g % kSD, n = t >> 1, dir = t & 1;
     const double pos2 = d.lmcc[2 * n + 1];
@@ -526,40 +529,54 @@ __global__ void k_mls_spread(Dev d) {
                                  : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
     if (!used) return;
     const size_t plane = static_cast<size_t>(dir) * d.NK * d.P;
-    constexpr int kMax = 48;  // touchers of one cell (about 3 x 3 cells of markers)
-    int cand[kMax], slotm[kMax];
-    int nc = 0;
+    // lowest-index toucher only
     for (int dj = 0; dj <= 2; ++dj)
         for (int dk = 0; dk <= 2; ++dk) {
             const int sj = j - dj, sk = k - dk;
             if (sj < 1 || sk < 0) continue;
             const size_t cell = plane + fidx(d, sj, sk);
             const int c = min(d.bcnt[cell], d.bcap);
-            for (int q = 0; q < c; ++q) {
-                const int nn = d.bucket[cell * d.bcap + q];
-                if (nn < n) return;  // a lower-index toucher owns this cell
-                if (nc == kMax) {
-                    raise_status(d, FB_ERR_UNSUPPORTED);
-                    return;
-                }
-                cand[nc] = nn;
-                slotm[nc] = dj * 3 + dk;  // position of the cell in that marker's box
-                ++nc;
-            }
+            for (int q = 0; q < c; ++q)
+                if (d.bucket[cell * d.bcap + q] < n) return;
         }
-    // this marker has the lowest index: sum in increasing marker order
-    double fe = 0.0;
-    int last = -1;
-    for (int r = 0; r < nc; ++r) {
-        int best = -1;
-        for (int q = 0; q < nc; ++q)
-            if (cand[q] > last && (best < 0 || cand[q] < cand[best])) best = q;
+    // walk the touchers in increasing marker index, linking their slots
+    int prev_slot = g, last = n;
+    for (;;) {
+        int best = -1, best_slot = -1;
+        for (int dj = 0; dj <= 2; ++dj)
+            for (int dk = 0; dk <= 2; ++dk) {
+                const int sj = j - dj, sk = k - dk;
+                if (sj < 1 || sk < 0) continue;
+                const size_t cell = plane + fidx(d, sj, sk);
+                const int c = min(d.bcnt[cell], d.bcap);
+                for (int q = 0; q < c; ++q) {
+                    const int nn = d.bucket[cell * d.bcap + q];
+                    if (nn > last && (best < 0 || nn < best)) {
+                        best = nn;
+                        best_slot = (2 * nn + dir) * kSD + dj * 3 + dk;
+                    }
+                }
+            }
         if (best < 0) break;
-        last = cand[best];
-        fe = fe + d.contrib[static_cast<size_t>(2 * cand[best] + dir) * kSD + slotm[best]];
+        d.chain[prev_slot] = best_slot;
+        prev_slot = best_slot;
+        last = best;
     }
+    d.chain[prev_slot] = -1;
+}
+
+__global__ void k_mls_spread(Dev d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= 2 * d.nlm * kSD) return;
+    if (*d.status) return;
+    if (d.chain[g] == -2) return;  // not the head of a cell's chain
+    const int t = g / kSD, dir = t & 1;
+    const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
+    const int m = g % kSD;
+    double fe = 0.0;
+    for (int s = g; s >= 0; s = d.chain[s]) fe = fe + d.contrib[s];
     double *r = (dir == 0) ? d.rhs2 : d.rhs3;
-    const size_t i = fidx(d, j, k);
+    const size_t i = fidx(d, eu[m], eu[kSD + m]);
     r[i] = r[i] + fe * d.dt;
 }
 
@@ -1142,6 +1159,10 @@ void launch_mls_setup(const Dev &d, cudaStream_t s) {
 }
 void launch_mls_interp(const Dev &d, cudaStream_t s) {
     if (d.nlm) k_mls_interp<<<(2 * d.nlm + 63) / 64, 64, 0, s>>>(d);
+}
+void launch_spread_chains(const Dev &d, cudaStream_t s) {
+    const int n = 2 * d.nlm * kSD;
+    if (n) k_spread_chains<<<(n + 127) / 128, 128, 0, s>>>(d);
 }
 void launch_mls_spread(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;

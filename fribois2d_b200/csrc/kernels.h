@@ -16,6 +16,7 @@ void launch_lgrdist(const Dev &d, cudaStream_t s);
 void launch_mls_setup(const Dev &d, cudaStream_t s);
 void launch_mls_interp(const Dev &d, cudaStream_t s);
 void launch_mls_spread(const Dev &d, cudaStream_t s);
+void launch_spread_chains(const Dev &d, cudaStream_t s);
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
 void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s);
