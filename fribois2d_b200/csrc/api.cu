@@ -388,6 +388,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         if ((st = dnew(c, &d.bcnt, 2 * nf))) return st;
         if ((st = dnew(c, &d.bucket, 2 * nf * static_cast<size_t>(d.bcap)))) return st;
         if ((st = dnew(c, &d.chain, nlm * 2 * fb::kSD))) return st;
+        if ((st = dnew(c, &d.chead, nlm * 2 * fb::kSD))) return st;
     }
     if ((st = dnew(c, &d.probe, nlm * 24))) return st;
     if ((st = dnew(c, &d.press, nlm))) return st;

@@ -55,7 +55,8 @@ struct Dev {
     int *bcnt, *bucket;      // markers per support-box start cell, [dir][cell] and [dir][cell][bcap]
     int bcap;
     int *chain;              // per contribution slot: next slot of the same cell in marker
-                             // order (>= 0), -1 at the end; -2 if the slot is not a chain head
+                             // order (>= 0) or -1 at the end, written by the cell's head
+    int *chead;              // per contribution slot: 1 if it heads its cell's chain
     double *probe;           // [marker][24]: ucy(7), ucz(7), pc(7), tan(2), flag
     double *press, *tau, *bcerrv, *bcerrw;
     // rigid body

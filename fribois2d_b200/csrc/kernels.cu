@@ -517,7 +517,7 @@ __global__ void k_mls_interp(Dev d) {
 __global__ void k_spread_chains(Dev d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
-    d.chain[g] = -2;
+    d.chead[g] = 0;
     if (*d.status) return;
     const int t = g / kSD, m = g % kSD, n = t >> 1, dir = t & 1;
     const double pos2 = d.lmcc[2 * n + 1];
@@ -540,6 +540,7 @@ __global__ void k_spread_chains(Dev d) {
                 if (d.bucket[cell * d.bcap + q] < n) return;
         }
     // walk the touchers in increasing marker index, linking their slots
+    d.chead[g] = 1;
     int prev_slot = g, last = n;
     for (;;) {
         int best = -1, best_slot = -1;
@@ -569,7 +570,7 @@ __global__ void k_mls_spread(Dev d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
     if (*d.status) return;
-    if (d.chain[g] == -2) return;  // not the head of a cell's chain
+    if (!d.chead[g]) return;  // not the head of a cell's chain
     const int t = g / kSD, dir = t & 1;
     const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
     const int m = g % kSD;
