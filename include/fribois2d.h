@@ -4,7 +4,7 @@
  * The reference (AleNit/FRiBoIS2D, Fortran 90 + MPI) has no plugin or FFI
  * boundary: its driver calls module subroutines on global state
  * (src/main.F90:51-97).  This header is the boundary a Fortran host binds
- * with ISO_C_BINDING (`bind(C)` interfaces; see INTEGRATION.md) to replace
+ * with ISO_C_BINDING (`bind(C)` interfaces) to replace
  * those subroutines with one GPU.  Conventions:
  *
  *  - every function returns an int status (FB_OK = 0); the reference aborts
