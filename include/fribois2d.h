@@ -189,6 +189,25 @@ int fb_host_array(fb_host *h, int id, double *out, int64_t n);
 int fb_eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr,
                      double *zmm, double *zmmt);
 
+/* ---- CFL number without any allocation ------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot let a library allocate device memory (their arrays live in another
+ * runtime's data regions or in an arena under a hard budget).  It computes
+ * what cfl.F90 computes -- out[0] = max over cells of
+ * (|(v_j + v_j+1)/2 * udx2m_j| + |(w_k + w_k+1)/2 * udx3m_k|) * dt and
+ * out[1] = the area-weighted mean of w -- from the caller's own device arrays:
+ * q2, q3 as (j, k) at q[k*pitch + j-1], k = 0..n3; rc (n2), zz (n3),
+ * udx2m (n2-1), udx3m (n3-1) 0-based; out: 2 doubles of device memory.
+ * The partial results go to a fixed array inside the library (room for
+ * FB_NOALLOC_MAX_ROWS rows of z cells; larger grids return FB_ERR_UNSUPPORTED).
+ * The first call on a device looks up that array's address (make it before
+ * any stream capture); every call shares the array, so calls whose kernels
+ * overlap on the GPU race.  Asynchronous on `stream` (a cudaStream_t, or NULL). */
+#define FB_NOALLOC_MAX_ROWS 8192
+int fb_cfl_noalloc(const double *q2, const double *q3, int pitch, int n2, int n3, const double *rc,
+                   const double *zz, const double *udx2m, const double *udx3m, double dt, double rext2,
+                   double alx3, double *out, void *stream);
+
 const char *fb_status_string(int status);
 const char *fb_version(void);
 
