@@ -37,7 +37,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config3"])
+    ap.add_argument("--config", default="galloping_rectangle_1024x768",
+                    choices=["viv_cylinder_384x256", "galloping_rectangle_1024x768", "viv_cylinder_2048x1536"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -51,9 +52,24 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(dist, x: float, device) -> float:
+    """Largest value of x over all ranks (every rank takes this collective)."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, cells: int, steps: int, max_ms: float) -> float:
+    """Whole-job cell-steps/s: every rank advanced its own replica `steps`
+    steps of `cells` cells; the job took as long as its slowest rank."""
+    return world * cells * steps / (max_ms * 1e-3)
+
+
 def make_case(name):
     from fribois2d_b200 import case as cases
-    return cases.CONFIGS[name]()
+    return cases.WORKLOADS[name]()
 
 
 def write_deck(c, rank=0):
@@ -264,11 +280,8 @@ def device_arm(args, rank, world, local):
     barrier()
     wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms_max = float(t.item())
-    value = world * c.cells * K / (dev_ms_max * 1e-3)
+    dev_ms_max = max_over_ranks(dist, dev_ms, dev)
+    value = replica_throughput(world, c.cells, K, dev_ms_max)
 
     # end to end through the C ABI with host buffers (loose FSI coupling as
     # the reference runs it: markers in, fluid step, rigid step, state out)
@@ -296,10 +309,8 @@ def device_arm(args, rank, world, local):
                 assert L.fb_get_array(s.ctx, idx, b, 2 * nlm) == 0
         barrier()
         te = time.perf_counter() - te0
-        tt = torch.tensor([te], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * c.cells * Ke / float(tt.item()), "unit": UNIT,
+        te_max = max_over_ranks(dist, te, dev)
+        e2e = {"value": replica_throughput(world, c.cells, Ke, 1e3 * te_max), "unit": UNIT,
                "h2d_bytes_per_step": 4 * 2 * nlm * 8, "d2h_bytes_per_step": 4 * 2 * nlm * 8 + 8 * 8,
                "steps": Ke, "timing": "host wall clock, per-step synchronous C-ABI calls"}
 

@@ -392,17 +392,17 @@ def galloping_rectangle(n3m: int = 1024, n2m: int = 768, h: float = 1.0 / 96,
                 v_noise=0.0, steps=steps)
 
 
-def config1() -> Case:
+def viv_cylinder_384x256() -> Case:
     """VIV cylinder, 384 (z) x 256 (y) cells, h = D/48, 302 markers."""
     return viv_cylinder(name="viv_cylinder_384x256")
 
 
-def config2() -> Case:
+def galloping_rectangle_1024x768() -> Case:
     """Rotational galloping rectangle, 1024 (z) x 768 (y) cells, h = D/96."""
     return galloping_rectangle(name="galloping_rectangle_1024x768")
 
 
-def config3() -> Case:
+def viv_cylinder_2048x1536() -> Case:
     """VIV cylinder, 2048 (z) x 1536 (y) cells, h = D/192, 604 markers, Re 200."""
     return viv_cylinder(n3m=2048, n2m=1536, h=1.0 / 192, zwin=(-2.0, 6.0), ywin=(-3.0, 3.0),
                         nlm=604, re=200.0, name="viv_cylinder_2048x1536")
@@ -425,4 +425,4 @@ def tiny_rectangle(n3m: int = 64, n2m: int = 40, h: float = 1.0 / 8, nlm: int = 
                                name=f"tiny_rectangle_{n3m}x{n2m}")
 
 
-CONFIGS = {"config1": config1, "config2": config2, "config3": config3}
+WORKLOADS = {f.__name__: f for f in (viv_cylinder_384x256, galloping_rectangle_1024x768, viv_cylinder_2048x1536)}

@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol():
     assert "sm_100a" in fb.version()
 
 
-@pytest.mark.parametrize("maker", [cases.tiny_cylinder, cases.tiny_rectangle, cases.config1])
+@pytest.mark.parametrize("maker", [cases.tiny_cylinder, cases.tiny_rectangle, cases.viv_cylinder_384x256])
 def test_host_setup_bit_identical_to_oracle(maker, tmp_path):
     c = maker()
     path = c.write(str(tmp_path / c.name))
@@ -56,7 +56,7 @@ def test_host_setup_bit_identical_to_oracle(maker, tmp_path):
 def test_eigen_setup_reproduces_lapack_poisson_operator(tmp_path):
     """The symmetric-tridiagonal eigen-decomposition (host.cpp) replaces
     phini's DGEEV + DGESV: same spectrum, Z diag(wr) Z^-1 equals the operator."""
-    c = cases.config1()
+    c = cases.viv_cylinder_384x256()
     path = c.write(str(tmp_path / c.name))
     h = fb.HostSetup(path)
     d = oracle.parse_deck(path)
