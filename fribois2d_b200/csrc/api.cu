@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -44,6 +45,7 @@ struct fb_ctx {
     double last_ms = 0.0;
     double *zmm = nullptr, *zmmt = nullptr;  // Poisson eigenvectors and inverse
     int null_mode = -1;
+    bool allow_win = true;    // windowed helsolve allowed (FRIBOIS2D_HELSOLVE=scan turns it off)
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
     int step_kernels = 0;     // own kernels per captured step
     // host copies of the scalar state the reference keeps in modules
@@ -93,9 +95,29 @@ int dup(fb_ctx *c, T **p, const std::vector<T> &v) {
     return FB_OK;
 }
 
+// Smallest K such that every product of K+1 consecutive |c(i)| is at most
+// 2^-56: a recurrence x(i) = c(i) x(i-1) + ... started K positions early from
+// zero then agrees with the full recurrence to below the rounding of FP64.
+int window_len(const std::vector<double> &c, int kmax) {
+    const int n = static_cast<int>(c.size());
+    std::vector<double> L(c.size());
+    for (int i = 0; i < n; ++i)
+        L[static_cast<size_t>(i)] = (c[static_cast<size_t>(i)] == 0.0) ? -HUGE_VAL : std::log2(std::fabs(c[static_cast<size_t>(i)]));
+    for (int K = 0; K <= kmax; ++K) {
+        bool ok = true;
+        for (int m = 0; m + K < n && ok; ++m) {
+            double sum = 0.0;
+            for (int i = m; i <= m + K; ++i) sum += L[static_cast<size_t>(i)];
+            if (sum > -56.0) ok = false;
+        }
+        if (ok) return K;
+    }
+    return kmax + 1;
+}
+
 // tridiagonal system (lower(2:n), diag, upper(1:n-1)) -> device factors
 int upload_tri(fb_ctx *c, TriDev &t, fb::ScanSys &sc, const std::vector<double> &lo,
-               const std::vector<double> &di, const std::vector<double> &up) {
+               const std::vector<double> &di, const std::vector<double> &up, int *win = nullptr) {
     fb::TriLU f = fb::factor(lo, di, up);
     if (f.info != 0) return FB_ERR_NUMERIC;
     std::vector<double> dinv(f.d.size());
@@ -106,6 +128,7 @@ int upload_tri(fb_ctx *c, TriDev &t, fb::ScanSys &sc, const std::vector<double> 
         for (int i = 1; i < n; ++i) a[static_cast<size_t>(i)] = -f.dl[static_cast<size_t>(i - 1)];
         for (int i = 0; i + 1 < n; ++i)
             e[static_cast<size_t>(i)] = -f.du[static_cast<size_t>(i)] * dinv[static_cast<size_t>(i)];
+        if (win) *win = std::max(window_len(a, fb::kWinMax), window_len(e, fb::kWinMax));
         double *q;
         int st2;
         if ((st2 = dup(c, &q, a))) return st2;
@@ -146,6 +169,7 @@ int build_substep(fb_ctx *c, int n, double al) {
     std::vector<double> b(static_cast<size_t>(std::max(n2, n3)) + 2, 0.0);
     int st;
     double *p;
+    int wy2 = 0, wz2 = 0, wy3 = 0, wz3 = 0;
     {   // solq2j (solve_fluid.F90:126-153)
         std::vector<double> am(n2 + 1, 0.0), ap(n2 + 1, 0.0), lo, di(n2, 1.0), up;
         std::fill(b.begin(), b.end(), 0.0);
@@ -157,7 +181,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int j = 2; j <= n2; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2 - 1; ++j) up.push_back(ap[j]);
-        if ((st = upload_tri(c, s.y2, s.sy2, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.y2, s.sy2, lo, di, up, &wy2))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
         s.by2 = p;
     }
@@ -172,7 +196,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int k = 2; k <= n3m; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3m - 1; ++k) up.push_back(ap[k]);
-        if ((st = upload_tri(c, s.z2, s.sz2, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.z2, s.sz2, lo, di, up, &wz2))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
         s.bz2 = p;
         s.ugkks = 1.0 / (g.g3rm[1] * g.g3rc[1]) * g.dx3q * 2.0 * betadx;
@@ -189,7 +213,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int j = 2; j <= n2m; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2m - 1; ++j) up.push_back(ap[j]);
-        if ((st = upload_tri(c, s.y3, s.sy3, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.y3, s.sy3, lo, di, up, &wy3))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
         s.by3 = p;
     }
@@ -204,12 +228,15 @@ int build_substep(fb_ctx *c, int n, double al) {
         }
         for (int k = 2; k <= n3; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3 - 1; ++k) up.push_back(ap[k]);
-        if ((st = upload_tri(c, s.z3, s.sz3, lo, di, up))) return st;
+        if ((st = upload_tri(c, s.z3, s.sz3, lo, di, up, &wz3))) return st;
         if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
         s.bz3 = p;
     }
     c->usdtal[n] = 1.0 / (c->dt * al);
     s.scan_ok = !(s.y2.pivoted || s.z2.pivoted || s.y3.pivoted || s.z3.pivoted);
+    s.win_y = std::max(wy2, wy3);
+    s.win_z = std::max(wz2, wz3);
+    if (!s.scan_ok || !c->allow_win || s.win_y > fb::kWinMax || s.win_z > fb::kWinMax) s.win_y = s.win_z = 0;
     return FB_OK;
 }
 
@@ -281,6 +308,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         return FB_ERR_UNSUPPORTED;
     }
     c->device = device;
+    if (const char *hv = std::getenv("FRIBOIS2D_HELSOLVE")) c->allow_win = std::strcmp(hv, "scan") != 0;
     CK(cudaSetDevice(device));
     CK(fb::scan_configure());
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -501,8 +529,15 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         fb::launch_mls_spread(d, st);
         break;
     case FB_ST_HELSOLVE:
-        if (s.scan_ok) fb::launch_scan_helsolve(d, s, st);
-        else fb::launch_helsolve(d, s, st);
+        if (s.win_y > 0) {
+            fb::launch_win_helsolve(d, s, st);
+            c->own_launches -= 3;
+        } else if (s.scan_ok) {
+            fb::launch_scan_helsolve(d, s, st);
+            c->own_launches -= 2;
+        } else {
+            fb::launch_helsolve(d, s, st);
+        }
         break;
     case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
     case FB_ST_PHCALC:
@@ -823,7 +858,7 @@ int fb_get_dims(fb_ctx *c, int32_t dims[8]) {
     dims[4] = c->d.P;
     dims[5] = c->d.ldh;
     dims[6] = c->sub[0].y2.pivoted | (c->sub[0].z3.pivoted << 1);
-    dims[7] = 0;
+    dims[7] = c->sub[0].win_y | (c->sub[0].win_z << 8);  // windowed helsolve (0: line scans)
     return FB_OK;
 }
 

@@ -28,6 +28,7 @@ struct SubDev {          // substep constants (fluid_tsch.F90:64-77)
     TriDev y2, z2, y3, z3;                // solq2j, solq2k, solq3j, solq3k systems
     ScanSys sy2, sz2, sy3, sz3;           // the same systems for the scan solver
     int scan_ok;                          // 0 if a system needed row interchanges
+    int win_y, win_z;                     // truncation windows (y, z) of the windowed helsolve; 0 = off
 };
 
 struct Dev {

@@ -454,6 +454,219 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb
     }
 }
 
+// ---------------------------------------------------------------- windowed ADI
+
+// helsolve (helsolve.F90:4-56 with solq2j/solq2k/solq3j/solq3k) as one
+// launch over 2-D tiles, both velocity components.  The four Helmholtz
+// operators are strongly diagonally dominant (off-diagonals ~ beta*al/h^2
+// against a unit diagonal), so the influence of a value on the LU
+// recurrences dies out geometrically: the products of K+1 consecutive
+// multipliers a(i) (forward) and e(i) (backward) fall below 2^-56 for a
+// window K that the host measures from the factors of each substep
+// (overlapped, truncated partitions: the truncated-SPIKE idea of Polizzi and
+// Sameh for diagonally dominant banded systems).  A thread computes a
+// segment of kWSeg values of one recurrence exactly as the sequential
+// recurrence would, except that it starts K positions early from zero;
+// segments need no communication.  A tile runs four phases through shared
+// memory: forward and backward y recurrences over the tile's rows plus a
+// halo of K rows on either side in k, then forward and backward z
+// recurrences over its columns, adding the result to q2/q3.  rhs2/rhs3 are
+// read once and q2/q3 read and written once.
+constexpr int kWTj = 32;    // tile columns (j): one lane each in the z phases
+constexpr int kWTk = 64;    // tile rows (k)
+constexpr int kWSeg = 8;    // values per thread segment
+constexpr int kWThreads = 256;
+
+namespace {
+
+// y(i) = a(i) y(i-1) + F(i) for i in [s, s+TS) below n, started from zero
+// at max(0, s-K)
+template <int TS, class FF>
+__device__ __forceinline__ void seg_fwd(const FF &F, int s, int n, int K, const double *__restrict__ a,
+                                        double (&y)[TS]) {
+    double v = 0.0;
+    for (int i = max(0, s - K); i < s; ++i) v = fma(__ldg(a + i), v, F(i));
+#pragma unroll
+    for (int t = 0; t < TS; ++t) {
+        const int i = s + t;
+        y[t] = 0.0;
+        if (i < n) {
+            v = fma(__ldg(a + i), v, F(i));
+            y[t] = v;
+        }
+    }
+}
+
+// x(i) = e(i) x(i+1) + g(i) Y(i) for i in [s, s+TS) below n, started from
+// zero at min(n-1, s+TS-1+K)
+template <int TS, class FY>
+__device__ __forceinline__ void seg_bwd(const FY &Y, int s, int n, int K, const double *__restrict__ e,
+                                        const double *__restrict__ g, double (&x)[TS]) {
+    double v = 0.0;
+    for (int i = min(n - 1, s + TS - 1 + K); i >= s + TS; --i) v = fma(__ldg(e + i), v, __ldg(g + i) * Y(i));
+#pragma unroll
+    for (int t = TS - 1; t >= 0; --t) {
+        const int i = s + t;
+        x[t] = 0.0;
+        if (i < n) {
+            v = fma(__ldg(e + i), v, __ldg(g + i) * Y(i));
+            x[t] = v;
+        }
+    }
+}
+
+struct WinShape {            // shared-memory layout of one tile
+    int cols, pitch, rows;   // right-hand side tile: rows x cols (row stride pitch, odd)
+    int nyf, ypitch;         // forward y segments per row; their row stride (odd)
+    int nzf;                 // forward z segments per column
+    int a_size, b_size;      // doubles in regions A (rhs, then y-solved) and B (y, then z partials)
+    __host__ __device__ WinShape(int Ky, int Kz) {
+        nyf = (kWTj + Ky + kWSeg - 1) / kWSeg;
+        cols = nyf * kWSeg + Ky;  // >= kWTj + 2 Ky: every forward segment reads inside its row
+        pitch = cols | 1;
+        rows = kWTk + 2 * Kz;
+        ypitch = (nyf * kWSeg) | 1;
+        nzf = (kWTk + Kz + kWSeg - 1) / kWSeg;
+        a_size = rows * pitch;
+        const int b1 = rows * ypitch, b2 = nzf * kWSeg * kWTj;
+        b_size = b1 > b2 ? b1 : b2;
+    }
+};
+
+}  // namespace
+
+// blockIdx.y = 0: v (solq2j + solq2k + walls), 1: w (solq3j + solq3k);
+// blockIdx.x = tile (tj fastest).
+__global__ void __launch_bounds__(kWThreads) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
+    extern __shared__ double sm[];
+    const WinShape sh(Ky, Kz);
+    double *A = sm, *B = sm + sh.a_size;
+    const int fld = blockIdx.y;
+    const int tj = blockIdx.x % ntj, tk = blockIdx.x / ntj;
+    const int j0 = 1 + tj * kWTj, k0 = 1 + tk * kWTk;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int kWarps = kWThreads / 32;
+    const ScanSys sy = fld ? sd.sy3 : sd.sy2, sz = fld ? sd.sz3 : sd.sz2;
+    const double *by = fld ? sd.by3 : sd.by2, *bz = fld ? sd.bz3 : sd.bz2;
+    const double *rhs = fld ? d.rhs3 : d.rhs2;
+    double *q = fld ? d.q3 : d.q2;
+    const int ny = fld ? d.n2m : d.n2;   // y unknowns (j = 1..ny, line index j-1)
+    const int nz = fld ? d.n3 : d.n3m;   // z unknowns (k = 1..nz, line index k-1)
+    const int jlo = fld ? 1 : 2;          // columns with a right-hand side
+    const int klo = fld ? 2 : 1;          // rows whose y lines are solved
+    const int rows = sh.rows;
+
+    // 1. right-hand side tile scaled by the y row normalisers (coalesced in j);
+    //    A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r)
+    for (int r = w; r < rows; r += kWarps) {
+        const int k = k0 - Kz + r;
+        const bool kok = (k >= klo && k <= d.n3m);
+        for (int c = lane; c < sh.cols; c += 32) {
+            const int j = j0 - Ky + c;
+            double v = 0.0;
+            if (kok && j >= jlo && j <= d.n2m) v = __ldcg(rhs + fidx(d, j, k)) * __ldg(by + j);
+            A[r * sh.pitch + c] = v;
+        }
+    }
+    __syncthreads();
+
+    // 2. forward y recurrences: lanes = rows, warps = (row group, segment);
+    //    B[r * ypitch + c] = y at column j0 + c, c < nyf * kWSeg
+    const int nrg = (rows + 31) / 32;
+    for (int task = w; task < nrg * sh.nyf; task += kWarps) {
+        const int rg = task / sh.nyf, sg = task - rg * sh.nyf;
+        const int r = rg * 32 + lane, rr = min(r, rows - 1);
+        const double *arow = A + rr * sh.pitch + (1 - j0 + Ky);  // arow[i]: line index i
+        const int s = j0 - 1 + sg * kWSeg;
+        double y[kWSeg];
+        seg_fwd<kWSeg>([&](int i) { return arow[i]; }, s, ny, Ky, sy.a, y);
+        if (r < rows) {
+#pragma unroll
+            for (int t = 0; t < kWSeg; ++t) B[r * sh.ypitch + sg * kWSeg + t] = y[t];
+        }
+    }
+    __syncthreads();
+
+    // 3. backward y recurrences over the tile's columns; A[r * kWTj + c] =
+    //    y-solved value at (j0 + c, k0 - Kz + r) (0 on rows without a y line)
+    for (int task = w; task < nrg * (kWTj / kWSeg); task += kWarps) {
+        const int rg = task / (kWTj / kWSeg), sg = task - rg * (kWTj / kWSeg);
+        const int r = rg * 32 + lane, rr = min(r, rows - 1);
+        const int k = k0 - Kz + r;
+        const bool live = (r < rows) && k >= klo && k <= d.n3m;
+        const double *brow = B + rr * sh.ypitch + (1 - j0);  // brow[i]: line index i
+        const int s = j0 - 1 + sg * kWSeg;
+        double x[kWSeg];
+        seg_bwd<kWSeg>([&](int i) { return brow[i]; }, s, ny, Ky, sy.e, sy.g, x);
+        if (r < rows) {
+#pragma unroll
+            for (int t = 0; t < kWSeg; ++t) A[r * kWTj + sg * kWSeg + t] = live ? x[t] : 0.0;
+        }
+    }
+    __syncthreads();
+
+    // 4. forward z recurrences: lanes = columns, warps = segments of rows;
+    //    B[c * kWTj + lane] = z partial at row k0 + c, c < nzf * kWSeg
+    const int j = j0 + lane;
+    const bool jlive = (j >= jlo && j <= d.n2m);
+    const int jj = min(max(j, 1), d.n2m);
+    double bs, bn;
+    if (fld == 0) {
+        bs = d.dqb2s[jj] * sd.ugkks;
+        bn = d.dqb2n[jj] * sd.ugkkn;
+    } else {
+        bs = d.dqb3s[jj];
+        bn = d.dqb3n[jj];
+    }
+    const double *acol = A + lane;
+    const int roff = Kz - k0 + 1;  // row of line index i: i + roff
+    auto Fz = [&](int i) {
+        const int k = i + 1;
+        const double v = acol[min(i + roff, rows - 1) * kWTj] * __ldg(bz + k);
+        if (fld == 0) {
+            double f = v;
+            if (k == 1) f = f + bs;
+            if (k == nz) f = f + bn;
+            return f;
+        }
+        return (k == 1) ? bs : ((k == nz) ? bn : v);
+    };
+    for (int sg = w; sg < sh.nzf; sg += kWarps) {
+        const int s = k0 - 1 + sg * kWSeg;
+        double y[kWSeg];
+        seg_fwd<kWSeg>(Fz, s, nz, Kz, sz.a, y);
+#pragma unroll
+        for (int t = 0; t < kWSeg; ++t) B[(sg * kWSeg + t) * kWTj + lane] = y[t];
+    }
+    __syncthreads();
+
+    // 5. backward z recurrences over the tile's rows; q += result
+    const double *bcol = B + lane + (1 - k0) * kWTj;  // bcol[i * kWTj]: line index i
+    for (int sg = w; sg < kWTk / kWSeg; sg += kWarps) {
+        const int s = k0 - 1 + sg * kWSeg;
+        if (s >= d.n3m) continue;
+        double x[kWSeg];
+        seg_bwd<kWSeg>([&](int i) { return bcol[i * kWTj]; }, s, nz, Kz, sz.e, sz.g, x);
+        if (jlive) {
+#pragma unroll
+            for (int t = 0; t < kWSeg; ++t) {
+                const int k = s + 1 + t;
+                if (k <= d.n3m) {
+                    double *p = q + fidx(d, j, k);
+                    *p = __ldcg(p) + x[t];
+                }
+            }
+        }
+    }
+    if (fld == 1 && jlive && w == 0 && k0 <= d.n3m && k0 + kWTk > d.n3m) Fv(q, j, d.n3) = Fv(q, j, d.n3) + bn;
+    if (fld == 0 && blockIdx.x == 0) {  // helsolve.F90:35-36: wall values of v
+        for (int k = threadIdx.x; k <= d.n3; k += kWThreads) {
+            Fv(d.q2, 1, k) = 0.0;
+            Fv(d.q2, d.n2, k) = 0.0;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- dispatch
 
 namespace {
@@ -505,8 +718,17 @@ cudaError_t scan_configure() {
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
     AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
+    AL(k_helsolve_win)
 #undef AL
     return cudaSuccess;
+}
+
+void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
+    const int ntj = (d.n2m + kWTj - 1) / kWTj, ntk = (d.n3m + kWTk - 1) / kWTk;
+    const dim3 grid(ntj * ntk, 2);
+    const WinShape sh(s.win_y, s.win_z);
+    const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size) * sizeof(double);
+    k_helsolve_win<<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
 }
 
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {

@@ -11,7 +11,10 @@ constexpr int kYLines = 2;  // contiguous lines per block
 constexpr int kYWarps = 2;  // warps per contiguous line
 constexpr int kZLines = 4;  // strided lines per block (one warp each)
 
+constexpr int kWinMax = 24;  // longest truncation window of the windowed helsolve
+
 cudaError_t scan_configure();
+void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
 void launch_scan_poisson(const Dev &d, cudaStream_t st);
 

@@ -155,7 +155,9 @@ int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const d
                    const double *lmnor);
 
 /* ---- state access --------------------------------------------------------- */
-int fb_get_dims(fb_ctx *ctx, int32_t dims[8]); /* n2, n3, nlm, nsst, ... */
+/* dims: n2, n3, nlm, nsst, field pitch, Poisson pitch, pivoting flags,
+ * helsolve windows of substep 1 (y | z << 8; 0 = full line scans) */
+int fb_get_dims(fb_ctx *ctx, int32_t dims[8]);
 int fb_get_array(fb_ctx *ctx, int id, double *host, int64_t n);
 int fb_set_array(fb_ctx *ctx, int id, const double *host, int64_t n);
 int fb_get_iarray(fb_ctx *ctx, int id, int32_t *host, int64_t n);

@@ -219,3 +219,36 @@ def test_unsupported_variable_dt_is_rejected(tmp_path):
     with pytest.raises(fb.FBError) as e:
         fb.Solver(c.write(str(tmp_path / c.name)))
     assert e.value.code == fb.FB_ERR_UNSUPPORTED
+
+
+def _windows(s):
+    import ctypes
+    dims = (ctypes.c_int32 * 8)()
+    assert fb.lib().fb_get_dims(s.ctx, dims) == 0
+    return dims[7] & 0xff, dims[7] >> 8
+
+
+@pytest.mark.parametrize("maker", [cases.tiny_rectangle, cases.viv_cylinder_384x256])
+def test_windowed_helsolve_matches_line_scans(maker, tmp_path, monkeypatch):
+    """The truncated-window helsolve agrees with the full line scans to
+    round-off over several steps (both are exact LU substitutions up to the
+    2^-56 truncation of the window)."""
+    c = maker()
+    path = c.write(str(tmp_path / c.name))
+    pert = c.v_perturbation()
+    out = []
+    for mode in ("", "scan"):
+        if mode:
+            monkeypatch.setenv("FRIBOIS2D_HELSOLVE", mode)
+        s = fb.Solver(path)
+        wy, wz = _windows(s)
+        assert (wy > 0 and wz > 0) if not mode else (wy == 0 and wz == 0)
+        q2 = s.get("q2")
+        q2[1:c.n3m + 1] += pert
+        s.set("q2", q2)
+        h = s.advance(0, 5)
+        out.append((s.get("q2"), s.get("q3"), s.get("pr"), h))
+        s.close()
+    (a2, a3, ap, ah), (b2, b3, bp, bh) = out
+    assert rel(a2, b2) <= 1e-13 and rel(a3, b3) <= 1e-13 and rel(ap, bp) <= 1e-11
+    assert rel(ah[:, 1:4], bh[:, 1:4]) <= 1e-11
