@@ -28,6 +28,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s (plain FP64 fluid time step, galloping rectangle 1024x768)"
+FORMS = {"fp64": "plain FP64", "tf32x3": "3xTF32 tensor-core Poisson transforms + FP64 refinement"}
+
+
+def metric_name(args) -> str:
+    if args.poisson == "fp64" and args.config == "galloping_rectangle_1024x768":
+        return METRIC
+    return f"cell-steps/s ({FORMS[args.poisson]} fluid time step, {args.config.replace('_', ' ')})"
 UNIT = "cell-steps/s"
 
 
@@ -42,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--poisson", default="fp64", choices=sorted(FORMS),
+                    help="eigen transforms of the Poisson solve: FP64 DGEMM, or 3xTF32 on the tensor cores")
     return ap.parse_args()
 
 
@@ -173,7 +182,7 @@ def reference_arm(args, rank, world):
         return
     c = make_case(args.config)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": c.name, "cells": c.cells, "markers": c.nlm, "host": "cpu"},
@@ -207,25 +216,36 @@ def fp64_gemm_peak(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def kernel_table(fb, path, c):
+def kernel_table(fb, path, c, poisson="fp64"):
     """Average device time of every kernel of one step, timed live with CUDA
     events on the launching stream, on a scratch context."""
     s = fb.Solver(path)
+    if poisson == "tf32x3":
+        s.set_poisson(fb.POISSON_TF32X3)
     s.advance(0, 2)
     s.set_substep(1, 1)
     cells = c.cells
     B = 8.0 * cells
     n2m, n3m = c.n2m, c.n3m
     # (name, stage, launches per step, algorithmic bytes or flops per launch, bound)
+    if poisson == "fp64":
+        transform = [
+            ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+            ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
+            ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+        ]
+    else:   # two solves per substep (the second on the residual), two transforms each
+        transform = [
+            ("tf32x3 GEMM (tcgen05, 3 products)", "tf32x3_gemm", 12, 3 * 2.0 * n2m * n3m * n3m, "tensor_tf32"),
+            ("poisson_tri", "poisson_tri", 6, 3 * B, "hbm"),
+        ]
     rows = [
         ("cfl", "cfl", 1, 2 * B, "hbm"),
         ("boucdq", "boucdq", 3, 8.0 * 8 * n2m, "hbm"),
         ("nl_rhs", "nl_rhs", 3, 9 * B, "hbm"),
-        ("helsolve(4 line-solve kernels)", "helsolve", 3, 10 * B, "hbm"),
+        ("helsolve (windowed, one launch)", "helsolve", 3, 10 * B, "hbm"),
         ("divg", "divg", 3, 3 * B, "hbm"),
-        ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
-        ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
-        ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+    ] + transform + [
         ("updvp_prcalc", "updvp", 3, 7 * B, "hbm"),
         ("submean_boucqt", "pr_submean", 3, 2 * B, "hbm"),
         ("forcing(interp+spread)", "forcing", 2, 0.0, "latency"),
@@ -254,6 +274,8 @@ def device_arm(args, rank, world, local):
     c = make_case(args.config)
     path = write_deck(c, rank)
     s = fb.Solver(path, device=local)
+    if args.poisson == "tf32x3":
+        s.set_poisson(fb.POISSON_TF32X3)
     pert = c.v_perturbation()
     q2 = s.get("q2")
     q2[1:c.n3m + 1] += pert
@@ -316,7 +338,7 @@ def device_arm(args, rank, world, local):
 
     result = None
     if rank == 0:
-        table = kernel_table(fb, path, c)
+        table = kernel_table(fb, path, c, args.poisson)
         peak_fp64 = fp64_gemm_peak(torch, dev)
         peaks = {}
         try:
@@ -329,7 +351,8 @@ def device_arm(args, rank, world, local):
         step_ms = dev_ms_max / K
         for r in table:
             r["share"] = r["ms"] * r["per_step"] / step_ms
-        dom = max((r for r in table if r["bound"] in ("hbm", "tensor")), key=lambda r: r["ms"] * r["per_step"])
+        dom = max((r for r in table if r["bound"] in ("hbm", "tensor", "tensor_tf32")),
+                  key=lambda r: r["ms"] * r["per_step"])
         traffic = None
         try:
             with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
@@ -343,6 +366,16 @@ def device_arm(args, rank, world, local):
                     "unit": "TFLOP/s", "frac": achieved / peak_fp64, "traffic": traffic,
                     "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
                     "work_per_launch": f"2*n2m*n3m^2 = {dom['work']:.4g} flop"}
+        elif dom["bound"] == "tensor_tf32":
+            # dense TF32 runs at half the bf16 rate on these tensor cores; the
+            # measured bf16 burst figure halved is the denominator
+            peak_tf32 = float(peaks.get("bf16_tflops", 1590.0)) / 2.0
+            achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e12
+            roof = {"kernel": dom["kernel"], "bound": "tensor", "achieved": achieved, "peak": peak_tf32,
+                    "unit": "TFLOP/s", "frac": achieved / peak_tf32, "traffic": traffic,
+                    "peak_source": ("of measured: MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32 rate)"
+                                    if "bf16_tflops" in peaks else "of fallback 1.59 PFLOP/s bf16 / 2"),
+                    "work_per_launch": f"3 products x 2*n2m*n3m^2 = {dom['work']:.4g} flop"}
         else:
             achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e9
             roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
@@ -353,10 +386,10 @@ def device_arm(args, rank, world, local):
             cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{steps} full time steps of {c.name} on the oracle ({secs:.1f} s)"}
         result = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": c.name, "cells": c.cells, "markers": c.nlm, "dt": c.params.dt,
+            "dtype": "f64" if args.poisson == "fp64" else "f64 (Poisson transforms: 3xtf32)", "data": "synthetic",
+            "config": {"workload": c.name, "poisson": args.poisson, "cells": c.cells, "markers": c.nlm, "dt": c.params.dt,
                        "parallelism": f"replicas x{world}" if world > 1 else "single case",
                        "l2": "flushed (256 MB write) between timed steps"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,

@@ -27,9 +27,10 @@ LIB_PATH = os.path.join(HERE, "libfribois2d.so")
 FB_OK = 0
 STATUS = {0: "FB_OK", 1: "FB_ERR_CFL", 2: "FB_ERR_MLS", 3: "FB_ERR_MARKER_OUT",
           4: "FB_ERR_INPUT", 5: "FB_ERR_CUDA", 6: "FB_ERR_STATE", 7: "FB_ERR_UNSUPPORTED",
-          8: "FB_ERR_NUMERIC"}
+          8: "FB_ERR_NUMERIC", 9: "FB_ERR_TIMEOUT"}
 FB_ERR_CFL, FB_ERR_MLS, FB_ERR_MARKER_OUT, FB_ERR_INPUT = 1, 2, 3, 4
-FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC = 5, 6, 7, 8
+FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC, FB_ERR_TIMEOUT = 5, 6, 7, 8, 9
+POISSON_FP64, POISSON_TF32X3 = 0, 1
 
 # array ids (include/fribois2d.h)
 IDS = dict(q2=0, q3=1, pr=2, dph=3, rhs2=7, rhs3=8, ru2=9, ru3=10, qb2s=20, qb2n=21, dqb2s=22,
@@ -43,10 +44,11 @@ FIELDS = ("q2", "q3", "pr", "dph", "rhs2", "rhs3", "ru2", "ru3")
 BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", "dq2x2o", "dq3x2o")
 STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
               phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17,
-              gemm_fwd=100, poisson_tri=101, gemm_bwd=102)
-HIST_COLS = 21
+              gemm_fwd=100, poisson_tri=101, gemm_bwd=102, tf32x3_gemm=103)
+HIST_COLS = 30
 HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
-              "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm")
+              "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm", "dt",
+              "cflm_end", "dmax", "ektot", "vorti", "vmax2", "vmax3", "vmin2", "vmin3")
 SCALAR_NAMES = ("time", "dt", "dt_o", "beta", "al", "ga", "ro", "cflm", "q3avg", "nbcv", "nbcw",
                 "ddmin", "pravg")
 
@@ -100,6 +102,12 @@ def lib() -> ctypes.CDLL:
         "fb_host_dims": ([vp, ip], ctypes.c_int),
         "fb_host_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
         "fb_eigen_tridiag": ([ctypes.c_int, dp, dp, dp, dp, dp, dp], ctypes.c_int),
+        "fb_set_poisson": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_set_report": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_last_history": ([vp, dp], ctypes.c_int),
+        "fb_write_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "fb_read_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "fb_gemm_tf32x3": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp], ctypes.c_int),
         "fb_status_string": ([ctypes.c_int], ctypes.c_char_p),
         "fb_version": ([], ctypes.c_char_p),
     }
@@ -150,6 +158,19 @@ class HostSetup:
         if name in ("zmm", "zmmt"):
             return out.reshape(self.n3m, self.n3m, order="F")
         return out
+
+
+def gemm_tf32x3(A: np.ndarray, B: np.ndarray, device: int = 0) -> np.ndarray:
+    """C = A @ B.T on the tensor cores in split precision (3xTF32)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    M, K = A.shape
+    N, K2 = B.shape
+    if K2 != K:
+        raise ValueError("inner dimensions differ")
+    C = np.zeros((M, N), dtype=np.float64, order="F")
+    _check(lib().fb_gemm_tf32x3(int(device), M, N, K, _dp(A), _dp(B), _dp(C)), "fb_gemm_tf32x3")
+    return C
 
 
 def eigen_tridiag(am: np.ndarray, ac: np.ndarray, ap: np.ndarray):
@@ -288,6 +309,27 @@ class Solver:
     def scalars(self) -> dict:
         s = self.get("scalars")
         return {k: float(s[i]) for i, k in enumerate(SCALAR_NAMES)}
+
+    def set_poisson(self, mode: int) -> None:
+        """POISSON_FP64 (the reference's FP64 transforms) or POISSON_TF32X3
+        (3xTF32 tensor-core transforms plus one FP64 refinement sweep)."""
+        _check(self._lib.fb_set_poisson(self.ctx, int(mode)), "fb_set_poisson")
+
+    def set_report(self, on: bool = True) -> None:
+        """End-of-step diagnostics of ttime.F90 into history columns 22..29."""
+        _check(self._lib.fb_set_report(self.ctx, int(bool(on))), "fb_set_report")
+
+    def last_history(self) -> np.ndarray:
+        row = np.zeros(HIST_COLS)
+        _check(self._lib.fb_last_history(self.ctx, _dp(row)), "fb_last_history")
+        return row
+
+    def write_restart(self, folder: str) -> None:
+        os.makedirs(folder, exist_ok=True)
+        _check(self._lib.fb_write_restart(self.ctx, folder.encode()), "fb_write_restart")
+
+    def read_restart(self, folder: str) -> None:
+        _check(self._lib.fb_read_restart(self.ctx, folder.encode()), "fb_read_restart")
 
     def synchronize(self) -> None:
         _check(self._lib.fb_synchronize(self.ctx), "fb_synchronize")

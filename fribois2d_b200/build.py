@@ -26,6 +26,7 @@ UNITS = [
     ("host.cpp", ["-fmad=false"]),
     ("kernels.cu", ["-fmad=false"]),
     ("tri.cu", []),
+    ("tc_gemm.cu", []),
     ("api.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]

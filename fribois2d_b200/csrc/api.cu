@@ -17,6 +17,7 @@
 #include "device.cuh"
 #include "host.h"
 #include "kernels.h"
+#include "tc_gemm.h"
 #include "tri.h"
 
 using fb::Dev;
@@ -46,6 +47,24 @@ struct fb_ctx {
     double *zmm = nullptr, *zmmt = nullptr;  // Poisson eigenvectors and inverse
     int null_mode = -1;
     bool allow_win = true;    // windowed helsolve allowed (FRIBOIS2D_HELSOLVE=scan turns it off)
+    bool report = false;      // end-of-step diagnostics (ttime.F90) into the history rows
+    // substep coefficients (Helmholtz factors, row normalisers) of all
+    // substeps in one device block, rebuilt for every step when dt varies:
+    // host image, pinned staging copy, device copy, pointer fix-ups
+    std::vector<double> coef_h;
+    std::vector<int> coef_hi;
+    double *coef_d = nullptr, *coef_pin = nullptr;
+    int *coef_di = nullptr, *coef_pini = nullptr;
+    std::vector<std::pair<const double **, size_t>> coef_fix;
+    std::vector<std::pair<const int **, size_t>> coef_fixi;
+    size_t coef_cap = 0, coef_capi = 0;
+    bool vardt = false;       // idtv = .false.: dt from the CFL number every step
+    // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
+    // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
+    int poisson_mode = FB_POISSON_FP64;
+    fb::SplitPlane pl_a{}, pl_a2{}, pl_zt{}, pl_z{};
+    fb::Tf32x3Plan plan_fwd{}, plan_bwd{};
+    double *pw = nullptr;
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
     int step_kernels = 0;     // own kernels per captured step
     // host copies of the scalar state the reference keeps in modules
@@ -115,7 +134,20 @@ int window_len(const std::vector<double> &c, int kmax) {
     return kmax + 1;
 }
 
-// tridiagonal system (lower(2:n), diag, upper(1:n-1)) -> device factors
+// appends v to the coefficient image; *slot points at it once uploaded
+void put(fb_ctx *c, const double **slot, const std::vector<double> &v) {
+    c->coef_fix.emplace_back(slot, c->coef_h.size());
+    c->coef_h.insert(c->coef_h.end(), v.begin(), v.end());
+    c->coef_h.resize((c->coef_h.size() + 31) / 32 * 32, 0.0);  // 256-byte aligned arrays
+}
+
+void put(fb_ctx *c, const int **slot, const std::vector<int> &v) {
+    c->coef_fixi.emplace_back(slot, c->coef_hi.size());
+    c->coef_hi.insert(c->coef_hi.end(), v.begin(), v.end());
+    c->coef_hi.resize((c->coef_hi.size() + 63) / 64 * 64, 0);
+}
+
+// tridiagonal system (lower(2:n), diag, upper(1:n-1)) -> factors in the image
 int upload_tri(fb_ctx *c, TriDev &t, fb::ScanSys &sc, const std::vector<double> &lo,
                const std::vector<double> &di, const std::vector<double> &up, int *win = nullptr) {
     fb::TriLU f = fb::factor(lo, di, up);
@@ -129,30 +161,17 @@ int upload_tri(fb_ctx *c, TriDev &t, fb::ScanSys &sc, const std::vector<double> 
         for (int i = 0; i + 1 < n; ++i)
             e[static_cast<size_t>(i)] = -f.du[static_cast<size_t>(i)] * dinv[static_cast<size_t>(i)];
         if (win) *win = std::max(window_len(a, fb::kWinMax), window_len(e, fb::kWinMax));
-        double *q;
-        int st2;
-        if ((st2 = dup(c, &q, a))) return st2;
-        sc.a = q;
-        if ((st2 = dup(c, &q, e))) return st2;
-        sc.e = q;
-        if ((st2 = dup(c, &q, dinv))) return st2;
-        sc.g = q;
+        put(c, &sc.a, a);
+        put(c, &sc.e, e);
+        put(c, &sc.g, dinv);
     }
     t.n = f.n;
     t.pivoted = f.pivoted ? 1 : 0;
-    double *p;
-    int *ip;
-    int st;
-    if ((st = dup(c, &p, f.dl))) return st;
-    t.dl = p;
-    if ((st = dup(c, &p, dinv))) return st;
-    t.dinv = p;
-    if ((st = dup(c, &p, f.du))) return st;
-    t.du = p;
-    if ((st = dup(c, &p, f.du2))) return st;
-    t.du2 = p;
-    if ((st = dup(c, &ip, f.ipiv))) return st;
-    t.ipiv = ip;
+    put(c, &t.dl, f.dl);
+    put(c, &t.dinv, dinv);
+    put(c, &t.du, f.du);
+    put(c, &t.du2, f.du2);
+    put(c, &t.ipiv, f.ipiv);
     return FB_OK;
 }
 
@@ -168,7 +187,6 @@ int build_substep(fb_ctx *c, int n, double al) {
     const double betadx = s.betadx;
     std::vector<double> b(static_cast<size_t>(std::max(n2, n3)) + 2, 0.0);
     int st;
-    double *p;
     int wy2 = 0, wz2 = 0, wy3 = 0, wz3 = 0;
     {   // solq2j (solve_fluid.F90:126-153)
         std::vector<double> am(n2 + 1, 0.0), ap(n2 + 1, 0.0), lo, di(n2, 1.0), up;
@@ -182,8 +200,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         for (int j = 2; j <= n2; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2 - 1; ++j) up.push_back(ap[j]);
         if ((st = upload_tri(c, s.y2, s.sy2, lo, di, up, &wy2))) return st;
-        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
-        s.by2 = p;
+        put(c, &s.by2, std::vector<double>(b.begin(), b.begin() + n2 + 2));
     }
     {   // solq2k (solve_fluid.F90:185-212)
         std::vector<double> am(n3m + 1, 0.0), ap(n3m + 1, 0.0), lo, di(n3m, 1.0), up;
@@ -197,8 +214,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         for (int k = 2; k <= n3m; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3m - 1; ++k) up.push_back(ap[k]);
         if ((st = upload_tri(c, s.z2, s.sz2, lo, di, up, &wz2))) return st;
-        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
-        s.bz2 = p;
+        put(c, &s.bz2, std::vector<double>(b.begin(), b.begin() + n3 + 2));
         s.ugkks = 1.0 / (g.g3rm[1] * g.g3rc[1]) * g.dx3q * 2.0 * betadx;
         s.ugkkn = 1.0 / (g.g3rm[n3m] * g.g3rc[n3]) * g.dx3q * 2.0 * betadx;
     }
@@ -214,8 +230,7 @@ int build_substep(fb_ctx *c, int n, double al) {
         for (int j = 2; j <= n2m; ++j) lo.push_back(am[j]);
         for (int j = 1; j <= n2m - 1; ++j) up.push_back(ap[j]);
         if ((st = upload_tri(c, s.y3, s.sy3, lo, di, up, &wy3))) return st;
-        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n2 + 2)))) return st;
-        s.by3 = p;
+        put(c, &s.by3, std::vector<double>(b.begin(), b.begin() + n2 + 2));
     }
     {   // solq3k (solve_fluid.F90:260-288)
         std::vector<double> am(n3 + 1, 0.0), ap(n3 + 1, 0.0), lo, di(n3, 1.0), up;
@@ -229,14 +244,46 @@ int build_substep(fb_ctx *c, int n, double al) {
         for (int k = 2; k <= n3; ++k) lo.push_back(am[k]);
         for (int k = 1; k <= n3 - 1; ++k) up.push_back(ap[k]);
         if ((st = upload_tri(c, s.z3, s.sz3, lo, di, up, &wz3))) return st;
-        if ((st = dup(c, &p, std::vector<double>(b.begin(), b.begin() + n3 + 2)))) return st;
-        s.bz3 = p;
+        put(c, &s.bz3, std::vector<double>(b.begin(), b.begin() + n3 + 2));
     }
     c->usdtal[n] = 1.0 / (c->dt * al);
     s.scan_ok = !(s.y2.pivoted || s.z2.pivoted || s.y3.pivoted || s.z3.pivoted);
     s.win_y = std::max(wy2, wy3);
     s.win_z = std::max(wz2, wz3);
     if (!s.scan_ok || !c->allow_win || s.win_y > fb::kWinMax || s.win_z > fb::kWinMax) s.win_y = s.win_z = 0;
+    return FB_OK;
+}
+
+// (Re)builds the coefficients of every substep for the current dt and
+// uploads them: allocated on the first call, then refreshed in place with one
+// asynchronous copy on the context stream (ordered before the next kernels).
+int build_substeps(fb_ctx *c) {
+    c->coef_h.clear();
+    c->coef_hi.clear();
+    c->coef_fix.clear();
+    c->coef_fixi.clear();
+    const int nsst = c->hc.deck.nsst;
+    int st;
+    for (int n = 0; n < nsst; ++n) {
+        const double al = (nsst == 3) ? c->hc.alm[n] : 1.0;
+        if ((st = build_substep(c, n, al))) return st;
+    }
+    const size_t nd = c->coef_h.size(), ni = std::max<size_t>(c->coef_hi.size(), 1);
+    if (!c->coef_d) {
+        if ((st = dnew(c, &c->coef_d, nd))) return st;
+        if ((st = dnew(c, &c->coef_di, ni))) return st;
+        CK(cudaMallocHost(&c->coef_pin, nd * sizeof(double)));
+        CK(cudaMallocHost(&c->coef_pini, ni * sizeof(int)));
+        c->coef_cap = nd;
+        c->coef_capi = ni;
+    }
+    if (nd != c->coef_cap || ni != c->coef_capi) return FB_ERR_STATE;  // sizes never change with dt
+    for (auto &f : c->coef_fix) *f.first = c->coef_d + f.second;
+    for (auto &f : c->coef_fixi) *f.first = c->coef_di + f.second;
+    std::memcpy(c->coef_pin, c->coef_h.data(), nd * sizeof(double));
+    if (!c->coef_hi.empty()) std::memcpy(c->coef_pini, c->coef_hi.data(), c->coef_hi.size() * sizeof(int));
+    CK(cudaMemcpyAsync(c->coef_d, c->coef_pin, nd * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->coef_di, c->coef_pini, ni * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     return FB_OK;
 }
 
@@ -299,10 +346,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     }
     const fb::Deck &dk = c->hc.deck;
     const fb::Grid &g = c->hc.grid;
-    if (!dk.idtv) {
-        std::fprintf(stderr, "fribois2d: variable time step (idtv = .false.) is not supported on the device path\n");
-        return FB_ERR_UNSUPPORTED;
-    }
+    c->vardt = !dk.idtv;
     if (g.n3 > 4096 || g.n2 > 2080) {
         std::fprintf(stderr, "fribois2d: grid larger than the line solvers support (n3 <= 4096, n2 <= 2080)\n");
         return FB_ERR_UNSUPPORTED;
@@ -335,6 +379,14 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     d.P = round_up(g.n2, 32);
     d.NK = g.n3 + 1;
     d.ldh = round_up(g.n2m, 32);
+    d.vardt = c->vardt ? 1 : 0;
+    {   // getintvort (utils_proc.F90:605-609): the zz node nearest z = 18.5; the
+        // line needs row indz + 1, so a domain without it has no vorticity line
+        int best = 1;
+        for (int k = 2; k <= g.n3; ++k)
+            if (std::fabs(g.zz[k] - 18.5) < std::fabs(g.zz[best] - 18.5)) best = k;
+        d.indz = (best < g.n3) ? best : 0;
+    }
     d.nlm = dk.ibact ? dk.nlm : 0;
     d.nsst = dk.nsst;
     d.wfun = dk.wfun;
@@ -452,10 +504,8 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     for (int i = 0; i < 9; ++i) d.kinori[i] = c->hc.kinori[i];
     d.rtcoup = dk.rtcoup ? 1 : 0;
 
-    for (int n = 0; n < dk.nsst; ++n) {
-        double al = (dk.nsst == 3) ? c->hc.alm[n] : 1.0;
-        if ((st = build_substep(c, n, al))) return st;
-    }
+    if ((st = build_substeps(c))) return st;
+    CK(cudaStreamSynchronize(c->stream));
     c->beta = c->dt / g.ren * 0.5;
     if ((st = build_poisson(c))) return st;
     if ((st = dup(c, &c->zmm, c->hc.zmm))) return st;
@@ -502,6 +552,57 @@ int gemm_bwd(fb_ctx *c) {   // phcalc_outflow.F90:61,65-69, dph = vmn * zmm^T
     return FB_OK;
 }
 
+// phcalc in the precision form: phi = Z T^-1 Z^-1 dph with 3xTF32 tensor-core
+// transforms (TF32 high/low splits, FP32 accumulation) and FP64 tridiagonal
+// solves, then one FP64 refinement sweep on the Poisson residual:
+// r = dph - L phi, dph <- phi + Z T^-1 Z^-1 r.
+int phcalc_tf32(fb_ctx *c) {
+    const Dev &d = c->d;
+    cudaStream_t st = c->stream;
+    fb::launch_split_t(d.dph + d.P, d.P, d.n2m, d.n3m, c->pl_a, st);
+    fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
+    fb::launch_scan_poisson(d, st);
+    fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
+    fb::launch_tf32x3(c->plan_bwd, c->pw + d.P, d.P, nullptr, 0, d.status, st);
+    fb::launch_poisson_residual(d, c->pw, c->pl_a, st);
+    fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
+    fb::launch_scan_poisson(d, st);
+    fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
+    fb::launch_tf32x3(c->plan_bwd, d.dph + d.P, d.P, c->pw + d.P, d.P, d.status, st);
+    c->own_launches += 9;
+    return FB_OK;
+}
+
+// allocates the precision-form buffers and splits the eigenvector matrices
+int setup_tf32(fb_ctx *c) {
+    if (c->pw) return FB_OK;
+    const Dev &d = c->d;
+    const long ld = round_up(d.n3m, 32);
+    auto plane = [&](fb::SplitPlane &pl, int rows) -> int {
+        int st;
+        if ((st = dnew(c, &pl.hi, static_cast<size_t>(rows) * ld))) return st;
+        if ((st = dnew(c, &pl.lo, static_cast<size_t>(rows) * ld))) return st;
+        pl.ld = ld;
+        return FB_OK;
+    };
+    int st;
+    if ((st = fb::tf32x3_configure())) return st;
+    if ((st = plane(c->pl_a, d.n2m)) || (st = plane(c->pl_a2, d.n2m)) || (st = plane(c->pl_zt, d.n3m)) ||
+        (st = plane(c->pl_z, d.n3m)))
+        return st;
+    double *pw = nullptr;
+    if ((st = dnew(c, &pw, static_cast<size_t>(d.NK) * d.P))) return st;
+    // B of the forward transform: zmmt(m, k) as [m][k]; of the backward one: zmm(k, m) as [k][m]
+    fb::launch_split_t(c->zmmt, d.n3m, d.n3m, d.n3m, c->pl_zt, c->stream);
+    fb::launch_split_t(c->zmm, d.n3m, d.n3m, d.n3m, c->pl_z, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    if ((st = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m))) return st;
+    if ((st = fb::tf32x3_plan(c->plan_bwd, c->pl_a2, c->pl_z, d.n2m, d.n3m, d.n3m))) return st;
+    c->pw = pw;
+    return FB_OK;
+}
+
 int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     double al, ga, ro;
     coefs(c, ns, n, al, ga, ro);
@@ -541,6 +642,10 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         break;
     case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
     case FB_ST_PHCALC:
+        if (c->poisson_mode == FB_POISSON_TF32X3) {
+            if ((r = phcalc_tf32(c))) return r;
+            break;
+        }
         if ((r = gemm_fwd(c))) return r;
         fb::launch_scan_poisson(d, st);
         if ((r = gemm_bwd(c))) return r;
@@ -553,6 +658,10 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_TK_GEMM_FWD: return gemm_fwd(c);
     case FB_TK_POISSON_TRI: fb::launch_scan_poisson(d, st); break;
     case FB_TK_GEMM_BWD: return gemm_bwd(c);
+    case FB_TK_TF32X3_GEMM:
+        if (!c->pw) return FB_ERR_STATE;
+        fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
+        break;
     default: return FB_ERR_STATE;
     }
     if (cudaGetLastError() != cudaSuccess) return FB_ERR_CUDA;
@@ -560,9 +669,33 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
 }
 
 // fluid_tsch.F90:30-182 enqueued on the context stream (no host sync)
+// variable dt (fluid_tsch.F90:34-48): the CFL number of the current field
+// sets dt = cflmax / cflm (at most dtmax) from the second step on; the
+// substep coefficients are rebuilt for it.  Runs cfl and waits for it.
+int vardt_update(fb_ctx *c, int ns) {
+    int r;
+    if ((r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
+    double am = 0.0;
+    CK(cudaMemcpyAsync(&am, c->d.scal + fb::S_CFLRAW, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double dt = c->dt;
+    if (ns > 0) {
+        dt = c->hc.deck.cflmax / am;
+        if (dt > c->hc.deck.dtmax) dt = c->hc.deck.dtmax;
+    }
+    if (!(dt >= 1.0e-8)) return FB_ERR_CFL;
+    if (dt != c->dt) {
+        c->dt = dt;
+        c->d.dt = dt;
+        if ((r = build_substeps(c))) return r;
+    }
+    return FB_OK;
+}
+
 int enqueue_fluid(fb_ctx *c, int ns) {
     const Dev &d = c->d;
     int r;
+    if (c->vardt && (r = vardt_update(c, ns))) return r;
     // The marker set-up of substep 1 (lgrdistribution, MLS weights) reads
     // only marker data: it runs on a side branch while cfl, boucdq and the
     // explicit terms run on the main stream.
@@ -576,7 +709,7 @@ int enqueue_fluid(fb_ctx *c, int ns) {
         CK(cudaGetLastError());
         CK(cudaEventRecord(c->ev_join, c->side));
     }
-    if ((r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
+    if (!c->vardt && (r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
     c->beta = c->dt / c->hc.grid.ren * 0.5;
     for (int n = 1; n <= d.nsst; ++n) {
         if ((r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
@@ -596,11 +729,28 @@ int enqueue_fluid(fb_ctx *c, int ns) {
     return FB_OK;
 }
 
+int enqueue_report(fb_ctx *c) {
+    if (!c->report || !c->d.nlm) return FB_OK;
+    fb::launch_diag(c->d, c->hist_cap, c->stream);
+    c->own_launches += 1;
+    return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+}
+
 int enqueue_step(fb_ctx *c, int ns) {
     int r = enqueue_fluid(c, ns);
     if (r) return r;
-    if (c->d.nlm) return stage_impl(c, FB_ST_RIGID, ns, 1);
+    if (c->d.nlm) {
+        if ((r = stage_impl(c, FB_ST_RIGID, ns, 1))) return r;
+        return enqueue_report(c);
+    }
     return FB_OK;
+}
+
+void drop_graph(fb_ctx *c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
 }
 
 int read_status(fb_ctx *c, int *status) {
@@ -720,6 +870,7 @@ const char *fb_status_string(int status) {
     case FB_ERR_STATE: return "invalid argument for this context";
     case FB_ERR_UNSUPPORTED: return "deck option not supported on the device path";
     case FB_ERR_NUMERIC: return "singular set-up system or non-finite value";
+    case FB_ERR_TIMEOUT: return "a device-side wait gave up";
     }
     return "unknown status";
 }
@@ -745,6 +896,8 @@ int fb_destroy(fb_ctx *c) {
     if (c->graph) cudaGraphDestroy(c->graph);
     for (void *p : c->allocs)
         if (p) cudaFree(p);
+    if (c->coef_pin) cudaFreeHost(c->coef_pin);
+    if (c->coef_pini) cudaFreeHost(c->coef_pini);
     if (c->blas) cublasDestroy(c->blas);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -769,6 +922,7 @@ int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
     if (!c) return FB_ERR_STATE;
     int r = stage_impl(c, FB_ST_RIGID, ns, 1);
     if (r) return r;
+    if ((r = enqueue_report(c))) return r;
     if (forcecomp) CK(cudaMemcpyAsync(forcecomp, c->d.forces, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     int status = 0;
     if ((r = read_status(c, &status))) return r;
@@ -776,10 +930,28 @@ int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
     return status;
 }
 
+int fb_last_history(fb_ctx *c, double *row);
+
 int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
     if (!c || nsteps < 0) return FB_ERR_STATE;
     if (!c->d.nlm) return FB_ERR_UNSUPPORTED;
     int r, status = 0, done = 0;
+    if (c->vardt) {   // dt changes every step: eager launches, no captured graph
+        c->last_ms = 0.0;
+        for (; done < nsteps; ++done) {
+            CK(cudaEventRecord(c->ev0, c->stream));
+            if ((r = enqueue_step(c, ns0 + done))) return r;
+            CK(cudaEventRecord(c->ev1, c->stream));
+            if ((r = read_status(c, &status))) return r;
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            c->last_ms += ms;
+            if (hist && (r = fb_last_history(c, hist + static_cast<size_t>(done) * FB_HIST_COLS))) return r;
+            host_clock(c, 1);
+            if (status) return status;
+        }
+        return FB_OK;
+    }
     // the first Adams-Bashforth step has its own coefficients: run it eagerly
     if (c->hc.deck.nsst == 1 && ns0 == 0 && nsteps > 0) {
         CK(cudaEventRecord(c->ev0, c->stream));
@@ -826,6 +998,154 @@ int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
         done += chunk;
         if (status) return status;
     }
+    return FB_OK;
+}
+
+int fb_last_history(fb_ctx *c, double *row) {
+    if (!c || !row || !c->d.nlm) return FB_ERR_STATE;
+    double step = 0.0;
+    CK(cudaMemcpyAsync(&step, c->d.scal + fb::S_STEP, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (step < 1.0) return FB_ERR_STATE;
+    const int r = (static_cast<int>(step) - 1) % c->hist_cap;
+    CK(cudaMemcpy(row, c->d.hist + static_cast<size_t>(r) * FB_HIST_COLS, FB_HIST_COLS * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    return FB_OK;
+}
+
+// ---- checkpoint / restart: raw little-endian FP64 files in place of the
+// reference's HDF5 restart set (mpi_routines.F90:532-806 rest_*.h5,
+// iobcs.F90:114-205 outflow.h5 / inflow.h5) and its text master_rigid.dat
+// (ttime.F90:117-124).  Each .bin file holds a 32-byte header (magic, format
+// version, n2, n3, nlm, count) followed by `count` doubles.
+namespace {
+
+struct RestartHeader {
+    char magic[8];
+    int32_t version, n2, n3, nlm;
+    int64_t count;
+};
+
+int write_blob(fb_ctx *c, const std::string &path, const std::vector<double> &v) {
+    RestartHeader h{};
+    std::memcpy(h.magic, "FBRST01", 8);
+    h.version = 1;
+    h.n2 = c->d.n2;
+    h.n3 = c->d.n3;
+    h.nlm = c->d.nlm;
+    h.count = static_cast<int64_t>(v.size());
+    std::FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return FB_ERR_INPUT;
+    const bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 &&
+                    std::fwrite(v.data(), sizeof(double), v.size(), f) == v.size();
+    return (std::fclose(f) == 0 && ok) ? FB_OK : FB_ERR_INPUT;
+}
+
+int read_blob(fb_ctx *c, const std::string &path, std::vector<double> &v) {
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return FB_ERR_INPUT;
+    RestartHeader h{};
+    bool ok = std::fread(&h, sizeof(h), 1, f) == 1 && std::memcmp(h.magic, "FBRST01", 8) == 0 && h.version == 1 &&
+              h.n2 == c->d.n2 && h.n3 == c->d.n3 && h.nlm == c->d.nlm && h.count >= 0 && h.count < (1LL << 34);
+    if (ok) {
+        v.resize(static_cast<size_t>(h.count));
+        ok = std::fread(v.data(), sizeof(double), v.size(), f) == v.size();
+    }
+    std::fclose(f);
+    return ok ? FB_OK : FB_ERR_INPUT;
+}
+
+// arrays of one restart file, in order
+struct RestartFile {
+    const char *name;
+    std::vector<int> ids;
+};
+
+const std::vector<RestartFile> &restart_files() {
+    static const std::vector<RestartFile> files = {
+        {"rest_q2.bin", {FB_Q2}},
+        {"rest_q3.bin", {FB_Q3}},
+        {"rest_pr.bin", {FB_PR}},
+        {"rest_ru2.bin", {FB_RU2}},
+        {"rest_ru3.bin", {FB_RU3}},
+        {"outflow.bin", {FB_QB2N, FB_QB3N, FB_DQ2X2O, FB_DQ3X2O}},
+        {"inflow.bin", {FB_QB2S, FB_QB3S}},
+        // state the reference rebuilds on restart, kept so that a restarted run
+        // continues bit for bit: boundary increments and the marker set
+        {"device_state.bin", {FB_DQB2S, FB_DQB2N, FB_DQB3S, FB_DQB3N, FB_LMCC, FB_LMVEL, FB_LMACC, FB_LMNOR,
+                              FB_VERT, FB_RIGID, FB_FORCES}},
+    };
+    return files;
+}
+
+int64_t array_len(fb_ctx *c, int id) {
+    double *p = nullptr;
+    if (field_ptr(c, id, &p) == FB_OK) return static_cast<int64_t>(c->d.NK) * c->d.n2;
+    int64_t n = 0;
+    bool ob = false;
+    return vec_ptr(c, id, &p, &n, &ob) == FB_OK ? n : -1;
+}
+
+}  // namespace
+
+int fb_write_restart(fb_ctx *c, const char *dir) {
+    if (!c || !dir) return FB_ERR_STATE;
+    const std::string root(dir);
+    int r;
+    for (const RestartFile &rf : restart_files()) {
+        std::vector<double> blob;
+        for (int id : rf.ids) {
+            const int64_t n = array_len(c, id);
+            if (n < 0) return FB_ERR_STATE;
+            std::vector<double> v(static_cast<size_t>(n));
+            if ((r = fb_get_array(c, id, v.data(), n))) return r;
+            blob.insert(blob.end(), v.begin(), v.end());
+        }
+        if ((r = write_blob(c, root + "/" + rf.name, blob))) return r;
+    }
+    {   // device scalars (clock, step counter, running sums) and host scalars
+        std::vector<double> sc(fb::S_COUNT + 2);
+        CK(cudaMemcpyAsync(sc.data(), c->d.scal, fb::S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        sc[fb::S_COUNT] = c->dt;
+        sc[fb::S_COUNT + 1] = c->dt_o;
+        if ((r = write_blob(c, root + "/scalars.bin", sc))) return r;
+        std::vector<double> rg(18);
+        if ((r = fb_get_array(c, FB_RIGID, rg.data(), 18))) return r;
+        std::FILE *f = std::fopen((root + "/master_rigid.dat").c_str(), "w");
+        if (!f) return FB_ERR_INPUT;
+        // list-directed layout: time / dt, dt_o / cmp_np1 / cmv_np1 / cma_np1
+        std::fprintf(f, " %25.17E\n %25.17E %25.17E\n", sc[fb::S_TIME], c->dt, c->dt_o);
+        for (int q = 0; q < 3; ++q)
+            std::fprintf(f, " %25.17E %25.17E %25.17E\n", rg[9 + 3 * q], rg[10 + 3 * q], rg[11 + 3 * q]);
+        if (std::fclose(f) != 0) return FB_ERR_INPUT;
+    }
+    return FB_OK;
+}
+
+int fb_read_restart(fb_ctx *c, const char *dir) {
+    if (!c || !dir) return FB_ERR_STATE;
+    const std::string root(dir);
+    int r;
+    for (const RestartFile &rf : restart_files()) {
+        std::vector<double> blob;
+        if ((r = read_blob(c, root + "/" + rf.name, blob))) return r;
+        size_t off = 0;
+        for (int id : rf.ids) {
+            const int64_t n = array_len(c, id);
+            if (n < 0 || off + static_cast<size_t>(n) > blob.size()) return FB_ERR_INPUT;
+            if ((r = fb_set_array(c, id, blob.data() + off, n))) return r;
+            off += static_cast<size_t>(n);
+        }
+        if (off != blob.size()) return FB_ERR_INPUT;
+    }
+    std::vector<double> sc;
+    if ((r = read_blob(c, root + "/scalars.bin", sc))) return r;
+    if (sc.size() != static_cast<size_t>(fb::S_COUNT + 2)) return FB_ERR_INPUT;
+    CK(cudaMemcpyAsync(c->d.scal, sc.data(), fb::S_COUNT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (sc[fb::S_COUNT] != c->dt) return FB_ERR_INPUT;  // the deck's dt must match the checkpoint's
+    c->dt_o = sc[fb::S_COUNT + 1];
     return FB_OK;
 }
 
@@ -1097,6 +1417,75 @@ int fb_host_array(fb_host *h, int id, double *out, int64_t n) {
     if (n != static_cast<int64_t>(v->size())) return FB_ERR_STATE;
     std::memcpy(out, v->data(), static_cast<size_t>(n) * sizeof(double));
     return FB_OK;
+}
+
+int fb_set_poisson(fb_ctx *c, int mode) {
+    if (!c || (mode != FB_POISSON_FP64 && mode != FB_POISSON_TF32X3)) return FB_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    if (mode == FB_POISSON_TF32X3) {
+        const int st = setup_tf32(c);
+        if (st) return st;
+    }
+    if (mode != c->poisson_mode) {   // the captured step no longer matches
+        CK(cudaStreamSynchronize(c->stream));
+        drop_graph(c);
+        c->poisson_mode = mode;
+    }
+    return FB_OK;
+}
+
+int fb_set_report(fb_ctx *c, int on) {
+    if (!c) return FB_ERR_STATE;
+    if ((on != 0) != c->report) {
+        CK(cudaStreamSynchronize(c->stream));
+        drop_graph(c);
+        c->report = (on != 0);
+    }
+    return FB_OK;
+}
+
+int fb_gemm_tf32x3(int device, int M, int N, int K, const double *A, const double *B, double *C) {
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return FB_ERR_STATE;
+    CK(cudaSetDevice(device));
+    int st = fb::tf32x3_configure();
+    if (st) return st;
+    const long ld = (K + 31) / 32 * 32;
+    std::vector<void *> mem;
+    auto alloc = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        mem.push_back(p);
+        return p;
+    };
+    double *dA = static_cast<double *>(alloc(sizeof(double) * M * K));
+    double *dB = static_cast<double *>(alloc(sizeof(double) * N * K));
+    double *dC = static_cast<double *>(alloc(sizeof(double) * M * N));
+    float *ah = static_cast<float *>(alloc(sizeof(float) * M * ld)), *al = static_cast<float *>(alloc(sizeof(float) * M * ld));
+    float *bh = static_cast<float *>(alloc(sizeof(float) * N * ld)), *bl = static_cast<float *>(alloc(sizeof(float) * N * ld));
+    int *status = static_cast<int *>(alloc(sizeof(int)));
+    st = FB_OK;
+    if (!dA || !dB || !dC || !ah || !al || !bh || !bl || !status) st = FB_ERR_CUDA;
+    fb::Tf32x3Plan plan{};
+    fb::SplitPlane pa{ah, al, ld}, pb{bh, bl, ld};
+    if (!st && (cudaMemcpy(dA, A, sizeof(double) * M * K, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(dB, B, sizeof(double) * N * K, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemset(status, 0, sizeof(int)) != cudaSuccess))
+        st = FB_ERR_CUDA;
+    if (!st) {
+        fb::launch_split_t(dA, M, M, K, pa, nullptr);  // A(m, k) at A[k * M + m] -> [m][k]
+        fb::launch_split_t(dB, N, N, K, pb, nullptr);
+        st = fb::tf32x3_plan(plan, pa, pb, M, N, K);
+    }
+    if (!st) {
+        fb::launch_tf32x3(plan, dC, M, nullptr, 0, status, nullptr);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = FB_ERR_CUDA;
+    }
+    int dev_status = 0;
+    if (!st && cudaMemcpy(&dev_status, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) st = FB_ERR_CUDA;
+    if (!st && dev_status) st = dev_status;
+    if (!st && cudaMemcpy(C, dC, sizeof(double) * M * N, cudaMemcpyDeviceToHost) != cudaSuccess) st = FB_ERR_CUDA;
+    for (void *p : mem) cudaFree(p);
+    return st;
 }
 
 int fb_eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr, double *zmm,

@@ -33,6 +33,8 @@ struct SubDev {          // substep constants (fluid_tsch.F90:64-77)
 
 struct Dev {
     int n2, n3, n2m, n3m, P, NK, nlm, nsst, wfun, ldh;
+    int indz;                // getintvort line (utils_proc.F90:607-609); 0 = none
+    int vardt;               // idtv = .false.: dt follows the CFL number (no fixed-dt check)
     double dx2, dx3, dx2q, dx3q, ren, visc, dt, cou, q3uw, q3lw, rext2, alx3;
     double radiusSD, kprobe, ddmin, area_out, cfllim;
     // grid (1-based)
@@ -75,7 +77,7 @@ struct Dev {
 
 // device scalar slots
 enum Scal {
-    S_TIME = 0, S_CFLM, S_Q3AVG, S_NBCV, S_NBCW, S_PRAVG, S_QOUT, S_DT, S_STEP, S_COUNT
+    S_TIME = 0, S_CFLM, S_Q3AVG, S_NBCV, S_NBCW, S_PRAVG, S_QOUT, S_DT, S_STEP, S_CFLRAW, S_COUNT
 };
 
 __host__ __device__ inline size_t fidx(const Dev &d, int j, int k) {

@@ -101,8 +101,11 @@ __global__ void __launch_bounds__(256) k_cfl(Dev d) {
         d.count[0] = 0u;
         const double cflm = am * d.dt;
         d.scal[S_CFLM] = cflm;
+        d.scal[S_CFLRAW] = am;
         d.scal[S_Q3AVG] = as / (d.rext2 * d.alx3);
-        if (cflm > d.cfllim || !(cflm == cflm)) raise_status(d, FB_ERR_CFL);
+        // fixed dt: the stability check of fluid_tsch.F90:49-55; variable dt
+        // is set from am on the host (fluid_tsch.F90:34-48)
+        if (!d.vardt && (cflm > d.cfllim || !(cflm == cflm))) raise_status(d, FB_ERR_CFL);
     }
 }
 
@@ -1131,8 +1134,84 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
             h[18] = d.scal[S_NBCV];
             h[19] = d.scal[S_NBCW];
             h[20] = d.scal[S_CFLM];
+            h[21] = d.dt;
+            for (int i = 22; i < FB_HIST_COLS; ++i) h[i] = 0.0;  // diagnostics, when enabled
         }
         d.scal[S_STEP] = static_cast<double>(row + 1);
+    }
+}
+
+// ------------------------------------------------------------ diagnostics
+
+// ttime.F90:24-147: diagnostics of the end-of-step field for the fluid report
+// (fluid_rep.out) -- vmaxv/vminv (vcheck.F90:4-80), cfl (cfl.F90) times dt,
+// divgck (divergence.F90:49-82), kinen (utils_proc.F90:474-515) and the line
+// vorticity of getintvort (utils_proc.F90:582-632) at row indz.  Eight block
+// reductions; the last block writes history columns 22..29 of the step.
+__global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    constexpr int kV = 8, kStride = 2048;  // partial v of block b at red[v * kStride + b]
+    const int t = threadIdx.x, nt = blockDim.x, b = blockIdx.x, nb = gridDim.x;
+    const long cells = static_cast<long>(d.n2m) * d.n3m;
+    double v[kV] = {-100.0, -100.0, -100.0, -100.0, 1.0e-8, -100.0, 0.0, 0.0};
+    for (long idx = static_cast<long>(b) * nt + t; idx < cells; idx += static_cast<long>(nb) * nt) {
+        const int j = static_cast<int>(idx % d.n2m) + 1, k = static_cast<int>(idx / d.n2m) + 1;
+        const int jp = j + 1, kp = k + 1;
+        const double q2c = Fv(d.q2, j, k), q3c = Fv(d.q3, j, k);
+        const double q2j = Fv(d.q2, jp, k), q3k = Fv(d.q3, j, kp);
+        v[0] = fmax(v[0], fabs(q2c));
+        v[1] = fmax(v[1], fabs(q3c));
+        v[2] = fmax(v[2], -q2c);
+        v[3] = fmax(v[3], -q3c);
+        v[4] = fmax(v[4], fabs((q2c + q2j) * 0.5 * d.udx2m[j]) + fabs((q3c + q3k) * 0.5 * d.udx3m[k]));
+        v[5] = fmax(v[5], fabs((q2j - q2c) * d.udx2m[j] + (q3k - q3c) * d.udx3m[k]));
+        const double vol = (d.zz[kp] - d.zz[k]) * (d.rc[jp] - d.rc[j]);
+        const double vccv = (q2c + q2j) * 0.5, vccw = (q3c + q3k) * 0.5;
+        v[6] = v[6] + (vccv * vccv + vccw * vccw) * vol;
+        if (k == d.indz) {
+            const double dz = d.zz[kp] - d.zz[k];
+            const double dwdy = (Fv(d.q3, jp, k) - q3c) / (d.rc[jp] - d.rc[j]);
+            const double dvdz = (Fv(d.q2, j, kp) - q2c) / dz;
+            v[7] = v[7] + (dwdy - dvdz) * (d.rc[jp] - d.rc[j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kV; ++i) {
+        const double r = (i < 6) ? block_reduce_fast<true>(v[i], sh) : block_reduce_fast<false>(v[i], sh);
+        if (t == 0) d.red[i * kStride + b] = r;
+    }
+    if (t == 0) {
+        __threadfence();
+        last = (atomicAdd(d.count + 3, 1u) == static_cast<unsigned>(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a[kV];
+#pragma unroll
+    for (int i = 0; i < kV; ++i) {
+        double x = (i < 6) ? -1.0e300 : 0.0;
+        for (int q = t; q < nb; q += nt) {
+            const double y = __ldcg(d.red + i * kStride + q);
+            x = (i < 6) ? fmax(x, y) : x + y;
+        }
+        a[i] = (i < 6) ? block_reduce_fast<true>(x, sh) : block_reduce_fast<false>(x, sh);
+    }
+    if (t == 0) {
+        d.count[3] = 0u;
+        if (hist_rows > 0) {
+            const int row = static_cast<int>(d.scal[S_STEP]) - 1;  // the step k_rigid closed
+            double *h = d.hist + static_cast<size_t>((row + hist_rows) % hist_rows) * FB_HIST_COLS;
+            h[22] = a[4] * d.dt;                                   // cflm at the end of the step
+            h[23] = a[5];                                          // dmax
+            h[24] = 0.5 * a[6] / (d.rext2 * d.alx3);               // ektot
+            h[25] = a[7];                                          // vorti
+            h[26] = a[0];                                          // vmax(1), vmax(2)
+            h[27] = a[1];
+            h[28] = -a[2];                                         // vmin(1), vmin(2)
+            h[29] = -a[3];
+        }
     }
 }
 
@@ -1190,6 +1269,9 @@ void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
     k_loads_probe<<<(3 * d.nlm + 63) / 64, 64, 0, s>>>(d);
     k_loads_finish<<<1, 256, 0, s>>>(d);
+}
+void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
+    k_diag<<<std::min(stride_blocks(d), 2048), 256, 0, s>>>(d, hist_rows);
 }
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s) {
     if (d.nlm) k_rigid<<<1, 256, 0, s>>>(d, hist_rows);

@@ -22,6 +22,7 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s);
 void launch_loads(const Dev &d, cudaStream_t s);
+void launch_diag(const Dev &d, int hist_rows, cudaStream_t s);
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s);
 
 }  // namespace fb

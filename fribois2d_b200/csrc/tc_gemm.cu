@@ -1,0 +1,383 @@
+// Split-precision (3xTF32) GEMM on the Blackwell tensor cores, for the
+// eigen transforms of the Poisson solve (phcalc_outflow.F90:31,61) in the
+// precision form of the time step.
+//
+//   C[M x N] = A[M x K] * B[N x K]^T,  A = Ahi + Alo, B = Bhi + Blo,
+//   C ~ Alo*Bhi + Ahi*Blo + Ahi*Bhi      (FP32 accumulation in TMEM)
+//
+// Operands are FP32 planes holding TF32-rounded high and low parts of FP64
+// values (k_split_t), K contiguous.  One CTA computes a 128 x 128 tile:
+// one thread issues TMA loads (128-byte swizzle, no multicast) into a
+// three-stage shared-memory ring, one thread issues tcgen05.mma (kind::tf32,
+// M = 128, N = 128, K = 8) into a TMEM accumulator, and the four warps read
+// the accumulator back with tcgen05.ld and store FP64 results.  Every
+// mbarrier wait gives up after one second, records FB_ERR_TIMEOUT and lets
+// the CTA finish (waiting for its own copies and MMAs, freeing its TMEM).
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/fribois2d.h"
+#include "device.cuh"
+#include "tc_gemm.h"
+
+namespace fb {
+
+namespace {
+
+constexpr int kBM = 128, kBN = 128, kBK = 32, kStages = 3, kThreads = 128;
+constexpr uint32_t kTileBytes = kBM * kBK * 4;    // 16 KB; A and B tiles alike (kBM == kBN)
+constexpr uint32_t kStageBytes = 4 * kTileBytes;  // A hi, A lo, B hi, B lo
+constexpr uint32_t kTmemCols = kBN;               // FP32 accumulator: 128 lanes x kBN columns
+constexpr size_t kSmemBytes = kStages * kStageBytes + 1024 + 256;
+// instruction descriptor: D FP32, A and B TF32, both K-major, N = kBN, M = kBM
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
+                            (static_cast<uint32_t>(kBM >> 4) << 24);
+static_assert(kBM == 128 && kBN % 16 == 0 && kBN <= 256, "tcgen05 kind::tf32 shape");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for the phase with the given parity; false after one second
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > 1000000000ull) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor: K-major operand, 128-byte swizzle atoms of
+// 8 rows x 128 bytes (stride between atoms 1024 bytes), sm100 version bits
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(1u) << 16;           // leading byte offset (16 B; unused when swizzled)
+    d |= static_cast<uint64_t>(1024u >> 4) << 32;   // stride byte offset
+    d |= static_cast<uint64_t>(1u) << 46;           // descriptor version
+    d |= static_cast<uint64_t>(2u) << 61;           // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tf32x3_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+                  const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+                  GemmOut o, int K, int *status) {
+    extern __shared__ uint8_t smraw[];
+    const uint32_t raw = smem_u32(smraw);
+    const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;  // swizzle atoms need 1024-byte alignment
+    uint8_t *sm = smraw + pad;
+    const uint32_t sbase = raw + pad;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kStages * kStageBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 1);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages), done = smem_u32(bars + 2 * kStages);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    const int nk = (K + kBK - 1) / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kStages;
+            const uint32_t ph = static_cast<uint32_t>(kb / kStages) & 1u;
+            if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                ok = false;
+                break;
+            }
+            const uint32_t st = sbase + s * kStageBytes, fb = full0 + 8 * s;
+            mbar_expect_tx(fb, kStageBytes);
+            tma_load_2d(st, &ma_hi, fb, kb * kBK, m0);
+            tma_load_2d(st + kTileBytes, &ma_lo, fb, kb * kBK, m0);
+            tma_load_2d(st + 2 * kTileBytes, &mb_hi, fb, kb * kBK, n0);
+            tma_load_2d(st + 3 * kTileBytes, &mb_lo, fb, kb * kBK, n0);
+            issued = kb + 1;
+        }
+        // every copy issued has landed before the CTA may finish
+        for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
+            if (!mbar_wait(full0 + 8 * (kb % kStages), static_cast<uint32_t>(kb / kStages) & 1u)) ok = false;
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kStages;
+            const uint32_t ph = static_cast<uint32_t>(kb / kStages) & 1u;
+            if (!mbar_wait(full0 + 8 * s, ph)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t st = sbase + s * kStageBytes;
+#pragma unroll
+            for (int k = 0; k < kBK / 8; ++k) {  // K = 8 per MMA: 32 bytes along the swizzled row
+                const uint64_t ahi = sw128_desc(st + 32 * k), alo = sw128_desc(st + kTileBytes + 32 * k);
+                const uint64_t bhi = sw128_desc(st + 2 * kTileBytes + 32 * k);
+                const uint64_t blo = sw128_desc(st + 3 * kTileBytes + 32 * k);
+                mma_tf32(tmem, alo, bhi, (kb > 0 || k > 0) ? 1u : 0u);
+                mma_tf32(tmem, ahi, blo, 1u);
+                mma_tf32(tmem, ahi, bhi, 1u);
+            }
+            mma_commit(empty0 + 8 * s);  // frees the stage once these MMAs have read it
+        }
+        mma_commit(done);  // arrives when every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // ---- epilogue: TMEM lane = tile row; warp w owns lanes 32w .. 32w+31
+    if (!mbar_wait(done, 0)) ok = false;
+    __syncwarp();
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    const bool rok = ok && row < o.M;
+#pragma unroll 1
+    for (int c = 0; c < kBN / 32; ++c) {
+        uint32_t r[32];
+        tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c * 32), r);
+        if (rok) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int col = n0 + c * 32 + i;
+                if (col < o.N) {
+                    double v = static_cast<double>(__uint_as_float(r[i]));
+                    if (o.base) v = o.base[static_cast<size_t>(col) * o.ldb + row] + v;
+                    o.out[static_cast<size_t>(col) * o.ldo + row] = v;
+                }
+            }
+        }
+    }
+    if (!ok) atomicCAS(status, 0, FB_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// dst[r * ldd + c] = (hi, lo) TF32 parts of src[c * lds + r], r < R, c < C:
+// the transposed split of a column-major FP64 matrix (32 x 32 tiles)
+__global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src, long lds, int R, int C,
+                                                  float *__restrict__ hi, float *__restrict__ lo, long ldd) {
+    __shared__ double t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int c = c0 + ty + 8 * i, r = r0 + tx;
+        t[ty + 8 * i][tx] = (r < R && c < C) ? src[static_cast<size_t>(c) * lds + r] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = r0 + ty + 8 * i, c = c0 + tx;
+        if (r < R && c < C) {
+            const double x = t[tx][ty + 8 * i];
+            const float h = tf32_round(static_cast<float>(x));
+            const float l = tf32_round(static_cast<float>(x - static_cast<double>(h)));
+            hi[static_cast<size_t>(r) * ldd + c] = h;
+            lo[static_cast<size_t>(r) * ldd + c] = l;
+        }
+    }
+}
+
+// FP64 residual of the Poisson equation that phcalc solves,
+//   r = dph - (A_yy + A_zz) phi,
+// with A_yy = tridiag(amphj, acphj, apphj) along j and A_zz = tridiag(amphk,
+// acphk, apphk) along k (the operators of phcalc_outflow.F90:36-45 and
+// phini.F90:59-65), written as the transposed TF32 split [j][k] that the
+// forward transform reads.  One 32 x 32 tile per block.
+__global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *__restrict__ phi, float *__restrict__ hi,
+                                                           float *__restrict__ lo, long ldd) {
+    __shared__ double t[32][33];
+    const int j0 = 1 + blockIdx.x * 32, k0 = 1 + blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int j = j0 + tx;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int k = k0 + ty + 8 * i;
+        double r = 0.0;
+        if (j <= d.n2m && k <= d.n3m) {
+            const double pc = phi[fidx(d, j, k)];
+            double lp = (d.acphj[j] + d.acphk[k]) * pc;
+            if (j > 1) lp = fma(d.amphj[j], phi[fidx(d, j - 1, k)], lp);
+            if (j < d.n2m) lp = fma(d.apphj[j], phi[fidx(d, j + 1, k)], lp);
+            if (k > 1) lp = fma(d.amphk[k], phi[fidx(d, j, k - 1)], lp);
+            if (k < d.n3m) lp = fma(d.apphk[k], phi[fidx(d, j, k + 1)], lp);
+            r = d.dph[fidx(d, j, k)] - lp;
+        }
+        t[ty + 8 * i][tx] = r;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int jj = j0 + ty + 8 * i, kk = k0 + tx;
+        if (jj <= d.n2m && kk <= d.n3m) {
+            const double x = t[tx][ty + 8 * i];
+            const float h = tf32_round(static_cast<float>(x));
+            const float l = tf32_round(static_cast<float>(x - static_cast<double>(h)));
+            hi[static_cast<size_t>(jj - 1) * ldd + (kk - 1)] = h;
+            lo[static_cast<size_t>(jj - 1) * ldd + (kk - 1)] = l;
+        }
+    }
+}
+
+void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st) {
+    const dim3 grid((d.n2m + 31) / 32, (d.n3m + 31) / 32);
+    k_poisson_residual<<<grid, 256, 0, st>>>(d, phi, dst.hi, dst.lo, dst.ld);
+}
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int encode_plane(CUtensorMap *m, const float *p, int rows, int K, long ld) {
+    if (!g_encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return FB_ERR_CUDA;
+        g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) || (ld % 4) || ld < K) return FB_ERR_STATE;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 4u};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(kBM)};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(p), dims, strides, box, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? FB_OK : FB_ERR_CUDA;
+}
+
+}  // namespace
+
+int tf32x3_configure() {
+    return cudaFuncSetAttribute(k_tf32x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kSmemBytes)) == cudaSuccess
+               ? FB_OK
+               : FB_ERR_CUDA;
+}
+
+int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K) {
+    int st;
+    if ((st = encode_plane(&p.a_hi, a.hi, M, K, a.ld))) return st;
+    if ((st = encode_plane(&p.a_lo, a.lo, M, K, a.ld))) return st;
+    if ((st = encode_plane(&p.b_hi, b.hi, N, K, b.ld))) return st;
+    if ((st = encode_plane(&p.b_lo, b.lo, N, K, b.ld))) return st;
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    return FB_OK;
+}
+
+void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *base, long ldb, int *status,
+                   cudaStream_t st) {
+    GemmOut o{out, ldo, base, ldb, p.M, p.N};
+    const dim3 grid((p.M + kBM - 1) / kBM, (p.N + kBN - 1) / kBN);
+    k_tf32x3_gemm<<<grid, kThreads, kSmemBytes, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+}
+
+void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st) {
+    const dim3 grid((R + 31) / 32, (C + 31) / 32);
+    k_split_t<<<grid, 256, 0, st>>>(src, lds, R, C, dst.hi, dst.lo, dst.ld);
+}
+
+}  // namespace fb

@@ -471,65 +471,72 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb
 // memory: forward and backward y recurrences over the tile's rows plus a
 // halo of K rows on either side in k, then forward and backward z
 // recurrences over its columns, adding the result to q2/q3.  rhs2/rhs3 are
-// read once and q2/q3 read and written once.
-constexpr int kWTj = 32;    // tile columns (j): one lane each in the z phases
-constexpr int kWTk = 64;    // tile rows (k)
-constexpr int kWSeg = 8;    // values per thread segment
+// read once and q2/q3 read and written once; the recurrence coefficients of
+// the tile are staged in shared memory with it.
+constexpr int kWTj = 32;        // tile columns (j): one lane each in the z phases
+constexpr int kWTk = 64;        // tile rows (k)
+constexpr int kWSeg = 16;       // values per thread segment
 constexpr int kWThreads = 256;
+constexpr int kWXp = kWTj + 1;  // row stride of the z right-hand side tile (odd: conflict-free column stores)
 
 namespace {
 
-// y(i) = a(i) y(i-1) + F(i) for i in [s, s+TS) below n, started from zero
-// at max(0, s-K)
-template <int TS, class FF>
-__device__ __forceinline__ void seg_fwd(const FF &F, int s, int n, int K, const double *__restrict__ a,
-                                        double (&y)[TS]) {
+// y(i) = a(i) y(i-1) + F(i) for the TS positions from s, started from zero K
+// positions earlier; a and F are indexed relative to the segment start
+// (a[u], F(u) for u = -K .. TS-1).  Positions at or past nmax are not set.
+template <int TS, int KM, class FA, class FF>
+__device__ __forceinline__ void seg_fwd(const FA &A, const FF &F, int K, int lo, int nmax, double (&y)[TS]) {
     double v = 0.0;
-    for (int i = max(0, s - K); i < s; ++i) v = fma(__ldg(a + i), v, F(i));
+#pragma unroll
+    for (int u = -KM; u < 0; ++u)
+        if (u >= -K && u >= lo) v = fma(A(u), v, F(u));
 #pragma unroll
     for (int t = 0; t < TS; ++t) {
-        const int i = s + t;
         y[t] = 0.0;
-        if (i < n) {
-            v = fma(__ldg(a + i), v, F(i));
+        if (t < nmax) {
+            v = fma(A(t), v, F(t));
             y[t] = v;
         }
     }
 }
 
-// x(i) = e(i) x(i+1) + g(i) Y(i) for i in [s, s+TS) below n, started from
-// zero at min(n-1, s+TS-1+K)
-template <int TS, class FY>
-__device__ __forceinline__ void seg_bwd(const FY &Y, int s, int n, int K, const double *__restrict__ e,
-                                        const double *__restrict__ g, double (&x)[TS]) {
+// x(i) = e(i) x(i+1) + g(i) Y(i) for the TS positions from s, started from
+// zero K positions after the segment; positions at or past nmax are not used
+template <int TS, int KM, class FE, class FG, class FY>
+__device__ __forceinline__ void seg_bwd(const FE &E, const FG &G, const FY &Y, int K, int nmax, double (&x)[TS]) {
     double v = 0.0;
-    for (int i = min(n - 1, s + TS - 1 + K); i >= s + TS; --i) v = fma(__ldg(e + i), v, __ldg(g + i) * Y(i));
+#pragma unroll
+    for (int u = TS + KM - 1; u >= TS; --u)
+        if (u < TS + K && u < nmax) v = fma(E(u), v, G(u) * Y(u));
 #pragma unroll
     for (int t = TS - 1; t >= 0; --t) {
-        const int i = s + t;
         x[t] = 0.0;
-        if (i < n) {
-            v = fma(__ldg(e + i), v, __ldg(g + i) * Y(i));
+        if (t < nmax) {
+            v = fma(E(t), v, G(t) * Y(t));
             x[t] = v;
         }
     }
 }
 
-struct WinShape {            // shared-memory layout of one tile
-    int cols, pitch, rows;   // right-hand side tile: rows x cols (row stride pitch, odd)
-    int nyf, ypitch;         // forward y segments per row; their row stride (odd)
-    int nzf;                 // forward z segments per column
-    int a_size, b_size;      // doubles in regions A (rhs, then y-solved) and B (y, then z partials)
+struct WinShape {            // shared-memory layout of one tile (in doubles)
+    int nyf, cols, pitch, rows;  // forward y segments per row; rhs tile rows x cols (stride pitch, odd)
+    int ypitch, nzf;             // row stride of the forward y values; forward z segments per column
+    int ncy, ncz;                // staged coefficient counts (y: a e g; z: a e g)
+    int a_size, b_size, c_size;  // regions A (rhs, then z rhs), B (y, then z partials), C (coefficients)
     __host__ __device__ WinShape(int Ky, int Kz) {
         nyf = (kWTj + Ky + kWSeg - 1) / kWSeg;
-        cols = nyf * kWSeg + Ky;  // >= kWTj + 2 Ky: every forward segment reads inside its row
+        cols = nyf * kWSeg + Ky;  // every forward y segment reads inside its row
         pitch = cols | 1;
         rows = kWTk + 2 * Kz;
         ypitch = (nyf * kWSeg) | 1;
         nzf = (kWTk + Kz + kWSeg - 1) / kWSeg;
-        a_size = rows * pitch;
+        ncy = cols;
+        ncz = nzf * kWSeg + Kz;
+        const int a1 = rows * pitch, a2 = rows * kWXp;
+        a_size = a1 > a2 ? a1 : a2;
         const int b1 = rows * ypitch, b2 = nzf * kWSeg * kWTj;
         b_size = b1 > b2 ? b1 : b2;
+        c_size = 3 * ncy + 3 * ncz;
     }
 };
 
@@ -537,10 +544,11 @@ struct WinShape {            // shared-memory layout of one tile
 
 // blockIdx.y = 0: v (solq2j + solq2k + walls), 1: w (solq3j + solq3k);
 // blockIdx.x = tile (tj fastest).
-__global__ void __launch_bounds__(kWThreads) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
+template <int KM>
+__global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
     extern __shared__ double sm[];
     const WinShape sh(Ky, Kz);
-    double *A = sm, *B = sm + sh.a_size;
+    double *A = sm, *B = sm + sh.a_size, *C = B + sh.b_size;
     const int fld = blockIdx.y;
     const int tj = blockIdx.x % ntj, tk = blockIdx.x / ntj;
     const int j0 = 1 + tj * kWTj, k0 = 1 + tk * kWTk;
@@ -554,32 +562,74 @@ __global__ void __launch_bounds__(kWThreads) k_helsolve_win(Dev d, SubDev sd, in
     const int nz = fld ? d.n3 : d.n3m;   // z unknowns (k = 1..nz, line index k-1)
     const int jlo = fld ? 1 : 2;          // columns with a right-hand side
     const int klo = fld ? 2 : 1;          // rows whose y lines are solved
-    const int rows = sh.rows;
+    const int rows = sh.rows, cols = sh.cols;
+    const int iy0 = j0 - 1 - Ky;          // y line index of tile column 0
+    const int iz0 = k0 - 1 - Kz;          // z line index of tile row 0
+    double *cya = C, *cye = C + sh.ncy, *cyg = C + 2 * sh.ncy;
+    double *cza = C + 3 * sh.ncy, *cze = cza + sh.ncz, *czg = cza + 2 * sh.ncz;
 
-    // 1. right-hand side tile scaled by the y row normalisers (coalesced in j);
-    //    A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r)
-    for (int r = w; r < rows; r += kWarps) {
-        const int k = k0 - Kz + r;
-        const bool kok = (k >= klo && k <= d.n3m);
-        for (int c = lane; c < sh.cols; c += 32) {
-            const int j = j0 - Ky + c;
-            double v = 0.0;
-            if (kok && j >= jlo && j <= d.n2m) v = __ldcg(rhs + fidx(d, j, k)) * __ldg(by + j);
-            A[r * sh.pitch + c] = v;
+    // 1. coefficients and the right-hand side tile scaled by the y row
+    //    normalisers; A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r)
+    for (int c = threadIdx.x; c < sh.ncy; c += kWThreads) {
+        const int i = iy0 + c;
+        const bool ok = (i >= 0 && i < ny);
+        cya[c] = ok ? __ldg(sy.a + i) : 0.0;
+        cye[c] = ok ? __ldg(sy.e + i) : 0.0;
+        cyg[c] = ok ? __ldg(sy.g + i) : 0.0;
+    }
+    for (int c = threadIdx.x; c < sh.ncz; c += kWThreads) {
+        const int i = iz0 + c;
+        const bool ok = (i >= 0 && i < nz);
+        cza[c] = ok ? __ldg(sz.a + i) : 0.0;
+        cze[c] = ok ? __ldg(sz.e + i) : 0.0;
+        czg[c] = ok ? __ldg(sz.g + i) : 0.0;
+    }
+    {
+        constexpr int kRB = 4;   // rows per batch
+        constexpr int kCC = 3;   // column chunks of 32 (cols <= 96)
+        int jc[kCC];
+        bool okc[kCC];
+        double sc[kCC];
+#pragma unroll
+        for (int cc = 0; cc < kCC; ++cc) {
+            const int c = lane + 32 * cc;
+            jc[cc] = j0 - Ky + c;
+            okc[cc] = (c < cols) && (jc[cc] >= jlo && jc[cc] <= d.n2m);
+            sc[cc] = okc[cc] ? __ldg(by + jc[cc]) : 0.0;
+        }
+        for (int r0 = w * kRB; r0 < rows; r0 += kWarps * kRB) {
+            double v[kRB][kCC];
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) {
+                const int r = r0 + u, k = k0 - Kz + r;
+                const bool kok = (r < rows) && (k >= klo && k <= d.n3m);
+#pragma unroll
+                for (int cc = 0; cc < kCC; ++cc)
+                    v[u][cc] = (kok && okc[cc]) ? __ldcg(rhs + fidx(d, jc[cc], k)) * sc[cc] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) {
+                const int r = r0 + u;
+#pragma unroll
+                for (int cc = 0; cc < kCC; ++cc)
+                    if (r < rows && lane + 32 * cc < cols) A[r * sh.pitch + lane + 32 * cc] = v[u][cc];
+            }
         }
     }
     __syncthreads();
 
     // 2. forward y recurrences: lanes = rows, warps = (row group, segment);
-    //    B[r * ypitch + c] = y at column j0 + c, c < nyf * kWSeg
+    //    B[r * ypitch + c] = y at tile column c (j = j0 + c), c < nyf * kWSeg
     const int nrg = (rows + 31) / 32;
     for (int task = w; task < nrg * sh.nyf; task += kWarps) {
         const int rg = task / sh.nyf, sg = task - rg * sh.nyf;
         const int r = rg * 32 + lane, rr = min(r, rows - 1);
-        const double *arow = A + rr * sh.pitch + (1 - j0 + Ky);  // arow[i]: line index i
-        const int s = j0 - 1 + sg * kWSeg;
+        const int c0 = Ky + sg * kWSeg;  // coefficient/rhs column of the segment start
+        const double *arow = A + rr * sh.pitch + c0;
+        const int lo = -(j0 - 1 + sg * kWSeg);  // line index 0 relative to the segment start
         double y[kWSeg];
-        seg_fwd<kWSeg>([&](int i) { return arow[i]; }, s, ny, Ky, sy.a, y);
+        seg_fwd<kWSeg, KM>([&](int u) { return cya[c0 + u]; }, [&](int u) { return arow[u]; }, Ky, lo,
+                           ny - (j0 - 1 + sg * kWSeg), y);
         if (r < rows) {
 #pragma unroll
             for (int t = 0; t < kWSeg; ++t) B[r * sh.ypitch + sg * kWSeg + t] = y[t];
@@ -587,78 +637,77 @@ __global__ void __launch_bounds__(kWThreads) k_helsolve_win(Dev d, SubDev sd, in
     }
     __syncthreads();
 
-    // 3. backward y recurrences over the tile's columns; A[r * kWTj + c] =
-    //    y-solved value at (j0 + c, k0 - Kz + r) (0 on rows without a y line)
+    // 3. backward y recurrences over the tile's columns, then the z right-hand
+    //    side: A[r * kWXp + c] = f at (j0 + c, k0 - Kz + r), scaled by the z
+    //    row normalisers, with the inflow/outflow terms (solve_fluid.F90:208-209,
+    //    266-275)
     for (int task = w; task < nrg * (kWTj / kWSeg); task += kWarps) {
         const int rg = task / (kWTj / kWSeg), sg = task - rg * (kWTj / kWSeg);
         const int r = rg * 32 + lane, rr = min(r, rows - 1);
         const int k = k0 - Kz + r;
         const bool live = (r < rows) && k >= klo && k <= d.n3m;
-        const double *brow = B + rr * sh.ypitch + (1 - j0);  // brow[i]: line index i
-        const int s = j0 - 1 + sg * kWSeg;
+        const int c0 = Ky + sg * kWSeg;
+        const double *brow = B + rr * sh.ypitch + sg * kWSeg;
         double x[kWSeg];
-        seg_bwd<kWSeg>([&](int i) { return brow[i]; }, s, ny, Ky, sy.e, sy.g, x);
+        seg_bwd<kWSeg, KM>([&](int u) { return cye[c0 + u]; }, [&](int u) { return cyg[c0 + u]; },
+                           [&](int u) { return brow[u]; }, Ky, ny - (j0 - 1 + sg * kWSeg), x);
         if (r < rows) {
+            const double bzk = (k >= 1 && k <= nz) ? __ldg(bz + k) : 0.0;
 #pragma unroll
-            for (int t = 0; t < kWSeg; ++t) A[r * kWTj + sg * kWSeg + t] = live ? x[t] : 0.0;
+            for (int t = 0; t < kWSeg; ++t) {
+                const int j = j0 + sg * kWSeg + t;
+                const int jj = min(max(j, 1), d.n2m);
+                double f = live ? x[t] * bzk : 0.0;
+                if (fld == 0) {
+                    if (k == 1) f = f + d.dqb2s[jj] * sd.ugkks;
+                    if (k == nz) f = f + d.dqb2n[jj] * sd.ugkkn;
+                } else {
+                    if (k == 1) f = d.dqb3s[jj];
+                    if (k == nz) f = d.dqb3n[jj];
+                }
+                A[r * kWXp + sg * kWSeg + t] = f;
+            }
         }
     }
     __syncthreads();
 
     // 4. forward z recurrences: lanes = columns, warps = segments of rows;
-    //    B[c * kWTj + lane] = z partial at row k0 + c, c < nzf * kWSeg
+    //    B[c * kWTj + lane] = z partial at tile row c from k0, c < nzf * kWSeg
     const int j = j0 + lane;
     const bool jlive = (j >= jlo && j <= d.n2m);
-    const int jj = min(max(j, 1), d.n2m);
-    double bs, bn;
-    if (fld == 0) {
-        bs = d.dqb2s[jj] * sd.ugkks;
-        bn = d.dqb2n[jj] * sd.ugkkn;
-    } else {
-        bs = d.dqb3s[jj];
-        bn = d.dqb3n[jj];
-    }
     const double *acol = A + lane;
-    const int roff = Kz - k0 + 1;  // row of line index i: i + roff
-    auto Fz = [&](int i) {
-        const int k = i + 1;
-        const double v = acol[min(i + roff, rows - 1) * kWTj] * __ldg(bz + k);
-        if (fld == 0) {
-            double f = v;
-            if (k == 1) f = f + bs;
-            if (k == nz) f = f + bn;
-            return f;
-        }
-        return (k == 1) ? bs : ((k == nz) ? bn : v);
-    };
     for (int sg = w; sg < sh.nzf; sg += kWarps) {
-        const int s = k0 - 1 + sg * kWSeg;
+        const int c0 = Kz + sg * kWSeg;  // tile row and coefficient index of the segment start
         double y[kWSeg];
-        seg_fwd<kWSeg>(Fz, s, nz, Kz, sz.a, y);
+        seg_fwd<kWSeg, KM>([&](int u) { return cza[c0 + u]; },
+                           [&](int u) { return acol[min(c0 + u, rows - 1) * kWXp]; }, Kz,
+                           -(k0 - 1 + sg * kWSeg), nz - (k0 - 1 + sg * kWSeg), y);
 #pragma unroll
         for (int t = 0; t < kWSeg; ++t) B[(sg * kWSeg + t) * kWTj + lane] = y[t];
     }
     __syncthreads();
 
     // 5. backward z recurrences over the tile's rows; q += result
-    const double *bcol = B + lane + (1 - k0) * kWTj;  // bcol[i * kWTj]: line index i
     for (int sg = w; sg < kWTk / kWSeg; sg += kWarps) {
         const int s = k0 - 1 + sg * kWSeg;
         if (s >= d.n3m) continue;
+        const int c0 = Kz + sg * kWSeg;
+        const double *bcol = B + sg * kWSeg * kWTj + lane;
         double x[kWSeg];
-        seg_bwd<kWSeg>([&](int i) { return bcol[i * kWTj]; }, s, nz, Kz, sz.e, sz.g, x);
+        seg_bwd<kWSeg, KM>([&](int u) { return cze[c0 + u]; }, [&](int u) { return czg[c0 + u]; },
+                           [&](int u) { return bcol[u * kWTj]; }, Kz, nz - s, x);
         if (jlive) {
+            double qv[kWSeg];
 #pragma unroll
-            for (int t = 0; t < kWSeg; ++t) {
-                const int k = s + 1 + t;
-                if (k <= d.n3m) {
-                    double *p = q + fidx(d, j, k);
-                    *p = __ldcg(p) + x[t];
-                }
-            }
+            for (int t = 0; t < kWSeg; ++t)
+                if (s + 1 + t <= d.n3m) qv[t] = __ldcg(q + fidx(d, j, s + 1 + t));
+#pragma unroll
+            for (int t = 0; t < kWSeg; ++t)
+                if (s + 1 + t <= d.n3m) q[fidx(d, j, s + 1 + t)] = qv[t] + x[t];
         }
     }
-    if (fld == 1 && jlive && w == 0 && k0 <= d.n3m && k0 + kWTk > d.n3m) Fv(q, j, d.n3) = Fv(q, j, d.n3) + bn;
+    if (fld == 1 && jlive && w == 0 && k0 <= d.n3m && k0 + kWTk > d.n3m)
+        Fv(q, j, d.n3) = Fv(q, j, d.n3) + d.dqb3n[j];
     if (fld == 0 && blockIdx.x == 0) {  // helsolve.F90:35-36: wall values of v
         for (int k = threadIdx.x; k <= d.n3; k += kWThreads) {
             Fv(d.q2, 1, k) = 0.0;
@@ -718,7 +767,7 @@ cudaError_t scan_configure() {
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
     AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
-    AL(k_helsolve_win)
+    AL(k_helsolve_win<12>) AL(k_helsolve_win<kWinMax>)
 #undef AL
     return cudaSuccess;
 }
@@ -727,8 +776,11 @@ void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
     const int ntj = (d.n2m + kWTj - 1) / kWTj, ntk = (d.n3m + kWTk - 1) / kWTk;
     const dim3 grid(ntj * ntk, 2);
     const WinShape sh(s.win_y, s.win_z);
-    const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size) * sizeof(double);
-    k_helsolve_win<<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+    const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
+    if (s.win_y <= 12 && s.win_z <= 12)
+        k_helsolve_win<12><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+    else
+        k_helsolve_win<kWinMax><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
 }
 
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {

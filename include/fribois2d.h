@@ -35,6 +35,7 @@ extern "C" {
 #define FB_ERR_STATE 6        /* bad argument for this context (id, size, order) */
 #define FB_ERR_UNSUPPORTED 7  /* deck option not implemented on the device path */
 #define FB_ERR_NUMERIC 8      /* a NaN/Inf or a singular set-up system was detected */
+#define FB_ERR_TIMEOUT 9      /* a device-side wait gave up (bounded waits in the tensor-core kernels) */
 
 typedef struct fb_ctx fb_ctx;     /* device context: one case on one GPU */
 typedef struct fb_host fb_host;   /* host-side set-up of one case (no GPU) */
@@ -103,8 +104,11 @@ typedef struct fb_host fb_host;   /* host-side set-up of one case (no GPU) */
 /* one row per step: forcecomp.out (rigid.F90:432) then rbkin.out (ttime.F90:146)
  *  [0] time (start of step)  [1] Fy  [2] Fz  [3] M  [4] Fyp [5] Fzp [6] Fyv [7] Fzv
  *  [8] time (end of step) [9..11] cmp_np1 [12..14] cmv_np1 [15..17] cma_np1
- *  [18] nbcv [19] nbcw [20] cflm */
-#define FB_HIST_COLS 21
+ *  [18] nbcv [19] nbcw [20] cflm (start of step) [21] dt
+ *  with fb_set_report on, the ttime.F90 diagnostics of the end-of-step field
+ *  (fluid_rep.out, ttime.F90:142): [22] cflm [23] dmax [24] ektot [25] vorti
+ *  [26] vmax(1) [27] vmax(2) [28] vmin(1) [29] vmin(2); zero otherwise */
+#define FB_HIST_COLS 30
 
 /* ---- stage ids for fb_stage: one per reference subroutine --------------- */
 #define FB_ST_CFL 0        /* cfl.F90 (fluid_tsch.F90:211-258) */
@@ -154,6 +158,23 @@ int fb_get_loads(fb_ctx *ctx, double *press, double *tau);
 int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const double *lmacc,
                    const double *lmnor);
 
+/* Last history row written (FB_HIST_COLS doubles), for per-step callers. */
+int fb_last_history(fb_ctx *ctx, double *row);
+/* End-of-step diagnostics of ttime.F90 (vmaxv, vminv, cfl, divgck, kinen,
+ * getintvort) into history columns 22..29 after every step; off by default. */
+int fb_set_report(fb_ctx *ctx, int on);
+
+/* ---- checkpoint / restart --------------------------------------------------
+ * The restart set of mpi_write_continua / writeqbns / master_rigid.dat
+ * (mpi_routines.F90:532-806, iobcs.F90:114-205, ttime.F90:117-124) as raw
+ * FP64 files in `dir` (rest_q2/q3/pr/ru2/ru3.bin, outflow.bin, inflow.bin,
+ * master_rigid.dat), plus device_state.bin and scalars.bin with the marker,
+ * boundary-increment and clock state, so that a run read back continues bit
+ * for bit.  The directory must exist; the deck of the reading context must
+ * have the same grid, markers and dt. */
+int fb_write_restart(fb_ctx *ctx, const char *dir);
+int fb_read_restart(fb_ctx *ctx, const char *dir);
+
 /* ---- state access --------------------------------------------------------- */
 /* dims: n2, n3, nlm, nsst, field pitch, Poisson pitch, pivoting flags,
  * helsolve windows of substep 1 (y | z << 8; 0 = full line scans) */
@@ -175,10 +196,25 @@ int fb_last_advance_ms(fb_ctx *ctx, double *ms);
 #define FB_TK_GEMM_FWD 100   /* phcalc_outflow.F90:31 eigen transform (cuBLAS DGEMM) */
 #define FB_TK_POISSON_TRI 101 /* phcalc_outflow.F90:34-56 per-mode y solves */
 #define FB_TK_GEMM_BWD 102   /* phcalc_outflow.F90:61 back transform */
+#define FB_TK_TF32X3_GEMM 103 /* one 3xTF32 tensor-core transform (precision form) */
 int fb_time_stage(fb_ctx *ctx, int stage, int n, int reps, double *ms);
 /* Number of this library's own kernels one captured time step launches
  * (library kernels of cuBLAS and CUB are not counted). */
 int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
+
+/* ---- precision form of the Poisson solve ---------------------------------
+ * FB_POISSON_FP64: phcalc as the reference computes it (FP64 DGEMM
+ * transforms).  FB_POISSON_TF32X3: the two eigen transforms on the tensor
+ * cores in split precision (TF32 high and low parts, three products, FP32
+ * accumulation), FP64 tridiagonal solves, then one FP64 iterative-refinement
+ * sweep on the Poisson residual.  No counterpart in the reference. */
+#define FB_POISSON_FP64 0
+#define FB_POISSON_TF32X3 1
+int fb_set_poisson(fb_ctx *ctx, int mode);
+/* C = A * B^T with the 3xTF32 tensor-core kernel: A (M x K) and B (N x K)
+ * column-major host arrays, C (M x N) column-major; allocates its own device
+ * buffers on `device` (a test and calibration entry point). */
+int fb_gemm_tf32x3(int device, int M, int N, int K, const double *A, const double *B, double *C);
 
 /* ---- host-only set-up (no GPU touched; usable on a CPU-only machine) ----- */
 int fb_host_create(const char *input_dir, fb_host **out);

@@ -213,12 +213,29 @@ def test_cfl_overflow_is_reported(tmp_path):
     assert e.value.code == fb.FB_ERR_CFL
 
 
-def test_unsupported_variable_dt_is_rejected(tmp_path):
+@pytest.mark.parametrize("nsst", [3, 1])
+def test_variable_dt_matches_oracle(nsst, tmp_path):
+    """idtv = .false. (fluid_tsch.F90:34-48): dt = cflmax / cflm from the
+    second step on, capped by dtmax; the device rebuilds its Helmholtz
+    factors for every new dt.  RK3 and Adams-Bashforth (whose coefficients
+    use dt/dt_o)."""
     c = cases.tiny_cylinder()
     c.params.idtv = False
-    with pytest.raises(fb.FBError) as e:
-        fb.Solver(c.write(str(tmp_path / c.name)))
-    assert e.value.code == fb.FB_ERR_UNSUPPORTED
+    c.params.cflmax = 0.25
+    c.params.dtmax = 0.02
+    c.params.nsst = nsst
+    p = Pair(c, str(tmp_path))
+    n2m, n3m = p.n2m, p.n3m
+    dts = []
+    for ns in range(8):
+        assert p.o.step(ns) == 0
+        h = p.s.advance(ns, 1)
+        dts.append(h[0, fb.HIST_NAMES.index("dt")])
+        assert dts[-1] == pytest.approx(p.o.scalars()["dt"], rel=1e-13)
+        for f in ("q2", "q3"):
+            assert rel(_sub(p.s.get(f), 1, n3m, 1, n2m), _sub(p.of(f), 1, n3m, 1, n2m)) <= 1e-10, (f, ns)
+        assert rel(p.s.get("rigid"), p.o.a("rigid")) <= 1e-12
+    assert dts[0] == c.params.dt and len(set(dts[1:])) > 1   # dt really varies
 
 
 def _windows(s):
