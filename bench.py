@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="advance N independent VIV cases (grid sizes 256x192..768x512 drawn by seed) "
+                         "with one graph launch per step instead of the single case")
     ap.add_argument("--poisson", default="fp64", choices=sorted(FORMS),
                     help="eigen transforms of the Poisson solve: FP64 DGEMM, or 3xTF32 on the tensor cores")
     return ap.parse_args()
@@ -74,6 +77,20 @@ def replica_throughput(world: int, cells: int, steps: int, max_ms: float) -> flo
     """Whole-job cell-steps/s: every rank advanced its own replica `steps`
     steps of `cells` cells; the job took as long as its slowest rank."""
     return world * cells * steps / (max_ms * 1e-3)
+
+
+def profiled_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum of one
+    ncu capture) from the '| workload | kernel | bytes |' rows of the ncu
+    summaries under profiles/, or None."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for ln in f:
+                cells = [x.strip() for x in ln.strip().strip("|").split("|")]
+                if len(cells) == 3 and cells[0] == workload and cells[1] == kernel and cells[2].isdigit():
+                    return int(cells[2])
+    return None
 
 
 def make_case(name):
@@ -259,6 +276,65 @@ def kernel_table(fb, path, c, poisson="fp64"):
     return out
 
 
+def batch_arm(args, rank, world, local):
+    """N independent VIV cases stepped together (fb_batch: one CUDA graph
+    launch per step) against the same cases stepped one after another."""
+    import torch
+    import fribois2d_b200 as fb
+    from fribois2d_b200 import case as cases
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cs = cases.viv_batch(args.batch, seed=rank)
+    root = tempfile.mkdtemp(prefix=f"fbbatch{rank}_")
+    solvers = []
+    for c in cs:
+        sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
+        if args.poisson == "tf32x3":
+            sv.set_poisson(fb.POISSON_TF32X3)
+        q2 = sv.get("q2")
+        q2[1:c.n3m + 1] += c.v_perturbation()
+        sv.set("q2", q2)
+        solvers.append(sv)
+    cells = sum(c.cells for c in cs)
+    W, K = max(3, args.warmup), max(1, args.steps)
+    # one after another: each case's own captured step, K steps each
+    seq_ms = 0.0
+    for sv in solvers:
+        sv.advance(0, W)
+        sv.advance(W, K, history=False)
+        seq_ms += sv.last_advance_ms()
+    batch = fb.Batch(solvers)
+    batch.advance(W)
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    batch.advance(K)
+    clk = clocks.stop()
+    ms = batch.last_ms()
+    per_step_kernels = sum(sv.kernel_count() for sv in solvers)
+    value = cells * K / (ms * 1e-3)
+    line = {
+        "metric": f"cell-steps/s ({FORMS[args.poisson]}, batch of {args.batch} VIV cases, one graph launch per step)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.poisson == "fp64" else "f64 (Poisson transforms: 3xtf32)", "data": "synthetic",
+        "config": {"workload": f"viv_batch_{args.batch}", "cells_total": cells,
+                   "grids": {f"{n3}x{n2}": sum(1 for c in cs if (c.n3m, c.n2m) == (n3, n2))
+                             for n3, n2, _ in cases.BATCH_GRIDS},
+                   "poisson": args.poisson, "l2": "working set far above L2 (all cases resident)"},
+        "sequential": {"value": cells * K / (seq_ms * 1e-3), "ms_per_step": seq_ms / K,
+                       "note": "the same cases, each advanced alone by its own captured step graph"},
+        "speedup_vs_sequential": seq_ms / ms,
+        "gpu_launches": per_step_kernels * K, "clocks": clk,
+    }
+    batch.close()
+    for sv in solvers:
+        sv.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def device_arm(args, rank, world, local):
     import torch
     import fribois2d_b200 as fb
@@ -276,6 +352,7 @@ def device_arm(args, rank, world, local):
     s = fb.Solver(path, device=local)
     if args.poisson == "tf32x3":
         s.set_poisson(fb.POISSON_TF32X3)
+    tiles = s.autotune()   # tile shapes for this grid size (state preserved)
     pert = c.v_perturbation()
     q2 = s.get("q2")
     q2[1:c.n3m + 1] += pert
@@ -353,13 +430,7 @@ def device_arm(args, rank, world, local):
             r["share"] = r["ms"] * r["per_step"] / step_ms
         dom = max((r for r in table if r["bound"] in ("hbm", "tensor", "tensor_tf32")),
                   key=lambda r: r["ms"] * r["per_step"])
-        traffic = None
-        try:
-            with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-                tr = json.load(f).get(c.name, {})
-            traffic = tr.get(dom["kernel"])
-        except (OSError, ValueError):
-            pass
+        traffic = profiled_traffic(c.name, dom["kernel"])
         if dom["bound"] == "tensor":
             achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e12
             roof = {"kernel": dom["kernel"], "bound": "tensor", "achieved": achieved, "peak": peak_fp64,
@@ -391,6 +462,7 @@ def device_arm(args, rank, world, local):
             "dtype": "f64" if args.poisson == "fp64" else "f64 (Poisson transforms: 3xtf32)", "data": "synthetic",
             "config": {"workload": c.name, "poisson": args.poisson, "cells": c.cells, "markers": c.nlm, "dt": c.params.dt,
                        "parallelism": f"replicas x{world}" if world > 1 else "single case",
+                       "tiles": {"helsolve_rows": tiles[0], "gemm_cols": tiles[1] if args.poisson == "tf32x3" else None},
                        "l2": "flushed (256 MB write) between timed steps"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": per_step_kernels * K, "clocks": clk,
@@ -411,6 +483,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.batch:
+        batch_arm(args, rank, world, local)
         return
     device_arm(args, rank, world, local)
 

@@ -104,10 +104,16 @@ def lib() -> ctypes.CDLL:
         "fb_eigen_tridiag": ([ctypes.c_int, dp, dp, dp, dp, dp, dp], ctypes.c_int),
         "fb_set_poisson": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_set_report": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_batch_create": ([P(vp), ctypes.c_int, P(vp)], ctypes.c_int),
+        "fb_batch_advance": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_batch_last_ms": ([vp, dp], ctypes.c_int),
+        "fb_batch_destroy": ([vp], ctypes.c_int),
         "fb_last_history": ([vp, dp], ctypes.c_int),
         "fb_write_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
         "fb_read_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
-        "fb_gemm_tf32x3": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp], ctypes.c_int),
+        "fb_gemm_tf32x3": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp],
+                           ctypes.c_int),
+        "fb_autotune": ([vp, ip], ctypes.c_int),
         "fb_status_string": ([ctypes.c_int], ctypes.c_char_p),
         "fb_version": ([], ctypes.c_char_p),
     }
@@ -160,7 +166,38 @@ class HostSetup:
         return out
 
 
-def gemm_tf32x3(A: np.ndarray, B: np.ndarray, device: int = 0) -> np.ndarray:
+class Batch:
+    """Independent cases (Solver objects on one device, fixed dt, RK3) advanced
+    together: one CUDA graph launch steps every case (fb_batch_*)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        self._lib = lib()
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
+        self.b = ctypes.c_void_p()
+        _check(self._lib.fb_batch_create(arr, len(self.solvers), ctypes.byref(self.b)), "fb_batch_create")
+
+    def advance(self, nsteps: int) -> None:
+        _check(self._lib.fb_batch_advance(self.b, int(nsteps)), "fb_batch_advance")
+
+    def last_ms(self) -> float:
+        ms = ctypes.c_double()
+        _check(self._lib.fb_batch_last_ms(self.b, ctypes.byref(ms)), "fb_batch_last_ms")
+        return ms.value
+
+    def close(self) -> None:
+        if self.b:
+            self._lib.fb_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gemm_tf32x3(A: np.ndarray, B: np.ndarray, device: int = 0, bn: int = 128) -> np.ndarray:
     """C = A @ B.T on the tensor cores in split precision (3xTF32)."""
     A = np.asfortranarray(A, dtype=np.float64)
     B = np.asfortranarray(B, dtype=np.float64)
@@ -169,7 +206,7 @@ def gemm_tf32x3(A: np.ndarray, B: np.ndarray, device: int = 0) -> np.ndarray:
     if K2 != K:
         raise ValueError("inner dimensions differ")
     C = np.zeros((M, N), dtype=np.float64, order="F")
-    _check(lib().fb_gemm_tf32x3(int(device), M, N, K, _dp(A), _dp(B), _dp(C)), "fb_gemm_tf32x3")
+    _check(lib().fb_gemm_tf32x3(int(device), M, N, K, int(bn), _dp(A), _dp(B), _dp(C)), "fb_gemm_tf32x3")
     return C
 
 
@@ -314,6 +351,13 @@ class Solver:
         """POISSON_FP64 (the reference's FP64 transforms) or POISSON_TF32X3
         (3xTF32 tensor-core transforms plus one FP64 refinement sweep)."""
         _check(self._lib.fb_set_poisson(self.ctx, int(mode)), "fb_set_poisson")
+
+    def autotune(self):
+        """Tile shapes for this grid size, timed on this context: returns
+        (helsolve tile height, tensor-core GEMM tile width)."""
+        ch = (ctypes.c_int32 * 2)()
+        _check(self._lib.fb_autotune(self.ctx, ch), "fb_autotune")
+        return int(ch[0]), int(ch[1])
 
     def set_report(self, on: bool = True) -> None:
         """End-of-step diagnostics of ttime.F90 into history columns 22..29."""

@@ -425,4 +425,29 @@ def tiny_rectangle(n3m: int = 64, n2m: int = 40, h: float = 1.0 / 8, nlm: int = 
                                name=f"tiny_rectangle_{n3m}x{n2m}")
 
 
+# grid sizes (z cells, y cells) of the batched VIV workload with their
+# uniform spacing: two markers per spacing on the circle, CFL ~ 0.1 at U = 1
+BATCH_GRIDS = ((256, 192, 1.0 / 24), (384, 256, 1.0 / 32), (512, 384, 1.0 / 48), (768, 512, 1.0 / 64))
+
+
+def viv_batch(n: int = 256, seed: int = 0, steps: int = 1000):
+    """Independent VIV cylinder cases drawn by seed: grid size from
+    BATCH_GRIDS, Re uniform in [60, 200], mass ratio log-uniform in [2, 20],
+    reduced velocity uniform in [2, 12]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        n3m, n2m, h = BATCH_GRIDS[int(rng.integers(len(BATCH_GRIDS)))]
+        re = float(rng.uniform(60.0, 200.0))
+        mr = float(np.exp(rng.uniform(np.log(2.0), np.log(20.0))))
+        ur = float(rng.uniform(2.0, 12.0))
+        cz, cy = int(0.4 * n3m) // 10 * 10, int(0.4 * n2m) // 10 * 10   # window cells
+        wz, wy = cz * h, cy * h
+        z0 = -round(0.3 * cz) * h
+        out.append(viv_cylinder(n3m=n3m, n2m=n2m, h=h, zwin=(z0, z0 + wz), ywin=(-0.5 * wy, 0.5 * wy),
+                                nlm=int(round(2.0 * math.pi / h)), re=re, mass_ratio=mr, u_red=ur,
+                                dt=0.1 * h, steps=steps, name=f"viv_batch_{i:03d}_{n3m}x{n2m}"))
+    return out
+
+
 WORKLOADS = {f.__name__: f for f in (viv_cylinder_384x256, galloping_rectangle_1024x768, viv_cylinder_2048x1536)}

@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -59,6 +61,8 @@ struct fb_ctx {
     std::vector<std::pair<const int **, size_t>> coef_fixi;
     size_t coef_cap = 0, coef_capi = 0;
     bool vardt = false;       // idtv = .false.: dt from the CFL number every step
+    int tune_tk = 64;         // windowed helsolve tile height (autotuned per grid size)
+    int tune_bn = 128;        // 3xTF32 GEMM tile width (autotuned per grid size)
     // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
     // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
     int poisson_mode = FB_POISSON_FP64;
@@ -251,6 +255,7 @@ int build_substep(fb_ctx *c, int n, double al) {
     s.win_y = std::max(wy2, wy3);
     s.win_z = std::max(wz2, wz3);
     if (!s.scan_ok || !c->allow_win || s.win_y > fb::kWinMax || s.win_z > fb::kWinMax) s.win_y = s.win_z = 0;
+    s.win_tk = c->tune_tk;
     return FB_OK;
 }
 
@@ -597,8 +602,8 @@ int setup_tf32(fb_ctx *c) {
     fb::launch_split_t(c->zmm, d.n3m, d.n3m, d.n3m, c->pl_z, c->stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
-    if ((st = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m))) return st;
-    if ((st = fb::tf32x3_plan(c->plan_bwd, c->pl_a2, c->pl_z, d.n2m, d.n3m, d.n3m))) return st;
+    if ((st = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, c->tune_bn))) return st;
+    if ((st = fb::tf32x3_plan(c->plan_bwd, c->pl_a2, c->pl_z, d.n2m, d.n3m, d.n3m, c->tune_bn))) return st;
     c->pw = pw;
     return FB_OK;
 }
@@ -1434,6 +1439,212 @@ int fb_set_poisson(fb_ctx *c, int mode) {
     return FB_OK;
 }
 
+int fb_autotune(fb_ctx *c, int32_t choice[2]);
+
+// ---- batches: independent cases advanced by one graph launch per step
+struct fb_batch {
+    std::vector<fb_ctx *> ctx;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> done;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int *status_h = nullptr;   // pinned: one status per case
+    double last_ms = 0.0;
+};
+
+int fb_batch_destroy(fb_batch *b) {
+    if (!b) return FB_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->done)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->status_h) cudaFreeHost(b->status_h);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return FB_OK;
+}
+
+int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
+    if (!ctxs || n < 1 || !out) return FB_ERR_STATE;
+    *out = nullptr;
+    fb_batch *b = new (std::nothrow) fb_batch;
+    if (!b) return FB_ERR_CUDA;
+    b->device = ctxs[0]->device;
+    for (int i = 0; i < n; ++i) {
+        fb_ctx *c = ctxs[i];
+        if (!c || c->device != b->device || !c->d.nlm) {
+            delete b;
+            return FB_ERR_STATE;
+        }
+        if (c->vardt || c->hc.deck.nsst != 3) {  // per-step host control or first-step coefficients
+            delete b;
+            return FB_ERR_UNSUPPORTED;
+        }
+        b->ctx.push_back(c);
+    }
+    int r = FB_OK;
+    auto fail = [&](int code) {
+        fb_batch_destroy(b);
+        return code;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMallocHost(&b->status_h, sizeof(int) * n) != cudaSuccess)
+        return fail(FB_ERR_CUDA);
+    b->done.assign(static_cast<size_t>(n), nullptr);
+    for (auto &e : b->done)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(FB_ERR_CUDA);
+    for (fb_ctx *c : b->ctx) {   // tile shapes per grid size, then the contexts go quiet
+        if ((r = fb_autotune(c, nullptr))) return fail(r);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(FB_ERR_CUDA);
+    }
+    // one step of every case captured from the master stream: each case's
+    // stream forks from it, runs the case's step (its own side branch,
+    // cuBLAS handle and buffers) and joins back
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail(FB_ERR_CUDA);
+    cudaError_t e = cudaEventRecord(b->fork, b->stream);
+    for (int i = 0; i < n && e == cudaSuccess && !r; ++i) {
+        fb_ctx *c = b->ctx[static_cast<size_t>(i)];
+        e = cudaStreamWaitEvent(c->stream, b->fork, 0);
+        if (e != cudaSuccess) break;
+        c->own_launches = 0;
+        r = enqueue_step(c, 1);
+        c->step_kernels = c->own_launches;
+        if (!r) e = cudaEventRecord(b->done[static_cast<size_t>(i)], c->stream);
+        if (!r && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->done[static_cast<size_t>(i)], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+    if (r || e != cudaSuccess || ee != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(r ? r : FB_ERR_CUDA);
+    }
+    b->graph = g;
+    if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return fail(FB_ERR_CUDA);
+    *out = b;
+    return FB_OK;
+}
+
+int fb_batch_advance(fb_batch *b, int nsteps) {
+    if (!b || nsteps < 0) return FB_ERR_STATE;
+    CK(cudaSetDevice(b->device));
+    CK(cudaEventRecord(b->ev0, b->stream));
+    for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(b->exec, b->stream));
+    CK(cudaEventRecord(b->ev1, b->stream));
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+        CK(cudaMemcpyAsync(b->status_h + i, b->ctx[i]->d.status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    b->last_ms = ms;
+    int status = FB_OK;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        host_clock(b->ctx[i], nsteps);
+        if (!status && b->status_h[i]) status = b->status_h[i];
+    }
+    return status;
+}
+
+int fb_batch_last_ms(fb_batch *b, double *ms) {
+    if (!b || !ms) return FB_ERR_STATE;
+    *ms = b->last_ms;
+    return FB_OK;
+}
+
+// Tile shapes per grid size: the windowed helsolve's tile height (32 or 64
+// rows) and, once the precision form is on, the 3xTF32 GEMM's tile width
+// (64 or 128 columns), each chosen by timing both on this context.  The
+// choice is remembered per (n2, n3) for the process, so a batch of cases of
+// a few grid sizes tunes each size once.  The timed stages' outputs (q2, q3,
+// hmn) are saved and restored around the measurement.
+int fb_autotune(fb_ctx *c, int32_t choice[2]) {
+    if (!c) return FB_ERR_STATE;
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, std::pair<int, int>> cache;   // (n2, n3) -> (tk, bn); bn 0: untuned
+    const std::pair<int, int> key(c->d.n2, c->d.n3);
+    int tk = 0, bn = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            tk = it->second.first;
+            bn = it->second.second;
+        }
+    }
+    const bool want_bn = (c->pw != nullptr);
+    if (!tk || (want_bn && !bn)) {
+        CK(cudaSetDevice(c->device));
+        const Dev &d = c->d;
+        const size_t fbytes = static_cast<size_t>(d.NK) * d.P * sizeof(double);
+        const size_t hbytes = static_cast<size_t>(d.n3m) * d.ldh * sizeof(double);
+        void *save = nullptr;
+        CK(cudaMalloc(&save, 2 * fbytes + hbytes));
+        char *sv = static_cast<char *>(save);
+        CK(cudaMemcpyAsync(sv, d.q2, fbytes, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(sv + fbytes, d.q3, fbytes, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(sv + 2 * fbytes, d.hmn, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+        int r = FB_OK;
+        if (!tk) {
+            double best = 1e30;
+            for (int cand : {32, 64}) {
+                for (int n = 0; n < d.nsst; ++n) c->sub[n].win_tk = cand;
+                double ms = 0.0;
+                if (c->sub[0].win_y == 0) {   // line scans: no tile to tune
+                    tk = 64;
+                    break;
+                }
+                if ((r = fb_time_stage(c, FB_ST_HELSOLVE, 1, 10, &ms))) break;
+                if (ms < best) {
+                    best = ms;
+                    tk = cand;
+                }
+            }
+        }
+        if (!r && want_bn && !bn) {
+            double best = 1e30;
+            for (int cand : {64, 128}) {
+                if ((r = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, cand))) break;
+                double ms = 0.0;
+                if ((r = fb_time_stage(c, FB_TK_TF32X3_GEMM, 1, 10, &ms))) break;
+                if (ms < best) {
+                    best = ms;
+                    bn = cand;
+                }
+            }
+        }
+        cudaMemcpyAsync(d.q2, sv, fbytes, cudaMemcpyDeviceToDevice, c->stream);
+        cudaMemcpyAsync(d.q3, sv + fbytes, fbytes, cudaMemcpyDeviceToDevice, c->stream);
+        cudaMemcpyAsync(d.hmn, sv + 2 * fbytes, hbytes, cudaMemcpyDeviceToDevice, c->stream);
+        cudaStreamSynchronize(c->stream);
+        cudaFree(save);
+        if (r) return r;
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = std::make_pair(tk, bn);
+    }
+    c->tune_tk = tk;
+    for (int n = 0; n < c->d.nsst; ++n) c->sub[n].win_tk = tk;
+    if (want_bn && bn) {
+        c->tune_bn = bn;
+        int r;
+        if ((r = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, c->d.n2m, c->d.n3m, c->d.n3m, bn))) return r;
+        if ((r = fb::tf32x3_plan(c->plan_bwd, c->pl_a2, c->pl_z, c->d.n2m, c->d.n3m, c->d.n3m, bn))) return r;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);
+    if (choice) {
+        choice[0] = c->tune_tk;
+        choice[1] = c->tune_bn;
+    }
+    return FB_OK;
+}
+
 int fb_set_report(fb_ctx *c, int on) {
     if (!c) return FB_ERR_STATE;
     if ((on != 0) != c->report) {
@@ -1444,8 +1655,8 @@ int fb_set_report(fb_ctx *c, int on) {
     return FB_OK;
 }
 
-int fb_gemm_tf32x3(int device, int M, int N, int K, const double *A, const double *B, double *C) {
-    if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return FB_ERR_STATE;
+int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, const double *B, double *C) {
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C || (bn != 64 && bn != 128)) return FB_ERR_STATE;
     CK(cudaSetDevice(device));
     int st = fb::tf32x3_configure();
     if (st) return st;
@@ -1474,7 +1685,7 @@ int fb_gemm_tf32x3(int device, int M, int N, int K, const double *A, const doubl
     if (!st) {
         fb::launch_split_t(dA, M, M, K, pa, nullptr);  // A(m, k) at A[k * M + m] -> [m][k]
         fb::launch_split_t(dB, N, N, K, pb, nullptr);
-        st = fb::tf32x3_plan(plan, pa, pb, M, N, K);
+        st = fb::tf32x3_plan(plan, pa, pb, M, N, K, bn);
     }
     if (!st) {
         fb::launch_tf32x3(plan, dC, M, nullptr, 0, status, nullptr);

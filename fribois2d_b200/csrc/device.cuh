@@ -29,6 +29,7 @@ struct SubDev {          // substep constants (fluid_tsch.F90:64-77)
     ScanSys sy2, sz2, sy3, sz3;           // the same systems for the scan solver
     int scan_ok;                          // 0 if a system needed row interchanges
     int win_y, win_z;                     // truncation windows (y, z) of the windowed helsolve; 0 = off
+    int win_tk;                           // its tile height in k (32 or 64; set by the autotuner)
 };
 
 struct Dev {

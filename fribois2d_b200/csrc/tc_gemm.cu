@@ -6,10 +6,10 @@
 //   C ~ Alo*Bhi + Ahi*Blo + Ahi*Bhi      (FP32 accumulation in TMEM)
 //
 // Operands are FP32 planes holding TF32-rounded high and low parts of FP64
-// values (k_split_t), K contiguous.  One CTA computes a 128 x 128 tile:
+// values (k_split_t), K contiguous.  One CTA computes a 128 x BN tile:
 // one thread issues TMA loads (128-byte swizzle, no multicast) into a
-// three-stage shared-memory ring, one thread issues tcgen05.mma (kind::tf32,
-// M = 128, N = 128, K = 8) into a TMEM accumulator, and the four warps read
+// shared-memory ring of 3 or 4 stages, one thread issues tcgen05.mma
+// (kind::tf32, M = 128, N = BN, K = 8) into a TMEM accumulator, and the four warps read
 // the accumulator back with tcgen05.ld and store FP64 results.  Every
 // mbarrier wait gives up after one second, records FB_ERR_TIMEOUT and lets
 // the CTA finish (waiting for its own copies and MMAs, freeing its TMEM).
@@ -28,15 +28,25 @@ namespace fb {
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 32, kStages = 3, kThreads = 128;
-constexpr uint32_t kTileBytes = kBM * kBK * 4;    // 16 KB; A and B tiles alike (kBM == kBN)
-constexpr uint32_t kStageBytes = 4 * kTileBytes;  // A hi, A lo, B hi, B lo
-constexpr uint32_t kTmemCols = kBN;               // FP32 accumulator: 128 lanes x kBN columns
-constexpr size_t kSmemBytes = kStages * kStageBytes + 1024 + 256;
-// instruction descriptor: D FP32, A and B TF32, both K-major, N = kBN, M = kBM
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
-                            (static_cast<uint32_t>(kBM >> 4) << 24);
-static_assert(kBM == 128 && kBN % 16 == 0 && kBN <= 256, "tcgen05 kind::tf32 shape");
+constexpr int kBM = 128, kBK = 32, kThreads = 128;
+
+// tile width BN (64 or 128) sets the B tiles, the stage count (192 KB ring),
+// the TMEM columns and the instruction descriptor
+template <int BN>
+struct TcCfg {
+    static constexpr int kStages = (BN == 64) ? 4 : 3;
+    static constexpr uint32_t kATile = kBM * kBK * 4;                  // 16 KB
+    static constexpr uint32_t kBTile = BN * kBK * 4;                   // 8 or 16 KB
+    static constexpr uint32_t kStageBytes = 2 * kATile + 2 * kBTile;   // A hi, A lo, B hi, B lo
+    static constexpr uint32_t kTmemCols = BN;                          // FP32 accumulator: 128 lanes x BN
+    static constexpr size_t kSmem = kStages * kStageBytes + 1024 + 256;
+    // instruction descriptor: D FP32, A and B TF32, both K-major, N = BN, M = kBM
+    static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                                       (static_cast<uint32_t>(BN >> 3) << 17) |
+                                       (static_cast<uint32_t>(kBM >> 4) << 24);
+    static_assert(BN == 64 || BN == 128, "tile widths built");
+    static_assert(kStages * kStageBytes + 1024 + 256 <= 227 * 1024, "shared memory per CTA");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -98,13 +108,14 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
     const uint32_t z = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
         : "memory");
 }
 
@@ -135,10 +146,16 @@ __device__ __forceinline__ float tf32_round(float x) {
 
 }  // namespace
 
+template <int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tf32x3_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                   const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
                   GemmOut o, int K, int *status) {
+    using Cfg = TcCfg<BN>;
+    constexpr int kStages = Cfg::kStages;
+    constexpr uint32_t kATile = Cfg::kATile, kBTile = Cfg::kBTile, kStageBytes = Cfg::kStageBytes;
+    constexpr uint32_t kTmemCols = Cfg::kTmemCols, kIdesc = Cfg::kIdesc;
+    constexpr int kBN = BN;
     extern __shared__ uint8_t smraw[];
     const uint32_t raw = smem_u32(smraw);
     const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;  // swizzle atoms need 1024-byte alignment
@@ -186,9 +203,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t st = sbase + s * kStageBytes, fb = full0 + 8 * s;
             mbar_expect_tx(fb, kStageBytes);
             tma_load_2d(st, &ma_hi, fb, kb * kBK, m0);
-            tma_load_2d(st + kTileBytes, &ma_lo, fb, kb * kBK, m0);
-            tma_load_2d(st + 2 * kTileBytes, &mb_hi, fb, kb * kBK, n0);
-            tma_load_2d(st + 3 * kTileBytes, &mb_lo, fb, kb * kBK, n0);
+            tma_load_2d(st + kATile, &ma_lo, fb, kb * kBK, m0);
+            tma_load_2d(st + 2 * kATile, &mb_hi, fb, kb * kBK, n0);
+            tma_load_2d(st + 2 * kATile + kBTile, &mb_lo, fb, kb * kBK, n0);
             issued = kb + 1;
         }
         // every copy issued has landed before the CTA may finish
@@ -207,12 +224,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t st = sbase + s * kStageBytes;
 #pragma unroll
             for (int k = 0; k < kBK / 8; ++k) {  // K = 8 per MMA: 32 bytes along the swizzled row
-                const uint64_t ahi = sw128_desc(st + 32 * k), alo = sw128_desc(st + kTileBytes + 32 * k);
-                const uint64_t bhi = sw128_desc(st + 2 * kTileBytes + 32 * k);
-                const uint64_t blo = sw128_desc(st + 3 * kTileBytes + 32 * k);
-                mma_tf32(tmem, alo, bhi, (kb > 0 || k > 0) ? 1u : 0u);
-                mma_tf32(tmem, ahi, blo, 1u);
-                mma_tf32(tmem, ahi, bhi, 1u);
+                const uint64_t ahi = sw128_desc(st + 32 * k), alo = sw128_desc(st + kATile + 32 * k);
+                const uint64_t bhi = sw128_desc(st + 2 * kATile + 32 * k);
+                const uint64_t blo = sw128_desc(st + 2 * kATile + kBTile + 32 * k);
+                mma_tf32(tmem, alo, bhi, kIdesc, (kb > 0 || k > 0) ? 1u : 0u);
+                mma_tf32(tmem, ahi, blo, kIdesc, 1u);
+                mma_tf32(tmem, ahi, bhi, kIdesc, 1u);
             }
             mma_commit(empty0 + 8 * s);  // frees the stage once these MMAs have read it
         }
@@ -327,7 +344,7 @@ namespace {
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
-int encode_plane(CUtensorMap *m, const float *p, int rows, int K, long ld) {
+int encode_plane(CUtensorMap *m, const float *p, int rows, int K, long ld, int box_rows) {
     if (!g_encode) {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -339,7 +356,7 @@ int encode_plane(CUtensorMap *m, const float *p, int rows, int K, long ld) {
     if ((reinterpret_cast<uintptr_t>(p) & 15u) || (ld % 4) || ld < K) return FB_ERR_STATE;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 4u};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(kBM)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t es[2] = {1, 1};
     const CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(p), dims, strides, box, es,
                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -350,29 +367,36 @@ int encode_plane(CUtensorMap *m, const float *p, int rows, int K, long ld) {
 }  // namespace
 
 int tf32x3_configure() {
-    return cudaFuncSetAttribute(k_tf32x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kSmemBytes)) == cudaSuccess
-               ? FB_OK
-               : FB_ERR_CUDA;
+    const bool ok =
+        cudaFuncSetAttribute(k_tf32x3_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg<64>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_tf32x3_gemm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg<128>::kSmem)) == cudaSuccess;
+    return ok ? FB_OK : FB_ERR_CUDA;
 }
 
-int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K) {
+int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K, int bn) {
+    if (bn != 64 && bn != 128) return FB_ERR_STATE;
     int st;
-    if ((st = encode_plane(&p.a_hi, a.hi, M, K, a.ld))) return st;
-    if ((st = encode_plane(&p.a_lo, a.lo, M, K, a.ld))) return st;
-    if ((st = encode_plane(&p.b_hi, b.hi, N, K, b.ld))) return st;
-    if ((st = encode_plane(&p.b_lo, b.lo, N, K, b.ld))) return st;
+    if ((st = encode_plane(&p.a_hi, a.hi, M, K, a.ld, kBM))) return st;
+    if ((st = encode_plane(&p.a_lo, a.lo, M, K, a.ld, kBM))) return st;
+    if ((st = encode_plane(&p.b_hi, b.hi, N, K, b.ld, bn))) return st;
+    if ((st = encode_plane(&p.b_lo, b.lo, N, K, b.ld, bn))) return st;
     p.M = M;
     p.N = N;
     p.K = K;
+    p.bn = bn;
     return FB_OK;
 }
 
 void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *base, long ldb, int *status,
                    cudaStream_t st) {
     GemmOut o{out, ldo, base, ldb, p.M, p.N};
-    const dim3 grid((p.M + kBM - 1) / kBM, (p.N + kBN - 1) / kBN);
-    k_tf32x3_gemm<<<grid, kThreads, kSmemBytes, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+    const dim3 grid((p.M + kBM - 1) / kBM, (p.N + p.bn - 1) / p.bn);
+    if (p.bn == 64)
+        k_tf32x3_gemm<64><<<grid, kThreads, TcCfg<64>::kSmem, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+    else
+        k_tf32x3_gemm<128><<<grid, kThreads, TcCfg<128>::kSmem, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
 }
 
 void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st) {

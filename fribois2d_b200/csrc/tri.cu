@@ -474,7 +474,6 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb
 // read once and q2/q3 read and written once; the recurrence coefficients of
 // the tile are staged in shared memory with it.
 constexpr int kWTj = 32;        // tile columns (j): one lane each in the z phases
-constexpr int kWTk = 64;        // tile rows (k)
 constexpr int kWSeg = 16;       // values per thread segment
 constexpr int kWThreads = 256;
 constexpr int kWXp = kWTj + 1;  // row stride of the z right-hand side tile (odd: conflict-free column stores)
@@ -518,7 +517,8 @@ __device__ __forceinline__ void seg_bwd(const FE &E, const FG &G, const FY &Y, i
     }
 }
 
-struct WinShape {            // shared-memory layout of one tile (in doubles)
+template <int kWTk>
+struct WinShape {            // shared-memory layout of one tile of kWTk rows (in doubles)
     int nyf, cols, pitch, rows;  // forward y segments per row; rhs tile rows x cols (stride pitch, odd)
     int ypitch, nzf;             // row stride of the forward y values; forward z segments per column
     int ncy, ncz;                // staged coefficient counts (y: a e g; z: a e g)
@@ -544,10 +544,10 @@ struct WinShape {            // shared-memory layout of one tile (in doubles)
 
 // blockIdx.y = 0: v (solq2j + solq2k + walls), 1: w (solq3j + solq3k);
 // blockIdx.x = tile (tj fastest).
-template <int KM>
+template <int KM, int kWTk>
 __global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
     extern __shared__ double sm[];
-    const WinShape sh(Ky, Kz);
+    const WinShape<kWTk> sh(Ky, Kz);
     double *A = sm, *B = sm + sh.a_size, *C = B + sh.b_size;
     const int fld = blockIdx.y;
     const int tj = blockIdx.x % ntj, tk = blockIdx.x / ntj;
@@ -767,20 +767,27 @@ cudaError_t scan_configure() {
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
     AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
-    AL(k_helsolve_win<12>) AL(k_helsolve_win<kWinMax>)
+    AL((k_helsolve_win<12, 32>)) AL((k_helsolve_win<12, 64>))
+    AL((k_helsolve_win<kWinMax, 32>)) AL((k_helsolve_win<kWinMax, 64>))
 #undef AL
     return cudaSuccess;
 }
 
-void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
-    const int ntj = (d.n2m + kWTj - 1) / kWTj, ntk = (d.n3m + kWTk - 1) / kWTk;
+template <int TK>
+void win_launch(const Dev &d, const SubDev &s, cudaStream_t st) {
+    const int ntj = (d.n2m + kWTj - 1) / kWTj, ntk = (d.n3m + TK - 1) / TK;
     const dim3 grid(ntj * ntk, 2);
-    const WinShape sh(s.win_y, s.win_z);
+    const WinShape<TK> sh(s.win_y, s.win_z);
     const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
     if (s.win_y <= 12 && s.win_z <= 12)
-        k_helsolve_win<12><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+        k_helsolve_win<12, TK><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
     else
-        k_helsolve_win<kWinMax><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+        k_helsolve_win<kWinMax, TK><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+}
+
+void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
+    if (s.win_tk == 32) win_launch<32>(d, s, st);
+    else win_launch<64>(d, s, st);
 }
 
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {

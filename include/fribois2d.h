@@ -39,6 +39,7 @@ extern "C" {
 
 typedef struct fb_ctx fb_ctx;     /* device context: one case on one GPU */
 typedef struct fb_host fb_host;   /* host-side set-up of one case (no GPU) */
+typedef struct fb_batch fb_batch; /* independent cases stepped together */
 
 /* ---- array ids for fb_get_array / fb_set_array / fb_host_array --------- */
 /* fields, (n3+1) x n2 doubles, k = 0..n3 */
@@ -164,6 +165,19 @@ int fb_last_history(fb_ctx *ctx, double *row);
  * getintvort) into history columns 22..29 after every step; off by default. */
 int fb_set_report(fb_ctx *ctx, int on);
 
+/* ---- batches of independent cases -------------------------------------------
+ * No counterpart in the reference (one case per MPI job there).  The cases
+ * (contexts on one device, fixed dt, RK3) are captured into one CUDA graph:
+ * every case's step forks from one stream and joins back, so a step of the
+ * whole batch is a single graph launch and the cases run concurrently.  Each
+ * context keeps its own state, history rows and status; the contexts must
+ * outlive the batch and must not be stepped on their own meanwhile.
+ * fb_batch_advance returns the first non-zero case status. */
+int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out);
+int fb_batch_advance(fb_batch *b, int nsteps);
+int fb_batch_last_ms(fb_batch *b, double *ms);  /* device time of the last advance */
+int fb_batch_destroy(fb_batch *b);
+
 /* ---- checkpoint / restart --------------------------------------------------
  * The restart set of mpi_write_continua / writeqbns / master_rigid.dat
  * (mpi_routines.F90:532-806, iobcs.F90:114-205, ttime.F90:117-124) as raw
@@ -214,7 +228,12 @@ int fb_set_poisson(fb_ctx *ctx, int mode);
 /* C = A * B^T with the 3xTF32 tensor-core kernel: A (M x K) and B (N x K)
  * column-major host arrays, C (M x N) column-major; allocates its own device
  * buffers on `device` (a test and calibration entry point). */
-int fb_gemm_tf32x3(int device, int M, int N, int K, const double *A, const double *B, double *C);
+int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, const double *B, double *C);
+/* Picks tile shapes for this grid size by timing the candidates on the
+ * context (state preserved): the windowed helsolve's tile height and, with
+ * the precision form on, the tensor-core GEMM's tile width.  Remembered per
+ * grid size for the process.  choice (may be NULL) receives {height, width}. */
+int fb_autotune(fb_ctx *ctx, int32_t choice[2]);
 
 /* ---- host-only set-up (no GPU touched; usable on a CPU-only machine) ----- */
 int fb_host_create(const char *input_dir, fb_host **out);

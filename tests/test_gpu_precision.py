@@ -20,12 +20,13 @@ from paritylib import rel
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("bn", [64, 128])
 @pytest.mark.parametrize("M,N,K", [(128, 128, 32), (200, 130, 77), (256, 384, 1000), (768, 1024, 1024)])
-def test_tf32x3_gemm_matches_fp64(M, N, K):
+def test_tf32x3_gemm_matches_fp64(M, N, K, bn):
     rng = np.random.default_rng(M * 7 + N * 3 + K)
     A = rng.standard_normal((M, K))
     B = rng.standard_normal((N, K))
-    C = fb.gemm_tf32x3(A, B)
+    C = fb.gemm_tf32x3(A, B, bn=bn)
     ref = A @ B.T
     scale = np.abs(A) @ np.abs(B).T
     err = np.max(np.abs(C - ref) / scale)
@@ -69,3 +70,24 @@ def test_precision_step_matches_fp64(maker, steps, tmp_path):
     for col in (1, 2, 3, 9, 10, 11):   # forces and displacements
         rng_ = max(np.ptp(ha[:, col]), np.max(np.abs(ha[:, col])), 1e-30)
         assert np.max(np.abs(hb[:, col] - ha[:, col])) <= 1e-6 * rng_, col
+
+
+def test_autotune_keeps_state_and_results(tmp_path):
+    """Tuning times candidates on the live context: the state afterwards and
+    the following steps are those of an untuned run (to round-off of the
+    chosen tile shapes, which do not change the arithmetic)."""
+    c = cases.tiny_rectangle()
+    path = c.write(str(tmp_path / c.name))
+    a, ha = _run(c, path, fb.POISSON_TF32X3, 5)
+    s = fb.Solver(path)
+    s.set_poisson(fb.POISSON_TF32X3)
+    q2 = s.get("q2")
+    q2[1:c.n3m + 1] += c.v_perturbation()
+    s.set("q2", q2)
+    tk, bn = s.autotune()
+    assert tk in (32, 64) and bn in (64, 128)
+    hb = s.advance(0, 5)
+    for f in ("q2", "q3"):
+        assert np.array_equal(s.get(f), a[f]), f
+    assert np.array_equal(ha, hb)
+    s.close()
