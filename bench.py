@@ -24,6 +24,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -335,6 +337,32 @@ def batch_arm(args, rank, world, local):
         print(json.dumps(line))
 
 
+def precision_error(fb, path, c, steps):
+    """The precision form against the plain FP64 path (itself within 1e-10
+    per step of the oracle) on the same case and inputs: lift, displacement
+    and post-projection divergence after `steps` steps."""
+    runs = {}
+    for mode in (fb.POISSON_FP64, fb.POISSON_TF32X3):
+        s = fb.Solver(path)
+        s.set_poisson(mode)
+        s.set_report(True)
+        q2 = s.get("q2")
+        q2[1:c.n3m + 1] += c.v_perturbation()
+        s.set("q2", q2)
+        runs[mode] = s.advance(0, steps)
+        s.close()
+    a, b = runs[fb.POISSON_FP64], runs[fb.POISSON_TF32X3]
+    col = {n: fb.HIST_NAMES.index(n) for n in ("Fy", "Fz", "py", "pa", "dmax")}
+    def rel(x, y):
+        return float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300))
+    return {"steps": steps, "lift_rel": rel(b[:, col["Fy"]], a[:, col["Fy"]]),
+            "drag_rel": rel(b[:, col["Fz"]], a[:, col["Fz"]]),
+            "displacement_abs": float(np.max(np.abs(b[:, col["py"]] - a[:, col["py"]]))),
+            "divergence_max_fp64": float(np.max(a[:, col["dmax"]])),
+            "divergence_max_tf32x3": float(np.max(b[:, col["dmax"]])),
+            "reference": "plain FP64 device path (parity with the oracle: 1e-10 per step)"}
+
+
 def device_arm(args, rank, world, local):
     import torch
     import fribois2d_b200 as fb
@@ -451,6 +479,9 @@ def device_arm(args, rank, world, local):
             achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e9
             roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": hbm_src}
+        accuracy = None
+        if args.poisson == "tf32x3":
+            accuracy = precision_error(fb, path, c, steps=50)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             v, steps, threads, secs = cpu_run(args.config, seconds=args.cpu_seconds, max_steps=1000)
@@ -464,7 +495,7 @@ def device_arm(args, rank, world, local):
                        "parallelism": f"replicas x{world}" if world > 1 else "single case",
                        "tiles": {"helsolve_rows": tiles[0], "gemm_cols": tiles[1] if args.poisson == "tf32x3" else None},
                        "l2": "flushed (256 MB write) between timed steps"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "accuracy": accuracy,
             "gpu_launches": per_step_kernels * K, "clocks": clk,
             "fp64_gemm_peak_tflops": peak_fp64,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()} for r in table],

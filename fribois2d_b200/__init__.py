@@ -31,6 +31,7 @@ STATUS = {0: "FB_OK", 1: "FB_ERR_CFL", 2: "FB_ERR_MLS", 3: "FB_ERR_MARKER_OUT",
 FB_ERR_CFL, FB_ERR_MLS, FB_ERR_MARKER_OUT, FB_ERR_INPUT = 1, 2, 3, 4
 FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC, FB_ERR_TIMEOUT = 5, 6, 7, 8, 9
 POISSON_FP64, POISSON_TF32X3 = 0, 1
+COUPLING_LOOSE, COUPLING_STRONG, COUPLING_LEARNED = 0, 1, 2
 
 # array ids (include/fribois2d.h)
 IDS = dict(q2=0, q3=1, pr=2, dph=3, rhs2=7, rhs3=8, ru2=9, ru3=10, qb2s=20, qb2n=21, dqb2s=22,
@@ -45,10 +46,10 @@ BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", 
 STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
               phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17,
               gemm_fwd=100, poisson_tri=101, gemm_bwd=102, tf32x3_gemm=103)
-HIST_COLS = 30
+HIST_COLS = 31
 HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
               "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm", "dt",
-              "cflm_end", "dmax", "ektot", "vorti", "vmax2", "vmax3", "vmin2", "vmin3")
+              "cflm_end", "dmax", "ektot", "vorti", "vmax2", "vmax3", "vmin2", "vmin3", "solves")
 SCALAR_NAMES = ("time", "dt", "dt_o", "beta", "al", "ga", "ro", "cflm", "q3avg", "nbcv", "nbcw",
                 "ddmin", "pravg")
 
@@ -104,6 +105,20 @@ def lib() -> ctypes.CDLL:
         "fb_eigen_tridiag": ([ctypes.c_int, dp, dp, dp, dp, dp, dp], ctypes.c_int),
         "fb_set_poisson": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_set_report": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_set_coupling": ([vp, ctypes.c_int, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+        "fb_set_predictor": ([vp, vp, P(ctypes.c_float)], ctypes.c_int),
+        "fb_coupling_stats": ([vp, dp], ctypes.c_int),
+        "fb_coupling_samples": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int, ip], ctypes.c_int),
+        "fb_mlp_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, P(vp)], ctypes.c_int),
+        "fb_mlp_destroy": ([vp], ctypes.c_int),
+        "fb_mlp_params": ([vp, ip], ctypes.c_int),
+        "fb_mlp_get": ([vp, P(ctypes.c_float)], ctypes.c_int),
+        "fb_mlp_set": ([vp, P(ctypes.c_float)], ctypes.c_int),
+        "fb_mlp_predict": ([vp, P(ctypes.c_float), ctypes.c_int, P(ctypes.c_float)], ctypes.c_int),
+        "fb_mlp_grad": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int, P(ctypes.c_float),
+                         P(ctypes.c_float)], ctypes.c_int),
+        "fb_mlp_train": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
         "fb_batch_create": ([P(vp), ctypes.c_int, P(vp)], ctypes.c_int),
         "fb_batch_advance": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_batch_last_ms": ([vp, dp], ctypes.c_int),
@@ -164,6 +179,68 @@ class HostSetup:
         if name in ("zmm", "zmmt"):
             return out.reshape(self.n3m, self.n3m, order="F")
         return out
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class MLP:
+    """The learned coupling predictor's perceptron (n_in -> 64 -> 64 -> n_out,
+    tanh, FP32), trained and evaluated by the library's own CUDA kernels."""
+
+    def __init__(self, n_in: int = 27, n_out: int = 2, seed: int = 0, device: int = 0):
+        self._lib = lib()
+        self.n_in, self.n_out = n_in, n_out
+        self.m = ctypes.c_void_p()
+        _check(self._lib.fb_mlp_create(int(device), n_in, n_out, int(seed), ctypes.byref(self.m)), "fb_mlp_create")
+        n = ctypes.c_int()
+        _check(self._lib.fb_mlp_params(self.m, ctypes.byref(n)), "fb_mlp_params")
+        self.n_params = n.value
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        _check(self._lib.fb_mlp_get(self.m, _fp(p)), "fb_mlp_get")
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self._lib.fb_mlp_set(self.m, _fp(p)), "fb_mlp_set")
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], self.n_out), dtype=np.float32)
+        _check(self._lib.fb_mlp_predict(self.m, _fp(x), x.shape[0], _fp(y)), "fb_mlp_predict")
+        return y
+
+    def grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(self._lib.fb_mlp_grad(self.m, _fp(x), _fp(t), x.shape[0], _fp(g), ctypes.byref(loss)),
+               "fb_mlp_grad")
+        return g, loss.value
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int = 256, lr: float = 1e-3,
+              seed: int = 0) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(self._lib.fb_mlp_train(self.m, _fp(x), _fp(t), x.shape[0], int(epochs), int(batch), float(lr),
+                                      int(seed), ctypes.byref(loss)), "fb_mlp_train")
+        return loss.value
+
+    def close(self) -> None:
+        if self.m:
+            self._lib.fb_mlp_destroy(self.m)
+            self.m = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:
@@ -358,6 +435,30 @@ class Solver:
         ch = (ctypes.c_int32 * 2)()
         _check(self._lib.fb_autotune(self.ctx, ch), "fb_autotune")
         return int(ch[0]), int(ch[1])
+
+    def set_coupling(self, mode: int, tol: float = 1e-8, max_iter: int = 50) -> None:
+        """COUPLING_LOOSE (the reference), COUPLING_STRONG or COUPLING_LEARNED."""
+        _check(self._lib.fb_set_coupling(self.ctx, int(mode), float(tol), int(max_iter)), "fb_set_coupling")
+
+    def set_predictor(self, mlp, norm) -> None:
+        self._norm = np.ascontiguousarray(norm, dtype=np.float32)
+        _check(self._lib.fb_set_predictor(self.ctx, mlp.m, _fp(self._norm)), "fb_set_predictor")
+        self._mlp = mlp   # keep it alive while the context uses it
+
+    def coupling_stats(self) -> dict:
+        out = np.zeros(4)
+        _check(self._lib.fb_coupling_stats(self.ctx, _dp(out)), "fb_coupling_stats")
+        return {"steps": out[0], "solves": out[1], "unconverged": out[2], "initial_residual": out[3]}
+
+    def coupling_samples(self):
+        n = ctypes.c_int()
+        _check(self._lib.fb_coupling_samples(self.ctx, None, None, 0, ctypes.byref(n)), "fb_coupling_samples")
+        x = np.zeros((n.value, 27), dtype=np.float32)
+        t = np.zeros((n.value, 2), dtype=np.float32)
+        if n.value:
+            _check(self._lib.fb_coupling_samples(self.ctx, _fp(x), _fp(t), n.value, ctypes.byref(n)),
+                   "fb_coupling_samples")
+        return x, t
 
     def set_report(self, on: bool = True) -> None:
         """End-of-step diagnostics of ttime.F90 into history columns 22..29."""

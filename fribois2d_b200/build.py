@@ -27,6 +27,7 @@ UNITS = [
     ("kernels.cu", ["-fmad=false"]),
     ("tri.cu", []),
     ("tc_gemm.cu", []),
+    ("mlp.cu", []),
     ("api.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]

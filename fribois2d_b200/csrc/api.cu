@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +62,21 @@ struct fb_ctx {
     std::vector<std::pair<const int **, size_t>> coef_fixi;
     size_t coef_cap = 0, coef_capi = 0;
     bool vardt = false;       // idtv = .false.: dt from the CFL number every step
+    // strong fluid-structure coupling (fb_set_coupling): mode, test, state
+    int coupling = FB_COUPLING_LOOSE;
+    double ctol = 1e-8;
+    int cmaxit = 50;
+    double omega0 = 0.5;
+    int free_dof = 0;                       // the body coordinate the predictor follows
+    std::vector<std::array<double, 3>> hist_p, hist_v, hist_f;   // converged steps, newest last
+    double stat_steps = 0, stat_solves = 0, stat_maxit = 0, stat_res0 = 0;
+    std::vector<float> samples_x, samples_t;   // (features, targets) of converged steps
+    fb_mlp *mlp = nullptr;
+    std::vector<float> mlp_norm;               // x mean, x std, t mean, t std
+    double *snap = nullptr;                    // device copy of the step's starting state
+    std::vector<std::pair<double *, size_t>> snap_fields, snap_body;  // (device array, doubles)
+    double *fin_d = nullptr, *fin_h = nullptr; // trial load (device, pinned host)
+    double *rd_h = nullptr;                    // pinned read-back: trial state, fluid load, its state
     int tune_tk = 64;         // windowed helsolve tile height (autotuned per grid size)
     int tune_bn = 128;        // 3xTF32 GEMM tile width (autotuned per grid size)
     // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
@@ -902,6 +918,8 @@ int fb_destroy(fb_ctx *c) {
     for (void *p : c->allocs)
         if (p) cudaFree(p);
     if (c->coef_pin) cudaFreeHost(c->coef_pin);
+    if (c->fin_h) cudaFreeHost(c->fin_h);
+    if (c->rd_h) cudaFreeHost(c->rd_h);
     if (c->coef_pini) cudaFreeHost(c->coef_pini);
     if (c->blas) cublasDestroy(c->blas);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -936,11 +954,205 @@ int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
 }
 
 int fb_last_history(fb_ctx *c, double *row);
+int fb_mlp_predict(fb_mlp *m, const float *x, int n, float *y);
+
+namespace {
+
+// ---- strong fluid-structure coupling ----------------------------------------
+// The reference couples explicitly: the fluid step sees the body where the
+// previous rigid update left it.  Here, optionally, each step iterates on the
+// body load F = (Fy, Fz, M): the markers are placed where F moves the body
+// (RK4 with the load frozen, as rigid.F90 integrates), the fluid step runs
+// from the saved start-of-step state, its loads give F', and F is relaxed
+// towards F' with Aitken's dynamic factor until the free coordinate's load
+// changes by at most tol * max(1, |F'|).  The accepted step commits the body
+// with F' exactly as the loose step would.
+
+constexpr int kPredIn = 27, kPredOut = 2, kPredDepth = 8;
+
+int snap_setup(fb_ctx *c) {
+    if (c->snap) return FB_OK;
+    Dev &d = c->d;
+    const size_t nf = static_cast<size_t>(d.NK) * d.P, nb = static_cast<size_t>(d.n2) + 2;
+    c->snap_fields = {{d.q2, nf}, {d.q3, nf}, {d.pr, nf}, {d.ru2, nf}, {d.ru3, nf},
+                      {d.qb2s, nb}, {d.qb2n, nb}, {d.dqb2s, nb}, {d.dqb2n, nb}, {d.qb3s, nb},
+                      {d.qb3n, nb}, {d.dqb3s, nb}, {d.dqb3n, nb}, {d.dq2x2o, nb}, {d.dq3x2o, nb},
+                      {d.scal, static_cast<size_t>(fb::S_COUNT)}};
+    const size_t nm = c->hc.lmcc.size();
+    c->snap_body = {{d.lmcc, nm}, {d.lmvel, nm}, {d.lmacc, nm}, {d.lmnor, nm},
+                    {d.vert, c->hc.vert.size()}, {d.rigid, 18}};
+    size_t total = 0;
+    for (auto &f : c->snap_fields) total += f.second;
+    for (auto &f : c->snap_body) total += f.second;
+    int st;
+    if ((st = dnew(c, &c->snap, total))) return st;
+    if ((st = dnew(c, &c->fin_d, 4))) return st;
+    CK(cudaMallocHost(&c->fin_h, 4 * sizeof(double)));
+    CK(cudaMallocHost(&c->rd_h, 16 * sizeof(double)));
+    return FB_OK;
+}
+
+// copies the listed state into (save) or out of (!save) the snapshot
+int snap_copy(fb_ctx *c, bool save, bool fields, bool body) {
+    size_t off = 0;
+    for (auto &f : c->snap_fields) {
+        if (fields) {
+            double *a = c->snap + off;
+            CK(cudaMemcpyAsync(save ? a : f.first, save ? f.first : a, f.second * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+        }
+        off += f.second;
+    }
+    for (auto &f : c->snap_body) {
+        if (body) {
+            double *a = c->snap + off;
+            CK(cudaMemcpyAsync(save ? a : f.first, save ? f.first : a, f.second * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+        }
+        off += f.second;
+    }
+    return FB_OK;
+}
+
+// features of the learned predictor for the free coordinate q: the last 8
+// displacements, velocities and loads encoded as increments between
+// consecutive steps (newest first), then Re, mass (or inertia) ratio and
+// reduced velocity; needs 9 converged steps
+bool fsi_features(const fb_ctx *c, float *x) {
+    const size_t n = c->hist_p.size();
+    if (n < static_cast<size_t>(kPredDepth) + 1) return false;
+    const int q = c->free_dof;
+    for (int i = 0; i < kPredDepth; ++i) {
+        x[i] = static_cast<float>(c->hist_p[n - 1 - i][q] - c->hist_p[n - 2 - i][q]);
+        x[kPredDepth + i] = static_cast<float>(c->hist_v[n - 1 - i][q] - c->hist_v[n - 2 - i][q]);
+        x[2 * kPredDepth + i] = static_cast<float>(c->hist_f[n - 1 - i][q] - c->hist_f[n - 2 - i][q]);
+    }
+    const fb::Deck &dk = c->hc.deck;
+    const double mass = dk.rbden * (q == 2 ? dk.rba[1] : dk.rba[0]);
+    const double kq = (q == 0) ? dk.kk[0] : (q == 1 ? dk.kk[1] : dk.kk[2]);
+    x[24] = static_cast<float>(1.0 / dk.visc);
+    x[25] = static_cast<float>(dk.rbden);
+    x[26] = static_cast<float>(kq > 0.0 ? 2.0 * M_PI * std::sqrt(mass / kq) : 0.0);
+    return true;
+}
+
+// initial guess of the coupling iteration
+void predict_load(fb_ctx *c, double F[3]) {
+    const size_t n = c->hist_f.size();
+    for (int i = 0; i < 3; ++i) {
+        if (n >= 2) F[i] = 2.0 * c->hist_f[n - 1][static_cast<size_t>(i)] - c->hist_f[n - 2][static_cast<size_t>(i)];
+        else if (n == 1) F[i] = c->hist_f[0][static_cast<size_t>(i)];
+        else F[i] = 0.0;
+    }
+    if (c->coupling != FB_COUPLING_LEARNED || !c->mlp) return;
+    float x[kPredIn], y[kPredOut];
+    if (!fsi_features(c, x)) return;
+    const float *nm = c->mlp_norm.data();
+    for (int i = 0; i < kPredIn; ++i) x[i] = (x[i] - nm[i]) / nm[kPredIn + i];
+    if (fb_mlp_predict(c->mlp, x, 1, y) != FB_OK) return;
+    // the network predicts the correction to the linear extrapolation above
+    const double dF = static_cast<double>(y[1] * nm[2 * kPredIn + kPredOut + 1] + nm[2 * kPredIn + 1]);
+    F[c->free_dof] += dF;
+}
+
+int coupled_step(fb_ctx *c, int ns) {
+    int r;
+    if ((r = snap_setup(c))) return r;
+    if ((r = snap_copy(c, true, true, true))) return r;
+    double F[3], Ff[3] = {0, 0, 0}, res_prev[3] = {0, 0, 0}, omega = c->omega0;
+    predict_load(c, F);
+    const int q = c->free_dof;
+    int it = 0;
+    bool conv = false;
+    for (; it < c->cmaxit && !conv; ++it) {
+        if (it > 0 && (r = snap_copy(c, false, true, true))) return r;
+        for (int i = 0; i < 3; ++i) c->fin_h[i] = F[i];
+        c->fin_h[3] = 0.0;
+        CK(cudaMemcpyAsync(c->fin_d, c->fin_h, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_PLACE, c->fin_d);
+        if ((r = enqueue_fluid(c, ns))) return r;
+        fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_FORCES, nullptr);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->rd_h, c->d.forces + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        int status = 0;
+        if ((r = read_status(c, &status))) return r;
+        if (status) return status;
+        double res[3];
+        for (int i = 0; i < 3; ++i) {
+            Ff[i] = c->rd_h[i];
+            res[i] = Ff[i] - F[i];
+        }
+        if (it == 0) c->stat_res0 += std::fabs(res[q]) / std::max(1.0, std::fabs(Ff[q]));
+        conv = std::fabs(res[q]) <= c->ctol * std::max(1.0, std::fabs(Ff[q]));
+        if (conv) break;
+        if (it > 0) {   // Aitken's factor from the free coordinate's residuals
+            const double dr = res[q] - res_prev[q];
+            if (dr != 0.0) omega = -omega * res_prev[q] / dr;
+        }
+        for (int i = 0; i < 3; ++i) {
+            F[i] = F[i] + omega * res[i];
+            res_prev[i] = res[i];
+        }
+    }
+    const int solves = conv ? it + 1 : it;
+    // accept: body back to the start of the step, then the loose update with F'
+    if ((r = snap_copy(c, false, false, true))) return r;
+    for (int i = 0; i < 3; ++i) c->fin_h[i] = Ff[i];
+    c->fin_h[3] = static_cast<double>(solves);
+    CK(cudaMemcpyAsync(c->fin_d, c->fin_h, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // the loads of the accepted fluid step are those F' came from
+    CK(cudaMemcpyAsync(c->d.forces + 1, c->fin_d, 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_COMMIT, c->fin_d);
+    if ((r = enqueue_report(c))) return r;
+    CK(cudaMemcpyAsync(c->rd_h, c->d.rigid, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    int status = 0;
+    if ((r = read_status(c, &status))) return r;
+    // features of the step just converged, then its targets, for training
+    float x[kPredIn];
+    const bool have_x = fsi_features(c, x);
+    std::array<double, 3> p{c->rd_h[0], c->rd_h[1], c->rd_h[2]}, v{c->rd_h[3], c->rd_h[4], c->rd_h[5]},
+        f{Ff[0], Ff[1], Ff[2]};
+    if (have_x) {   // targets: corrections to the linear extrapolations of p and F
+        const size_t n = c->hist_p.size();
+        c->samples_x.insert(c->samples_x.end(), x, x + kPredIn);
+        c->samples_t.push_back(static_cast<float>(p[q] - (2.0 * c->hist_p[n - 1][q] - c->hist_p[n - 2][q])));
+        c->samples_t.push_back(static_cast<float>(f[q] - (2.0 * c->hist_f[n - 1][q] - c->hist_f[n - 2][q])));
+    }
+    c->hist_p.push_back(p);
+    c->hist_v.push_back(v);
+    c->hist_f.push_back(f);
+    if (c->hist_p.size() > 64) {
+        c->hist_p.erase(c->hist_p.begin());
+        c->hist_v.erase(c->hist_v.begin());
+        c->hist_f.erase(c->hist_f.begin());
+    }
+    c->stat_steps += 1;
+    c->stat_solves += solves;
+    if (!conv) c->stat_maxit += 1;
+    return status;
+}
+
+}  // namespace
 
 int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
     if (!c || nsteps < 0) return FB_ERR_STATE;
     if (!c->d.nlm) return FB_ERR_UNSUPPORTED;
     int r, status = 0, done = 0;
+    if (c->coupling != FB_COUPLING_LOOSE) {   // iterated steps: eager launches
+        c->last_ms = 0.0;
+        for (; done < nsteps; ++done) {
+            CK(cudaEventRecord(c->ev0, c->stream));
+            if ((r = coupled_step(c, ns0 + done))) return r;
+            CK(cudaEventRecord(c->ev1, c->stream));
+            CK(cudaEventSynchronize(c->ev1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            c->last_ms += ms;
+            if (hist && (r = fb_last_history(c, hist + static_cast<size_t>(done) * FB_HIST_COLS))) return r;
+            host_clock(c, 1);
+        }
+        return FB_OK;
+    }
     if (c->vardt) {   // dt changes every step: eager launches, no captured graph
         c->last_ms = 0.0;
         for (; done < nsteps; ++done) {
@@ -1642,6 +1854,68 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
         choice[0] = c->tune_tk;
         choice[1] = c->tune_bn;
     }
+    return FB_OK;
+}
+
+int fb_set_coupling(fb_ctx *c, int mode, double tol, int max_iter) {
+    if (!c || mode < FB_COUPLING_LOOSE || mode > FB_COUPLING_LEARNED || !(tol > 0.0) || max_iter < 1)
+        return FB_ERR_STATE;
+    if (mode != FB_COUPLING_LOOSE && (c->vardt || !c->d.nlm)) return FB_ERR_UNSUPPORTED;
+    if (mode != FB_COUPLING_LOOSE && c->coupling == FB_COUPLING_LOOSE && c->hist_p.empty()) {
+        // seed the predictor's history with the steps already taken (history ring)
+        double step = 0.0;
+        CK(cudaMemcpyAsync(&step, c->d.scal + fb::S_STEP, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        const int done = static_cast<int>(step), take = std::min(done, std::min(64, c->hist_cap));
+        std::vector<double> row(FB_HIST_COLS);
+        for (int i = done - take; i < done; ++i) {
+            CK(cudaMemcpy(row.data(), c->d.hist + static_cast<size_t>(i % c->hist_cap) * FB_HIST_COLS,
+                          FB_HIST_COLS * sizeof(double), cudaMemcpyDeviceToHost));
+            c->hist_p.push_back({row[9], row[10], row[11]});
+            c->hist_v.push_back({row[12], row[13], row[14]});
+            c->hist_f.push_back({row[1], row[2], row[3]});
+        }
+    }
+    c->coupling = mode;
+    c->ctol = tol;
+    c->cmaxit = max_iter;
+    const fb::Deck &dk = c->hc.deck;
+    c->free_dof = 0;
+    for (int i = 0; i < 3; ++i)
+        if (dk.rbmcon[i] == 0) {
+            c->free_dof = i;
+            break;
+        }
+    return FB_OK;
+}
+
+int fb_set_predictor(fb_ctx *c, fb_mlp *m, const float *norm) {
+    if (!c || (m && !norm)) return FB_ERR_STATE;
+    c->mlp = m;
+    c->mlp_norm.assign(norm ? norm : nullptr, norm ? norm + 2 * 27 + 2 * 2 : nullptr);
+    return FB_OK;
+}
+
+int fb_coupling_stats(fb_ctx *c, double out[4]) {
+    if (!c || !out) return FB_ERR_STATE;
+    out[0] = c->stat_steps;
+    out[1] = c->stat_solves;
+    out[2] = c->stat_maxit;
+    out[3] = c->stat_steps > 0 ? c->stat_res0 / c->stat_steps : 0.0;
+    return FB_OK;
+}
+
+int fb_coupling_samples(fb_ctx *c, float *x, float *t, int cap, int *n) {
+    if (!c || !n) return FB_ERR_STATE;
+    const int have = static_cast<int>(c->samples_t.size() / 2);
+    *n = have;
+    if (!x || !t) return FB_OK;
+    const int m = std::min(cap, have);
+    std::memcpy(x, c->samples_x.data(), sizeof(float) * static_cast<size_t>(m) * 27);
+    std::memcpy(t, c->samples_t.data(), sizeof(float) * static_cast<size_t>(m) * 2);
+    c->samples_x.erase(c->samples_x.begin(), c->samples_x.begin() + static_cast<long>(m) * 27);
+    c->samples_t.erase(c->samples_t.begin(), c->samples_t.begin() + static_cast<long>(m) * 2);
+    *n = m;
     return FB_OK;
 }
 

@@ -12,6 +12,7 @@
 
 #include "device.cuh"
 #include "kernels.h"
+#include "pdl.h"
 #include "../../include/fribois2d.h"
 
 namespace fb {
@@ -63,6 +64,7 @@ __device__ double block_reduce_fast(double v, double *sh) {
 // Both reductions (max for the CFL number, sum for the mean w) share one
 // last-block pass so that a single block finalises them.
 __global__ void __launch_bounds__(256) k_cfl(Dev d) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     __shared__ bool last;
     const int t = threadIdx.x, nt = blockDim.x;
@@ -113,6 +115,7 @@ __global__ void __launch_bounds__(256) k_cfl(Dev d) {
 
 // iobcs.F90:5-77 (boucdq): radiative outflow increments + mass-flux correction
 __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     const int n3 = d.n3, n3m = d.n3m;
     double qout = 0.0;
@@ -144,6 +147,7 @@ __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
 // reference's invtr does (ru2 = dph, ru3 = qcap).  q2f/q3f are not stored:
 // the forcing stage forms q + rhs at the few support nodes it reads.
 __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
+    FB_GRID_WAIT();
     const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int n2m = d.n2m, n3m = d.n3m;
@@ -258,6 +262,7 @@ __device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
 
 // lgrdistribution.F90:189-267: nearest nodes per marker and direction
 __global__ void k_lgrdist(Dev d) {
+    FB_GRID_WAIT();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nlm) return;
     {   // empty the support-box buckets this marker filled at the previous step
@@ -410,6 +415,7 @@ __device__ void wkernel(int wfun, double difc, double sdds, double &wc, double &
 // (forcing_MLS.F90:57-94, MLSint.F90:115-166, compute_AB :284-338), and the
 // spreading keys.  One thread per (marker, direction).
 __global__ void k_mls_setup(Dev d) {
+    FB_GRID_WAIT();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * d.nlm) return;
     const int n = t >> 1, idir = (t & 1) + 1;
@@ -477,6 +483,7 @@ __global__ void k_mls_setup(Dev d) {
 // provisional velocity q* = q + rhs (INVTR.F90:147,275) at the support,
 // direct forcing F = (V - u*)/dt and the per-node contributions cl*phi*F.
 __global__ void k_mls_interp(Dev d) {
+    FB_GRID_WAIT();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * d.nlm) return;
     if (*d.status) return;
@@ -518,6 +525,7 @@ __global__ void k_mls_interp(Dev d) {
 // toucher.  Every substep the heads then add their chain's sum fe*dt to rhs
 // (helsolve.F90:22,47).
 __global__ void k_spread_chains(Dev d) {
+    FB_GRID_WAIT();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
     d.chead[g] = 0;
@@ -570,6 +578,7 @@ __global__ void k_spread_chains(Dev d) {
 }
 
 __global__ void k_mls_spread(Dev d) {
+    FB_GRID_WAIT();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
     if (*d.status) return;
@@ -625,6 +634,7 @@ __device__ __forceinline__ void gtts2(const TriDev &f, size_t off, double *b, si
 
 // solve_fluid.F90:110-160 (solq2j): v, y lines of n2 unknowns, k = 1..n3m
 __global__ void k_tri_y2(Dev d, SubDev s) {
+    FB_GRID_WAIT();
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (k > d.n3m) return;
     double *b = d.rhs2 + fidx(d, 1, k);
@@ -637,6 +647,7 @@ __global__ void k_tri_y2(Dev d, SubDev s) {
 // solve_fluid.F90:164-229 (solq2k) then helsolve.F90:32-33: v, z lines of
 // n3m unknowns with the inflow/outflow terms, q2 += x, wall columns zeroed
 __global__ void k_tri_z2(Dev d, SubDev s) {
+    FB_GRID_WAIT();
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (j > d.n2m) return;
     if (j == 1) {
@@ -658,6 +669,7 @@ __global__ void k_tri_z2(Dev d, SubDev s) {
 // solve_fluid.F90:61-104 (solq3j): w, y lines of n2m unknowns, k = 2..n3m
 // (the k = 1 line of the reference is overwritten by solq3k and skipped)
 __global__ void k_tri_y3(Dev d, SubDev s) {
+    FB_GRID_WAIT();
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 2;
     if (k > d.n3m) return;
     double *b = d.rhs3 + fidx(d, 1, k);
@@ -668,6 +680,7 @@ __global__ void k_tri_y3(Dev d, SubDev s) {
 // solve_fluid.F90:233-312 (solq3k): w, z lines of n3 unknowns with
 // Dirichlet end rows, q3 += x, outflow row advanced by dqb3n
 __global__ void k_tri_z3(Dev d, SubDev s) {
+    FB_GRID_WAIT();
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (j > d.n2m) return;
     double *b = d.rhs3 + fidx(d, j, 1);
@@ -684,6 +697,7 @@ __global__ void k_tri_z3(Dev d, SubDev s) {
 
 // divergence.F90:88-115 (divg)
 __global__ void k_divg(Dev d, double usdtal) {
+    FB_GRID_WAIT();
     const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (jc > d.n2m || kc > d.n3m) return;
@@ -695,6 +709,7 @@ __global__ void k_divg(Dev d, double usdtal) {
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
 // partial sums of pr_submean (updvp.F90:320-333)
 __global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double be) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     __shared__ bool last;
     const int t = threadIdx.x, nt = blockDim.x, b = blockIdx.x, nb = gridDim.x;
@@ -741,6 +756,7 @@ __global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double b
 
 // pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
 __global__ void k_submean_boucqt(Dev d) {
+    FB_GRID_WAIT();
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
     const double pravg = d.scal[S_PRAVG];
@@ -861,6 +877,7 @@ __device__ void getpbup_one(const Dev &d, const double *f, const int eul[2][kSD]
 // thread per marker and quantity); the v and w threads also form checkbcs
 // (ckbcs.F90:29-60) with the substep-1 weights.
 __global__ void k_loads_probe(Dev d) {
+    FB_GRID_WAIT();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * d.nlm) return;
     const int n = t / 3, idir = t % 3 + 1;
@@ -911,6 +928,7 @@ __global__ void k_loads_probe(Dev d) {
 // pressure extrapolation (Wang et al. 2019 eq. 20) and wall shear (eq. 26).
 // Also the L2 norms of checkbcs (ckbcs.F90:76-81).  Single block.
 __global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     const double hpr = d.ddmin * d.kprobe, visc = d.visc;
     double sv = 0.0, sw = 0.0;
@@ -997,43 +1015,64 @@ __device__ void modfn(double K[6], const double t[6], const double FF[6], const 
 // rigid.F90:4-138 (rigid) with int_stress :373-464, kinem_RK4 :165-228 /
 // kinem_RK4i :233-299, get_rotmat :142-161, createnorm :468-495; then the
 // clock update of main.F90:92 and one history row.  Single block.
-__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
+// mode RIGID_STEP: the reference's loose coupling (loads -> forces -> RK4 ->
+// markers -> commit).  The strong coupling iteration splits it:
+// RIGID_PLACE moves the markers to the state that the load fin[0..2] (Fy,
+// Fz, M) gives, without committing; RIGID_FORCES integrates the loads of the
+// markers at that new state (moment about the new centre) and evaluates the
+// RK4 update they give into rigid[9..17] only; RIGID_COMMIT is RIGID_STEP
+// with the load fin (markers restored to the start of the step first).
+__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     __shared__ double cm[18];
     __shared__ double rot[4];
     const int tid = threadIdx.x, nt = blockDim.x, nlm = d.nlm;
     double *R = d.rigid;
+    const bool from_loads = (mode == RIGID_STEP || mode == RIGID_FORCES);
     double fyp = 0.0, fzp = 0.0, fyv = 0.0, fzv = 0.0, mom = 0.0;
-    for (int i = tid; i < nlm; i += nt) {
-        const double p = d.press[i], A = d.lmA[i];
-        const double Fp1 = -p * d.lmnor[2 * i] * A, Fp2 = -p * d.lmnor[2 * i + 1] * A;
-        const double Fv1 = d.tau[2 * i] * A, Fv2 = d.tau[2 * i + 1] * A;
-        fyp = fyp + Fp1;
-        fzp = fzp + Fp2;
-        fyv = fyv + Fv1;
-        fzv = fzv + Fv2;
-        const double r1 = d.lmcc[2 * i] - R[0], r2 = d.lmcc[2 * i + 1] - R[1];
-        mom = mom + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
+    if (from_loads) {
+        const double c0 = (mode == RIGID_FORCES) ? R[9] : R[0], c1 = (mode == RIGID_FORCES) ? R[10] : R[1];
+        for (int i = tid; i < nlm; i += nt) {
+            const double p = d.press[i], A = d.lmA[i];
+            const double Fp1 = -p * d.lmnor[2 * i] * A, Fp2 = -p * d.lmnor[2 * i + 1] * A;
+            const double Fv1 = d.tau[2 * i] * A, Fv2 = d.tau[2 * i + 1] * A;
+            fyp = fyp + Fp1;
+            fzp = fzp + Fp2;
+            fyv = fyv + Fv1;
+            fzv = fzv + Fv2;
+            const double r1 = d.lmcc[2 * i] - c0, r2 = d.lmcc[2 * i + 1] - c1;
+            mom = mom + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
+        }
+        fyp = block_reduce_fast<false>(fyp, sh);
+        fzp = block_reduce_fast<false>(fzp, sh);
+        fyv = block_reduce_fast<false>(fyv, sh);
+        fzv = block_reduce_fast<false>(fzv, sh);
+        mom = block_reduce_fast<false>(mom, sh);
     }
-    fyp = block_reduce_fast<false>(fyp, sh);
-    fzp = block_reduce_fast<false>(fzp, sh);
-    fyv = block_reduce_fast<false>(fyv, sh);
-    fzv = block_reduce_fast<false>(fzv, sh);
-    mom = block_reduce_fast<false>(mom, sh);
     if (tid == 0) {
         const double time = d.scal[S_TIME], dt = d.dt;
-        const double fy = fyp + fyv, fz = fzp + fzv;
-        const double g0 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF0;
-        const double g1 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF1;
-        const double Fy = fy + g0, Fz = fz + g1, M = mom;
-        d.forces[0] = time;
-        d.forces[1] = Fy;
-        d.forces[2] = Fz;
-        d.forces[3] = M;
-        d.forces[4] = fyp;
-        d.forces[5] = fzp;
-        d.forces[6] = fyv;
-        d.forces[7] = fzv;
+        double Fy, Fz, M;
+        if (from_loads) {
+            const double fy = fyp + fyv, fz = fzp + fzv;
+            const double g0 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF0;
+            const double g1 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF1;
+            Fy = fy + g0;
+            Fz = fz + g1;
+            M = mom;
+            d.forces[0] = time;
+            d.forces[1] = Fy;
+            d.forces[2] = Fz;
+            d.forces[3] = M;
+            d.forces[4] = fyp;
+            d.forces[5] = fzp;
+            d.forces[6] = fyv;
+            d.forces[7] = fzv;
+        } else {
+            Fy = fin[0];
+            Fz = fin[1];
+            M = fin[2];
+        }
         // explicit RK4 with loads frozen over the stages
         const double csp[3] = {d.cmposi0, d.cmposi1, d.cmroti};
         double xo[6], FF[6] = {0.0, 0.0, 0.0, 0.0, Fz, M}, Mi[3];
@@ -1089,6 +1128,7 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
         for (int i = 0; i < 18; ++i) cm[i] = R[i];
     }
     __syncthreads();
+    if (mode == RIGID_FORCES) return;   // the update the loads give, markers untouched
     const double *P0 = cm, *P1 = cm + 9, *V1 = cm + 12, *A1 = cm + 15;
     for (int i = tid; i < nlm; i += nt) {
         const double rho0 = d.lmcc[2 * i] - P0[0], rho1 = d.lmcc[2 * i + 1] - P0[1];
@@ -1120,6 +1160,7 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
         d.lmnor[2 * i] = c1 / den;
         d.lmnor[2 * i + 1] = c2 / den;
     }
+    if (mode == RIGID_PLACE) return;     // markers at the trial state; nothing committed
     if (tid == 0) {
         for (int i = 0; i < 9; ++i) R[i] = cm[9 + i];
         const double t0 = d.scal[S_TIME];
@@ -1136,6 +1177,7 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
             h[20] = d.scal[S_CFLM];
             h[21] = d.dt;
             for (int i = 22; i < FB_HIST_COLS; ++i) h[i] = 0.0;  // diagnostics, when enabled
+            h[30] = (mode == RIGID_COMMIT) ? fin[3] : 1.0;        // fluid solves this step
         }
         d.scal[S_STEP] = static_cast<double>(row + 1);
     }
@@ -1149,6 +1191,7 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows) {
 // vorticity of getintvort (utils_proc.F90:582-632) at row indz.  Eight block
 // reductions; the last block writes history columns 22..29 of the step.
 __global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
+    FB_GRID_WAIT();
     __shared__ double sh[32];
     __shared__ bool last;
     constexpr int kV = 8, kStride = 2048;  // partial v of block b at red[v * kStride + b]
@@ -1225,56 +1268,56 @@ int stride_blocks(const Dev &d) {
     const long cells = static_cast<long>(d.n2m) * d.n3m;
     return static_cast<int>(std::min<long>((cells + 255) / 256, 148L * 8));
 }
-void launch_cfl(const Dev &d, cudaStream_t s) { k_cfl<<<stride_blocks(d), 256, 0, s>>>(d); }
-void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { k_boucdq<<<1, 1024, 0, s>>>(d, ga, ro); }
+void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(stride_blocks(d)), dim3(256), 0, s, d); }
+void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
 void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s) {
     dim3 b(32, 8);
-    k_nl_rhs<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, al, ga, ro);
+    pdl(k_nl_rhs, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, al, ga, ro);
 }
 void launch_lgrdist(const Dev &d, cudaStream_t s) {
-    if (d.nlm) k_lgrdist<<<(d.nlm + 127) / 128, 128, 0, s>>>(d);
+    if (d.nlm) pdl(k_lgrdist, dim3((d.nlm + 127) / 128), dim3(128), 0, s, d);
 }
 void launch_mls_setup(const Dev &d, cudaStream_t s) {
-    if (d.nlm) k_mls_setup<<<(2 * d.nlm + 63) / 64, 64, 0, s>>>(d);
+    if (d.nlm) pdl(k_mls_setup, dim3((2 * d.nlm + 63) / 64), dim3(64), 0, s, d);
 }
 void launch_mls_interp(const Dev &d, cudaStream_t s) {
-    if (d.nlm) k_mls_interp<<<(2 * d.nlm + 63) / 64, 64, 0, s>>>(d);
+    if (d.nlm) pdl(k_mls_interp, dim3((2 * d.nlm + 63) / 64), dim3(64), 0, s, d);
 }
 void launch_spread_chains(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;
-    if (n) k_spread_chains<<<(n + 127) / 128, 128, 0, s>>>(d);
+    if (n) pdl(k_spread_chains, dim3((n + 127) / 128), dim3(128), 0, s, d);
 }
 void launch_mls_spread(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;
-    if (n) k_mls_spread<<<(n + 127) / 128, 128, 0, s>>>(d);
+    if (n) pdl(k_mls_spread, dim3((n + 127) / 128), dim3(128), 0, s, d);
 }
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s) {
-    k_tri_y2<<<(d.n3m + 63) / 64, 64, 0, s>>>(d, sd);
-    k_tri_z2<<<(d.n2m + 63) / 64, 64, 0, s>>>(d, sd);
-    k_tri_y3<<<(d.n3m + 63) / 64, 64, 0, s>>>(d, sd);
-    k_tri_z3<<<(d.n2m + 63) / 64, 64, 0, s>>>(d, sd);
+    pdl(k_tri_y2, dim3((d.n3m + 63) / 64), dim3(64), 0, s, d, sd);
+    pdl(k_tri_z2, dim3((d.n2m + 63) / 64), dim3(64), 0, s, d, sd);
+    pdl(k_tri_y3, dim3((d.n3m + 63) / 64), dim3(64), 0, s, d, sd);
+    pdl(k_tri_z3, dim3((d.n2m + 63) / 64), dim3(64), 0, s, d, sd);
 }
 void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     dim3 b(32, 8);
-    k_divg<<<grid2(d.n2m, d.n3m, b), b, 0, s>>>(d, usdtal);
+    pdl(k_divg, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, usdtal);
 }
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
-    k_updvp_prcalc<<<stride_blocks(d), 256, 0, s>>>(d, al, be);
+    pdl(k_updvp_prcalc, dim3(stride_blocks(d)), dim3(256), 0, s, d, al, be);
 }
 void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
     dim3 b(32, 8);
-    k_submean_boucqt<<<grid2(d.n2, d.n3 + 1, b), b, 0, s>>>(d);
+    pdl(k_submean_boucqt, dim3(grid2(d.n2, d.n3 + 1, b)), dim3(b), 0, s, d);
 }
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
-    k_loads_probe<<<(3 * d.nlm + 63) / 64, 64, 0, s>>>(d);
-    k_loads_finish<<<1, 256, 0, s>>>(d);
+    pdl(k_loads_probe, dim3((3 * d.nlm + 63) / 64), dim3(64), 0, s, d);
+    pdl(k_loads_finish, dim3(1), dim3(256), 0, s, d);
 }
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
-    k_diag<<<std::min(stride_blocks(d), 2048), 256, 0, s>>>(d, hist_rows);
+    pdl(k_diag, dim3(std::min(stride_blocks(d), 2048)), dim3(256), 0, s, d, hist_rows);
 }
-void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s) {
-    if (d.nlm) k_rigid<<<1, 256, 0, s>>>(d, hist_rows);
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin) {
+    if (d.nlm) pdl(k_rigid, dim3(1), dim3(256), 0, s, d, hist_rows, mode, fin);
 }
 
 }  // namespace fb

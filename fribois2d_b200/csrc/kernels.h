@@ -23,6 +23,7 @@ void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s);
 void launch_loads(const Dev &d, cudaStream_t s);
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s);
-void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s);
+enum RigidMode { RIGID_STEP = 0, RIGID_PLACE = 1, RIGID_FORCES = 2, RIGID_COMMIT = 3 };
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode = RIGID_STEP, const double *fin = nullptr);
 
 }  // namespace fb

@@ -22,6 +22,7 @@
 
 #include "../../include/fribois2d.h"
 #include "device.cuh"
+#include "pdl.h"
 #include "tc_gemm.h"
 
 namespace fb {
@@ -151,6 +152,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_tf32x3_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                   const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
                   GemmOut o, int K, int *status) {
+    FB_GRID_WAIT();
     using Cfg = TcCfg<BN>;
     constexpr int kStages = Cfg::kStages;
     constexpr uint32_t kATile = Cfg::kATile, kBTile = Cfg::kBTile, kStageBytes = Cfg::kStageBytes;
@@ -272,6 +274,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // the transposed split of a column-major FP64 matrix (32 x 32 tiles)
 __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src, long lds, int R, int C,
                                                   float *__restrict__ hi, float *__restrict__ lo, long ldd) {
+    FB_GRID_WAIT();
     __shared__ double t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
@@ -302,6 +305,7 @@ __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src,
 // forward transform reads.  One 32 x 32 tile per block.
 __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *__restrict__ phi, float *__restrict__ hi,
                                                            float *__restrict__ lo, long ldd) {
+    FB_GRID_WAIT();
     __shared__ double t[32][33];
     const int j0 = 1 + blockIdx.x * 32, k0 = 1 + blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *_
 
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st) {
     const dim3 grid((d.n2m + 31) / 32, (d.n3m + 31) / 32);
-    k_poisson_residual<<<grid, 256, 0, st>>>(d, phi, dst.hi, dst.lo, dst.ld);
+    pdl(k_poisson_residual, dim3(grid), dim3(256), 0, st, d, phi, dst.hi, dst.lo, dst.ld);
 }
 
 namespace {
@@ -394,14 +398,14 @@ void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *bas
     GemmOut o{out, ldo, base, ldb, p.M, p.N};
     const dim3 grid((p.M + kBM - 1) / kBM, (p.N + p.bn - 1) / p.bn);
     if (p.bn == 64)
-        k_tf32x3_gemm<64><<<grid, kThreads, TcCfg<64>::kSmem, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+        pdl(k_tf32x3_gemm<64>, dim3(grid), dim3(kThreads), TcCfg<64>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
     else
-        k_tf32x3_gemm<128><<<grid, kThreads, TcCfg<128>::kSmem, st>>>(p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+        pdl(k_tf32x3_gemm<128>, dim3(grid), dim3(kThreads), TcCfg<128>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
 }
 
 void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st) {
     const dim3 grid((R + 31) / 32, (C + 31) / 32);
-    k_split_t<<<grid, 256, 0, st>>>(src, lds, R, C, dst.hi, dst.lo, dst.ld);
+    pdl(k_split_t, dim3(grid), dim3(256), 0, st, src, lds, R, C, dst.hi, dst.lo, dst.ld);
 }
 
 }  // namespace fb

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "device.cuh"
+#include "pdl.h"
 #include "tri.h"
 
 namespace fb {
@@ -308,6 +309,7 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
 template <int M, int kKind>
 __global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSys s2, const double *by2,
                                                                    ScanSys s3, const double *by3) {
+    FB_GRID_WAIT();
     extern __shared__ double sm[];
     __shared__ double shx[kYLines][2 * kYWarps];
     const int wl = (threadIdx.x >> 5) / kYWarps;       // line slot in the block
@@ -383,6 +385,7 @@ __global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSy
 // rest, one launch (the two are independent).  Lines j0..j0+3.
 template <int M, int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb2) {
+    FB_GRID_WAIT();
     __shared__ double shA[16 * kZLines], shC[16 * kZLines];
     const int kKind = (static_cast<int>(blockIdx.x) < nb2) ? 0 : 1;
     const int blk = (kKind == 0) ? blockIdx.x : blockIdx.x - nb2;
@@ -546,6 +549,7 @@ struct WinShape {            // shared-memory layout of one tile of kWTk rows (i
 // blockIdx.x = tile (tj fastest).
 template <int KM, int kWTk>
 __global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
+    FB_GRID_WAIT();
     extern __shared__ double sm[];
     const WinShape<kWTk> sh(Ky, Kz);
     double *A = sm, *B = sm + sh.a_size, *C = B + sh.b_size;
@@ -730,9 +734,9 @@ void ylaunch(const Dev &d, const SubDev *sd, cudaStream_t st) {
     const ScanSys s2 = sd ? sd->sy2 : z, s3 = sd ? sd->sy3 : z;
     const double *b2 = sd ? sd->by2 : nullptr, *b3 = sd ? sd->by3 : nullptr;
     const int threads = kYLines * kYWarps * 32;
-    if (m <= 9) k_ylines<9, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
-    else if (m <= 17) k_ylines<17, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
-    else k_ylines<33, kKind><<<blocks, threads, smem, st>>>(d, s2, b2, s3, b3);
+    if (m <= 9) pdl(k_ylines<9, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
+    else if (m <= 17) pdl(k_ylines<17, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
+    else pdl(k_ylines<33, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
 }
 
 void zlaunch(const Dev &d, const SubDev &sd, cudaStream_t st) {
@@ -742,16 +746,16 @@ void zlaunch(const Dev &d, const SubDev &sd, cudaStream_t st) {
     constexpr int kChunksPerWarp = 32 / kZLines;
     int warps = (n + kChunksPerWarp * 16 - 1) / (kChunksPerWarp * 16);
     if (warps <= 16) {
-        k_zlines<16, 512><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
+        pdl(k_zlines<16, 512>, dim3(blocks), dim3(warps * 32), 0, st, d, sd, nb2);
         return;
     }
     warps = (n + kChunksPerWarp * 32 - 1) / (kChunksPerWarp * 32);
     if (warps <= 10) {
-        k_zlines<32, 320><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
+        pdl(k_zlines<32, 320>, dim3(blocks), dim3(warps * 32), 0, st, d, sd, nb2);
         return;
     }
     warps = (n + kChunksPerWarp * 64 - 1) / (kChunksPerWarp * 64);
-    k_zlines<64, 256><<<blocks, warps * 32, 0, st>>>(d, sd, nb2);
+    pdl(k_zlines<64, 256>, dim3(blocks), dim3(warps * 32), 0, st, d, sd, nb2);
 }
 
 template <class K>
@@ -780,9 +784,9 @@ void win_launch(const Dev &d, const SubDev &s, cudaStream_t st) {
     const WinShape<TK> sh(s.win_y, s.win_z);
     const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
     if (s.win_y <= 12 && s.win_z <= 12)
-        k_helsolve_win<12, TK><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+        pdl(k_helsolve_win<12, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
     else
-        k_helsolve_win<kWinMax, TK><<<grid, kWThreads, smem, st>>>(d, s, ntj, s.win_y, s.win_z);
+        pdl(k_helsolve_win<kWinMax, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
 }
 
 void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {

@@ -40,6 +40,7 @@ extern "C" {
 typedef struct fb_ctx fb_ctx;     /* device context: one case on one GPU */
 typedef struct fb_host fb_host;   /* host-side set-up of one case (no GPU) */
 typedef struct fb_batch fb_batch; /* independent cases stepped together */
+typedef struct fb_mlp fb_mlp;     /* small perceptron: learned coupling predictor */
 
 /* ---- array ids for fb_get_array / fb_set_array / fb_host_array --------- */
 /* fields, (n3+1) x n2 doubles, k = 0..n3 */
@@ -108,8 +109,10 @@ typedef struct fb_batch fb_batch; /* independent cases stepped together */
  *  [18] nbcv [19] nbcw [20] cflm (start of step) [21] dt
  *  with fb_set_report on, the ttime.F90 diagnostics of the end-of-step field
  *  (fluid_rep.out, ttime.F90:142): [22] cflm [23] dmax [24] ektot [25] vorti
- *  [26] vmax(1) [27] vmax(2) [28] vmin(1) [29] vmin(2); zero otherwise */
-#define FB_HIST_COLS 30
+ *  [26] vmax(1) [27] vmax(2) [28] vmin(1) [29] vmin(2); zero otherwise
+ *  [30] fluid solves in the step (1 with loose coupling; the coupling
+ *  iterations with fb_set_coupling) */
+#define FB_HIST_COLS 31
 
 /* ---- stage ids for fb_stage: one per reference subroutine --------------- */
 #define FB_ST_CFL 0        /* cfl.F90 (fluid_tsch.F90:211-258) */
@@ -177,6 +180,45 @@ int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out);
 int fb_batch_advance(fb_batch *b, int nsteps);
 int fb_batch_last_ms(fb_batch *b, double *ms);  /* device time of the last advance */
 int fb_batch_destroy(fb_batch *b);
+
+/* ---- strong fluid-structure coupling and its learned predictor ------------
+ * No counterpart in the reference (its coupling is explicit: FB_COUPLING_LOOSE,
+ * the default).  FB_COUPLING_STRONG iterates each step on the body load
+ * (Fy, Fz, M): markers placed where the load moves the body, fluid step from
+ * the saved start-of-step state, Aitken relaxation towards the fluid's load,
+ * until the free coordinate's load changes by <= tol * max(1, |F|); the
+ * initial guess extrapolates the last two converged loads.
+ * FB_COUPLING_LEARNED takes the initial guess of the free coordinate's load
+ * from a trained fb_mlp (27 features: last 8 displacement increments,
+ * velocities and loads as increments, Re, mass ratio, reduced velocity; 2
+ * outputs: the corrections to the linear extrapolations of the displacement
+ * and the load), standardised with `norm`
+ * (x mean[27], x std[27], t mean[2], t std[2]).  fb_advance runs the
+ * iteration; history column 30 counts the fluid solves of each step.
+ * fb_coupling_samples hands out (features, targets) of converged steps for
+ * training (at most cap; consumed).  Fixed dt only. */
+#define FB_COUPLING_LOOSE 0
+#define FB_COUPLING_STRONG 1
+#define FB_COUPLING_LEARNED 2
+int fb_set_coupling(fb_ctx *ctx, int mode, double tol, int max_iter);
+int fb_set_predictor(fb_ctx *ctx, fb_mlp *mlp, const float *norm);
+/* steps, fluid solves, steps that hit max_iter, mean relative load residual
+ * of the initial guess (the predictor's error as the coupling test sees it) */
+int fb_coupling_stats(fb_ctx *ctx, double out[4]);
+int fb_coupling_samples(fb_ctx *ctx, float *x, float *t, int cap, int *n);
+
+/* The perceptron (n_in -> 64 -> 64 -> n_out, tanh, FP32) with its own CUDA
+ * training (Adam, deterministic block-ordered gradient sums) and inference
+ * kernels.  Host arrays are row-major samples. */
+int fb_mlp_create(int device, int n_in, int n_out, uint64_t seed, fb_mlp **out);
+int fb_mlp_destroy(fb_mlp *m);
+int fb_mlp_params(fb_mlp *m, int *n);
+int fb_mlp_get(fb_mlp *m, float *params);
+int fb_mlp_set(fb_mlp *m, const float *params);
+int fb_mlp_predict(fb_mlp *m, const float *x, int n, float *y);
+int fb_mlp_grad(fb_mlp *m, const float *x, const float *t, int n, float *grad, float *loss);
+int fb_mlp_train(fb_mlp *m, const float *x, const float *t, int n, int epochs, int batch, float lr,
+                 uint64_t seed, float *loss_out);
 
 /* ---- checkpoint / restart --------------------------------------------------
  * The restart set of mpi_write_continua / writeqbns / master_rigid.dat
