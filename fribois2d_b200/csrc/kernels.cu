@@ -206,7 +206,9 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
         }
         const double dcq2 = d22q2 + d33q2;
         const size_t i = fidx(d, jc, kc);
-        d.rhs2[i] = (ga * dph + ro * d.ru2[i] + alre * dcq2 - dpx22) * dt;
+        // the first RK3 substep has ro = 0: ru2 is not read (one field pass less)
+        const double ru = (ro != 0.0) ? d.ru2[i] : 0.0;
+        d.rhs2[i] = (ga * dph + ro * ru + alre * dcq2 - dpx22) * dt;
         d.ru2[i] = dph;
     }
 
@@ -239,7 +241,8 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
         const double dcq3 = dq32 + dq33;
         const double dpx33 = (Fv(pr, jc, kc) - Fv(pr, jc, km)) * udx3;
         const size_t i = fidx(d, jc, kc);
-        d.rhs3[i] = (ga * qcap + ro * d.ru3[i] + alre * dcq3 - dpx33) * dt;
+        const double ru = (ro != 0.0) ? d.ru3[i] : 0.0;
+        d.rhs3[i] = (ga * qcap + ro * ru + alre * dcq3 - dpx33) * dt;
         d.ru3[i] = qcap;
     }
 }

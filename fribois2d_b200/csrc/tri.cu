@@ -478,6 +478,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_zlines(Dev d, SubDev sd, int nb
 // the tile are staged in shared memory with it.
 constexpr int kWTj = 32;        // tile columns (j): one lane each in the z phases
 constexpr int kWSeg = 16;       // values per thread segment
+constexpr int kWSegY = 24;      // values per forward-y segment (2 cover a tile row and its halo)
 constexpr int kWThreads = 256;
 constexpr int kWXp = kWTj + 1;  // row stride of the z right-hand side tile (odd: conflict-free column stores)
 
@@ -527,11 +528,11 @@ struct WinShape {            // shared-memory layout of one tile of kWTk rows (i
     int ncy, ncz;                // staged coefficient counts (y: a e g; z: a e g)
     int a_size, b_size, c_size;  // regions A (rhs, then z rhs), B (y, then z partials), C (coefficients)
     __host__ __device__ WinShape(int Ky, int Kz) {
-        nyf = (kWTj + Ky + kWSeg - 1) / kWSeg;
-        cols = nyf * kWSeg + Ky;  // every forward y segment reads inside its row
+        nyf = (kWTj + Ky + kWSegY - 1) / kWSegY;
+        cols = nyf * kWSegY + Ky;  // every forward y segment reads inside its row
         pitch = cols | 1;
         rows = kWTk + 2 * Kz;
-        ypitch = (nyf * kWSeg) | 1;
+        ypitch = (nyf * kWSegY) | 1;
         nzf = (kWTk + Kz + kWSeg - 1) / kWSeg;
         ncy = cols;
         ncz = nzf * kWSeg + Kz;
@@ -623,20 +624,20 @@ __global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd,
     __syncthreads();
 
     // 2. forward y recurrences: lanes = rows, warps = (row group, segment);
-    //    B[r * ypitch + c] = y at tile column c (j = j0 + c), c < nyf * kWSeg
+    //    B[r * ypitch + c] = y at tile column c (j = j0 + c), c < nyf * kWSegY
     const int nrg = (rows + 31) / 32;
     for (int task = w; task < nrg * sh.nyf; task += kWarps) {
         const int rg = task / sh.nyf, sg = task - rg * sh.nyf;
         const int r = rg * 32 + lane, rr = min(r, rows - 1);
-        const int c0 = Ky + sg * kWSeg;  // coefficient/rhs column of the segment start
+        const int c0 = Ky + sg * kWSegY;  // coefficient/rhs column of the segment start
         const double *arow = A + rr * sh.pitch + c0;
-        const int lo = -(j0 - 1 + sg * kWSeg);  // line index 0 relative to the segment start
-        double y[kWSeg];
-        seg_fwd<kWSeg, KM>([&](int u) { return cya[c0 + u]; }, [&](int u) { return arow[u]; }, Ky, lo,
-                           ny - (j0 - 1 + sg * kWSeg), y);
+        const int lo = -(j0 - 1 + sg * kWSegY);  // line index 0 relative to the segment start
+        double y[kWSegY];
+        seg_fwd<kWSegY, KM>([&](int u) { return cya[c0 + u]; }, [&](int u) { return arow[u]; }, Ky, lo,
+                           ny - (j0 - 1 + sg * kWSegY), y);
         if (r < rows) {
 #pragma unroll
-            for (int t = 0; t < kWSeg; ++t) B[r * sh.ypitch + sg * kWSeg + t] = y[t];
+            for (int t = 0; t < kWSegY; ++t) B[r * sh.ypitch + sg * kWSegY + t] = y[t];
         }
     }
     __syncthreads();
