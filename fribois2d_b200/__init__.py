@@ -39,7 +39,7 @@ IDS = dict(q2=0, q3=1, pr=2, dph=3, rhs2=7, rhs3=8, ru2=9, ru3=10, qb2s=20, qb2n
            zz=42, zm=43, udx2c=48, udx2m=49, udx3c=50, udx3m=51, amphj=64, acphj=65, apphj=66,
            amphk=67, acphk=68, apphk=69, wr=80, zmm=81, zmmt=82, lmcc=90, lmvel=91, lmacc=92,
            lmnor=93, lmA=94, vert=95, phi=96, cl=97, press=98, tau=99, bcerrv=100, bcerrw=101,
-           rigid=110, scalars=111, forces=112)
+           rigid=110, scalars=111, forces=112, hmn=113)
 IIDS = dict(lmind=0, eulins=1)
 FIELDS = ("q2", "q3", "pr", "dph", "rhs2", "rhs3", "ru2", "ru3")
 BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", "dq2x2o", "dq3x2o")
@@ -393,7 +393,7 @@ class Solver:
                 "lmnor": 2 * self.nlm, "lmA": self.nlm, "vert": 2 * (self.nlm + 1),
                 "phi": 18 * self.nlm, "cl": 2 * self.nlm, "press": self.nlm, "tau": 2 * self.nlm,
                 "bcerrv": self.nlm, "bcerrw": self.nlm, "rigid": 18, "scalars": 13,
-                "forces": 8}[name]
+                "forces": 8, "hmn": self.n3m * self.ldh}[name]
 
     def get(self, name: str) -> np.ndarray:
         """Copy of a device array; fields come back as ``(n3+1, n2)``: row k, column j-1."""

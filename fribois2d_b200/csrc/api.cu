@@ -83,6 +83,7 @@ struct fb_ctx {
     // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
     int poisson_mode = FB_POISSON_FP64;
     fb::SplitPlane pl_a{}, pl_a2{}, pl_zt{}, pl_z{};
+    double *zs_d = nullptr, *zsinv_d = nullptr;  // S and S^-1 of zmm = S U (the transforms use U)
     fb::Tf32x3Plan plan_fwd{}, plan_bwd{};
     double *pw = nullptr;
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
@@ -116,13 +117,26 @@ namespace {
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// Device allocations are zeroed and filled on the context stream and waited
+// for: the stream is non-blocking, so work issued on the legacy default
+// stream (cudaMemset, pageable cudaMemcpy, which may return before its DMA
+// lands) would not be ordered before the context's kernels.
 template <class T>
 int dnew(fb_ctx *c, T **p, size_t n) {
     void *q = nullptr;
     CK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
-    CK(cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T)));
     c->allocs.push_back(q);
+    CK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     *p = static_cast<T *>(q);
+    return FB_OK;
+}
+
+// host -> device copy ordered on the context stream and complete on return
+int h2d(fb_ctx *c, void *dst, const void *src, size_t bytes) {
+    if (!bytes) return FB_OK;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return FB_OK;
 }
 
@@ -130,8 +144,7 @@ template <class T>
 int dup(fb_ctx *c, T **p, const std::vector<T> &v) {
     int st = dnew(c, p, v.size());
     if (st) return st;
-    if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-    return FB_OK;
+    return h2d(c, *p, v.data(), v.size() * sizeof(T));
 }
 
 // Smallest K such that every product of K+1 consecutive |c(i)| is at most
@@ -461,7 +474,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         std::vector<double> one(nf, 0.0);
         for (int k = 0; k <= g.n3; ++k)
             for (int j = 1; j <= g.n2; ++j) one[fb::fidx(d, j, k)] = 1.0;
-        CK(cudaMemcpy(d.q3, one.data(), nf * sizeof(double), cudaMemcpyHostToDevice));
+        if ((st = h2d(c, d.q3, one.data(), nf * sizeof(double)))) return st;
     }
     double **bnd[] = {&d.qb2s, &d.qb2n, &d.dqb2s, &d.dqb2n, &d.qb3s, &d.qb3n, &d.dqb3s, &d.dqb3n, &d.dq2x2o, &d.dq3x2o};
     for (double **b : bnd)
@@ -469,8 +482,8 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     {
         std::vector<double> v(static_cast<size_t>(g.n2) + 2, 0.0);
         for (int j = 1; j <= g.n2m; ++j) v[j] = 1.0;
-        CK(cudaMemcpy(d.qb3s, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.qb3n, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        if ((st = h2d(c, d.qb3s, v.data(), v.size() * sizeof(double)))) return st;
+        if ((st = h2d(c, d.qb3n, v.data(), v.size() * sizeof(double)))) return st;
     }
     const size_t nlm = static_cast<size_t>(std::max(d.nlm, 1));
     if ((st = dup(c, &d.lmcc, c->hc.lmcc))) return st;
@@ -497,7 +510,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = dnew(c, &d.bcerrv, nlm))) return st;
     if ((st = dnew(c, &d.bcerrw, nlm))) return st;
     if ((st = dnew(c, &d.rigid, 18))) return st;
-    CK(cudaMemcpy(d.rigid, c->hc.rigid, 18 * sizeof(double), cudaMemcpyHostToDevice));
+    if ((st = h2d(c, d.rigid, c->hc.rigid, 18 * sizeof(double)))) return st;
     if ((st = dnew(c, &d.forces, 8))) return st;
     if ((st = dnew(c, &d.scal, fb::S_COUNT))) return st;
     c->hist_cap = 4096;
@@ -580,16 +593,16 @@ int gemm_bwd(fb_ctx *c) {   // phcalc_outflow.F90:61,65-69, dph = vmn * zmm^T
 int phcalc_tf32(fb_ctx *c) {
     const Dev &d = c->d;
     cudaStream_t st = c->stream;
-    fb::launch_split_t(d.dph + d.P, d.P, d.n2m, d.n3m, c->pl_a, st);
+    fb::launch_split_t(d.dph + d.P, d.P, d.n2m, d.n3m, c->pl_a, st, c->zsinv_d);
     fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
     fb::launch_scan_poisson(d, st);
     fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
-    fb::launch_tf32x3(c->plan_bwd, c->pw + d.P, d.P, nullptr, 0, d.status, st);
-    fb::launch_poisson_residual(d, c->pw, c->pl_a, st);
+    fb::launch_tf32x3(c->plan_bwd, c->pw + d.P, d.P, nullptr, 0, d.status, st, c->zs_d);
+    fb::launch_poisson_residual(d, c->pw, c->pl_a, st, c->zsinv_d);
     fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
     fb::launch_scan_poisson(d, st);
     fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
-    fb::launch_tf32x3(c->plan_bwd, d.dph + d.P, d.P, c->pw + d.P, d.P, d.status, st);
+    fb::launch_tf32x3(c->plan_bwd, d.dph + d.P, d.P, c->pw + d.P, d.P, d.status, st, c->zs_d);
     c->own_launches += 9;
     return FB_OK;
 }
@@ -613,11 +626,33 @@ int setup_tf32(fb_ctx *c) {
         return st;
     double *pw = nullptr;
     if ((st = dnew(c, &pw, static_cast<size_t>(d.NK) * d.P))) return st;
-    // B of the forward transform: zmmt(m, k) as [m][k]; of the backward one: zmm(k, m) as [k][m]
-    fb::launch_split_t(c->zmmt, d.n3m, d.n3m, d.n3m, c->pl_zt, c->stream);
-    fb::launch_split_t(c->zmm, d.n3m, d.n3m, d.n3m, c->pl_z, c->stream);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(c->stream));
+    // zmm = S U with U orthogonal: the tensor cores transform with U, which is
+    // perfectly conditioned, and the diagonal S is applied in FP64 (to the
+    // forward operand and to the backward output)
+    const int n = d.n3m;
+    const std::vector<double> &zs = c->hc.zs;
+    std::vector<double> zinv(static_cast<size_t>(n)), urm(static_cast<size_t>(n) * n), ucm(urm.size());
+    for (int r = 0; r < n; ++r) zinv[static_cast<size_t>(r)] = 1.0 / zs[static_cast<size_t>(r)];
+    for (int col = 0; col < n; ++col)
+        for (int r = 0; r < n; ++r) {
+            const double u = c->hc.zmm[static_cast<size_t>(col) * n + r] / zs[static_cast<size_t>(r)];
+            urm[static_cast<size_t>(r) * n + col] = u;
+            ucm[static_cast<size_t>(col) * n + r] = u;
+        }
+    if ((st = dup(c, &c->zs_d, zs)) || (st = dup(c, &c->zsinv_d, zinv))) return st;
+    double *tmp = nullptr;
+    CK(cudaMalloc(&tmp, 2 * urm.size() * sizeof(double)));
+    if ((st = h2d(c, tmp, urm.data(), urm.size() * sizeof(double))) ||
+        (st = h2d(c, tmp + urm.size(), ucm.data(), ucm.size() * sizeof(double)))) {
+        cudaFree(tmp);
+        return st;
+    }
+    // B of the forward transform: U(k, m) as [m][k]; of the backward one: U(k, m) as [k][m]
+    fb::launch_split_t(tmp, n, n, n, c->pl_zt, c->stream);
+    fb::launch_split_t(tmp + urm.size(), n, n, n, c->pl_z, c->stream);
+    const cudaError_t e1 = cudaGetLastError(), e2 = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return FB_ERR_CUDA;
     if ((st = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, c->tune_bn))) return st;
     if ((st = fb::tf32x3_plan(c->plan_bwd, c->pl_a2, c->pl_z, d.n2m, d.n3m, d.n3m, c->tune_bn))) return st;
     c->pw = pw;
@@ -868,6 +903,7 @@ int vec_ptr(fb_ctx *c, int id, double **p, int64_t *n, bool *one_based) {
     case FB_BCERRW: *p = d.bcerrw; *n = nlm; return FB_OK;
     case FB_RIGID: *p = d.rigid; *n = 18; return FB_OK;
     case FB_FORCES: *p = d.forces; *n = 8; return FB_OK;
+    case FB_HMN: *p = d.hmn; *n = n3m * d.ldh; return FB_OK;
     }
     return FB_ERR_STATE;
 }
@@ -1821,7 +1857,7 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
         }
         if (!r && want_bn && !bn) {
             double best = 1e30;
-            for (int cand : {64, 128}) {
+            for (int cand : {64, 128, fb::kPairTile + 128, fb::kPairTile + 192, fb::kPairTile + 256}) {
                 if ((r = fb::tf32x3_plan(c->plan_fwd, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, cand))) break;
                 double ms = 0.0;
                 if ((r = fb_time_stage(c, FB_TK_TF32X3_GEMM, 1, 10, &ms))) break;
@@ -1930,7 +1966,7 @@ int fb_set_report(fb_ctx *c, int on) {
 }
 
 int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, const double *B, double *C) {
-    if (M < 1 || N < 1 || K < 1 || !A || !B || !C || (bn != 64 && bn != 128)) return FB_ERR_STATE;
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C || !fb::tf32x3_shape_ok(bn)) return FB_ERR_STATE;
     CK(cudaSetDevice(device));
     int st = fb::tf32x3_configure();
     if (st) return st;

@@ -483,7 +483,7 @@ void build_grid(const Deck &d, Grid &g) {
 // the eigenvectors of B are Z = S U and their inverse is U^T S^-1, exactly
 // what phini obtains from DGEEV followed by DGESV.
 int eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr,
-                  double *zmm, double *zmmt) {
+                  double *zmm, double *zmmt, double *zs) {
     std::vector<double> d(ac, ac + n), e(static_cast<size_t>(n), 0.0), s(static_cast<size_t>(n), 1.0);
     for (int i = 0; i + 1 < n; ++i) {
         double up = ap[i], lo = am[i + 1];
@@ -566,6 +566,8 @@ int eigen_tridiag(int n, const double *am, const double *ac, const double *ap, d
             zmmt[static_cast<size_t>(r) * n + c] = u / s[static_cast<size_t>(r)];   // Zinv(c,r)
         }
     }
+    if (zs)
+        for (int r = 0; r < n; ++r) zs[r] = s[static_cast<size_t>(r)];
     for (int i = 0; i < n; ++i)
         if (!std::isfinite(wr[i])) return 3;
     return 0;
@@ -614,7 +616,9 @@ std::string setup_case(const std::string &dir, HostCase &hc) {
     hc.wr.assign(static_cast<size_t>(n3m), 0.0);
     hc.zmm.assign(static_cast<size_t>(n3m) * n3m, 0.0);
     hc.zmmt.assign(static_cast<size_t>(n3m) * n3m, 0.0);
-    if (eigen_tridiag(n3m, am.data(), ac.data(), ap.data(), hc.wr.data(), hc.zmm.data(), hc.zmmt.data()))
+    hc.zs.assign(static_cast<size_t>(n3m), 1.0);
+    if (eigen_tridiag(n3m, am.data(), ac.data(), ap.data(), hc.wr.data(), hc.zmm.data(), hc.zmmt.data(),
+                      hc.zs.data()))
         return "eigen-decomposition of the z Poisson operator failed";
 
     // markers: utils_proc.F90:540-548 then rigid_pre.F90:42-118

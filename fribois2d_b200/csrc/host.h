@@ -64,9 +64,11 @@ void build_grid(const Deck &d, Grid &g);
 
 // Symmetric-tridiagonal eigen-decomposition of the z Poisson operator.
 // am/ac/ap: sub (row i, col i-1), diagonal, super (row i, col i+1), 0-based.
-// zmm: eigenvectors (column-major), zmmt: their inverse.  Returns 0 on success.
+// zmm: eigenvectors (column-major), zmmt: their inverse; zs (may be null):
+// the diagonal S with zmm = S U, zmmt = U^T S^-1, U orthogonal.  Returns 0 on
+// success.
 int eigen_tridiag(int n, const double *am, const double *ac, const double *ap, double *wr,
-                  double *zmm, double *zmmt);
+                  double *zmm, double *zmmt, double *zs = nullptr);
 
 // Everything the device needs for one case.
 struct HostCase {
@@ -74,6 +76,7 @@ struct HostCase {
     Grid grid;
     double gam[3] = {0, 0, 0}, rom[3] = {0, 0, 0}, alm[3] = {0, 0, 0};
     std::vector<double> wr, zmm, zmmt;    // n3m, n3m^2 (column-major)
+    std::vector<double> zs;               // n3m: zmm = diag(zs) U with U orthogonal
     // initial state (inqpr, initial_sol.F90:251-299) and markers after rigid_pre
     std::vector<double> lmcc, lmvel, lmacc, lmnor, lmA, vert;
     double rigid[18] = {0};               // cmp_n, cmv_n, cma_n, cmp_np1, cmv_np1, cma_np1

@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int col = n0 + c * 32 + i;
                 if (col < o.N) {
                     double v = static_cast<double>(__uint_as_float(r[i]));
+                    if (o.cscale) v = o.cscale[col] * v;
                     if (o.base) v = o.base[static_cast<size_t>(col) * o.ldb + row] + v;
                     o.out[static_cast<size_t>(col) * o.ldo + row] = v;
                 }
@@ -270,10 +271,214 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ---- the same product on CTA pairs (tcgen05 cta_group::2) ------------------
+// A cluster of two CTAs computes a 256 x BN tile: CTA r holds rows
+// 128 r .. 128 r + 127 of A and half of B (BN/2 rows) in its shared memory,
+// CTA 0's thread issues tcgen05.mma.cta_group::2 (M = 256, N = BN, K = 8)
+// which reads both halves, and each CTA's TMEM receives its 128 rows.  Both
+// CTAs' TMA loads (no multicast) complete on CTA 0's full barrier; the MMA
+// commits arrive on both CTAs' empty and done barriers.  Per CTA and k-block
+// this loads 32 KB of A and BN/4 KB of B for 12 MMAs: less operand traffic per
+// tensor-core cycle than one CTA per 128 x 128 tile.
+template <int BN>
+struct TcCfg2 {
+    static constexpr int kBH = BN / 2;                                 // B rows per CTA
+    static constexpr uint32_t kATile = kBM * kBK * 4;                  // 16 KB
+    static constexpr uint32_t kBTile = kBH * kBK * 4;
+    static constexpr uint32_t kStageBytes = 2 * kATile + 2 * kBTile;
+    static constexpr int kStages = (kStageBytes * 4 + 2048 <= 227 * 1024) ? 4 : 3;
+    static constexpr uint32_t kTmemCols = BN <= 128 ? 128 : 256;      // power of two >= BN
+    static constexpr size_t kSmem = kStages * kStageBytes + 1024 + 256;
+    static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                                       (static_cast<uint32_t>(BN >> 3) << 17) |
+                                       (static_cast<uint32_t>(256 >> 4) << 24);
+    static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256 && kBH % 8 == 0, "tile widths built");
+    static_assert(kStages * kStageBytes + 1024 + 256 <= 227 * 1024, "shared memory per CTA");
+};
+
+namespace {
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// address of the same shared-memory location in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t addr, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(addr), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, uint32_t bar_cluster, int x,
+                                                 int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                              uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z),
+        "r"(z), "r"(z)
+        : "memory");
+}
+
+// arrives once on the barrier at this shared-memory offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
+    const uint16_t mask = 0x3;
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 ::"r"(bar), "h"(mask)
+                 : "memory");
+}
+
+}  // namespace
+
+template <int BN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    k_tf32x3_gemm2(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+                   const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+                   GemmOut o, int K, int *status) {
+    FB_GRID_WAIT();
+    using Cfg = TcCfg2<BN>;
+    constexpr int kStages = Cfg::kStages;
+    constexpr uint32_t kATile = Cfg::kATile, kBTile = Cfg::kBTile, kStageBytes = Cfg::kStageBytes;
+    constexpr uint32_t kTmemCols = Cfg::kTmemCols, kIdesc = Cfg::kIdesc;
+    extern __shared__ uint8_t smraw[];
+    const uint32_t raw = smem_u32(smraw);
+    const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+    uint8_t *sm = smraw + pad;
+    const uint32_t sbase = raw + pad;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kStages * kStageBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 1);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages), done = smem_u32(bars + 2 * kStages);
+
+    const uint32_t rank = cluster_rank();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pair = blockIdx.x >> 1;
+    const int m0 = pair * 2 * kBM + static_cast<int>(rank) * kBM;   // this CTA's rows of A and C
+    const int n0 = blockIdx.y * BN;                                  // the pair's columns of C
+    const int nb0 = n0 + static_cast<int>(rank) * Cfg::kBH;          // this CTA's rows of B
+    const int nk = (K + kBK - 1) / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync();   // both CTAs' barriers and TMEM exist before either signals the other
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer of this CTA: its A rows and B half land on CTA 0's full barrier
+        int issued = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kStages;
+            const uint32_t ph = static_cast<uint32_t>(kb / kStages) & 1u;
+            if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                ok = false;
+                break;
+            }
+            const uint32_t st = sbase + s * kStageBytes, fb_local = full0 + 8 * s;
+            const uint32_t fb0 = map_to_rank(fb_local, 0);
+            if (rank == 0) mbar_expect_tx(fb_local, 2 * kStageBytes);
+            tma_load_2d_pair(st, &ma_hi, fb0, kb * kBK, m0);
+            tma_load_2d_pair(st + kATile, &ma_lo, fb0, kb * kBK, m0);
+            tma_load_2d_pair(st + 2 * kATile, &mb_hi, fb0, kb * kBK, nb0);
+            tma_load_2d_pair(st + 2 * kATile + kBTile, &mb_lo, fb0, kb * kBK, nb0);
+            issued = kb + 1;
+        }
+        // the copies in flight have been consumed (or landed) before the CTA may finish
+        for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
+            if (!mbar_wait(empty0 + 8 * (kb % kStages), static_cast<uint32_t>(kb / kStages) & 1u)) ok = false;
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---- MMA issuer of the pair
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kStages;
+            const uint32_t ph = static_cast<uint32_t>(kb / kStages) & 1u;
+            if (!mbar_wait(full0 + 8 * s, ph)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t st = sbase + s * kStageBytes;
+#pragma unroll
+            for (int k = 0; k < kBK / 8; ++k) {
+                const uint64_t ahi = sw128_desc(st + 32 * k), alo = sw128_desc(st + kATile + 32 * k);
+                const uint64_t bhi = sw128_desc(st + 2 * kATile + 32 * k);
+                const uint64_t blo = sw128_desc(st + 2 * kATile + kBTile + 32 * k);
+                mma_tf32_pair(tmem, alo, bhi, kIdesc, (kb > 0 || k > 0) ? 1u : 0u);
+                mma_tf32_pair(tmem, ahi, blo, kIdesc, 1u);
+                mma_tf32_pair(tmem, ahi, bhi, kIdesc, 1u);
+            }
+            mma_commit_pair(empty0 + 8 * s);
+        }
+        mma_commit_pair(done);
+    }
+    __syncwarp();
+
+    // ---- epilogue: this CTA's 128 rows of the pair's tile
+    if (!mbar_wait(done, 0)) ok = false;
+    __syncwarp();
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    const bool rok = ok && row < o.M;
+#pragma unroll 1
+    for (int c = 0; c < BN / 32; ++c) {
+        uint32_t r[32];
+        tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c * 32), r);
+        if (rok) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int col = n0 + c * 32 + i;
+                if (col < o.N) {
+                    double v = static_cast<double>(__uint_as_float(r[i]));
+                    if (o.cscale) v = o.cscale[col] * v;
+                    if (o.base) v = o.base[static_cast<size_t>(col) * o.ldb + row] + v;
+                    o.out[static_cast<size_t>(col) * o.ldo + row] = v;
+                }
+            }
+        }
+    }
+    if (!ok) atomicCAS(status, 0, FB_ERR_TIMEOUT);
+    tc_fence_before();
+    cluster_sync();   // neither CTA frees its TMEM or leaves while the pair still uses it
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
 // dst[r * ldd + c] = (hi, lo) TF32 parts of src[c * lds + r], r < R, c < C:
 // the transposed split of a column-major FP64 matrix (32 x 32 tiles)
 __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src, long lds, int R, int C,
-                                                  float *__restrict__ hi, float *__restrict__ lo, long ldd) {
+                                                  float *__restrict__ hi, float *__restrict__ lo, long ldd,
+                                                  const double *__restrict__ cscale) {
     FB_GRID_WAIT();
     __shared__ double t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
@@ -281,7 +486,9 @@ __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src,
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int c = c0 + ty + 8 * i, r = r0 + tx;
-        t[ty + 8 * i][tx] = (r < R && c < C) ? src[static_cast<size_t>(c) * lds + r] : 0.0;
+        double v = (r < R && c < C) ? src[static_cast<size_t>(c) * lds + r] : 0.0;
+        if (cscale && c < C) v = cscale[c] * v;
+        t[ty + 8 * i][tx] = v;
     }
     __syncthreads();
 #pragma unroll
@@ -304,7 +511,8 @@ __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src,
 // phini.F90:59-65), written as the transposed TF32 split [j][k] that the
 // forward transform reads.  One 32 x 32 tile per block.
 __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *__restrict__ phi, float *__restrict__ hi,
-                                                           float *__restrict__ lo, long ldd) {
+                                                           float *__restrict__ lo, long ldd,
+                                                           const double *__restrict__ kscale) {
     FB_GRID_WAIT();
     __shared__ double t[32][33];
     const int j0 = 1 + blockIdx.x * 32, k0 = 1 + blockIdx.y * 32;
@@ -322,6 +530,7 @@ __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *_
             if (k > 1) lp = fma(d.amphk[k], phi[fidx(d, j, k - 1)], lp);
             if (k < d.n3m) lp = fma(d.apphk[k], phi[fidx(d, j, k + 1)], lp);
             r = d.dph[fidx(d, j, k)] - lp;
+            if (kscale) r = kscale[k - 1] * r;
         }
         t[ty + 8 * i][tx] = r;
     }
@@ -339,9 +548,10 @@ __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *_
     }
 }
 
-void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st) {
+void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
+                             const double *kscale) {
     const dim3 grid((d.n2m + 31) / 32, (d.n3m + 31) / 32);
-    pdl(k_poisson_residual, dim3(grid), dim3(256), 0, st, d, phi, dst.hi, dst.lo, dst.ld);
+    pdl(k_poisson_residual, dim3(grid), dim3(256), 0, st, d, phi, dst.hi, dst.lo, dst.ld, kscale);
 }
 
 namespace {
@@ -375,17 +585,29 @@ int tf32x3_configure() {
         cudaFuncSetAttribute(k_tf32x3_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(TcCfg<64>::kSmem)) == cudaSuccess &&
         cudaFuncSetAttribute(k_tf32x3_gemm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(TcCfg<128>::kSmem)) == cudaSuccess;
+                             static_cast<int>(TcCfg<128>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_tf32x3_gemm2<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<128>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_tf32x3_gemm2<192>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<192>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_tf32x3_gemm2<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<256>::kSmem)) == cudaSuccess;
     return ok ? FB_OK : FB_ERR_CUDA;
 }
 
+bool tf32x3_shape_ok(int bn) {
+    return bn == 64 || bn == 128 || bn == kPairTile + 128 || bn == kPairTile + 192 || bn == kPairTile + 256;
+}
+
 int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K, int bn) {
-    if (bn != 64 && bn != 128) return FB_ERR_STATE;
+    if (!tf32x3_shape_ok(bn)) return FB_ERR_STATE;
+    // B boxes: a CTA's tile width, or half the pair's width for CTA pairs
+    const int brows = (bn > kPairTile) ? (bn - kPairTile) / 2 : bn;
     int st;
     if ((st = encode_plane(&p.a_hi, a.hi, M, K, a.ld, kBM))) return st;
     if ((st = encode_plane(&p.a_lo, a.lo, M, K, a.ld, kBM))) return st;
-    if ((st = encode_plane(&p.b_hi, b.hi, N, K, b.ld, bn))) return st;
-    if ((st = encode_plane(&p.b_lo, b.lo, N, K, b.ld, bn))) return st;
+    if ((st = encode_plane(&p.b_hi, b.hi, N, K, b.ld, brows))) return st;
+    if ((st = encode_plane(&p.b_lo, b.lo, N, K, b.ld, brows))) return st;
     p.M = M;
     p.N = N;
     p.K = K;
@@ -394,8 +616,22 @@ int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, 
 }
 
 void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *base, long ldb, int *status,
-                   cudaStream_t st) {
-    GemmOut o{out, ldo, base, ldb, p.M, p.N};
+                   cudaStream_t st, const double *cscale) {
+    GemmOut o{out, ldo, base, ldb, cscale, p.M, p.N};
+    if (p.bn > kPairTile) {   // CTA pairs: 256 rows per cluster of two
+        const int bn = p.bn - kPairTile;
+        const dim3 g2(2 * ((p.M + 2 * kBM - 1) / (2 * kBM)), (p.N + bn - 1) / bn);
+        if (bn == 128)
+            pdl(k_tf32x3_gemm2<128>, g2, dim3(kThreads), TcCfg2<128>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o,
+                p.K, status);
+        else if (bn == 192)
+            pdl(k_tf32x3_gemm2<192>, g2, dim3(kThreads), TcCfg2<192>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o,
+                p.K, status);
+        else
+            pdl(k_tf32x3_gemm2<256>, g2, dim3(kThreads), TcCfg2<256>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o,
+                p.K, status);
+        return;
+    }
     const dim3 grid((p.M + kBM - 1) / kBM, (p.N + p.bn - 1) / p.bn);
     if (p.bn == 64)
         pdl(k_tf32x3_gemm<64>, dim3(grid), dim3(kThreads), TcCfg<64>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
@@ -403,9 +639,10 @@ void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *bas
         pdl(k_tf32x3_gemm<128>, dim3(grid), dim3(kThreads), TcCfg<128>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
 }
 
-void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st) {
+void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st,
+                    const double *cscale) {
     const dim3 grid((R + 31) / 32, (C + 31) / 32);
-    pdl(k_split_t, dim3(grid), dim3(256), 0, st, src, lds, R, C, dst.hi, dst.lo, dst.ld);
+    pdl(k_split_t, dim3(grid), dim3(256), 0, st, src, lds, R, C, dst.hi, dst.lo, dst.ld, cscale);
 }
 
 }  // namespace fb

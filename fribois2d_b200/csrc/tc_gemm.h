@@ -13,25 +13,34 @@ struct SplitPlane {      // TF32 high/low parts of an FP64 matrix: rows x K floa
     long ld;
 };
 
-struct GemmOut {         // out[col * ldo + row] = (base ? base[col * ldb + row] : 0) + C[row][col]
+struct GemmOut {         // out[col * ldo + row] = (base ? base[col * ldb + row] : 0) + cscale[col] C[row][col]
     double *out;
     long ldo;
     const double *base;
     long ldb;
+    const double *cscale;  // per-column factor (null: 1)
     int M, N;
 };
+
+// tile codes: 64 or 128 = one CTA per 128 x code tile; kPairTile + w = a CTA
+// pair (tcgen05 cta_group::2) per 256 x w tile, w = 128, 192 or 256
+constexpr int kPairTile = 1000;
 
 struct Tf32x3Plan {      // tensor maps of one C = A * B^T product
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
     int M, N, K;
-    int bn;              // tile width: 64 or 128 columns of C per CTA
+    int bn;              // tile code (kPairTile above)
 };
 
 int tf32x3_configure();
+bool tf32x3_shape_ok(int bn);
 int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K, int bn);
 void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *base, long ldb, int *status,
-                   cudaStream_t st);
-void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st);
-void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st);
+                   cudaStream_t st, const double *cscale = nullptr);
+// cscale (may be null): factor of source column c before splitting
+void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st,
+                    const double *cscale = nullptr);
+void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
+                             const double *kscale = nullptr);
 
 }  // namespace fb

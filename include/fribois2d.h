@@ -98,6 +98,7 @@ typedef struct fb_mlp fb_mlp;     /* small perceptron: learned coupling predicto
 #define FB_RIGID 110   /* 18: cmp_n, cmv_n, cma_n, cmp_np1, cmv_np1, cma_np1 */
 #define FB_SCALARS 111 /* 13: time, dt, dt_o, beta, al, ga, ro, cflm, q3avg, nbcv, nbcw, ddmin, pravg */
 #define FB_FORCES 112  /* 8: forcecomp.out row: time, Fy, Fz, M, Fyp, Fzp, Fyv, Fzv */
+#define FB_HMN 113     /* n3m x ldh (ldh = dims[5]): Poisson modal work array [mode][j], read only */
 /* integer arrays for fb_get_iarray */
 #define FB_LMIND 0     /* nlm x 2 x 2: nearest node per marker and direction */
 #define FB_EULINS 1    /* nlm x 2 x 2 x 9: MLS support node indices (j, k) */
@@ -269,12 +270,15 @@ int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
 int fb_set_poisson(fb_ctx *ctx, int mode);
 /* C = A * B^T with the 3xTF32 tensor-core kernel: A (M x K) and B (N x K)
  * column-major host arrays, C (M x N) column-major; allocates its own device
- * buffers on `device` (a test and calibration entry point). */
+ * buffers on `device` (a test and calibration entry point).  bn: 64 or 128
+ * (one CTA per 128 x bn tile) or 1000 + w, w = 128, 192, 256 (a CTA pair,
+ * tcgen05 cta_group::2, per 256 x w tile). */
 int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, const double *B, double *C);
 /* Picks tile shapes for this grid size by timing the candidates on the
  * context (state preserved): the windowed helsolve's tile height and, with
- * the precision form on, the tensor-core GEMM's tile width.  Remembered per
- * grid size for the process.  choice (may be NULL) receives {height, width}. */
+ * the precision form on, the tensor-core GEMM's tile (code as fb_gemm_tf32x3's
+ * bn).  Remembered per grid size for the process.  choice (may be NULL)
+ * receives {height, tile code}. */
 int fb_autotune(fb_ctx *ctx, int32_t choice[2]);
 
 /* ---- host-only set-up (no GPU touched; usable on a CPU-only machine) ----- */

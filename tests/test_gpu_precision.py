@@ -20,7 +20,7 @@ from paritylib import rel
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("bn", [64, 128])
+@pytest.mark.parametrize("bn", [64, 128, 1128, 1192, 1256])
 @pytest.mark.parametrize("M,N,K", [(128, 128, 32), (200, 130, 77), (256, 384, 1000), (768, 1024, 1024)])
 def test_tf32x3_gemm_matches_fp64(M, N, K, bn):
     rng = np.random.default_rng(M * 7 + N * 3 + K)
@@ -85,7 +85,7 @@ def test_autotune_keeps_state_and_results(tmp_path):
     q2[1:c.n3m + 1] += c.v_perturbation()
     s.set("q2", q2)
     tk, bn = s.autotune()
-    assert tk in (32, 64) and bn in (64, 128)
+    assert tk in (32, 64) and bn in (64, 128, 1128, 1192, 1256)
     hb = s.advance(0, 5)
     for f in ("q2", "q3"):
         assert np.array_equal(s.get(f), a[f]), f
