@@ -241,6 +241,7 @@ def kernel_table(fb, path, c, poisson="fp64"):
     s = fb.Solver(path)
     if poisson == "tf32x3":
         s.set_poisson(fb.POISSON_TF32X3)
+    s.autotune()   # the tile shapes the timed run uses (remembered per grid size)
     s.advance(0, 2)
     s.set_substep(1, 1)
     cells = c.cells
