@@ -32,6 +32,7 @@ FB_ERR_CFL, FB_ERR_MLS, FB_ERR_MARKER_OUT, FB_ERR_INPUT = 1, 2, 3, 4
 FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC, FB_ERR_TIMEOUT = 5, 6, 7, 8, 9
 POISSON_FP64, POISSON_TF32X3 = 0, 1
 COUPLING_LOOSE, COUPLING_STRONG, COUPLING_LEARNED = 0, 1, 2
+BATCH_GROUPED, BATCH_GRAPH = 0, 1
 
 # array ids (include/fribois2d.h)
 IDS = dict(q2=0, q3=1, pr=2, dph=3, rhs2=7, rhs3=8, ru2=9, ru3=10, qb2s=20, qb2n=21, dqb2s=22,
@@ -120,6 +121,8 @@ def lib() -> ctypes.CDLL:
         "fb_mlp_train": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                           ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
         "fb_batch_create": ([P(vp), ctypes.c_int, P(vp)], ctypes.c_int),
+        "fb_batch_create_mode": ([P(vp), ctypes.c_int, ctypes.c_int, P(vp)], ctypes.c_int),
+        "fb_batch_info": ([vp, P(ctypes.c_int32)], ctypes.c_int),
         "fb_batch_advance": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_batch_last_ms": ([vp, dp], ctypes.c_int),
         "fb_batch_destroy": ([vp], ctypes.c_int),
@@ -245,14 +248,24 @@ class MLP:
 
 class Batch:
     """Independent cases (Solver objects on one device, fixed dt, RK3) advanced
-    together: one CUDA graph launch steps every case (fb_batch_*)."""
+    together by one CUDA graph launch per step (fb_batch_*).  mode
+    BATCH_GROUPED (default): one launch per stage over every group of cases of
+    one launch geometry; BATCH_GRAPH: every case's own captured step on its
+    own graph branch (bitwise equal to stepping it alone)."""
 
-    def __init__(self, solvers):
+    def __init__(self, solvers, mode: int = BATCH_GROUPED):
         self.solvers = list(solvers)
         self._lib = lib()
         arr = (ctypes.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
         self.b = ctypes.c_void_p()
-        _check(self._lib.fb_batch_create(arr, len(self.solvers), ctypes.byref(self.b)), "fb_batch_create")
+        _check(self._lib.fb_batch_create_mode(arr, len(self.solvers), int(mode), ctypes.byref(self.b)),
+               "fb_batch_create_mode")
+
+    def info(self) -> dict:
+        """groups, cases on their own branch, own kernel launches per step."""
+        out = (ctypes.c_int32 * 3)()
+        _check(self._lib.fb_batch_info(self.b, out), "fb_batch_info")
+        return {"groups": out[0], "singles": out[1], "launches": out[2]}
 
     def advance(self, nsteps: int) -> None:
         _check(self._lib.fb_batch_advance(self.b, int(nsteps)), "fb_batch_advance")

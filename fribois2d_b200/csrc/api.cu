@@ -280,6 +280,13 @@ int build_substep(fb_ctx *c, int n, double al) {
         put(c, &s.bz3, std::vector<double>(b.begin(), b.begin() + n3 + 2));
     }
     c->usdtal[n] = 1.0 / (c->dt * al);
+    // the constants grouped launches read from the substep (the single-case
+    // launches take them as arguments): RK3 coefficients, 1/(dt al)
+    s.usdtal = c->usdtal[n];
+    if (c->hc.deck.nsst == 3) {
+        s.ga = c->hc.gam[n];
+        s.ro = c->hc.rom[n];
+    }
     s.scan_ok = !(s.y2.pivoted || s.z2.pivoted || s.y3.pivoted || s.z3.pivoted);
     s.win_y = std::max(wy2, wy3);
     s.win_z = std::max(wz2, wz3);
@@ -1690,23 +1697,242 @@ int fb_set_poisson(fb_ctx *c, int mode) {
 int fb_autotune(fb_ctx *c, int32_t choice[2]);
 
 // ---- batches: independent cases advanced by one graph launch per step
+//
+// FB_BATCH_GROUPED: cases of one launch geometry (grid, marker count,
+// helsolve tile height, options) form a group, and every stage of the step
+// is one launch over the whole group (gridDim.z = cases, the case's view
+// staged from a device array) plus, per transform, one batched cuBLAS DGEMM
+// (FP64) or one grouped 3xTF32 tensor-core launch (precision form, tensor
+// maps of every case in device memory); the groups run on parallel branches
+// of one graph.  Cases that cannot be grouped (line-scan helsolve) run their
+// own captured step on a branch of the same graph.  FB_BATCH_GRAPH: every case runs its own
+// captured step on its own branch (bitwise equal to stepping it alone).
+struct BatchGroup {
+    fb::Group g{};
+    fb::GroupCase *dcases = nullptr;
+    std::vector<fb_ctx *> members;
+    double **ptr = nullptr;     // device: 6 arrays of n pointers (forward A, B, C; backward A, B, C)
+    cublasHandle_t blas = nullptr;
+    void *ws = nullptr;
+    cudaStream_t st = nullptr, side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, done = nullptr;
+    bool cbody = false, report = false;
+    int launches = 0;           // own kernels per step
+    // precision form: the products, splits and residuals of every case
+    bool tf32 = false;
+    fb::Tf32x3Plan plan_fwd{}, plan_bwd{};   // launch geometry (the first case's plans)
+    fb::GemmTask *gt = nullptr;      // 3 x n: forward -> hmn; backward -> pw; backward -> dph (+ pw)
+    fb::SplitTask *sp = nullptr;     // 2 x n: dph S^-1 -> a; hmn -> a2
+    fb::ResidualTask *rt = nullptr;  // n: pw -> a (S^-1)
+};
+
 struct fb_batch {
     std::vector<fb_ctx *> ctx;
     int device = 0;
+    int mode = FB_BATCH_GROUPED;
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> done;
+    std::vector<cudaEvent_t> done;   // per ungrouped case
+    std::vector<fb_ctx *> singles;   // cases stepped by their own captured step
+    std::vector<BatchGroup *> groups;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int *status_h = nullptr;   // pinned: one status per case
     double last_ms = 0.0;
+    int launches = 0;          // own kernels per step
 };
+
+namespace {
+
+void group_free(BatchGroup *bg) {
+    if (!bg) return;
+    if (bg->st) cudaStreamSynchronize(bg->st);
+    if (bg->blas) cublasDestroy(bg->blas);
+    if (bg->ws) cudaFree(bg->ws);
+    if (bg->dcases) cudaFree(bg->dcases);
+    if (bg->ptr) cudaFree(bg->ptr);
+    if (bg->gt) cudaFree(bg->gt);
+    if (bg->sp) cudaFree(bg->sp);
+    if (bg->rt) cudaFree(bg->rt);
+    for (cudaEvent_t e : {bg->fork, bg->join, bg->done})
+        if (e) cudaEventDestroy(e);
+    if (bg->st) cudaStreamDestroy(bg->st);
+    if (bg->side) cudaStreamDestroy(bg->side);
+    delete bg;
+}
+
+// grouped launches need the windowed helsolve in every substep
+bool groupable(const fb_ctx *c) {
+    if (c->hc.deck.nsst != 3) return false;
+    if (c->poisson_mode == FB_POISSON_TF32X3 && !c->pw) return false;
+    for (int n = 0; n < 3; ++n)
+        if (c->sub[n].win_y <= 0 || c->sub[n].win_tk != c->sub[0].win_tk) return false;
+    return true;
+}
+
+// cases that may share launches: same launch geometry and options
+using GroupKey = std::array<int, 11>;
+GroupKey group_key(const fb_ctx *c) {
+    const Dev &d = c->d;
+    const bool tf = c->poisson_mode == FB_POISSON_TF32X3;
+    return {d.n2, d.n3, d.nlm, d.P, d.ldh, d.NK, c->sub[0].win_tk, c->hc.deck.cbody ? 1 : 0,
+            (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0};
+}
+
+// the precision form's task arrays (phcalc_tf32's launches, per case)
+int group_setup_tf32(BatchGroup *bg) {
+    const int n = static_cast<int>(bg->members.size());
+    std::vector<fb::GemmTask> gt(static_cast<size_t>(3 * n));
+    std::vector<fb::SplitTask> sp(static_cast<size_t>(2 * n));
+    std::vector<fb::ResidualTask> rt(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        const fb_ctx *c = bg->members[static_cast<size_t>(i)];
+        const Dev &d = c->d;
+        const size_t k = static_cast<size_t>(i), m = static_cast<size_t>(n);
+        const int M = c->plan_fwd.M, N = c->plan_fwd.N;
+        gt[k] = {c->plan_fwd, fb::GemmOut{d.hmn, d.ldh, nullptr, 0, nullptr, M, N}, d.status};
+        gt[m + k] = {c->plan_bwd, fb::GemmOut{c->pw + d.P, d.P, nullptr, 0, c->zs_d, M, N}, d.status};
+        gt[2 * m + k] = {c->plan_bwd, fb::GemmOut{d.dph + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status};
+        sp[k] = {d.dph + d.P, d.P, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
+        sp[m + k] = {d.hmn, d.ldh, c->pl_a2.hi, c->pl_a2.lo, c->pl_a2.ld, nullptr};
+        rt[k] = {c->pw, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
+    }
+    CK(cudaMalloc(&bg->gt, sizeof(fb::GemmTask) * gt.size()));
+    CK(cudaMalloc(&bg->sp, sizeof(fb::SplitTask) * sp.size()));
+    CK(cudaMalloc(&bg->rt, sizeof(fb::ResidualTask) * rt.size()));
+    CK(cudaMemcpyAsync(bg->gt, gt.data(), sizeof(fb::GemmTask) * gt.size(), cudaMemcpyHostToDevice, bg->st));
+    CK(cudaMemcpyAsync(bg->sp, sp.data(), sizeof(fb::SplitTask) * sp.size(), cudaMemcpyHostToDevice, bg->st));
+    CK(cudaMemcpyAsync(bg->rt, rt.data(), sizeof(fb::ResidualTask) * rt.size(), cudaMemcpyHostToDevice, bg->st));
+    CK(cudaStreamSynchronize(bg->st));
+    bg->plan_fwd = bg->members[0]->plan_fwd;
+    bg->plan_bwd = bg->members[0]->plan_bwd;
+    bg->tf32 = true;
+    return FB_OK;
+}
+
+int group_setup(BatchGroup *bg) {
+    const int n = static_cast<int>(bg->members.size());
+    const fb_ctx *c0 = bg->members[0];
+    CK(cudaStreamCreateWithFlags(&bg->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&bg->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&bg->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&bg->join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&bg->done, cudaEventDisableTiming));
+    std::vector<fb::GroupCase> hc(static_cast<size_t>(n));
+    std::vector<double *> ptr(static_cast<size_t>(6 * n));
+    fb::Group &g = bg->g;
+    g.n = n;
+    g.rep = c0->d;
+    g.win_tk = c0->sub[0].win_tk;
+    for (int k = 0; k < 3; ++k) g.win_ky[k] = g.win_kz[k] = 0;
+    for (int i = 0; i < n; ++i) {
+        const fb_ctx *c = bg->members[static_cast<size_t>(i)];
+        fb::GroupCase &gc = hc[static_cast<size_t>(i)];
+        std::memset(static_cast<void *>(&gc), 0, sizeof(gc));
+        gc.d = c->d;
+        for (int k = 0; k < 3; ++k) {
+            gc.s[k] = c->sub[k];
+            g.win_ky[k] = std::max(g.win_ky[k], c->sub[k].win_y);
+            g.win_kz[k] = std::max(g.win_kz[k], c->sub[k].win_z);
+        }
+        gc.hist_rows = c->hist_cap;
+        const Dev &d = c->d;
+        ptr[static_cast<size_t>(0 * n + i)] = d.dph + d.P;
+        ptr[static_cast<size_t>(1 * n + i)] = c->zmmt;
+        ptr[static_cast<size_t>(2 * n + i)] = d.hmn;
+        ptr[static_cast<size_t>(3 * n + i)] = d.hmn;
+        ptr[static_cast<size_t>(4 * n + i)] = c->zmm;
+        ptr[static_cast<size_t>(5 * n + i)] = d.dph + d.P;
+    }
+    CK(cudaMalloc(&bg->dcases, sizeof(fb::GroupCase) * n));
+    CK(cudaMalloc(&bg->ptr, sizeof(double *) * 6 * n));
+    CK(cudaMemcpyAsync(bg->dcases, hc.data(), sizeof(fb::GroupCase) * n, cudaMemcpyHostToDevice, bg->st));
+    CK(cudaMemcpyAsync(bg->ptr, ptr.data(), sizeof(double *) * 6 * n, cudaMemcpyHostToDevice, bg->st));
+    CK(cudaStreamSynchronize(bg->st));
+    g.cases = bg->dcases;
+    CB(cublasCreate(&bg->blas));
+    CB(cublasSetStream(bg->blas, bg->st));
+    CB(cublasSetPointerMode(bg->blas, CUBLAS_POINTER_MODE_HOST));
+    CK(cudaMalloc(&bg->ws, 32u << 20));
+    CB(cublasSetWorkspace(bg->blas, bg->ws, 32u << 20));
+    bg->cbody = c0->hc.deck.cbody;
+    bg->report = c0->report && c0->d.nlm;
+    if (c0->poisson_mode == FB_POISSON_TF32X3) return group_setup_tf32(bg);
+    return FB_OK;
+}
+
+// one step of a group (fluid_tsch.F90:30-182 + loads + rigid, in the order
+// enqueue_fluid and enqueue_step use), enqueued on the group's stream
+int enqueue_group(BatchGroup *bg) {
+    const fb::Group &g = bg->g;
+    const Dev &d = g.rep;
+    const int n = g.n;
+    cudaStream_t st = bg->st;
+    int k = 0;
+    CK(cudaEventRecord(bg->fork, st));
+    CK(cudaStreamWaitEvent(bg->side, bg->fork, 0));
+    fb::glaunch_marker_setup(g, bg->side);
+    k += 3;
+    CK(cudaEventRecord(bg->join, bg->side));
+    fb::glaunch_cfl(g, st);
+    k += 1;
+    const double one = 1.0, zero = 0.0;
+    double **p = bg->ptr;
+    for (int s = 0; s < 3; ++s) {
+        fb::glaunch_boucdq(g, s, st);
+        fb::glaunch_nl_rhs(g, s, st);
+        if (s == 0) CK(cudaStreamWaitEvent(st, bg->join, 0));
+        fb::glaunch_forcing(g, st);
+        fb::glaunch_win_helsolve(g, s, st);
+        fb::glaunch_divg(g, s, st);
+        if (bg->tf32) {   // phcalc_tf32's launches, each over the whole group
+            fb::launch_split_t_group(bg->sp, d.n2m, d.n3m, n, st);
+            fb::launch_tf32x3_group(bg->gt, bg->plan_fwd, n, st);
+            fb::glaunch_scan_poisson(g, st);
+            fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
+            fb::launch_tf32x3_group(bg->gt + n, bg->plan_bwd, n, st);
+            fb::launch_poisson_residual_group(g, bg->rt, st);
+            fb::launch_tf32x3_group(bg->gt, bg->plan_fwd, n, st);
+            fb::glaunch_scan_poisson(g, st);
+            fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
+            fb::launch_tf32x3_group(bg->gt + 2 * n, bg->plan_bwd, n, st);
+            k += 10;
+        } else {
+            // phcalc_outflow.F90:31,61-69: hmn = dph zmmt^T, dph = vmn zmm^T
+            CB(cublasDgemmBatched(bg->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, p, d.P, p + n,
+                                  d.n3m, &zero, p + 2 * n, d.ldh, n));
+            fb::glaunch_scan_poisson(g, st);
+            CB(cublasDgemmBatched(bg->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, p + 3 * n, d.ldh,
+                                  p + 4 * n, d.n3m, &zero, p + 5 * n, d.P, n));
+            k += 1;
+        }
+        fb::glaunch_updvp_prcalc(g, s, st);
+        fb::glaunch_submean_boucqt(g, st);
+        k += 8;
+    }
+    if (bg->cbody) {
+        fb::glaunch_loads(g, st);
+        k += 2;
+    }
+    fb::glaunch_rigid(g, st);
+    k += 1;
+    if (bg->report) {
+        fb::glaunch_diag(g, st);
+        k += 1;
+    }
+    CK(cudaGetLastError());
+    bg->launches = k;
+    return FB_OK;
+}
+
+}  // namespace
 
 int fb_batch_destroy(fb_batch *b) {
     if (!b) return FB_OK;
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    for (BatchGroup *bg : b->groups) group_free(bg);
     for (cudaEvent_t e : b->done)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
@@ -1718,12 +1944,13 @@ int fb_batch_destroy(fb_batch *b) {
     return FB_OK;
 }
 
-int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
-    if (!ctxs || n < 1 || !out) return FB_ERR_STATE;
+int fb_batch_create_mode(fb_ctx *const *ctxs, int n, int mode, fb_batch **out) {
+    if (!ctxs || n < 1 || !out || (mode != FB_BATCH_GROUPED && mode != FB_BATCH_GRAPH)) return FB_ERR_STATE;
     *out = nullptr;
     fb_batch *b = new (std::nothrow) fb_batch;
     if (!b) return FB_ERR_CUDA;
     b->device = ctxs[0]->device;
+    b->mode = mode;
     for (int i = 0; i < n; ++i) {
         fb_ctx *c = ctxs[i];
         if (!c || c->device != b->device || !c->d.nlm) {
@@ -1734,6 +1961,11 @@ int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
             delete b;
             return FB_ERR_UNSUPPORTED;
         }
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == c) {   // a case may appear once
+                delete b;
+                return FB_ERR_STATE;
+            }
         b->ctx.push_back(c);
     }
     int r = FB_OK;
@@ -1746,27 +1978,56 @@ int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
         cudaMallocHost(&b->status_h, sizeof(int) * n) != cudaSuccess)
         return fail(FB_ERR_CUDA);
-    b->done.assign(static_cast<size_t>(n), nullptr);
-    for (auto &e : b->done)
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(FB_ERR_CUDA);
     for (fb_ctx *c : b->ctx) {   // tile shapes per grid size, then the contexts go quiet
         if ((r = fb_autotune(c, nullptr))) return fail(r);
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(FB_ERR_CUDA);
     }
-    // one step of every case captured from the master stream: each case's
-    // stream forks from it, runs the case's step (its own side branch,
-    // cuBLAS handle and buffers) and joins back
+    // groups in order of first appearance
+    std::map<GroupKey, BatchGroup *> by_key;
+    for (fb_ctx *c : b->ctx) {
+        if (mode != FB_BATCH_GROUPED || !groupable(c)) {
+            b->singles.push_back(c);
+            continue;
+        }
+        const auto key = group_key(c);
+        auto it = by_key.find(key);
+        if (it == by_key.end()) {
+            BatchGroup *bg = new (std::nothrow) BatchGroup;
+            if (!bg) return fail(FB_ERR_CUDA);
+            b->groups.push_back(bg);
+            it = by_key.emplace(key, bg).first;
+        }
+        it->second->members.push_back(c);
+    }
+    for (BatchGroup *bg : b->groups)
+        if ((r = group_setup(bg))) return fail(r);
+    b->done.assign(b->singles.size(), nullptr);
+    for (auto &e : b->done)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(FB_ERR_CUDA);
+    // one step of every group and every ungrouped case captured from the
+    // master stream: each branch forks from it and joins back
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail(FB_ERR_CUDA);
     cudaError_t e = cudaEventRecord(b->fork, b->stream);
-    for (int i = 0; i < n && e == cudaSuccess && !r; ++i) {
-        fb_ctx *c = b->ctx[static_cast<size_t>(i)];
+    b->launches = 0;
+    for (BatchGroup *bg : b->groups) {
+        if (e != cudaSuccess || r) break;
+        e = cudaStreamWaitEvent(bg->st, b->fork, 0);
+        if (e != cudaSuccess) break;
+        r = enqueue_group(bg);
+        b->launches += bg->launches;
+        if (!r) e = cudaEventRecord(bg->done, bg->st);
+        if (!r && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, bg->done, 0);
+    }
+    for (size_t i = 0; i < b->singles.size() && e == cudaSuccess && !r; ++i) {
+        fb_ctx *c = b->singles[i];
         e = cudaStreamWaitEvent(c->stream, b->fork, 0);
         if (e != cudaSuccess) break;
         c->own_launches = 0;
         r = enqueue_step(c, 1);
         c->step_kernels = c->own_launches;
-        if (!r) e = cudaEventRecord(b->done[static_cast<size_t>(i)], c->stream);
-        if (!r && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->done[static_cast<size_t>(i)], 0);
+        b->launches += c->own_launches;
+        if (!r) e = cudaEventRecord(b->done[i], c->stream);
+        if (!r && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->done[i], 0);
     }
     cudaGraph_t g = nullptr;
     const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
@@ -1777,6 +2038,18 @@ int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
     b->graph = g;
     if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return fail(FB_ERR_CUDA);
     *out = b;
+    return FB_OK;
+}
+
+int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out) {
+    return fb_batch_create_mode(ctxs, n, FB_BATCH_GROUPED, out);
+}
+
+int fb_batch_info(fb_batch *b, int32_t info[3]) {
+    if (!b || !info) return FB_ERR_STATE;
+    info[0] = static_cast<int32_t>(b->groups.size());
+    info[1] = static_cast<int32_t>(b->singles.size());
+    info[2] = b->launches;
     return FB_OK;
 }
 

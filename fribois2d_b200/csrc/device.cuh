@@ -76,6 +76,49 @@ struct Dev {
     int rbmcon[3], rtcoup;
 };
 
+// One case of a grouped launch: cases of one launch geometry are stepped by
+// single launches whose blockIdx.z selects the case; each block reads its
+// case's view and substep constants from a device array of these.
+constexpr int kMaxSub = 3;
+struct GroupCase {
+    Dev d;
+    SubDev s[kMaxSub];
+    int hist_rows;
+};
+
+#ifdef __CUDACC__
+// copies case blockIdx.z's view of a group (and the constants of substep n
+// when ss is given) to shared memory, then waits for the preceding kernel
+// (programmatic dependent launch) and the block.  The group array is written
+// once by the host, so the copy may run before the grid dependency wait.
+template <class T>
+__device__ __forceinline__ void copy_words(const T &src, T *dst, int t, int nt) {
+    static_assert(sizeof(T) % 8 == 0, "copied in 8-byte words");
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(&src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+    for (int i = t; i < static_cast<int>(sizeof(T) / 8); i += nt) d[i] = __ldg(s + i);
+}
+__device__ __forceinline__ void stage_case(const GroupCase *__restrict__ g, Dev *sd, SubDev *ss = nullptr,
+                                           int n = 0) {
+    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    copy_words(g[blockIdx.z].d, sd, t, nt);
+    if (ss) copy_words(g[blockIdx.z].s[n], ss, t, nt);
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    __syncthreads();
+}
+#endif
+
+// Host view of a launch group: cases whose launches have one geometry (grid
+// sizes, marker count, helsolve tiles), stepped by launches with gridDim.z = n.
+struct Group {
+    const GroupCase *cases;  // device array of n
+    int n;
+    Dev rep;                 // the first case: launch geometry only
+    int win_tk;              // windowed helsolve tile height
+    int win_ky[kMaxSub], win_kz[kMaxSub];  // largest windows of the group per substep
+};
+
 // device scalar slots
 enum Scal {
     S_TIME = 0, S_CFLM, S_Q3AVG, S_NBCV, S_NBCW, S_PRAVG, S_QOUT, S_DT, S_STEP, S_CFLRAW, S_COUNT

@@ -63,8 +63,7 @@ __device__ double block_reduce_fast(double v, double *sh) {
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
 // Both reductions (max for the CFL number, sum for the mean w) share one
 // last-block pass so that a single block finalises them.
-__global__ void __launch_bounds__(256) k_cfl(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void cfl_body(const Dev &d) {
     __shared__ double sh[32];
     __shared__ bool last;
     const int t = threadIdx.x, nt = blockDim.x;
@@ -111,11 +110,15 @@ __global__ void __launch_bounds__(256) k_cfl(Dev d) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_cfl(Dev d) {
+    FB_GRID_WAIT();
+    cfl_body(d);
+}
+
 // ------------------------------------------------------------ boundaries
 
 // iobcs.F90:5-77 (boucdq): radiative outflow increments + mass-flux correction
-__global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void boucdq_body(const Dev &d, double ga, double ro) {
     __shared__ double sh[32];
     const int n3 = d.n3, n3m = d.n3m;
     double qout = 0.0;
@@ -140,14 +143,18 @@ __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
     for (int j = threadIdx.x + 1; j <= d.n2m; j += blockDim.x) d.dqb3n[j] = d.dqb3n[j] + cor;
 }
 
+__global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
+    FB_GRID_WAIT();
+    boucdq_body(d, ga, ro);
+}
+
 // ------------------------------------------------------------ explicit terms
 
 // HDNL.F90:5-171 (hdnl2, hdnl3) fused with INVTR.F90:4-280 (invtr2, invtr3).
 // The convective terms stay in registers; ru2/ru3 receive them as the
 // reference's invtr does (ru2 = dph, ru3 = qcap).  q2f/q3f are not stored:
 // the forcing stage forms q + rhs at the few support nodes it reads.
-__global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, double ro) {
     const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int n2m = d.n2m, n3m = d.n3m;
@@ -247,6 +254,11 @@ __global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
     }
 }
 
+__global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
+    FB_GRID_WAIT();
+    nl_rhs_body(d, al, ga, ro);
+}
+
 // ------------------------------------------------------------ MLS forcing
 
 __device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
@@ -264,8 +276,7 @@ __device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
 }
 
 // lgrdistribution.F90:189-267: nearest nodes per marker and direction
-__global__ void k_lgrdist(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void lgrdist_body(const Dev &d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nlm) return;
     {   // empty the support-box buckets this marker filled at the previous step
@@ -293,6 +304,11 @@ __global__ void k_lgrdist(Dev d) {
     else ind = nearest_sorted(d.rm, 1, d.n2, y);
     d.lmind[4 * i + 2] = ind;
     d.lmind[4 * i + 3] = nearest_sorted(d.zz, 1, d.n3, z);
+}
+
+__global__ void k_lgrdist(Dev d) {
+    FB_GRID_WAIT();
+    lgrdist_body(d);
 }
 
 // MLSint.F90:4-104 (MLS_SD_ind): 3x3 support moved inside the field.
@@ -417,8 +433,7 @@ __device__ void wkernel(int wfun, double difc, double sdds, double &wc, double &
 // Marker set-up at substep 1: MLS_SD_ind + MLS_SF + momentum coefficient cl
 // (forcing_MLS.F90:57-94, MLSint.F90:115-166, compute_AB :284-338), and the
 // spreading keys.  One thread per (marker, direction).
-__global__ void k_mls_setup(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void mls_setup_body(const Dev &d) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * d.nlm) return;
     const int n = t >> 1, idir = (t & 1) + 1;
@@ -482,11 +497,15 @@ __global__ void k_mls_setup(Dev d) {
     else raise_status(d, FB_ERR_UNSUPPORTED);
 }
 
+__global__ void k_mls_setup(Dev d) {
+    FB_GRID_WAIT();
+    mls_setup_body(d);
+}
+
 // interp_spread (forcing_MLS.F90:135-182), interpolation half: the
 // provisional velocity q* = q + rhs (INVTR.F90:147,275) at the support,
 // direct forcing F = (V - u*)/dt and the per-node contributions cl*phi*F.
-__global__ void k_mls_interp(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void mls_interp_body(const Dev &d) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * d.nlm) return;
     if (*d.status) return;
@@ -520,6 +539,11 @@ __global__ void k_mls_interp(Dev d) {
     for (int m = 0; m < kSD; ++m) c[m] = clv * phi[m] * f;
 }
 
+__global__ void k_mls_interp(Dev d) {
+    FB_GRID_WAIT();
+    mls_interp_body(d);
+}
+
 // interp_spread, spreading half, without atomics on the field.  Once per
 // step (the supports are fixed for the three substeps) every cell's touchers
 // are found in the buckets of the 3 x 3 possible box start cells and chained
@@ -527,8 +551,7 @@ __global__ void k_mls_interp(Dev d) {
 // forcing_MLS.F90:51-104); the head of each chain is the lowest-index
 // toucher.  Every substep the heads then add their chain's sum fe*dt to rhs
 // (helsolve.F90:22,47).
-__global__ void k_spread_chains(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void spread_chains_body(const Dev &d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
     d.chead[g] = 0;
@@ -580,8 +603,12 @@ __global__ void k_spread_chains(Dev d) {
     d.chain[prev_slot] = -1;
 }
 
-__global__ void k_mls_spread(Dev d) {
+__global__ void k_spread_chains(Dev d) {
     FB_GRID_WAIT();
+    spread_chains_body(d);
+}
+
+__device__ __forceinline__ void mls_spread_body(const Dev &d) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 2 * d.nlm * kSD) return;
     if (*d.status) return;
@@ -594,6 +621,11 @@ __global__ void k_mls_spread(Dev d) {
     double *r = (dir == 0) ? d.rhs2 : d.rhs3;
     const size_t i = fidx(d, eu[m], eu[kSD + m]);
     r[i] = r[i] + fe * d.dt;
+}
+
+__global__ void k_mls_spread(Dev d) {
+    FB_GRID_WAIT();
+    mls_spread_body(d);
 }
 
 // ------------------------------------------------------------ tridiagonal
@@ -699,8 +731,7 @@ __global__ void k_tri_z3(Dev d, SubDev s) {
 // ------------------------------------------------------------ Poisson
 
 // divergence.F90:88-115 (divg)
-__global__ void k_divg(Dev d, double usdtal) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void divg_body(const Dev &d, double usdtal) {
     const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (jc > d.n2m || kc > d.n3m) return;
@@ -709,10 +740,14 @@ __global__ void k_divg(Dev d, double usdtal) {
     Fv(d.dph, jc, kc) = dqcap * usdtal;
 }
 
+__global__ void k_divg(Dev d, double usdtal) {
+    FB_GRID_WAIT();
+    divg_body(d, usdtal);
+}
+
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
 // partial sums of pr_submean (updvp.F90:320-333)
-__global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double be) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be) {
     __shared__ double sh[32];
     __shared__ bool last;
     const int t = threadIdx.x, nt = blockDim.x, b = blockIdx.x, nb = gridDim.x;
@@ -757,9 +792,13 @@ __global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double b
     }
 }
 
-// pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
-__global__ void k_submean_boucqt(Dev d) {
+__global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double be) {
     FB_GRID_WAIT();
+    updvp_prcalc_body(d, al, be);
+}
+
+// pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
+__device__ __forceinline__ void submean_boucqt_body(const Dev &d) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
     const double pravg = d.scal[S_PRAVG];
@@ -770,6 +809,11 @@ __global__ void k_submean_boucqt(Dev d) {
         d.qb2n[j] = d.qb2n[j] + d.dqb2n[j];
         d.qb3n[j] = d.qb3n[j] + d.dqb3n[j];
     }
+}
+
+__global__ void k_submean_boucqt(Dev d) {
+    FB_GRID_WAIT();
+    submean_boucqt_body(d);
 }
 
 // ------------------------------------------------------------ loads
@@ -879,8 +923,7 @@ __device__ void getpbup_one(const Dev &d, const double *f, const int eul[2][kSD]
 // probe interpolation of v, w or p with first and second derivatives (one
 // thread per marker and quantity); the v and w threads also form checkbcs
 // (ckbcs.F90:29-60) with the substep-1 weights.
-__global__ void k_loads_probe(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void loads_probe_body(const Dev &d) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * d.nlm) return;
     const int n = t / 3, idir = t % 3 + 1;
@@ -926,12 +969,16 @@ __global__ void k_loads_probe(Dev d) {
     for (int i = 0; i < 7; ++i) pb[7 * (idir - 1) + i] = res[i];
 }
 
+__global__ void k_loads_probe(Dev d) {
+    FB_GRID_WAIT();
+    loads_probe_body(d);
+}
+
 // loads_transfer_c (loads_transfer.F90:187-214): the tangent carries over
 // from the previous marker when the probe's tangential velocity vanishes;
 // pressure extrapolation (Wang et al. 2019 eq. 20) and wall shear (eq. 26).
 // Also the L2 norms of checkbcs (ckbcs.F90:76-81).  Single block.
-__global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void loads_finish_body(const Dev &d) {
     __shared__ double sh[32];
     const double hpr = d.ddmin * d.kprobe, visc = d.visc;
     double sv = 0.0, sw = 0.0;
@@ -1002,6 +1049,11 @@ __global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
+    FB_GRID_WAIT();
+    loads_finish_body(d);
+}
+
 // ------------------------------------------------------------ rigid body
 
 // rigid.F90:341-369 (modfn) for the uncoupled 3-DOF system
@@ -1025,8 +1077,7 @@ __device__ void modfn(double K[6], const double t[6], const double FF[6], const 
 // markers at that new state (moment about the new centre) and evaluates the
 // RK4 update they give into rigid[9..17] only; RIGID_COMMIT is RIGID_STEP
 // with the load fin (markers restored to the start of the step first).
-__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode, const double *fin) {
     __shared__ double sh[32];
     __shared__ double cm[18];
     __shared__ double rot[4];
@@ -1186,6 +1237,11 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, c
     }
 }
 
+__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
+    FB_GRID_WAIT();
+    rigid_body(d, hist_rows, mode, fin);
+}
+
 // ------------------------------------------------------------ diagnostics
 
 // ttime.F90:24-147: diagnostics of the end-of-step field for the fluid report
@@ -1193,8 +1249,7 @@ __global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, c
 // divgck (divergence.F90:49-82), kinen (utils_proc.F90:474-515) and the line
 // vorticity of getintvort (utils_proc.F90:582-632) at row indz.  Eight block
 // reductions; the last block writes history columns 22..29 of the step.
-__global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void diag_body(const Dev &d, int hist_rows) {
     __shared__ double sh[32];
     __shared__ bool last;
     constexpr int kV = 8, kStride = 2048;  // partial v of block b at red[v * kStride + b]
@@ -1261,6 +1316,112 @@ __global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
+    FB_GRID_WAIT();
+    diag_body(d, hist_rows);
+}
+
+// ------------------------------------------------------------ grouped launches
+
+// The same kernels over a group of cases of one launch geometry: blockIdx.z
+// selects the case; its view (and substep n's constants, n 0-based) are
+// staged in shared memory from the group's device array (the single-case
+// kernels take them by value).
+
+__global__ void __launch_bounds__(256) kg_cfl(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    cfl_body(d);
+}
+
+__global__ void __launch_bounds__(1024) kg_boucdq(const GroupCase *__restrict__ g, int n) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    boucdq_body(d, s.ga, s.ro);
+}
+
+__global__ void kg_nl_rhs(const GroupCase *__restrict__ g, int n) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    nl_rhs_body(d, s.al, s.ga, s.ro);
+}
+
+__global__ void kg_lgrdist(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    lgrdist_body(d);
+}
+
+__global__ void kg_mls_setup(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    mls_setup_body(d);
+}
+
+__global__ void kg_spread_chains(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    spread_chains_body(d);
+}
+
+__global__ void kg_mls_interp(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    mls_interp_body(d);
+}
+
+__global__ void kg_mls_spread(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    mls_spread_body(d);
+}
+
+__global__ void kg_divg(const GroupCase *__restrict__ g, int n) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    divg_body(d, s.usdtal);
+}
+
+__global__ void __launch_bounds__(256) kg_updvp_prcalc(const GroupCase *__restrict__ g, int n) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    updvp_prcalc_body(d, s.al, s.al * s.beta);
+}
+
+__global__ void kg_submean_boucqt(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    submean_boucqt_body(d);
+}
+
+__global__ void kg_loads_probe(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    loads_probe_body(d);
+}
+
+__global__ void __launch_bounds__(256) kg_loads_finish(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    loads_finish_body(d);
+}
+
+__global__ void __launch_bounds__(256) kg_rigid(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    rigid_body(d, g[blockIdx.z].hist_rows, RIGID_STEP, nullptr);
+}
+
+__global__ void __launch_bounds__(256) kg_diag(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    diag_body(d, g[blockIdx.z].hist_rows);
+}
+
 // ------------------------------------------------------------ launchers
 
 namespace {
@@ -1321,6 +1482,59 @@ void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
 }
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin) {
     if (d.nlm) pdl(k_rigid, dim3(1), dim3(256), 0, s, d, hist_rows, mode, fin);
+}
+
+
+// grouped launchers: the geometry of the group's first case, gridDim.z = cases
+namespace {
+inline dim3 zgrid(dim3 g, const Group &gr) { return dim3(g.x, g.y, static_cast<unsigned>(gr.n)); }
+}  // namespace
+
+void glaunch_cfl(const Group &g, cudaStream_t s) {
+    pdl(kg_cfl, zgrid(dim3(stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases);
+}
+void glaunch_boucdq(const Group &g, int n, cudaStream_t s) {
+    pdl(kg_boucdq, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases, n);
+}
+void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s) {
+    dim3 b(32, 8);
+    pdl(kg_nl_rhs, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
+}
+void glaunch_marker_setup(const Group &g, cudaStream_t s) {
+    const Dev &d = g.rep;
+    if (!d.nlm) return;
+    pdl(kg_lgrdist, zgrid(dim3((d.nlm + 127) / 128), g), dim3(128), 0, s, g.cases);
+    pdl(kg_mls_setup, zgrid(dim3((2 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
+    pdl(kg_spread_chains, zgrid(dim3((2 * d.nlm * kSD + 127) / 128), g), dim3(128), 0, s, g.cases);
+}
+void glaunch_forcing(const Group &g, cudaStream_t s) {
+    const Dev &d = g.rep;
+    if (!d.nlm) return;
+    pdl(kg_mls_interp, zgrid(dim3((2 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
+    pdl(kg_mls_spread, zgrid(dim3((2 * d.nlm * kSD + 127) / 128), g), dim3(128), 0, s, g.cases);
+}
+void glaunch_divg(const Group &g, int n, cudaStream_t s) {
+    dim3 b(32, 8);
+    pdl(kg_divg, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
+}
+void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s) {
+    pdl(kg_updvp_prcalc, zgrid(dim3(stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases, n);
+}
+void glaunch_submean_boucqt(const Group &g, cudaStream_t s) {
+    dim3 b(32, 8);
+    pdl(kg_submean_boucqt, zgrid(grid2(g.rep.n2, g.rep.n3 + 1, b), g), dim3(b), 0, s, g.cases);
+}
+void glaunch_loads(const Group &g, cudaStream_t s) {
+    const Dev &d = g.rep;
+    if (!d.nlm) return;
+    pdl(kg_loads_probe, zgrid(dim3((3 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
+    pdl(kg_loads_finish, zgrid(dim3(1), g), dim3(256), 0, s, g.cases);
+}
+void glaunch_rigid(const Group &g, cudaStream_t s) {
+    if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(256), 0, s, g.cases);
+}
+void glaunch_diag(const Group &g, cudaStream_t s) {
+    pdl(kg_diag, zgrid(dim3(std::min(stride_blocks(g.rep), 2048)), g), dim3(256), 0, s, g.cases);
 }
 
 }  // namespace fb

@@ -26,4 +26,17 @@ void launch_diag(const Dev &d, int hist_rows, cudaStream_t s);
 enum RigidMode { RIGID_STEP = 0, RIGID_PLACE = 1, RIGID_FORCES = 2, RIGID_COMMIT = 3 };
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode = RIGID_STEP, const double *fin = nullptr);
 
+// grouped forms (one launch over a group of cases; substep n 0-based)
+void glaunch_cfl(const Group &g, cudaStream_t s);
+void glaunch_boucdq(const Group &g, int n, cudaStream_t s);
+void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s);
+void glaunch_marker_setup(const Group &g, cudaStream_t s);   // lgrdist, MLS weights, spreading chains
+void glaunch_forcing(const Group &g, cudaStream_t s);        // interpolation and spreading
+void glaunch_divg(const Group &g, int n, cudaStream_t s);
+void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s);
+void glaunch_submean_boucqt(const Group &g, cudaStream_t s);
+void glaunch_loads(const Group &g, cudaStream_t s);
+void glaunch_rigid(const Group &g, cudaStream_t s);
+void glaunch_diag(const Group &g, cudaStream_t s);
+
 }  // namespace fb

@@ -3,7 +3,9 @@
 // kernel before them drains; each such kernel starts with FB_GRID_WAIT, which
 // returns once the preceding grid has completed and its writes are visible.
 // Every kernel that this header launches waits before its first access to
-// global memory, so ordering is the stream's as without the attribute.
+// global memory that earlier kernels write (grouped kernels first stage their
+// case's view, which only the host writes), so ordering is the stream's as
+// without the attribute.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -95,6 +95,16 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// tensor maps that the host copied into global memory: make the generic-proxy
+// writes visible to the tensor-map proxy before the first TMA copy uses them
+__device__ __forceinline__ void acquire_maps(const CUtensorMap *a, const CUtensorMap *b, const CUtensorMap *c,
+                                             const CUtensorMap *d) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(a) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(b) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(c) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(d) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -147,12 +157,12 @@ __device__ __forceinline__ float tf32_round(float x) {
 
 }  // namespace
 
-template <int BN>
-__global__ void __launch_bounds__(kThreads, 1)
-    k_tf32x3_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
-                  const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
-                  GemmOut o, int K, int *status) {
-    FB_GRID_WAIT();
+// The kernel bodies take the tensor maps by address: kernel parameters for a
+// single product, a task array in global memory for grouped products (whose
+// maps the producer thread acquires for the tensor-map proxy first).
+template <int BN, bool kGlobalMaps>
+__device__ __forceinline__ void gemm_body(const CUtensorMap *ma_hi, const CUtensorMap *ma_lo, const CUtensorMap *mb_hi,
+                                          const CUtensorMap *mb_lo, const GemmOut &o, int K, int *status) {
     using Cfg = TcCfg<BN>;
     constexpr int kStages = Cfg::kStages;
     constexpr uint32_t kATile = Cfg::kATile, kBTile = Cfg::kBTile, kStageBytes = Cfg::kStageBytes;
@@ -194,6 +204,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     bool ok = true;
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
+        if (kGlobalMaps) acquire_maps(ma_hi, ma_lo, mb_hi, mb_lo);
         int issued = 0;
         for (int kb = 0; kb < nk; ++kb) {
             const int s = kb % kStages;
@@ -204,10 +215,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             const uint32_t st = sbase + s * kStageBytes, fb = full0 + 8 * s;
             mbar_expect_tx(fb, kStageBytes);
-            tma_load_2d(st, &ma_hi, fb, kb * kBK, m0);
-            tma_load_2d(st + kATile, &ma_lo, fb, kb * kBK, m0);
-            tma_load_2d(st + 2 * kATile, &mb_hi, fb, kb * kBK, n0);
-            tma_load_2d(st + 2 * kATile + kBTile, &mb_lo, fb, kb * kBK, n0);
+            tma_load_2d(st, ma_hi, fb, kb * kBK, m0);
+            tma_load_2d(st + kATile, ma_lo, fb, kb * kBK, m0);
+            tma_load_2d(st + 2 * kATile, mb_hi, fb, kb * kBK, n0);
+            tma_load_2d(st + 2 * kATile + kBTile, mb_lo, fb, kb * kBK, n0);
             issued = kb + 1;
         }
         // every copy issued has landed before the CTA may finish
@@ -269,6 +280,24 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
                      : "memory");
     }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tf32x3_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+                  const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+                  GemmOut o, int K, int *status) {
+    FB_GRID_WAIT();
+    gemm_body<BN, false>(&ma_hi, &ma_lo, &mb_hi, &mb_lo, o, K, status);
+}
+
+// grouped: blockIdx.z selects the product
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1) kg_tf32x3_gemm(const GemmTask *__restrict__ t) {
+    FB_GRID_WAIT();
+    const GemmTask &tk = t[blockIdx.z];
+    const GemmOut o = tk.o;
+    gemm_body<BN, true>(&tk.p.a_hi, &tk.p.a_lo, &tk.p.b_hi, &tk.p.b_lo, o, tk.p.K, tk.status);
 }
 
 // ---- the same product on CTA pairs (tcgen05 cta_group::2) ------------------
@@ -346,12 +375,9 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
 
 }  // namespace
 
-template <int BN>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-    k_tf32x3_gemm2(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
-                   const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
-                   GemmOut o, int K, int *status) {
-    FB_GRID_WAIT();
+template <int BN, bool kGlobalMaps>
+__device__ __forceinline__ void gemm2_body(const CUtensorMap *ma_hi, const CUtensorMap *ma_lo, const CUtensorMap *mb_hi,
+                                           const CUtensorMap *mb_lo, const GemmOut &o, int K, int *status) {
     using Cfg = TcCfg2<BN>;
     constexpr int kStages = Cfg::kStages;
     constexpr uint32_t kATile = Cfg::kATile, kBTile = Cfg::kBTile, kStageBytes = Cfg::kStageBytes;
@@ -396,6 +422,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     bool ok = true;
     if (warp == 0 && lane == 0) {
         // ---- TMA producer of this CTA: its A rows and B half land on CTA 0's full barrier
+        if (kGlobalMaps) acquire_maps(ma_hi, ma_lo, mb_hi, mb_lo);
         int issued = 0;
         for (int kb = 0; kb < nk; ++kb) {
             const int s = kb % kStages;
@@ -407,10 +434,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             const uint32_t st = sbase + s * kStageBytes, fb_local = full0 + 8 * s;
             const uint32_t fb0 = map_to_rank(fb_local, 0);
             if (rank == 0) mbar_expect_tx(fb_local, 2 * kStageBytes);
-            tma_load_2d_pair(st, &ma_hi, fb0, kb * kBK, m0);
-            tma_load_2d_pair(st + kATile, &ma_lo, fb0, kb * kBK, m0);
-            tma_load_2d_pair(st + 2 * kATile, &mb_hi, fb0, kb * kBK, nb0);
-            tma_load_2d_pair(st + 2 * kATile + kBTile, &mb_lo, fb0, kb * kBK, nb0);
+            tma_load_2d_pair(st, ma_hi, fb0, kb * kBK, m0);
+            tma_load_2d_pair(st + kATile, ma_lo, fb0, kb * kBK, m0);
+            tma_load_2d_pair(st + 2 * kATile, mb_hi, fb0, kb * kBK, nb0);
+            tma_load_2d_pair(st + 2 * kATile + kBTile, mb_lo, fb0, kb * kBK, nb0);
             issued = kb + 1;
         }
         // the copies in flight have been consumed (or landed) before the CTA may finish
@@ -474,12 +501,29 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     }
 }
 
+template <int BN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    k_tf32x3_gemm2(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+                   const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+                   GemmOut o, int K, int *status) {
+    FB_GRID_WAIT();
+    gemm2_body<BN, false>(&ma_hi, &ma_lo, &mb_hi, &mb_lo, o, K, status);
+}
+
+// grouped: blockIdx.z selects the product (a cluster never spans two)
+template <int BN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) kg_tf32x3_gemm2(const GemmTask *__restrict__ t) {
+    FB_GRID_WAIT();
+    const GemmTask &tk = t[blockIdx.z];
+    const GemmOut o = tk.o;
+    gemm2_body<BN, true>(&tk.p.a_hi, &tk.p.a_lo, &tk.p.b_hi, &tk.p.b_lo, o, tk.p.K, tk.status);
+}
+
 // dst[r * ldd + c] = (hi, lo) TF32 parts of src[c * lds + r], r < R, c < C:
 // the transposed split of a column-major FP64 matrix (32 x 32 tiles)
-__global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src, long lds, int R, int C,
-                                                  float *__restrict__ hi, float *__restrict__ lo, long ldd,
-                                                  const double *__restrict__ cscale) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void split_t_body(const double *__restrict__ src, long lds, int R, int C,
+                                             float *__restrict__ hi, float *__restrict__ lo, long ldd,
+                                             const double *__restrict__ cscale) {
     __shared__ double t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
@@ -504,16 +548,29 @@ __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src,
     }
 }
 
+__global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src, long lds, int R, int C,
+                                                  float *__restrict__ hi, float *__restrict__ lo, long ldd,
+                                                  const double *__restrict__ cscale) {
+    FB_GRID_WAIT();
+    split_t_body(src, lds, R, C, hi, lo, ldd, cscale);
+}
+
+// grouped: blockIdx.z selects the matrix (the task array is host-written)
+__global__ void __launch_bounds__(256) kg_split_t(const SplitTask *__restrict__ tk, int R, int C) {
+    const SplitTask t = tk[blockIdx.z];
+    FB_GRID_WAIT();
+    split_t_body(t.src, t.lds, R, C, t.hi, t.lo, t.ldd, t.cscale);
+}
+
 // FP64 residual of the Poisson equation that phcalc solves,
 //   r = dph - (A_yy + A_zz) phi,
 // with A_yy = tridiag(amphj, acphj, apphj) along j and A_zz = tridiag(amphk,
 // acphk, apphk) along k (the operators of phcalc_outflow.F90:36-45 and
 // phini.F90:59-65), written as the transposed TF32 split [j][k] that the
 // forward transform reads.  One 32 x 32 tile per block.
-__global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *__restrict__ phi, float *__restrict__ hi,
-                                                           float *__restrict__ lo, long ldd,
-                                                           const double *__restrict__ kscale) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void poisson_residual_body(const Dev &d, const double *__restrict__ phi,
+                                                      float *__restrict__ hi, float *__restrict__ lo, long ldd,
+                                                      const double *__restrict__ kscale) {
     __shared__ double t[32][33];
     const int j0 = 1 + blockIdx.x * 32, k0 = 1 + blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -546,6 +603,21 @@ __global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *_
             lo[static_cast<size_t>(jj - 1) * ldd + (kk - 1)] = l;
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_poisson_residual(Dev d, const double *__restrict__ phi, float *__restrict__ hi,
+                                                           float *__restrict__ lo, long ldd,
+                                                           const double *__restrict__ kscale) {
+    FB_GRID_WAIT();
+    poisson_residual_body(d, phi, hi, lo, ldd, kscale);
+}
+
+__global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__restrict__ g,
+                                                            const ResidualTask *__restrict__ tk) {
+    __shared__ Dev d;
+    const ResidualTask t = tk[blockIdx.z];
+    stage_case(g, &d);
+    poisson_residual_body(d, t.phi, t.hi, t.lo, t.ldd, t.kscale);
 }
 
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
@@ -591,6 +663,16 @@ int tf32x3_configure() {
         cudaFuncSetAttribute(k_tf32x3_gemm2<192>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(TcCfg2<192>::kSmem)) == cudaSuccess &&
         cudaFuncSetAttribute(k_tf32x3_gemm2<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<256>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(kg_tf32x3_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg<64>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(kg_tf32x3_gemm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg<128>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(kg_tf32x3_gemm2<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<128>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(kg_tf32x3_gemm2<192>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(TcCfg2<192>::kSmem)) == cudaSuccess &&
+        cudaFuncSetAttribute(kg_tf32x3_gemm2<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(TcCfg2<256>::kSmem)) == cudaSuccess;
     return ok ? FB_OK : FB_ERR_CUDA;
 }
@@ -637,6 +719,30 @@ void launch_tf32x3(const Tf32x3Plan &p, double *out, long ldo, const double *bas
         pdl(k_tf32x3_gemm<64>, dim3(grid), dim3(kThreads), TcCfg<64>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
     else
         pdl(k_tf32x3_gemm<128>, dim3(grid), dim3(kThreads), TcCfg<128>::kSmem, st, p.a_hi, p.a_lo, p.b_hi, p.b_lo, o, p.K, status);
+}
+
+void launch_tf32x3_group(const GemmTask *tasks, const Tf32x3Plan &p, int n, cudaStream_t st) {
+    if (p.bn > kPairTile) {
+        const int bn = p.bn - kPairTile;
+        const dim3 g2(2 * ((p.M + 2 * kBM - 1) / (2 * kBM)), (p.N + bn - 1) / bn, n);
+        if (bn == 128) pdl(kg_tf32x3_gemm2<128>, g2, dim3(kThreads), TcCfg2<128>::kSmem, st, tasks);
+        else if (bn == 192) pdl(kg_tf32x3_gemm2<192>, g2, dim3(kThreads), TcCfg2<192>::kSmem, st, tasks);
+        else pdl(kg_tf32x3_gemm2<256>, g2, dim3(kThreads), TcCfg2<256>::kSmem, st, tasks);
+        return;
+    }
+    const dim3 grid((p.M + kBM - 1) / kBM, (p.N + p.bn - 1) / p.bn, n);
+    if (p.bn == 64) pdl(kg_tf32x3_gemm<64>, grid, dim3(kThreads), TcCfg<64>::kSmem, st, tasks);
+    else pdl(kg_tf32x3_gemm<128>, grid, dim3(kThreads), TcCfg<128>::kSmem, st, tasks);
+}
+
+void launch_split_t_group(const SplitTask *tasks, int R, int C, int n, cudaStream_t st) {
+    const dim3 grid((R + 31) / 32, (C + 31) / 32, n);
+    pdl(kg_split_t, grid, dim3(256), 0, st, tasks, R, C);
+}
+
+void launch_poisson_residual_group(const Group &g, const ResidualTask *tasks, cudaStream_t st) {
+    const dim3 grid((g.rep.n2m + 31) / 32, (g.rep.n3m + 31) / 32, g.n);
+    pdl(kg_poisson_residual, grid, dim3(256), 0, st, g.cases, tasks);
 }
 
 void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane &dst, cudaStream_t st,

@@ -32,6 +32,26 @@ struct Tf32x3Plan {      // tensor maps of one C = A * B^T product
     int bn;              // tile code (kPairTile above)
 };
 
+// grouped launches (blockIdx.z = product or case), task arrays in device memory
+struct GemmTask {        // one product: its tensor maps, output and status word
+    Tf32x3Plan p;
+    GemmOut o;
+    int *status;
+};
+struct SplitTask {       // one transposed split: src (lds) -> hi, lo (ldd), column factors
+    const double *src;
+    long lds;
+    float *hi, *lo;
+    long ldd;
+    const double *cscale;
+};
+struct ResidualTask {    // one Poisson residual: phi -> hi, lo (ldd), row factors
+    const double *phi;
+    float *hi, *lo;
+    long ldd;
+    const double *kscale;
+};
+
 int tf32x3_configure();
 bool tf32x3_shape_ok(int bn);
 int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K, int bn);
@@ -42,5 +62,9 @@ void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane 
                     const double *cscale = nullptr);
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
                              const double *kscale = nullptr);
+// the same over n products / cases; every product has the shape and tile of p
+void launch_tf32x3_group(const GemmTask *tasks, const Tf32x3Plan &p, int n, cudaStream_t st);
+void launch_split_t_group(const SplitTask *tasks, int R, int C, int n, cudaStream_t st);
+void launch_poisson_residual_group(const Group &g, const ResidualTask *tasks, cudaStream_t st);
 
 }  // namespace fb

@@ -307,9 +307,7 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
 // k = 1..n3m of rhs2, then solq3j on rows k = 2..n3m of rhs3; they are
 // independent).  kKind 2: Poisson modes (rows of hmn).
 template <int M, int kKind>
-__global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSys s2, const double *by2,
-                                                                   ScanSys s3, const double *by3) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, const double *by2, const ScanSys &s3, const double *by3) {
     extern __shared__ double sm[];
     __shared__ double shx[kYLines][2 * kYWarps];
     const int wl = (threadIdx.x >> 5) / kYWarps;       // line slot in the block
@@ -377,6 +375,12 @@ __global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSy
             if (i < n) row[i] = buf[i];
         }
     }
+}
+
+template <int M, int kKind>
+__global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSys s2, const double *by2, ScanSys s3, const double *by3) {
+    FB_GRID_WAIT();
+    ylines_body<M, kKind>(d, s2, by2, s3, by3);
 }
 
 // ---------------------------------------------------------------- z lines
@@ -549,8 +553,7 @@ struct WinShape {            // shared-memory layout of one tile of kWTk rows (i
 // blockIdx.y = 0: v (solq2j + solq2k + walls), 1: w (solq3j + solq3k);
 // blockIdx.x = tile (tj fastest).
 template <int KM, int kWTk>
-__global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd, int ntj, int Ky, int Kz) {
     extern __shared__ double sm[];
     const WinShape<kWTk> sh(Ky, Kz);
     double *A = sm, *B = sm + sh.a_size, *C = B + sh.b_size;
@@ -721,6 +724,30 @@ __global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd,
     }
 }
 
+template <int KM, int kWTk>
+__global__ void __launch_bounds__(kWThreads, 3) k_helsolve_win(Dev d, SubDev sd, int ntj, int Ky, int Kz) {
+    FB_GRID_WAIT();
+    helsolve_win_body<KM, kWTk>(d, sd, ntj, Ky, Kz);
+}
+
+// grouped forms (blockIdx.z = case; substep n 0-based): each case keeps its
+// own windows, the group's shared memory fits the largest
+template <int KM, int kWTk>
+__global__ void __launch_bounds__(kWThreads, 3) kg_helsolve_win(const GroupCase *__restrict__ g, int n, int ntj) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    helsolve_win_body<KM, kWTk>(d, s, ntj, s.win_y, s.win_z);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kYLines * kYWarps * 32) kg_ylines_poisson(const GroupCase *__restrict__ g) {
+    __shared__ Dev d;
+    stage_case(g, &d);
+    const ScanSys z{nullptr, nullptr, nullptr};
+    ylines_body<M, 2>(d, z, nullptr, z, nullptr);
+}
+
 // ---------------------------------------------------------------- dispatch
 
 namespace {
@@ -774,6 +801,9 @@ cudaError_t scan_configure() {
     AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
     AL((k_helsolve_win<12, 32>)) AL((k_helsolve_win<12, 64>))
     AL((k_helsolve_win<kWinMax, 32>)) AL((k_helsolve_win<kWinMax, 64>))
+    AL((kg_helsolve_win<12, 32>)) AL((kg_helsolve_win<12, 64>))
+    AL((kg_helsolve_win<kWinMax, 32>)) AL((kg_helsolve_win<kWinMax, 64>))
+    AL((kg_ylines_poisson<9>)) AL((kg_ylines_poisson<17>)) AL((kg_ylines_poisson<33>))
 #undef AL
     return cudaSuccess;
 }
@@ -801,5 +831,36 @@ void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
 }
 
 void launch_scan_poisson(const Dev &d, cudaStream_t st) { ylaunch<2>(d, nullptr, st); }
+
+template <int TK>
+void gwin_launch(const Group &g, int n, cudaStream_t st) {
+    const Dev &d = g.rep;
+    const int ntj = (d.n2m + kWTj - 1) / kWTj, ntk = (d.n3m + TK - 1) / TK;
+    const dim3 grid(ntj * ntk, 2, g.n);
+    const int ky = g.win_ky[n], kz = g.win_kz[n];
+    const WinShape<TK> sh(ky, kz);   // sizes grow with the windows: fits every case
+    const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
+    if (ky <= 12 && kz <= 12)
+        pdl(kg_helsolve_win<12, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
+    else
+        pdl(kg_helsolve_win<kWinMax, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
+}
+
+void glaunch_win_helsolve(const Group &g, int n, cudaStream_t st) {
+    if (g.win_tk == 32) gwin_launch<32>(g, n, st);
+    else gwin_launch<64>(g, n, st);
+}
+
+void glaunch_scan_poisson(const Group &g, cudaStream_t st) {
+    const Dev &d = g.rep;
+    const int blocks = (d.n3m + kYLines - 1) / kYLines;
+    const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
+    const size_t smem = static_cast<size_t>(kYLines) * (d.n2 + 1) * sizeof(double);
+    const int threads = kYLines * kYWarps * 32;
+    const dim3 grid(blocks, 1, g.n);
+    if (m <= 9) pdl(kg_ylines_poisson<9>, grid, dim3(threads), smem, st, g.cases);
+    else if (m <= 17) pdl(kg_ylines_poisson<17>, grid, dim3(threads), smem, st, g.cases);
+    else pdl(kg_ylines_poisson<33>, grid, dim3(threads), smem, st, g.cases);
+}
 
 }  // namespace fb

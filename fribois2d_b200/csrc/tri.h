@@ -17,5 +17,7 @@ cudaError_t scan_configure();
 void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
 void launch_scan_poisson(const Dev &d, cudaStream_t st);
+void glaunch_win_helsolve(const Group &g, int n, cudaStream_t st);  // substep n (0-based)
+void glaunch_scan_poisson(const Group &g, cudaStream_t st);
 
 }  // namespace fb

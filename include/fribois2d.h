@@ -171,15 +171,29 @@ int fb_set_report(fb_ctx *ctx, int on);
 
 /* ---- batches of independent cases -------------------------------------------
  * No counterpart in the reference (one case per MPI job there).  The cases
- * (contexts on one device, fixed dt, RK3) are captured into one CUDA graph:
- * every case's step forks from one stream and joins back, so a step of the
- * whole batch is a single graph launch and the cases run concurrently.  Each
- * context keeps its own state, history rows and status; the contexts must
- * outlive the batch and must not be stepped on their own meanwhile.
- * fb_batch_advance returns the first non-zero case status. */
+ * (contexts on one device, fixed dt, RK3) are stepped by one CUDA graph
+ * launch per step.  Each context keeps its own state, history rows and
+ * status; the contexts must outlive the batch and must not be stepped on
+ * their own meanwhile.  fb_batch_advance returns the first non-zero case
+ * status.
+ *   FB_BATCH_GROUPED (fb_batch_create's mode): cases with one launch geometry
+ *     (grid, marker count, helsolve tiles, options) form a group; each stage
+ *     of the step is one kernel launch over the whole group; each Poisson
+ *     transform is one batched DGEMM, or in the precision form one grouped
+ *     3xTF32 tensor-core launch (same Poisson form and GEMM tile within a
+ *     group).  Cases without the windowed helsolve run as in FB_BATCH_GRAPH
+ *     inside the same graph.
+ *   FB_BATCH_GRAPH: every case's own step on its own graph branch; bitwise
+ *     equal to stepping the case alone. */
+#define FB_BATCH_GROUPED 0
+#define FB_BATCH_GRAPH 1
 int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out);
+int fb_batch_create_mode(fb_ctx *const *ctxs, int n, int mode, fb_batch **out);
 int fb_batch_advance(fb_batch *b, int nsteps);
 int fb_batch_last_ms(fb_batch *b, double *ms);  /* device time of the last advance */
+/* info[0] groups, info[1] cases stepped on their own branch, info[2] own
+ * kernel launches per step of the whole batch */
+int fb_batch_info(fb_batch *b, int32_t info[3]);
 int fb_batch_destroy(fb_batch *b);
 
 /* ---- strong fluid-structure coupling and its learned predictor ------------

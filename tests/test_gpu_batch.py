@@ -1,5 +1,8 @@
-"""Batches of independent cases: one graph launch steps every case, with
-results bit for bit equal to stepping each case on its own."""
+"""Batches of independent cases: one graph launch steps every case.  The
+graph mode holds every case's own captured step; the grouped mode launches
+each stage once over every group of cases of one launch geometry (batched
+DGEMMs for the transforms).  Both are checked against stepping each case on
+its own."""
 import numpy as np
 import pytest
 
@@ -26,13 +29,18 @@ def _open(c, root):
     return s
 
 
-def test_batch_equals_separate_runs(tmp_path):
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_batch_graph_equals_separate_runs(tmp_path):
     cs = _cases()
     alone = [_open(c, tmp_path / "alone") for c in cs]
     for s in alone:
         s.advance(0, 7)
     together = [_open(c, tmp_path / "batch") for c in cs]
-    batch = fb.Batch(together)
+    batch = fb.Batch(together, mode=fb.BATCH_GRAPH)
+    assert batch.info()["groups"] == 0 and batch.info()["singles"] == len(cs)
     batch.advance(3)
     batch.advance(4)
     assert batch.last_ms() > 0.0
@@ -53,3 +61,76 @@ def test_batch_rejects_variable_dt(tmp_path):
         fb.Batch([s])
     assert e.value.code == fb.FB_ERR_UNSUPPORTED
     s.close()
+
+
+def _grouped_cases():
+    """Two cases on one grid with different Re (one group), a second grid, a
+    rectangle, and two cases of the first grid in the precision form (a
+    group of grouped 3xTF32 transforms)."""
+    a = cases.tiny_cylinder()
+    b = cases.tiny_cylinder()
+    b.name = "tiny_cylinder_re150"
+    b.params.visc = 1.0 / 150.0
+    c = cases.tiny_cylinder(n3m=64, n2m=40, nlm=48, dt=4e-3)
+    d = cases.tiny_rectangle()
+    e = cases.tiny_cylinder()
+    e.name = "tiny_cylinder_tf32"
+    f = cases.tiny_cylinder()
+    f.name = "tiny_cylinder_tf32_re120"
+    f.params.visc = 1.0 / 120.0
+    return [a, b, c, d, e, f], {4, 5}
+
+
+def test_batch_grouped_matches_separate_runs(tmp_path):
+    cs, precision = _grouped_cases()
+    alone, together = [], []
+    for i, c in enumerate(cs):
+        s1 = _open(c, tmp_path / "alone")
+        s2 = _open(c, tmp_path / "grouped")
+        if i in precision:
+            s1.set_poisson(fb.POISSON_TF32X3)
+            s2.set_poisson(fb.POISSON_TF32X3)
+        alone.append(s1)
+        together.append(s2)
+    for s in alone:
+        s.autotune()
+        s.advance(0, 6)
+    batch = fb.Batch(together)
+    info = batch.info()
+    print("grouped batch:", info)
+    assert info["groups"] >= 2 and info["launches"] > 0
+    batch.advance(2)
+    batch.advance(4)
+    worst = {False: 0.0, True: 0.0}
+    for i, (s1, s2) in enumerate(zip(alone, together)):
+        for f in ("q2", "q3", "pr"):
+            e = rel(s2.get(f), s1.get(f))
+            worst[i in precision] = max(worst[i in precision], e)
+            assert e <= 1e-12, (i, f, e)
+        h1, h2 = s1.last_history(), s2.last_history()
+        assert h2[8] == h1[8] and h2[30] == h1[30]          # clock, fluid solves
+        np.testing.assert_allclose(h2[:21], h1[:21], rtol=1e-10, atol=1e-14)
+    print("grouped vs alone, worst field difference (FP64, precision form):", worst[False], worst[True])
+    batch.close()
+    for s in alone + together:
+        s.close()
+
+
+def test_batch_grouped_one_launch_per_stage(tmp_path):
+    """A group's launches per step do not grow with its size."""
+    counts = []
+    for n in (1, 4):
+        ss = []
+        for i in range(n):
+            c = cases.tiny_cylinder()
+            c.name = f"tiny_cylinder_{n}_{i}"
+            c.params.visc = 1.0 / (100.0 + 10.0 * i)
+            ss.append(_open(c, tmp_path / f"n{n}"))
+        b = fb.Batch(ss)
+        b.advance(2)
+        counts.append(b.info())
+        b.close()
+        for s in ss:
+            s.close()
+    assert counts[0]["groups"] == 1 and counts[1]["groups"] == 1 and counts[1]["singles"] == 0
+    assert counts[1]["launches"] == counts[0]["launches"]
