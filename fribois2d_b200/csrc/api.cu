@@ -396,6 +396,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if (const char *hv = std::getenv("FRIBOIS2D_HELSOLVE")) c->allow_win = std::strcmp(hv, "scan") != 0;
     CK(cudaSetDevice(device));
     CK(fb::scan_configure());
+    CK(fb::kernels_configure());
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));

@@ -58,6 +58,16 @@ __device__ double block_reduce_fast(double v, double *sh) {
     return r;
 }
 
+// asynchronous 8-byte global -> shared copies (no register round trip, all
+// of a thread's copies in flight at once); cp_wait completes this thread's
+// copies, a barrier then publishes them to the block
+__device__ __forceinline__ void cp8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ------------------------------------------------------------ cfl
 
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
@@ -154,69 +164,93 @@ __global__ void __launch_bounds__(1024) k_boucdq(Dev d, double ga, double ro) {
 // The convective terms stay in registers; ru2/ru3 receive them as the
 // reference's invtr does (ru2 = dph, ru3 = qcap).  q2f/q3f are not stored:
 // the forcing stage forms q + rhs at the few support nodes it reads.
-__device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, double ro) {
-    const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+// Tiles of kNlJ x kNlK cells: a block holds q2, q3 and pr of a tile plus a
+// one-cell halo, and the tile's j and k coefficients, in shared memory, so
+// each cell's stencil reads shared memory instead of issuing ~24 global
+// loads.  Blocks are persistent over tiles with two buffers: the copies of
+// the next tile (cp.async) and its ru2/ru3 (registers) are in flight while
+// the current tile is computed.  Thread (tx, ty) of the 32 x 8 block computes
+// the cells j = j0 + tx, k = k0 + 4 ty + i, i = 0..3 of a tile (consecutive
+// rows share their stencil loads).
+constexpr int kNlJ = 32, kNlK = 32, kNlS = kNlJ + 3;  // odd row stride
+constexpr int kNlBlocksPerSM = 2;
+struct NlTile {
+    double q2[kNlK + 2][kNlS], q3[kNlK + 2][kNlS], pr[kNlK + 2][kNlS];  // rows k0-1.., cols j0-1..
+    double udx3m[kNlK], ap3sk[kNlK], ac3sk[kNlK], am3sk[kNlK];           // k coefficients, rows k0..
+    double udx3c[kNlK], ap3ck[kNlK], ac3ck[kNlK], am3ck[kNlK];
+    double udx2c[kNlJ], am2j[kNlJ], ac2j[kNlJ], ap2j[kNlJ];              // j coefficients, columns j0..
+    double udx2m[kNlJ], am3j[kNlJ], ac3j[kNlJ], ap3j[kNlJ];
+};
+constexpr size_t kNlSmem = 2 * sizeof(NlTile);
+
+// ru2v, ru3v: ru2/ru3 at the cell, read before any cell of the thread is
+// stored (0 when ro = 0)
+__device__ __forceinline__ void nl_cell(const Dev &d, const NlTile &t, int j0, int k0, int jc, int kc, double al,
+                                        double ga, double ro, double ru2v, double ru3v) {
+#define S2(j, k) t.q2[(k) - k0 + 1][(j) - j0 + 1]
+#define S3(j, k) t.q3[(k) - k0 + 1][(j) - j0 + 1]
+#define SP(j, k) t.pr[(k) - k0 + 1][(j) - j0 + 1]
     const int n2m = d.n2m, n3m = d.n3m;
-    if (jc > n2m || kc > n3m) return;
     const double dt = d.dt, alre = al / d.ren;
-    const double *q2 = d.q2, *q3 = d.q3, *pr = d.pr;
 
     // ---- v momentum at (jc, kc), jc = 2..n2m
     if (jc >= 2) {
         const int jm = jc - 1, jp = jc + 1;
-        double h22 = ((Fv(q2, jp, kc) + Fv(q2, jc, kc)) * (Fv(q2, jp, kc) + Fv(q2, jc, kc)) -
-                      (Fv(q2, jm, kc) + Fv(q2, jc, kc)) * (Fv(q2, jm, kc) + Fv(q2, jc, kc))) *
-                     d.udx2c[jc] * 0.25;
+        double h22 = ((S2(jp, kc) + S2(jc, kc)) * (S2(jp, kc) + S2(jc, kc)) -
+                      (S2(jm, kc) + S2(jc, kc)) * (S2(jm, kc) + S2(jc, kc))) *
+                     t.udx2c[jc - j0] * 0.25;
         double dph = -h22;
         const int jmv = jc - 1;  // jmv(jc) for jc >= 2
         if (kc >= 2 && kc <= n3m - 1) {
             const int kmm = kc - 1, kpp = kc + 1, kp = kc + 1;  // kmv, kpv in the interior
-            double h23 = ((Fv(q3, jc, kp) + Fv(q3, jmv, kp)) * (Fv(q2, jc, kpp) + Fv(q2, jc, kc)) -
-                          (Fv(q3, jc, kc) + Fv(q3, jmv, kc)) * (Fv(q2, jc, kc) + Fv(q2, jc, kmm))) *
-                         d.udx3m[kc] * 0.25;
+            double h23 = ((S3(jc, kp) + S3(jmv, kp)) * (S2(jc, kpp) + S2(jc, kc)) -
+                          (S3(jc, kc) + S3(jmv, kc)) * (S2(jc, kc) + S2(jc, kmm))) *
+                         t.udx3m[kc - k0] * 0.25;
             dph = dph - h23;
         } else if (kc == n3m) {
             const int kmm = kc - 1;
             double h23 = (d.qb2n[jc] * (d.qb3n[jc] + d.qb3n[jmv]) -
-                          (Fv(q3, jc, kc) + Fv(q3, jmv, kc)) * (Fv(q2, jc, kc) + Fv(q2, jc, kmm)) * 0.5) *
-                         d.udx3m[kc] * 0.5;
+                          (S3(jc, kc) + S3(jmv, kc)) * (S2(jc, kc) + S2(jc, kmm)) * 0.5) *
+                         t.udx3m[kc - k0] * 0.5;
             dph = dph - h23;
         }
         if (kc == 1) {
             const int kp = kc + 1;
-            double h23 = ((Fv(q3, jc, kp) + Fv(q3, jmv, kp)) * (Fv(q2, jc, kc) + Fv(q2, jc, kp)) * 0.5 -
+            double h23 = ((S3(jc, kp) + S3(jmv, kp)) * (S2(jc, kc) + S2(jc, kp)) * 0.5 -
                           d.qb2s[jc] * (d.qb3s[jc] + d.qb3s[jmv])) *
-                         d.udx3m[kc] * 0.5;
+                         t.udx3m[kc - k0] * 0.5;
             dph = dph - h23;
         }
-        const double ammj = d.am2j[jc], accj = d.ac2j[jc], appj = d.ap2j[jc];
-        const double d22q2 = Fv(q2, jp, kc) * appj + Fv(q2, jc, kc) * accj + Fv(q2, jm, kc) * ammj;
+        const double ammj = t.am2j[jc - j0], accj = t.ac2j[jc - j0], appj = t.ap2j[jc - j0];
+        const double d22q2 = S2(jp, kc) * appj + S2(jc, kc) * accj + S2(jm, kc) * ammj;
         double d33q2, dpx22;
         if (kc >= 2 && kc <= n3m - 1) {
             const int km = kc - 1, kp = kc + 1;
-            d33q2 = Fv(q2, jc, kp) * d.ap3sk[kc] + Fv(q2, jc, kc) * d.ac3sk[kc] + Fv(q2, jc, km) * d.am3sk[kc];
-            const double udx2 = al * d.udx2c[jc];
-            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * udx2;
+            d33q2 = S2(jc, kp) * t.ap3sk[kc - k0] + S2(jc, kc) * t.ac3sk[kc - k0] + S2(jc, km) * t.am3sk[kc - k0];
+            const double udx2 = al * t.udx2c[jc - j0];
+            dpx22 = (SP(jc, kc) - SP(jm, kc)) * udx2;
         } else if (kc == 1) {
             const int kp = kc + 1;
             const double codea = d.dx3q / (d.g3rc[kp] * d.g3rm[kc]);
             const double codeb = d.dx3q / (d.g3rc[kc] * d.g3rm[kc]);
-            d33q2 = ((Fv(q2, jc, kp) - Fv(q2, jc, kc)) * codea - (Fv(q2, jc, kc) - d.qb2s[jc]) * codeb * 2.0);
-            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * d.udx2c[jc] * al;
+            d33q2 = ((S2(jc, kp) - S2(jc, kc)) * codea - (S2(jc, kc) - d.qb2s[jc]) * codeb * 2.0);
+            dpx22 = (SP(jc, kc) - SP(jm, kc)) * t.udx2c[jc - j0] * al;
         } else {
             const int km = kc - 1, kp = kc + 1;
             const double codea = d.dx3q / (d.g3rc[kp] * d.g3rm[kc]);
             const double codeb = d.dx3q / (d.g3rc[kc] * d.g3rm[kc]);
-            d33q2 = ((d.qb2n[jc] - Fv(q2, jc, kc)) * codea * 2.0 - (Fv(q2, jc, kc) - Fv(q2, jc, km)) * codeb);
-            dpx22 = (Fv(pr, jc, kc) - Fv(pr, jm, kc)) * d.udx2c[jc] * al;
+            d33q2 = ((d.qb2n[jc] - S2(jc, kc)) * codea * 2.0 - (S2(jc, kc) - S2(jc, km)) * codeb);
+            dpx22 = (SP(jc, kc) - SP(jm, kc)) * t.udx2c[jc - j0] * al;
         }
         const double dcq2 = d22q2 + d33q2;
         const size_t i = fidx(d, jc, kc);
         // the first RK3 substep has ro = 0: ru2 is not read (one field pass less)
-        const double ru = (ro != 0.0) ? d.ru2[i] : 0.0;
-        d.rhs2[i] = (ga * dph + ro * ru + alre * dcq2 - dpx22) * dt;
-        d.ru2[i] = dph;
+        const double ru = ru2v;
+        // global stores (st.global): the compiler then knows they do not
+        // alias the shared-memory tile and reuses the tile loads across the
+        // thread's consecutive cells
+        __stcg(d.rhs2 + i, (ga * dph + ro * ru + alre * dcq2 - dpx22) * dt);
+        __stcg(d.ru2 + i, dph);
     }
 
     // ---- w momentum at (jc, kc), kc = 2..n3m
@@ -225,38 +259,140 @@ __device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, 
         if (kc <= n3m - 1) {
             const int kmm = kc - 1, km = kc - 1, kp = kc + 1;
             const int jmm = jmv_(jc), jpp = jpv_(d, jc), jp = jc + 1;
-            double h32 = (((Fv(q2, jp, kc) + Fv(q2, jp, km)) * (Fv(q3, jpp, kc) + Fv(q3, jc, kc))) -
-                          ((Fv(q2, jc, kc) + Fv(q2, jc, km)) * (Fv(q3, jc, kc) + Fv(q3, jmm, kc)))) *
-                         d.udx2m[jc] * 0.25;
-            double h33 = ((Fv(q3, jc, kp) + Fv(q3, jc, kc)) * (Fv(q3, jc, kp) + Fv(q3, jc, kc)) -
-                          (Fv(q3, jc, kc) + Fv(q3, jc, kmm)) * (Fv(q3, jc, kc) + Fv(q3, jc, kmm))) *
-                         d.udx3c[kc] * 0.25;
+            double h32 = (((S2(jp, kc) + S2(jp, km)) * (S3(jpp, kc) + S3(jc, kc))) -
+                          ((S2(jc, kc) + S2(jc, km)) * (S3(jc, kc) + S3(jmm, kc)))) *
+                         t.udx2m[jc - j0] * 0.25;
+            double h33 = ((S3(jc, kp) + S3(jc, kc)) * (S3(jc, kp) + S3(jc, kc)) -
+                          (S3(jc, kc) + S3(jc, kmm)) * (S3(jc, kc) + S3(jc, kmm))) *
+                         t.udx3c[kc - k0] * 0.25;
             qcap = -(h32 + h33);
         }
         const int km = kc - 1, kp = kc + 1;
-        const double udx3 = al * d.udx3c[kc];
-        const double ammj = d.am3j[jc], accj = d.ac3j[jc], appj = d.ap3j[jc];
+        const double udx3 = al * t.udx3c[kc - k0];
+        const double ammj = t.am3j[jc - j0], accj = t.ac3j[jc - j0], appj = t.ap3j[jc - j0];
         double dq32;
         if (jc == 1) {
-            dq32 = Fv(q3, jc + 1, kc) * appj + Fv(q3, jc, kc) * accj + d.q3lw * ammj;
+            dq32 = S3(jc + 1, kc) * appj + S3(jc, kc) * accj + d.q3lw * ammj;
         } else if (jc == n2m) {
-            dq32 = d.q3uw * appj + Fv(q3, jc, kc) * accj + Fv(q3, jc - 1, kc) * ammj;
+            dq32 = d.q3uw * appj + S3(jc, kc) * accj + S3(jc - 1, kc) * ammj;
         } else {
-            dq32 = Fv(q3, jpv_(d, jc), kc) * appj + Fv(q3, jc, kc) * accj + Fv(q3, jmv_(jc), kc) * ammj;
+            dq32 = S3(jpv_(d, jc), kc) * appj + S3(jc, kc) * accj + S3(jmv_(jc), kc) * ammj;
         }
-        const double dq33 = Fv(q3, jc, kp) * d.ap3ck[kc] + Fv(q3, jc, kc) * d.ac3ck[kc] + Fv(q3, jc, km) * d.am3ck[kc];
+        const double dq33 = S3(jc, kp) * t.ap3ck[kc - k0] + S3(jc, kc) * t.ac3ck[kc - k0] + S3(jc, km) * t.am3ck[kc - k0];
         const double dcq3 = dq32 + dq33;
-        const double dpx33 = (Fv(pr, jc, kc) - Fv(pr, jc, km)) * udx3;
+        const double dpx33 = (SP(jc, kc) - SP(jc, km)) * udx3;
         const size_t i = fidx(d, jc, kc);
-        const double ru = (ro != 0.0) ? d.ru3[i] : 0.0;
-        d.rhs3[i] = (ga * qcap + ro * ru + alre * dcq3 - dpx33) * dt;
-        d.ru3[i] = qcap;
+        const double ru = ru3v;
+        __stcg(d.rhs3 + i, (ga * qcap + ro * ru + alre * dcq3 - dpx33) * dt);
+        __stcg(d.ru3 + i, qcap);
+    }
+}
+#undef S2
+#undef S3
+#undef SP
+
+// issues the copies of one tile into t (one cp.async group per thread)
+__device__ __forceinline__ void nl_prefetch(const Dev &d, NlTile &t, int tile, int ntj, int tid) {
+    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+    // tile + halo: j = j0-1 .. j0+kNlJ, k = k0-1 .. k0+kNlK (entries outside
+    // the stored arrays, j < 1, j > n2, k > n3, are never read by a cell)
+    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
+    for (int e = tid; e < kW * kH; e += 256) {
+        const int r = e / kW, c = e % kW;
+        const int j = j0 - 1 + c, k = k0 - 1 + r;
+        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) {
+            const size_t i = fidx(d, j, k);
+            cp8(&t.q2[r][c], d.q2 + i);
+            cp8(&t.q3[r][c], d.q3 + i);
+            cp8(&t.pr[r][c], d.pr + i);
+        } else {
+            t.q2[r][c] = 0.0;
+            t.q3[r][c] = 0.0;
+            t.pr[r][c] = 0.0;
+        }
+    }
+    if (tid < kNlK) {
+        const int k = min(k0 + tid, d.n3m);
+        cp8(&t.udx3m[tid], d.udx3m + k);
+        cp8(&t.ap3sk[tid], d.ap3sk + k);
+        cp8(&t.ac3sk[tid], d.ac3sk + k);
+        cp8(&t.am3sk[tid], d.am3sk + k);
+        cp8(&t.udx3c[tid], d.udx3c + k);
+        cp8(&t.ap3ck[tid], d.ap3ck + k);
+        cp8(&t.ac3ck[tid], d.ac3ck + k);
+        cp8(&t.am3ck[tid], d.am3ck + k);
+    } else if (tid < kNlK + kNlJ) {
+        const int c = tid - kNlK, j = min(j0 + c, d.n2m);
+        cp8(&t.udx2c[c], d.udx2c + j);
+        cp8(&t.am2j[c], d.am2j + j);
+        cp8(&t.ac2j[c], d.ac2j + j);
+        cp8(&t.ap2j[c], d.ap2j + j);
+        cp8(&t.udx2m[c], d.udx2m + j);
+        cp8(&t.am3j[c], d.am3j + j);
+        cp8(&t.ac3j[c], d.ac3j + j);
+        cp8(&t.ap3j[c], d.ap3j + j);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// ru2/ru3 at this thread's cells of a tile (0 when ro = 0)
+__device__ __forceinline__ void nl_ru(const Dev &d, int tile, int ntj, double ro, double (&r2)[kNlK / 8],
+                                      double (&r3)[kNlK / 8]) {
+    const int jc = 1 + (tile % ntj) * kNlJ + threadIdx.x, k0 = 1 + (tile / ntj) * kNlK;
+#pragma unroll
+    for (int i = 0; i < kNlK / 8; ++i) {
+        const int kc = k0 + (kNlK / 8) * threadIdx.y + i;
+        const bool ok = jc <= d.n2m && kc <= d.n3m && ro != 0.0;
+        const size_t x = fidx(d, min(jc, d.n2m), min(kc, d.n3m));
+        r2[i] = ok ? d.ru2[x] : 0.0;
+        r3[i] = ok ? d.ru3[x] : 0.0;
     }
 }
 
-__global__ void k_nl_rhs(Dev d, double al, double ga, double ro) {
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...; buf: two NlTile in shared memory
+__device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, double ro, NlTile *buf) {
+    const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    nl_prefetch(d, buf[0], tile, ntj, tid);
+    double r2n[kNlK / 8], r3n[kNlK / 8];
+    nl_ru(d, tile, ntj, ro, r2n, r3n);
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        const NlTile &t = buf[it & 1];
+        double r2[kNlK / 8], r3[kNlK / 8];
+#pragma unroll
+        for (int i = 0; i < kNlK / 8; ++i) {
+            r2[i] = r2n[i];
+            r3[i] = r3n[i];
+        }
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) {
+            nl_prefetch(d, buf[(it + 1) & 1], nxt, ntj, tid);
+            nl_ru(d, nxt, ntj, ro, r2n, r3n);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+        const int jc = j0 + threadIdx.x;
+        if (jc <= d.n2m) {
+#pragma unroll
+            for (int i = 0; i < kNlK / 8; ++i) {
+                const int kc = k0 + (kNlK / 8) * threadIdx.y + i;
+                if (kc > d.n3m) break;
+                nl_cell(d, t, j0, k0, jc, kc, al, ga, ro, r2[i], r3[i]);
+            }
+        }
+        __syncthreads();   // this buffer is refilled two tiles on
+    }
+}
+
+__global__ void __launch_bounds__(256, kNlBlocksPerSM) k_nl_rhs(Dev d, double al, double ga, double ro) {
+    extern __shared__ __align__(16) unsigned char nl_smem[];
     FB_GRID_WAIT();
-    nl_rhs_body(d, al, ga, ro);
+    nl_rhs_body(d, al, ga, ro, reinterpret_cast<NlTile *>(nl_smem));
 }
 
 // ------------------------------------------------------------ MLS forcing
@@ -746,32 +882,123 @@ __global__ void k_divg(Dev d, double usdtal) {
 }
 
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
-// partial sums of pr_submean (updvp.F90:320-333)
-__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be) {
+// partial sums of pr_submean (updvp.F90:320-333).  Tiles of kNlJ x kNlK cells
+// as in nl_rhs: dph with its halo in shared memory; the block partial sums
+// of the pressure mean are finished by the case's last block.
+struct UpTile {
+    double dph[kNlK + 2][kNlS];   // dph tile + one-cell halo (rows k0-1.., cols j0-1..)
+    double kc[6][kNlK];           // udx3c, apphk, acphk, amphk, zz(k), zz(k+1) at rows k0..
+    double jc[6][kNlJ];           // udx2c, apphj, acphj, amphj, rc(j), rc(j+1) at columns j0..
+};
+constexpr size_t kUpSmem = 2 * sizeof(UpTile);
+constexpr int kUpBlocksPerSM = 3;
+
+__device__ __forceinline__ void up_prefetch(const Dev &d, UpTile &t, int tile, int ntj, int tid) {
+    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
+    for (int e = tid; e < kW * kH; e += 256) {
+        const int r = e / kW, c = e % kW;
+        const int j = j0 - 1 + c, k = k0 - 1 + r;
+        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) cp8(&t.dph[r][c], d.dph + fidx(d, j, k));
+        else t.dph[r][c] = 0.0;
+    }
+    if (tid < kNlK) {
+        const int k = min(k0 + tid, d.n3m);
+        cp8(&t.kc[0][tid], d.udx3c + k);
+        cp8(&t.kc[1][tid], d.apphk + k);
+        cp8(&t.kc[2][tid], d.acphk + k);
+        cp8(&t.kc[3][tid], d.amphk + k);
+        cp8(&t.kc[4][tid], d.zz + k);
+        cp8(&t.kc[5][tid], d.zz + k + 1);
+    } else if (tid < kNlK + kNlJ) {
+        const int c = tid - kNlK, j = min(j0 + c, d.n2m);
+        cp8(&t.jc[0][c], d.udx2c + j);
+        cp8(&t.jc[1][c], d.apphj + j);
+        cp8(&t.jc[2][c], d.acphj + j);
+        cp8(&t.jc[3][c], d.amphj + j);
+        cp8(&t.jc[4][c], d.rc + j);
+        cp8(&t.jc[5][c], d.rc + j + 1);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// q2, q3, pr at this thread's cells of a tile, read before any is written
+__device__ __forceinline__ void up_own(const Dev &d, int tile, int ntj, double (&q2)[kNlK / 8], double (&q3)[kNlK / 8],
+                                       double (&pr)[kNlK / 8]) {
+    const int jc = 1 + (tile % ntj) * kNlJ + threadIdx.x, k0 = 1 + (tile / ntj) * kNlK;
+#pragma unroll
+    for (int i = 0; i < kNlK / 8; ++i) {
+        const int kc = k0 + threadIdx.y + 8 * i;
+        const bool ok = jc <= d.n2m && kc <= d.n3m;
+        const size_t x = fidx(d, min(jc, d.n2m), min(kc, d.n3m));
+        q2[i] = ok ? d.q2[x] : 0.0;
+        q3[i] = ok ? d.q3[x] : 0.0;
+        pr[i] = ok ? d.pr[x] : 0.0;
+    }
+}
+
+__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be, UpTile *buf) {
     __shared__ double sh[32];
     __shared__ bool last;
-    const int t = threadIdx.x, nt = blockDim.x, b = blockIdx.x, nb = gridDim.x;
-    const long cells = static_cast<long>(d.n2m) * d.n3m;
-    const double *dph = d.dph;
+    const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
+    const int t = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+    const int b = blockIdx.x, nb = gridDim.x;
+    constexpr int kC = kNlK / 8;
     double part = 0.0;
-    for (long idx = static_cast<long>(b) * nt + t; idx < cells; idx += static_cast<long>(nb) * nt) {
-        const int jc = static_cast<int>(idx % d.n2m) + 1, kc = static_cast<int>(idx / d.n2m) + 1;
-        const int jm = jmv_(jc), jp = jpv_(d, jc);
-        const double usujm = al * d.dt * d.udx2c[jc];
-        const double locdph = Fv(dph, jc, kc);
-        Fv(d.q2, jc, kc) = Fv(d.q2, jc, kc) - (locdph - Fv(dph, jm, kc)) * usujm;
-        if (kc >= 2) {
-            const double usukm = al * d.dt * d.udx3c[kc];
-            Fv(d.q3, jc, kc) = Fv(d.q3, jc, kc) - (Fv(dph, jc, kc) - Fv(dph, jc, kc - 1)) * usukm;
+    int tile = blockIdx.x;
+    double q2n[kC], q3n[kC], prn[kC];
+    if (tile < ntiles) {
+        up_prefetch(d, buf[0], tile, ntj, t);
+        up_own(d, tile, ntj, q2n, q3n, prn);
+    }
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        const UpTile &u = buf[it & 1];
+        double q2v[kC], q3v[kC], prv[kC];
+#pragma unroll
+        for (int i = 0; i < kC; ++i) {
+            q2v[i] = q2n[i];
+            q3v[i] = q3n[i];
+            prv[i] = prn[i];
         }
-        const int kp = kpv_(d, kc), km = kmv_(kc);
-        const double p = Fv(d.pr, jc, kc) + Fv(dph, jc, kc) -
-                         be * ((Fv(dph, jp, kc) * d.apphj[jc] + Fv(dph, jc, kc) * d.acphj[jc] +
-                                Fv(dph, jm, kc) * d.amphj[jc]) +
-                               (Fv(dph, jc, kp) * d.apphk[kc] + Fv(dph, jc, kc) * d.acphk[kc] +
-                                Fv(dph, jc, km) * d.amphk[kc]));
-        Fv(d.pr, jc, kc) = p;
-        part = part + p * (d.zz[kc + 1] - d.zz[kc]) * (d.rc[jc + 1] - d.rc[jc]);
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) {
+            up_prefetch(d, buf[(it + 1) & 1], nxt, ntj, t);
+            up_own(d, nxt, ntj, q2n, q3n, prn);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+        const int jc = j0 + threadIdx.x;
+#define TD(j, k) u.dph[(k) - k0 + 1][(j) - j0 + 1]
+        if (jc <= d.n2m) {
+            const int cj = jc - j0;
+            const int jm = jmv_(jc), jp = jpv_(d, jc);
+            const double usujm = al * d.dt * u.jc[0][cj];
+            const double apj = u.jc[1][cj], acj = u.jc[2][cj], amj = u.jc[3][cj];
+            const double dyc = u.jc[5][cj] - u.jc[4][cj];
+#pragma unroll
+            for (int i = 0; i < kC; ++i) {
+                const int kc = k0 + threadIdx.y + 8 * i;
+                if (kc > d.n3m) break;
+                const int r = kc - k0;
+                const double locdph = TD(jc, kc);
+                Fv(d.q2, jc, kc) = q2v[i] - (locdph - TD(jm, kc)) * usujm;
+                if (kc >= 2) {
+                    const double usukm = al * d.dt * u.kc[0][r];
+                    Fv(d.q3, jc, kc) = q3v[i] - (TD(jc, kc) - TD(jc, kc - 1)) * usukm;
+                }
+                const int kp = kpv_(d, kc), km = kmv_(kc);
+                const double p = prv[i] + TD(jc, kc) -
+                                 be * ((TD(jp, kc) * apj + TD(jc, kc) * acj + TD(jm, kc) * amj) +
+                                       (TD(jc, kp) * u.kc[1][r] + TD(jc, kc) * u.kc[2][r] + TD(jc, km) * u.kc[3][r]));
+                Fv(d.pr, jc, kc) = p;
+                part = part + p * (u.kc[5][r] - u.kc[4][r]) * dyc;
+            }
+        }
+#undef TD
+        __syncthreads();   // this buffer is refilled two tiles on
     }
     const double bsum = block_reduce_fast<false>(part, sh);
     double *red = d.red + 2 * static_cast<size_t>(kRedSlot);
@@ -792,9 +1019,10 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
     }
 }
 
-__global__ void __launch_bounds__(256) k_updvp_prcalc(Dev d, double al, double be) {
+__global__ void __launch_bounds__(256, kUpBlocksPerSM) k_updvp_prcalc(Dev d, double al, double be) {
+    extern __shared__ __align__(16) unsigned char up_smem[];
     FB_GRID_WAIT();
-    updvp_prcalc_body(d, al, be);
+    updvp_prcalc_body(d, al, be, reinterpret_cast<UpTile *>(up_smem));
 }
 
 // pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
@@ -1341,13 +1569,13 @@ __global__ void __launch_bounds__(1024) kg_boucdq(const GroupCase *__restrict__ 
     boucdq_body(d, s.ga, s.ro);
 }
 
-__global__ void kg_nl_rhs(const GroupCase *__restrict__ g, int n) {
+__global__ void __launch_bounds__(256, kNlBlocksPerSM) kg_nl_rhs(const GroupCase *__restrict__ g, int n) {
+    extern __shared__ __align__(16) unsigned char nl_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
     stage_case(g, &d, &s, n);
-    nl_rhs_body(d, s.al, s.ga, s.ro);
+    nl_rhs_body(d, s.al, s.ga, s.ro, reinterpret_cast<NlTile *>(nl_smem));
 }
-
 __global__ void kg_lgrdist(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     stage_case(g, &d);
@@ -1385,11 +1613,12 @@ __global__ void kg_divg(const GroupCase *__restrict__ g, int n) {
     divg_body(d, s.usdtal);
 }
 
-__global__ void __launch_bounds__(256) kg_updvp_prcalc(const GroupCase *__restrict__ g, int n) {
+__global__ void __launch_bounds__(256, kUpBlocksPerSM) kg_updvp_prcalc(const GroupCase *__restrict__ g, int n) {
+    extern __shared__ __align__(16) unsigned char up_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
     stage_case(g, &d, &s, n);
-    updvp_prcalc_body(d, s.al, s.al * s.beta);
+    updvp_prcalc_body(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem));
 }
 
 __global__ void kg_submean_boucqt(const GroupCase *__restrict__ g) {
@@ -1432,11 +1661,21 @@ int stride_blocks(const Dev &d) {
     const long cells = static_cast<long>(d.n2m) * d.n3m;
     return static_cast<int>(std::min<long>((cells + 255) / 256, 148L * 8));
 }
+
+// grid-stride reductions of a group: the cases fill the GPU together, so each
+// case takes fewer blocks (about eight cells per thread) and the block and
+// last-block reductions are paid less often
+int group_stride_blocks(const Dev &d) {
+    const long cells = static_cast<long>(d.n2m) * d.n3m;
+    return static_cast<int>(std::max<long>(1, std::min<long>((cells + 2047) / 2048, 148L * 8)));
+}
 void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(stride_blocks(d)), dim3(256), 0, s, d); }
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
+int nl_tiles(const Dev &d) { return ((d.n2m + kNlJ - 1) / kNlJ) * ((d.n3m + kNlK - 1) / kNlK); }
+
 void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s) {
-    dim3 b(32, 8);
-    pdl(k_nl_rhs, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, al, ga, ro);
+    const int blocks = std::min(nl_tiles(d), 148 * kNlBlocksPerSM);
+    pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro);
 }
 void launch_lgrdist(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_lgrdist, dim3((d.nlm + 127) / 128), dim3(128), 0, s, d);
@@ -1466,7 +1705,8 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     pdl(k_divg, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, usdtal);
 }
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
-    pdl(k_updvp_prcalc, dim3(stride_blocks(d)), dim3(256), 0, s, d, al, be);
+    const int blocks = std::min(nl_tiles(d), 148 * kUpBlocksPerSM);
+    pdl(k_updvp_prcalc, dim3(blocks), dim3(32, 8), kUpSmem, s, d, al, be);
 }
 void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
     dim3 b(32, 8);
@@ -1491,14 +1731,29 @@ inline dim3 zgrid(dim3 g, const Group &gr) { return dim3(g.x, g.y, static_cast<u
 }  // namespace
 
 void glaunch_cfl(const Group &g, cudaStream_t s) {
-    pdl(kg_cfl, zgrid(dim3(stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases);
+    pdl(kg_cfl, zgrid(dim3(group_stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases);
 }
 void glaunch_boucdq(const Group &g, int n, cudaStream_t s) {
     pdl(kg_boucdq, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases, n);
 }
 void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s) {
-    dim3 b(32, 8);
-    pdl(kg_nl_rhs, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
+    // about two waves of resident blocks over the whole group
+    const int per_case = std::max(1, std::min(nl_tiles(g.rep), (2 * 148 * kNlBlocksPerSM + g.n - 1) / g.n));
+    pdl(kg_nl_rhs, zgrid(dim3(per_case), g), dim3(32, 8), kNlSmem, s, g.cases, n);
+}
+
+cudaError_t kernels_configure() {
+    cudaError_t e = cudaFuncSetAttribute(k_nl_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kNlSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kg_nl_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kNlSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_updvp_prcalc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kUpSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kg_updvp_prcalc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kUpSmem));
+    return e;
 }
 void glaunch_marker_setup(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
@@ -1518,7 +1773,8 @@ void glaunch_divg(const Group &g, int n, cudaStream_t s) {
     pdl(kg_divg, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
 }
 void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s) {
-    pdl(kg_updvp_prcalc, zgrid(dim3(stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases, n);
+    const int per_case = std::max(1, std::min(nl_tiles(g.rep), (2 * 148 * kUpBlocksPerSM + g.n - 1) / g.n));
+    pdl(kg_updvp_prcalc, zgrid(dim3(per_case), g), dim3(32, 8), kUpSmem, s, g.cases, n);
 }
 void glaunch_submean_boucqt(const Group &g, cudaStream_t s) {
     dim3 b(32, 8);
@@ -1534,7 +1790,7 @@ void glaunch_rigid(const Group &g, cudaStream_t s) {
     if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(256), 0, s, g.cases);
 }
 void glaunch_diag(const Group &g, cudaStream_t s) {
-    pdl(kg_diag, zgrid(dim3(std::min(stride_blocks(g.rep), 2048)), g), dim3(256), 0, s, g.cases);
+    pdl(kg_diag, zgrid(dim3(std::min(group_stride_blocks(g.rep), 2048)), g), dim3(256), 0, s, g.cases);
 }
 
 }  // namespace fb

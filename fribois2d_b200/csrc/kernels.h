@@ -9,6 +9,7 @@ namespace fb {
 
 constexpr int kRedSlot = 65536;  // block partials per reduction slot
 
+cudaError_t kernels_configure();   // shared-memory limits (once per device)
 void launch_cfl(const Dev &d, cudaStream_t s);
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s);
 void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s);

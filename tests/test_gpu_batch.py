@@ -95,18 +95,23 @@ def test_batch_grouped_matches_separate_runs(tmp_path):
     for s in alone:
         s.autotune()
         s.advance(0, 6)
-    batch = fb.Batch(together)
+    batch = fb.Batch(together)  # advanced 6 steps below
     info = batch.info()
     print("grouped batch:", info)
     assert info["groups"] >= 2 and info["launches"] > 0
+    steps = 6
     batch.advance(2)
-    batch.advance(4)
+    batch.advance(steps - 2)
     worst = {False: 0.0, True: 0.0}
     for i, (s1, s2) in enumerate(zip(alone, together)):
         for f in ("q2", "q3", "pr"):
             e = rel(s2.get(f), s1.get(f))
             worst[i in precision] = max(worst[i in precision], e)
-            assert e <= 1e-12, (i, f, e)
+            # the grouped reductions (pressure mean) sum in another order; in
+            # the precision form such last-bit differences can move a TF32
+            # rounding, so its bound is the form's own tolerance against the
+            # FP64 path, 1e-9 per step
+            assert e <= (1e-9 * steps if i in precision else 1e-12), (i, f, e)
         h1, h2 = s1.last_history(), s2.last_history()
         assert h2[8] == h1[8] and h2[30] == h1[30]          # clock, fluid solves
         np.testing.assert_allclose(h2[:21], h1[:21], rtol=1e-10, atol=1e-14)
