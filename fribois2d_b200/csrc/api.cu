@@ -1780,9 +1780,65 @@ GroupKey group_key(const fb_ctx *c) {
             (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0};
 }
 
+// The product tile of a group's grouped launches, timed over the whole group
+// (the per-grid choice of fb_autotune is made on one case, whose few tiles
+// fill the GPU differently): forward products of every case into one
+// scratch output (their inputs untouched), a few launches per candidate.
+int group_gemm_tile(BatchGroup *bg, int *best) {
+    const int n = static_cast<int>(bg->members.size());
+    const Dev &d0 = bg->members[0]->d;
+    *best = bg->members[0]->plan_fwd.bn;
+    double *scratch = nullptr;
+    fb::GemmTask *tasks = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int r = FB_OK;
+    if (cudaMalloc(&scratch, sizeof(double) * static_cast<size_t>(d0.n3m) * d0.ldh) != cudaSuccess ||
+        cudaMalloc(&tasks, sizeof(fb::GemmTask) * n) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess)
+        r = FB_ERR_CUDA;
+    double best_ms = 1e30;
+    std::vector<fb::GemmTask> h(static_cast<size_t>(n));
+    for (int cand : {64, 128, fb::kPairTile + 128, fb::kPairTile + 192, fb::kPairTile + 256}) {
+        if (r) break;
+        for (int i = 0; i < n && !r; ++i) {
+            const fb_ctx *c = bg->members[static_cast<size_t>(i)];
+            const Dev &d = c->d;
+            fb::GemmTask &t = h[static_cast<size_t>(i)];
+            r = fb::tf32x3_plan(t.p, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, cand);
+            t.o = fb::GemmOut{scratch, d.ldh, nullptr, 0, nullptr, d.n2m, d.n3m};
+            t.status = d.status;
+        }
+        if (r) break;
+        if (cudaMemcpyAsync(tasks, h.data(), sizeof(fb::GemmTask) * n, cudaMemcpyHostToDevice, bg->st) != cudaSuccess) {
+            r = FB_ERR_CUDA;
+            break;
+        }
+        fb::launch_tf32x3_group(tasks, h[0].p, n, bg->st);
+        cudaEventRecord(e0, bg->st);
+        for (int k = 0; k < 3; ++k) fb::launch_tf32x3_group(tasks, h[0].p, n, bg->st);
+        cudaEventRecord(e1, bg->st);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            r = FB_ERR_CUDA;
+            break;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            *best = cand;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (tasks) cudaFree(tasks);
+    if (scratch) cudaFree(scratch);
+    return r;
+}
+
 // the precision form's task arrays (phcalc_tf32's launches, per case)
 int group_setup_tf32(BatchGroup *bg) {
     const int n = static_cast<int>(bg->members.size());
+    int bn = 0, r;
+    if ((r = group_gemm_tile(bg, &bn))) return r;
     std::vector<fb::GemmTask> gt(static_cast<size_t>(3 * n));
     std::vector<fb::SplitTask> sp(static_cast<size_t>(2 * n));
     std::vector<fb::ResidualTask> rt(static_cast<size_t>(n));
@@ -1791,9 +1847,17 @@ int group_setup_tf32(BatchGroup *bg) {
         const Dev &d = c->d;
         const size_t k = static_cast<size_t>(i), m = static_cast<size_t>(n);
         const int M = c->plan_fwd.M, N = c->plan_fwd.N;
-        gt[k] = {c->plan_fwd, fb::GemmOut{d.hmn, d.ldh, nullptr, 0, nullptr, M, N}, d.status};
-        gt[m + k] = {c->plan_bwd, fb::GemmOut{c->pw + d.P, d.P, nullptr, 0, c->zs_d, M, N}, d.status};
-        gt[2 * m + k] = {c->plan_bwd, fb::GemmOut{d.dph + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status};
+        fb::Tf32x3Plan pf{}, pb{};
+        if ((r = fb::tf32x3_plan(pf, c->pl_a, c->pl_zt, d.n2m, d.n3m, d.n3m, bn)) ||
+            (r = fb::tf32x3_plan(pb, c->pl_a2, c->pl_z, d.n2m, d.n3m, d.n3m, bn)))
+            return r;
+        if (i == 0) {
+            bg->plan_fwd = pf;
+            bg->plan_bwd = pb;
+        }
+        gt[k] = {pf, fb::GemmOut{d.hmn, d.ldh, nullptr, 0, nullptr, M, N}, d.status};
+        gt[m + k] = {pb, fb::GemmOut{c->pw + d.P, d.P, nullptr, 0, c->zs_d, M, N}, d.status};
+        gt[2 * m + k] = {pb, fb::GemmOut{d.dph + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status};
         sp[k] = {d.dph + d.P, d.P, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
         sp[m + k] = {d.hmn, d.ldh, c->pl_a2.hi, c->pl_a2.lo, c->pl_a2.ld, nullptr};
         rt[k] = {c->pw, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
@@ -1805,8 +1869,6 @@ int group_setup_tf32(BatchGroup *bg) {
     CK(cudaMemcpyAsync(bg->sp, sp.data(), sizeof(fb::SplitTask) * sp.size(), cudaMemcpyHostToDevice, bg->st));
     CK(cudaMemcpyAsync(bg->rt, rt.data(), sizeof(fb::ResidualTask) * rt.size(), cudaMemcpyHostToDevice, bg->st));
     CK(cudaStreamSynchronize(bg->st));
-    bg->plan_fwd = bg->members[0]->plan_fwd;
-    bg->plan_bwd = bg->members[0]->plan_bwd;
     bg->tf32 = true;
     return FB_OK;
 }
