@@ -1834,6 +1834,62 @@ int group_gemm_tile(BatchGroup *bg, int *best) {
     return r;
 }
 
+// The windowed helsolve's tile height for the group's launches, timed over
+// the whole group like the GEMM tile (q2 and q3 of every case saved and
+// restored around the trial launches; rhs2/rhs3 are only read).
+int group_helsolve_tile(BatchGroup *bg) {
+    const int n = static_cast<int>(bg->members.size());
+    const Dev &d0 = bg->members[0]->d;
+    const size_t fb = static_cast<size_t>(d0.NK) * d0.P;
+    double *save = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int r = FB_OK;
+    if (cudaMalloc(&save, sizeof(double) * 2 * fb * n) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess)
+        r = FB_ERR_CUDA;
+    for (int i = 0; i < n && !r; ++i) {
+        const Dev &d = bg->members[static_cast<size_t>(i)]->d;
+        if (cudaMemcpyAsync(save + 2 * fb * i, d.q2, fb * sizeof(double), cudaMemcpyDeviceToDevice, bg->st) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(save + 2 * fb * i + fb, d.q3, fb * sizeof(double), cudaMemcpyDeviceToDevice, bg->st) !=
+                cudaSuccess)
+            r = FB_ERR_CUDA;
+    }
+    double best_ms = 1e30;
+    int best = bg->g.win_tk;
+    for (int cand : {32, 64}) {
+        if (r) break;
+        bg->g.win_tk = cand;
+        fb::glaunch_win_helsolve(bg->g, 0, bg->st);
+        cudaEventRecord(e0, bg->st);
+        for (int k = 0; k < 3; ++k) fb::glaunch_win_helsolve(bg->g, 0, bg->st);
+        cudaEventRecord(e1, bg->st);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            r = FB_ERR_CUDA;
+            break;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cand;
+        }
+    }
+    bg->g.win_tk = best;
+    for (int i = 0; i < n && save && !r; ++i) {
+        const Dev &d = bg->members[static_cast<size_t>(i)]->d;
+        if (cudaMemcpyAsync(d.q2, save + 2 * fb * i, fb * sizeof(double), cudaMemcpyDeviceToDevice, bg->st) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(d.q3, save + 2 * fb * i + fb, fb * sizeof(double), cudaMemcpyDeviceToDevice, bg->st) !=
+                cudaSuccess)
+            r = FB_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(bg->st) != cudaSuccess && !r) r = FB_ERR_CUDA;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (save) cudaFree(save);
+    return r;
+}
+
 // the precision form's task arrays (phcalc_tf32's launches, per case)
 int group_setup_tf32(BatchGroup *bg) {
     const int n = static_cast<int>(bg->members.size());
@@ -1920,6 +1976,8 @@ int group_setup(BatchGroup *bg) {
     CB(cublasSetWorkspace(bg->blas, bg->ws, 32u << 20));
     bg->cbody = c0->hc.deck.cbody;
     bg->report = c0->report && c0->d.nlm;
+    int r;
+    if ((r = group_helsolve_tile(bg))) return r;
     if (c0->poisson_mode == FB_POISSON_TF32X3) return group_setup_tf32(bg);
     return FB_OK;
 }

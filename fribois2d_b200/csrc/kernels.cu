@@ -78,16 +78,19 @@ __device__ __forceinline__ void cfl_body(const Dev &d) {
     __shared__ bool last;
     const int t = threadIdx.x, nt = blockDim.x;
     const int b = blockIdx.x, nb = gridDim.x;
-    const long cells = static_cast<long>(d.n2m) * d.n3m;
     double qcf = 1.0e-8, q3a = 0.0;
-    for (long idx = static_cast<long>(b) * nt + t; idx < cells; idx += static_cast<long>(nb) * nt) {
-        const int j = static_cast<int>(idx % d.n2m) + 1, k = static_cast<int>(idx / d.n2m) + 1;
-        const int jp = j + 1, kp = k + 1;
-        const double udx2 = d.udx2m[j], udx3 = d.udx3m[k];
-        const double q = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
-                          fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
-        qcf = fmax(qcf, q);
-        q3a = q3a + Fv(d.q3, j, k) * (d.zz[kp] - d.zz[k]) * (d.rc[jp] - d.rc[j]);
+    // rows k over the blocks, columns j over the threads (no index division)
+    for (int k = b + 1; k <= d.n3m; k += nb) {
+        const int kp = k + 1;
+        const double udx3 = d.udx3m[k], dz = d.zz[kp] - d.zz[k];
+        for (int j = t + 1; j <= d.n2m; j += nt) {
+            const int jp = j + 1;
+            const double udx2 = d.udx2m[j];
+            const double q = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
+                              fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
+            qcf = fmax(qcf, q);
+            q3a = q3a + Fv(d.q3, j, k) * dz * (d.rc[jp] - d.rc[j]);
+        }
     }
     const double pm = block_reduce_fast<true>(qcf, sh);
     const double ps = block_reduce_fast<false>(q3a, sh);
@@ -1669,7 +1672,7 @@ int group_stride_blocks(const Dev &d) {
     const long cells = static_cast<long>(d.n2m) * d.n3m;
     return static_cast<int>(std::max<long>(1, std::min<long>((cells + 2047) / 2048, 148L * 8)));
 }
-void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(stride_blocks(d)), dim3(256), 0, s, d); }
+void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(std::min(d.n3m, 148 * 8)), dim3(256), 0, s, d); }
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
 int nl_tiles(const Dev &d) { return ((d.n2m + kNlJ - 1) / kNlJ) * ((d.n3m + kNlK - 1) / kNlK); }
 
@@ -1731,7 +1734,8 @@ inline dim3 zgrid(dim3 g, const Group &gr) { return dim3(g.x, g.y, static_cast<u
 }  // namespace
 
 void glaunch_cfl(const Group &g, cudaStream_t s) {
-    pdl(kg_cfl, zgrid(dim3(group_stride_blocks(g.rep)), g), dim3(256), 0, s, g.cases);
+    pdl(kg_cfl, zgrid(dim3(std::max(1, std::min(g.rep.n3m, (2 * 148 * 8 + g.n - 1) / g.n))), g), dim3(256), 0, s,
+        g.cases);
 }
 void glaunch_boucdq(const Group &g, int n, cudaStream_t s) {
     pdl(kg_boucdq, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases, n);
