@@ -70,7 +70,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lgomp", "-Xcompiler", "-fPIC"]
+    cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcublasLt", "-lgomp", "-Xcompiler", "-fPIC"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -1,5 +1,6 @@
 // C ABI of the B200-native FRiBoIS2D fluid time step (include/fribois2d.h):
 // context set-up, device memory, substep orchestration, CUDA-graph replay.
+#include <cublasLt.h>
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
@@ -38,6 +39,14 @@ struct fb_ctx {
     cudaStream_t side = nullptr;              // marker set-up branch
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cublasHandle_t blas = nullptr;
+    void *blas_ws = nullptr;                  // 32 MB workspace of cuBLAS / cuBLASLt
+    // FP64 transforms through cuBLASLt with an algorithm timed per grid size
+    // (fb_autotune); [0] forward hmn = dph zmmt^T, [1] backward dph = hmn zmm^T
+    cublasLtHandle_t lt = nullptr;
+    cublasLtMatmulDesc_t lt_op = nullptr;
+    cublasLtMatrixLayout_t lt_l[6] = {};      // A, B, C of the forward, then of the backward product
+    cublasLtMatmulAlgo_t lt_algo[2] = {};
+    bool lt_on[2] = {false, false};
     Dev d{};
     SubDev sub[3]{};
     double usdtal[3] = {0, 0, 0};
@@ -410,6 +419,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         void *ws = nullptr;
         CK(cudaMalloc(&ws, 32u << 20));
         c->allocs.push_back(ws);
+        c->blas_ws = ws;
         CB(cublasSetWorkspace(c->blas, ws, 32u << 20));
     }
 
@@ -578,7 +588,20 @@ void coefs(const fb_ctx *c, int ns, int n, double &al, double &ga, double &ro) {
     }
 }
 
+// cuBLASLt form of product w (0 forward, 1 backward) with algorithm a
+int gemm_lt(fb_ctx *c, int w, const cublasLtMatmulAlgo_t *a) {
+    const Dev &d = c->d;
+    const double one = 1.0, zero = 0.0;
+    const double *A = w ? d.hmn : d.dph + d.P, *B = w ? c->zmm : c->zmmt;
+    double *C = w ? d.dph + d.P : d.hmn;
+    cublasLtMatrixLayout_t *l = c->lt_l + 3 * w;
+    CB(cublasLtMatmul(c->lt, c->lt_op, &one, A, l[0], B, l[1], &zero, C, l[2], C, l[2], a, c->blas_ws, 32u << 20,
+                      c->stream));
+    return FB_OK;
+}
+
 int gemm_fwd(fb_ctx *c) {   // phcalc_outflow.F90:31, hmn = dph * zmmt^T
+    if (c->lt_on[0]) return gemm_lt(c, 0, &c->lt_algo[0]);
     const Dev &d = c->d;
     const double one = 1.0, zero = 0.0;
     CB(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, d.dph + d.P, d.P,
@@ -587,10 +610,111 @@ int gemm_fwd(fb_ctx *c) {   // phcalc_outflow.F90:31, hmn = dph * zmmt^T
 }
 
 int gemm_bwd(fb_ctx *c) {   // phcalc_outflow.F90:61,65-69, dph = vmn * zmm^T
+    if (c->lt_on[1]) return gemm_lt(c, 1, &c->lt_algo[1]);
     const Dev &d = c->d;
     const double one = 1.0, zero = 0.0;
     CB(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, d.hmn, d.ldh, c->zmm,
                    d.n3m, &zero, d.dph + d.P, d.P));
+    return FB_OK;
+}
+
+// mean device ms of `reps` calls of fn after one warm-up call (-1 on error)
+template <class F>
+double time_calls(fb_ctx *c, int reps, F fn) {
+    if (fn()) return -1.0;
+    if (cudaEventRecord(c->ev0, c->stream) != cudaSuccess) return -1.0;
+    for (int i = 0; i < reps; ++i)
+        if (fn()) return -1.0;
+    float ms = 0.f;
+    if (cudaEventRecord(c->ev1, c->stream) != cudaSuccess || cudaEventSynchronize(c->ev1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1) != cudaSuccess)
+        return -1.0;
+    return static_cast<double>(ms) / reps;
+}
+
+// The FP64 transforms' algorithms: cuBLASLt's heuristic candidates for each
+// product timed against cublasDgemm on the live buffers (hmn and dph are
+// work arrays between steps; both are saved and restored all the same).
+// The fastest is kept, so the products follow the reference's DGEMMs with
+// a summation order that cuBLAS picks per shape.  The choice is cached per
+// (n2, n3) for the process.
+int tune_dgemm(fb_ctx *c) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, std::array<std::pair<bool, cublasLtMatmulAlgo_t>, 2>> cache;
+    const Dev &d = c->d;
+    const std::pair<int, int> key(d.n2, d.n3);
+    if (!c->lt) {
+        CB(cublasLtCreate(&c->lt));
+        CB(cublasLtMatmulDescCreate(&c->lt_op, CUBLAS_COMPUTE_64F, CUDA_R_64F));
+        const cublasOperation_t tn = CUBLAS_OP_N, tt = CUBLAS_OP_T;
+        CB(cublasLtMatmulDescSetAttribute(c->lt_op, CUBLASLT_MATMUL_DESC_TRANSA, &tn, sizeof(tn)));
+        CB(cublasLtMatmulDescSetAttribute(c->lt_op, CUBLASLT_MATMUL_DESC_TRANSB, &tt, sizeof(tt)));
+        const uint64_t m = d.n2m, n = d.n3m;
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[0], CUDA_R_64F, m, n, d.P));
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[1], CUDA_R_64F, n, n, n));
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[2], CUDA_R_64F, m, n, d.ldh));
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[3], CUDA_R_64F, m, n, d.ldh));
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[4], CUDA_R_64F, n, n, n));
+        CB(cublasLtMatrixLayoutCreate(&c->lt_l[5], CUDA_R_64F, m, n, d.P));
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            for (int w = 0; w < 2; ++w) {
+                c->lt_on[w] = it->second[static_cast<size_t>(w)].first;
+                c->lt_algo[w] = it->second[static_cast<size_t>(w)].second;
+            }
+            return FB_OK;
+        }
+    }
+    const size_t fbytes = static_cast<size_t>(d.NK) * d.P * sizeof(double);
+    const size_t hbytes = static_cast<size_t>(d.n3m) * d.ldh * sizeof(double);
+    char *save = nullptr;
+    CK(cudaMalloc(&save, fbytes + hbytes));
+    CK(cudaMemcpyAsync(save, d.dph, fbytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(save + fbytes, d.hmn, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+    cublasLtMatmulPreference_t pref = nullptr;
+    int r = FB_OK;
+    const uint64_t wsb = 32u << 20;
+    if (cublasLtMatmulPreferenceCreate(&pref) != CUBLAS_STATUS_SUCCESS ||
+        cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &wsb, sizeof(wsb)) !=
+            CUBLAS_STATUS_SUCCESS)
+        r = FB_ERR_CUDA;
+    for (int w = 0; w < 2 && !r; ++w) {
+        c->lt_on[w] = false;
+        const double base = time_calls(c, 5, [&] { return w ? gemm_bwd(c) : gemm_fwd(c); });
+        if (base < 0.0) {
+            r = FB_ERR_CUDA;
+            break;
+        }
+        cublasLtMatmulHeuristicResult_t res[16];
+        int cnt = 0;
+        cublasLtMatrixLayout_t *l = c->lt_l + 3 * w;
+        if (cublasLtMatmulAlgoGetHeuristic(c->lt, c->lt_op, l[0], l[1], l[2], l[2], pref, 16, res, &cnt) !=
+            CUBLAS_STATUS_SUCCESS)
+            cnt = 0;
+        double best = 0.98 * base;   // a candidate must beat cublasDgemm clearly
+        for (int i = 0; i < cnt; ++i) {
+            if (res[i].state != CUBLAS_STATUS_SUCCESS || res[i].workspaceSize > wsb) continue;
+            const double t = time_calls(c, 5, [&] { return gemm_lt(c, w, &res[i].algo); });
+            if (t > 0.0 && t < best) {
+                best = t;
+                c->lt_algo[w] = res[i].algo;
+                c->lt_on[w] = true;
+            }
+        }
+        cudaGetLastError();
+    }
+    if (pref) cublasLtMatmulPreferenceDestroy(pref);
+    cudaMemcpyAsync(d.dph, save, fbytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(d.hmn, save + fbytes, hbytes, cudaMemcpyDeviceToDevice, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(save);
+    if (r) return r;
+    if (e != cudaSuccess) return FB_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = {std::make_pair(c->lt_on[0], c->lt_algo[0]), std::make_pair(c->lt_on[1], c->lt_algo[1])};
     return FB_OK;
 }
 
@@ -966,6 +1090,10 @@ int fb_destroy(fb_ctx *c) {
     if (c->rd_h) cudaFreeHost(c->rd_h);
     if (c->coef_pini) cudaFreeHost(c->coef_pini);
     if (c->blas) cublasDestroy(c->blas);
+    for (cublasLtMatrixLayout_t l : c->lt_l)
+        if (l) cublasLtMatrixLayoutDestroy(l);
+    if (c->lt_op) cublasLtMatmulDescDestroy(c->lt_op);
+    if (c->lt) cublasLtDestroy(c->lt);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->side) cudaStreamDestroy(c->side);
@@ -2269,6 +2397,10 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
         if (r) return r;
         std::lock_guard<std::mutex> lk(mu);
         cache[key] = std::make_pair(tk, bn);
+    }
+    {
+        int rt;
+        if ((rt = tune_dgemm(c))) return rt;
     }
     c->tune_tk = tk;
     for (int n = 0; n < c->d.nsst; ++n) c->sub[n].win_tk = tk;
