@@ -400,16 +400,30 @@ __global__ void __launch_bounds__(256, kNlBlocksPerSM) k_nl_rhs(Dev d, double al
 
 // ------------------------------------------------------------ MLS forcing
 
-__device__ int nearest_sorted(const double *a, int lo, int hi, double x) {
-    // first index of min |a(i) - x| over a(lo..hi), a strictly increasing
-    int l = lo, h = hi;
+__device__ int nearest_sorted(const double *a, int lo, int hi, double x, int guess) {
+    // first index of min |a(i) - x| over a(lo..hi), a strictly increasing.
+    // The bracket a(l) <= x < a(l+1) is unique: it is searched from the
+    // marker's index of the previous step (a few steps) and by bisection
+    // when that guess is off; both give the same l.
     if (x <= a[lo]) return lo;
     if (x >= a[hi]) return hi;
-    while (h - l > 1) {
-        int m = (l + h) >> 1;
-        if (a[m] <= x) l = m;
-        else h = m;
+    int l = -1;
+    if (guess >= lo && guess < hi) {
+        int g = guess;
+        for (int s = 0; s < 16 && g > lo && a[g] > x; ++s) --g;
+        for (int s = 0; s < 16 && g < hi - 1 && a[g + 1] <= x; ++s) ++g;
+        if (a[g] <= x && x < a[g + 1]) l = g;
     }
+    if (l < 0) {
+        int h = hi;
+        l = lo;
+        while (h - l > 1) {
+            int m = (l + h) >> 1;
+            if (a[m] <= x) l = m;
+            else h = m;
+        }
+    }
+    const int h = l + 1;
     double dl = fabs(a[l] - x), dh = fabs(a[h] - x);
     return (dh < dl) ? h : l;
 }
@@ -433,16 +447,17 @@ __device__ __forceinline__ void lgrdist_body(const Dev &d) {
         return;
     }
     int ind;
-    d.lmind[4 * i + 0] = nearest_sorted(d.rc, 1, d.n2, y);
+    const int g0 = d.lmind[4 * i + 0], g1 = d.lmind[4 * i + 1], g2 = d.lmind[4 * i + 2], g3 = d.lmind[4 * i + 3];
+    d.lmind[4 * i + 0] = nearest_sorted(d.rc, 1, d.n2, y, g0);
     if (z < d.zm[1] && z > 0.0) ind = 1;
     else if (z > d.zm[d.n3m] && z < d.alx3) ind = d.n3m;
-    else ind = nearest_sorted(d.zm, 1, d.n3, z);
+    else ind = nearest_sorted(d.zm, 1, d.n3, z, g1);
     d.lmind[4 * i + 1] = ind;
     if (y < d.rm[1] && y > 0.0) ind = 1;
     else if (y > d.rm[d.n2m] && y < d.rext2) ind = d.n2m;
-    else ind = nearest_sorted(d.rm, 1, d.n2, y);
+    else ind = nearest_sorted(d.rm, 1, d.n2, y, g2);
     d.lmind[4 * i + 2] = ind;
-    d.lmind[4 * i + 3] = nearest_sorted(d.zz, 1, d.n3, z);
+    d.lmind[4 * i + 3] = nearest_sorted(d.zz, 1, d.n3, z, g3);
 }
 
 __global__ void k_lgrdist(Dev d) {
@@ -705,39 +720,43 @@ __device__ __forceinline__ void spread_chains_body(const Dev &d) {
                                  : (j >= 1 && j <= d.n2m && k >= 2 && k <= d.n3m);
     if (!used) return;
     const size_t plane = static_cast<size_t>(dir) * d.NK * d.P;
-    // lowest-index toucher only
-    for (int dj = 0; dj <= 2; ++dj)
-        for (int dk = 0; dk <= 2; ++dk) {
-            const int sj = j - dj, sk = k - dk;
-            if (sj < 1 || sk < 0) continue;
-            const size_t cell = plane + fidx(d, sj, sk);
-            const int c = min(d.bcnt[cell], d.bcap);
-            for (int q = 0; q < c; ++q)
-                if (d.bucket[cell * d.bcap + q] < n) return;
-        }
-    // walk the touchers in increasing marker index, linking their slots
-    d.chead[g] = 1;
-    int prev_slot = g, last = n;
-    for (;;) {
-        int best = -1, best_slot = -1;
-        for (int dj = 0; dj <= 2; ++dj)
-            for (int dk = 0; dk <= 2; ++dk) {
-                const int sj = j - dj, sk = k - dk;
-                if (sj < 1 || sk < 0) continue;
-                const size_t cell = plane + fidx(d, sj, sk);
-                const int c = min(d.bcnt[cell], d.bcap);
-                for (int q = 0; q < c; ++q) {
-                    const int nn = d.bucket[cell * d.bcap + q];
-                    if (nn > last && (best < 0 || nn < best)) {
-                        best = nn;
-                        best_slot = (2 * nn + dir) * kSD + dj * 3 + dk;
-                    }
-                }
+    // the cell's touchers are the markers registered at the 3 x 3 possible
+    // box start cells: all counts first, then all entries (two rounds of
+    // loads); a lower-index toucher means this slot is not the head
+    int cnt[9];
+    size_t base[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int sj = j - q / 3, sk = k - q % 3;
+        const bool ok = !(sj < 1 || sk < 0);
+        const size_t cell = plane + fidx(d, ok ? sj : 1, ok ? sk : 0);
+        cnt[q] = ok ? min(d.bcnt[cell], d.bcap) : 0;
+        base[q] = cell * d.bcap;
+    }
+    constexpr int kMaxTouch = 9 * 16;   // 9 start cells x bucket capacity (bcap <= 16)
+    int ln[kMaxTouch], ls[kMaxTouch];   // touchers after n, ascending marker index
+    int L = 0;
+    for (int q = 0; q < 9; ++q)
+        for (int e = 0; e < cnt[q] && e < 16; ++e) {
+            const int nn = d.bucket[base[q] + e];
+            if (nn < n) return;
+            if (nn == n || L >= kMaxTouch) continue;
+            // insertion in increasing marker index (a marker has one box start cell)
+            int p = L++;
+            while (p > 0 && ln[p - 1] > nn) {
+                ln[p] = ln[p - 1];
+                ls[p] = ls[p - 1];
+                --p;
             }
-        if (best < 0) break;
-        d.chain[prev_slot] = best_slot;
-        prev_slot = best_slot;
-        last = best;
+            ln[p] = nn;
+            ls[p] = (2 * nn + dir) * kSD + q;   // node (dj, dk) = (q / 3, q % 3) of marker nn
+        }
+    // this slot heads the cell's chain: link the touchers in marker order
+    d.chead[g] = 1;
+    int prev_slot = g;
+    for (int p = 0; p < L; ++p) {
+        d.chain[prev_slot] = ls[p];
+        prev_slot = ls[p];
     }
     d.chain[prev_slot] = -1;
 }
