@@ -1299,7 +1299,7 @@ __device__ __forceinline__ void loads_finish_body(const Dev &d) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_loads_finish(Dev d) {
+__global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
     FB_GRID_WAIT();
     loads_finish_body(d);
 }
@@ -1487,7 +1487,7 @@ __device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode
     }
 }
 
-__global__ void __launch_bounds__(256) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
+__global__ void __launch_bounds__(512) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
     FB_GRID_WAIT();
     rigid_body(d, hist_rows, mode, fin);
 }
@@ -1655,13 +1655,13 @@ __global__ void kg_loads_probe(const GroupCase *__restrict__ g) {
     loads_probe_body(d);
 }
 
-__global__ void __launch_bounds__(256) kg_loads_finish(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(1024) kg_loads_finish(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     stage_case(g, &d);
     loads_finish_body(d);
 }
 
-__global__ void __launch_bounds__(256) kg_rigid(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(512) kg_rigid(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     stage_case(g, &d);
     rigid_body(d, g[blockIdx.z].hist_rows, RIGID_STEP, nullptr);
@@ -1737,13 +1737,13 @@ void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
     pdl(k_loads_probe, dim3((3 * d.nlm + 63) / 64), dim3(64), 0, s, d);
-    pdl(k_loads_finish, dim3(1), dim3(256), 0, s, d);
+    pdl(k_loads_finish, dim3(1), dim3(1024), 0, s, d);
 }
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
     pdl(k_diag, dim3(std::min(stride_blocks(d), 2048)), dim3(256), 0, s, d, hist_rows);
 }
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin) {
-    if (d.nlm) pdl(k_rigid, dim3(1), dim3(256), 0, s, d, hist_rows, mode, fin);
+    if (d.nlm) pdl(k_rigid, dim3(1), dim3(512), 0, s, d, hist_rows, mode, fin);
 }
 
 
@@ -1807,10 +1807,10 @@ void glaunch_loads(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
     if (!d.nlm) return;
     pdl(kg_loads_probe, zgrid(dim3((3 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
-    pdl(kg_loads_finish, zgrid(dim3(1), g), dim3(256), 0, s, g.cases);
+    pdl(kg_loads_finish, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases);
 }
 void glaunch_rigid(const Group &g, cudaStream_t s) {
-    if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(256), 0, s, g.cases);
+    if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(512), 0, s, g.cases);
 }
 void glaunch_diag(const Group &g, cudaStream_t s) {
     pdl(kg_diag, zgrid(dim3(std::min(group_stride_blocks(g.rep), 2048)), g), dim3(256), 0, s, g.cases);
