@@ -54,7 +54,8 @@ struct CoefShared {      // y or z systems: 1-D factors shared by all lines
     }
 };
 
-struct CoefMode {        // Poisson mode: reciprocal pivots per mode, 1-based off-diagonals
+struct CoefModeS {       // Poisson mode: reciprocal pivots of the mode and the 1-based y
+                         // off-diagonals, staged in shared memory
     const double *g, *amphj, *apphj;
     int n;
     template <int M>
@@ -63,7 +64,7 @@ struct CoefMode {        // Poisson mode: reciprocal pivots per mode, 1-based of
         for (int t = 0; t < M; ++t)
             if (t < cnt) {
                 const int i = i0 + t;
-                c[t] = (i == 0) ? 0.0 : -(__ldg(amphj + i + 1) * __ldg(g + i - 1));
+                c[t] = (i == 0) ? 0.0 : -(amphj[i + 1] * g[i - 1]);
             }
     }
     template <int M>
@@ -72,14 +73,14 @@ struct CoefMode {        // Poisson mode: reciprocal pivots per mode, 1-based of
         for (int t = 0; t < M; ++t)
             if (t < cnt) {
                 const int i = i0 + t;
-                c[t] = (i == n - 1) ? 0.0 : -(__ldg(apphj + i + 1) * __ldg(g + i));
+                c[t] = (i == n - 1) ? 0.0 : -(apphj[i + 1] * g[i]);
             }
     }
     template <int M>
     __device__ __forceinline__ void loadG(double (&c)[M], int i0, int cnt) const {
 #pragma unroll
         for (int t = 0; t < M; ++t)
-            if (t < cnt) c[t] = __ldg(g + i0 + t);
+            if (t < cnt) c[t] = g[i0 + t];
     }
 };
 
@@ -335,8 +336,19 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
     const double *by = (sys == 0) ? by2 : by3;
     double *buf = sm + wl * (d.n2 + 1);
     constexpr int kT = 32 * kYWarps;
+    // Poisson modes: the mode's reciprocal pivots and the y off-diagonals
+    // are staged with the line, so the recurrences read shared memory only
+    double *pgs = sm + kYLines * (d.n2 + 1) + wl * (d.n2m + 1);
+    double *ams = sm + kYLines * (d.n2 + 1) + kYLines * (d.n2m + 1), *aps = ams + (d.n2m + 2);
+    if (kKind == 2) {
+        for (int i = threadIdx.x; i <= d.n2m; i += blockDim.x) {
+            ams[i] = __ldg(d.amphj + i);
+            aps[i] = __ldg(d.apphj + i);
+        }
+    }
     // coalesced staging: thread-strided loads, all independent
     if (live) {
+        const double *pgr = d.pg + static_cast<size_t>(r) * d.ldh;
 #pragma unroll
         for (int it = 0; it < M; ++it) {
             const int i = tl + kT * it;
@@ -345,6 +357,8 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
                 if (kKind != 2) {
                     if (sys == 0) v = (i >= 1 && i <= n - 2) ? v * __ldg(by + i + 1) : 0.0;
                     else v = v * __ldg(by + i + 1);
+                } else {
+                    pgs[i] = __ldg(pgr + i);
                 }
                 buf[i] = v;
             }
@@ -358,8 +372,7 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
     for (int t = 0; t < M; ++t)
         if (t < cnt) v[t] = buf[i0 + t];
     if (kKind == 2) {
-        group_line<M, kYWarps>(v, i0, cnt, CoefMode{d.pg + static_cast<size_t>(live ? r : 0) * d.ldh, d.amphj, d.apphj, n},
-                               shx[wl]);
+        group_line<M, kYWarps>(v, i0, cnt, CoefModeS{pgs, ams, aps, n}, shx[wl]);
     } else {
         const ScanSys &s = (sys == 0) ? s2 : s3;
         group_line<M, kYWarps>(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shx[wl]);
@@ -752,12 +765,20 @@ __global__ void __launch_bounds__(kYLines * kYWarps * 32) kg_ylines_poisson(cons
 
 namespace {
 
+// line buffers; for the Poisson modes also the pivot rows and the two y
+// off-diagonal arrays
+size_t ylines_smem(const Dev &d, int kind) {
+    size_t n = static_cast<size_t>(kYLines) * (d.n2 + 1);
+    if (kind == 2) n += static_cast<size_t>(kYLines) * (d.n2m + 1) + 2 * static_cast<size_t>(d.n2m + 2);
+    return n * sizeof(double);
+}
+
 template <int kKind>
 void ylaunch(const Dev &d, const SubDev *sd, cudaStream_t st) {
     const int lines = (kKind == 2) ? d.n3m : d.n3m + (d.n3m - 1);
     const int blocks = (lines + kYLines - 1) / kYLines;
     const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
-    const size_t smem = static_cast<size_t>(kYLines) * (d.n2 + 1) * sizeof(double);
+    const size_t smem = ylines_smem(d, kKind);
     const ScanSys z{nullptr, nullptr, nullptr};
     const ScanSys s2 = sd ? sd->sy2 : z, s3 = sd ? sd->sy3 : z;
     const double *b2 = sd ? sd->by2 : nullptr, *b3 = sd ? sd->by3 : nullptr;
@@ -855,7 +876,7 @@ void glaunch_scan_poisson(const Group &g, cudaStream_t st) {
     const Dev &d = g.rep;
     const int blocks = (d.n3m + kYLines - 1) / kYLines;
     const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
-    const size_t smem = static_cast<size_t>(kYLines) * (d.n2 + 1) * sizeof(double);
+    const size_t smem = ylines_smem(d, 2);
     const int threads = kYLines * kYWarps * 32;
     const dim3 grid(blocks, 1, g.n);
     if (m <= 9) pdl(kg_ylines_poisson<9>, grid, dim3(threads), smem, st, g.cases);
