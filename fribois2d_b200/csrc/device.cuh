@@ -87,6 +87,16 @@ struct GroupCase {
 };
 
 #ifdef __CUDACC__
+// asynchronous 8-byte global -> shared copies (no register round trip, all
+// of a thread's copies in flight at once); cp_wait completes this thread's
+// copies, a barrier then publishes them to the block
+__device__ __forceinline__ void cp8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // copies case blockIdx.z's view of a group (and the constants of substep n
 // when ss is given) to shared memory, then waits for the preceding kernel
 // (programmatic dependent launch) and the block.  The group array is written

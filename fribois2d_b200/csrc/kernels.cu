@@ -58,16 +58,6 @@ __device__ double block_reduce_fast(double v, double *sh) {
     return r;
 }
 
-// asynchronous 8-byte global -> shared copies (no register round trip, all
-// of a thread's copies in flight at once); cp_wait completes this thread's
-// copies, a barrier then publishes them to the block
-__device__ __forceinline__ void cp8(double *dst, const double *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
-                 "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // ------------------------------------------------------------ cfl
 
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.

@@ -591,22 +591,29 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
 
     // 1. coefficients and the right-hand side tile scaled by the y row
     //    normalisers; A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r)
+    // all of the tile's copies are issued at once (cp.async); each thread then
+    // scales the rhs values it copied by the y row normalisers
     for (int c = threadIdx.x; c < sh.ncy; c += kWThreads) {
         const int i = iy0 + c;
-        const bool ok = (i >= 0 && i < ny);
-        cya[c] = ok ? __ldg(sy.a + i) : 0.0;
-        cye[c] = ok ? __ldg(sy.e + i) : 0.0;
-        cyg[c] = ok ? __ldg(sy.g + i) : 0.0;
+        if (i >= 0 && i < ny) {
+            cp8(cya + c, sy.a + i);
+            cp8(cye + c, sy.e + i);
+            cp8(cyg + c, sy.g + i);
+        } else {
+            cya[c] = cye[c] = cyg[c] = 0.0;
+        }
     }
     for (int c = threadIdx.x; c < sh.ncz; c += kWThreads) {
         const int i = iz0 + c;
-        const bool ok = (i >= 0 && i < nz);
-        cza[c] = ok ? __ldg(sz.a + i) : 0.0;
-        cze[c] = ok ? __ldg(sz.e + i) : 0.0;
-        czg[c] = ok ? __ldg(sz.g + i) : 0.0;
+        if (i >= 0 && i < nz) {
+            cp8(cza + c, sz.a + i);
+            cp8(cze + c, sz.e + i);
+            cp8(czg + c, sz.g + i);
+        } else {
+            cza[c] = cze[c] = czg[c] = 0.0;
+        }
     }
     {
-        constexpr int kRB = 4;   // rows per batch
         constexpr int kCC = 3;   // column chunks of 32 (cols <= 96)
         int jc[kCC];
         bool okc[kCC];
@@ -618,22 +625,26 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
             okc[cc] = (c < cols) && (jc[cc] >= jlo && jc[cc] <= d.n2m);
             sc[cc] = okc[cc] ? __ldg(by + jc[cc]) : 0.0;
         }
-        for (int r0 = w * kRB; r0 < rows; r0 += kWarps * kRB) {
-            double v[kRB][kCC];
+        for (int r = w; r < rows; r += kWarps) {
+            const int k = k0 - Kz + r;
+            const bool kok = (k >= klo && k <= d.n3m);
 #pragma unroll
-            for (int u = 0; u < kRB; ++u) {
-                const int r = r0 + u, k = k0 - Kz + r;
-                const bool kok = (r < rows) && (k >= klo && k <= d.n3m);
-#pragma unroll
-                for (int cc = 0; cc < kCC; ++cc)
-                    v[u][cc] = (kok && okc[cc]) ? __ldcg(rhs + fidx(d, jc[cc], k)) * sc[cc] : 0.0;
+            for (int cc = 0; cc < kCC; ++cc) {
+                if (lane + 32 * cc >= cols) continue;
+                double *dst = A + r * sh.pitch + lane + 32 * cc;
+                if (kok && okc[cc]) cp8(dst, rhs + fidx(d, jc[cc], k));
+                else *dst = 0.0;
             }
+        }
+        cp_wait();
+        for (int r = w; r < rows; r += kWarps) {
+            const int k = k0 - Kz + r;
+            const bool kok = (k >= klo && k <= d.n3m);
 #pragma unroll
-            for (int u = 0; u < kRB; ++u) {
-                const int r = r0 + u;
-#pragma unroll
-                for (int cc = 0; cc < kCC; ++cc)
-                    if (r < rows && lane + 32 * cc < cols) A[r * sh.pitch + lane + 32 * cc] = v[u][cc];
+            for (int cc = 0; cc < kCC; ++cc) {
+                if (lane + 32 * cc >= cols || !(kok && okc[cc])) continue;
+                double *dst = A + r * sh.pitch + lane + 32 * cc;
+                *dst = *dst * sc[cc];
             }
         }
     }
