@@ -54,6 +54,8 @@ struct fb_ctx {
     int hist_cap = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    cudaGraph_t fgraph = nullptr;             // fluid step alone (fb_fluid_tsch), fixed dt
+    cudaGraphExec_t fgraph_exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     double *zmm = nullptr, *zmmt = nullptr;  // Poisson eigenvectors and inverse
@@ -937,8 +939,12 @@ int enqueue_step(fb_ctx *c, int ns) {
 void drop_graph(fb_ctx *c) {
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->fgraph_exec) cudaGraphExecDestroy(c->fgraph_exec);
+    if (c->fgraph) cudaGraphDestroy(c->fgraph);
     c->graph_exec = nullptr;
     c->graph = nullptr;
+    c->fgraph_exec = nullptr;
+    c->fgraph = nullptr;
 }
 
 int read_status(fb_ctx *c, int *status) {
@@ -1081,8 +1087,7 @@ int fb_create(const char *input_dir, int device, fb_ctx **out) {
 int fb_destroy(fb_ctx *c) {
     if (!c) return FB_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    if (c->graph) cudaGraphDestroy(c->graph);
+    drop_graph(c);
     for (void *p : c->allocs)
         if (p) cudaFree(p);
     if (c->coef_pin) cudaFreeHost(c->coef_pin);
@@ -1106,8 +1111,26 @@ int fb_destroy(fb_ctx *c) {
 
 int fb_fluid_tsch(fb_ctx *c, int ns) {
     if (!c) return FB_ERR_STATE;
-    int r = enqueue_fluid(c, ns);
-    if (r) return r;
+    int r;
+    if (!c->vardt && ns >= 1) {
+        // fixed dt after the first step: the same launches every step,
+        // replayed from a graph captured at the first such call
+        if (!c->fgraph_exec) {
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            r = enqueue_fluid(c, ns);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (r || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return r ? r : FB_ERR_CUDA;
+            }
+            c->fgraph = g;
+            CK(cudaGraphInstantiate(&c->fgraph_exec, g, 0));
+        }
+        CK(cudaGraphLaunch(c->fgraph_exec, c->stream));
+    } else if ((r = enqueue_fluid(c, ns))) {
+        return r;
+    }
     int status = 0;
     if ((r = read_status(c, &status))) return r;
     return status;
