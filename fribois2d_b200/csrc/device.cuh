@@ -114,7 +114,7 @@ __device__ __forceinline__ void stage_case(const GroupCase *__restrict__ g, Dev 
     const int nt = blockDim.x * blockDim.y * blockDim.z;
     copy_words(g[blockIdx.z].d, sd, t, nt);
     if (ss) copy_words(g[blockIdx.z].s[n], ss, t, nt);
-    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory");
     __syncthreads();
 }
 #endif

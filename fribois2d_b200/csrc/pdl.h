@@ -14,7 +14,13 @@
 #include <cstring>
 #include <utility>
 
-#define FB_GRID_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+// After its wait, every block lets the next kernel of the stream launch: that
+// kernel's blocks take free SM slots while this grid's last blocks run and
+// wait in their own FB_GRID_WAIT, so the launch latency is hidden.  Since a
+// block triggers only once it is running, the next grid launches after all of
+// this grid's blocks have started: a waiting grid never holds slots that this
+// one still needs.
+#define FB_GRID_WAIT() asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory")
 
 namespace fb {
 
