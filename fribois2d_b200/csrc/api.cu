@@ -532,7 +532,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = dnew(c, &d.rigid, 18))) return st;
     if ((st = h2d(c, d.rigid, c->hc.rigid, 18 * sizeof(double)))) return st;
     if ((st = dnew(c, &d.forces, 8))) return st;
-    if ((st = dnew(c, &d.scal, fb::S_COUNT))) return st;
+    if ((st = dnew(c, &d.scal, fb::S_SLOTS))) return st;
     c->hist_cap = 4096;
     if ((st = dnew(c, &d.hist, static_cast<size_t>(c->hist_cap) * FB_HIST_COLS))) return st;
     if ((st = dnew(c, &d.red, static_cast<size_t>(3) * fb::kRedSlot))) return st;
@@ -901,9 +901,22 @@ int enqueue_fluid(fb_ctx *c, int ns) {
     }
     if (!c->vardt && (r = stage_impl(c, FB_ST_CFL, ns, 1))) return r;
     c->beta = c->dt / c->hc.grid.ren * 0.5;
+    // RK3: pr_submean of substeps 1 and 2 is deferred; nl_rhs and updvp of
+    // the next substep subtract the mean as they read pr, and the mean is
+    // kept for the entries updvp does not rewrite, which the last pr_submean
+    // brings up to date.  boucqt and the next boucdq share one launch.
+    const bool defer = (d.nsst == 3);
     for (int n = 1; n <= d.nsst; ++n) {
-        if ((r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
-        if ((r = stage_impl(c, FB_ST_NL_RHS, ns, n))) return r;
+        const bool pend = defer && n > 1;
+        double al, ga, ro;
+        coefs(c, ns, n, al, ga, ro);
+        if (!pend && (r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
+        if (pend) {
+            fb::launch_nl_rhs(d, al, ga, ro, c->stream, true);
+            c->own_launches += 1;
+        } else if ((r = stage_impl(c, FB_ST_NL_RHS, ns, n))) {
+            return r;
+        }
         if (d.nlm) {
             if (n == 1) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
             // the weights are ready: interpolation and spreading only
@@ -912,8 +925,24 @@ int enqueue_fluid(fb_ctx *c, int ns) {
         if ((r = stage_impl(c, FB_ST_HELSOLVE, ns, n))) return r;
         if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
         if ((r = stage_impl(c, FB_ST_PHCALC, ns, n))) return r;
-        if ((r = stage_impl(c, FB_ST_UPDVP, ns, n))) return r;
-        if ((r = stage_impl(c, FB_ST_PRSUBMEAN, ns, n))) return r;
+        if (pend) {
+            fb::launch_updvp_prcalc(d, al, al * c->beta, c->stream, true);
+            c->own_launches += 1;
+        } else if ((r = stage_impl(c, FB_ST_UPDVP, ns, n))) {
+            return r;
+        }
+        if (defer && n < d.nsst) {
+            double al1, ga1, ro1;
+            coefs(c, ns, n + 1, al1, ga1, ro1);
+            fb::launch_substep_mid(d, n == 1 ? fb::S_PRAVG1 : fb::S_PRAVG2, ga1, ro1, c->stream);
+            c->own_launches += 1;
+        } else if (defer) {
+            fb::launch_submean_boucqt(d, c->stream, true);
+            c->own_launches += 1;
+        } else if ((r = stage_impl(c, FB_ST_PRSUBMEAN, ns, n))) {
+            return r;
+        }
+        CK(cudaGetLastError());
     }
     if (d.nlm && c->hc.deck.cbody && (r = stage_impl(c, FB_ST_LOADS, ns, 1))) return r;
     return FB_OK;
@@ -2150,9 +2179,12 @@ int enqueue_group(BatchGroup *bg) {
     k += 1;
     const double one = 1.0, zero = 0.0;
     double **p = bg->ptr;
-    for (int s = 0; s < 3; ++s) {
-        fb::glaunch_boucdq(g, s, st);
-        fb::glaunch_nl_rhs(g, s, st);
+    for (int s = 0; s < 3; ++s) {   // pr_submean deferred as in enqueue_fluid
+        if (s == 0) {
+            fb::glaunch_boucdq(g, s, st);
+            k += 1;
+        }
+        fb::glaunch_nl_rhs(g, s, st, s > 0);
         if (s == 0) CK(cudaStreamWaitEvent(st, bg->join, 0));
         fb::glaunch_forcing(g, st);
         fb::glaunch_win_helsolve(g, s, st);
@@ -2178,9 +2210,10 @@ int enqueue_group(BatchGroup *bg) {
                                   p + 4 * n, d.n3m, &zero, p + 5 * n, d.P, n));
             k += 1;
         }
-        fb::glaunch_updvp_prcalc(g, s, st);
-        fb::glaunch_submean_boucqt(g, st);
-        k += 8;
+        fb::glaunch_updvp_prcalc(g, s, st, s > 0);
+        if (s < 2) fb::glaunch_substep_mid(g, s + 1, s == 0 ? fb::S_PRAVG1 : fb::S_PRAVG2, st);
+        else fb::glaunch_submean_boucqt(g, st, true);
+        k += 7;
     }
     if (bg->cbody) {
         fb::glaunch_loads(g, st);

@@ -131,7 +131,10 @@ struct Group {
 
 // device scalar slots
 enum Scal {
-    S_TIME = 0, S_CFLM, S_Q3AVG, S_NBCV, S_NBCW, S_PRAVG, S_QOUT, S_DT, S_STEP, S_CFLRAW, S_COUNT
+    S_TIME = 0, S_CFLM, S_Q3AVG, S_NBCV, S_NBCW, S_PRAVG, S_QOUT, S_DT, S_STEP, S_CFLRAW, S_COUNT,
+    // transient within a step (not part of the saved state): the pressure
+    // means of RK3 substeps 1 and 2 while their subtraction is deferred
+    S_PRAVG1 = S_COUNT, S_PRAVG2, S_SLOTS
 };
 
 __host__ __device__ inline size_t fidx(const Dev &d, int j, int k) {

@@ -343,7 +343,12 @@ __device__ __forceinline__ void nl_ru(const Dev &d, int tile, int ntj, double ro
 }
 
 // tiles blockIdx.x, blockIdx.x + gridDim.x, ...; buf: two NlTile in shared memory
-__device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, double ro, NlTile *buf) {
+// pend: the previous substep's pressure mean (scal[S_PRAVG]) is still to be
+// subtracted from pr (the fused step defers pr_submean of RK3 substeps 1 and
+// 2): the staged tile gets pr - pravg, the value pr_submean would have stored.
+__device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, double ro, NlTile *buf,
+                                            bool pend = false) {
+    const double pravg = pend ? d.scal[S_PRAVG] : 0.0;
     const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
     int tile = blockIdx.x;
@@ -368,6 +373,14 @@ __device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, 
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
+        if (pend) {
+            NlTile &tw = buf[it & 1];
+            for (int e = tid; e < (kNlK + 2) * (kNlJ + 2); e += 256) {
+                double &x = tw.pr[e / (kNlJ + 2)][e % (kNlJ + 2)];
+                x = x - pravg;
+            }
+            __syncthreads();
+        }
         const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
         const int jc = j0 + threadIdx.x;
         if (jc <= d.n2m) {
@@ -382,10 +395,10 @@ __device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, 
     }
 }
 
-__global__ void __launch_bounds__(256, kNlBlocksPerSM) k_nl_rhs(Dev d, double al, double ga, double ro) {
+__global__ void __launch_bounds__(256, kNlBlocksPerSM) k_nl_rhs(Dev d, double al, double ga, double ro, int pend) {
     extern __shared__ __align__(16) unsigned char nl_smem[];
     FB_GRID_WAIT();
-    nl_rhs_body(d, al, ga, ro, reinterpret_cast<NlTile *>(nl_smem));
+    nl_rhs_body(d, al, ga, ro, reinterpret_cast<NlTile *>(nl_smem), pend != 0);
 }
 
 // ------------------------------------------------------------ MLS forcing
@@ -949,9 +962,14 @@ __device__ __forceinline__ void up_own(const Dev &d, int tile, int ntj, double (
     }
 }
 
-__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be, UpTile *buf) {
+// pend: as for nl_rhs, pr - pravg of the previous substep is the pressure
+// this update starts from (read before this grid's last block stores the new
+// mean)
+__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be, UpTile *buf,
+                                                  bool pend = false) {
     __shared__ double sh[32];
     __shared__ bool last;
+    const double pravg = pend ? d.scal[S_PRAVG] : 0.0;
     const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
     const int t = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
     const int b = blockIdx.x, nb = gridDim.x;
@@ -1002,7 +1020,8 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
                     Fv(d.q3, jc, kc) = q3v[i] - (TD(jc, kc) - TD(jc, kc - 1)) * usukm;
                 }
                 const int kp = kpv_(d, kc), km = kmv_(kc);
-                const double p = prv[i] + TD(jc, kc) -
+                const double pr0 = pend ? prv[i] - pravg : prv[i];
+                const double p = pr0 + TD(jc, kc) -
                                  be * ((TD(jp, kc) * apj + TD(jc, kc) * acj + TD(jm, kc) * amj) +
                                        (TD(jc, kp) * u.kc[1][r] + TD(jc, kc) * u.kc[2][r] + TD(jc, km) * u.kc[3][r]));
                 Fv(d.pr, jc, kc) = p;
@@ -1031,18 +1050,25 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
     }
 }
 
-__global__ void __launch_bounds__(256, kUpBlocksPerSM) k_updvp_prcalc(Dev d, double al, double be) {
+__global__ void __launch_bounds__(256, kUpBlocksPerSM) k_updvp_prcalc(Dev d, double al, double be, int pend) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     FB_GRID_WAIT();
-    updvp_prcalc_body(d, al, be, reinterpret_cast<UpTile *>(up_smem));
+    updvp_prcalc_body(d, al, be, reinterpret_cast<UpTile *>(up_smem), pend != 0);
 }
 
 // pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
-__device__ __forceinline__ void submean_boucqt_body(const Dev &d) {
+// deferred: the means of RK3 substeps 1 and 2 were applied to the cells that
+// updvp rewrites (j <= n2m, 1 <= k <= n3m) as it read them; the other
+// entries of the array get all three subtractions here, in order.
+__device__ __forceinline__ void submean_boucqt_body(const Dev &d, bool deferred = false) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
     const double pravg = d.scal[S_PRAVG];
-    if (j <= d.n2 && k <= d.n3) Fv(d.pr, j, k) = Fv(d.pr, j, k) - pravg;
+    if (j <= d.n2 && k <= d.n3) {
+        double p = Fv(d.pr, j, k);
+        if (deferred && (j > d.n2m || k < 1 || k > d.n3m)) p = (p - d.scal[S_PRAVG1]) - d.scal[S_PRAVG2];
+        Fv(d.pr, j, k) = p - pravg;
+    }
     if (blockIdx.y == 0 && threadIdx.y == 0 && j <= d.n2m) {
         d.qb2s[j] = d.qb2s[j] + d.dqb2s[j];
         d.qb3s[j] = d.qb3s[j] + d.dqb3s[j];
@@ -1051,9 +1077,30 @@ __device__ __forceinline__ void submean_boucqt_body(const Dev &d) {
     }
 }
 
-__global__ void k_submean_boucqt(Dev d) {
+__global__ void k_submean_boucqt(Dev d, int deferred) {
     FB_GRID_WAIT();
-    submean_boucqt_body(d);
+    submean_boucqt_body(d, deferred != 0);
+}
+
+// The end of RK3 substep 1 or 2 in the fused step: boucqt (iobcs.F90:97-105),
+// the substep's pressure mean kept in slot for the final pr_submean, then
+// boucdq of the next substep (iobcs.F90:5-77) in the same block.  The mean
+// itself is subtracted by the next nl_rhs and updvp as they read pr.
+__device__ __forceinline__ void substep_mid_body(const Dev &d, int slot, double ga, double ro) {
+    for (int j = threadIdx.x + 1; j <= d.n2m; j += blockDim.x) {
+        d.qb2s[j] = d.qb2s[j] + d.dqb2s[j];
+        d.qb3s[j] = d.qb3s[j] + d.dqb3s[j];
+        d.qb2n[j] = d.qb2n[j] + d.dqb2n[j];
+        d.qb3n[j] = d.qb3n[j] + d.dqb3n[j];
+    }
+    if (threadIdx.x == 0) d.scal[slot] = d.scal[S_PRAVG];
+    __syncthreads();
+    boucdq_body(d, ga, ro);
+}
+
+__global__ void __launch_bounds__(1024) k_substep_mid(Dev d, int slot, double ga, double ro) {
+    FB_GRID_WAIT();
+    substep_mid_body(d, slot, ga, ro);
 }
 
 // ------------------------------------------------------------ loads
@@ -1581,12 +1628,12 @@ __global__ void __launch_bounds__(1024) kg_boucdq(const GroupCase *__restrict__ 
     boucdq_body(d, s.ga, s.ro);
 }
 
-__global__ void __launch_bounds__(256, kNlBlocksPerSM) kg_nl_rhs(const GroupCase *__restrict__ g, int n) {
+__global__ void __launch_bounds__(256, kNlBlocksPerSM) kg_nl_rhs(const GroupCase *__restrict__ g, int n, int pend) {
     extern __shared__ __align__(16) unsigned char nl_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
     stage_case(g, &d, &s, n);
-    nl_rhs_body(d, s.al, s.ga, s.ro, reinterpret_cast<NlTile *>(nl_smem));
+    nl_rhs_body(d, s.al, s.ga, s.ro, reinterpret_cast<NlTile *>(nl_smem), pend != 0);
 }
 __global__ void kg_lgrdist(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
@@ -1625,18 +1672,27 @@ __global__ void kg_divg(const GroupCase *__restrict__ g, int n) {
     divg_body(d, s.usdtal);
 }
 
-__global__ void __launch_bounds__(256, kUpBlocksPerSM) kg_updvp_prcalc(const GroupCase *__restrict__ g, int n) {
+__global__ void __launch_bounds__(256, kUpBlocksPerSM) kg_updvp_prcalc(const GroupCase *__restrict__ g, int n,
+                                                                       int pend) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
     stage_case(g, &d, &s, n);
-    updvp_prcalc_body(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem));
+    updvp_prcalc_body(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem), pend != 0);
 }
 
-__global__ void kg_submean_boucqt(const GroupCase *__restrict__ g) {
+__global__ void kg_submean_boucqt(const GroupCase *__restrict__ g, int deferred) {
     __shared__ Dev d;
     stage_case(g, &d);
-    submean_boucqt_body(d);
+    submean_boucqt_body(d, deferred != 0);
+}
+
+// n: the next substep (0-based) whose boucdq runs here
+__global__ void __launch_bounds__(1024) kg_substep_mid(const GroupCase *__restrict__ g, int n, int slot) {
+    __shared__ Dev d;
+    __shared__ SubDev s;
+    stage_case(g, &d, &s, n);
+    substep_mid_body(d, slot, s.ga, s.ro);
 }
 
 __global__ void kg_loads_probe(const GroupCase *__restrict__ g) {
@@ -1685,9 +1741,9 @@ void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(std::min(d.n3m, 
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
 int nl_tiles(const Dev &d) { return ((d.n2m + kNlJ - 1) / kNlJ) * ((d.n3m + kNlK - 1) / kNlK); }
 
-void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s) {
+void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s, bool pend) {
     const int blocks = std::min(nl_tiles(d), 148 * kNlBlocksPerSM);
-    pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro);
+    pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro, pend ? 1 : 0);
 }
 void launch_lgrdist(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_lgrdist, dim3((d.nlm + 127) / 128), dim3(128), 0, s, d);
@@ -1716,13 +1772,16 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     dim3 b(32, 8);
     pdl(k_divg, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, usdtal);
 }
-void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s) {
+void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend) {
     const int blocks = std::min(nl_tiles(d), 148 * kUpBlocksPerSM);
-    pdl(k_updvp_prcalc, dim3(blocks), dim3(32, 8), kUpSmem, s, d, al, be);
+    pdl(k_updvp_prcalc, dim3(blocks), dim3(32, 8), kUpSmem, s, d, al, be, pend ? 1 : 0);
 }
-void launch_submean_boucqt(const Dev &d, cudaStream_t s) {
+void launch_submean_boucqt(const Dev &d, cudaStream_t s, bool deferred) {
     dim3 b(32, 8);
-    pdl(k_submean_boucqt, dim3(grid2(d.n2, d.n3 + 1, b)), dim3(b), 0, s, d);
+    pdl(k_submean_boucqt, dim3(grid2(d.n2, d.n3 + 1, b)), dim3(b), 0, s, d, deferred ? 1 : 0);
+}
+void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream_t s) {
+    pdl(k_substep_mid, dim3(1), dim3(1024), 0, s, d, slot, ga, ro);
 }
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
@@ -1749,10 +1808,10 @@ void glaunch_cfl(const Group &g, cudaStream_t s) {
 void glaunch_boucdq(const Group &g, int n, cudaStream_t s) {
     pdl(kg_boucdq, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases, n);
 }
-void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s) {
+void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s, bool pend) {
     // about two waves of resident blocks over the whole group
     const int per_case = std::max(1, std::min(nl_tiles(g.rep), (2 * 148 * kNlBlocksPerSM + g.n - 1) / g.n));
-    pdl(kg_nl_rhs, zgrid(dim3(per_case), g), dim3(32, 8), kNlSmem, s, g.cases, n);
+    pdl(kg_nl_rhs, zgrid(dim3(per_case), g), dim3(32, 8), kNlSmem, s, g.cases, n, pend ? 1 : 0);
 }
 
 cudaError_t kernels_configure() {
@@ -1785,13 +1844,16 @@ void glaunch_divg(const Group &g, int n, cudaStream_t s) {
     dim3 b(32, 8);
     pdl(kg_divg, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
 }
-void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s) {
+void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s, bool pend) {
     const int per_case = std::max(1, std::min(nl_tiles(g.rep), (2 * 148 * kUpBlocksPerSM + g.n - 1) / g.n));
-    pdl(kg_updvp_prcalc, zgrid(dim3(per_case), g), dim3(32, 8), kUpSmem, s, g.cases, n);
+    pdl(kg_updvp_prcalc, zgrid(dim3(per_case), g), dim3(32, 8), kUpSmem, s, g.cases, n, pend ? 1 : 0);
 }
-void glaunch_submean_boucqt(const Group &g, cudaStream_t s) {
+void glaunch_submean_boucqt(const Group &g, cudaStream_t s, bool deferred) {
     dim3 b(32, 8);
-    pdl(kg_submean_boucqt, zgrid(grid2(g.rep.n2, g.rep.n3 + 1, b), g), dim3(b), 0, s, g.cases);
+    pdl(kg_submean_boucqt, zgrid(grid2(g.rep.n2, g.rep.n3 + 1, b), g), dim3(b), 0, s, g.cases, deferred ? 1 : 0);
+}
+void glaunch_substep_mid(const Group &g, int n_next, int slot, cudaStream_t s) {
+    pdl(kg_substep_mid, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases, n_next, slot);
 }
 void glaunch_loads(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
