@@ -30,7 +30,7 @@ STATUS = {0: "FB_OK", 1: "FB_ERR_CFL", 2: "FB_ERR_MLS", 3: "FB_ERR_MARKER_OUT",
           8: "FB_ERR_NUMERIC", 9: "FB_ERR_TIMEOUT"}
 FB_ERR_CFL, FB_ERR_MLS, FB_ERR_MARKER_OUT, FB_ERR_INPUT = 1, 2, 3, 4
 FB_ERR_CUDA, FB_ERR_STATE, FB_ERR_UNSUPPORTED, FB_ERR_NUMERIC, FB_ERR_TIMEOUT = 5, 6, 7, 8, 9
-POISSON_FP64, POISSON_TF32X3 = 0, 1
+POISSON_FP64, POISSON_TF32X3, POISSON_INT8X8 = 0, 1, 2
 COUPLING_LOOSE, COUPLING_STRONG, COUPLING_LEARNED = 0, 1, 2
 BATCH_GROUPED, BATCH_GRAPH = 0, 1
 
@@ -129,6 +129,7 @@ def lib() -> ctypes.CDLL:
         "fb_last_history": ([vp, dp], ctypes.c_int),
         "fb_write_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
         "fb_read_restart": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "fb_gemm_i8x8": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp], ctypes.c_int),
         "fb_gemm_tf32x3": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp],
                            ctypes.c_int),
         "fb_autotune": ([vp, ip], ctypes.c_int),
@@ -285,6 +286,17 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def gemm_i8x8(A: np.ndarray, B: np.ndarray, device: int = 0) -> np.ndarray:
+    """C = A @ B.T to FP64 accuracy on the INT8 tensor cores (8 digit slices)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    M, K = A.shape
+    N = B.shape[0]
+    C = np.zeros((M, N), dtype=np.float64, order="F")
+    _check(lib().fb_gemm_i8x8(int(device), M, N, K, _dp(A), _dp(B), _dp(C)), "fb_gemm_i8x8")
+    return C
 
 
 def gemm_tf32x3(A: np.ndarray, B: np.ndarray, device: int = 0, bn: int = 128) -> np.ndarray:

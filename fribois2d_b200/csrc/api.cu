@@ -97,6 +97,10 @@ struct fb_ctx {
     double *zs_d = nullptr, *zsinv_d = nullptr;  // S and S^-1 of zmm = S U (the transforms use U)
     fb::Tf32x3Plan plan_fwd{}, plan_bwd{};
     double *pw = nullptr;
+    // FP64 transforms on the INT8 tensor cores: digit planes of the data
+    // operand (dph, then hmn) and of the two eigenvector matrices
+    fb::I8Plan i8a{}, i8f{}, i8b{};
+    bool i8_ready = false;
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
     int step_kernels = 0;     // own kernels per captured step
     // host copies of the scalar state the reference keeps in modules
@@ -793,6 +797,47 @@ int setup_tf32(fb_ctx *c) {
     return FB_OK;
 }
 
+// allocates the INT8 digit planes and cuts the eigenvector matrices once
+int setup_i8(fb_ctx *c) {
+    if (c->i8_ready) return FB_OK;
+    const Dev &d = c->d;
+    int st;
+    if ((st = fb::i8_configure())) return st;
+    const long ldk = (d.n3m + fb::kI8BK - 1) / fb::kI8BK * fb::kI8BK;
+    auto make = [&](fb::I8Plan &p, int rows, int box) -> int {
+        p.ldk = ldk;
+        p.rows_pad = (rows + 127) / 128 * 128;
+        int r;
+        if ((r = dnew(c, &p.dig, static_cast<size_t>(fb::kI8S) * p.rows_pad * ldk))) return r;
+        if ((r = dnew(c, &p.scale, static_cast<size_t>(p.rows_pad)))) return r;
+        if ((r = dnew(c, &p.cmax, static_cast<size_t>(p.rows_pad) * ((d.n3m + 255) / 256)))) return r;
+        return fb::i8_plan(p, rows, d.n3m, box);
+    };
+    if ((st = make(c->i8a, d.n2m, 128)) || (st = make(c->i8f, d.n3m, fb::kI8BN)) || (st = make(c->i8b, d.n3m, fb::kI8BN)))
+        return st;
+    // forward B(m, k) = zmmt(m, k); backward B(k, m) = zmm(k, m): both column-major
+    fb::launch_i8_split(c->zmmt, d.n3m, d.n3m, d.n3m, c->i8f, c->stream);
+    fb::launch_i8_split(c->zmm, d.n3m, d.n3m, d.n3m, c->i8b, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    c->i8_ready = true;
+    return FB_OK;
+}
+
+// phcalc with the transforms on the INT8 tensor cores (phcalc_outflow.F90:31,
+// 61-69): hmn = dph zmmt^T, per-mode y solves, dph = hmn zmm^T
+int phcalc_i8(fb_ctx *c) {
+    const Dev &d = c->d;
+    cudaStream_t st = c->stream;
+    fb::launch_i8_split(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, st);
+    fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
+    fb::launch_scan_poisson(d, st);
+    fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
+    fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st);
+    c->own_launches += 4;
+    return FB_OK;
+}
+
 int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     double al, ga, ro;
     coefs(c, ns, n, al, ga, ro);
@@ -834,6 +879,10 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_ST_PHCALC:
         if (c->poisson_mode == FB_POISSON_TF32X3) {
             if ((r = phcalc_tf32(c))) return r;
+            break;
+        }
+        if (c->poisson_mode == FB_POISSON_INT8X8) {
+            if ((r = phcalc_i8(c))) return r;
             break;
         }
         if ((r = gemm_fwd(c))) return r;
@@ -1861,10 +1910,14 @@ int fb_host_array(fb_host *h, int id, double *out, int64_t n) {
 }
 
 int fb_set_poisson(fb_ctx *c, int mode) {
-    if (!c || (mode != FB_POISSON_FP64 && mode != FB_POISSON_TF32X3)) return FB_ERR_STATE;
+    if (!c || (mode != FB_POISSON_FP64 && mode != FB_POISSON_TF32X3 && mode != FB_POISSON_INT8X8)) return FB_ERR_STATE;
     CK(cudaSetDevice(c->device));
     if (mode == FB_POISSON_TF32X3) {
         const int st = setup_tf32(c);
+        if (st) return st;
+    }
+    if (mode == FB_POISSON_INT8X8) {
+        const int st = setup_i8(c);
         if (st) return st;
     }
     if (mode != c->poisson_mode) {   // the captured step no longer matches
@@ -1946,6 +1999,7 @@ void group_free(BatchGroup *bg) {
 bool groupable(const fb_ctx *c) {
     if (c->hc.deck.nsst != 3) return false;
     if (c->poisson_mode == FB_POISSON_TF32X3 && !c->pw) return false;
+    if (c->poisson_mode == FB_POISSON_INT8X8) return false;   // own branch
     for (int n = 0; n < 3; ++n)
         if (c->sub[n].win_y <= 0 || c->sub[n].win_tk != c->sub[0].win_tk) return false;
     return true;
@@ -2581,6 +2635,56 @@ int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, con
     }
     if (!st) {
         fb::launch_tf32x3(plan, dC, M, nullptr, 0, status, nullptr);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = FB_ERR_CUDA;
+    }
+    int dev_status = 0;
+    if (!st && cudaMemcpy(&dev_status, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) st = FB_ERR_CUDA;
+    if (!st && dev_status) st = dev_status;
+    if (!st && cudaMemcpy(C, dC, sizeof(double) * M * N, cudaMemcpyDeviceToHost) != cudaSuccess) st = FB_ERR_CUDA;
+    for (void *p : mem) cudaFree(p);
+    return st;
+}
+
+int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double *B, double *C) {
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return FB_ERR_STATE;
+    CK(cudaSetDevice(device));
+    int st = fb::i8_configure();
+    if (st) return st;
+    const long ldk = (K + fb::kI8BK - 1) / fb::kI8BK * fb::kI8BK;
+    std::vector<void *> mem;
+    auto alloc = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        mem.push_back(p);
+        return p;
+    };
+    fb::I8Plan pa{}, pb{};
+    pa.ldk = pb.ldk = ldk;
+    pa.rows_pad = (M + 127) / 128 * 128;
+    pb.rows_pad = (N + 127) / 128 * 128;
+    double *dA = static_cast<double *>(alloc(sizeof(double) * M * K));
+    double *dB = static_cast<double *>(alloc(sizeof(double) * N * K));
+    double *dC = static_cast<double *>(alloc(sizeof(double) * M * N));
+    pa.dig = static_cast<int8_t *>(alloc(static_cast<size_t>(fb::kI8S) * pa.rows_pad * ldk));
+    pb.dig = static_cast<int8_t *>(alloc(static_cast<size_t>(fb::kI8S) * pb.rows_pad * ldk));
+    pa.scale = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad));
+    pb.scale = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad));
+    pa.cmax = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad * ((K + 255) / 256)));
+    pb.cmax = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad * ((K + 255) / 256)));
+    int *status = static_cast<int *>(alloc(sizeof(int)));
+    st = FB_OK;
+    if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !pa.cmax || !pb.cmax || !status)
+        st = FB_ERR_CUDA;
+    if (!st && (cudaMemcpy(dA, A, sizeof(double) * M * K, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(dB, B, sizeof(double) * N * K, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemset(status, 0, sizeof(int)) != cudaSuccess))
+        st = FB_ERR_CUDA;
+    if (!st) st = fb::i8_plan(pa, M, K, 128);
+    if (!st) st = fb::i8_plan(pb, N, K, fb::kI8BN);
+    if (!st) {
+        fb::launch_i8_split(dA, M, M, K, pa, nullptr);
+        fb::launch_i8_split(dB, N, N, K, pb, nullptr);
+        fb::launch_i8x8(pa, pb, dC, M, status, nullptr);
         if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = FB_ERR_CUDA;
     }
     int dev_status = 0;

@@ -149,6 +149,23 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
 __device__ __forceinline__ float tf32_round(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -620,6 +637,260 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
     poisson_residual_body(d, t.phi, t.hi, t.lo, t.ldd, t.kscale);
 }
 
+// ---- FP64 products on the INT8 tensor cores -------------------------------
+// C = A B^T to FP64 accuracy from exact integer products (the Ozaki scheme
+// with power-of-two row scaling, Ozaki, Ogita, Oishi and Rump): every row r
+// of A is scaled by 2^-e(r) (|A(r,k)| < 2^e(r)) and cut into kI8S signed
+// 8-bit digits, a = sum_i d_i 128^-(i+1), likewise the rows of B with f(c).
+// Then
+//   C(r,c) = 2^(e(r)+f(c)) sum_t 128^-(t+2) G_t(r,c),  G_t = sum_{i+j=t} D_i E_j^T,
+// keeping the digit pairs with i + j < kI8S (the dropped ones are below
+// 2^-63 K of the row and column maxima).  Each G_t is an exact int32 sum of
+// tcgen05.mma kind::i8 products accumulated in its own TMEM columns; the
+// epilogue adds the G_t in FP64 from the smallest weight up and applies the
+// power-of-two scales (exact).  The error is that of those FP64 additions
+// and of the dropped digits: ~2e-16 of sum |a||b| for K = 1024, as FP64
+// DGEMM.
+
+// Digit split in two launches so that the whole GPU takes part: the
+// maxima of |A(r, k)| over chunks of kI8Chunk columns (one block per 32 rows
+// and chunk), then the digits of 32 x 32 tiles (one block each), every block
+// of a row deriving the same exponent from the chunk maxima.
+constexpr int kI8Chunk = 256;
+
+__global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
+                                                    double *__restrict__ cmax, int rows_pad) {
+    FB_GRID_WAIT();
+    __shared__ double mx[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r = blockIdx.x * 32 + lane, k0 = blockIdx.y * kI8Chunk;
+    double m = 0.0;
+    if (r < R) {
+#pragma unroll 8
+        for (int q = 0; q < kI8Chunk / 8; ++q) {
+            const int k = k0 + w + 8 * q;
+            if (k < K) m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
+        }
+    }
+    mx[w][lane] = m;
+    __syncthreads();
+    if (w == 0) {
+        for (int q = 1; q < 8; ++q) m = fmax(m, mx[q][lane]);
+        cmax[static_cast<size_t>(blockIdx.y) * rows_pad + blockIdx.x * 32 + lane] = m;
+    }
+}
+
+// dig[i * plane + r * ldk + k] = digit i of row r (k < K; 0 for k >= K or
+// r >= R, up to the padded rows and ldk), rowscale[r] = 2^e(r); the source is
+// column-major, A(r, k) at src[k * lds + r].  Block (x, y): rows 32x.., columns 32y..
+__global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ src, long lds, int R, int K,
+                                                    const double *__restrict__ cmax, int nchunk, int8_t *dig,
+                                                    long ldk, long plane, double *rowscale, int rows_pad) {
+    FB_GRID_WAIT();
+    __shared__ double sc[32];
+    __shared__ __align__(16) int8_t tile[kI8S][32][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r0 = blockIdx.x * 32, r = r0 + lane, k0 = blockIdx.y * 32;
+    if (w == 0) {
+        double m = 0.0;
+        for (int q = 0; q < nchunk; ++q) m = fmax(m, cmax[static_cast<size_t>(q) * rows_pad + r0 + lane]);
+        int e = 0;
+        if (m > 0.0) frexp(m, &e);   // m < 2^e
+        sc[lane] = ldexp(1.0, -e);
+        if (blockIdx.y == 0 && r < R) rowscale[r] = ldexp(1.0, e);
+    }
+    __syncthreads();
+    const double s = sc[lane];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int kk = w + 8 * q, k = k0 + kk;
+        double a = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
+#pragma unroll
+        for (int i = 0; i < kI8S; ++i) {
+            a = a * 128.0;
+            const double d = trunc(a);
+            a = a - d;
+            tile[i][lane][kk] = static_cast<int8_t>(d);
+        }
+    }
+    __syncthreads();
+    {   // slice i = w, row lane: 32 bytes
+        const uint4 *t = reinterpret_cast<const uint4 *>(&tile[w][lane][0]);
+        uint4 *o = reinterpret_cast<uint4 *>(dig + static_cast<size_t>(w) * plane + static_cast<size_t>(r0 + lane) * ldk + k0);
+        o[0] = t[0];
+        o[1] = t[1];
+    }
+}
+
+struct I8Cfg {
+    static constexpr uint32_t kATile = 128 * kI8BK;                 // one A digit slice: 128 rows x 128 B
+    static constexpr uint32_t kBSlice = kI8BN * kI8BK;              // one B digit slice
+    static constexpr uint32_t kBStage = kI8S * kI8BN * kI8BK;       // all B slices of a k-block
+    static constexpr int kASlots = 5;
+    static constexpr size_t kSmem = 2 * kBStage + kASlots * kATile + 1024 + 256;
+    static constexpr uint32_t kTmemCols = kI8S * kI8BN;             // one s32 accumulator per digit-weight class
+    // D s32 (2), A and B signed 8-bit (1), both K-major, N = kI8BN, M = 128
+    static constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                                       (static_cast<uint32_t>(kI8BN >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+    static_assert(kTmemCols == 512, "TMEM columns");
+    static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
+};
+
+// One CTA per 128 x kI8BN tile of C.  Per k-block of 128: the producer
+// thread loads all B slices (one barrier) and streams the A slices through
+// a ring; the MMA thread multiplies A slice i with B slices j < kI8S - i into
+// accumulator i + j (4 MMAs of K = 32 each).  Every wait gives up after one
+// second with FB_ERR_TIMEOUT.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
+                int *status) {
+    FB_GRID_WAIT();
+    using Cfg = I8Cfg;
+    constexpr int kS = kI8S, kAS = Cfg::kASlots;
+    extern __shared__ uint8_t smraw[];
+    const uint32_t raw = smem_u32(smraw);
+    const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+    uint8_t *sm = smraw + pad;
+    const uint32_t sbase = raw + pad;
+    const uint32_t sB = sbase, sA = sbase + 2 * Cfg::kBStage;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + 2 * Cfg::kBStage + kAS * Cfg::kATile);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * 2 + 2 * kAS + 1);
+    const uint32_t bfull0 = smem_u32(bars), bempty0 = smem_u32(bars + 2);
+    const uint32_t afull0 = smem_u32(bars + 4), aempty0 = smem_u32(bars + 4 + kAS), done = smem_u32(bars + 4 + 2 * kAS);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * kI8BN;
+    const int nk = (K + kI8BK - 1) / kI8BK;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(bfull0 + 8 * q, 1);
+            mbar_init(bempty0 + 8 * q, 1);
+        }
+        for (int q = 0; q < kAS; ++q) {
+            mbar_init(afull0 + 8 * q, 1);
+            mbar_init(aempty0 + 8 * q, 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(Cfg::kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer
+        int ia = 0, nb = 0;
+        for (int kb = 0; kb < nk && ok; ++kb) {
+            const int sb = kb & 1;
+            if (!mbar_wait(bempty0 + 8 * sb, (static_cast<uint32_t>(kb >> 1) & 1u) ^ 1u)) {
+                ok = false;
+                break;
+            }
+            mbar_expect_tx(bfull0 + 8 * sb, Cfg::kBStage);
+            for (int j = 0; j < kS; ++j)
+                tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, &mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
+            nb = kb + 1;
+            for (int i = 0; i < kS; ++i) {
+                const int slot = ia % kAS;
+                if (!mbar_wait(aempty0 + 8 * slot, (static_cast<uint32_t>(ia / kAS) & 1u) ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(afull0 + 8 * slot, Cfg::kATile);
+                tma_load_3d(sA + slot * Cfg::kATile, &ma, afull0 + 8 * slot, kb * kI8BK, m0, i);
+                ++ia;
+            }
+        }
+        // every copy issued has landed before the CTA may finish
+        for (int q = (ia > kAS ? ia - kAS : 0); q < ia; ++q)
+            if (!mbar_wait(afull0 + 8 * (q % kAS), static_cast<uint32_t>(q / kAS) & 1u)) ok = false;
+        for (int q = (nb > 2 ? nb - 2 : 0); q < nb; ++q)
+            if (!mbar_wait(bfull0 + 8 * (q & 1), static_cast<uint32_t>(q >> 1) & 1u)) ok = false;
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer
+        int ia = 0;
+        for (int kb = 0; kb < nk && ok; ++kb) {
+            const int sb = kb & 1;
+            if (!mbar_wait(bfull0 + 8 * sb, static_cast<uint32_t>(kb >> 1) & 1u)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t bst = sB + sb * Cfg::kBStage;
+            for (int i = 0; i < kS; ++i) {
+                const int slot = ia % kAS;
+                if (!mbar_wait(afull0 + 8 * slot, static_cast<uint32_t>(ia / kAS) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ast = sA + slot * Cfg::kATile;
+                for (int j = 0; j < kS - i; ++j) {
+                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j) * kI8BN);
+#pragma unroll
+                    for (int kk = 0; kk < kI8BK / 32; ++kk) {   // K = 32 bytes per MMA
+                        const uint64_t a = sw128_desc(ast + 32 * kk);
+                        const uint64_t b = sw128_desc(bst + j * Cfg::kBSlice + 32 * kk);
+                        mma_i8(acc_t, a, b, Cfg::kIdesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(aempty0 + 8 * slot);   // frees the A slot once these MMAs have read it
+                ++ia;
+            }
+            if (!ok) break;
+            mma_commit(bempty0 + 8 * sb);
+        }
+        mma_commit(done);
+    }
+    __syncwarp();
+
+    // ---- epilogue: TMEM lane = tile row; accumulators summed in FP64 from the smallest weight up
+    if (!mbar_wait(done, 0)) ok = false;
+    __syncwarp();
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    const bool rok = ok && row < o.M;
+    const double rs = rok ? o.rowscale[row] : 0.0;
+#pragma unroll 1
+    for (int c = 0; c < kI8BN / 32; ++c) {
+        double acc[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+#pragma unroll 1
+        for (int t = kS - 1; t >= 0; --t) {
+            uint32_t v[32];
+            tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * kI8BN + c * 32), v);
+            const double wgt = ldexp(1.0, -7 * (t + 2));
+#pragma unroll
+            for (int q = 0; q < 32; ++q) acc[q] = acc[q] + static_cast<double>(static_cast<int32_t>(v[q])) * wgt;
+        }
+        if (rok) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const int col = n0 + c * 32 + q;
+                if (col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
+            }
+        }
+    }
+    if (!ok) atomicCAS(status, 0, FB_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols)
+                     : "memory");
+    }
+}
+
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
                              const double *kscale) {
     const dim3 grid((d.n2m + 31) / 32, (d.n3m + 31) / 32);
@@ -749,6 +1020,54 @@ void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane 
                     const double *cscale) {
     const dim3 grid((R + 31) / 32, (C + 31) / 32);
     pdl(k_split_t, dim3(grid), dim3(256), 0, st, src, lds, R, C, dst.hi, dst.lo, dst.ld, cscale);
+}
+
+
+// ---- INT8 FP64 products: buffers, maps, launches
+int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
+    if (!p.dig || (p.ldk % 128) || p.rows_pad < rows) return FB_ERR_STATE;
+    if (!g_encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return FB_ERR_CUDA;
+        g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if (reinterpret_cast<uintptr_t>(p.dig) & 15u) return FB_ERR_STATE;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(p.ldk), static_cast<cuuint64_t>(p.rows_pad),
+                                static_cast<cuuint64_t>(kI8S)};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(p.ldk),
+                                   static_cast<cuuint64_t>(p.ldk) * static_cast<cuuint64_t>(p.rows_pad)};
+    const cuuint32_t box[3] = {static_cast<cuuint32_t>(kI8BK), static_cast<cuuint32_t>(box_rows), 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = g_encode(&p.map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, p.dig, dims, strides, box, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    p.rows = rows;
+    p.K = K;
+    return r == CUDA_SUCCESS ? FB_OK : FB_ERR_CUDA;
+}
+
+int i8_configure() {
+    return cudaFuncSetAttribute(k_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(I8Cfg::kSmem)) == cudaSuccess
+               ? FB_OK
+               : FB_ERR_CUDA;
+}
+
+void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {
+    const int nchunk = (K + kI8Chunk - 1) / kI8Chunk;
+    pdl(k_i8_rowmax, dim3(p.rows_pad / 32, nchunk), dim3(256), 0, st, src, lds, R, K, p.cmax, p.rows_pad);
+    pdl(k_i8_digits, dim3(p.rows_pad / 32, static_cast<unsigned>(p.ldk / 32)), dim3(256), 0, st, src, lds, R, K,
+        static_cast<const double *>(p.cmax), nchunk, p.dig, p.ldk, p.ldk * static_cast<long>(p.rows_pad), p.scale,
+        p.rows_pad);
+}
+
+void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st) {
+    I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows};
+    const dim3 grid((a.rows + 127) / 128, (b.rows + kI8BN - 1) / kI8BN);
+    pdl(k_i8x8_gemm, grid, dim3(kThreads), I8Cfg::kSmem, st, a.map, b.map, o, a.K, status);
 }
 
 }  // namespace fb

@@ -52,6 +52,34 @@ struct ResidualTask {    // one Poisson residual: phi -> hi, lo (ldd), row facto
     const double *kscale;
 };
 
+// FP64 products C = A B^T on the INT8 tensor cores (kI8S digit slices per
+// operand; tc_gemm.cu).  An operand: digit planes [slice][row][k] of
+// rows_pad x ldk bytes (ldk a multiple of 128), 2^e per row, its tensor map.
+constexpr int kI8S = 8;       // digit slices per operand
+constexpr int kI8BK = 128;    // K bytes per k-block (one 128-byte swizzle row)
+constexpr int kI8BN = 64;     // output tile width
+struct I8Plan {
+    CUtensorMap map;
+    int8_t *dig;
+    double *scale;            // 2^e(row)
+    double *cmax;             // split scratch: row maxima per 256-column chunk, [chunk][rows_pad]
+    long ldk;
+    int rows_pad, rows, K;
+};
+struct I8Out {
+    double *out;
+    long ldo;
+    const double *rowscale, *colscale;
+    int M, N;
+};
+int i8_configure();
+// box_rows: 128 for the A operand, kI8BN for B
+int i8_plan(I8Plan &p, int rows, int K, int box_rows);
+// digits of the column-major source A(r, k) = src[k * lds + r], r < R, k < K
+void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
+// out[c * ldo + r] = sum_k A(r, k) B(c, k)
+void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st);
+
 int tf32x3_configure();
 bool tf32x3_shape_ok(int bn);
 int tf32x3_plan(Tf32x3Plan &p, const SplitPlane &a, const SplitPlane &b, int M, int N, int K, int bn);

@@ -281,7 +281,16 @@ int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
  * sweep on the Poisson residual.  No counterpart in the reference. */
 #define FB_POISSON_FP64 0
 #define FB_POISSON_TF32X3 1
+/* FB_POISSON_INT8X8: the two FP64 eigen transforms computed exactly in
+ * integer arithmetic on the INT8 tensor cores (rows scaled by powers of two
+ * and cut into 8 signed 8-bit digits; the digit products summed in FP64):
+ * FP64-level accuracy (~2e-16 of sum |a||b| at K = 1024, as DGEMM), no
+ * refinement sweep.  No counterpart in the reference. */
+#define FB_POISSON_INT8X8 2
 int fb_set_poisson(fb_ctx *ctx, int mode);
+/* C = A * B^T with the INT8 digit-slice kernel (conventions and buffers as
+ * fb_gemm_tf32x3; a test entry point). */
+int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double *B, double *C);
 /* C = A * B^T with the 3xTF32 tensor-core kernel: A (M x K) and B (N x K)
  * column-major host arrays, C (M x N) column-major; allocates its own device
  * buffers on `device` (a test and calibration entry point).  bn: 64 or 128
