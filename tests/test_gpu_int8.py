@@ -75,3 +75,15 @@ def test_int8_step_matches_fp64(maker, steps, tmp_path):
     for col in (1, 2, 3, 9, 10, 11):   # forces and displacements
         rng_ = max(np.ptp(ha[:, col]), np.max(np.abs(ha[:, col])), 1e-30)
         assert np.max(np.abs(hb[:, col] - ha[:, col])) <= 1e-10 * rng_, col
+
+
+def test_i8x8_gemm_equals_restatement():
+    """The device computes exactly the NumPy restatement's operations: the
+    digits, the exact integer class sums and the FP64 additions in the same
+    order give the same bits."""
+    from oracle import i8x8
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((100, 300)) * np.exp(rng.uniform(-5, 5, (100, 1)))
+    B = rng.standard_normal((70, 300)) * np.exp(rng.uniform(-5, 5, (70, 1)))
+    B[9] = 0.0
+    np.testing.assert_array_equal(fb.gemm_i8x8(A, B), i8x8.gemm(A, B))
