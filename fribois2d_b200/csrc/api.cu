@@ -810,7 +810,7 @@ int setup_i8(fb_ctx *c) {
         int r;
         if ((r = dnew(c, &p.dig, static_cast<size_t>(fb::kI8S) * p.rows_pad * ldk))) return r;
         if ((r = dnew(c, &p.scale, static_cast<size_t>(p.rows_pad)))) return r;
-        if ((r = dnew(c, &p.cmax, static_cast<size_t>(p.rows_pad) * ((d.n3m + 255) / 256)))) return r;
+        if ((r = dnew(c, &p.cmax, static_cast<size_t>(p.rows_pad) * ((d.n3m + fb::kI8Chunk - 1) / fb::kI8Chunk)))) return r;
         return fb::i8_plan(p, rows, d.n3m, box);
     };
     if ((st = make(c->i8a, d.n2m, 128)) || (st = make(c->i8f, d.n3m, fb::kI8BN)) || (st = make(c->i8b, d.n3m, fb::kI8BN)))
@@ -2669,8 +2669,8 @@ int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double 
     pb.dig = static_cast<int8_t *>(alloc(static_cast<size_t>(fb::kI8S) * pb.rows_pad * ldk));
     pa.scale = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad));
     pb.scale = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad));
-    pa.cmax = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad * ((K + 255) / 256)));
-    pb.cmax = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad * ((K + 255) / 256)));
+    pa.cmax = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad * ((K + fb::kI8Chunk - 1) / fb::kI8Chunk)));
+    pb.cmax = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad * ((K + fb::kI8Chunk - 1) / fb::kI8Chunk)));
     int *status = static_cast<int *>(alloc(sizeof(int)));
     st = FB_OK;
     if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !pa.cmax || !pb.cmax || !status)

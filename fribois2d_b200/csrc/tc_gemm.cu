@@ -656,7 +656,6 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // maxima of |A(r, k)| over chunks of kI8Chunk columns (one block per 32 rows
 // and chunk), then the digits of 32 x 32 tiles (one block each), every block
 // of a row deriving the same exponent from the chunk maxima.
-constexpr int kI8Chunk = 256;
 
 __global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
                                                     double *__restrict__ cmax, int rows_pad) {
@@ -666,7 +665,7 @@ __global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ sr
     const int r = blockIdx.x * 32 + lane, k0 = blockIdx.y * kI8Chunk;
     double m = 0.0;
     if (r < R) {
-#pragma unroll 8
+#pragma unroll
         for (int q = 0; q < kI8Chunk / 8; ++q) {
             const int k = k0 + w + 8 * q;
             if (k < K) m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
@@ -688,7 +687,7 @@ __global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ sr
                                                     long ldk, long plane, double *rowscale, int rows_pad) {
     FB_GRID_WAIT();
     __shared__ double sc[32];
-    __shared__ __align__(16) int8_t tile[kI8S][32][32];
+    __shared__ uint32_t tile[kI8S][32][9];   // 4 digits per word, rows padded to 9 words
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int r0 = blockIdx.x * 32, r = r0 + lane, k0 = blockIdx.y * 32;
     if (w == 0) {
@@ -701,24 +700,31 @@ __global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ sr
     }
     __syncthreads();
     const double s = sc[lane];
+    // thread (lane, w): row r, columns k0 + 4w .. k0 + 4w + 3 (loads coalesced over the rows)
+    double a[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int kk = w + 8 * q, k = k0 + kk;
-        double a = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
+        const int k = k0 + 4 * w + q;
+        a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
+    }
 #pragma unroll
-        for (int i = 0; i < kI8S; ++i) {
-            a = a * 128.0;
-            const double d = trunc(a);
-            a = a - d;
-            tile[i][lane][kk] = static_cast<int8_t>(d);
+    for (int i = 0; i < kI8S; ++i) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            a[q] = a[q] * 128.0;
+            const double d = trunc(a[q]);
+            a[q] = a[q] - d;
+            word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
         }
+        tile[i][lane][w] = word;
     }
     __syncthreads();
     {   // slice i = w, row lane: 32 bytes
-        const uint4 *t = reinterpret_cast<const uint4 *>(&tile[w][lane][0]);
+        const uint32_t *t = &tile[w][lane][0];
         uint4 *o = reinterpret_cast<uint4 *>(dig + static_cast<size_t>(w) * plane + static_cast<size_t>(r0 + lane) * ldk + k0);
-        o[0] = t[0];
-        o[1] = t[1];
+        o[0] = make_uint4(t[0], t[1], t[2], t[3]);
+        o[1] = make_uint4(t[4], t[5], t[6], t[7]);
     }
 }
 
@@ -729,9 +735,8 @@ struct I8Cfg {
     static constexpr int kASlots = 5;
     static constexpr size_t kSmem = 2 * kBStage + kASlots * kATile + 1024 + 256;
     static constexpr uint32_t kTmemCols = kI8S * kI8BN;             // one s32 accumulator per digit-weight class
-    // D s32 (2), A and B signed 8-bit (1), both K-major, N = kI8BN, M = 128
-    static constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
-                                       (static_cast<uint32_t>(kI8BN >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+    // D s32 (2), A and B signed 8-bit (1), both K-major, M = 128; N set per MMA
+    static constexpr uint32_t kIdescBase = (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(128 >> 4) << 24);
     static_assert(kTmemCols == 512, "TMEM columns");
     static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
 };
@@ -739,7 +744,7 @@ struct I8Cfg {
 // One CTA per 128 x kI8BN tile of C.  Per k-block of 128: the producer
 // thread loads all B slices (one barrier) and streams the A slices through
 // a ring; the MMA thread multiplies A slice i with B slices j < kI8S - i into
-// accumulator i + j (4 MMAs of K = 32 each).  Every wait gives up after one
+// accumulators i + j (MMAs of K = 32 over up to four slices at once).  Every wait gives up after one
 // second with FB_ERR_TIMEOUT.
 __global__ void __launch_bounds__(kThreads, 1)
     k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
@@ -835,13 +840,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 tc_fence_after();
                 const uint32_t ast = sA + slot * Cfg::kATile;
-                for (int j = 0; j < kS - i; ++j) {
-                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j) * kI8BN);
+                // B slices j0 .. j0+nsl-1 are consecutive rows in shared memory and
+                // their classes i+j0 .. consecutive TMEM column blocks: one MMA of
+                // N = nsl * kI8BN covers up to four digit pairs
+                for (int j0 = 0; j0 < kS - i; j0 += 4) {
+                    const int nsl = min(4, kS - i - j0);
+                    const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * kI8BN) >> 3) << 17);
+                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * kI8BN);
 #pragma unroll
                     for (int kk = 0; kk < kI8BK / 32; ++kk) {   // K = 32 bytes per MMA
                         const uint64_t a = sw128_desc(ast + 32 * kk);
-                        const uint64_t b = sw128_desc(bst + j * Cfg::kBSlice + 32 * kk);
-                        mma_i8(acc_t, a, b, Cfg::kIdesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
+                        const uint64_t b = sw128_desc(bst + j0 * Cfg::kBSlice + 32 * kk);
+                        mma_i8(acc_t, a, b, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
                     }
                 }
                 mma_commit(aempty0 + 8 * slot);   // frees the A slot once these MMAs have read it

@@ -58,11 +58,12 @@ struct ResidualTask {    // one Poisson residual: phi -> hi, lo (ldd), row facto
 constexpr int kI8S = 8;       // digit slices per operand
 constexpr int kI8BK = 128;    // K bytes per k-block (one 128-byte swizzle row)
 constexpr int kI8BN = 64;     // output tile width
+constexpr int kI8Chunk = 64;  // columns per row-maximum block of the digit split
 struct I8Plan {
     CUtensorMap map;
     int8_t *dig;
     double *scale;            // 2^e(row)
-    double *cmax;             // split scratch: row maxima per 256-column chunk, [chunk][rows_pad]
+    double *cmax;             // split scratch: row maxima per kI8Chunk columns, [chunk][rows_pad]
     long ldk;
     int rows_pad, rows, K;
 };
