@@ -1958,6 +1958,11 @@ struct BatchGroup {
     fb::GemmTask *gt = nullptr;      // 3 x n: forward -> hmn; backward -> pw; backward -> dph (+ pw)
     fb::SplitTask *sp = nullptr;     // 2 x n: dph S^-1 -> a; hmn -> a2
     fb::ResidualTask *rt = nullptr;  // n: pw -> a (S^-1)
+    // FP64 transforms on the INT8 tensor cores: digit cuts and products of every case
+    bool i8 = false;
+    fb::I8Plan i8rep{};              // split geometry (the first case's data operand)
+    fb::I8SplitTask *i8s = nullptr;  // 2 x n: dph, then hmn, into the case's digit planes
+    fb::I8Task *i8t = nullptr;       // 2 x n: forward -> hmn, backward -> dph
 };
 
 struct fb_batch {
@@ -1988,6 +1993,8 @@ void group_free(BatchGroup *bg) {
     if (bg->gt) cudaFree(bg->gt);
     if (bg->sp) cudaFree(bg->sp);
     if (bg->rt) cudaFree(bg->rt);
+    if (bg->i8s) cudaFree(bg->i8s);
+    if (bg->i8t) cudaFree(bg->i8t);
     for (cudaEvent_t e : {bg->fork, bg->join, bg->done})
         if (e) cudaEventDestroy(e);
     if (bg->st) cudaStreamDestroy(bg->st);
@@ -1999,7 +2006,7 @@ void group_free(BatchGroup *bg) {
 bool groupable(const fb_ctx *c) {
     if (c->hc.deck.nsst != 3) return false;
     if (c->poisson_mode == FB_POISSON_TF32X3 && !c->pw) return false;
-    if (c->poisson_mode == FB_POISSON_INT8X8) return false;   // own branch
+    if (c->poisson_mode == FB_POISSON_INT8X8 && !c->i8_ready) return false;
     for (int n = 0; n < 3; ++n)
         if (c->sub[n].win_y <= 0 || c->sub[n].win_tk != c->sub[0].win_tk) return false;
     return true;
@@ -2124,6 +2131,32 @@ int group_helsolve_tile(BatchGroup *bg) {
     return r;
 }
 
+// the INT8 form's task arrays (phcalc_i8's launches, per case)
+int group_setup_i8(BatchGroup *bg) {
+    const int n = static_cast<int>(bg->members.size());
+    std::vector<fb::I8SplitTask> sp(static_cast<size_t>(2 * n));
+    std::vector<fb::I8Task> gt(static_cast<size_t>(2 * n));
+    for (int i = 0; i < n; ++i) {
+        const fb_ctx *c = bg->members[static_cast<size_t>(i)];
+        const Dev &d = c->d;
+        const size_t k = static_cast<size_t>(i), m = static_cast<size_t>(n);
+        const fb::I8Plan &a = c->i8a;
+        sp[k] = {d.dph + d.P, d.P, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad};
+        sp[m + k] = {d.hmn, d.ldh, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad};
+        gt[k] = {a.map, c->i8f.map, fb::I8Out{d.hmn, d.ldh, a.scale, c->i8f.scale, d.n2m, d.n3m}, d.n3m, d.status};
+        gt[m + k] = {a.map, c->i8b.map, fb::I8Out{d.dph + d.P, d.P, a.scale, c->i8b.scale, d.n2m, d.n3m}, d.n3m,
+                     d.status};
+    }
+    CK(cudaMalloc(&bg->i8s, sizeof(fb::I8SplitTask) * sp.size()));
+    CK(cudaMalloc(&bg->i8t, sizeof(fb::I8Task) * gt.size()));
+    CK(cudaMemcpyAsync(bg->i8s, sp.data(), sizeof(fb::I8SplitTask) * sp.size(), cudaMemcpyHostToDevice, bg->st));
+    CK(cudaMemcpyAsync(bg->i8t, gt.data(), sizeof(fb::I8Task) * gt.size(), cudaMemcpyHostToDevice, bg->st));
+    CK(cudaStreamSynchronize(bg->st));
+    bg->i8rep = bg->members[0]->i8a;
+    bg->i8 = true;
+    return FB_OK;
+}
+
 // the precision form's task arrays (phcalc_tf32's launches, per case)
 int group_setup_tf32(BatchGroup *bg) {
     const int n = static_cast<int>(bg->members.size());
@@ -2213,6 +2246,7 @@ int group_setup(BatchGroup *bg) {
     int r;
     if ((r = group_helsolve_tile(bg))) return r;
     if (c0->poisson_mode == FB_POISSON_TF32X3) return group_setup_tf32(bg);
+    if (c0->poisson_mode == FB_POISSON_INT8X8) return group_setup_i8(bg);
     return FB_OK;
 }
 
@@ -2255,6 +2289,13 @@ int enqueue_group(BatchGroup *bg) {
             fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
             fb::launch_tf32x3_group(bg->gt + 2 * n, bg->plan_bwd, n, st);
             k += 10;
+        } else if (bg->i8) {   // phcalc_i8's launches, each over the whole group
+            fb::launch_i8_split_group(bg->i8s, bg->i8rep, d.n2m, d.n3m, n, st);
+            fb::launch_i8x8_group(bg->i8t, d.n2m, d.n3m, n, st);
+            fb::glaunch_scan_poisson(g, st);
+            fb::launch_i8_split_group(bg->i8s + n, bg->i8rep, d.n2m, d.n3m, n, st);
+            fb::launch_i8x8_group(bg->i8t + n, d.n2m, d.n3m, n, st);
+            k += 7;
         } else {
             // phcalc_outflow.F90:31,61-69: hmn = dph zmmt^T, dph = vmn zmm^T
             CB(cublasDgemmBatched(bg->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, p, d.P, p + n,

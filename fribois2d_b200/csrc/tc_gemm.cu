@@ -657,9 +657,8 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // and chunk), then the digits of 32 x 32 tiles (one block each), every block
 // of a row deriving the same exponent from the chunk maxima.
 
-__global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
-                                                    double *__restrict__ cmax, int rows_pad) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void i8_rowmax_body(const double *__restrict__ src, long lds, int R, int K,
+                                               double *__restrict__ cmax, int rows_pad) {
     __shared__ double mx[8][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int r = blockIdx.x * 32 + lane, k0 = blockIdx.y * kI8Chunk;
@@ -679,13 +678,25 @@ __global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ sr
     }
 }
 
+__global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
+                                                    double *__restrict__ cmax, int rows_pad) {
+    FB_GRID_WAIT();
+    i8_rowmax_body(src, lds, R, K, cmax, rows_pad);
+}
+
+// grouped (blockIdx.z = case): the task array is host-written
+__global__ void __launch_bounds__(256) kg_i8_rowmax(const I8SplitTask *__restrict__ tk, int R, int K) {
+    const I8SplitTask t = tk[blockIdx.z];
+    FB_GRID_WAIT();
+    i8_rowmax_body(t.src, t.lds, R, K, t.cmax, t.rows_pad);
+}
+
 // dig[i * plane + r * ldk + k] = digit i of row r (k < K; 0 for k >= K or
 // r >= R, up to the padded rows and ldk), rowscale[r] = 2^e(r); the source is
 // column-major, A(r, k) at src[k * lds + r].  Block (x, y): rows 32x.., columns 32y..
-__global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ src, long lds, int R, int K,
-                                                    const double *__restrict__ cmax, int nchunk, int8_t *dig,
-                                                    long ldk, long plane, double *rowscale, int rows_pad) {
-    FB_GRID_WAIT();
+__device__ __forceinline__ void i8_digits_body(const double *__restrict__ src, long lds, int R, int K,
+                                               const double *__restrict__ cmax, int nchunk, int8_t *dig, long ldk,
+                                               long plane, double *rowscale, int rows_pad) {
     __shared__ double sc[32];
     __shared__ uint32_t tile[kI8S][32][9];   // 4 digits per word, rows padded to 9 words
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -728,6 +739,20 @@ __global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ sr
     }
 }
 
+__global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ src, long lds, int R, int K,
+                                                    const double *__restrict__ cmax, int nchunk, int8_t *dig,
+                                                    long ldk, long plane, double *rowscale, int rows_pad) {
+    FB_GRID_WAIT();
+    i8_digits_body(src, lds, R, K, cmax, nchunk, dig, ldk, plane, rowscale, rows_pad);
+}
+
+__global__ void __launch_bounds__(256) kg_i8_digits(const I8SplitTask *__restrict__ tk, int R, int K, int nchunk) {
+    const I8SplitTask t = tk[blockIdx.z];
+    FB_GRID_WAIT();
+    i8_digits_body(t.src, t.lds, R, K, t.cmax, nchunk, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale,
+                   t.rows_pad);
+}
+
 struct I8Cfg {
     static constexpr uint32_t kATile = 128 * kI8BK;                 // one A digit slice: 128 rows x 128 B
     static constexpr uint32_t kBSlice = kI8BN * kI8BK;              // one B digit slice
@@ -746,10 +771,9 @@ struct I8Cfg {
 // a ring; the MMA thread multiplies A slice i with B slices j < kI8S - i into
 // accumulators i + j (MMAs of K = 32 over up to four slices at once).  Every wait gives up after one
 // second with FB_ERR_TIMEOUT.
-__global__ void __launch_bounds__(kThreads, 1)
-    k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
-                int *status) {
-    FB_GRID_WAIT();
+template <bool kGlobalMaps>
+__device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorMap *mb, const I8Out &o, int K,
+                                          int *status) {
     using Cfg = I8Cfg;
     constexpr int kS = kI8S, kAS = Cfg::kASlots;
     extern __shared__ uint8_t smraw[];
@@ -794,6 +818,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     bool ok = true;
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
+        if (kGlobalMaps) acquire_maps(ma, ma, mb, mb);
         int ia = 0, nb = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
@@ -803,7 +828,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             mbar_expect_tx(bfull0 + 8 * sb, Cfg::kBStage);
             for (int j = 0; j < kS; ++j)
-                tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, &mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
+                tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
             nb = kb + 1;
             for (int i = 0; i < kS; ++i) {
                 const int slot = ia % kAS;
@@ -812,7 +837,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 mbar_expect_tx(afull0 + 8 * slot, Cfg::kATile);
-                tma_load_3d(sA + slot * Cfg::kATile, &ma, afull0 + 8 * slot, kb * kI8BK, m0, i);
+                tma_load_3d(sA + slot * Cfg::kATile, ma, afull0 + 8 * slot, kb * kI8BK, m0, i);
                 ++ia;
             }
         }
@@ -899,6 +924,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols)
                      : "memory");
     }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
+                int *status) {
+    FB_GRID_WAIT();
+    i8x8_body<false>(&ma, &mb, o, K, status);
+}
+
+// grouped: blockIdx.z selects the product
+__global__ void __launch_bounds__(kThreads, 1) kg_i8x8_gemm(const I8Task *__restrict__ t) {
+    FB_GRID_WAIT();
+    const I8Task &tk = t[blockIdx.z];
+    const I8Out o = tk.o;
+    i8x8_body<true>(&tk.a, &tk.b, o, tk.K, tk.status);
 }
 
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
@@ -1060,10 +1100,23 @@ int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
 }
 
 int i8_configure() {
-    return cudaFuncSetAttribute(k_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(I8Cfg::kSmem)) == cudaSuccess
-               ? FB_OK
-               : FB_ERR_CUDA;
+    const bool ok = cudaFuncSetAttribute(k_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(kg_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg::kSmem)) == cudaSuccess;
+    return ok ? FB_OK : FB_ERR_CUDA;
+}
+
+void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st) {
+    const int nchunk = (K + kI8Chunk - 1) / kI8Chunk;
+    pdl(kg_i8_rowmax, dim3(rep.rows_pad / 32, nchunk, n), dim3(256), 0, st, tasks, R, K);
+    pdl(kg_i8_digits, dim3(rep.rows_pad / 32, static_cast<unsigned>(rep.ldk / 32), n), dim3(256), 0, st, tasks, R, K,
+        nchunk);
+}
+
+void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, cudaStream_t st) {
+    const dim3 grid((M + 127) / 128, (N + kI8BN - 1) / kI8BN, n);
+    pdl(kg_i8x8_gemm, grid, dim3(kThreads), I8Cfg::kSmem, st, tasks);
 }
 
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {

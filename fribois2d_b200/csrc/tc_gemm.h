@@ -73,6 +73,21 @@ struct I8Out {
     const double *rowscale, *colscale;
     int M, N;
 };
+// grouped launches (blockIdx.z = case): per-case split sources and products
+struct I8SplitTask {
+    const double *src;
+    long lds;
+    int8_t *dig;
+    long ldk;
+    double *scale, *cmax;
+    int rows_pad;
+};
+struct I8Task {
+    CUtensorMap a, b;
+    I8Out o;
+    int K;
+    int *status;
+};
 int i8_configure();
 // box_rows: 128 for the A operand, kI8BN for B
 int i8_plan(I8Plan &p, int rows, int K, int box_rows);
@@ -80,6 +95,9 @@ int i8_plan(I8Plan &p, int rows, int K, int box_rows);
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
 // out[c * ldo + r] = sum_k A(r, k) B(c, k)
 void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st);
+// the same over n cases of one shape (rep: geometry of the split)
+void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st);
+void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, cudaStream_t st);
 
 int tf32x3_configure();
 bool tf32x3_shape_ok(int bn);

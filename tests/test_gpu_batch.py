@@ -65,8 +65,8 @@ def test_batch_rejects_variable_dt(tmp_path):
 
 def _grouped_cases():
     """Two cases on one grid with different Re (one group), a second grid, a
-    rectangle, and two cases of the first grid in the precision form (a
-    group of grouped 3xTF32 transforms)."""
+    rectangle, two cases of the first grid in the precision form (a group of
+    grouped 3xTF32 transforms) and two with the INT8 FP64 transforms."""
     a = cases.tiny_cylinder()
     b = cases.tiny_cylinder()
     b.name = "tiny_cylinder_re150"
@@ -78,11 +78,16 @@ def _grouped_cases():
     f = cases.tiny_cylinder()
     f.name = "tiny_cylinder_tf32_re120"
     f.params.visc = 1.0 / 120.0
-    return [a, b, c, d, e, f], {4, 5}
+    g = cases.tiny_cylinder()
+    g.name = "tiny_cylinder_int8"
+    h = cases.tiny_cylinder()
+    h.name = "tiny_cylinder_int8_re130"
+    h.params.visc = 1.0 / 130.0
+    return [a, b, c, d, e, f, g, h], {4, 5}, {6, 7}
 
 
 def test_batch_grouped_matches_separate_runs(tmp_path):
-    cs, precision = _grouped_cases()
+    cs, precision, int8 = _grouped_cases()
     alone, together = [], []
     for i, c in enumerate(cs):
         s1 = _open(c, tmp_path / "alone")
@@ -90,6 +95,9 @@ def test_batch_grouped_matches_separate_runs(tmp_path):
         if i in precision:
             s1.set_poisson(fb.POISSON_TF32X3)
             s2.set_poisson(fb.POISSON_TF32X3)
+        if i in int8:
+            s1.set_poisson(fb.POISSON_INT8X8)
+            s2.set_poisson(fb.POISSON_INT8X8)
         alone.append(s1)
         together.append(s2)
     for s in alone:
@@ -98,7 +106,7 @@ def test_batch_grouped_matches_separate_runs(tmp_path):
     batch = fb.Batch(together)  # advanced 6 steps below
     info = batch.info()
     print("grouped batch:", info)
-    assert info["groups"] >= 2 and info["launches"] > 0
+    assert info["groups"] >= 3 and info["launches"] > 0 and info["singles"] == 0
     steps = 6
     batch.advance(2)
     batch.advance(steps - 2)
