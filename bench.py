@@ -30,7 +30,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s (plain FP64 fluid time step, galloping rectangle 1024x768)"
-FORMS = {"fp64": "plain FP64", "tf32x3": "3xTF32 tensor-core Poisson transforms + FP64 refinement"}
+FORMS = {"fp64": "plain FP64", "tf32x3": "3xTF32 tensor-core Poisson transforms + FP64 refinement",
+         "int8x8": "FP64 Poisson transforms on the INT8 tensor cores (8 digit slices)"}
 
 
 def metric_name(args) -> str:
@@ -56,7 +57,10 @@ def parse():
                          "with one graph launch per step instead of the single case")
     ap.add_argument("--poisson", default="fp64", choices=sorted(FORMS),
                     help="eigen transforms of the Poisson solve: FP64 DGEMM, or 3xTF32 on the tensor cores")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.poisson == "int8x8" and not args.batch and args.impl != "reference":
+        ap.error("--poisson int8x8 is measured in batches (--batch N)")
+    return args
 
 
 def dist_env():
@@ -297,6 +301,8 @@ def batch_arm(args, rank, world, local):
         sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
         if args.poisson == "tf32x3":
             sv.set_poisson(fb.POISSON_TF32X3)
+        elif args.poisson == "int8x8":
+            sv.set_poisson(fb.POISSON_INT8X8)
         q2 = sv.get("q2")
         q2[1:c.n3m + 1] += c.v_perturbation()
         sv.set("q2", q2)
@@ -332,7 +338,8 @@ def batch_arm(args, rank, world, local):
                   "one launch per stage per group of equal grids)",
         "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.poisson == "fp64" else "f64 (Poisson transforms: 3xtf32)", "data": "synthetic",
+        "dtype": {"fp64": "f64", "tf32x3": "f64 (Poisson transforms: 3xtf32)",
+                  "int8x8": "f64 (Poisson transforms: exact int8 digit products)"}[args.poisson], "data": "synthetic",
         "config": {"workload": f"viv_batch_{args.batch}", "cells_total": cells,
                    "grids": {f"{n3}x{n2}": sum(1 for c in cs if (c.n3m, c.n2m) == (n3, n2))
                              for n3, n2, _ in cases.BATCH_GRIDS},
