@@ -30,12 +30,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s (plain FP64 fluid time step, galloping rectangle 1024x768)"
-FORMS = {"fp64": "plain FP64", "tf32x3": "3xTF32 tensor-core Poisson transforms + FP64 refinement",
-         "int8x8": "FP64 Poisson transforms on the INT8 tensor cores (8 digit slices)"}
+# Poisson transform forms: the plain FP64 path computes them on the INT8
+# tensor cores to FP64 accuracy (the default); "fp64" runs them as cuBLAS
+# DGEMMs, the comparison arm
+FORMS = {"int8x8": "plain FP64", "fp64": "plain FP64 with cuBLAS DGEMM transforms",
+         "tf32x3": "3xTF32 tensor-core Poisson transforms + FP64 refinement"}
+POISSON_IDS = {"int8x8": 2, "fp64": 0, "tf32x3": 1}
+DTYPES = {"int8x8": "f64 (Poisson transforms: exact int8 digit products)", "fp64": "f64",
+          "tf32x3": "f64 (Poisson transforms: 3xtf32)"}
 
 
 def metric_name(args) -> str:
-    if args.poisson == "fp64" and args.config == "galloping_rectangle_1024x768":
+    if args.poisson == "int8x8" and args.config == "galloping_rectangle_1024x768":
         return METRIC
     return f"cell-steps/s ({FORMS[args.poisson]} fluid time step, {args.config.replace('_', ' ')})"
 UNIT = "cell-steps/s"
@@ -55,12 +61,10 @@ def parse():
     ap.add_argument("--batch", type=int, default=0,
                     help="advance N independent VIV cases (grid sizes 256x192..768x512 drawn by seed) "
                          "with one graph launch per step instead of the single case")
-    ap.add_argument("--poisson", default="fp64", choices=sorted(FORMS),
-                    help="eigen transforms of the Poisson solve: FP64 DGEMM, or 3xTF32 on the tensor cores")
-    args = ap.parse_args()
-    if args.poisson == "int8x8" and not args.batch and args.impl != "reference":
-        ap.error("--poisson int8x8 is measured in batches (--batch N)")
-    return args
+    ap.add_argument("--poisson", default="int8x8", choices=sorted(FORMS),
+                    help="eigen transforms of the Poisson solve: FP64-accurate INT8 tensor-core products "
+                         "(default), cuBLAS DGEMM (comparison arm), or 3xTF32 on the tensor cores")
+    return ap.parse_args()
 
 
 def dist_env():
@@ -239,28 +243,41 @@ def fp64_gemm_peak(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def kernel_table(fb, path, c, poisson="fp64"):
+def kernel_table(fb, path, c, poisson="int8x8"):
     """Average device time of every kernel of one step, timed live with CUDA
     events on the launching stream, on a scratch context."""
     s = fb.Solver(path)
-    if poisson == "tf32x3":
-        s.set_poisson(fb.POISSON_TF32X3)
+    s.set_poisson(POISSON_IDS[poisson])
     s.autotune()   # the tile shapes the timed run uses (remembered per grid size)
     s.advance(0, 2)
     s.set_substep(1, 1)
     cells = c.cells
     B = 8.0 * cells
     n2m, n3m = c.n2m, c.n3m
-    # (name, stage, launches per step, algorithmic bytes or flops per launch, bound)
-    if poisson == "fp64":
+    gemm = 2.0 * n2m * n3m * n3m
+    # (name, stage, launches per step, algorithmic bytes or flops per launch, bound);
+    # rows with 0 launches per step are comparison rows, not part of the step
+    dgemm_rows = [
+        ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 0, gemm, "tensor"),
+        ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 0, gemm, "tensor"),
+    ]
+    if poisson == "int8x8":
+        # 36 digit-pair products of 2*n2m*n3m^2 integer ops each; the digit cut
+        # reads the FP64 operand and writes 8 int8 planes (16 B per cell)
         transform = [
-            ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+            ("i8x8 GEMM (tcgen05 kind::i8, 36 digit pairs)", "i8x8_gemm", 6, 36 * gemm, "tensor_i8"),
+            ("i8 digit cut (row maxima + digits)", "i8_split", 6, 2.0 * B, "hbm"),
             ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
-            ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, 2.0 * n2m * n3m * n3m, "tensor"),
+        ] + dgemm_rows
+    elif poisson == "fp64":
+        transform = [
+            ("gemm_fwd (cuBLAS DGEMM)", "gemm_fwd", 3, gemm, "tensor"),
+            ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
+            ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, gemm, "tensor"),
         ]
     else:   # two solves per substep (the second on the residual), two transforms each
         transform = [
-            ("tf32x3 GEMM (tcgen05, 3 products)", "tf32x3_gemm", 12, 3 * 2.0 * n2m * n3m * n3m, "tensor_tf32"),
+            ("tf32x3 GEMM (tcgen05, 3 products)", "tf32x3_gemm", 12, 3 * gemm, "tensor_tf32"),
             ("poisson_tri", "poisson_tri", 6, 3 * B, "hbm"),
         ]
     rows = [
@@ -299,10 +316,7 @@ def batch_arm(args, rank, world, local):
     solvers = []
     for c in cs:
         sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
-        if args.poisson == "tf32x3":
-            sv.set_poisson(fb.POISSON_TF32X3)
-        elif args.poisson == "int8x8":
-            sv.set_poisson(fb.POISSON_INT8X8)
+        sv.set_poisson(POISSON_IDS[args.poisson])
         q2 = sv.get("q2")
         q2[1:c.n3m + 1] += c.v_perturbation()
         sv.set("q2", q2)
@@ -338,8 +352,7 @@ def batch_arm(args, rank, world, local):
                   "one launch per stage per group of equal grids)",
         "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp64": "f64", "tf32x3": "f64 (Poisson transforms: 3xtf32)",
-                  "int8x8": "f64 (Poisson transforms: exact int8 digit products)"}[args.poisson], "data": "synthetic",
+        "dtype": DTYPES[args.poisson], "data": "synthetic",
         "config": {"workload": f"viv_batch_{args.batch}", "cells_total": cells,
                    "grids": {f"{n3}x{n2}": sum(1 for c in cs if (c.n3m, c.n2m) == (n3, n2))
                              for n3, n2, _ in cases.BATCH_GRIDS},
@@ -401,8 +414,7 @@ def device_arm(args, rank, world, local):
     c = make_case(args.config)
     path = write_deck(c, rank)
     s = fb.Solver(path, device=local)
-    if args.poisson == "tf32x3":
-        s.set_poisson(fb.POISSON_TF32X3)
+    s.set_poisson(POISSON_IDS[args.poisson])
     tiles = s.autotune()   # tile shapes for this grid size (state preserved)
     pert = c.v_perturbation()
     q2 = s.get("q2")
@@ -479,10 +491,24 @@ def device_arm(args, rank, world, local):
         step_ms = dev_ms_max / K
         for r in table:
             r["share"] = r["ms"] * r["per_step"] / step_ms
-        dom = max((r for r in table if r["bound"] in ("hbm", "tensor", "tensor_tf32")),
+        # the dominant kernel of this library (library kernels are comparison rows)
+        dom = max((r for r in table if r["bound"] in ("hbm", "tensor", "tensor_tf32", "tensor_i8")
+                   and "cuBLAS" not in r["kernel"] and r["per_step"] > 0),
                   key=lambda r: r["ms"] * r["per_step"])
         traffic = profiled_traffic(c.name, dom["kernel"])
-        if dom["bound"] == "tensor":
+        if dom["bound"] == "tensor_i8":
+            # dense INT8 runs at twice the bf16 rate on these tensor cores; the
+            # measured bf16 burst figure doubled is the denominator
+            peak_i8 = float(peaks.get("bf16_tflops", 1590.0)) * 2.0
+            achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e12
+            roof = {"kernel": dom["kernel"], "bound": "tensor", "achieved": achieved, "peak": peak_i8,
+                    "unit": "TFLOP/s", "frac": achieved / peak_i8, "traffic": traffic,
+                    "peak_source": ("of measured: MEASURED_PEAKS.json bf16_tflops x 2 (dense INT8 rate; "
+                                    "integer ops counted as flop)" if "bf16_tflops" in peaks
+                                    else "of fallback 1.59 PFLOP/s bf16 x 2"),
+                    "work_per_launch": f"36 digit pairs x 2*n2m*n3m^2 = {dom['work']:.4g} integer ops",
+                    "fp64_equivalent_tflops": dom["work"] / 36.0 / (dom["ms"] * 1e-3) / 1e12}
+        elif dom["bound"] == "tensor":
             achieved = dom["work"] / (dom["ms"] * 1e-3) / 1e12
             roof = {"kernel": dom["kernel"], "bound": "tensor", "achieved": achieved, "peak": peak_fp64,
                     "unit": "TFLOP/s", "frac": achieved / peak_fp64, "traffic": traffic,
@@ -513,7 +539,7 @@ def device_arm(args, rank, world, local):
         result = {
             "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.poisson == "fp64" else "f64 (Poisson transforms: 3xtf32)", "data": "synthetic",
+            "dtype": DTYPES[args.poisson], "data": "synthetic",
             "config": {"workload": c.name, "poisson": args.poisson, "cells": c.cells, "markers": c.nlm, "dt": c.params.dt,
                        "parallelism": f"replicas x{world}" if world > 1 else "single case",
                        "tiles": {"helsolve_rows": tiles[0], "gemm_cols": tiles[1] if args.poisson == "tf32x3" else None},

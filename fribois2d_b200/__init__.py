@@ -46,7 +46,8 @@ FIELDS = ("q2", "q3", "pr", "dph", "rhs2", "rhs3", "ru2", "ru3")
 BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", "dq2x2o", "dq3x2o")
 STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
               phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17,
-              gemm_fwd=100, poisson_tri=101, gemm_bwd=102, tf32x3_gemm=103)
+              gemm_fwd=100, poisson_tri=101, gemm_bwd=102, tf32x3_gemm=103, i8_split=104,
+              i8x8_gemm=105)
 HIST_COLS = 31
 HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
               "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm", "dt",
@@ -450,8 +451,10 @@ class Solver:
         return {k: float(s[i]) for i, k in enumerate(SCALAR_NAMES)}
 
     def set_poisson(self, mode: int) -> None:
-        """POISSON_FP64 (the reference's FP64 transforms) or POISSON_TF32X3
-        (3xTF32 tensor-core transforms plus one FP64 refinement sweep)."""
+        """POISSON_INT8X8 (the default: FP64-accurate transforms on the INT8
+        tensor cores), POISSON_FP64 (the transforms as cuBLAS DGEMMs, the
+        comparison arm) or POISSON_TF32X3 (3xTF32 tensor-core transforms plus
+        FP64 refinement sweeps)."""
         _check(self._lib.fb_set_poisson(self.ctx, int(mode)), "fb_set_poisson")
 
     def autotune(self):
@@ -503,6 +506,13 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self._lib.fb_synchronize(self.ctx), "fb_synchronize")
+
+    def dims(self) -> list:
+        """n2, n3, nlm, nsst, field pitch, Poisson pitch, pivoting flags,
+        helsolve windows of substep 1 (y | z << 8; 0 = full line scans)."""
+        d = (ctypes.c_int32 * 8)()
+        _check(self._lib.fb_get_dims(self.ctx, d), "fb_get_dims")
+        return list(d)
 
 
 def version() -> str:

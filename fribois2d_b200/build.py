@@ -61,14 +61,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    objs, cmds = [], []
     for src, extra in UNITS:
         obj = os.path.join(BUILD, src + ".o")
-        cmd = [nvcc, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append([nvcc, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # the units compile independently: one nvcc per unit, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    if verbose:
+        for cmd in cmds:
+            print(" ".join(cmd))
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for _ in ex.map(subprocess.check_call, cmds):
+            pass
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcublasLt", "-lgomp", "-Xcompiler", "-fPIC"]
     if verbose:

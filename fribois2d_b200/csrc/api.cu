@@ -393,6 +393,8 @@ int build_poisson(fb_ctx *c) {
     return FB_OK;
 }
 
+int setup_i8(fb_ctx *c);
+
 int create_impl(const char *dir, int device, fb_ctx *c) {
     std::string err = fb::setup_case(dir, c->hc);
     if (!err.empty()) {
@@ -568,6 +570,11 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = build_poisson(c))) return st;
     if ((st = dup(c, &c->zmm, c->hc.zmm))) return st;
     if ((st = dup(c, &c->zmmt, c->hc.zmmt))) return st;
+    // the default Poisson transforms: FP64-accurate products of this
+    // library's INT8 tensor-core kernel (cuBLAS DGEMM stays selectable with
+    // fb_set_poisson(FB_POISSON_FP64) as the comparison arm)
+    if ((st = setup_i8(c))) return st;
+    c->poisson_mode = FB_POISSON_INT8X8;
     CK(cudaDeviceSynchronize());
     return FB_OK;
 }
@@ -834,7 +841,7 @@ int phcalc_i8(fb_ctx *c) {
     fb::launch_scan_poisson(d, st);
     fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
     fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st);
-    c->own_launches += 4;
+    c->own_launches += 7;   // two splits of two launches, two products, the mode solves
     return FB_OK;
 }
 
@@ -900,6 +907,14 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_TK_TF32X3_GEMM:
         if (!c->pw) return FB_ERR_STATE;
         fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
+        break;
+    case FB_TK_I8_SPLIT:
+        if (!c->i8_ready) return FB_ERR_STATE;
+        fb::launch_i8_split(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, st);
+        break;
+    case FB_TK_I8X8_GEMM:
+        if (!c->i8_ready) return FB_ERR_STATE;
+        fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
         break;
     default: return FB_ERR_STATE;
     }
@@ -2688,6 +2703,7 @@ int fb_gemm_tf32x3(int device, int M, int N, int K, int bn, const double *A, con
 
 int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double *B, double *C) {
     if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return FB_ERR_STATE;
+    if (K > fb::kI8MaxK) return FB_ERR_UNSUPPORTED;   // int32 class sums would overflow
     CK(cudaSetDevice(device));
     int st = fb::i8_configure();
     if (st) return st;

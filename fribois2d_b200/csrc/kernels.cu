@@ -78,7 +78,9 @@ __device__ __forceinline__ void cfl_body(const Dev &d) {
             const double udx2 = d.udx2m[j];
             const double q = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
                               fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
-            qcf = fmax(qcf, q);
+            // fmax drops a NaN: a non-finite velocity turns into +inf, which
+            // every later fmax keeps, so the CFL test below catches it
+            qcf = fmax(qcf, (q == q) ? q : INFINITY);
             q3a = q3a + Fv(d.q3, j, k) * dz * (d.rc[jp] - d.rc[j]);
         }
     }
@@ -109,7 +111,7 @@ __device__ __forceinline__ void cfl_body(const Dev &d) {
         d.scal[S_Q3AVG] = as / (d.rext2 * d.alx3);
         // fixed dt: the stability check of fluid_tsch.F90:49-55; variable dt
         // is set from am on the host (fluid_tsch.F90:34-48)
-        if (!d.vardt && (cflm > d.cfllim || !(cflm == cflm))) raise_status(d, FB_ERR_CFL);
+        if (!d.vardt && !(cflm <= d.cfllim)) raise_status(d, FB_ERR_CFL);
     }
 }
 

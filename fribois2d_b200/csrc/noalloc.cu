@@ -17,6 +17,7 @@
 // GPU (different streams, no ordering between them) race on the array.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 
@@ -56,7 +57,8 @@ __global__ void __launch_bounds__(kThreads) k_cfl_rows(double *scratch, const do
     for (int j = t + 1; j <= n2m; j += kThreads) {
         const double a = (q2[static_cast<size_t>(k) * pitch + j - 1] + q2[static_cast<size_t>(k) * pitch + j]) * 0.5 * udx2m[j - 1];
         const double b = (q3[static_cast<size_t>(k) * pitch + j - 1] + q3[static_cast<size_t>(k + 1) * pitch + j - 1]) * 0.5 * udx3;
-        mx = fmax(mx, fabs(a) + fabs(b));
+        const double q = fabs(a) + fabs(b);
+        mx = fmax(mx, (q == q) ? q : INFINITY);   // a NaN velocity reads as +inf
         sm = sm + q3[static_cast<size_t>(k) * pitch + j - 1] * (zz[k] - zz[k - 1]) * (rc[j] - rc[j - 1]);
     }
     mx = warp_max(mx);
@@ -92,15 +94,19 @@ __global__ void __launch_bounds__(kThreads) k_cfl_rows(double *scratch, const do
 }
 
 double *scratch_for_device(int dev) {
-    // device addresses of g_cfl_scratch, looked up on first use per device
-    static double *addr[64] = {nullptr};
+    // device addresses of g_cfl_scratch, looked up on first use per device;
+    // two host threads may both look it up the first time, and both store
+    // the same address
+    static std::atomic<double *> addr[64];
     if (dev < 0 || dev >= 64) return nullptr;
-    if (!addr[dev]) {
+    double *a = addr[dev].load(std::memory_order_acquire);
+    if (!a) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_cfl_scratch) != cudaSuccess) return nullptr;
-        addr[dev] = static_cast<double *>(p);
+        a = static_cast<double *>(p);
+        addr[dev].store(a, std::memory_order_release);
     }
-    return addr[dev];
+    return a;
 }
 
 }  // namespace
@@ -126,7 +132,14 @@ extern "C" int fb_cfl_noalloc(const double *q2, const double *q3, int pitch, int
     // short; clear it so that this call's last block is found correctly
     if (cudaMemsetAsync(scratch + 2 * FB_NOALLOC_MAX_ROWS, 0, sizeof(unsigned), st) != cudaSuccess)
         return FB_ERR_CUDA;
-    k_cfl_rows<<<n3m, kThreads, 0, st>>>(scratch, q2, q3, pitch, n2m, n3m, rc, zz, udx2m, udx3m, dt, rext2, alx3,
-                                         out);
-    return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+    // the launch's own status (cudaGetLastError would also return, and clear,
+    // an earlier error of the caller's); the runtime may still report an
+    // earlier asynchronous error here
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(n3m));
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = st;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_cfl_rows, scratch, q2, q3, pitch, n2m, n3m, rc, zz, udx2m,
+                                             udx3m, dt, rext2, alx3, out);
+    return e == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }

@@ -644,13 +644,17 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // 8-bit digits, a = sum_i d_i 128^-(i+1), likewise the rows of B with f(c).
 // Then
 //   C(r,c) = 2^(e(r)+f(c)) sum_t 128^-(t+2) G_t(r,c),  G_t = sum_{i+j=t} D_i E_j^T,
-// keeping the digit pairs with i + j < kI8S (the dropped ones are below
-// 2^-63 K of the row and column maxima).  Each G_t is an exact int32 sum of
-// tcgen05.mma kind::i8 products accumulated in its own TMEM columns; the
-// epilogue adds the G_t in FP64 from the smallest weight up and applies the
-// power-of-two scales (exact).  The error is that of those FP64 additions
-// and of the dropped digits: ~2e-16 of sum |a||b| for K = 1024, as FP64
-// DGEMM.
+// keeping the digit pairs with i + j < kI8S.  Each G_t is an exact int32
+// sum of tcgen05.mma kind::i8 products accumulated in its own TMEM columns
+// (exact while K <= kI8MaxK); the epilogue adds the G_t in FP64 from the
+// smallest weight up and applies the power-of-two scales (exact).  The
+// error is absolute, relative to the row and column maxima: the digit
+// truncation and the dropped pairs leave at most about
+// K 2^-55 max|A(r,:)| max|B(c,:)| (each operand is cut to 56 bits of its
+// row maximum), plus the rounding of the FP64 additions.  For rows of
+// moderate dynamic range that is ~2e-16 of sum |a||b| at K = 1024, as FP64
+// DGEMM; a row whose entries span many decades is reproduced only to
+// 2^-55 of its largest entry.
 
 // Digit split in two launches so that the whole GPU takes part: the
 // maxima of |A(r, k)| over chunks of kI8Chunk columns (one block per 32 rows
@@ -1075,6 +1079,7 @@ void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane 
 
 // ---- INT8 FP64 products: buffers, maps, launches
 int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
+    if (K > kI8MaxK) return FB_ERR_UNSUPPORTED;   // the int32 class sums would overflow
     if (!p.dig || (p.ldk % 128) || p.rows_pad < rows) return FB_ERR_STATE;
     if (!g_encode) {
         void *fn = nullptr;

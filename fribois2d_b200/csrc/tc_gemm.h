@@ -59,6 +59,10 @@ constexpr int kI8S = 8;       // digit slices per operand
 constexpr int kI8BK = 128;    // K bytes per k-block (one 128-byte swizzle row)
 constexpr int kI8BN = 64;     // output tile width
 constexpr int kI8Chunk = 64;  // columns per row-maximum block of the digit split
+// Largest K of one product: weight class t = kI8S - 1 sums kI8S digit pairs
+// of at most 127 * 127 per k into an int32 TMEM accumulator, so
+// K * kI8S * 127^2 must stay below 2^31 (K <= 16642); i8_plan rejects more.
+constexpr int kI8MaxK = 16384;
 struct I8Plan {
     CUtensorMap map;
     int8_t *dig;

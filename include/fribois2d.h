@@ -268,24 +268,30 @@ int fb_last_advance_ms(fb_ctx *ctx, double *ms);
 #define FB_TK_POISSON_TRI 101 /* phcalc_outflow.F90:34-56 per-mode y solves */
 #define FB_TK_GEMM_BWD 102   /* phcalc_outflow.F90:61 back transform */
 #define FB_TK_TF32X3_GEMM 103 /* one 3xTF32 tensor-core transform (precision form) */
+#define FB_TK_I8_SPLIT 104    /* digit cut of dph for the INT8 transform (two launches) */
+#define FB_TK_I8X8_GEMM 105   /* one INT8 digit-slice transform, hmn = dph zmmt^T */
 int fb_time_stage(fb_ctx *ctx, int stage, int n, int reps, double *ms);
 /* Number of this library's own kernels one captured time step launches
  * (library kernels of cuBLAS and CUB are not counted). */
 int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
 
-/* ---- precision form of the Poisson solve ---------------------------------
- * FB_POISSON_FP64: phcalc as the reference computes it (FP64 DGEMM
- * transforms).  FB_POISSON_TF32X3: the two eigen transforms on the tensor
- * cores in split precision (TF32 high and low parts, three products, FP32
- * accumulation), FP64 tridiagonal solves, then one FP64 iterative-refinement
- * sweep on the Poisson residual.  No counterpart in the reference. */
+/* ---- forms of the Poisson eigen transforms --------------------------------
+ * The reference computes phcalc's two transforms with FP64 DGEMM
+ * (phcalc_outflow.F90:31,61).  A new context computes them to the same FP64
+ * accuracy with this library's INT8 tensor-core kernel (FB_POISSON_INT8X8,
+ * below), the default.  FB_POISSON_FP64: the transforms as cuBLAS DGEMMs,
+ * kept as the comparison arm.  FB_POISSON_TF32X3: the two eigen transforms on
+ * the tensor cores in split precision (TF32 high and low parts, three
+ * products, FP32 accumulation), FP64 tridiagonal solves, then FP64
+ * iterative-refinement sweeps on the Poisson residual.  The forms have no
+ * counterpart in the reference. */
 #define FB_POISSON_FP64 0
 #define FB_POISSON_TF32X3 1
-/* FB_POISSON_INT8X8: the two FP64 eigen transforms computed exactly in
- * integer arithmetic on the INT8 tensor cores (rows scaled by powers of two
- * and cut into 8 signed 8-bit digits; the digit products summed in FP64):
- * FP64-level accuracy (~2e-16 of sum |a||b| at K = 1024, as DGEMM), no
- * refinement sweep.  No counterpart in the reference. */
+/* FB_POISSON_INT8X8 (the default): the two FP64 eigen transforms computed
+ * exactly in integer arithmetic on the INT8 tensor cores (rows scaled by
+ * powers of two and cut into 8 signed 8-bit digits; the digit products summed
+ * in FP64): FP64-level accuracy (~2e-16 of sum |a||b| at K = 1024, as DGEMM),
+ * no refinement sweep; K (= n3 - 1) at most 16384. */
 #define FB_POISSON_INT8X8 2
 int fb_set_poisson(fb_ctx *ctx, int mode);
 /* C = A * B^T with the INT8 digit-slice kernel (conventions and buffers as
@@ -328,7 +334,8 @@ int fb_eigen_tridiag(int n, const double *am, const double *ac, const double *ap
  * FB_NOALLOC_MAX_ROWS rows of z cells; larger grids return FB_ERR_UNSUPPORTED).
  * The first call on a device looks up that array's address (make it before
  * any stream capture); every call shares the array, so calls whose kernels
- * overlap on the GPU race.  Asynchronous on `stream` (a cudaStream_t, or NULL). */
+ * overlap on the GPU race.  Asynchronous on `stream` (a cudaStream_t, or NULL).
+ * A NaN or infinite velocity gives out[0] = +inf. */
 #define FB_NOALLOC_MAX_ROWS 8192
 int fb_cfl_noalloc(const double *q2, const double *q3, int pitch, int n2, int n3, const double *rc,
                    const double *zz, const double *udx2m, const double *udx3m, double dt, double rext2,

@@ -10,9 +10,15 @@ golden vectors, so the fixtures pin the two things that can be pinned:
   the small cylinder case, exactly as src/phini.F90:52-92 calls them;
 * ``traj_<case>.npz`` -- short trajectories of the CPU oracle on the two
   small cases (per-step loads and rigid-body state, final fields), used to
-  catch regressions in the oracle and as a fixed target for the device.
+  catch regressions in the oracle and as a fixed target for the device;
+* ``hist_<case>.npz`` -- full-length oracle histories of the benched cases
+  (the 384 x 256 VIV cylinder over 2000 steps, the 1024 x 768 galloping
+  rectangle over 5000 steps): the forcecomp.out and rigid-state rows of
+  every step and the final q2, q3, pr sampled every 4th row and column.
+  The oracle computes phini through LAPACK here, as the reference does.
 
-Run:  python tests/golden/make_golden.py
+Run:  python tests/golden/make_golden.py            (small fixtures)
+      python tests/golden/make_golden.py --hist NAME [THREADS] (one long history)
 """
 from __future__ import annotations
 
@@ -60,7 +66,38 @@ def lapack_systems(seed: int = 7):
     return out
 
 
+HIST_STEPS = {"viv_cylinder_384x256": 2000, "galloping_rectangle_1024x768": 5000}
+HIST_STRIDE = 4
+
+
+def long_history(name: str, threads: int = 0) -> None:
+    """Oracle history of a benched case over its full step count."""
+    c = cases.WORKLOADS[name]()
+    root = tempfile.mkdtemp(prefix="golden_")
+    path = c.write(os.path.join(root, c.name))
+    o = oracle.Oracle(oracle.parse_deck(path), threads=threads)
+    o.add_v_perturbation(c.v_perturbation())
+    steps = HIST_STEPS[name]
+    forces = np.zeros((steps, 8))
+    rigid = np.zeros((steps, 18))
+    for ns in range(steps):
+        st = o.step(ns)
+        assert st == 0, (ns, st)
+        forces[ns] = o.a("forces")
+        rigid[ns] = o.a("rigid")
+        if ns % 250 == 0:
+            print(name, ns, flush=True)
+    sub = np.s_[::HIST_STRIDE, ::HIST_STRIDE]
+    np.savez_compressed(
+        os.path.join(HERE, f"hist_{name}.npz"), forces=forces, rigid=rigid, steps=np.array([steps]),
+        stride=np.array([HIST_STRIDE]), q2=o.field("q2", 0, o.n3)[sub].copy(),
+        q3=o.field("q3", 0, o.n3)[sub].copy(), pr=o.field("pr", 0, o.n3)[sub].copy())
+
+
 def main() -> None:
+    if len(sys.argv) in (3, 4) and sys.argv[1] == "--hist":
+        long_history(sys.argv[2], threads=int(sys.argv[3]) if len(sys.argv) == 4 else 0)
+        return
     np.savez_compressed(os.path.join(HERE, "lapack_gtt.npz"), **lapack_systems())
     root = tempfile.mkdtemp(prefix="golden_")
     c = cases.tiny_cylinder()

@@ -31,20 +31,25 @@ def deck_dir(c: cases.Case, root: str = None) -> str:
 class Pair:
     """The same case on the oracle and on the device."""
 
-    def __init__(self, c: cases.Case, root: str = None, gpu: bool = True, threads: int = 0):
+    def __init__(self, c: cases.Case = None, root: str = None, gpu: bool = True, threads: int = 0,
+                 deck: str = None):
+        """A generated case `c` (written under `root`, seeded v noise added
+        to both sides) or an existing deck directory `deck` (taken as is)."""
         self.case = c
-        self.dir = deck_dir(c, root)
+        self.dir = deck if deck else deck_dir(c, root)
         self.host = fb.HostSetup(self.dir)
         eig = (self.host.array("wr"), self.host.array("zmm"), self.host.array("zmmt"))
         self.o = oracle.Oracle(oracle.parse_deck(self.dir), eigen=eig, threads=threads)
-        pert = c.v_perturbation()
-        self.o.add_v_perturbation(pert)
+        pert = c.v_perturbation() if c is not None else None
+        if pert is not None:
+            self.o.add_v_perturbation(pert)
         self.s = None
         if gpu:
             self.s = fb.Solver(self.dir)
-            q2 = self.s.get("q2")
-            q2[1:c.n3m + 1] += pert
-            self.s.set("q2", q2)
+            if pert is not None:
+                q2 = self.s.get("q2")
+                q2[1:c.n3m + 1] += pert
+                self.s.set("q2", q2)
         self.n2, self.n3 = self.o.n2, self.o.n3
         self.n2m, self.n3m = self.n2 - 1, self.n3 - 1
 

@@ -1,8 +1,8 @@
 """Batches of independent cases: one graph launch steps every case.  The
 graph mode holds every case's own captured step; the grouped mode launches
-each stage once over every group of cases of one launch geometry (batched
-DGEMMs for the transforms).  Both are checked against stepping each case on
-its own."""
+each stage once over every group of cases of one launch geometry (grouped
+INT8 tensor-core transforms, or batched DGEMMs in the FP64 comparison form).
+Both are checked against stepping each case on its own."""
 import numpy as np
 import pytest
 
@@ -64,9 +64,10 @@ def test_batch_rejects_variable_dt(tmp_path):
 
 
 def _grouped_cases():
-    """Two cases on one grid with different Re (one group), a second grid, a
-    rectangle, two cases of the first grid in the precision form (a group of
-    grouped 3xTF32 transforms) and two with the INT8 FP64 transforms."""
+    """Two cases on one grid with different Re (one group, transforms as
+    batched cuBLAS DGEMMs), a second grid, a rectangle, two cases of the
+    first grid in the precision form (a group of grouped 3xTF32 transforms)
+    and two more with the INT8 FP64 transforms (the default form)."""
     a = cases.tiny_cylinder()
     b = cases.tiny_cylinder()
     b.name = "tiny_cylinder_re150"
@@ -98,6 +99,9 @@ def test_batch_grouped_matches_separate_runs(tmp_path):
         if i in int8:
             s1.set_poisson(fb.POISSON_INT8X8)
             s2.set_poisson(fb.POISSON_INT8X8)
+        if i in (0, 1):
+            s1.set_poisson(fb.POISSON_FP64)
+            s2.set_poisson(fb.POISSON_FP64)
         alone.append(s1)
         together.append(s2)
     for s in alone:

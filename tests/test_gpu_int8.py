@@ -50,8 +50,7 @@ def test_i8x8_gemm_zero_rows():
 
 def _run(c, path, mode, steps):
     s = fb.Solver(path)
-    if mode:
-        s.set_poisson(mode)
+    s.set_poisson(mode)
     q2 = s.get("q2")
     q2[1:c.n3m + 1] += c.v_perturbation()
     s.set("q2", q2)
@@ -65,7 +64,7 @@ def _run(c, path, mode, steps):
 def test_int8_step_matches_fp64(maker, steps, tmp_path):
     c = maker()
     path = c.write(str(tmp_path / c.name))
-    a, ha = _run(c, path, 0, steps)
+    a, ha = _run(c, path, fb.POISSON_FP64, steps)
     b, hb = _run(c, path, fb.POISSON_INT8X8, steps)
     n2m, n3m = c.n2m, c.n3m
     for f in ("q2", "q3", "pr"):

@@ -213,6 +213,19 @@ def test_cfl_overflow_is_reported(tmp_path):
     assert e.value.code == fb.FB_ERR_CFL
 
 
+def test_nan_velocity_is_reported(tmp_path):
+    """A NaN velocity is a CFL failure, not a finite CFL number: the max
+    reduction keeps it (as +inf) instead of dropping it."""
+    c = cases.tiny_cylinder()
+    s = fb.Solver(c.write(str(tmp_path / c.name)))
+    q2 = s.get("q2")
+    q2[5, 3] = np.nan
+    s.set("q2", q2)
+    with pytest.raises(fb.FBError) as e:
+        s.fluid_tsch(0)
+    assert e.value.code == fb.FB_ERR_CFL
+
+
 @pytest.mark.parametrize("nsst", [3, 1])
 def test_variable_dt_matches_oracle(nsst, tmp_path):
     """idtv = .false. (fluid_tsch.F90:34-48): dt = cflmax / cflm from the

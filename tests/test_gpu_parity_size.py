@@ -1,0 +1,103 @@
+"""Parity at the benched sizes and on the reference's own input decks.
+
+* Per step against the oracle run beside the device on identical inputs
+  (the device's eigen data handed to both): the 384 x 256 VIV cylinder
+  over 100 steps, the 1024 x 768 galloping rectangle over 30 steps, and the
+  reference's two decks (test_OscCyl1DOF: 811 x 673 nodes, 377 markers;
+  test_GallRect1DOF: 731 x 561 nodes, 798 markers) over 20 steps.  Bar:
+  1e-10 relative per step on the velocities, the mean-free pressure and the
+  loads, 1e-12 on the rigid-body state.
+* Full-length histories against committed oracle runs
+  (tests/golden/hist_*.npz, made by tests/golden/make_golden.py with
+  phini through LAPACK, as the reference computes it): 2000 steps of the
+  cylinder and 5000 of the rectangle through the graph-replayed fb_advance.
+  Bar: lift (or moment) and displacement (or pitch) within 1e-8 of their
+  range; the final fields, sampled every 4th row and column, within 1e-8.
+
+The windowed helsolve (truncated LU recurrences, window K = 9 on the
+rectangle) and the INT8 digit-slice transforms run at these sizes exactly
+as in the benchmark.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import fribois2d_b200 as fb
+from fribois2d_b200 import case as cases
+from paritylib import Pair, rel
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+DECKS = os.path.join(GOLD, "decks")
+
+
+def _sub(a, n2m, n3m):
+    return a[1:n3m + 1, :n2m]
+
+
+def _step_by_step(p, steps):
+    n2m, n3m = p.n2m, p.n3m
+    worst = {"q2": 0.0, "q3": 0.0, "pr": 0.0, "forces": 0.0, "rigid": 0.0}
+    for ns in range(steps):
+        assert p.o.step(ns) == 0
+        p.s.fluid_tsch(ns)
+        p.s.rigid(ns)
+        for f in ("q2", "q3", "pr"):
+            e = rel(_sub(p.s.get(f), n2m, n3m), _sub(p.of(f), n2m, n3m))
+            worst[f] = max(worst[f], e)
+            assert e <= 1e-10, (f, ns, e)
+        e = rel(p.s.get("forces")[1:4], p.o.a("forces")[1:4])
+        worst["forces"] = max(worst["forces"], e)
+        assert e <= 1e-10, ("forces", ns, e)
+        e = rel(p.s.get("rigid"), p.o.a("rigid"))
+        worst["rigid"] = max(worst["rigid"], e)
+        assert e <= 1e-12, ("rigid", ns, e)
+    return worst
+
+
+@pytest.mark.parametrize("maker,steps", [(cases.viv_cylinder_384x256, 100),
+                                         (cases.galloping_rectangle_1024x768, 30)])
+def test_benched_case_per_step(maker, steps, tmp_path):
+    p = Pair(maker(), str(tmp_path))
+    dims = p.s.dims()
+    worst = _step_by_step(p, steps)
+    print(f"{p.case.name}: helsolve windows {dims[7] & 0xff}/{dims[7] >> 8}, "
+          f"worst relative difference over {steps} steps: {worst}")
+    p.s.close()
+
+
+@pytest.mark.parametrize("deck", ["OscCyl1DOF", "GallRect1DOF"])
+def test_reference_deck_per_step(deck):
+    p = Pair(deck=os.path.join(DECKS, deck))
+    worst = _step_by_step(p, 20)
+    print(f"reference deck {deck} ({p.n2} x {p.n3} nodes): worst relative difference over 20 steps: {worst}")
+    p.s.close()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name,col", [("viv_cylinder_384x256", ("Fy", "py")),
+                                      ("galloping_rectangle_1024x768", ("M", "pa"))])
+def test_full_length_history(name, col, tmp_path):
+    z = np.load(os.path.join(GOLD, f"hist_{name}.npz"))
+    steps, stride = int(z["steps"][0]), int(z["stride"][0])
+    c = cases.WORKLOADS[name]()
+    s = fb.Solver(c.write(str(tmp_path / c.name)))
+    q2 = s.get("q2")
+    q2[1:c.n3m + 1] += c.v_perturbation()
+    s.set("q2", q2)
+    hist = s.advance(0, steps)
+    fcol = {"Fy": 1, "M": 3}[col[0]]
+    dcol = {"py": 0, "pa": 2}[col[1]]
+    force = hist[:, fb.HIST_NAMES.index(col[0])]
+    disp = hist[:, fb.HIST_NAMES.index(col[1])]
+    ref_f, ref_d = z["forces"][:, fcol], z["rigid"][:, 9 + dcol]
+    ef = float(np.max(np.abs(force - ref_f)) / max(np.ptp(ref_f), 1e-300))
+    ed = float(np.max(np.abs(disp - ref_d)) / max(np.ptp(ref_d), 1e-300))
+    sub = np.s_[::stride, ::stride]
+    ev = {f: rel(s.get(f)[sub], z[f]) for f in ("q2", "q3", "pr")}
+    print(f"{name}, {steps} steps: {col[0]} {ef:.3e}, {col[1]} {ed:.3e} of range; final fields {ev}")
+    assert ef <= 1e-8 and ed <= 1e-8, (ef, ed)
+    for f, e in ev.items():
+        assert e <= 1e-8, (f, e)
+    s.close()

@@ -15,7 +15,7 @@ from fribois2d_b200 import case as cases
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "fribois2d.h")
-REF = "/root/reference"
+DECKS = os.path.join(ROOT, "tests", "golden", "decks")
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -35,6 +35,38 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n)
     assert "sm_100a" in fb.version()
+
+
+def test_fortran_module_binds_every_entry_point():
+    """include/fribois2d.f90 (no Fortran compiler here, so checked as text):
+    one bind(C) interface per header function and the header's constants
+    with the same values."""
+    hdr = open(HEADER).read()
+    f90 = open(os.path.join(ROOT, "include", "fribois2d.f90")).read()
+    names = re.findall(r"^\s*(?:int|const char \*)\s*(fb_\w+)\s*\(", hdr, re.M)
+    bound = re.findall(r'bind\(C, name="(fb_\w+)"\)', f90)
+    assert sorted(names) == sorted(bound)
+    consts = dict(re.findall(r"^#define (FB_\w+) (-?\d+)", hdr, re.M))
+    fvals = dict((k, v) for k, v in re.findall(r"(FB_\w+) = (-?\d+)", f90))
+    assert set(fvals) == set(consts)
+    for k, v in consts.items():
+        assert fvals[k] == v, k
+
+
+def test_int8_product_bound_is_enforced_before_any_device_work():
+    """The INT8 digit product keeps its weight classes in int32: K is bounded
+    by 2^31 / (S * 127^2) and larger K is refused without touching the GPU."""
+    from oracle import i8x8
+    src = open(os.path.join(ROOT, "fribois2d_b200", "csrc", "tc_gemm.h")).read()
+    kmax = int(re.search(r"kI8MaxK = (\d+);", src).group(1))
+    assert int(re.search(r"kI8S = (\d+);", src).group(1)) == i8x8.S
+    assert kmax * i8x8.S * 127 * 127 < 2 ** 31
+    a = np.zeros(4 * (kmax + 1))
+    c = np.zeros(16)
+    import ctypes
+    f = fb.lib().fb_gemm_i8x8
+    p = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert f(0, 4, 4, kmax + 1, p(a), p(a), p(c)) == fb.FB_ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("maker", [cases.tiny_cylinder, cases.tiny_rectangle, cases.viv_cylinder_384x256])
@@ -92,12 +124,11 @@ def test_eigen_tridiag_on_uniform_neumann_operator():
     np.testing.assert_allclose(np.sort(wr), np.sort(exact), atol=1e-13)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference decks not present")
-@pytest.mark.parametrize("deck,nlm", [("test_OscCyl1DOF", 377), ("test_GallRect1DOF", 798)])
+@pytest.mark.parametrize("deck,nlm", [("OscCyl1DOF", 377), ("GallRect1DOF", 798)])
 def test_reference_decks_parse_identically(deck, nlm, tmp_path):
     """The reference's own input decks: both parsers agree, markers are
     counted as newlines - 1 (utils_proc.F90:529-535)."""
-    src = os.path.join(REF, deck, "input_FSI")
+    src = os.path.join(DECKS, deck)
     dst = str(tmp_path / "input_FSI")
     shutil.copytree(src, dst)
     d = oracle.parse_deck(dst)

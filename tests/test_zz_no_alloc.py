@@ -50,6 +50,14 @@ def test_cfl_noalloc_matches_context(tmp_path):
         got = out.cpu().numpy()
         assert got[0] == pytest.approx(ref["cflm"], rel=1e-13, abs=0), call
         assert got[1] == pytest.approx(ref["q3avg"], rel=1e-13, abs=0), call
+    # a NaN velocity is not hidden by the max reduction: the CFL number is +inf
+    t["q2"][5, 3] = float("nan")
+    st = f(t["q2"].data_ptr(), t["q3"].data_ptr(), p.n2, p.n2, p.n3, t["rc"].data_ptr(),
+           t["zz"].data_ptr(), udx2m.data_ptr(), udx3m.data_ptr(), p.dt, p.rext2, p.alx3,
+           out.data_ptr(), None)
+    assert st == 0, st
+    torch.cuda.synchronize()
+    assert out.cpu().numpy()[0] == float("inf")
 
 
 def test_cfl_noalloc_rejects_grids_beyond_its_scratch():
