@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=0,
                     help="advance N independent VIV cases (grid sizes 256x192..768x512 drawn by seed) "
                          "with one graph launch per step instead of the single case")
+    ap.add_argument("--sweeps", type=int, default=2, help="FP64 refinement sweeps of the tf32x3 form")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the tf32x3 form's accuracy comparison with the FP64 path")
     ap.add_argument("--poisson", default="int8x8", choices=sorted(FORMS),
                     help="eigen transforms of the Poisson solve: FP64-accurate INT8 tensor-core products "
                          "(default), cuBLAS DGEMM (comparison arm), or 3xTF32 on the tensor cores")
@@ -243,11 +246,12 @@ def fp64_gemm_peak(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def kernel_table(fb, path, c, poisson="int8x8"):
+def kernel_table(fb, path, c, poisson="int8x8", sweeps=2):
     """Average device time of every kernel of one step, timed live with CUDA
     events on the launching stream, on a scratch context."""
     s = fb.Solver(path)
     s.set_poisson(POISSON_IDS[poisson])
+    s.set_refinement(sweeps)
     s.autotune()   # the tile shapes the timed run uses (remembered per grid size)
     s.advance(0, 2)
     s.set_substep(1, 1)
@@ -275,10 +279,10 @@ def kernel_table(fb, path, c, poisson="int8x8"):
             ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
             ("gemm_bwd (cuBLAS DGEMM)", "gemm_bwd", 3, gemm, "tensor"),
         ]
-    else:   # two solves per substep (the second on the residual), two transforms each
+    else:   # 1 + sweeps solves per substep (the later ones on the residual), two transforms each
         transform = [
-            ("tf32x3 GEMM (tcgen05, 3 products)", "tf32x3_gemm", 12, 3 * gemm, "tensor_tf32"),
-            ("poisson_tri", "poisson_tri", 6, 3 * B, "hbm"),
+            ("tf32x3 GEMM (tcgen05, 3 products)", "tf32x3_gemm", 6 * (1 + sweeps), 3 * gemm, "tensor_tf32"),
+            ("poisson_tri", "poisson_tri", 3 * (1 + sweeps), 3 * B, "hbm"),
         ]
     rows = [
         ("cfl", "cfl", 1, 2 * B, "hbm"),
@@ -317,6 +321,7 @@ def batch_arm(args, rank, world, local):
     for c in cs:
         sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
         sv.set_poisson(POISSON_IDS[args.poisson])
+        sv.set_refinement(args.sweeps)
         q2 = sv.get("q2")
         q2[1:c.n3m + 1] += c.v_perturbation()
         sv.set("q2", q2)
@@ -373,21 +378,22 @@ def batch_arm(args, rank, world, local):
         print(json.dumps(line))
 
 
-def precision_error(fb, path, c, steps):
+def precision_error(fb, path, c, steps, sweeps):
     """The precision form against the plain FP64 path (itself within 1e-10
     per step of the oracle) on the same case and inputs: lift, displacement
-    and post-projection divergence after `steps` steps."""
+    and post-projection divergence over `steps` steps."""
     runs = {}
-    for mode in (fb.POISSON_FP64, fb.POISSON_TF32X3):
+    for mode in (fb.POISSON_INT8X8, fb.POISSON_TF32X3):
         s = fb.Solver(path)
         s.set_poisson(mode)
+        s.set_refinement(sweeps)
         s.set_report(True)
         q2 = s.get("q2")
         q2[1:c.n3m + 1] += c.v_perturbation()
         s.set("q2", q2)
         runs[mode] = s.advance(0, steps)
         s.close()
-    a, b = runs[fb.POISSON_FP64], runs[fb.POISSON_TF32X3]
+    a, b = runs[fb.POISSON_INT8X8], runs[fb.POISSON_TF32X3]
     col = {n: fb.HIST_NAMES.index(n) for n in ("Fy", "Fz", "py", "pa", "dmax")}
     def rel(x, y):
         return float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300))
@@ -396,6 +402,7 @@ def precision_error(fb, path, c, steps):
             "displacement_abs": float(np.max(np.abs(b[:, col["py"]] - a[:, col["py"]]))),
             "divergence_max_fp64": float(np.max(a[:, col["dmax"]])),
             "divergence_max_tf32x3": float(np.max(b[:, col["dmax"]])),
+            "refinement_sweeps": sweeps, "resid": 1e-7,
             "reference": "plain FP64 device path (parity with the oracle: 1e-10 per step)"}
 
 
@@ -415,6 +422,7 @@ def device_arm(args, rank, world, local):
     path = write_deck(c, rank)
     s = fb.Solver(path, device=local)
     s.set_poisson(POISSON_IDS[args.poisson])
+    s.set_refinement(args.sweeps)
     tiles = s.autotune()   # tile shapes for this grid size (state preserved)
     pert = c.v_perturbation()
     q2 = s.get("q2")
@@ -478,7 +486,7 @@ def device_arm(args, rank, world, local):
 
     result = None
     if rank == 0:
-        table = kernel_table(fb, path, c, args.poisson)
+        table = kernel_table(fb, path, c, args.poisson, args.sweeps)
         peak_fp64 = fp64_gemm_peak(torch, dev)
         peaks = {}
         try:
@@ -530,7 +538,7 @@ def device_arm(args, rank, world, local):
                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": hbm_src}
         accuracy = None
         if args.poisson == "tf32x3":
-            accuracy = precision_error(fb, path, c, steps=50)
+            accuracy = precision_error(fb, path, c, steps=args.accuracy_steps, sweeps=args.sweeps)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             v, steps, threads, secs = cpu_run(args.config, seconds=args.cpu_seconds, max_steps=1000)

@@ -106,6 +106,7 @@ def lib() -> ctypes.CDLL:
         "fb_host_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
         "fb_eigen_tridiag": ([ctypes.c_int, dp, dp, dp, dp, dp, dp], ctypes.c_int),
         "fb_set_poisson": ([vp, ctypes.c_int], ctypes.c_int),
+        "fb_set_refinement": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_set_report": ([vp, ctypes.c_int], ctypes.c_int),
         "fb_set_coupling": ([vp, ctypes.c_int, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "fb_set_predictor": ([vp, vp, P(ctypes.c_float)], ctypes.c_int),
@@ -456,6 +457,10 @@ class Solver:
         comparison arm) or POISSON_TF32X3 (3xTF32 tensor-core transforms plus
         FP64 refinement sweeps)."""
         _check(self._lib.fb_set_poisson(self.ctx, int(mode)), "fb_set_poisson")
+
+    def set_refinement(self, sweeps: int) -> None:
+        """FP64 refinement sweeps of the precision form (1..4, default 2)."""
+        _check(self._lib.fb_set_refinement(self.ctx, int(sweeps)), "fb_set_refinement")
 
     def autotune(self):
         """Tile shapes for this grid size, timed on this context: returns

@@ -28,6 +28,7 @@ UNITS = [
     ("tri.cu", []),
     ("tc_gemm.cu", []),
     ("mlp.cu", []),
+    ("couple.cu", ["-fmad=false"]),
     ("api.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]

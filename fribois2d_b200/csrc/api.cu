@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "../../include/fribois2d.h"
+#include "couple.h"
 #include "device.cuh"
 #include "host.h"
 #include "kernels.h"
@@ -73,26 +75,27 @@ struct fb_ctx {
     std::vector<std::pair<const int **, size_t>> coef_fixi;
     size_t coef_cap = 0, coef_capi = 0;
     bool vardt = false;       // idtv = .false.: dt from the CFL number every step
-    // strong fluid-structure coupling (fb_set_coupling): mode, test, state
+    // strong fluid-structure coupling (fb_set_coupling), iterated on the device
     int coupling = FB_COUPLING_LOOSE;
-    double ctol = 1e-8;
     int cmaxit = 50;
-    double omega0 = 0.5;
-    int free_dof = 0;                       // the body coordinate the predictor follows
-    std::vector<std::array<double, 3>> hist_p, hist_v, hist_f;   // converged steps, newest last
-    double stat_steps = 0, stat_solves = 0, stat_maxit = 0, stat_res0 = 0;
-    std::vector<float> samples_x, samples_t;   // (features, targets) of converged steps
-    fb_mlp *mlp = nullptr;
-    std::vector<float> mlp_norm;               // x mean, x std, t mean, t std
+    fb::Couple *cpl = nullptr;                 // device: the iteration's set-up, state, history
+    fb::Couple **cpl_list = nullptr;           // device: {cpl}, the form the coupling kernels take
+    fb::SnapList snapl{};                      // the saved start-of-step state's arrays
+    fb::SnapList *snapl_d = nullptr;           // ... in device memory
+    long snap_longest = 0;
     double *snap = nullptr;                    // device copy of the step's starting state
-    std::vector<std::pair<double *, size_t>> snap_fields, snap_body;  // (device array, doubles)
-    double *fin_d = nullptr, *fin_h = nullptr; // trial load (device, pinned host)
-    double *rd_h = nullptr;                    // pinned read-back: trial state, fluid load, its state
+    float *smp_x = nullptr, *smp_t = nullptr;  // device ring of training samples
+    int smp_cap = 8192;
+    unsigned long long smp_drained = 0;
+    fb_mlp *mlp = nullptr;
+    float *mlp_norm_d = nullptr;               // x mean, x std, t mean, t std
+    bool cond_graph = true;                    // coupled step as a graph WHILE node (else a host loop)
     int tune_tk = 64;         // windowed helsolve tile height (autotuned per grid size)
     int tune_bn = 128;        // 3xTF32 GEMM tile width (autotuned per grid size)
     // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
     // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
     int poisson_mode = FB_POISSON_FP64;
+    int tf32_sweeps = 2;      // FP64 refinement sweeps of the precision form
     fb::SplitPlane pl_a{}, pl_a2{}, pl_zt{}, pl_z{};
     double *zs_d = nullptr, *zsinv_d = nullptr;  // S and S^-1 of zmm = S U (the transforms use U)
     fb::Tf32x3Plan plan_fwd{}, plan_bwd{};
@@ -102,7 +105,8 @@ struct fb_ctx {
     fb::I8Plan i8a{}, i8f{}, i8b{};
     bool i8_ready = false;
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
-    int step_kernels = 0;     // own kernels per captured step
+    int step_kernels = 0;     // own kernels per captured step (coupled: with one fluid solve)
+    int iter_kernels = 0;     // own kernels per fluid solve of a coupled step
     // host copies of the scalar state the reference keeps in modules
     double dt = 0, dt_o = 0, beta = 0, al = 0, ga = 0, ro = 0;
     int cur_ns = 0, cur_n = 1;
@@ -738,17 +742,22 @@ int tune_dgemm(fb_ctx *c) {
 int phcalc_tf32(fb_ctx *c) {
     const Dev &d = c->d;
     cudaStream_t st = c->stream;
+    // phi_0 = Z T^-1 Z^-1 dph into pw
     fb::launch_split_t(d.dph + d.P, d.P, d.n2m, d.n3m, c->pl_a, st, c->zsinv_d);
     fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
     fb::launch_scan_poisson(d, st);
     fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
     fb::launch_tf32x3(c->plan_bwd, c->pw + d.P, d.P, nullptr, 0, d.status, st, c->zs_d);
-    fb::launch_poisson_residual(d, c->pw, c->pl_a, st, c->zsinv_d);
-    fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
-    fb::launch_scan_poisson(d, st);
-    fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
-    fb::launch_tf32x3(c->plan_bwd, d.dph + d.P, d.P, c->pw + d.P, d.P, d.status, st, c->zs_d);
-    c->own_launches += 9;
+    // refinement sweeps: phi += Z T^-1 Z^-1 (dph - L phi); the last lands in dph
+    for (int sw = 1; sw <= c->tf32_sweeps; ++sw) {
+        const bool last = (sw == c->tf32_sweeps);
+        fb::launch_poisson_residual(d, c->pw, c->pl_a, st, c->zsinv_d);
+        fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
+        fb::launch_scan_poisson(d, st);
+        fb::launch_split_t(d.hmn, d.ldh, d.n2m, d.n3m, c->pl_a2, st);
+        fb::launch_tf32x3(c->plan_bwd, (last ? d.dph : c->pw) + d.P, d.P, c->pw + d.P, d.P, d.status, st, c->zs_d);
+    }
+    c->own_launches += 5 + 5 * c->tf32_sweeps;
     return FB_OK;
 }
 
@@ -1051,8 +1060,11 @@ void host_clock(fb_ctx *c, int nsteps) {
     for (int i = 0; i < nsteps; ++i) c->dt_o = c->dt;
 }
 
+int capture_coupled(fb_ctx *c);
+
 int capture_step(fb_ctx *c) {
     if (c->graph_exec) return FB_OK;
+    if (c->coupling != FB_COUPLING_LOOSE) return capture_coupled(c);
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     c->own_launches = 0;
     int r = enqueue_step(c, 1);
@@ -1184,8 +1196,6 @@ int fb_destroy(fb_ctx *c) {
     for (void *p : c->allocs)
         if (p) cudaFree(p);
     if (c->coef_pin) cudaFreeHost(c->coef_pin);
-    if (c->fin_h) cudaFreeHost(c->fin_h);
-    if (c->rd_h) cudaFreeHost(c->rd_h);
     if (c->coef_pini) cudaFreeHost(c->coef_pini);
     if (c->blas) cublasDestroy(c->blas);
     for (cublasLtMatrixLayout_t l : c->lt_l)
@@ -1242,204 +1252,230 @@ int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
 }
 
 int fb_last_history(fb_ctx *c, double *row);
-int fb_mlp_predict(fb_mlp *m, const float *x, int n, float *y);
+
+}  // extern "C"
 
 namespace {
 
 // ---- strong fluid-structure coupling ----------------------------------------
 // The reference couples explicitly: the fluid step sees the body where the
-// previous rigid update left it.  Here, optionally, each step iterates on the
-// body load F = (Fy, Fz, M): the markers are placed where F moves the body
-// (RK4 with the load frozen, as rigid.F90 integrates), the fluid step runs
-// from the saved start-of-step state, its loads give F', and F is relaxed
-// towards F' with Aitken's dynamic factor until the free coordinate's load
-// changes by at most tol * max(1, |F'|).  The accepted step commits the body
-// with F' exactly as the loose step would.
+// previous rigid update left it.  Optionally each step iterates on the body
+// load instead (couple.cu: device-side initial guess, restore, trial
+// placement, fluid step, loads, Aitken update, accept), either as a CUDA
+// graph WHILE node whose condition the update kernel sets -- no host
+// synchronisation inside the step -- or, where such a graph cannot be
+// built, as a host loop over the same kernels.
 
-constexpr int kPredIn = 27, kPredOut = 2, kPredDepth = 8;
+constexpr int kNoConditionalGraph = -1;
 
-int snap_setup(fb_ctx *c) {
-    if (c->snap) return FB_OK;
+// the saved state (the fluid step's inputs that a trial step overwrites) and
+// the device structures of the iteration
+int couple_alloc(fb_ctx *c) {
+    if (c->cpl) return FB_OK;
     Dev &d = c->d;
-    const size_t nf = static_cast<size_t>(d.NK) * d.P, nb = static_cast<size_t>(d.n2) + 2;
-    c->snap_fields = {{d.q2, nf}, {d.q3, nf}, {d.pr, nf}, {d.ru2, nf}, {d.ru3, nf},
-                      {d.qb2s, nb}, {d.qb2n, nb}, {d.dqb2s, nb}, {d.dqb2n, nb}, {d.qb3s, nb},
-                      {d.qb3n, nb}, {d.dqb3s, nb}, {d.dqb3n, nb}, {d.dq2x2o, nb}, {d.dq3x2o, nb},
-                      {d.scal, static_cast<size_t>(fb::S_COUNT)}};
-    const size_t nm = c->hc.lmcc.size();
-    c->snap_body = {{d.lmcc, nm}, {d.lmvel, nm}, {d.lmacc, nm}, {d.lmnor, nm},
-                    {d.vert, c->hc.vert.size()}, {d.rigid, 18}};
-    size_t total = 0;
-    for (auto &f : c->snap_fields) total += f.second;
-    for (auto &f : c->snap_body) total += f.second;
+    const long nf = static_cast<long>(d.NK) * d.P, nb = static_cast<long>(d.n2) + 2;
+    fb::SnapList &l = c->snapl;
+    std::memset(static_cast<void *>(&l), 0, sizeof(l));
+    auto add = [&](double *a, long n) {
+        l.arr[l.n] = a;
+        l.len[l.n] = n;
+        ++l.n;
+    };
+    for (double *f : {d.q2, d.q3, d.pr, d.ru2, d.ru3}) add(f, nf);
+    for (double *b : {d.qb2s, d.qb2n, d.dqb2s, d.dqb2n, d.qb3s, d.qb3n, d.dqb3s, d.dqb3n, d.dq2x2o, d.dq3x2o})
+        add(b, nb);
+    add(d.scal, fb::S_COUNT);
+    l.nfield = l.n;
+    const long nm = static_cast<long>(c->hc.lmcc.size());
+    for (double *m : {d.lmcc, d.lmvel, d.lmacc, d.lmnor}) add(m, nm);
+    add(d.vert, static_cast<long>(c->hc.vert.size()));
+    add(d.rigid, 18);
+    long total = 0;
+    for (int i = 0; i < l.n; ++i) {
+        total += l.len[i];
+        c->snap_longest = std::max(c->snap_longest, l.len[i]);
+    }
     int st;
-    if ((st = dnew(c, &c->snap, total))) return st;
-    if ((st = dnew(c, &c->fin_d, 4))) return st;
-    CK(cudaMallocHost(&c->fin_h, 4 * sizeof(double)));
-    CK(cudaMallocHost(&c->rd_h, 16 * sizeof(double)));
+    if ((st = dnew(c, &c->snap, static_cast<size_t>(total)))) return st;
+    long off = 0;
+    for (int i = 0; i < l.n; ++i) {
+        l.copy[i] = c->snap + off;
+        off += l.len[i];
+    }
+    if ((st = dnew(c, &c->smp_x, static_cast<size_t>(c->smp_cap) * fb::kCplIn)) ||
+        (st = dnew(c, &c->smp_t, static_cast<size_t>(c->smp_cap) * fb::kCplOut)))
+        return st;
+    fb::Couple *cpl = nullptr;
+    if ((st = dnew(c, &cpl, 1)) || (st = dnew(c, &c->cpl_list, 1)) || (st = dnew(c, &c->snapl_d, 1))) return st;
+    l.c = cpl;
+    if ((st = h2d(c, c->cpl_list, &cpl, sizeof(cpl))) || (st = h2d(c, c->snapl_d, &l, sizeof(l)))) return st;
+    c->cpl = cpl;
     return FB_OK;
 }
 
-// copies the listed state into (save) or out of (!save) the snapshot
-int snap_copy(fb_ctx *c, bool save, bool fields, bool body) {
-    size_t off = 0;
-    for (auto &f : c->snap_fields) {
-        if (fields) {
-            double *a = c->snap + off;
-            CK(cudaMemcpyAsync(save ? a : f.first, save ? f.first : a, f.second * sizeof(double),
-                               cudaMemcpyDeviceToDevice, c->stream));
-        }
-        off += f.second;
+// reads the device iteration state, lets fn change it, writes it back
+template <class F>
+int couple_edit(fb_ctx *c, F fn) {
+    fb::Couple h;
+    CK(cudaMemcpyAsync(&h, c->cpl, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    fn(h);
+    return h2d(c, c->cpl, &h, sizeof(h));
+}
+
+double *couple_fin(fb_ctx *c) {
+    return reinterpret_cast<double *>(reinterpret_cast<char *>(c->cpl) + offsetof(fb::Couple, fin));
+}
+
+// the flag that gates a coupled case's grouped launches (null: loose case)
+const int *couple_gate(const fb_ctx *c) {
+    if (c->coupling == FB_COUPLING_LOOSE || !c->cpl) return nullptr;
+    return reinterpret_cast<const int *>(reinterpret_cast<const char *>(c->cpl) + offsetof(fb::Couple, active));
+}
+
+// initial guess and the saved start state
+int enqueue_couple_begin(fb_ctx *c) {
+    fb::launch_couple_begin(c->cpl_list, 1, c->stream);
+    fb::launch_snap(c->snapl_d, 1, fb::SNAP_SAVE, c->snap_longest, c->stream);
+    c->own_launches += 2;
+    return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+}
+
+// one fluid solve of the iteration (restore, trial placement, fluid step,
+// loads at the trial position, update); set_cond: write the WHILE condition
+int enqueue_couple_iter(fb_ctx *c, int ns, cudaGraphConditionalHandle h, int set_cond) {
+    fb::launch_snap(c->snapl_d, 1, fb::SNAP_RESTORE_LOOP, c->snap_longest, c->stream);
+    fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_PLACE, couple_fin(c));
+    c->own_launches += 2;
+    int r = enqueue_fluid(c, ns);
+    if (r) return r;
+    fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_FORCES, nullptr);
+    fb::launch_couple_update(c->cpl_list, 1, h, set_cond, nullptr, c->stream);
+    c->own_launches += 2;
+    return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+}
+
+// accept: body back to the start of the step, commit with the fluid's load,
+// record the step for the predictors
+int enqueue_couple_end(fb_ctx *c) {
+    fb::launch_snap(c->snapl_d, 1, fb::SNAP_RESTORE_BODY, c->snap_longest, c->stream);
+    fb::launch_couple_accept(c->cpl_list, 1, c->stream);
+    fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_COMMIT, couple_fin(c));
+    fb::launch_couple_record(c->cpl_list, 1, c->stream);
+    c->own_launches += 4;
+    if (cudaGetLastError() != cudaSuccess) return FB_ERR_CUDA;
+    return enqueue_report(c);
+}
+
+// the coupled step as one graph: begin -> WHILE(any iterating){iteration} -> end
+int capture_coupled(fb_ctx *c) {
+    cudaGraph_t G = nullptr, ga = nullptr, gb = nullptr, gd = nullptr;
+    int r = FB_OK;
+    auto cap = [&](cudaGraph_t *out, auto fn) -> int {
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
+        const int rr = fn();
+        const cudaError_t e = cudaStreamEndCapture(c->stream, out);
+        return rr ? rr : (e == cudaSuccess ? FB_OK : FB_ERR_CUDA);
+    };
+    auto cleanup = [&] {
+        for (cudaGraph_t g : {ga, gb, gd, G})
+            if (g) cudaGraphDestroy(g);
+    };
+    cudaGraphConditionalHandle h{};
+    if (cudaGraphCreate(&G, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&h, G, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return kNoConditionalGraph;
     }
-    for (auto &f : c->snap_body) {
-        if (body) {
-            double *a = c->snap + off;
-            CK(cudaMemcpyAsync(save ? a : f.first, save ? f.first : a, f.second * sizeof(double),
-                               cudaMemcpyDeviceToDevice, c->stream));
-        }
-        off += f.second;
+    c->own_launches = 0;
+    if ((r = cap(&ga, [&] { return enqueue_couple_begin(c); }))) {
+        cleanup();
+        return r;
     }
+    const int k_begin = c->own_launches;
+    if ((r = cap(&gb, [&] { return enqueue_couple_iter(c, 1, h, 1); }))) {
+        cleanup();
+        return r;
+    }
+    const int k_iter = c->own_launches - k_begin;
+    if ((r = cap(&gd, [&] { return enqueue_couple_end(c); }))) {
+        cleanup();
+        return r;
+    }
+    c->step_kernels = c->own_launches;   // begin, one fluid solve, end
+    c->iter_kernels = k_iter;
+    cudaGraphNode_t na = nullptr, nc = nullptr, nb = nullptr, nd = nullptr;
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    bool ok = cudaGraphAddChildGraphNode(&na, G, nullptr, 0, ga) == cudaSuccess &&
+              cudaGraphAddNode(&nc, G, &na, 1, &p) == cudaSuccess &&
+              cudaGraphAddChildGraphNode(&nb, p.conditional.phGraph_out[0], nullptr, 0, gb) == cudaSuccess &&
+              cudaGraphAddChildGraphNode(&nd, G, &nc, 1, gd) == cudaSuccess;
+    if (ok) ok = cudaGraphInstantiate(&c->graph_exec, G, 0) == cudaSuccess;
+    for (cudaGraph_t g : {ga, gb, gd}) cudaGraphDestroy(g);
+    ga = gb = gd = nullptr;
+    if (!ok) {
+        cudaGetLastError();
+        c->graph_exec = nullptr;
+        cleanup();
+        return kNoConditionalGraph;
+    }
+    c->graph = G;
     return FB_OK;
 }
 
-// features of the learned predictor for the free coordinate q: the last 8
-// displacements, velocities and loads encoded as increments between
-// consecutive steps (newest first), then Re, mass (or inertia) ratio and
-// reduced velocity; needs 9 converged steps
-bool fsi_features(const fb_ctx *c, float *x) {
-    const size_t n = c->hist_p.size();
-    if (n < static_cast<size_t>(kPredDepth) + 1) return false;
-    const int q = c->free_dof;
-    for (int i = 0; i < kPredDepth; ++i) {
-        x[i] = static_cast<float>(c->hist_p[n - 1 - i][q] - c->hist_p[n - 2 - i][q]);
-        x[kPredDepth + i] = static_cast<float>(c->hist_v[n - 1 - i][q] - c->hist_v[n - 2 - i][q]);
-        x[2 * kPredDepth + i] = static_cast<float>(c->hist_f[n - 1 - i][q] - c->hist_f[n - 2 - i][q]);
-    }
-    const fb::Deck &dk = c->hc.deck;
-    const double mass = dk.rbden * (q == 2 ? dk.rba[1] : dk.rba[0]);
-    const double kq = (q == 0) ? dk.kk[0] : (q == 1 ? dk.kk[1] : dk.kk[2]);
-    x[24] = static_cast<float>(1.0 / dk.visc);
-    x[25] = static_cast<float>(dk.rbden);
-    x[26] = static_cast<float>(kq > 0.0 ? 2.0 * M_PI * std::sqrt(mass / kq) : 0.0);
-    return true;
-}
-
-// initial guess of the coupling iteration
-void predict_load(fb_ctx *c, double F[3]) {
-    const size_t n = c->hist_f.size();
-    for (int i = 0; i < 3; ++i) {
-        if (n >= 2) F[i] = 2.0 * c->hist_f[n - 1][static_cast<size_t>(i)] - c->hist_f[n - 2][static_cast<size_t>(i)];
-        else if (n == 1) F[i] = c->hist_f[0][static_cast<size_t>(i)];
-        else F[i] = 0.0;
-    }
-    if (c->coupling != FB_COUPLING_LEARNED || !c->mlp) return;
-    float x[kPredIn], y[kPredOut];
-    if (!fsi_features(c, x)) return;
-    const float *nm = c->mlp_norm.data();
-    for (int i = 0; i < kPredIn; ++i) x[i] = (x[i] - nm[i]) / nm[kPredIn + i];
-    if (fb_mlp_predict(c->mlp, x, 1, y) != FB_OK) return;
-    // the network predicts the correction to the linear extrapolation above
-    const double dF = static_cast<double>(y[1] * nm[2 * kPredIn + kPredOut + 1] + nm[2 * kPredIn + 1]);
-    F[c->free_dof] += dF;
-}
-
-int coupled_step(fb_ctx *c, int ns) {
+// the same step with the iteration driven from the host (one read of the
+// device flag per fluid solve): the first Adams-Bashforth step, and devices
+// where the conditional graph is not available
+int coupled_step_host(fb_ctx *c, int ns) {
     int r;
-    if ((r = snap_setup(c))) return r;
-    if ((r = snap_copy(c, true, true, true))) return r;
-    double F[3], Ff[3] = {0, 0, 0}, res_prev[3] = {0, 0, 0}, omega = c->omega0;
-    predict_load(c, F);
-    const int q = c->free_dof;
-    int it = 0;
-    bool conv = false;
-    for (; it < c->cmaxit && !conv; ++it) {
-        if (it > 0 && (r = snap_copy(c, false, true, true))) return r;
-        for (int i = 0; i < 3; ++i) c->fin_h[i] = F[i];
-        c->fin_h[3] = 0.0;
-        CK(cudaMemcpyAsync(c->fin_d, c->fin_h, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_PLACE, c->fin_d);
-        if ((r = enqueue_fluid(c, ns))) return r;
-        fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_FORCES, nullptr);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(c->rd_h, c->d.forces + 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        int status = 0;
-        if ((r = read_status(c, &status))) return r;
-        if (status) return status;
-        double res[3];
-        for (int i = 0; i < 3; ++i) {
-            Ff[i] = c->rd_h[i];
-            res[i] = Ff[i] - F[i];
-        }
-        if (it == 0) c->stat_res0 += std::fabs(res[q]) / std::max(1.0, std::fabs(Ff[q]));
-        conv = std::fabs(res[q]) <= c->ctol * std::max(1.0, std::fabs(Ff[q]));
-        if (conv) break;
-        if (it > 0) {   // Aitken's factor from the free coordinate's residuals
-            const double dr = res[q] - res_prev[q];
-            if (dr != 0.0) omega = -omega * res_prev[q] / dr;
-        }
-        for (int i = 0; i < 3; ++i) {
-            F[i] = F[i] + omega * res[i];
-            res_prev[i] = res[i];
-        }
+    if ((r = enqueue_couple_begin(c))) return r;
+    for (int it = 0; it < c->cmaxit; ++it) {
+        if ((r = enqueue_couple_iter(c, ns, cudaGraphConditionalHandle{}, 0))) return r;
+        int active = 0;
+        CK(cudaMemcpyAsync(&active, reinterpret_cast<char *>(c->cpl) + offsetof(fb::Couple, active), sizeof(int),
+                           cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (!active) break;
     }
-    const int solves = conv ? it + 1 : it;
-    // accept: body back to the start of the step, then the loose update with F'
-    if ((r = snap_copy(c, false, false, true))) return r;
-    for (int i = 0; i < 3; ++i) c->fin_h[i] = Ff[i];
-    c->fin_h[3] = static_cast<double>(solves);
-    CK(cudaMemcpyAsync(c->fin_d, c->fin_h, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    // the loads of the accepted fluid step are those F' came from
-    CK(cudaMemcpyAsync(c->d.forces + 1, c->fin_d, 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    fb::launch_rigid(c->d, c->hist_cap, c->stream, fb::RIGID_COMMIT, c->fin_d);
-    if ((r = enqueue_report(c))) return r;
-    CK(cudaMemcpyAsync(c->rd_h, c->d.rigid, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    int status = 0;
-    if ((r = read_status(c, &status))) return r;
-    // features of the step just converged, then its targets, for training
-    float x[kPredIn];
-    const bool have_x = fsi_features(c, x);
-    std::array<double, 3> p{c->rd_h[0], c->rd_h[1], c->rd_h[2]}, v{c->rd_h[3], c->rd_h[4], c->rd_h[5]},
-        f{Ff[0], Ff[1], Ff[2]};
-    if (have_x) {   // targets: corrections to the linear extrapolations of p and F
-        const size_t n = c->hist_p.size();
-        c->samples_x.insert(c->samples_x.end(), x, x + kPredIn);
-        c->samples_t.push_back(static_cast<float>(p[q] - (2.0 * c->hist_p[n - 1][q] - c->hist_p[n - 2][q])));
-        c->samples_t.push_back(static_cast<float>(f[q] - (2.0 * c->hist_f[n - 1][q] - c->hist_f[n - 2][q])));
-    }
-    c->hist_p.push_back(p);
-    c->hist_v.push_back(v);
-    c->hist_f.push_back(f);
-    if (c->hist_p.size() > 64) {
-        c->hist_p.erase(c->hist_p.begin());
-        c->hist_v.erase(c->hist_v.begin());
-        c->hist_f.erase(c->hist_f.begin());
-    }
-    c->stat_steps += 1;
-    c->stat_solves += solves;
-    if (!conv) c->stat_maxit += 1;
-    return status;
+    return enqueue_couple_end(c);
 }
 
 }  // namespace
+
+extern "C" {
 
 int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
     if (!c || nsteps < 0) return FB_ERR_STATE;
     if (!c->d.nlm) return FB_ERR_UNSUPPORTED;
     int r, status = 0, done = 0;
-    if (c->coupling != FB_COUPLING_LOOSE) {   // iterated steps: eager launches
+    if (c->coupling != FB_COUPLING_LOOSE && c->cond_graph && !c->graph_exec) {
+        r = capture_step(c);
+        if (r == kNoConditionalGraph) c->cond_graph = false;
+        else if (r) return r;
+    }
+    const bool host_loop = c->coupling != FB_COUPLING_LOOSE && !c->cond_graph;
+    if (host_loop || (c->coupling != FB_COUPLING_LOOSE && c->hc.deck.nsst == 1 && ns0 == 0)) {
+        // coupled steps driven from the host: all of them, or the first
+        // Adams-Bashforth step (its own coefficients) before the graph
         c->last_ms = 0.0;
-        for (; done < nsteps; ++done) {
+        for (; done < nsteps && (host_loop || done < 1); ++done) {
             CK(cudaEventRecord(c->ev0, c->stream));
-            if ((r = coupled_step(c, ns0 + done))) return r;
+            if ((r = coupled_step_host(c, ns0 + done))) return r;
             CK(cudaEventRecord(c->ev1, c->stream));
-            CK(cudaEventSynchronize(c->ev1));
+            if ((r = read_status(c, &status))) return r;
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
             c->last_ms += ms;
             if (hist && (r = fb_last_history(c, hist + static_cast<size_t>(done) * FB_HIST_COLS))) return r;
             host_clock(c, 1);
+            if (status) return status;
         }
-        return FB_OK;
+        if (done == nsteps) return FB_OK;
     }
     if (c->vardt) {   // dt changes every step: eager launches, no captured graph
         c->last_ms = 0.0;
@@ -1458,7 +1494,7 @@ int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
         return FB_OK;
     }
     // the first Adams-Bashforth step has its own coefficients: run it eagerly
-    if (c->hc.deck.nsst == 1 && ns0 == 0 && nsteps > 0) {
+    if (c->coupling == FB_COUPLING_LOOSE && c->hc.deck.nsst == 1 && ns0 == 0 && nsteps > 0) {
         CK(cudaEventRecord(c->ev0, c->stream));
         if ((r = enqueue_step(c, 0))) return r;
         CK(cudaEventRecord(c->ev1, c->stream));
@@ -1476,7 +1512,7 @@ int fb_advance(fb_ctx *c, int ns0, int nsteps, double *hist) {
         host_clock(c, 1);
         if (status) return status;
         done = 1;
-    } else {
+    } else if (done == 0) {
         c->last_ms = 0.0;
     }
     if ((r = capture_step(c))) return r;
@@ -1943,6 +1979,17 @@ int fb_set_poisson(fb_ctx *c, int mode) {
     return FB_OK;
 }
 
+int fb_set_refinement(fb_ctx *c, int sweeps) {
+    if (!c || sweeps < 1 || sweeps > 4) return FB_ERR_STATE;
+    if (sweeps != c->tf32_sweeps) {   // the captured step no longer matches
+        CK(cudaSetDevice(c->device));
+        CK(cudaStreamSynchronize(c->stream));
+        drop_graph(c);
+        c->tf32_sweeps = sweeps;
+    }
+    return FB_OK;
+}
+
 int fb_autotune(fb_ctx *c, int32_t choice[2]);
 
 // ---- batches: independent cases advanced by one graph launch per step
@@ -1969,8 +2016,9 @@ struct BatchGroup {
     int launches = 0;           // own kernels per step
     // precision form: the products, splits and residuals of every case
     bool tf32 = false;
+    int sweeps = 1;                  // refinement sweeps (one value per group)
     fb::Tf32x3Plan plan_fwd{}, plan_bwd{};   // launch geometry (the first case's plans)
-    fb::GemmTask *gt = nullptr;      // 3 x n: forward -> hmn; backward -> pw; backward -> dph (+ pw)
+    fb::GemmTask *gt = nullptr;      // 4 x n: forward -> hmn; backward -> pw; -> dph (+ pw); -> pw (+ pw)
     fb::SplitTask *sp = nullptr;     // 2 x n: dph S^-1 -> a; hmn -> a2
     fb::ResidualTask *rt = nullptr;  // n: pw -> a (S^-1)
     // FP64 transforms on the INT8 tensor cores: digit cuts and products of every case
@@ -1993,7 +2041,17 @@ struct fb_batch {
     cudaGraphExec_t exec = nullptr;
     int *status_h = nullptr;   // pinned: one status per case
     double last_ms = 0.0;
-    int launches = 0;          // own kernels per step
+    int launches = 0;          // own kernels per step (coupled: with one fluid solve)
+    // strongly coupled cases: one iteration over the whole batch, converged
+    // cases gated out of every launch until all have converged
+    bool coupled = false;
+    fb::Couple **cpls = nullptr;    // device: the cases' iteration states
+    fb::SnapList *snaps = nullptr;  // device: the cases' saved states
+    long snap_longest = 0;
+    int maxit = 1;                  // the largest iteration limit of the cases
+    int *any_d = nullptr;           // device flag of the host-driven loop
+    bool cond_graph = true;
+    cudaGraphExec_t exec_a = nullptr, exec_b = nullptr, exec_d = nullptr;   // host-driven loop's parts
 };
 
 namespace {
@@ -2028,12 +2086,12 @@ bool groupable(const fb_ctx *c) {
 }
 
 // cases that may share launches: same launch geometry and options
-using GroupKey = std::array<int, 11>;
+using GroupKey = std::array<int, 12>;
 GroupKey group_key(const fb_ctx *c) {
     const Dev &d = c->d;
     const bool tf = c->poisson_mode == FB_POISSON_TF32X3;
     return {d.n2, d.n3, d.nlm, d.P, d.ldh, d.NK, c->sub[0].win_tk, c->hc.deck.cbody ? 1 : 0,
-            (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0};
+            (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0, tf ? c->tf32_sweeps : 0};
 }
 
 // The product tile of a group's grouped launches, timed over the whole group
@@ -2156,11 +2214,13 @@ int group_setup_i8(BatchGroup *bg) {
         const Dev &d = c->d;
         const size_t k = static_cast<size_t>(i), m = static_cast<size_t>(n);
         const fb::I8Plan &a = c->i8a;
-        sp[k] = {d.dph + d.P, d.P, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad};
-        sp[m + k] = {d.hmn, d.ldh, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad};
-        gt[k] = {a.map, c->i8f.map, fb::I8Out{d.hmn, d.ldh, a.scale, c->i8f.scale, d.n2m, d.n3m}, d.n3m, d.status};
+        const int *gate = couple_gate(c);
+        sp[k] = {d.dph + d.P, d.P, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad, gate};
+        sp[m + k] = {d.hmn, d.ldh, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad, gate};
+        gt[k] = {a.map, c->i8f.map, fb::I8Out{d.hmn, d.ldh, a.scale, c->i8f.scale, d.n2m, d.n3m}, d.n3m, d.status,
+                 gate};
         gt[m + k] = {a.map, c->i8b.map, fb::I8Out{d.dph + d.P, d.P, a.scale, c->i8b.scale, d.n2m, d.n3m}, d.n3m,
-                     d.status};
+                     d.status, gate};
     }
     CK(cudaMalloc(&bg->i8s, sizeof(fb::I8SplitTask) * sp.size()));
     CK(cudaMalloc(&bg->i8t, sizeof(fb::I8Task) * gt.size()));
@@ -2177,7 +2237,7 @@ int group_setup_tf32(BatchGroup *bg) {
     const int n = static_cast<int>(bg->members.size());
     int bn = 0, r;
     if ((r = group_gemm_tile(bg, &bn))) return r;
-    std::vector<fb::GemmTask> gt(static_cast<size_t>(3 * n));
+    std::vector<fb::GemmTask> gt(static_cast<size_t>(4 * n));
     std::vector<fb::SplitTask> sp(static_cast<size_t>(2 * n));
     std::vector<fb::ResidualTask> rt(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) {
@@ -2193,11 +2253,13 @@ int group_setup_tf32(BatchGroup *bg) {
             bg->plan_fwd = pf;
             bg->plan_bwd = pb;
         }
-        gt[k] = {pf, fb::GemmOut{d.hmn, d.ldh, nullptr, 0, nullptr, M, N}, d.status};
-        gt[m + k] = {pb, fb::GemmOut{c->pw + d.P, d.P, nullptr, 0, c->zs_d, M, N}, d.status};
-        gt[2 * m + k] = {pb, fb::GemmOut{d.dph + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status};
-        sp[k] = {d.dph + d.P, d.P, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
-        sp[m + k] = {d.hmn, d.ldh, c->pl_a2.hi, c->pl_a2.lo, c->pl_a2.ld, nullptr};
+        const int *gate = couple_gate(c);
+        gt[k] = {pf, fb::GemmOut{d.hmn, d.ldh, nullptr, 0, nullptr, M, N}, d.status, gate};
+        gt[m + k] = {pb, fb::GemmOut{c->pw + d.P, d.P, nullptr, 0, c->zs_d, M, N}, d.status, gate};
+        gt[2 * m + k] = {pb, fb::GemmOut{d.dph + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status, gate};
+        gt[3 * m + k] = {pb, fb::GemmOut{c->pw + d.P, d.P, c->pw + d.P, d.P, c->zs_d, M, N}, d.status, gate};
+        sp[k] = {d.dph + d.P, d.P, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d, gate};
+        sp[m + k] = {d.hmn, d.ldh, c->pl_a2.hi, c->pl_a2.lo, c->pl_a2.ld, nullptr, gate};
         rt[k] = {c->pw, c->pl_a.hi, c->pl_a.lo, c->pl_a.ld, c->zsinv_d};
     }
     CK(cudaMalloc(&bg->gt, sizeof(fb::GemmTask) * gt.size()));
@@ -2208,6 +2270,7 @@ int group_setup_tf32(BatchGroup *bg) {
     CK(cudaMemcpyAsync(bg->rt, rt.data(), sizeof(fb::ResidualTask) * rt.size(), cudaMemcpyHostToDevice, bg->st));
     CK(cudaStreamSynchronize(bg->st));
     bg->tf32 = true;
+    bg->sweeps = bg->members[0]->tf32_sweeps;
     return FB_OK;
 }
 
@@ -2237,6 +2300,8 @@ int group_setup(BatchGroup *bg) {
             g.win_kz[k] = std::max(g.win_kz[k], c->sub[k].win_z);
         }
         gc.hist_rows = c->hist_cap;
+        gc.gate = couple_gate(c);
+        gc.fin = c->coupling != FB_COUPLING_LOOSE ? couple_fin(const_cast<fb_ctx *>(c)) : nullptr;
         const Dev &d = c->d;
         ptr[static_cast<size_t>(0 * n + i)] = d.dph + d.P;
         ptr[static_cast<size_t>(1 * n + i)] = c->zmmt;
@@ -2265,14 +2330,13 @@ int group_setup(BatchGroup *bg) {
     return FB_OK;
 }
 
-// one step of a group (fluid_tsch.F90:30-182 + loads + rigid, in the order
-// enqueue_fluid and enqueue_step use), enqueued on the group's stream
-int enqueue_group(BatchGroup *bg) {
+// the fluid step of a group (fluid_tsch.F90:30-182 + loads, in the order
+// enqueue_fluid uses), enqueued on the group's stream; k counts launches
+int enqueue_group_fluid(BatchGroup *bg, int &k) {
     const fb::Group &g = bg->g;
     const Dev &d = g.rep;
     const int n = g.n;
     cudaStream_t st = bg->st;
-    int k = 0;
     CK(cudaEventRecord(bg->fork, st));
     CK(cudaStreamWaitEvent(bg->side, bg->fork, 0));
     fb::glaunch_marker_setup(g, bg->side);
@@ -2298,12 +2362,14 @@ int enqueue_group(BatchGroup *bg) {
             fb::glaunch_scan_poisson(g, st);
             fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
             fb::launch_tf32x3_group(bg->gt + n, bg->plan_bwd, n, st);
-            fb::launch_poisson_residual_group(g, bg->rt, st);
-            fb::launch_tf32x3_group(bg->gt, bg->plan_fwd, n, st);
-            fb::glaunch_scan_poisson(g, st);
-            fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
-            fb::launch_tf32x3_group(bg->gt + 2 * n, bg->plan_bwd, n, st);
-            k += 10;
+            for (int sw = 1; sw <= bg->sweeps; ++sw) {   // the last sweep lands in dph
+                fb::launch_poisson_residual_group(g, bg->rt, st);
+                fb::launch_tf32x3_group(bg->gt, bg->plan_fwd, n, st);
+                fb::glaunch_scan_poisson(g, st);
+                fb::launch_split_t_group(bg->sp + n, d.n2m, d.n3m, n, st);
+                fb::launch_tf32x3_group(bg->gt + (sw == bg->sweeps ? 2 : 3) * n, bg->plan_bwd, n, st);
+            }
+            k += 5 + 5 * bg->sweeps;
         } else if (bg->i8) {   // phcalc_i8's launches, each over the whole group
             fb::launch_i8_split_group(bg->i8s, bg->i8rep, d.n2m, d.n3m, n, st);
             fb::launch_i8x8_group(bg->i8t, d.n2m, d.n3m, n, st);
@@ -2329,10 +2395,19 @@ int enqueue_group(BatchGroup *bg) {
         fb::glaunch_loads(g, st);
         k += 2;
     }
-    fb::glaunch_rigid(g, st);
+    CK(cudaGetLastError());
+    return FB_OK;
+}
+
+// one loose step of a group: the fluid step, then rigid (rigid.F90:4-138)
+int enqueue_group(BatchGroup *bg) {
+    int k = 0;
+    int r = enqueue_group_fluid(bg, k);
+    if (r) return r;
+    fb::glaunch_rigid(bg->g, bg->st);
     k += 1;
     if (bg->report) {
-        fb::glaunch_diag(g, st);
+        fb::glaunch_diag(bg->g, bg->st);
         k += 1;
     }
     CK(cudaGetLastError());
@@ -2354,10 +2429,153 @@ int fb_batch_destroy(fb_batch *b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->status_h) cudaFreeHost(b->status_h);
+    for (cudaGraphExec_t e : {b->exec_a, b->exec_b, b->exec_d})
+        if (e) cudaGraphExecDestroy(e);
+    if (b->cpls) cudaFree(b->cpls);
+    if (b->snaps) cudaFree(b->snaps);
+    if (b->any_d) cudaFree(b->any_d);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return FB_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+// The parts of one strongly coupled step of a batch: begin (initial guesses,
+// saved states), one fluid solve of every case still iterating (converged
+// cases sit out every launch), end (accept, commit, record).
+int enqueue_batch_begin(fb_batch *b) {
+    const int n = static_cast<int>(b->ctx.size());
+    fb::launch_couple_begin(b->cpls, n, b->stream);
+    fb::launch_snap(b->snaps, n, fb::SNAP_SAVE, b->snap_longest, b->stream);
+    CK(cudaGetLastError());
+    return FB_OK;
+}
+
+// forks every group off the batch stream, runs fn(group) on it, joins back
+template <class F>
+int over_groups(fb_batch *b, F fn) {
+    CK(cudaEventRecord(b->fork, b->stream));
+    for (BatchGroup *bg : b->groups) {
+        CK(cudaStreamWaitEvent(bg->st, b->fork, 0));
+        int r = fn(bg);
+        if (r) return r;
+        CK(cudaEventRecord(bg->done, bg->st));
+        CK(cudaStreamWaitEvent(b->stream, bg->done, 0));
+    }
+    return FB_OK;
+}
+
+int enqueue_batch_iter(fb_batch *b, cudaGraphConditionalHandle h, int set_cond, int *launches) {
+    const int n = static_cast<int>(b->ctx.size());
+    fb::launch_snap(b->snaps, n, fb::SNAP_RESTORE_LOOP, b->snap_longest, b->stream);
+    int k = 2;
+    int r = over_groups(b, [&](BatchGroup *bg) -> int {
+        fb::glaunch_rigid(bg->g, bg->st, fb::RIGID_PLACE);
+        int kk = 2;
+        const int rr = enqueue_group_fluid(bg, kk);
+        fb::glaunch_rigid(bg->g, bg->st, fb::RIGID_FORCES);
+        k += kk;
+        return rr;
+    });
+    if (r) return r;
+    fb::launch_couple_update(b->cpls, n, h, set_cond, set_cond ? nullptr : b->any_d, b->stream);
+    CK(cudaGetLastError());
+    if (launches) *launches = k;
+    return FB_OK;
+}
+
+int enqueue_batch_end(fb_batch *b, int *launches) {
+    const int n = static_cast<int>(b->ctx.size());
+    fb::launch_snap(b->snaps, n, fb::SNAP_RESTORE_BODY, b->snap_longest, b->stream);
+    fb::launch_couple_accept(b->cpls, n, b->stream);
+    int k = 3;
+    int r = over_groups(b, [&](BatchGroup *bg) -> int {
+        fb::glaunch_rigid(bg->g, bg->st, fb::RIGID_COMMIT);
+        k += 1;
+        return FB_OK;
+    });
+    if (r) return r;
+    fb::launch_couple_record(b->cpls, n, b->stream);
+    r = over_groups(b, [&](BatchGroup *bg) -> int {
+        if (bg->report) {
+            fb::glaunch_diag(bg->g, bg->st);
+            k += 1;
+        }
+        return FB_OK;
+    });
+    if (r) return r;
+    CK(cudaGetLastError());
+    if (launches) *launches = k;
+    return FB_OK;
+}
+
+// the coupled batch step: one graph with a WHILE node around the fluid solves
+// (or, without conditional graphs, three graphs that the host loop replays)
+int capture_batch_coupled(fb_batch *b) {
+    auto cap = [&](cudaGraph_t *out, auto fn) -> int {
+        if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
+        const int rr = fn();
+        const cudaError_t e = cudaStreamEndCapture(b->stream, out);
+        return rr ? rr : (e == cudaSuccess ? FB_OK : FB_ERR_CUDA);
+    };
+    cudaGraph_t G = nullptr, ga = nullptr, gb = nullptr, gd = nullptr;
+    auto cleanup = [&] {
+        for (cudaGraph_t g : {ga, gb, gd, G})
+            if (g) cudaGraphDestroy(g);
+    };
+    int r, ki = 0, ke = 0;
+    cudaGraphConditionalHandle h{};
+    b->cond_graph = cudaGraphCreate(&G, 0) == cudaSuccess &&
+                    cudaGraphConditionalHandleCreate(&h, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGetLastError();
+    if ((r = cap(&ga, [&] { return enqueue_batch_begin(b); })) ||
+        (r = cap(&gb, [&] { return enqueue_batch_iter(b, h, b->cond_graph ? 1 : 0, &ki); })) ||
+        (r = cap(&gd, [&] { return enqueue_batch_end(b, &ke); }))) {
+        cleanup();
+        return r;
+    }
+    b->launches = 2 + ki + ke;
+    if (b->cond_graph) {
+        cudaGraphNode_t na = nullptr, nc = nullptr, nb = nullptr, nd = nullptr;
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        b->cond_graph = cudaGraphAddChildGraphNode(&na, G, nullptr, 0, ga) == cudaSuccess &&
+                        cudaGraphAddNode(&nc, G, &na, 1, &p) == cudaSuccess &&
+                        cudaGraphAddChildGraphNode(&nb, p.conditional.phGraph_out[0], nullptr, 0, gb) == cudaSuccess &&
+                        cudaGraphAddChildGraphNode(&nd, G, &nc, 1, gd) == cudaSuccess &&
+                        cudaGraphInstantiate(&b->exec, G, 0) == cudaSuccess;
+        cudaGetLastError();
+        if (b->cond_graph) {
+            b->graph = G;
+            G = nullptr;
+            cleanup();
+            return FB_OK;
+        }
+        b->exec = nullptr;
+        // the iteration graph was captured to set the condition: capture it again
+        cudaGraphDestroy(gb);
+        gb = nullptr;
+        if ((r = cap(&gb, [&] { return enqueue_batch_iter(b, h, 0, nullptr); }))) {
+            cleanup();
+            return r;
+        }
+    }
+    const bool ok = cudaGraphInstantiate(&b->exec_a, ga, 0) == cudaSuccess &&
+                    cudaGraphInstantiate(&b->exec_b, gb, 0) == cudaSuccess &&
+                    cudaGraphInstantiate(&b->exec_d, gd, 0) == cudaSuccess;
+    cleanup();
+    return ok ? FB_OK : FB_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
 
 int fb_batch_create_mode(fb_ctx *const *ctxs, int n, int mode, fb_batch **out) {
     if (!ctxs || n < 1 || !out || (mode != FB_BATCH_GROUPED && mode != FB_BATCH_GRAPH)) return FB_ERR_STATE;
@@ -2382,6 +2600,20 @@ int fb_batch_create_mode(fb_ctx *const *ctxs, int n, int mode, fb_batch **out) {
                 return FB_ERR_STATE;
             }
         b->ctx.push_back(c);
+    }
+    // strongly coupled cases iterate together: all of a batch or none, every
+    // case in a grouped launch with a transform form whose launches can sit
+    // a converged case out (the library's own tensor-core kernels)
+    int ncoupled = 0;
+    for (fb_ctx *c : b->ctx) ncoupled += (c->coupling != FB_COUPLING_LOOSE) ? 1 : 0;
+    if (ncoupled) {
+        bool ok = ncoupled == n && mode == FB_BATCH_GROUPED;
+        for (fb_ctx *c : b->ctx) ok = ok && c->poisson_mode != FB_POISSON_FP64;
+        if (!ok) {
+            delete b;
+            return FB_ERR_UNSUPPORTED;
+        }
+        b->coupled = true;
     }
     int r = FB_OK;
     auto fail = [&](int code) {
@@ -2414,8 +2646,29 @@ int fb_batch_create_mode(fb_ctx *const *ctxs, int n, int mode, fb_batch **out) {
         }
         it->second->members.push_back(c);
     }
+    if (b->coupled && !b->singles.empty()) return fail(FB_ERR_UNSUPPORTED);   // every case grouped
     for (BatchGroup *bg : b->groups)
         if ((r = group_setup(bg))) return fail(r);
+    if (b->coupled) {
+        std::vector<fb::Couple *> cp;
+        std::vector<fb::SnapList> sl;
+        for (fb_ctx *c : b->ctx) {
+            if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(FB_ERR_CUDA);
+            cp.push_back(c->cpl);
+            sl.push_back(c->snapl);
+            b->snap_longest = std::max(b->snap_longest, c->snap_longest);
+            b->maxit = std::max(b->maxit, c->cmaxit);
+        }
+        if (cudaMalloc(&b->cpls, sizeof(fb::Couple *) * n) != cudaSuccess ||
+            cudaMalloc(&b->snaps, sizeof(fb::SnapList) * n) != cudaSuccess ||
+            cudaMalloc(&b->any_d, sizeof(int)) != cudaSuccess ||
+            cudaMemcpy(b->cpls, cp.data(), sizeof(fb::Couple *) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(b->snaps, sl.data(), sizeof(fb::SnapList) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(FB_ERR_CUDA);
+        if ((r = capture_batch_coupled(b))) return fail(r);
+        *out = b;
+        return FB_OK;
+    }
     b->done.assign(b->singles.size(), nullptr);
     for (auto &e : b->done)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(FB_ERR_CUDA);
@@ -2472,7 +2725,21 @@ int fb_batch_advance(fb_batch *b, int nsteps) {
     if (!b || nsteps < 0) return FB_ERR_STATE;
     CK(cudaSetDevice(b->device));
     CK(cudaEventRecord(b->ev0, b->stream));
-    for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(b->exec, b->stream));
+    if (b->coupled && !b->cond_graph) {   // the fluid solves driven from the host
+        for (int i = 0; i < nsteps; ++i) {
+            CK(cudaGraphLaunch(b->exec_a, b->stream));
+            for (int it = 0; it < b->maxit; ++it) {
+                CK(cudaGraphLaunch(b->exec_b, b->stream));
+                int any = 0;
+                CK(cudaMemcpyAsync(&any, b->any_d, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+                CK(cudaStreamSynchronize(b->stream));
+                if (!any) break;
+            }
+            CK(cudaGraphLaunch(b->exec_d, b->stream));
+        }
+    } else {
+        for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(b->exec, b->stream));
+    }
     CK(cudaEventRecord(b->ev1, b->stream));
     for (size_t i = 0; i < b->ctx.size(); ++i)
         CK(cudaMemcpyAsync(b->status_h + i, b->ctx[i]->d.status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
@@ -2589,60 +2856,140 @@ int fb_set_coupling(fb_ctx *c, int mode, double tol, int max_iter) {
     if (!c || mode < FB_COUPLING_LOOSE || mode > FB_COUPLING_LEARNED || !(tol > 0.0) || max_iter < 1)
         return FB_ERR_STATE;
     if (mode != FB_COUPLING_LOOSE && (c->vardt || !c->d.nlm)) return FB_ERR_UNSUPPORTED;
-    if (mode != FB_COUPLING_LOOSE && c->coupling == FB_COUPLING_LOOSE && c->hist_p.empty()) {
-        // seed the predictor's history with the steps already taken (history ring)
+    CK(cudaSetDevice(c->device));
+    if (mode == FB_COUPLING_LOOSE) {
+        if (c->coupling != FB_COUPLING_LOOSE) {   // the captured step changes
+            CK(cudaStreamSynchronize(c->stream));
+            drop_graph(c);
+        }
+        c->coupling = mode;
+        return FB_OK;
+    }
+    int st = couple_alloc(c);
+    if (st) return st;
+    const bool fresh = (c->coupling == FB_COUPLING_LOOSE);
+    // the predictor's history: the steps already taken (history ring)
+    std::vector<std::array<double, 9>> seed;
+    if (fresh) {
         double step = 0.0;
         CK(cudaMemcpyAsync(&step, c->d.scal + fb::S_STEP, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        const int done = static_cast<int>(step), take = std::min(done, std::min(64, c->hist_cap));
+        const int done = static_cast<int>(step), take = std::min(done, std::min(fb::kCplHist, c->hist_cap));
         std::vector<double> row(FB_HIST_COLS);
         for (int i = done - take; i < done; ++i) {
             CK(cudaMemcpy(row.data(), c->d.hist + static_cast<size_t>(i % c->hist_cap) * FB_HIST_COLS,
                           FB_HIST_COLS * sizeof(double), cudaMemcpyDeviceToHost));
-            c->hist_p.push_back({row[9], row[10], row[11]});
-            c->hist_v.push_back({row[12], row[13], row[14]});
-            c->hist_f.push_back({row[1], row[2], row[3]});
+            seed.push_back({row[9], row[10], row[11], row[12], row[13], row[14], row[1], row[2], row[3]});
         }
     }
-    c->coupling = mode;
-    c->ctol = tol;
-    c->cmaxit = max_iter;
     const fb::Deck &dk = c->hc.deck;
-    c->free_dof = 0;
+    int q = 0;
     for (int i = 0; i < 3; ++i)
         if (dk.rbmcon[i] == 0) {
-            c->free_dof = i;
+            q = i;
             break;
         }
+    const double mass = dk.rbden * (q == 2 ? dk.rba[1] : dk.rba[0]);
+    const double kq = dk.kk[q];
+    int nin = 0, nout = 0;
+    const float *params = c->mlp ? fb::mlp_params_device(c->mlp, &nin, &nout) : nullptr;
+    st = couple_edit(c, [&](fb::Couple &h) {
+        h.tol = tol;
+        h.omega0 = 0.5;
+        h.maxit = max_iter;
+        h.q = q;
+        h.learned = (mode == FB_COUPLING_LEARNED) ? 1 : 0;
+        h.cap = c->smp_cap;
+        h.feat_re = 1.0 / dk.visc;
+        h.feat_mr = dk.rbden;
+        h.feat_ur = kq > 0.0 ? 2.0 * M_PI * std::sqrt(mass / kq) : 0.0;
+        h.mlp = params;
+        h.norm = c->mlp_norm_d;
+        h.forces = c->d.forces;
+        h.rigid = c->d.rigid;
+        h.sx = c->smp_x;
+        h.st = c->smp_t;
+        if (fresh) {
+            h.nh = static_cast<int>(seed.size());
+            for (int i = 0; i < h.nh; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    h.hp[i][k] = seed[static_cast<size_t>(i)][k];
+                    h.hv[i][k] = seed[static_cast<size_t>(i)][3 + k];
+                    h.hf[i][k] = seed[static_cast<size_t>(i)][6 + k];
+                }
+        }
+    });
+    if (st) return st;
+    if (fresh) {   // the captured step changes
+        CK(cudaStreamSynchronize(c->stream));
+        drop_graph(c);
+    }
+    c->coupling = mode;
+    c->cmaxit = max_iter;
     return FB_OK;
 }
 
 int fb_set_predictor(fb_ctx *c, fb_mlp *m, const float *norm) {
     if (!c || (m && !norm)) return FB_ERR_STATE;
+    int nin = 0, nout = 0;
+    const float *params = m ? fb::mlp_params_device(m, &nin, &nout) : nullptr;
+    if (m && (nin != fb::kCplIn || nout != fb::kCplOut)) return FB_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    int st;
+    const size_t nn = 2 * fb::kCplIn + 2 * fb::kCplOut;
+    if (m) {
+        if (!c->mlp_norm_d && (st = dnew(c, &c->mlp_norm_d, nn))) return st;
+        if ((st = h2d(c, c->mlp_norm_d, norm, nn * sizeof(float)))) return st;
+    }
     c->mlp = m;
-    c->mlp_norm.assign(norm ? norm : nullptr, norm ? norm + 2 * 27 + 2 * 2 : nullptr);
+    if (c->cpl)
+        return couple_edit(c, [&](fb::Couple &h) {
+            h.mlp = params;
+            h.norm = m ? c->mlp_norm_d : nullptr;
+        });
     return FB_OK;
 }
 
 int fb_coupling_stats(fb_ctx *c, double out[4]) {
     if (!c || !out) return FB_ERR_STATE;
-    out[0] = c->stat_steps;
-    out[1] = c->stat_solves;
-    out[2] = c->stat_maxit;
-    out[3] = c->stat_steps > 0 ? c->stat_res0 / c->stat_steps : 0.0;
+    for (int i = 0; i < 4; ++i) out[i] = 0.0;
+    if (!c->cpl) return FB_OK;
+    fb::Couple h;
+    CK(cudaMemcpyAsync(&h, c->cpl, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out[0] = h.steps;
+    out[1] = h.solves;
+    out[2] = h.maxit_hits;
+    out[3] = h.steps > 0 ? h.res0 / h.steps : 0.0;
     return FB_OK;
 }
 
+// the samples written since the last call, oldest first (a ring of smp_cap:
+// samples older than that are lost)
 int fb_coupling_samples(fb_ctx *c, float *x, float *t, int cap, int *n) {
     if (!c || !n) return FB_ERR_STATE;
-    const int have = static_cast<int>(c->samples_t.size() / 2);
+    *n = 0;
+    if (!c->cpl) return FB_OK;
+    unsigned long long written = 0;
+    CK(cudaMemcpyAsync(&written, reinterpret_cast<char *>(c->cpl) + offsetof(fb::Couple, nsamples), sizeof(written),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const unsigned long long ring = static_cast<unsigned long long>(c->smp_cap);
+    if (written - c->smp_drained > ring) c->smp_drained = written - ring;
+    const int have = static_cast<int>(written - c->smp_drained);
     *n = have;
     if (!x || !t) return FB_OK;
-    const int m = std::min(cap, have);
-    std::memcpy(x, c->samples_x.data(), sizeof(float) * static_cast<size_t>(m) * 27);
-    std::memcpy(t, c->samples_t.data(), sizeof(float) * static_cast<size_t>(m) * 2);
-    c->samples_x.erase(c->samples_x.begin(), c->samples_x.begin() + static_cast<long>(m) * 27);
-    c->samples_t.erase(c->samples_t.begin(), c->samples_t.begin() + static_cast<long>(m) * 2);
+    const int m = std::max(0, std::min(cap, have));
+    for (int done = 0; done < m;) {   // up to the ring's end, then from its start
+        const size_t slot = static_cast<size_t>((c->smp_drained + static_cast<unsigned long long>(done)) % ring);
+        const int run = std::min(m - done, static_cast<int>(ring - slot));
+        CK(cudaMemcpy(x + static_cast<size_t>(done) * fb::kCplIn, c->smp_x + slot * fb::kCplIn,
+                      sizeof(float) * static_cast<size_t>(run) * fb::kCplIn, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t + static_cast<size_t>(done) * fb::kCplOut, c->smp_t + slot * fb::kCplOut,
+                      sizeof(float) * static_cast<size_t>(run) * fb::kCplOut, cudaMemcpyDeviceToHost));
+        done += run;
+    }
+    c->smp_drained += static_cast<unsigned long long>(m);
     *n = m;
     return FB_OK;
 }

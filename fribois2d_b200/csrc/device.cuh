@@ -84,6 +84,10 @@ struct GroupCase {
     Dev d;
     SubDev s[kMaxSub];
     int hist_rows;
+    // strongly coupled batches: the case takes part in a launch only while
+    // *gate is non-zero (null: always); fin is its trial load for k_rigid
+    const int *gate;
+    const double *fin;
 };
 
 #ifdef __CUDACC__
@@ -108,14 +112,18 @@ __device__ __forceinline__ void copy_words(const T &src, T *dst, int t, int nt) 
     unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
     for (int i = t; i < static_cast<int>(sizeof(T) / 8); i += nt) d[i] = __ldg(s + i);
 }
-__device__ __forceinline__ void stage_case(const GroupCase *__restrict__ g, Dev *sd, SubDev *ss = nullptr,
-                                           int n = 0) {
+// Returns false when the case sits out this launch (its coupling iteration
+// has converged): the whole block then returns at once.
+__device__ __forceinline__ bool stage_case(const GroupCase *__restrict__ g, Dev *sd, SubDev *ss = nullptr,
+                                           int n = 0, bool gated = true) {
     const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     const int nt = blockDim.x * blockDim.y * blockDim.z;
     copy_words(g[blockIdx.z].d, sd, t, nt);
     if (ss) copy_words(g[blockIdx.z].s[n], ss, t, nt);
     asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory");
     __syncthreads();
+    const int *gate = g[blockIdx.z].gate;   // written by earlier kernels: read after the wait
+    return !gated || !gate || *gate != 0;
 }
 #endif
 

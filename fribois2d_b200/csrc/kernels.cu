@@ -1619,14 +1619,14 @@ __global__ void __launch_bounds__(256) k_diag(Dev d, int hist_rows) {
 
 __global__ void __launch_bounds__(256) kg_cfl(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     cfl_body(d);
 }
 
 __global__ void __launch_bounds__(1024) kg_boucdq(const GroupCase *__restrict__ g, int n) {
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     boucdq_body(d, s.ga, s.ro);
 }
 
@@ -1634,43 +1634,43 @@ __global__ void __launch_bounds__(256, kNlBlocksPerSM) kg_nl_rhs(const GroupCase
     extern __shared__ __align__(16) unsigned char nl_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     nl_rhs_body(d, s.al, s.ga, s.ro, reinterpret_cast<NlTile *>(nl_smem), pend != 0);
 }
 __global__ void kg_lgrdist(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     lgrdist_body(d);
 }
 
 __global__ void kg_mls_setup(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     mls_setup_body(d);
 }
 
 __global__ void kg_spread_chains(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     spread_chains_body(d);
 }
 
 __global__ void kg_mls_interp(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     mls_interp_body(d);
 }
 
 __global__ void kg_mls_spread(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     mls_spread_body(d);
 }
 
 __global__ void kg_divg(const GroupCase *__restrict__ g, int n) {
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     divg_body(d, s.usdtal);
 }
 
@@ -1679,13 +1679,13 @@ __global__ void __launch_bounds__(256, kUpBlocksPerSM) kg_updvp_prcalc(const Gro
     extern __shared__ __align__(16) unsigned char up_smem[];
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     updvp_prcalc_body(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem), pend != 0);
 }
 
 __global__ void kg_submean_boucqt(const GroupCase *__restrict__ g, int deferred) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     submean_boucqt_body(d, deferred != 0);
 }
 
@@ -1693,31 +1693,33 @@ __global__ void kg_submean_boucqt(const GroupCase *__restrict__ g, int deferred)
 __global__ void __launch_bounds__(1024) kg_substep_mid(const GroupCase *__restrict__ g, int n, int slot) {
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     substep_mid_body(d, slot, s.ga, s.ro);
 }
 
 __global__ void kg_loads_probe(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     loads_probe_body(d);
 }
 
 __global__ void __launch_bounds__(1024) kg_loads_finish(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     loads_finish_body(d);
 }
 
-__global__ void __launch_bounds__(512) kg_rigid(const GroupCase *__restrict__ g) {
+// mode as k_rigid, with the case's trial load; the commit after a coupling
+// iteration runs for every case (no gate)
+__global__ void __launch_bounds__(512) kg_rigid(const GroupCase *__restrict__ g, int mode) {
     __shared__ Dev d;
-    stage_case(g, &d);
-    rigid_body(d, g[blockIdx.z].hist_rows, RIGID_STEP, nullptr);
+    if (!stage_case(g, &d, nullptr, 0, mode == RIGID_PLACE || mode == RIGID_FORCES)) return;
+    rigid_body(d, g[blockIdx.z].hist_rows, mode, g[blockIdx.z].fin);
 }
 
 __global__ void __launch_bounds__(256) kg_diag(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d, nullptr, 0, false)) return;
     diag_body(d, g[blockIdx.z].hist_rows);
 }
 
@@ -1863,8 +1865,8 @@ void glaunch_loads(const Group &g, cudaStream_t s) {
     pdl(kg_loads_probe, zgrid(dim3((3 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
     pdl(kg_loads_finish, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases);
 }
-void glaunch_rigid(const Group &g, cudaStream_t s) {
-    if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(512), 0, s, g.cases);
+void glaunch_rigid(const Group &g, cudaStream_t s, int mode) {
+    if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(512), 0, s, g.cases, mode);
 }
 void glaunch_diag(const Group &g, cudaStream_t s) {
     pdl(kg_diag, zgrid(dim3(std::min(group_stride_blocks(g.rep), 2048)), g), dim3(256), 0, s, g.cases);

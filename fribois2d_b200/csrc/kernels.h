@@ -40,7 +40,7 @@ void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s, bool pend = fal
 void glaunch_submean_boucqt(const Group &g, cudaStream_t s, bool deferred = false);
 void glaunch_substep_mid(const Group &g, int n_next, int slot, cudaStream_t s);
 void glaunch_loads(const Group &g, cudaStream_t s);
-void glaunch_rigid(const Group &g, cudaStream_t s);
+void glaunch_rigid(const Group &g, cudaStream_t s, int mode = RIGID_STEP);
 void glaunch_diag(const Group &g, cudaStream_t s);
 
 }  // namespace fb

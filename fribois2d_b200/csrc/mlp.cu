@@ -395,3 +395,13 @@ int fb_mlp_train(fb_mlp *m, const float *x, const float *t, int n, int epochs, i
 }
 
 }  // extern "C"
+
+namespace fb {
+// the parameters as the coupling's device-side inference reads them
+const float *mlp_params_device(const fb_mlp *m, int *n_in, int *n_out) {
+    if (!m) return nullptr;
+    if (n_in) *n_in = m->sh.nin;
+    if (n_out) *n_out = m->sh.nout;
+    return m->P;
+}
+}  // namespace fb

@@ -313,6 +313,7 @@ template <int BN>
 __global__ void __launch_bounds__(kThreads, 1) kg_tf32x3_gemm(const GemmTask *__restrict__ t) {
     FB_GRID_WAIT();
     const GemmTask &tk = t[blockIdx.z];
+    if (tk.gate && !*tk.gate) return;
     const GemmOut o = tk.o;
     gemm_body<BN, true>(&tk.p.a_hi, &tk.p.a_lo, &tk.p.b_hi, &tk.p.b_lo, o, tk.p.K, tk.status);
 }
@@ -532,6 +533,7 @@ template <int BN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) kg_tf32x3_gemm2(const GemmTask *__restrict__ t) {
     FB_GRID_WAIT();
     const GemmTask &tk = t[blockIdx.z];
+    if (tk.gate && !*tk.gate) return;   // both CTAs of the pair: one case
     const GemmOut o = tk.o;
     gemm2_body<BN, true>(&tk.p.a_hi, &tk.p.a_lo, &tk.p.b_hi, &tk.p.b_lo, o, tk.p.K, tk.status);
 }
@@ -576,6 +578,7 @@ __global__ void __launch_bounds__(256) k_split_t(const double *__restrict__ src,
 __global__ void __launch_bounds__(256) kg_split_t(const SplitTask *__restrict__ tk, int R, int C) {
     const SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
+    if (t.gate && !*t.gate) return;
     split_t_body(t.src, t.lds, R, C, t.hi, t.lo, t.ldd, t.cscale);
 }
 
@@ -633,7 +636,7 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
                                                             const ResidualTask *__restrict__ tk) {
     __shared__ Dev d;
     const ResidualTask t = tk[blockIdx.z];
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     poisson_residual_body(d, t.phi, t.hi, t.lo, t.ldd, t.kscale);
 }
 
@@ -692,6 +695,7 @@ __global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ sr
 __global__ void __launch_bounds__(256) kg_i8_rowmax(const I8SplitTask *__restrict__ tk, int R, int K) {
     const I8SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
+    if (t.gate && !*t.gate) return;
     i8_rowmax_body(t.src, t.lds, R, K, t.cmax, t.rows_pad);
 }
 
@@ -753,6 +757,7 @@ __global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ sr
 __global__ void __launch_bounds__(256) kg_i8_digits(const I8SplitTask *__restrict__ tk, int R, int K, int nchunk) {
     const I8SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
+    if (t.gate && !*t.gate) return;
     i8_digits_body(t.src, t.lds, R, K, t.cmax, nchunk, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale,
                    t.rows_pad);
 }
@@ -941,6 +946,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 __global__ void __launch_bounds__(kThreads, 1) kg_i8x8_gemm(const I8Task *__restrict__ t) {
     FB_GRID_WAIT();
     const I8Task &tk = t[blockIdx.z];
+    if (tk.gate && !*tk.gate) return;
     const I8Out o = tk.o;
     i8x8_body<true>(&tk.a, &tk.b, o, tk.K, tk.status);
 }

@@ -33,10 +33,13 @@ struct Tf32x3Plan {      // tensor maps of one C = A * B^T product
 };
 
 // grouped launches (blockIdx.z = product or case), task arrays in device memory
+// gate (all task kinds): the product or split runs only while *gate is
+// non-zero (null: always) -- the case's strong-coupling iteration is active
 struct GemmTask {        // one product: its tensor maps, output and status word
     Tf32x3Plan p;
     GemmOut o;
     int *status;
+    const int *gate;
 };
 struct SplitTask {       // one transposed split: src (lds) -> hi, lo (ldd), column factors
     const double *src;
@@ -44,6 +47,7 @@ struct SplitTask {       // one transposed split: src (lds) -> hi, lo (ldd), col
     float *hi, *lo;
     long ldd;
     const double *cscale;
+    const int *gate;
 };
 struct ResidualTask {    // one Poisson residual: phi -> hi, lo (ldd), row factors
     const double *phi;
@@ -85,12 +89,14 @@ struct I8SplitTask {
     long ldk;
     double *scale, *cmax;
     int rows_pad;
+    const int *gate;
 };
 struct I8Task {
     CUtensorMap a, b;
     I8Out o;
     int K;
     int *status;
+    const int *gate;
 };
 int i8_configure();
 // box_rows: 128 for the A operand, kI8BN for B

@@ -760,14 +760,14 @@ template <int KM, int kWTk>
 __global__ void __launch_bounds__(kWThreads, 3) kg_helsolve_win(const GroupCase *__restrict__ g, int n, int ntj) {
     __shared__ Dev d;
     __shared__ SubDev s;
-    stage_case(g, &d, &s, n);
+    if (!stage_case(g, &d, &s, n)) return;
     helsolve_win_body<KM, kWTk>(d, s, ntj, s.win_y, s.win_z);
 }
 
 template <int M>
 __global__ void __launch_bounds__(kYLines * kYWarps * 32) kg_ylines_poisson(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
-    stage_case(g, &d);
+    if (!stage_case(g, &d)) return;
     const ScanSys z{nullptr, nullptr, nullptr};
     ylines_body<M, 2>(d, z, nullptr, z, nullptr);
 }

@@ -1,15 +1,22 @@
 """The learned initial guess of the strong coupling iteration.
 
-Training data come from the solver itself: a seeded sweep of small VIV
-cylinder cases advanced with strong coupling and the plain (extrapolating)
-predictor; every converged step yields its 27 features (the last 8
-displacements, velocities and loads of the free coordinate as increments
-between steps, Re, mass ratio, reduced velocity) and its 2 targets (the
-corrections that the next displacement and load need on top of their linear
-extrapolations).  The perceptron is trained and evaluated by the library's own CUDA
-kernels (fribois2d_b200.MLP); the coupling then adds the load correction it
-predicts to the extrapolated initial guess and keeps its convergence test
-unchanged.
+Training data come from the solver itself: a seeded sweep of VIV cylinder
+cases advanced together (one coupled batch: the fluid solves of every case
+in grouped launches, the iteration on the device) with strong coupling and
+the plain (extrapolating) predictor.  Every converged step yields 27
+features -- for the free coordinate's displacement, velocity and load, the
+second differences of the last 8 converged values divided by their root
+mean square (the shape of the recent curvature), then Re, mass ratio and
+reduced velocity -- and 2 targets: the corrections that the step's
+displacement and load needed on top of their linear extrapolations, in units
+of that root mean square, less a structured prior (the curvature
+extrapolated linearly, i.e. a cubic extrapolation of the history, switched
+off in windows where one value dominates).  The perceptron learns that
+residual; it is trained and evaluated by the library's own CUDA kernels
+(fribois2d_b200.MLP).  The coupling adds prior + residual to the linear
+extrapolation of the load as its initial guess and keeps its convergence
+test unchanged; without a network set, the learned mode uses the prior
+alone.
 """
 from __future__ import annotations
 
@@ -20,7 +27,7 @@ from typing import List, Sequence, Tuple
 
 import numpy as np
 
-from . import COUPLING_LEARNED, COUPLING_STRONG, MLP, Solver
+from . import COUPLING_LEARNED, COUPLING_STRONG, MLP, Batch, Solver
 from . import case as cases
 
 
@@ -49,22 +56,31 @@ def _open(c: cases.Case, root: str, device: int = 0) -> Solver:
     return s
 
 
-def generate(case_list: Sequence[cases.Case], steps: int, tol: float = 1e-8, device: int = 0
-             ) -> Tuple[np.ndarray, np.ndarray, float]:
+def generate(case_list: Sequence[cases.Case], steps: int, tol: float = 1e-8, device: int = 0,
+             chunk: int = 4096) -> Tuple[np.ndarray, np.ndarray, float]:
     """(features, targets, mean fluid solves per step) of strongly coupled
-    runs with the plain predictor."""
+    runs with the plain predictor, all cases advanced as one batch."""
     root = tempfile.mkdtemp(prefix="fbsweep_")
-    xs, ts, solves, nsteps = [], [], 0.0, 0.0
-    for c in case_list:
-        s = _open(c, root, device)
+    solvers = [_open(c, root, device) for c in case_list]
+    for s in solvers:
         s.set_coupling(COUPLING_STRONG, tol)
-        s.advance(0, steps, history=False)
-        x, t = s.coupling_samples()
+    b = Batch(solvers)
+    xs, ts = [], []
+    done = 0
+    while done < steps:   # the samples of every case drained before its ring fills
+        k = min(chunk, steps - done)
+        b.advance(k)
+        for s in solvers:
+            x, t = s.coupling_samples()
+            xs.append(x)
+            ts.append(t)
+        done += k
+    b.close()
+    solves = nsteps = 0.0
+    for s in solvers:
         st = s.coupling_stats()
         solves += st["solves"]
         nsteps += st["steps"]
-        xs.append(x)
-        ts.append(t)
         s.close()
     return np.concatenate(xs), np.concatenate(ts), solves / max(nsteps, 1.0)
 
@@ -96,8 +112,18 @@ class Predictor:
     final_loss: float
 
 
+def predictable(t: np.ndarray, bound: float = 1.0) -> np.ndarray:
+    """Samples whose targets (the prior's residuals, in units of the history's
+    scale) are within `bound`: the steps a smooth history can predict.  The
+    rest -- jumps of the loads as markers cross grid lines -- are left out of
+    training, and the device clamps the network's residual to the same bound."""
+    return np.all(np.abs(t) <= bound, axis=1)
+
+
 def train(x: np.ndarray, t: np.ndarray, epochs: int = 300, batch: int = 128, lr: float = 2e-3, seed: int = 0,
           device: int = 0) -> Predictor:
+    keep = predictable(t)
+    x, t = x[keep], t[keep]
     norm = standardise(x, t)
     xn, tn = apply_norm(norm, x, t)
     m = MLP(x.shape[1], t.shape[1], seed=seed, device=device)
@@ -105,19 +131,23 @@ def train(x: np.ndarray, t: np.ndarray, epochs: int = 300, batch: int = 128, lr:
     return Predictor(m, norm, loss)
 
 
-def mean_solves(c: cases.Case, steps: int, predictor: Predictor = None, tol: float = 1e-8, device: int = 0
-                ) -> Tuple[float, np.ndarray, float]:
-    """Mean fluid solves per step of a strongly coupled run (learned
-    predictor if given, else the plain one), its history rows and the mean
-    relative load residual of the initial guesses."""
+def mean_solves(c: cases.Case, steps: int, predictor=None, tol: float = 1e-8, device: int = 0,
+                skip: int = 0) -> Tuple[float, np.ndarray, float]:
+    """Mean fluid solves per step of a strongly coupled run over the steps
+    after the first `skip`, its history rows and the mean relative load
+    residual of the initial guesses (over all steps).  predictor: None (the
+    plain predictor), "prior" (the learned mode's structured prior without a
+    network) or a trained Predictor."""
     root = tempfile.mkdtemp(prefix="fbeval_")
     s = _open(c, root, device)
     if predictor is None:
         s.set_coupling(COUPLING_STRONG, tol)
     else:
         s.set_coupling(COUPLING_LEARNED, tol)
-        s.set_predictor(predictor.mlp, predictor.norm)
+        if predictor != "prior":
+            s.set_predictor(predictor.mlp, predictor.norm)
     h = s.advance(0, steps)
     st = s.coupling_stats()
     s.close()
-    return st["solves"] / st["steps"], h, st["initial_residual"]
+    col = h[skip:, 30]
+    return float(col.mean()), h, st["initial_residual"]

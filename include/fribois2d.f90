@@ -276,6 +276,11 @@ module fribois2d_gpu
       type(c_ptr), value :: ctx
       integer(c_int), value :: mode
     end function
+    integer(c_int) function fb_set_refinement(ctx, sweeps) bind(C, name="fb_set_refinement")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: sweeps
+    end function
     integer(c_int) function fb_gemm_i8x8(device, m, n, k, a, b, c) bind(C, name="fb_gemm_i8x8")
       import :: c_int, c_double
       integer(c_int), value :: device, m, n, k

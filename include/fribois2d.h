@@ -283,7 +283,7 @@ int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
  * kept as the comparison arm.  FB_POISSON_TF32X3: the two eigen transforms on
  * the tensor cores in split precision (TF32 high and low parts, three
  * products, FP32 accumulation), FP64 tridiagonal solves, then FP64
- * iterative-refinement sweeps on the Poisson residual.  The forms have no
+ * iterative-refinement sweeps on the Poisson residual (fb_set_refinement).  The forms have no
  * counterpart in the reference. */
 #define FB_POISSON_FP64 0
 #define FB_POISSON_TF32X3 1
@@ -294,6 +294,11 @@ int fb_kernel_count(fb_ctx *ctx, int32_t *per_step);
  * no refinement sweep; K (= n3 - 1) at most 16384. */
 #define FB_POISSON_INT8X8 2
 int fb_set_poisson(fb_ctx *ctx, int mode);
+/* FP64 iterative-refinement sweeps of FB_POISSON_TF32X3 (1..4, default 2):
+ * each sweep solves again, with the same tensor-core transforms, for the
+ * FP64 residual r = dph - (A_yy + A_zz) phi and adds the correction.  No
+ * counterpart in the reference. */
+int fb_set_refinement(fb_ctx *ctx, int sweeps);
 /* C = A * B^T with the INT8 digit-slice kernel (conventions and buffers as
  * fb_gemm_tf32x3; a test entry point). */
 int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double *B, double *C);

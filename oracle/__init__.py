@@ -282,6 +282,13 @@ def _load():
     lib.fbo_dgttrf.restype = ctypes.c_int
     lib.fbo_dgtts2.argtypes = [ctypes.c_int, dp, dp, dp, dp, P(ctypes.c_int), dp]
     lib.fbo_set_threads.argtypes = [ctypes.c_int]
+    lib.fbo_coupled_step.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_double, dp]
+    lib.fbo_coupled_step.restype = ctypes.c_int
+    lib.fbo_rigid_mode.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    lib.fbo_rigid_mode.restype = ctypes.c_int
+    lib.fbo_snapshot.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.fbo_snapshot.restype = ctypes.c_int
     return lib
 
 
@@ -395,6 +402,35 @@ class Oracle:
         keys = ("time", "dt", "dt_o", "beta", "al", "ga", "ro", "cflm", "q3avg", "nbcv",
                 "nbcw", "ddmin", "pravg")
         return {k: float(s[i]) for i, k in enumerate(keys)}
+
+    def coupled_step(self, ns: int, tol: float = 1e-8, maxit: int = 50, omega0: float = 0.5,
+                     guess: np.ndarray = None) -> Tuple[int, int, float]:
+        """One strongly coupled step (fbo_coupled_step; the project's own
+        iteration, the reference couples explicitly).  The initial guess is
+        the plain predictor's -- the last two converged loads extrapolated
+        linearly -- unless `guess` (Fy, Fz, M) is given; the relaxation
+        starts from the last Aitken factor of an earlier step.  Returns
+        (status, fluid solves, relative load residual of the guess)."""
+        hist = self.__dict__.setdefault("_coupled_loads", [])
+        last = self.__dict__.setdefault("_aitken", [])
+        if guess is not None:
+            F0 = np.asarray(guess, dtype=np.float64)
+        elif len(hist) >= 2:
+            F0 = 2.0 * hist[-1] - hist[-2]
+        elif len(hist) == 1:
+            F0 = hist[-1].copy()
+        else:
+            F0 = np.zeros(3)
+        F0 = np.ascontiguousarray(F0, dtype=np.float64)
+        q = next((i for i in range(3) if int(self.deck["rbmcon"][i]) == 0), 0)
+        out = np.zeros(7)
+        w0 = min(2.0, max(0.05, last[-1])) if last else omega0
+        st = self.lib.fbo_coupled_step(self.h, ns, _dptr(F0), tol, maxit, q, w0, _dptr(out))
+        if st == 0:
+            hist.append(out[:3].copy())
+            if out[6] != 0.0:
+                last.append(float(out[6]))
+        return st, int(out[3]), float(out[4])
 
     def add_v_perturbation(self, pert: np.ndarray) -> None:
         """Add a ``(n3m, n2)`` perturbation to ``q2`` rows ``k = 1..n3m``."""

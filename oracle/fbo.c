@@ -48,6 +48,7 @@ struct fbo_state {
     double kinori[3][3];
     double forces[8];
     double scalars[13];
+    double *snap; /* saved start-of-step state of the coupling iteration */
 };
 
 #define FLD(a, j, k) (a)[(size_t)((k) + KG) * (size_t)n2 + (size_t)((j) - 1)]
@@ -552,7 +553,7 @@ void fbo_destroy(fbo_state *s)
         (void **)&s->lmvel, (void **)&s->lmacc, (void **)&s->lmnor, (void **)&s->lmA,
         (void **)&s->vert, (void **)&s->lmind, (void **)&s->eulins, (void **)&s->phi,
         (void **)&s->cl, (void **)&s->press, (void **)&s->tau, (void **)&s->bcerrv,
-        (void **)&s->bcerrw};
+        (void **)&s->bcerrw, (void **)&s->snap};
     for (size_t i = 0; i < sizeof(pp) / sizeof(pp[0]); i++) free(*pp[i]);
     free(s);
 }
@@ -1654,8 +1655,15 @@ static void kinem(fbo_state *s, double Fy, double Fz, double M)
     }
 }
 
-/* rigid.F90:373-464 (int_stress): F = sum(-p n + tau) A, moment about cm */
+/* rigid.F90:373-464 (int_stress): F = sum(-p n + tau) A, moment about cm
+ * (the start-of-step centre cmp_n, or the trial centre in the coupling) */
+static void int_stress_about(fbo_state *s, const double *centre, double *forcm, double *momcm);
 static void int_stress(fbo_state *s, double *forcm, double *momcm)
+{
+    int_stress_about(s, CMP_N, forcm, momcm);
+}
+
+static void int_stress_about(fbo_state *s, const double *centre, double *forcm, double *momcm)
 {
     double fyp = 0.0, fzp = 0.0, fyv = 0.0, fzv = 0.0, fy, fz, forgcm[2], mom;
     int i, nlm = s->nlm;
@@ -1675,7 +1683,7 @@ static void int_stress(fbo_state *s, double *forcm, double *momcm)
     forcm[1] = fz + forgcm[1];
     *momcm = 0.0;
     for (i = 1; i <= nlm; i++) {
-        double r1 = M2(s->lmcc, i, 1) - CMP_N[0], r2 = M2(s->lmcc, i, 2) - CMP_N[1];
+        double r1 = M2(s->lmcc, i, 1) - centre[0], r2 = M2(s->lmcc, i, 2) - centre[1];
         double Ft1 = -s->press[i - 1] * M2(s->lmnor, i, 1) * s->lmA[i - 1] + s->tau[2 * (i - 1)] * s->lmA[i - 1];
         double Ft2 = -s->press[i - 1] * M2(s->lmnor, i, 2) * s->lmA[i - 1] + s->tau[2 * (i - 1) + 1] * s->lmA[i - 1];
         mom = r1 * Ft2 - r2 * Ft1;
@@ -1691,20 +1699,37 @@ static void int_stress(fbo_state *s, double *forcm, double *momcm)
     s->forces[7] = fzv;
 }
 
-/* rigid.F90:4-138 */
-int fbo_rigid(fbo_state *s, int ns)
+/* rigid.F90:58-62: constrained coordinates keep their initial kinematics */
+static void constrain(fbo_state *s)
 {
-    double forcm[2], momcm, r[2][2], cmrot;
-    int i, nlm = s->nlm;
-    (void)ns;
-    int_stress(s, forcm, &momcm);
-    kinem(s, forcm[0], forcm[1], momcm);
-    for (i = 0; i < 3; i++)
+    for (int i = 0; i < 3; i++)
         if (s->p.rbmcon[i] == 1) {
             CMP_NP1[i] = s->kinori[0][i];
             CMV_NP1[i] = s->kinori[1][i];
             CMA_NP1[i] = s->kinori[2][i];
         }
+}
+
+/* rigid.F90:64-126: the markers and vertices moved to the np1 state; commit
+ * makes it the new n state (the loose step always commits) */
+static void move_body(fbo_state *s, int commit);
+
+/* rigid.F90:4-138 */
+int fbo_rigid(fbo_state *s, int ns)
+{
+    double forcm[2], momcm;
+    (void)ns;
+    int_stress(s, forcm, &momcm);
+    kinem(s, forcm[0], forcm[1], momcm);
+    constrain(s);
+    move_body(s, 1);
+    return FBO_OK;
+}
+
+static void move_body(fbo_state *s, int commit)
+{
+    double r[2][2], cmrot;
+    int i, nlm = s->nlm;
     cmrot = CMP_NP1[2] - CMP_N[2];
     get_rotmat(cmrot, r);
     for (i = 1; i <= nlm; i++) {
@@ -1724,20 +1749,154 @@ int fbo_rigid(fbo_state *s, int ns)
         M2(s->lmacc, i, 1) = CMA_NP1[0] + c2[0] + c3[0];
         M2(s->lmacc, i, 2) = CMA_NP1[1] + c2[1] + c3[1];
     }
-    for (i = 0; i < 3; i++) {
-        CMP_N[i] = CMP_NP1[i];
-        CMV_N[i] = CMV_NP1[i];
-        CMA_N[i] = CMA_NP1[i];
-    }
+    if (commit)
+        for (i = 0; i < 3; i++) {
+            CMP_N[i] = CMP_NP1[i];
+            CMV_N[i] = CMV_NP1[i];
+            CMA_N[i] = CMA_NP1[i];
+        }
     /* vertices are rotated about the updated centre (rigid.F90:117-121) */
     for (i = 1; i <= nlm + 1; i++) {
         double rho[2];
-        rho[0] = M2(s->vert, i, 1) - CMP_N[0];
-        rho[1] = M2(s->vert, i, 2) - CMP_N[1];
+        rho[0] = M2(s->vert, i, 1) - CMP_NP1[0];
+        rho[1] = M2(s->vert, i, 2) - CMP_NP1[1];
         M2(s->vert, i, 1) = CMP_NP1[0] + (r[0][0] * rho[0] + r[0][1] * rho[1]);
         M2(s->vert, i, 2) = CMP_NP1[1] + (r[1][0] * rho[0] + r[1][1] * rho[1]);
     }
     createnorm(nlm, s->vert, -1.0, s->lmnor);
+}
+
+/* ------------------------------------------------ strong coupling
+ * No counterpart in the reference, which couples explicitly
+ * (main.F90:85-88: fluid_tsch, then rigid).  This restates the strong
+ * coupling iteration of fribois2d_b200/csrc/couple.cu on the CPU so that
+ * the device's coupled steps have a checker: the step's start state is
+ * saved; the body is placed where a trial load moves it (RK4 with the load
+ * frozen, as kinem integrates), the fluid step runs from the saved state,
+ * its loads are integrated at the trial position (moment about the trial
+ * centre), and the trial load is relaxed towards the fluid's with Aitken's
+ * factor on the free coordinate q until |F' - F|_q <= tol max(1, |F'_q|).
+ * The accepted step commits the body with the fluid's load F'. */
+
+/* save (or restore) the fields, inflow/outflow data and scalars, and/or the
+ * body (markers, vertices, normals, centre-of-mass state) */
+int fbo_snapshot(fbo_state *s, int save, int fields, int body)
+{
+    const size_t nf = (size_t)(s->n3 + 1 + 2 * KG) * (size_t)s->n2;
+    const size_t nb = (size_t)s->n2 + 2, nlm = (size_t)s->nlm;
+    double *fl[] = {s->q2, s->q3, s->pr, s->ru2, s->ru3};
+    double *bl[] = {s->qb2s, s->qb2n, s->dqb2s, s->dqb2n, s->qb3s, s->qb3n, s->dqb3s, s->dqb3n,
+                    s->dq2x2o, s->dq3x2o};
+    double *sc[] = {&s->al, &s->ga, &s->ro, &s->beta, &s->dt, &s->dt_o, &s->time, &s->cflm, &s->q3avg,
+                    &s->nbcv, &s->nbcw, &s->ddmin, &s->pravg};
+    double *ml[] = {s->lmcc, s->lmvel, s->lmacc, s->lmnor};
+    const size_t nfield = 5 * nf + 10 * nb + 13, nbody = 4 * 2 * nlm + 2 * (nlm + 1) + 18;
+    size_t off = 0;
+    int i;
+    if (!s->snap) {
+        s->snap = dalloc(nfield + nbody);
+        if (!s->snap) return FBO_ERR_INPUT;
+    }
+#define SNAP(ptr, n)                                                             \
+    do {                                                                         \
+        if (save) memcpy(s->snap + off, (ptr), sizeof(double) * (n));           \
+        else memcpy((ptr), s->snap + off, sizeof(double) * (n));                 \
+    } while (0)
+    if (fields) {
+        for (i = 0; i < 5; i++, off += nf) SNAP(fl[i], nf);
+        for (i = 0; i < 10; i++, off += nb) SNAP(bl[i], nb);
+        for (i = 0; i < 13; i++, off += 1) SNAP(sc[i], 1);
+    } else {
+        off += nfield;
+    }
+    if (body) {
+        for (i = 0; i < 4; i++, off += 2 * nlm) SNAP(ml[i], 2 * nlm);
+        SNAP(s->vert, 2 * (nlm + 1));
+        off += 2 * (nlm + 1);
+        SNAP(s->rigid, 18);
+    }
+#undef SNAP
+    return FBO_OK;
+}
+
+/* the rigid update split for the coupling: PLACE moves the body to the
+ * state the load fin (Fy, Fz, M) gives, without committing; FORCES
+ * integrates the loads at that trial state (moment about the trial centre)
+ * into the forcecomp row and the np1 state only; COMMIT is the loose update
+ * with the load fin */
+int fbo_rigid_mode(fbo_state *s, int mode, const double *fin)
+{
+    double forcm[2], momcm;
+    switch (mode) {
+    case FBO_RIGID_PLACE:
+        kinem(s, fin[0], fin[1], fin[2]);
+        constrain(s);
+        move_body(s, 0);
+        return FBO_OK;
+    case FBO_RIGID_FORCES:
+        int_stress_about(s, CMP_NP1, forcm, &momcm);
+        kinem(s, forcm[0], forcm[1], momcm);
+        constrain(s);
+        return FBO_OK;
+    case FBO_RIGID_COMMIT:
+        kinem(s, fin[0], fin[1], fin[2]);
+        constrain(s);
+        move_body(s, 1);
+        return FBO_OK;
+    default:
+        return FBO_ERR_INPUT;
+    }
+}
+
+/* one strongly coupled step from the initial guess F0 and relaxation factor
+ * omega0 (the caller passes the last Aitken factor of an earlier step,
+ * clamped to [0.05, 2], or 0.5 before the first); out: F' (3), fluid
+ * solves, relative load residual of the initial guess, converged flag, the
+ * last Aitken factor computed in this step (0 if none) */
+int fbo_coupled_step(fbo_state *s, int ns, const double F0[3], double tol, int maxit, int q, double omega0,
+                     double out[7])
+{
+    double F[3], Ff[3] = {0.0, 0.0, 0.0}, res[3], rprev[3] = {0.0, 0.0, 0.0}, omega = omega0, res0 = 0.0;
+    double aitken = 0.0;
+    int it, i, conv = 0, st;
+    fbo_snapshot(s, 1, 1, 1);
+    for (i = 0; i < 3; i++) F[i] = F0[i];
+    for (it = 0; it < maxit; it++) {
+        if (it > 0) fbo_snapshot(s, 0, 1, 1);
+        fbo_rigid_mode(s, FBO_RIGID_PLACE, F);
+        st = fbo_fluid_tsch(s, ns);
+        if (st) return st;
+        fbo_rigid_mode(s, FBO_RIGID_FORCES, NULL);
+        for (i = 0; i < 3; i++) {
+            Ff[i] = s->forces[1 + i];
+            res[i] = Ff[i] - F[i];
+        }
+        if (it == 0) res0 = fabs(res[q]) / fmax(1.0, fabs(Ff[q]));
+        conv = fabs(res[q]) <= tol * fmax(1.0, fabs(Ff[q]));
+        if (conv) break;
+        if (it > 0) {
+            const double dr = res[q] - rprev[q];
+            if (dr != 0.0) {
+                omega = -omega * rprev[q] / dr;
+                aitken = omega;
+            }
+        }
+        for (i = 0; i < 3; i++) {
+            F[i] = F[i] + omega * res[i];
+            rprev[i] = res[i];
+        }
+    }
+    /* accept: body back to the start of the step, then the update with F' */
+    fbo_snapshot(s, 0, 0, 1);
+    for (i = 0; i < 3; i++) s->forces[1 + i] = Ff[i];
+    fbo_rigid_mode(s, FBO_RIGID_COMMIT, Ff);
+    s->time = s->time + s->dt;
+    s->dt_o = s->dt;
+    for (i = 0; i < 3; i++) out[i] = Ff[i];
+    out[3] = (double)(conv ? it + 1 : it);
+    out[4] = res0;
+    out[5] = (double)conv;
+    out[6] = aitken;
     return FBO_OK;
 }
 

@@ -84,6 +84,12 @@ int fbo_step(fbo_state *s, int ns);             /* main.F90:85-97 */
 int fbo_set_substep(fbo_state *s, int ns, int n);
 int fbo_stage(fbo_state *s, int stage, int n);
 int fbo_status(fbo_state *s);
+/* strong coupling (no reference counterpart): see fbo.c */
+enum { FBO_RIGID_PLACE = 1, FBO_RIGID_FORCES = 2, FBO_RIGID_COMMIT = 3 };
+int fbo_snapshot(fbo_state *s, int save, int fields, int body);
+int fbo_rigid_mode(fbo_state *s, int mode, const double *fin);
+int fbo_coupled_step(fbo_state *s, int ns, const double F0[3], double tol, int maxit, int q, double omega0,
+                     double out[7]);
 /* LAPACK restatements, exported so the tests can pin them against LAPACK */
 int fbo_dgttrf(int n, double *dl, double *d, double *du, double *du2, int *ipiv);
 void fbo_dgtts2(int n, const double *dl, const double *d, const double *du, const double *du2,
