@@ -62,6 +62,11 @@ def parse():
                     help="advance N independent VIV cases (grid sizes 256x192..768x512 drawn by seed) "
                          "with one graph launch per step instead of the single case")
     ap.add_argument("--sweeps", type=int, default=2, help="FP64 refinement sweeps of the tf32x3 form")
+    ap.add_argument("--coupling", default="loose", choices=["loose", "strong", "learned"],
+                    help="with --batch: strong fluid-structure coupling, with the plain or the learned initial guess")
+    ap.add_argument("--train-cases", type=int, default=256, help="sweep cases generating the predictor's samples")
+    ap.add_argument("--train-steps", type=int, default=4000, help="coupled steps per sweep case")
+    ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="steps of the tf32x3 form's accuracy comparison with the FP64 path")
     ap.add_argument("--poisson", default="int8x8", choices=sorted(FORMS),
@@ -270,7 +275,7 @@ def kernel_table(fb, path, c, poisson="int8x8", sweeps=2):
         # reads the FP64 operand and writes 8 int8 planes (16 B per cell)
         transform = [
             ("i8x8 GEMM (tcgen05 kind::i8, 36 digit pairs)", "i8x8_gemm", 6, 36 * gemm, "tensor_i8"),
-            ("i8 digit cut (row maxima + digits)", "i8_split", 6, 2.0 * B, "hbm"),
+            ("i8 digit cut (one cluster launch)", "i8_split", 6, 2.0 * B, "hbm"),
             ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
         ] + dgemm_rows
     elif poisson == "fp64":
@@ -374,6 +379,148 @@ def batch_arm(args, rank, world, local):
     batch.close()
     for sv in solvers:
         sv.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def coupled_batch_arm(args, rank, world, local):
+    """Strongly coupled batch: N VIV cases of the batching form advanced
+    together with the coupling iteration on the device (a graph WHILE node;
+    converged cases sit out the grouped launches), with the learned initial
+    guess (or the plain one).  Reported beside the plain FP64 path -- the
+    same cases loosely coupled, each stepped alone by its own captured step --
+    and the same batch with the plain predictor; the accuracy block compares
+    a subset's lift and displacement histories with the FP64 path
+    (INT8-exact transforms, strong coupling, plain predictor)."""
+    import torch
+    import fribois2d_b200 as fb
+    from fribois2d_b200 import case as cases
+    from fribois2d_b200 import learn
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W, K = max(3, args.warmup), max(1, args.steps)
+    pred, train = None, None
+    if args.coupling == "learned":
+        t0 = time.perf_counter()
+        x, t, plain_train = learn.generate(learn.sweep(args.train_cases, seed=1000 + rank), steps=args.train_steps,
+                                           device=local)
+        t1 = time.perf_counter()
+        pred = learn.train(x, t, epochs=args.train_epochs, batch=1024, lr=1e-3, seed=rank, device=local)
+        train = {"coupling_steps": int(x.shape[0]), "kept": float(learn.predictable(t).mean()),
+                 "cases": args.train_cases, "steps_per_case": args.train_steps,
+                 "generate_s": t1 - t0, "train_s": time.perf_counter() - t1, "final_loss": pred.final_loss,
+                 "plain_solves_per_step": plain_train,
+                 "sweep": "small VIV cylinders (48x32 cells), Re, mass ratio, reduced velocity drawn by seed"}
+    cs = cases.viv_batch(args.batch, seed=rank)
+    cells = sum(c.cells for c in cs)
+    root = tempfile.mkdtemp(prefix=f"fbcbatch{rank}_")
+
+    def open_all(form):
+        out = []
+        for c in cs:
+            sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
+            sv.set_poisson(POISSON_IDS[form])
+            sv.set_refinement(args.sweeps)
+            q2 = sv.get("q2")
+            q2[1:c.n3m + 1] += c.v_perturbation()
+            sv.set("q2", q2)
+            out.append(sv)
+        return out
+
+    # the plain FP64 path: each case loosely coupled, stepped alone
+    solvers = open_all("int8x8")
+    seq_ms = 0.0
+    for sv in solvers:
+        sv.advance(0, W)
+        sv.advance(W, K, history=False)
+        seq_ms += sv.last_advance_ms()
+        sv.close()
+
+    def coupled_run(mode, predictor):
+        svs = open_all(args.poisson)
+        for sv in svs:
+            sv.set_coupling(mode, 1e-8)
+            if predictor is not None:
+                sv.set_predictor(predictor.mlp, predictor.norm)
+        b = fb.Batch(svs)
+        info = b.info()
+        b.advance(W)
+        before = [sv.coupling_stats() for sv in svs]
+        clocks = ClockSampler(local)
+        torch.cuda.synchronize(dev)
+        clocks.start()
+        b.advance(K)
+        clk = clocks.stop()
+        ms = b.last_ms()
+        after = [sv.coupling_stats() for sv in svs]
+        solves = sum(a["solves"] - q["solves"] for a, q in zip(after, before))
+        steps = sum(a["steps"] - q["steps"] for a, q in zip(after, before))
+        b.close()
+        for sv in svs:
+            sv.close()
+        return ms, solves / max(steps, 1.0), info, clk
+
+    mode = fb.COUPLING_LEARNED if pred is not None else fb.COUPLING_STRONG
+    ms, solves, info, clk = coupled_run(mode, pred)
+    plain_ms, plain_solves = None, None
+    if pred is not None:
+        plain_ms, plain_solves, _, _ = coupled_run(fb.COUPLING_STRONG, None)
+    # accuracy: a subset against the FP64 path, each case alone
+    acc = None
+    if args.accuracy_steps > 0:
+        picks = []
+        for n3, n2, _ in cases.BATCH_GRIDS:
+            picks += [c for c in cs if (c.n3m, c.n2m) == (n3, n2)][:2]
+        worst_f = worst_d = 0.0
+        for c in picks:
+            hs = {}
+            for form, md, pr_ in (("int8x8", fb.COUPLING_STRONG, None), (args.poisson, mode, pred)):
+                sv = fb.Solver(c.write(os.path.join(root, "acc_" + c.name)), device=local)
+                sv.set_poisson(POISSON_IDS[form])
+                sv.set_refinement(args.sweeps)
+                q2 = sv.get("q2")
+                q2[1:c.n3m + 1] += c.v_perturbation()
+                sv.set("q2", q2)
+                sv.set_coupling(md, 1e-8)
+                if pr_ is not None:
+                    sv.set_predictor(pr_.mlp, pr_.norm)
+                hs[form + str(md)] = sv.advance(0, args.accuracy_steps)
+                sv.close()
+            a, b_ = list(hs.values())
+            f_ref, d_ref = a[:, 1], a[:, 9]
+            worst_f = max(worst_f, float(np.max(np.abs(b_[:, 1] - f_ref)) / max(np.ptp(f_ref), 1e-300)))
+            worst_d = max(worst_d, float(np.max(np.abs(b_[:, 9] - d_ref)) / max(np.ptp(d_ref), 1e-300)))
+        acc = {"cases": len(picks), "steps": args.accuracy_steps, "lift_rel_of_range": worst_f,
+               "displacement_rel_of_range": worst_d,
+               "reference": "FP64 device path (INT8-exact transforms), strong coupling, plain predictor; "
+                            "its coupled steps follow the oracle's fbo_coupled_step to round-off (tests)"}
+    value = cells * K / (ms * 1e-3)
+    seq_value = cells * K / (seq_ms * 1e-3)
+    line = {
+        "metric": f"cell-steps/s (batch of {args.batch} VIV cases, {FORMS[args.poisson]}, strong coupling, "
+                  f"{'learned' if pred is not None else 'plain'} predictor)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPES[args.poisson], "data": "synthetic",
+        "config": {"workload": f"viv_batch_{args.batch}_coupled", "cells_total": cells,
+                   "grids": {f"{n3}x{n2}": sum(1 for c in cs if (c.n3m, c.n2m) == (n3, n2))
+                             for n3, n2, _ in cases.BATCH_GRIDS},
+                   "groups": info["groups"], "poisson": args.poisson, "coupling": args.coupling,
+                   "tol": 1e-8, "l2": "working set far above L2 (all cases resident)"},
+        "fluid_solves_per_step": solves,
+        "plain_fp64_sequential": {"value": seq_value, "ms_per_step": seq_ms / K,
+                                  "note": "the same cases, FP64 (INT8-exact transforms), loose coupling as the "
+                                          "reference, each advanced alone by its own captured step"},
+        "speedup_vs_plain_fp64": value / seq_value,
+        "plain_predictor": None if plain_ms is None else {
+            "value": cells * K / (plain_ms * 1e-3), "ms_per_step": plain_ms / K,
+            "fluid_solves_per_step": plain_solves},
+        "training": train, "accuracy": acc,
+        "gpu_launches": info["launches"] * K, "clocks": clk,
+    }
+    if pred is not None:
+        pred.mlp.close()
     if rank == 0:
         print(json.dumps(line))
 
@@ -571,6 +718,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.batch and args.coupling != "loose":
+        coupled_batch_arm(args, rank, world, local)
         return
     if args.batch:
         batch_arm(args, rank, world, local)

@@ -92,6 +92,8 @@ struct fb_ctx {
     bool cond_graph = true;                    // coupled step as a graph WHILE node (else a host loop)
     int tune_tk = 64;         // windowed helsolve tile height (autotuned per grid size)
     int tune_bn = 128;        // 3xTF32 GEMM tile width (autotuned per grid size)
+    int tune_i8bn = fb::kI8BN;  // INT8 digit-product tile width, 48 or 64 (autotuned per grid size)
+    bool i8_fixed = false;      // the width set by FRIBOIS2D_I8_TILE: not tuned
     // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
     // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
     int poisson_mode = FB_POISSON_FP64;
@@ -415,6 +417,13 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     }
     c->device = device;
     if (const char *hv = std::getenv("FRIBOIS2D_HELSOLVE")) c->allow_win = std::strcmp(hv, "scan") != 0;
+    if (const char *tw = std::getenv("FRIBOIS2D_I8_TILE")) {   // fixed INT8 product tile width (48 or 64)
+        const int w = std::atoi(tw);
+        if (w == 48 || w == 64) {
+            c->tune_i8bn = w;
+            c->i8_fixed = true;
+        }
+    }
     CK(cudaSetDevice(device));
     CK(fb::scan_configure());
     CK(fb::kernels_configure());
@@ -826,10 +835,10 @@ int setup_i8(fb_ctx *c) {
         int r;
         if ((r = dnew(c, &p.dig, static_cast<size_t>(fb::kI8S) * p.rows_pad * ldk))) return r;
         if ((r = dnew(c, &p.scale, static_cast<size_t>(p.rows_pad)))) return r;
-        if ((r = dnew(c, &p.cmax, static_cast<size_t>(p.rows_pad) * ((d.n3m + fb::kI8Chunk - 1) / fb::kI8Chunk)))) return r;
         return fb::i8_plan(p, rows, d.n3m, box);
     };
-    if ((st = make(c->i8a, d.n2m, 128)) || (st = make(c->i8f, d.n3m, fb::kI8BN)) || (st = make(c->i8b, d.n3m, fb::kI8BN)))
+    if ((st = make(c->i8a, d.n2m, 128)) || (st = make(c->i8f, d.n3m, c->tune_i8bn)) ||
+        (st = make(c->i8b, d.n3m, c->tune_i8bn)))
         return st;
     // forward B(m, k) = zmmt(m, k); backward B(k, m) = zmm(k, m): both column-major
     fb::launch_i8_split(c->zmmt, d.n3m, d.n3m, d.n3m, c->i8f, c->stream);
@@ -850,7 +859,7 @@ int phcalc_i8(fb_ctx *c) {
     fb::launch_scan_poisson(d, st);
     fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
     fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st);
-    c->own_launches += 7;   // two splits of two launches, two products, the mode solves
+    c->own_launches += 5;   // two digit cuts, two products, the mode solves
     return FB_OK;
 }
 
@@ -2024,6 +2033,7 @@ struct BatchGroup {
     // FP64 transforms on the INT8 tensor cores: digit cuts and products of every case
     bool i8 = false;
     fb::I8Plan i8rep{};              // split geometry (the first case's data operand)
+    int i8bn = fb::kI8BN;            // product tile width of the group
     fb::I8SplitTask *i8s = nullptr;  // 2 x n: dph, then hmn, into the case's digit planes
     fb::I8Task *i8t = nullptr;       // 2 x n: forward -> hmn, backward -> dph
 };
@@ -2086,12 +2096,13 @@ bool groupable(const fb_ctx *c) {
 }
 
 // cases that may share launches: same launch geometry and options
-using GroupKey = std::array<int, 12>;
+using GroupKey = std::array<int, 13>;
 GroupKey group_key(const fb_ctx *c) {
     const Dev &d = c->d;
-    const bool tf = c->poisson_mode == FB_POISSON_TF32X3;
+    const bool tf = c->poisson_mode == FB_POISSON_TF32X3, i8 = c->poisson_mode == FB_POISSON_INT8X8;
     return {d.n2, d.n3, d.nlm, d.P, d.ldh, d.NK, c->sub[0].win_tk, c->hc.deck.cbody ? 1 : 0,
-            (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0, tf ? c->tf32_sweeps : 0};
+            (c->report && d.nlm) ? 1 : 0, c->poisson_mode, tf ? c->plan_fwd.bn : 0, tf ? c->tf32_sweeps : 0,
+            i8 ? c->i8b.box : 0};
 }
 
 // The product tile of a group's grouped launches, timed over the whole group
@@ -2215,8 +2226,8 @@ int group_setup_i8(BatchGroup *bg) {
         const size_t k = static_cast<size_t>(i), m = static_cast<size_t>(n);
         const fb::I8Plan &a = c->i8a;
         const int *gate = couple_gate(c);
-        sp[k] = {d.dph + d.P, d.P, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad, gate};
-        sp[m + k] = {d.hmn, d.ldh, a.dig, a.ldk, a.scale, a.cmax, a.rows_pad, gate};
+        sp[k] = {d.dph + d.P, d.P, a.dig, a.ldk, a.scale, a.rows_pad, gate};
+        sp[m + k] = {d.hmn, d.ldh, a.dig, a.ldk, a.scale, a.rows_pad, gate};
         gt[k] = {a.map, c->i8f.map, fb::I8Out{d.hmn, d.ldh, a.scale, c->i8f.scale, d.n2m, d.n3m}, d.n3m, d.status,
                  gate};
         gt[m + k] = {a.map, c->i8b.map, fb::I8Out{d.dph + d.P, d.P, a.scale, c->i8b.scale, d.n2m, d.n3m}, d.n3m,
@@ -2228,6 +2239,7 @@ int group_setup_i8(BatchGroup *bg) {
     CK(cudaMemcpyAsync(bg->i8t, gt.data(), sizeof(fb::I8Task) * gt.size(), cudaMemcpyHostToDevice, bg->st));
     CK(cudaStreamSynchronize(bg->st));
     bg->i8rep = bg->members[0]->i8a;
+    bg->i8bn = bg->members[0]->i8b.box;
     bg->i8 = true;
     return FB_OK;
 }
@@ -2372,11 +2384,11 @@ int enqueue_group_fluid(BatchGroup *bg, int &k) {
             k += 5 + 5 * bg->sweeps;
         } else if (bg->i8) {   // phcalc_i8's launches, each over the whole group
             fb::launch_i8_split_group(bg->i8s, bg->i8rep, d.n2m, d.n3m, n, st);
-            fb::launch_i8x8_group(bg->i8t, d.n2m, d.n3m, n, st);
+            fb::launch_i8x8_group(bg->i8t, d.n2m, d.n3m, n, bg->i8bn, st);
             fb::glaunch_scan_poisson(g, st);
             fb::launch_i8_split_group(bg->i8s + n, bg->i8rep, d.n2m, d.n3m, n, st);
-            fb::launch_i8x8_group(bg->i8t + n, d.n2m, d.n3m, n, st);
-            k += 7;
+            fb::launch_i8x8_group(bg->i8t + n, d.n2m, d.n3m, n, bg->i8bn, st);
+            k += 5;
         } else {
             // phcalc_outflow.F90:31,61-69: hmn = dph zmmt^T, dph = vmn zmm^T
             CB(cublasDgemmBatched(bg->blas, CUBLAS_OP_N, CUBLAS_OP_T, d.n2m, d.n3m, d.n3m, &one, p, d.P, p + n,
@@ -2770,19 +2782,27 @@ int fb_batch_last_ms(fb_batch *b, double *ms) {
 int fb_autotune(fb_ctx *c, int32_t choice[2]) {
     if (!c) return FB_ERR_STATE;
     static std::mutex mu;
-    static std::map<std::pair<int, int>, std::pair<int, int>> cache;   // (n2, n3) -> (tk, bn); bn 0: untuned
+    // (n2, n3) -> (tk, bn, i8 bn); bn 0: untuned
+    static std::map<std::pair<int, int>, std::array<int, 3>> cache;
     const std::pair<int, int> key(c->d.n2, c->d.n3);
-    int tk = 0, bn = 0;
+    int tk = 0, bn = 0, ibn = 0;
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
         if (it != cache.end()) {
-            tk = it->second.first;
-            bn = it->second.second;
+            tk = it->second[0];
+            bn = it->second[1];
+            ibn = it->second[2];
         }
     }
-    const bool want_bn = (c->pw != nullptr);
-    if (!tk || (want_bn && !bn)) {
+    const bool want_bn = (c->pw != nullptr), want_ibn = c->i8_ready && !c->i8_fixed;
+    auto i8_tile = [&](int w) -> int {   // the B operands' boxes set the product tile width
+        int r = fb::i8_plan(c->i8f, c->d.n3m, c->d.n3m, w);
+        if (!r) r = fb::i8_plan(c->i8b, c->d.n3m, c->d.n3m, w);
+        if (!r) c->tune_i8bn = w;
+        return r;
+    };
+    if (!tk || (want_bn && !bn) || (want_ibn && !ibn)) {
         CK(cudaSetDevice(c->device));
         const Dev &d = c->d;
         const size_t fbytes = static_cast<size_t>(d.NK) * d.P * sizeof(double);
@@ -2810,6 +2830,17 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
                 }
             }
         }
+        if (!r && want_ibn && !ibn) {
+            double best = 1e30;
+            for (int cand : {64, 48}) {
+                double ms = 0.0;
+                if ((r = i8_tile(cand)) || (r = fb_time_stage(c, FB_TK_I8X8_GEMM, 1, 10, &ms))) break;
+                if (ms < best * 0.98) {   // 48 must win clearly
+                    best = ms;
+                    ibn = cand;
+                }
+            }
+        }
         if (!r && want_bn && !bn) {
             double best = 1e30;
             for (int cand : {64, 128, fb::kPairTile + 128, fb::kPairTile + 192, fb::kPairTile + 256}) {
@@ -2829,7 +2860,11 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
         cudaFree(save);
         if (r) return r;
         std::lock_guard<std::mutex> lk(mu);
-        cache[key] = std::make_pair(tk, bn);
+        cache[key] = {tk, bn, ibn};
+    }
+    if (want_ibn && ibn) {
+        int r;
+        if ((r = i8_tile(ibn))) return r;
     }
     {
         int rt;
@@ -3073,11 +3108,9 @@ int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double 
     pb.dig = static_cast<int8_t *>(alloc(static_cast<size_t>(fb::kI8S) * pb.rows_pad * ldk));
     pa.scale = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad));
     pb.scale = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad));
-    pa.cmax = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad * ((K + fb::kI8Chunk - 1) / fb::kI8Chunk)));
-    pb.cmax = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad * ((K + fb::kI8Chunk - 1) / fb::kI8Chunk)));
     int *status = static_cast<int *>(alloc(sizeof(int)));
     st = FB_OK;
-    if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !pa.cmax || !pb.cmax || !status)
+    if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !status)
         st = FB_ERR_CUDA;
     if (!st && (cudaMemcpy(dA, A, sizeof(double) * M * K, cudaMemcpyHostToDevice) != cudaSuccess ||
                 cudaMemcpy(dB, B, sizeof(double) * N * K, cudaMemcpyHostToDevice) != cudaSuccess ||

@@ -71,6 +71,8 @@ __device__ double prior(const float *x) {
     return (m > 2.0f) ? 0.0 : 2.0 * static_cast<double>(x[0]) - static_cast<double>(x[1]);
 }
 
+constexpr double kResidualBound = 0.02;
+
 __device__ double extrap(const double (*h)[3], int n, int i) {
     if (n >= 2) return 2.0 * h[n - 1][i] - h[n - 2][i];
     if (n == 1) return h[0][i];
@@ -104,7 +106,9 @@ __device__ void mlp_one(const float *__restrict__ P, const float *xs, float *h1,
 // one block (kCplH threads) per case.  Initial guess: the last two
 // converged loads extrapolated linearly (the plain predictor); with the
 // learned predictor the free coordinate's load adds scale x (prior + the
-// network's residual, clamped to [-1, 1] -- the range it was trained on).
+// network's residual, clamped to +-kResidualBound -- the range it was
+// trained on: on smooth steps the prior's residual is ~1e-3 of the scale,
+// and larger residuals are jumps of the loads that no history predicts).
 __global__ void __launch_bounds__(kCplH) k_couple_begin(Couple *const *cs) {
     FB_GRID_WAIT();
     Couple &c = *cs[blockIdx.x];
@@ -129,7 +133,7 @@ __global__ void __launch_bounds__(kCplH) k_couple_begin(Couple *const *cs) {
     if (threadIdx.x == 0) {
         if (net) {
             const double r = static_cast<double>(y[1] * c.norm[2 * kCplIn + kCplOut + 1] + c.norm[2 * kCplIn + 1]);
-            corr = corr + sF * fmin(1.0, fmax(-1.0, r));
+            corr = corr + sF * fmin(kResidualBound, fmax(-kResidualBound, r));
         }
         if (have) c.F[c.q] += corr;
         for (int i = 0; i < 3; ++i) c.fin[i] = c.F[i];

@@ -13,6 +13,7 @@
 // the accumulator back with tcgen05.ld and store FP64 results.  Every
 // mbarrier wait gives up after one second, records FB_ERR_TIMEOUT and lets
 // the CTA finish (waiting for its own copies and MMAs, freeing its TMEM).
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -659,131 +660,123 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // DGEMM; a row whose entries span many decades is reproduced only to
 // 2^-55 of its largest entry.
 
-// Digit split in two launches so that the whole GPU takes part: the
-// maxima of |A(r, k)| over chunks of kI8Chunk columns (one block per 32 rows
-// and chunk), then the digits of 32 x 32 tiles (one block each), every block
-// of a row deriving the same exponent from the chunk maxima.
+// The digit cut in one launch: a cluster of kCutCl CTAs per 32 rows, each
+// CTA over its own range of columns.  Every CTA takes the maxima of |A(r, k)|
+// of its columns, the cluster exchanges them through distributed shared
+// memory (so every CTA derives each row's exponent from the whole row), and
+// each CTA cuts the digits of its columns: the operand is read once.
+// Columns past K and rows past R get zero digits, up to ldk and rows_pad.
+constexpr int kCutCl = 8;
 
-__device__ __forceinline__ void i8_rowmax_body(const double *__restrict__ src, long lds, int R, int K,
-                                               double *__restrict__ cmax, int rows_pad) {
+__device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long lds, int R, int K, int8_t *dig,
+                                            long ldk, long plane, double *rowscale) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double part[32];
     __shared__ double mx[8][32];
+    __shared__ double sc[32];
+    __shared__ uint32_t tile[kI8S][32][9];   // 4 digits per word, rows padded to 9 words
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int r = blockIdx.x * 32 + lane, k0 = blockIdx.y * kI8Chunk;
+    const int rank = static_cast<int>(cl.block_rank());
+    const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
+    // this CTA's columns: whole 32-column tiles
+    const int tiles = static_cast<int>(ldk / 32), per = (tiles + kCutCl - 1) / kCutCl;
+    const int t0 = min(tiles, rank * per), t1 = min(tiles, t0 + per);
     double m = 0.0;
-    if (r < R) {
-#pragma unroll
-        for (int q = 0; q < kI8Chunk / 8; ++q) {
-            const int k = k0 + w + 8 * q;
-            if (k < K) m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
-        }
-    }
+    if (r < R)
+        for (int k = t0 * 32 + w; k < min(K, t1 * 32); k += 8) m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
     mx[w][lane] = m;
     __syncthreads();
     if (w == 0) {
         for (int q = 1; q < 8; ++q) m = fmax(m, mx[q][lane]);
-        cmax[static_cast<size_t>(blockIdx.y) * rows_pad + blockIdx.x * 32 + lane] = m;
+        part[lane] = m;
     }
-}
-
-__global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
-                                                    double *__restrict__ cmax, int rows_pad) {
-    FB_GRID_WAIT();
-    i8_rowmax_body(src, lds, R, K, cmax, rows_pad);
-}
-
-// grouped (blockIdx.z = case): the task array is host-written
-__global__ void __launch_bounds__(256) kg_i8_rowmax(const I8SplitTask *__restrict__ tk, int R, int K) {
-    const I8SplitTask t = tk[blockIdx.z];
-    FB_GRID_WAIT();
-    if (t.gate && !*t.gate) return;
-    i8_rowmax_body(t.src, t.lds, R, K, t.cmax, t.rows_pad);
-}
-
-// dig[i * plane + r * ldk + k] = digit i of row r (k < K; 0 for k >= K or
-// r >= R, up to the padded rows and ldk), rowscale[r] = 2^e(r); the source is
-// column-major, A(r, k) at src[k * lds + r].  Block (x, y): rows 32x.., columns 32y..
-__device__ __forceinline__ void i8_digits_body(const double *__restrict__ src, long lds, int R, int K,
-                                               const double *__restrict__ cmax, int nchunk, int8_t *dig, long ldk,
-                                               long plane, double *rowscale, int rows_pad) {
-    __shared__ double sc[32];
-    __shared__ uint32_t tile[kI8S][32][9];   // 4 digits per word, rows padded to 9 words
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int r0 = blockIdx.x * 32, r = r0 + lane, k0 = blockIdx.y * 32;
+    cl.sync();   // every CTA's maxima are written
     if (w == 0) {
-        double m = 0.0;
-        for (int q = 0; q < nchunk; ++q) m = fmax(m, cmax[static_cast<size_t>(q) * rows_pad + r0 + lane]);
+        double mm = 0.0;
+        for (int q = 0; q < kCutCl; ++q) mm = fmax(mm, *cl.map_shared_rank(&part[lane], q));
         int e = 0;
-        if (m > 0.0) frexp(m, &e);   // m < 2^e
+        if (mm > 0.0) frexp(mm, &e);   // mm < 2^e
         sc[lane] = ldexp(1.0, -e);
-        if (blockIdx.y == 0 && r < R) rowscale[r] = ldexp(1.0, e);
+        if (rank == 0 && r < R) rowscale[r] = ldexp(1.0, e);
     }
-    __syncthreads();
+    cl.sync();   // no CTA leaves while another still reads its maxima
     const double s = sc[lane];
-    // thread (lane, w): row r, columns k0 + 4w .. k0 + 4w + 3 (loads coalesced over the rows)
-    double a[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int k = k0 + 4 * w + q;
-        a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < kI8S; ++i) {
-        uint32_t word = 0;
+    for (int tt = t0; tt < t1; ++tt) {
+        const int k0 = tt * 32;
+        // thread (lane, w): row r, columns k0 + 4w .. k0 + 4w + 3 (loads coalesced over the rows)
+        double a[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            a[q] = a[q] * 128.0;
-            const double d = trunc(a[q]);
-            a[q] = a[q] - d;
-            word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
+            const int k = k0 + 4 * w + q;
+            a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
         }
-        tile[i][lane][w] = word;
-    }
-    __syncthreads();
-    {   // slice i = w, row lane: 32 bytes
-        const uint32_t *t = &tile[w][lane][0];
-        uint4 *o = reinterpret_cast<uint4 *>(dig + static_cast<size_t>(w) * plane + static_cast<size_t>(r0 + lane) * ldk + k0);
-        o[0] = make_uint4(t[0], t[1], t[2], t[3]);
-        o[1] = make_uint4(t[4], t[5], t[6], t[7]);
+#pragma unroll
+        for (int i = 0; i < kI8S; ++i) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q] = a[q] * 128.0;
+                const double d = trunc(a[q]);
+                a[q] = a[q] - d;
+                word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
+            }
+            tile[i][lane][w] = word;
+        }
+        __syncthreads();
+        {   // slice i = w, row lane: 32 bytes
+            const uint32_t *t = &tile[w][lane][0];
+            uint4 *o = reinterpret_cast<uint4 *>(dig + static_cast<size_t>(w) * plane + static_cast<size_t>(r0 + lane) * ldk + k0);
+            o[0] = make_uint4(t[0], t[1], t[2], t[3]);
+            o[1] = make_uint4(t[4], t[5], t[6], t[7]);
+        }
+        __syncthreads();
     }
 }
 
-__global__ void __launch_bounds__(256) k_i8_digits(const double *__restrict__ src, long lds, int R, int K,
-                                                    const double *__restrict__ cmax, int nchunk, int8_t *dig,
-                                                    long ldk, long plane, double *rowscale, int rows_pad) {
+__global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
+    k_i8_cut(const double *__restrict__ src, long lds, int R, int K, int8_t *dig, long ldk, long plane,
+             double *rowscale) {
     FB_GRID_WAIT();
-    i8_digits_body(src, lds, R, K, cmax, nchunk, dig, ldk, plane, rowscale, rows_pad);
+    i8_cut_body(src, lds, R, K, dig, ldk, plane, rowscale);
 }
 
-__global__ void __launch_bounds__(256) kg_i8_digits(const I8SplitTask *__restrict__ tk, int R, int K, int nchunk) {
+// grouped (blockIdx.z = case; a cluster never spans two cases)
+__global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
+    kg_i8_cut(const I8SplitTask *__restrict__ tk, int R, int K) {
     const I8SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
-    if (t.gate && !*t.gate) return;
-    i8_digits_body(t.src, t.lds, R, K, t.cmax, nchunk, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale,
-                   t.rows_pad);
+    if (t.gate && !*t.gate) return;   // the whole cluster: one case
+    i8_cut_body(t.src, t.lds, R, K, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale);
 }
 
+// BN: output tile width, 64 or 48 (a 128 x 48 tile puts 132 CTAs on a
+// 768 x 1024 product where 128 x 64 tiles leave a third of the 148 SMs idle)
+template <int BN>
 struct I8Cfg {
     static constexpr uint32_t kATile = 128 * kI8BK;                 // one A digit slice: 128 rows x 128 B
-    static constexpr uint32_t kBSlice = kI8BN * kI8BK;              // one B digit slice
-    static constexpr uint32_t kBStage = kI8S * kI8BN * kI8BK;       // all B slices of a k-block
-    static constexpr int kASlots = 5;
+    static constexpr uint32_t kBSlice = BN * kI8BK;                 // one B digit slice
+    static constexpr uint32_t kBStage = kI8S * BN * kI8BK;          // all B slices of a k-block
+    // as many A slots as the shared memory holds beside two B stages
+    static constexpr int kASlots = static_cast<int>((227u * 1024u - 1280u - 2u * kBStage) / kATile);
     static constexpr size_t kSmem = 2 * kBStage + kASlots * kATile + 1024 + 256;
-    static constexpr uint32_t kTmemCols = kI8S * kI8BN;             // one s32 accumulator per digit-weight class
+    static constexpr uint32_t kTmemCols = 512;                      // kI8S class accumulators of BN columns
     // D s32 (2), A and B signed 8-bit (1), both K-major, M = 128; N set per MMA
     static constexpr uint32_t kIdescBase = (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(128 >> 4) << 24);
-    static_assert(kTmemCols == 512, "TMEM columns");
-    static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
+    static_assert(kI8S * BN <= 512, "TMEM columns");
+    static_assert(BN % 16 == 0 && 4 * BN <= 256, "MMA N of four slices: a multiple of 16, at most 256");
+    static_assert(kASlots >= 2 && kSmem <= 227 * 1024, "shared memory per CTA");
 };
 
-// One CTA per 128 x kI8BN tile of C.  Per k-block of 128: the producer
+// One CTA per 128 x BN tile of C.  Per k-block of 128: the producer
 // thread loads all B slices (one barrier) and streams the A slices through
 // a ring; the MMA thread multiplies A slice i with B slices j < kI8S - i into
 // accumulators i + j (MMAs of K = 32 over up to four slices at once).  Every wait gives up after one
 // second with FB_ERR_TIMEOUT.
-template <bool kGlobalMaps>
+template <int BN, bool kGlobalMaps>
 __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorMap *mb, const I8Out &o, int K,
                                           int *status) {
-    using Cfg = I8Cfg;
+    using Cfg = I8Cfg<BN>;
     constexpr int kS = kI8S, kAS = Cfg::kASlots;
     extern __shared__ uint8_t smraw[];
     const uint32_t raw = smem_u32(smraw);
@@ -797,7 +790,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     const uint32_t afull0 = smem_u32(bars + 4), aempty0 = smem_u32(bars + 4 + kAS), done = smem_u32(bars + 4 + 2 * kAS);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * kI8BN;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN;
     const int nk = (K + kI8BK - 1) / kI8BK;
 
     if (threadIdx.x == 0) {
@@ -876,11 +869,11 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
                 const uint32_t ast = sA + slot * Cfg::kATile;
                 // B slices j0 .. j0+nsl-1 are consecutive rows in shared memory and
                 // their classes i+j0 .. consecutive TMEM column blocks: one MMA of
-                // N = nsl * kI8BN covers up to four digit pairs
+                // N = nsl * BN covers up to four digit pairs
                 for (int j0 = 0; j0 < kS - i; j0 += 4) {
                     const int nsl = min(4, kS - i - j0);
-                    const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * kI8BN) >> 3) << 17);
-                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * kI8BN);
+                    const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * BN) >> 3) << 17);
+                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * BN);
 #pragma unroll
                     for (int kk = 0; kk < kI8BK / 32; ++kk) {   // K = 32 bytes per MMA
                         const uint64_t a = sw128_desc(ast + 32 * kk);
@@ -905,15 +898,17 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     const int row = m0 + warp * 32 + lane;
     const bool rok = ok && row < o.M;
     const double rs = rok ? o.rowscale[row] : 0.0;
+    // 32 columns at a time; with BN = 48 the second load also reads the next
+    // class's first 16 columns (inside the allocation), which are not used
 #pragma unroll 1
-    for (int c = 0; c < kI8BN / 32; ++c) {
+    for (int c = 0; c < (BN + 31) / 32; ++c) {
         double acc[32];
 #pragma unroll
         for (int q = 0; q < 32; ++q) acc[q] = 0.0;
 #pragma unroll 1
         for (int t = kS - 1; t >= 0; --t) {
             uint32_t v[32];
-            tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * kI8BN + c * 32), v);
+            tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * BN + c * 32), v);
             const double wgt = ldexp(1.0, -7 * (t + 2));
 #pragma unroll
             for (int q = 0; q < 32; ++q) acc[q] = acc[q] + static_cast<double>(static_cast<int32_t>(v[q])) * wgt;
@@ -922,7 +917,8 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
 #pragma unroll
             for (int q = 0; q < 32; ++q) {
                 const int col = n0 + c * 32 + q;
-                if (col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
+                if (c * 32 + q < BN && col < o.N)
+                    o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
             }
         }
     }
@@ -935,20 +931,22 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     }
 }
 
+template <int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
                 int *status) {
     FB_GRID_WAIT();
-    i8x8_body<false>(&ma, &mb, o, K, status);
+    i8x8_body<BN, false>(&ma, &mb, o, K, status);
 }
 
 // grouped: blockIdx.z selects the product
+template <int BN>
 __global__ void __launch_bounds__(kThreads, 1) kg_i8x8_gemm(const I8Task *__restrict__ t) {
     FB_GRID_WAIT();
     const I8Task &tk = t[blockIdx.z];
     if (tk.gate && !*tk.gate) return;
     const I8Out o = tk.o;
-    i8x8_body<true>(&tk.a, &tk.b, o, tk.K, tk.status);
+    i8x8_body<BN, true>(&tk.a, &tk.b, o, tk.K, tk.status);
 }
 
 void launch_poisson_residual(const Dev &d, const double *phi, const SplitPlane &dst, cudaStream_t st,
@@ -1086,6 +1084,7 @@ void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane 
 // ---- INT8 FP64 products: buffers, maps, launches
 int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
     if (K > kI8MaxK) return FB_ERR_UNSUPPORTED;   // the int32 class sums would overflow
+    if (box_rows != 128 && box_rows != 64 && box_rows != 48) return FB_ERR_STATE;
     if (!p.dig || (p.ldk % 128) || p.rows_pad < rows) return FB_ERR_STATE;
     if (!g_encode) {
         void *fn = nullptr;
@@ -1107,41 +1106,43 @@ int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     p.rows = rows;
     p.K = K;
+    p.box = box_rows;
     return r == CUDA_SUCCESS ? FB_OK : FB_ERR_CUDA;
 }
 
 int i8_configure() {
-    const bool ok = cudaFuncSetAttribute(k_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(I8Cfg::kSmem)) == cudaSuccess &&
-                    cudaFuncSetAttribute(kg_i8x8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(I8Cfg::kSmem)) == cudaSuccess;
+    const bool ok = cudaFuncSetAttribute(k_i8x8_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<64>::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(kg_i8x8_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<64>::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(k_i8x8_gemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<48>::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(kg_i8x8_gemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<48>::kSmem)) == cudaSuccess;
     return ok ? FB_OK : FB_ERR_CUDA;
 }
 
 void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st) {
-    const int nchunk = (K + kI8Chunk - 1) / kI8Chunk;
-    pdl(kg_i8_rowmax, dim3(rep.rows_pad / 32, nchunk, n), dim3(256), 0, st, tasks, R, K);
-    pdl(kg_i8_digits, dim3(rep.rows_pad / 32, static_cast<unsigned>(rep.ldk / 32), n), dim3(256), 0, st, tasks, R, K,
-        nchunk);
+    pdl(kg_i8_cut, dim3(rep.rows_pad / 32 * kCutCl, 1, n), dim3(256), 0, st, tasks, R, K);
 }
 
-void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, cudaStream_t st) {
-    const dim3 grid((M + 127) / 128, (N + kI8BN - 1) / kI8BN, n);
-    pdl(kg_i8x8_gemm, grid, dim3(kThreads), I8Cfg::kSmem, st, tasks);
+void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st) {
+    const dim3 grid((M + 127) / 128, (N + bn - 1) / bn, n);
+    if (bn == 48) pdl(kg_i8x8_gemm<48>, grid, dim3(kThreads), I8Cfg<48>::kSmem, st, tasks);
+    else pdl(kg_i8x8_gemm<64>, grid, dim3(kThreads), I8Cfg<64>::kSmem, st, tasks);
 }
 
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {
-    const int nchunk = (K + kI8Chunk - 1) / kI8Chunk;
-    pdl(k_i8_rowmax, dim3(p.rows_pad / 32, nchunk), dim3(256), 0, st, src, lds, R, K, p.cmax, p.rows_pad);
-    pdl(k_i8_digits, dim3(p.rows_pad / 32, static_cast<unsigned>(p.ldk / 32)), dim3(256), 0, st, src, lds, R, K,
-        static_cast<const double *>(p.cmax), nchunk, p.dig, p.ldk, p.ldk * static_cast<long>(p.rows_pad), p.scale,
-        p.rows_pad);
+    pdl(k_i8_cut, dim3(p.rows_pad / 32 * kCutCl), dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk,
+        p.ldk * static_cast<long>(p.rows_pad), p.scale);
 }
 
+// the tile width is the B operand's box height (i8_plan)
 void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st) {
     I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows};
-    const dim3 grid((a.rows + 127) / 128, (b.rows + kI8BN - 1) / kI8BN);
-    pdl(k_i8x8_gemm, grid, dim3(kThreads), I8Cfg::kSmem, st, a.map, b.map, o, a.K, status);
+    const dim3 grid((a.rows + 127) / 128, (b.rows + b.box - 1) / b.box);
+    if (b.box == 48) pdl(k_i8x8_gemm<48>, grid, dim3(kThreads), I8Cfg<48>::kSmem, st, a.map, b.map, o, a.K, status);
+    else pdl(k_i8x8_gemm<64>, grid, dim3(kThreads), I8Cfg<64>::kSmem, st, a.map, b.map, o, a.K, status);
 }
 
 }  // namespace fb

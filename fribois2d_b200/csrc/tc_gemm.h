@@ -61,8 +61,7 @@ struct ResidualTask {    // one Poisson residual: phi -> hi, lo (ldd), row facto
 // rows_pad x ldk bytes (ldk a multiple of 128), 2^e per row, its tensor map.
 constexpr int kI8S = 8;       // digit slices per operand
 constexpr int kI8BK = 128;    // K bytes per k-block (one 128-byte swizzle row)
-constexpr int kI8BN = 64;     // output tile width
-constexpr int kI8Chunk = 64;  // columns per row-maximum block of the digit split
+constexpr int kI8BN = 64;     // output tile width (the default; 48 is the other choice)
 // Largest K of one product: weight class t = kI8S - 1 sums kI8S digit pairs
 // of at most 127 * 127 per k into an int32 TMEM accumulator, so
 // K * kI8S * 127^2 must stay below 2^31 (K <= 16642); i8_plan rejects more.
@@ -71,9 +70,9 @@ struct I8Plan {
     CUtensorMap map;
     int8_t *dig;
     double *scale;            // 2^e(row)
-    double *cmax;             // split scratch: row maxima per kI8Chunk columns, [chunk][rows_pad]
     long ldk;
     int rows_pad, rows, K;
+    int box;                  // rows per TMA box: 128 (A) or the output tile width (B: 48 or 64)
 };
 struct I8Out {
     double *out;
@@ -87,7 +86,7 @@ struct I8SplitTask {
     long lds;
     int8_t *dig;
     long ldk;
-    double *scale, *cmax;
+    double *scale;
     int rows_pad;
     const int *gate;
 };
@@ -99,7 +98,7 @@ struct I8Task {
     const int *gate;
 };
 int i8_configure();
-// box_rows: 128 for the A operand, kI8BN for B
+// box_rows: 128 for the A operand, the output tile width (48 or 64) for B
 int i8_plan(I8Plan &p, int rows, int K, int box_rows);
 // digits of the column-major source A(r, k) = src[k * lds + r], r < R, k < K
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
@@ -107,7 +106,7 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
 void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st);
 // the same over n cases of one shape (rep: geometry of the split)
 void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st);
-void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, cudaStream_t st);
+void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st);
 
 int tf32x3_configure();
 bool tf32x3_shape_ok(int bn);

@@ -112,7 +112,14 @@ class Predictor:
     final_loss: float
 
 
-def predictable(t: np.ndarray, bound: float = 1.0) -> np.ndarray:
+# The network's residual, in units of the history's scale, is trained and
+# applied within this bound (couple.cu clamps to the same value): on smooth
+# steps the prior's residual is ~1e-3 of that scale, and beyond a few
+# hundredths it is a jump of the loads that no smooth history predicts.
+RESIDUAL_BOUND = 0.02
+
+
+def predictable(t: np.ndarray, bound: float = RESIDUAL_BOUND) -> np.ndarray:
     """Samples whose targets (the prior's residuals, in units of the history's
     scale) are within `bound`: the steps a smooth history can predict.  The
     rest -- jumps of the loads as markers cross grid lines -- are left out of

@@ -268,7 +268,7 @@ int fb_last_advance_ms(fb_ctx *ctx, double *ms);
 #define FB_TK_POISSON_TRI 101 /* phcalc_outflow.F90:34-56 per-mode y solves */
 #define FB_TK_GEMM_BWD 102   /* phcalc_outflow.F90:61 back transform */
 #define FB_TK_TF32X3_GEMM 103 /* one 3xTF32 tensor-core transform (precision form) */
-#define FB_TK_I8_SPLIT 104    /* digit cut of dph for the INT8 transform (two launches) */
+#define FB_TK_I8_SPLIT 104    /* digit cut of dph for the INT8 transform */
 #define FB_TK_I8X8_GEMM 105   /* one INT8 digit-slice transform, hmn = dph zmmt^T */
 int fb_time_stage(fb_ctx *ctx, int stage, int n, int reps, double *ms);
 /* Number of this library's own kernels one captured time step launches

@@ -125,22 +125,30 @@ def test_coupled_batch_matches_separate_runs(tmp_path):
 
 def test_learned_predictor_reduces_fluid_solves():
     """Trains the perceptron on the solver's own coupled steps (a seeded
-    sweep run as one coupled batch) and runs a case outside the sweep with
+    sweep run as one coupled batch) and runs cases outside the sweep with
     it.  Under the unchanged 1e-8 convergence test the learned initial guess
-    must need strictly fewer fluid solves per step than the plain
-    (extrapolating) one, and start closer to the converged load."""
+    (structured prior + the network's residual) must need clearly fewer
+    fluid solves per step than the plain (extrapolating) one.  What the
+    network adds to its prior is measured too (the learned mode without a
+    network runs the prior alone) and must not cost solves."""
     train_cases = learn.sweep(24, seed=0)
     x, t, plain_train = learn.generate(train_cases, steps=400)
     assert x.shape == (t.shape[0], 27) and x.shape[0] > 5000
-    pred = learn.train(x, t, epochs=60, batch=256, lr=2e-3, seed=0)
-    held_out = learn.sweep(1, seed=99)[0]
-    plain, h0, r_plain = learn.mean_solves(held_out, 300, skip=20)
-    learned, h1, r_learned = learn.mean_solves(held_out, 300, pred, skip=20)
+    pred = learn.train(x, t, epochs=30, batch=256, lr=2e-3, seed=0)
     col = fb.HIST_NAMES.index("solves")
-    assert np.all(h1[:, col] < 50) and np.all(h0[:, col] < 50)
-    print(f"training: {x.shape[0]} samples, plain predictor {plain_train:.3f} solves/step; "
-          f"held-out case, mean solves/step after step 20: plain {plain:.3f} learned {learned:.3f}; "
-          f"initial load residual: plain {r_plain:.3e} learned {r_learned:.3e}")
-    assert learned < plain - 0.05, (learned, plain)
-    assert r_learned < r_plain
+    rows = []
+    for seed in (99, 98, 97):
+        held_out = learn.sweep(1, seed=seed)[0]
+        plain, h0, _ = learn.mean_solves(held_out, 300, skip=20)
+        prior, h1, _ = learn.mean_solves(held_out, 300, "prior", skip=20)
+        learned, h2, _ = learn.mean_solves(held_out, 300, pred, skip=20)
+        for h in (h0, h1, h2):
+            assert np.all(h[:, col] < 50)
+        rows.append((plain, prior, learned))
+    plain, prior, learned = np.mean(rows, axis=0)
+    print(f"training: {x.shape[0]} samples ({learn.predictable(t).mean():.2f} predictable), plain predictor "
+          f"{plain_train:.3f} solves/step; held-out cases, mean solves/step after step 20: plain {plain:.3f}, "
+          f"prior alone {prior:.3f}, learned (prior + network) {learned:.3f}; per case {rows}")
+    assert learned < plain - 0.1, (learned, plain)
+    assert learned <= prior + 0.05, (learned, prior)
     pred.mlp.close()
