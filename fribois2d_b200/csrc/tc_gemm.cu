@@ -661,13 +661,17 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // 2^-55 of its largest entry.
 
 // The digit cut in one launch: a cluster of kCutCl CTAs per 32 rows, each
-// CTA over its own range of columns.  Every CTA takes the maxima of |A(r, k)|
-// of its columns, the cluster exchanges them through distributed shared
-// memory (so every CTA derives each row's exponent from the whole row), and
-// each CTA cuts the digits of its columns: the operand is read once.
-// Columns past K and rows past R get zero digits, up to ldk and rows_pad.
+// CTA over its own range of 8 V columns.  Thread (lane, warp w) holds row
+// lane's columns c0 + w + 8 q, q < V, in registers (all its loads in flight
+// at once); the CTA's row maxima go to the cluster through distributed
+// shared memory, so every CTA derives each row's exponent from the whole
+// row; then each CTA cuts the digits from its registers and writes them one
+// slice at a time through a shared-memory transpose (16-byte stores along
+// k).  The operand is read once.  Columns past K and rows past R get zero
+// digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
+template <int V>
 __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long lds, int R, int K, int8_t *dig,
                                             long ldk, long plane, double *rowscale) {
     namespace cg = cooperative_groups;
@@ -675,16 +679,20 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
-    __shared__ uint32_t tile[kI8S][32][9];   // 4 digits per word, rows padded to 9 words
+    __shared__ __align__(16) uint8_t buf[32][8 * V];   // one digit slice of the CTA's rows x columns
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int rank = static_cast<int>(cl.block_rank());
     const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
-    // this CTA's columns: whole 32-column tiles
-    const int tiles = static_cast<int>(ldk / 32), per = (tiles + kCutCl - 1) / kCutCl;
-    const int t0 = min(tiles, rank * per), t1 = min(tiles, t0 + per);
+    const int c0 = rank * 8 * V;
+    double a[V];
     double m = 0.0;
-    if (r < R)
-        for (int k = t0 * 32 + w; k < min(K, t1 * 32); k += 8) m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+        const int k = c0 + w + 8 * q;
+        a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < V; ++q) m = fmax(m, fabs(a[q]));
     mx[w][lane] = m;
     __syncthreads();
     if (w == 0) {
@@ -702,52 +710,51 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     }
     cl.sync();   // no CTA leaves while another still reads its maxima
     const double s = sc[lane];
-    for (int tt = t0; tt < t1; ++tt) {
-        const int k0 = tt * 32;
-        // thread (lane, w): row r, columns k0 + 4w .. k0 + 4w + 3 (loads coalesced over the rows)
-        double a[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = k0 + 4 * w + q;
-            a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] * s : 0.0;
-        }
+    for (int q = 0; q < V; ++q) a[q] = a[q] * s;
+    // this CTA's columns that lie inside ldk, in 16-byte pieces per row
+    const int ncol = static_cast<int>(max(0L, min(static_cast<long>(8 * V), ldk - c0)));
+    const int pieces = ncol / 16;
+    for (int i = 0; i < kI8S; ++i) {
 #pragma unroll
-        for (int i = 0; i < kI8S; ++i) {
-            uint32_t word = 0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = a[q] * 128.0;
-                const double d = trunc(a[q]);
-                a[q] = a[q] - d;
-                word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
-            }
-            tile[i][lane][w] = word;
+        for (int q = 0; q < V; ++q) {
+            a[q] = a[q] * 128.0;
+            const double d = trunc(a[q]);
+            a[q] = a[q] - d;
+            buf[lane][w + 8 * q] = static_cast<uint8_t>(static_cast<int8_t>(d));
         }
         __syncthreads();
-        {   // slice i = w, row lane: 32 bytes
-            const uint32_t *t = &tile[w][lane][0];
-            uint4 *o = reinterpret_cast<uint4 *>(dig + static_cast<size_t>(w) * plane + static_cast<size_t>(r0 + lane) * ldk + k0);
-            o[0] = make_uint4(t[0], t[1], t[2], t[3]);
-            o[1] = make_uint4(t[4], t[5], t[6], t[7]);
+        for (int p = threadIdx.x; p < 32 * pieces; p += blockDim.x) {
+            const int row = p / pieces, pc = p - row * pieces;
+            *reinterpret_cast<uint4 *>(dig + static_cast<size_t>(i) * plane + static_cast<size_t>(r0 + row) * ldk + c0 +
+                                       16 * pc) = *reinterpret_cast<const uint4 *>(&buf[row][16 * pc]);
         }
         __syncthreads();
     }
 }
 
+template <int V>
 __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
     k_i8_cut(const double *__restrict__ src, long lds, int R, int K, int8_t *dig, long ldk, long plane,
              double *rowscale) {
     FB_GRID_WAIT();
-    i8_cut_body(src, lds, R, K, dig, ldk, plane, rowscale);
+    i8_cut_body<V>(src, lds, R, K, dig, ldk, plane, rowscale);
 }
 
 // grouped (blockIdx.z = case; a cluster never spans two cases)
+template <int V>
 __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
     kg_i8_cut(const I8SplitTask *__restrict__ tk, int R, int K) {
     const I8SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
     if (t.gate && !*t.gate) return;   // the whole cluster: one case
-    i8_cut_body(t.src, t.lds, R, K, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale);
+    i8_cut_body<V>(t.src, t.lds, R, K, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale);
+}
+
+// columns per thread: the CTA's share of ldk over its 8 warps
+inline int cut_values(long ldk) {
+    const long per = (ldk + 8 * kCutCl - 1) / (8 * kCutCl);
+    return per <= 4 ? 4 : per <= 8 ? 8 : per <= 16 ? 16 : per <= 32 ? 32 : 64;
 }
 
 // BN: output tile width, 64 or 48 (a 128 x 48 tile puts 132 CTAs on a
@@ -1123,7 +1130,14 @@ int i8_configure() {
 }
 
 void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st) {
-    pdl(kg_i8_cut, dim3(rep.rows_pad / 32 * kCutCl, 1, n), dim3(256), 0, st, tasks, R, K);
+    const dim3 grid(rep.rows_pad / 32 * kCutCl, 1, n);
+    switch (cut_values(rep.ldk)) {
+    case 4: pdl(kg_i8_cut<4>, grid, dim3(256), 0, st, tasks, R, K); break;
+    case 8: pdl(kg_i8_cut<8>, grid, dim3(256), 0, st, tasks, R, K); break;
+    case 16: pdl(kg_i8_cut<16>, grid, dim3(256), 0, st, tasks, R, K); break;
+    case 32: pdl(kg_i8_cut<32>, grid, dim3(256), 0, st, tasks, R, K); break;
+    default: pdl(kg_i8_cut<64>, grid, dim3(256), 0, st, tasks, R, K); break;
+    }
 }
 
 void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st) {
@@ -1133,8 +1147,15 @@ void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStr
 }
 
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {
-    pdl(k_i8_cut, dim3(p.rows_pad / 32 * kCutCl), dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk,
-        p.ldk * static_cast<long>(p.rows_pad), p.scale);
+    const dim3 grid(p.rows_pad / 32 * kCutCl);
+    const long plane = p.ldk * static_cast<long>(p.rows_pad);
+    switch (cut_values(p.ldk)) {
+    case 4: pdl(k_i8_cut<4>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+    case 8: pdl(k_i8_cut<8>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+    case 16: pdl(k_i8_cut<16>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+    case 32: pdl(k_i8_cut<32>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+    default: pdl(k_i8_cut<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+    }
 }
 
 // the tile width is the B operand's box height (i8_plan)

@@ -307,12 +307,14 @@ __device__ __forceinline__ void block_lines(double (&v)[M], int i0, int cnt, con
 // kKind 0: the v and w systems of helsolve in one launch (solq2j on rows
 // k = 1..n3m of rhs2, then solq3j on rows k = 2..n3m of rhs3; they are
 // independent).  kKind 2: Poisson modes (rows of hmn).
-template <int M, int kKind>
+// W: warps per line (the Poisson modes use 4: fewer values and registers per
+// thread, more lines resident per SM)
+template <int M, int kKind, int W = kYWarps>
 __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, const double *by2, const ScanSys &s3, const double *by3) {
     extern __shared__ double sm[];
-    __shared__ double shx[kYLines][2 * kYWarps];
-    const int wl = (threadIdx.x >> 5) / kYWarps;       // line slot in the block
-    const int tl = threadIdx.x % (32 * kYWarps);       // thread within the line group
+    __shared__ double shx[kYLines][2 * W];
+    const int wl = (threadIdx.x >> 5) / W;       // line slot in the block
+    const int tl = threadIdx.x % (32 * W);       // thread within the line group
     int line = blockIdx.x * kYLines + wl;
     int sys = 0, n, r;
     if (kKind == 2) {
@@ -335,7 +337,7 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
     if (live) row = (kKind == 2) ? d.hmn + static_cast<size_t>(r) * d.ldh : (sys == 0 ? d.rhs2 : d.rhs3) + fidx(d, 1, r);
     const double *by = (sys == 0) ? by2 : by3;
     double *buf = sm + wl * (d.n2 + 1);
-    constexpr int kT = 32 * kYWarps;
+    constexpr int kT = 32 * W;
     // Poisson modes: the mode's reciprocal pivots and the y off-diagonals
     // are staged with the line, so the recurrences read shared memory only
     double *pgs = sm + kYLines * (d.n2 + 1) + wl * (d.n2m + 1);
@@ -372,10 +374,10 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
     for (int t = 0; t < M; ++t)
         if (t < cnt) v[t] = buf[i0 + t];
     if (kKind == 2) {
-        group_line<M, kYWarps>(v, i0, cnt, CoefModeS{pgs, ams, aps, n}, shx[wl]);
+        group_line<M, W>(v, i0, cnt, CoefModeS{pgs, ams, aps, n}, shx[wl]);
     } else {
         const ScanSys &s = (sys == 0) ? s2 : s3;
-        group_line<M, kYWarps>(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shx[wl]);
+        group_line<M, W>(v, i0, cnt, CoefShared{s.a, s.e, s.g}, shx[wl]);
     }
 #pragma unroll
     for (int t = 0; t < M; ++t)
@@ -390,10 +392,10 @@ __device__ __forceinline__ void ylines_body(const Dev &d, const ScanSys &s2, con
     }
 }
 
-template <int M, int kKind>
-__global__ void __launch_bounds__(kYLines * kYWarps * 32) k_ylines(Dev d, ScanSys s2, const double *by2, ScanSys s3, const double *by3) {
+template <int M, int kKind, int W = kYWarps>
+__global__ void __launch_bounds__(kYLines * W * 32) k_ylines(Dev d, ScanSys s2, const double *by2, ScanSys s3, const double *by3) {
     FB_GRID_WAIT();
-    ylines_body<M, kKind>(d, s2, by2, s3, by3);
+    ylines_body<M, kKind, W>(d, s2, by2, s3, by3);
 }
 
 // ---------------------------------------------------------------- z lines
@@ -765,11 +767,11 @@ __global__ void __launch_bounds__(kWThreads, 3) kg_helsolve_win(const GroupCase 
 }
 
 template <int M>
-__global__ void __launch_bounds__(kYLines * kYWarps * 32) kg_ylines_poisson(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(kYLines * kYPoissonWarps * 32) kg_ylines_poisson(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     if (!stage_case(g, &d)) return;
     const ScanSys z{nullptr, nullptr, nullptr};
-    ylines_body<M, 2>(d, z, nullptr, z, nullptr);
+    ylines_body<M, 2, kYPoissonWarps>(d, z, nullptr, z, nullptr);
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -786,17 +788,18 @@ size_t ylines_smem(const Dev &d, int kind) {
 
 template <int kKind>
 void ylaunch(const Dev &d, const SubDev *sd, cudaStream_t st) {
+    constexpr int W = (kKind == 2) ? kYPoissonWarps : kYWarps;
     const int lines = (kKind == 2) ? d.n3m : d.n3m + (d.n3m - 1);
     const int blocks = (lines + kYLines - 1) / kYLines;
-    const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
+    const int m = ((d.n2 + 32 * W - 1) / (32 * W)) | 1;
     const size_t smem = ylines_smem(d, kKind);
     const ScanSys z{nullptr, nullptr, nullptr};
     const ScanSys s2 = sd ? sd->sy2 : z, s3 = sd ? sd->sy3 : z;
     const double *b2 = sd ? sd->by2 : nullptr, *b3 = sd ? sd->by3 : nullptr;
-    const int threads = kYLines * kYWarps * 32;
-    if (m <= 9) pdl(k_ylines<9, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
-    else if (m <= 17) pdl(k_ylines<17, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
-    else pdl(k_ylines<33, kKind>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
+    const int threads = kYLines * W * 32;
+    if (m <= 9) pdl(k_ylines<9, kKind, W>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
+    else if (m <= 17) pdl(k_ylines<17, kKind, W>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
+    else pdl(k_ylines<33, kKind, W>, dim3(blocks), dim3(threads), smem, st, d, s2, b2, s3, b3);
 }
 
 void zlaunch(const Dev &d, const SubDev &sd, cudaStream_t st) {
@@ -830,7 +833,8 @@ cudaError_t scan_configure() {
 #define AL(K)                                  \
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
-    AL((k_ylines<9, 2>)) AL((k_ylines<17, 2>)) AL((k_ylines<33, 2>))
+    AL((k_ylines<9, 2, kYPoissonWarps>)) AL((k_ylines<17, 2, kYPoissonWarps>))
+    AL((k_ylines<33, 2, kYPoissonWarps>))
     AL((k_helsolve_win<12, 32>)) AL((k_helsolve_win<12, 64>))
     AL((k_helsolve_win<kWinMax, 32>)) AL((k_helsolve_win<kWinMax, 64>))
     AL((kg_helsolve_win<12, 32>)) AL((kg_helsolve_win<12, 64>))
@@ -886,9 +890,9 @@ void glaunch_win_helsolve(const Group &g, int n, cudaStream_t st) {
 void glaunch_scan_poisson(const Group &g, cudaStream_t st) {
     const Dev &d = g.rep;
     const int blocks = (d.n3m + kYLines - 1) / kYLines;
-    const int m = ((d.n2 + 32 * kYWarps - 1) / (32 * kYWarps)) | 1;
+    const int m = ((d.n2 + 32 * kYPoissonWarps - 1) / (32 * kYPoissonWarps)) | 1;
     const size_t smem = ylines_smem(d, 2);
-    const int threads = kYLines * kYWarps * 32;
+    const int threads = kYLines * kYPoissonWarps * 32;
     const dim3 grid(blocks, 1, g.n);
     if (m <= 9) pdl(kg_ylines_poisson<9>, grid, dim3(threads), smem, st, g.cases);
     else if (m <= 17) pdl(kg_ylines_poisson<17>, grid, dim3(threads), smem, st, g.cases);

@@ -9,6 +9,7 @@ namespace fb {
 
 constexpr int kYLines = 2;  // contiguous lines per block
 constexpr int kYWarps = 2;  // warps per contiguous line
+constexpr int kYPoissonWarps = 4;  // warps per line of the Poisson mode solves
 constexpr int kZLines = 4;  // strided lines per block (one warp each)
 
 constexpr int kWinMax = 24;  // longest truncation window of the windowed helsolve
