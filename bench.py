@@ -387,11 +387,13 @@ def coupled_batch_arm(args, rank, world, local):
     """Strongly coupled batch: N VIV cases of the batching form advanced
     together with the coupling iteration on the device (a graph WHILE node;
     converged cases sit out the grouped launches), with the learned initial
-    guess (or the plain one).  Reported beside the plain FP64 path -- the
-    same cases loosely coupled, each stepped alone by its own captured step --
-    and the same batch with the plain predictor; the accuracy block compares
-    a subset's lift and displacement histories with the FP64 path
-    (INT8-exact transforms, strong coupling, plain predictor)."""
+    guess (or the plain one).  All arms run on one set of cases, in turn, on
+    the continuing trajectory after a loosely coupled warm-up of W steps (a
+    developed flow, where the predictors have a history): the plain FP64
+    path with the reference's loose coupling and with strong coupling (each
+    case stepped alone by its own captured graph), then the batched form
+    with the plain and with the learned predictor.  The accuracy block runs a
+    subset from the start against the FP64 path with strong coupling."""
     import torch
     import fribois2d_b200 as fb
     from fribois2d_b200 import case as cases
@@ -415,37 +417,42 @@ def coupled_batch_arm(args, rank, world, local):
     cs = cases.viv_batch(args.batch, seed=rank)
     cells = sum(c.cells for c in cs)
     root = tempfile.mkdtemp(prefix=f"fbcbatch{rank}_")
+    form, fp64 = POISSON_IDS[args.poisson], POISSON_IDS["int8x8"]
+    svs = []
+    for c in cs:
+        sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
+        sv.set_refinement(args.sweeps)
+        q2 = sv.get("q2")
+        q2[1:c.n3m + 1] += c.v_perturbation()
+        sv.set("q2", q2)
+        svs.append(sv)
+    done = 0
 
-    def open_all(form):
-        out = []
-        for c in cs:
-            sv = fb.Solver(c.write(os.path.join(root, c.name)), device=local)
-            sv.set_poisson(POISSON_IDS[form])
-            sv.set_refinement(args.sweeps)
-            q2 = sv.get("q2")
-            q2[1:c.n3m + 1] += c.v_perturbation()
-            sv.set("q2", q2)
-            out.append(sv)
-        return out
+    def solves_of(before):
+        after = [sv.coupling_stats() for sv in svs]
+        n = sum(a["solves"] - q["solves"] for a, q in zip(after, before))
+        k = sum(a["steps"] - q["steps"] for a, q in zip(after, before))
+        return n / max(k, 1.0)
 
-    # the plain FP64 path: each case loosely coupled, stepped alone
-    solvers = open_all("int8x8")
-    seq_ms = 0.0
-    for sv in solvers:
-        sv.advance(0, W)
-        sv.advance(W, K, history=False)
-        seq_ms += sv.last_advance_ms()
-        sv.close()
-
-    def coupled_run(mode, predictor):
-        svs = open_all(args.poisson)
+    def sequential():   # each case alone, its own captured graph
+        nonlocal done
+        ms = 0.0
         for sv in svs:
+            sv.set_poisson(fp64)
+            sv.advance(done, K, history=False)
+            ms += sv.last_advance_ms()
+        done += K
+        return ms
+
+    def batched(mode, predictor):
+        nonlocal done
+        for sv in svs:
+            sv.set_poisson(form)
             sv.set_coupling(mode, 1e-8)
             if predictor is not None:
                 sv.set_predictor(predictor.mlp, predictor.norm)
         b = fb.Batch(svs)
         info = b.info()
-        b.advance(W)
         before = [sv.coupling_stats() for sv in svs]
         clocks = ClockSampler(local)
         torch.cuda.synchronize(dev)
@@ -453,31 +460,44 @@ def coupled_batch_arm(args, rank, world, local):
         b.advance(K)
         clk = clocks.stop()
         ms = b.last_ms()
-        after = [sv.coupling_stats() for sv in svs]
-        solves = sum(a["solves"] - q["solves"] for a, q in zip(after, before))
-        steps = sum(a["steps"] - q["steps"] for a, q in zip(after, before))
         b.close()
-        for sv in svs:
-            sv.close()
-        return ms, solves / max(steps, 1.0), info, clk
+        done += K
+        return ms, solves_of(before), info, clk
 
-    mode = fb.COUPLING_LEARNED if pred is not None else fb.COUPLING_STRONG
-    ms, solves, info, clk = coupled_run(mode, pred)
-    plain_ms, plain_solves = None, None
+    # loosely coupled warm-up as a batch in the FP64 form: a developed flow
+    for sv in svs:
+        sv.set_poisson(fp64)
+    wb = fb.Batch(svs)
+    wb.advance(W)
+    wb.close()
+    done += W
+    seq_loose_ms = sequential()
+    for sv in svs:
+        sv.set_coupling(fb.COUPLING_STRONG, 1e-8)
+    before = [sv.coupling_stats() for sv in svs]
+    seq_coupled_ms = sequential()
+    seq_coupled_solves = solves_of(before)
+    plain_ms, plain_solves, _, _ = batched(fb.COUPLING_STRONG, None)
+    ms, solves, info, clk = plain_ms, plain_solves, None, None
     if pred is not None:
-        plain_ms, plain_solves, _, _ = coupled_run(fb.COUPLING_STRONG, None)
-    # accuracy: a subset against the FP64 path, each case alone
+        ms, solves, info, clk = batched(fb.COUPLING_LEARNED, pred)
+    else:
+        ms, solves, info, clk = batched(fb.COUPLING_STRONG, None)
+    for sv in svs:
+        sv.close()
+    # accuracy: a subset from the start against the FP64 path, each case alone
     acc = None
+    mode = fb.COUPLING_LEARNED if pred is not None else fb.COUPLING_STRONG
     if args.accuracy_steps > 0:
         picks = []
         for n3, n2, _ in cases.BATCH_GRIDS:
             picks += [c for c in cs if (c.n3m, c.n2m) == (n3, n2)][:2]
         worst_f = worst_d = 0.0
         for c in picks:
-            hs = {}
-            for form, md, pr_ in (("int8x8", fb.COUPLING_STRONG, None), (args.poisson, mode, pred)):
+            hs = []
+            for pform, md, pr_ in ((fp64, fb.COUPLING_STRONG, None), (form, mode, pred)):
                 sv = fb.Solver(c.write(os.path.join(root, "acc_" + c.name)), device=local)
-                sv.set_poisson(POISSON_IDS[form])
+                sv.set_poisson(pform)
                 sv.set_refinement(args.sweeps)
                 q2 = sv.get("q2")
                 q2[1:c.n3m + 1] += c.v_perturbation()
@@ -485,9 +505,9 @@ def coupled_batch_arm(args, rank, world, local):
                 sv.set_coupling(md, 1e-8)
                 if pr_ is not None:
                     sv.set_predictor(pr_.mlp, pr_.norm)
-                hs[form + str(md)] = sv.advance(0, args.accuracy_steps)
+                hs.append(sv.advance(0, args.accuracy_steps))
                 sv.close()
-            a, b_ = list(hs.values())
+            a, b_ = hs
             f_ref, d_ref = a[:, 1], a[:, 9]
             worst_f = max(worst_f, float(np.max(np.abs(b_[:, 1] - f_ref)) / max(np.ptp(f_ref), 1e-300)))
             worst_d = max(worst_d, float(np.max(np.abs(b_[:, 9] - d_ref)) / max(np.ptp(d_ref), 1e-300)))
@@ -496,7 +516,8 @@ def coupled_batch_arm(args, rank, world, local):
                "reference": "FP64 device path (INT8-exact transforms), strong coupling, plain predictor; "
                             "its coupled steps follow the oracle's fbo_coupled_step to round-off (tests)"}
     value = cells * K / (ms * 1e-3)
-    seq_value = cells * K / (seq_ms * 1e-3)
+    seq_loose = cells * K / (seq_loose_ms * 1e-3)
+    seq_coupled = cells * K / (seq_coupled_ms * 1e-3)
     line = {
         "metric": f"cell-steps/s (batch of {args.batch} VIV cases, {FORMS[args.poisson]}, strong coupling, "
                   f"{'learned' if pred is not None else 'plain'} predictor)",
@@ -507,15 +528,20 @@ def coupled_batch_arm(args, rank, world, local):
                    "grids": {f"{n3}x{n2}": sum(1 for c in cs if (c.n3m, c.n2m) == (n3, n2))
                              for n3, n2, _ in cases.BATCH_GRIDS},
                    "groups": info["groups"], "poisson": args.poisson, "coupling": args.coupling,
-                   "tol": 1e-8, "l2": "working set far above L2 (all cases resident)"},
+                   "tol": 1e-8, "l2": "working set far above L2 (all cases resident)",
+                   "warmup": f"{W} loosely coupled steps as a batch, then each arm {K} steps in turn"},
         "fluid_solves_per_step": solves,
-        "plain_fp64_sequential": {"value": seq_value, "ms_per_step": seq_ms / K,
+        "plain_fp64_sequential": {"value": seq_loose, "ms_per_step": seq_loose_ms / K,
                                   "note": "the same cases, FP64 (INT8-exact transforms), loose coupling as the "
                                           "reference, each advanced alone by its own captured step"},
-        "speedup_vs_plain_fp64": value / seq_value,
-        "plain_predictor": None if plain_ms is None else {
-            "value": cells * K / (plain_ms * 1e-3), "ms_per_step": plain_ms / K,
-            "fluid_solves_per_step": plain_solves},
+        "plain_fp64_coupled_sequential": {"value": seq_coupled, "ms_per_step": seq_coupled_ms / K,
+                                          "fluid_solves_per_step": seq_coupled_solves,
+                                          "note": "the same cases, FP64, strong coupling with the plain "
+                                                  "predictor, each advanced alone"},
+        "speedup_vs_plain_fp64": value / seq_loose,
+        "speedup_vs_plain_fp64_coupled": value / seq_coupled,
+        "batched_plain_predictor": {"value": cells * K / (plain_ms * 1e-3), "ms_per_step": plain_ms / K,
+                                    "fluid_solves_per_step": plain_solves},
         "training": train, "accuracy": acc,
         "gpu_launches": info["launches"] * K, "clocks": clk,
     }

@@ -662,13 +662,14 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 
 // The digit cut in one launch: a cluster of kCutCl CTAs per 32 rows, each
 // CTA over its own range of 8 V columns.  Thread (lane, warp w) holds row
-// lane's columns c0 + w + 8 q, q < V, in registers (all its loads in flight
-// at once); the CTA's row maxima go to the cluster through distributed
-// shared memory, so every CTA derives each row's exponent from the whole
-// row; then each CTA cuts the digits from its registers and writes them one
-// slice at a time through a shared-memory transpose (16-byte stores along
-// k).  The operand is read once.  Columns past K and rows past R get zero
-// digits, up to ldk and rows_pad.
+// lane's columns c0 + 32 p + 4 w + q (p < V / 4, q < 4) in registers, all
+// its loads in flight at once (each load coalesced over the 32 rows); the
+// CTA's row maxima go to the cluster through distributed shared memory, so
+// every CTA derives each row's exponent from the whole row; then each CTA
+// cuts the digits from its registers, four columns to a 32-bit word, and
+// writes one slice at a time through shared memory (rows of 2 V + 1 words:
+// conflict-free) with coalesced stores along k.  The operand is read once.
+// Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
 template <int V>
@@ -676,23 +677,28 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
                                             long ldk, long plane, double *rowscale) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
+    constexpr int kP = V / 4, kRow = 2 * V + 1;   // words per row of the slice buffer (odd)
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
-    __shared__ __align__(16) uint8_t buf[32][8 * V];   // one digit slice of the CTA's rows x columns
+    __shared__ uint32_t buf[32 * kRow];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int rank = static_cast<int>(cl.block_rank());
     const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
     const int c0 = rank * 8 * V;
-    double a[V];
+    double a[kP][4];
     double m = 0.0;
 #pragma unroll
-    for (int q = 0; q < V; ++q) {
-        const int k = c0 + w + 8 * q;
-        a[q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
-    }
+    for (int p = 0; p < kP; ++p)
 #pragma unroll
-    for (int q = 0; q < V; ++q) m = fmax(m, fabs(a[q]));
+        for (int q = 0; q < 4; ++q) {
+            const int k = c0 + 32 * p + 4 * w + q;
+            a[p][q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
+        }
+#pragma unroll
+    for (int p = 0; p < kP; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(a[p][q]));
     mx[w][lane] = m;
     __syncthreads();
     if (w == 0) {
@@ -711,23 +717,30 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     cl.sync();   // no CTA leaves while another still reads its maxima
     const double s = sc[lane];
 #pragma unroll
-    for (int q = 0; q < V; ++q) a[q] = a[q] * s;
-    // this CTA's columns that lie inside ldk, in 16-byte pieces per row
-    const int ncol = static_cast<int>(max(0L, min(static_cast<long>(8 * V), ldk - c0)));
-    const int pieces = ncol / 16;
+    for (int p = 0; p < kP; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[p][q] = a[p][q] * s;
+    // this CTA's words that lie inside ldk, per row
+    const int nwords = static_cast<int>(max(0L, min(static_cast<long>(2 * V), (ldk - c0) / 4)));
     for (int i = 0; i < kI8S; ++i) {
 #pragma unroll
-        for (int q = 0; q < V; ++q) {
-            a[q] = a[q] * 128.0;
-            const double d = trunc(a[q]);
-            a[q] = a[q] - d;
-            buf[lane][w + 8 * q] = static_cast<uint8_t>(static_cast<int8_t>(d));
+        for (int p = 0; p < kP; ++p) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[p][q] = a[p][q] * 128.0;
+                const double d = trunc(a[p][q]);
+                a[p][q] = a[p][q] - d;
+                word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
+            }
+            buf[lane * kRow + 8 * p + w] = word;
         }
         __syncthreads();
-        for (int p = threadIdx.x; p < 32 * pieces; p += blockDim.x) {
-            const int row = p / pieces, pc = p - row * pieces;
-            *reinterpret_cast<uint4 *>(dig + static_cast<size_t>(i) * plane + static_cast<size_t>(r0 + row) * ldk + c0 +
-                                       16 * pc) = *reinterpret_cast<const uint4 *>(&buf[row][16 * pc]);
+        for (int t = threadIdx.x; t < 32 * 2 * V; t += blockDim.x) {
+            const int row = t / (2 * V), wd = t - row * (2 * V);
+            if (wd < nwords)
+                *reinterpret_cast<uint32_t *>(dig + static_cast<size_t>(i) * plane +
+                                              static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) = buf[row * kRow + wd];
         }
         __syncthreads();
     }

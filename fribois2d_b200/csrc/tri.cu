@@ -20,6 +20,8 @@
 // interleaves four lines over its lanes and splits k among its warps.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device.cuh"
 #include "pdl.h"
 #include "tri.h"
@@ -398,6 +400,106 @@ __global__ void __launch_bounds__(kYLines * W * 32) k_ylines(Dev d, ScanSys s2, 
     ylines_body<M, kKind, W>(d, s2, by2, s3, by3);
 }
 
+// ---------------------------------------------------------------- Poisson modes
+
+// The per-mode y solves of phcalc (phcalc_outflow.F90:34-56): one warp per
+// mode.  The block loads the y off-diagonals once; each warp copies its
+// mode's right-hand side (a row of hmn) and reciprocal pivots to its own
+// shared-memory rows with coalesced loads, then solves with lane chunks of
+// an odd length m (conflict-free 8-byte shared accesses): each lane composes
+// its chunk of the forward recurrence y(i) = a(i) y(i-1) + b(i),
+// a(i) = -amphj(i+1) g(i-1), the warp scans the composites, the lanes apply
+// them, scale by g(i), and do the same backward with
+// e(i) = -apphj(i+1) g(i); only warp-level synchronisation inside the
+// solve.  nw warps (modes) per block, as many as the shared memory holds.
+__device__ __forceinline__ void ymodes_body(const Dev &d, int nw) {
+    extern __shared__ double sm[];
+    const int n = d.n2m, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *am = sm, *ap = sm + (n + 2);                       // 1-based off-diagonals
+    double *line = sm + 2 * (n + 2) + static_cast<size_t>(w) * 2 * (n + 1);
+    double *piv = line + (n + 1);
+    for (int i = threadIdx.x; i <= n + 1; i += blockDim.x) {
+        am[i] = d.amphj[i];
+        ap[i] = d.apphj[i];
+    }
+    const int r = blockIdx.x * nw + w;
+    const bool live = (w < nw) && (r < d.n3m);
+    double *row = live ? d.hmn + static_cast<size_t>(r) * d.ldh : nullptr;
+    if (live) {
+        const double *pgr = d.pg + static_cast<size_t>(r) * d.ldh;
+        for (int i = lane; i < n; i += 32) {
+            line[i] = __ldcg(row + i);
+            piv[i] = __ldg(pgr + i);
+        }
+    }
+    __syncthreads();   // the off-diagonals (and every line) are staged
+    if (!live) return;
+    const int m = ((n + 31) / 32) | 1;
+    const int i0 = min(lane * m, n), cnt = min(m, n - i0);
+    // forward: composite of the chunk, y_out = A y_in + C
+    double A = 1.0, C = 0.0;
+    for (int t = 0; t < cnt; ++t) {
+        const int i = i0 + t;
+        const double a = (i == 0) ? 0.0 : -(am[i + 1] * piv[i - 1]);
+        C = fma(a, C, line[i]);
+        A *= a;
+    }
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+        const double Ao = __shfl_up_sync(kFull, A, dd), Co = __shfl_up_sync(kFull, C, dd);
+        if (lane >= dd) {
+            C = fma(A, Co, C);
+            A *= Ao;
+        }
+    }
+    double y = __shfl_up_sync(kFull, C, 1);
+    if (lane == 0) y = 0.0;
+    for (int t = 0; t < cnt; ++t) {
+        const int i = i0 + t;
+        const double a = (i == 0) ? 0.0 : -(am[i + 1] * piv[i - 1]);
+        y = fma(a, y, line[i]);
+        line[i] = piv[i] * y;   // g(i) y(i)
+    }
+    // backward: x(i) = e(i) x(i+1) + g(i) y(i)
+    A = 1.0;
+    C = 0.0;
+    for (int t = cnt - 1; t >= 0; --t) {
+        const int i = i0 + t;
+        const double e = (i == n - 1) ? 0.0 : -(ap[i + 1] * piv[i]);
+        C = fma(e, C, line[i]);
+        A *= e;
+    }
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+        const double Ao = __shfl_down_sync(kFull, A, dd), Co = __shfl_down_sync(kFull, C, dd);
+        if (lane + dd < 32) {
+            C = fma(A, Co, C);
+            A *= Ao;
+        }
+    }
+    double x = __shfl_down_sync(kFull, C, 1);
+    if (lane == 31) x = 0.0;
+    for (int t = cnt - 1; t >= 0; --t) {
+        const int i = i0 + t;
+        const double e = (i == n - 1) ? 0.0 : -(ap[i + 1] * piv[i]);
+        x = fma(e, x, line[i]);
+        line[i] = x;
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) row[i] = line[i];
+}
+
+__global__ void __launch_bounds__(256) k_ymodes(Dev d, int nw) {
+    FB_GRID_WAIT();
+    ymodes_body(d, nw);
+}
+
+__global__ void __launch_bounds__(256) kg_ymodes(const GroupCase *__restrict__ g, int nw) {
+    __shared__ Dev d;
+    if (!stage_case(g, &d)) return;
+    ymodes_body(d, nw);
+}
+
 // ---------------------------------------------------------------- z lines
 
 // solq2k (+ helsolve wall columns) on blocks [0, nb2) and solq3k on the
@@ -766,13 +868,6 @@ __global__ void __launch_bounds__(kWThreads, 3) kg_helsolve_win(const GroupCase 
     helsolve_win_body<KM, kWTk>(d, s, ntj, s.win_y, s.win_z);
 }
 
-template <int M>
-__global__ void __launch_bounds__(kYLines * kYPoissonWarps * 32) kg_ylines_poisson(const GroupCase *__restrict__ g) {
-    __shared__ Dev d;
-    if (!stage_case(g, &d)) return;
-    const ScanSys z{nullptr, nullptr, nullptr};
-    ylines_body<M, 2, kYPoissonWarps>(d, z, nullptr, z, nullptr);
-}
 
 // ---------------------------------------------------------------- dispatch
 
@@ -833,13 +928,13 @@ cudaError_t scan_configure() {
 #define AL(K)                                  \
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
-    AL((k_ylines<9, 2, kYPoissonWarps>)) AL((k_ylines<17, 2, kYPoissonWarps>))
-    AL((k_ylines<33, 2, kYPoissonWarps>))
     AL((k_helsolve_win<12, 32>)) AL((k_helsolve_win<12, 64>))
     AL((k_helsolve_win<kWinMax, 32>)) AL((k_helsolve_win<kWinMax, 64>))
     AL((kg_helsolve_win<12, 32>)) AL((kg_helsolve_win<12, 64>))
     AL((kg_helsolve_win<kWinMax, 32>)) AL((kg_helsolve_win<kWinMax, 64>))
-    AL((kg_ylines_poisson<9>)) AL((kg_ylines_poisson<17>)) AL((kg_ylines_poisson<33>))
+    if ((e = cudaFuncSetAttribute(k_ymodes, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(kg_ymodes, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024)) != cudaSuccess)
+        return e;
 #undef AL
     return cudaSuccess;
 }
@@ -866,7 +961,24 @@ void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st) {
     zlaunch(d, s, st);
 }
 
-void launch_scan_poisson(const Dev &d, cudaStream_t st) { ylaunch<2>(d, nullptr, st); }
+namespace {
+// modes per block and shared bytes of k_ymodes: as many warps as fit (<= 8)
+int ymodes_shape(const Dev &d, size_t *smem) {
+    const size_t shared = 2 * static_cast<size_t>(d.n2m + 2) * sizeof(double);
+    const size_t per = 2 * static_cast<size_t>(d.n2m + 1) * sizeof(double);
+    const size_t cap = 225u * 1024u;   // the 227 KB opt-in less the grouped kernel's static Dev
+    int nw = static_cast<int>(std::min<size_t>(8, (cap - shared) / per));
+    if (nw < 1) nw = 1;
+    *smem = shared + per * static_cast<size_t>(nw);
+    return nw;
+}
+}  // namespace
+
+void launch_scan_poisson(const Dev &d, cudaStream_t st) {
+    size_t smem = 0;
+    const int nw = ymodes_shape(d, &smem);
+    pdl(k_ymodes, dim3((d.n3m + nw - 1) / nw), dim3(32 * nw), smem, st, d, nw);
+}
 
 template <int TK>
 void gwin_launch(const Group &g, int n, cudaStream_t st) {
@@ -889,14 +1001,9 @@ void glaunch_win_helsolve(const Group &g, int n, cudaStream_t st) {
 
 void glaunch_scan_poisson(const Group &g, cudaStream_t st) {
     const Dev &d = g.rep;
-    const int blocks = (d.n3m + kYLines - 1) / kYLines;
-    const int m = ((d.n2 + 32 * kYPoissonWarps - 1) / (32 * kYPoissonWarps)) | 1;
-    const size_t smem = ylines_smem(d, 2);
-    const int threads = kYLines * kYPoissonWarps * 32;
-    const dim3 grid(blocks, 1, g.n);
-    if (m <= 9) pdl(kg_ylines_poisson<9>, grid, dim3(threads), smem, st, g.cases);
-    else if (m <= 17) pdl(kg_ylines_poisson<17>, grid, dim3(threads), smem, st, g.cases);
-    else pdl(kg_ylines_poisson<33>, grid, dim3(threads), smem, st, g.cases);
+    size_t smem = 0;
+    const int nw = ymodes_shape(d, &smem);
+    pdl(kg_ymodes, dim3((d.n3m + nw - 1) / nw, 1, g.n), dim3(32 * nw), smem, st, g.cases, nw);
 }
 
 }  // namespace fb
