@@ -666,9 +666,11 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // its loads in flight at once (each load coalesced over the 32 rows); the
 // CTA's row maxima go to the cluster through distributed shared memory, so
 // every CTA derives each row's exponent from the whole row; then each CTA
-// cuts the digits from its registers, four columns to a 32-bit word, and
-// writes one slice at a time through shared memory (rows of 2 V + 1 words:
-// conflict-free) with coalesced stores along k.  The operand is read once.
+// turns its values into 56-bit integers (one conversion each), takes the
+// digits from them with shifts, four columns to a 32-bit word, and writes
+// one slice at a time through two alternating shared-memory buffers (rows
+// of 2 V + 1 words: conflict-free) with coalesced stores along k.  The
+// operand is read once.
 // Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
@@ -681,7 +683,7 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
-    __shared__ uint32_t buf[32 * kRow];
+    __shared__ uint32_t buf[2 * 32 * kRow];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int rank = static_cast<int>(cl.block_rank());
     const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
@@ -716,33 +718,43 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     }
     cl.sync();   // no CTA leaves while another still reads its maxima
     const double s = sc[lane];
+    // |a s| < 1, so a s 2^(7 kI8S) (exact: powers of two) truncated toward
+    // zero is an integer below 2^(7 kI8S) whose base-128 digits, carrying the
+    // sign of a, are the kI8S digits: d_i = sign(a) floor(|a s| 128^(i+1)) mod 128
+    unsigned long long u[kP][4];
+    uint32_t neg[kP];
 #pragma unroll
-    for (int p = 0; p < kP; ++p)
+    for (int p = 0; p < kP; ++p) {
+        neg[p] = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) a[p][q] = a[p][q] * s;
+        for (int q = 0; q < 4; ++q) {
+            const long long v = __double2ll_rz((a[p][q] * s) * 72057594037927936.0);   // 2^56
+            u[p][q] = static_cast<unsigned long long>(v < 0 ? -v : v);
+            neg[p] |= (v < 0 ? 0xFFu : 0u) << (8 * q);
+        }
+    }
+    static_assert(kI8S == 8, "2^56 = 128^kI8S");
     // this CTA's words that lie inside ldk, per row
     const int nwords = static_cast<int>(max(0L, min(static_cast<long>(2 * V), (ldk - c0) / 4)));
     for (int i = 0; i < kI8S; ++i) {
+        uint32_t *bi = buf + (i & 1) * (32 * kRow);   // two buffers: one barrier per slice
+        const int sh = 7 * (kI8S - 1 - i);
 #pragma unroll
         for (int p = 0; p < kP; ++p) {
-            uint32_t word = 0;
+            uint32_t mag = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[p][q] = a[p][q] * 128.0;
-                const double d = trunc(a[p][q]);
-                a[p][q] = a[p][q] - d;
-                word |= (static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(d)))) << (8 * q);
-            }
-            buf[lane * kRow + 8 * p + w] = word;
+            for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
+            // the negative values' bytes negated (bytewise, no carries between bytes)
+            const uint32_t m = neg[p];
+            bi[lane * kRow + 8 * p + w] = (mag & ~m) | (__vsub4(0u, mag) & m);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < 32 * 2 * V; t += blockDim.x) {
             const int row = t / (2 * V), wd = t - row * (2 * V);
             if (wd < nwords)
                 *reinterpret_cast<uint32_t *>(dig + static_cast<size_t>(i) * plane +
-                                              static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) = buf[row * kRow + wd];
+                                              static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) = bi[row * kRow + wd];
         }
-        __syncthreads();
     }
 }
 

@@ -4,11 +4,14 @@
 
 WORKLOAD is one of the benchmark cases (``case.WORKLOADS``), STAGE a name of
 ``fribois2d_b200.STAGES`` (``helsolve``, ``i8x8_gemm``, ``poisson_tri`` ...) or
-``step`` (one full time step), POISSON ``int8x8`` (default), ``fp64`` or
+``step`` (full time steps), POISSON ``int8x8`` (default), ``fp64`` or
 ``tf32x3``.  The case is set up, autotuned and advanced two steps; then the
 stage runs once as a warm-up and REPS times (default 2) from a captured
-graph, and its mean device time is printed.  Few launches precede the timed
-ones, which makes this the driver for kernel captures with a profiler.
+graph, and its mean device time is printed; with ``step``, REPS steps run
+from the step's captured graph and the time per step and the kernel launches
+per step are printed (the last REPS x launches of a profiler's launch list
+are those steps).  Few launches precede the timed ones, which makes this the
+driver for kernel captures with a profiler.
 """
 from __future__ import annotations
 
@@ -38,8 +41,9 @@ def main(argv) -> int:
     s.set("q2", q2)
     s.advance(0, 2, history=False)
     if stage == "step":
-        s.advance(2, 1, history=False)
-        print(f"{name} step: {s.last_advance_ms() * 1e3:.1f} us (tiles {tiles})")
+        s.advance(2, reps, history=False)
+        print(f"{name} step: {s.last_advance_ms() * 1e3 / reps:.1f} us per step over {reps} steps, "
+              f"{s.kernel_count()} kernel launches per step (tiles {tiles})")
     else:
         s.set_substep(2, 1)
         ms = s.time_stage(stage, 1, reps=reps)
