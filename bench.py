@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--train-cases", type=int, default=256, help="sweep cases generating the predictor's samples")
     ap.add_argument("--train-steps", type=int, default=4000, help="coupled steps per sweep case")
     ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--windows", type=int, default=4,
+                    help="windows in which the batched coupled arms alternate over one stretch of the trajectory")
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="steps of the tf32x3 form's accuracy comparison with the FP64 path")
     ap.add_argument("--poisson", default="int8x8", choices=sorted(FORMS),
@@ -383,6 +385,19 @@ def batch_arm(args, rank, world, local):
         print(json.dumps(line))
 
 
+def merge_clocks(a, b):
+    """Clock records of two sampled windows as one: the reasons seen in
+    either, the lower median SM clock, the samples of both."""
+    if a is None:
+        return b
+    out = dict(b)
+    out["reasons"] = sorted(set(a.get("reasons", [])) | set(b.get("reasons", [])))
+    mhz = [x["sm_mhz"] for x in (a, b) if x.get("sm_mhz") is not None]
+    out["sm_mhz"] = min(mhz) if mhz else None
+    out["samples"] = a.get("samples", 0) + b.get("samples", 0)
+    return out
+
+
 def coupled_batch_arm(args, rank, world, local):
     """Strongly coupled batch: N VIV cases of the batching form advanced
     together with the coupling iteration on the device (a graph WHILE node;
@@ -392,8 +407,10 @@ def coupled_batch_arm(args, rank, world, local):
     developed flow, where the predictors have a history): the plain FP64
     path with the reference's loose coupling and with strong coupling (each
     case stepped alone by its own captured graph), then the batched form
-    with the plain and with the learned predictor.  The accuracy block runs a
-    subset from the start against the FP64 path with strong coupling."""
+    with the plain and with the learned predictor, alternating in short
+    windows so that the two predictors meet the same stretch of the flow.
+    The accuracy block runs a subset from the start against the FP64 path
+    with strong coupling."""
     import torch
     import fribois2d_b200 as fb
     from fribois2d_b200 import case as cases
@@ -434,6 +451,11 @@ def coupled_batch_arm(args, rank, world, local):
         k = sum(a["steps"] - q["steps"] for a, q in zip(after, before))
         return n / max(k, 1.0)
 
+    def solve_count(before):
+        after = [sv.coupling_stats() for sv in svs]
+        return (sum(a["solves"] - q["solves"] for a, q in zip(after, before)),
+                sum(a["steps"] - q["steps"] for a, q in zip(after, before)))
+
     def sequential():   # each case alone, its own captured graph
         nonlocal done
         ms = 0.0
@@ -444,7 +466,7 @@ def coupled_batch_arm(args, rank, world, local):
         done += K
         return ms
 
-    def batched(mode, predictor):
+    def batched(mode, predictor, steps):
         nonlocal done
         for sv in svs:
             sv.set_poisson(form)
@@ -457,12 +479,12 @@ def coupled_batch_arm(args, rank, world, local):
         clocks = ClockSampler(local)
         torch.cuda.synchronize(dev)
         clocks.start()
-        b.advance(K)
+        b.advance(steps)
         clk = clocks.stop()
         ms = b.last_ms()
         b.close()
-        done += K
-        return ms, solves_of(before), info, clk
+        done += steps
+        return ms, solve_count(before), info, clk
 
     # loosely coupled warm-up as a batch in the FP64 form: a developed flow
     for sv in svs:
@@ -477,12 +499,28 @@ def coupled_batch_arm(args, rank, world, local):
     before = [sv.coupling_stats() for sv in svs]
     seq_coupled_ms = sequential()
     seq_coupled_solves = solves_of(before)
-    plain_ms, plain_solves, _, _ = batched(fb.COUPLING_STRONG, None)
-    ms, solves, info, clk = plain_ms, plain_solves, None, None
-    if pred is not None:
-        ms, solves, info, clk = batched(fb.COUPLING_LEARNED, pred)
-    else:
-        ms, solves, info, clk = batched(fb.COUPLING_STRONG, None)
+    # the batched arms alternate in windows over the same stretch of the
+    # trajectory, so that both see the same flow
+    nwin = max(1, min(args.windows, K))
+    bounds = [K * w // nwin for w in range(nwin + 1)]
+    arms = {"plain": [0.0, 0, 0], "main": [0.0, 0, 0]}
+    info = clk = None
+    for w in range(nwin):
+        n = bounds[w + 1] - bounds[w]
+        if n == 0:
+            continue
+        for arm in ("plain", "main"):
+            mode, pr_ = (fb.COUPLING_STRONG, None) if (arm == "plain" or pred is None) else (fb.COUPLING_LEARNED, pred)
+            wms, (ns, nk), winfo, wclk = batched(mode, pr_, n)
+            a = arms[arm]
+            a[0] += wms
+            a[1] += ns
+            a[2] += nk
+            if arm == "main":
+                info = winfo
+                clk = merge_clocks(clk, wclk)
+    plain_ms, plain_solves = arms["plain"][0], arms["plain"][1] / max(arms["plain"][2], 1)
+    ms, solves = arms["main"][0], arms["main"][1] / max(arms["main"][2], 1)
     for sv in svs:
         sv.close()
     # accuracy: a subset from the start against the FP64 path, each case alone
@@ -529,7 +567,8 @@ def coupled_batch_arm(args, rank, world, local):
                              for n3, n2, _ in cases.BATCH_GRIDS},
                    "groups": info["groups"], "poisson": args.poisson, "coupling": args.coupling,
                    "tol": 1e-8, "l2": "working set far above L2 (all cases resident)",
-                   "warmup": f"{W} loosely coupled steps as a batch, then each arm {K} steps in turn"},
+                   "warmup": f"{W} loosely coupled steps as a batch, then the sequential arms {K} steps each, "
+                             f"then the two batched arms alternating in {nwin} windows ({K} steps each in all)"},
         "fluid_solves_per_step": solves,
         "plain_fp64_sequential": {"value": seq_loose, "ms_per_step": seq_loose_ms / K,
                                   "note": "the same cases, FP64 (INT8-exact transforms), loose coupling as the "

@@ -536,10 +536,15 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     if ((st = dnew(c, &d.phi, nlm * 2 * fb::kSD))) return st;
     if ((st = dnew(c, &d.cl, nlm * 2))) return st;
     if ((st = dnew(c, &d.contrib, nlm * 2 * fb::kSD))) return st;
-    d.bcap = 16;
+    // spreading table: at least 8 entries per (marker, direction), a load of 1/8 at most
+    d.hlog = 10;
+    while ((static_cast<size_t>(1) << d.hlog) < 16 * nlm) ++d.hlog;
     if (d.nlm) {
-        if ((st = dnew(c, &d.bcnt, 2 * nf))) return st;
-        if ((st = dnew(c, &d.bucket, 2 * nf * static_cast<size_t>(d.bcap)))) return st;
+        const size_t hcap = static_cast<size_t>(1) << d.hlog;
+        if ((st = dnew(c, &d.hkey, hcap))) return st;
+        if ((st = dnew(c, &d.hcnt, hcap))) return st;
+        if ((st = dnew(c, &d.hval, hcap * fb::kBucket))) return st;
+        if ((st = dnew(c, &d.hslot, nlm * 2))) return st;
         if ((st = dnew(c, &d.chain, nlm * 2 * fb::kSD))) return st;
         if ((st = dnew(c, &d.chead, nlm * 2 * fb::kSD))) return st;
     }

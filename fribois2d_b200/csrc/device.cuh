@@ -10,6 +10,8 @@
 namespace fb {
 
 constexpr int kSD = 9;  // MLS support nodes per marker and direction (dimSD)
+constexpr int kBucket = 16;        // marker slots per spreading-table entry
+constexpr int kBucketLevels = 16;  // entries per start cell at most (256 boxes)
 
 struct TriDev {          // factors of one tridiagonal system (DGTTRF output)
     int n;
@@ -56,8 +58,14 @@ struct Dev {
     int *eulins;             // [marker][dir][2][kSD]
     double *phi, *cl;        // [marker][dir][kSD], [marker][dir]
     double *contrib;         // [marker][dir][kSD] forcing contributions of one substep
-    int *bcnt, *bucket;      // markers per support-box start cell, [dir][cell] and [dir][cell][bcap]
-    int bcap;
+    // support-box start cell -> markers: an open-addressing table of 2^hlog
+    // entries (sized by the marker count), each a key ((dir, cell) x
+    // kBucketLevels + level, plus one; 0 = empty), a count and kBucket marker
+    // slots; a cell with more than kBucket boxes continues at the next level
+    unsigned long long *hkey;
+    int *hcnt, *hval;
+    int *hslot;              // per (marker, dir): its entry plus one, 0 = none
+    int hlog;
     int *chain;              // per contribution slot: next slot of the same cell in marker
                              // order (>= 0) or -1 at the end, written by the cell's head
     int *chead;              // per contribution slot: 1 if it heads its cell's chain

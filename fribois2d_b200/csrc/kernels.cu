@@ -433,16 +433,25 @@ __device__ int nearest_sorted(const double *a, int lo, int hi, double x, int gue
     return (dh < dl) ? h : l;
 }
 
+// entry of a spreading-table key (Fibonacci hashing: the top hlog bits of
+// key x 2^64 / golden ratio)
+__device__ __forceinline__ unsigned bucket_hash(unsigned long long key, int hlog) {
+    return static_cast<unsigned>((key * 0x9E3779B97F4A7C15ull) >> (64 - hlog));
+}
+
 // lgrdistribution.F90:189-267: nearest nodes per marker and direction
 __device__ __forceinline__ void lgrdist_body(const Dev &d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nlm) return;
-    {   // empty the support-box buckets this marker filled at the previous step
-        const size_t nf = static_cast<size_t>(d.NK) * d.P;
-        for (int dir = 0; dir < 2; ++dir) {
-            const int *eu = d.eulins + static_cast<size_t>(2 * i + dir) * 2 * kSD;
-            const int j0 = eu[0], k0 = eu[kSD];
-            if (j0 >= 1 && j0 <= d.n2 && k0 >= 0 && k0 <= d.n3) d.bcnt[dir * nf + fidx(d, j0, k0)] = 0;
+    // empty the spreading-table entries this marker filled at the previous
+    // step: every used entry is some marker's own entry, so the table is
+    // empty again before the set-up fills it
+    for (int dir = 0; dir < 2; ++dir) {
+        const int e = d.hslot[2 * i + dir];
+        if (e) {
+            d.hkey[e - 1] = 0ull;
+            d.hcnt[e - 1] = 0;
+            d.hslot[2 * i + dir] = 0;
         }
     }
     const double y = d.lmcc[2 * i], z = d.lmcc[2 * i + 1];
@@ -650,10 +659,28 @@ __device__ __forceinline__ void mls_setup_body(const Dev &d) {
         eu[kSD + m] = eul[1][m];
     }
     // register the support box (start cell = node m = 0) for the spreading
-    const size_t cell = static_cast<size_t>(idir - 1) * d.NK * d.P + fidx(d, eul[0][0], eul[1][0]);
-    const int slot = atomicAdd(d.bcnt + cell, 1);
-    if (slot < d.bcap) d.bucket[cell * d.bcap + slot] = n;
-    else raise_status(d, FB_ERR_UNSUPPORTED);
+    const unsigned long long cell = static_cast<unsigned long long>(idir - 1) * d.NK * d.P + fidx(d, eul[0][0], eul[1][0]);
+    const unsigned mask = (1u << d.hlog) - 1u;
+    for (int lev = 0; lev < kBucketLevels; ++lev) {
+        const unsigned long long key = cell * kBucketLevels + lev + 1;
+        unsigned h = bucket_hash(key, d.hlog);
+        for (unsigned probes = 0;; ++probes) {   // find or claim the key's entry
+            const unsigned long long prev = atomicCAS(d.hkey + h, 0ull, key);
+            if (prev == 0ull || prev == key) break;
+            if (probes == mask) {   // full: cannot happen at the table's sizing
+                raise_status(d, FB_ERR_UNSUPPORTED);
+                return;
+            }
+            h = (h + 1) & mask;
+        }
+        const int slot = atomicAdd(d.hcnt + h, 1);
+        if (slot < kBucket) {
+            d.hval[static_cast<size_t>(h) * kBucket + slot] = n;
+            d.hslot[t] = static_cast<int>(h) + 1;
+            return;
+        }
+    }
+    raise_status(d, FB_ERR_UNSUPPORTED);   // more than kBucket x kBucketLevels boxes start in one cell
 }
 
 __global__ void k_mls_setup(Dev d) {
@@ -726,36 +753,52 @@ __device__ __forceinline__ void spread_chains_body(const Dev &d) {
     if (!used) return;
     const size_t plane = static_cast<size_t>(dir) * d.NK * d.P;
     // the cell's touchers are the markers registered at the 3 x 3 possible
-    // box start cells: all counts first, then all entries (two rounds of
-    // loads); a lower-index toucher means this slot is not the head
-    int cnt[9];
-    size_t base[9];
-#pragma unroll
+    // box start cells (table lookups); a lower-index toucher means this slot
+    // is not the head
+    constexpr int kMaxTouch = 9 * kBucket;   // touchers of one cell kept at most
+    int ln[kMaxTouch], ls[kMaxTouch];         // touchers after n, ascending marker index
+    int L = 0;
+    bool over = false;
+    const unsigned mask = (1u << d.hlog) - 1u;
     for (int q = 0; q < 9; ++q) {
         const int sj = j - q / 3, sk = k - q % 3;
-        const bool ok = !(sj < 1 || sk < 0);
-        const size_t cell = plane + fidx(d, ok ? sj : 1, ok ? sk : 0);
-        cnt[q] = ok ? min(d.bcnt[cell], d.bcap) : 0;
-        base[q] = cell * d.bcap;
-    }
-    constexpr int kMaxTouch = 9 * 16;   // 9 start cells x bucket capacity (bcap <= 16)
-    int ln[kMaxTouch], ls[kMaxTouch];   // touchers after n, ascending marker index
-    int L = 0;
-    for (int q = 0; q < 9; ++q)
-        for (int e = 0; e < cnt[q] && e < 16; ++e) {
-            const int nn = d.bucket[base[q] + e];
-            if (nn < n) return;
-            if (nn == n || L >= kMaxTouch) continue;
-            // insertion in increasing marker index (a marker has one box start cell)
-            int p = L++;
-            while (p > 0 && ln[p - 1] > nn) {
-                ln[p] = ln[p - 1];
-                ls[p] = ls[p - 1];
-                --p;
+        if (sj < 1 || sk < 0) continue;
+        const unsigned long long cell = plane + fidx(d, sj, sk);
+        for (int lev = 0; lev < kBucketLevels; ++lev) {
+            const unsigned long long key = cell * kBucketLevels + lev + 1;
+            unsigned h = bucket_hash(key, d.hlog);
+            unsigned long long kh = d.hkey[h];
+            for (unsigned probes = 0; kh != key && kh != 0ull && probes < mask; ++probes) {
+                h = (h + 1) & mask;
+                kh = d.hkey[h];
             }
-            ln[p] = nn;
-            ls[p] = (2 * nn + dir) * kSD + q;   // node (dj, dk) = (q / 3, q % 3) of marker nn
+            if (kh != key) break;   // no (further) boxes start in this cell
+            const int cnt = d.hcnt[h];
+            for (int e = 0; e < min(cnt, kBucket); ++e) {
+                const int nn = d.hval[static_cast<size_t>(h) * kBucket + e];
+                if (nn < n) return;
+                if (nn == n) continue;
+                if (L >= kMaxTouch) {   // denser than the marker spacing the spreading is built for
+                    over = true;
+                    continue;
+                }
+                // insertion in increasing marker index (a marker has one box start cell)
+                int p = L++;
+                while (p > 0 && ln[p - 1] > nn) {
+                    ln[p] = ln[p - 1];
+                    ls[p] = ls[p - 1];
+                    --p;
+                }
+                ln[p] = nn;
+                ls[p] = (2 * nn + dir) * kSD + q;   // node (dj, dk) = (q / 3, q % 3) of marker nn
+            }
+            if (cnt <= kBucket) break;   // the cell's last entry
         }
+    }
+    if (over) {
+        raise_status(d, FB_ERR_UNSUPPORTED);
+        return;
+    }
     // this slot heads the cell's chain: link the touchers in marker order
     d.chead[g] = 1;
     int prev_slot = g;

@@ -188,6 +188,41 @@ def test_advance_is_bitwise_equal_to_stepwise(tmp_path):
     assert h[-1, 8] == pytest.approx(25 * c.params.dt, rel=1e-12)
 
 
+def test_dense_markers_spread_in_marker_order(tmp_path):
+    """400 markers on the small cylinder (radius 0.5, h = 1/8): about 16 per
+    grid spacing, so more support boxes start in some cells than one entry
+    of the spreading table holds and those cells continue at the next
+    level.  The forcing stage still adds every cell's contributions in
+    marker order (bit for bit with the oracle), and full steps follow the
+    oracle to 1e-10."""
+    p = Pair(cases.tiny_cylinder(nlm=400), str(tmp_path))
+    o, s = p.o, p.s
+    n2m, n3m = p.n2m, p.n3m
+    for ns in range(2):
+        assert o.step(ns) == 0
+    p.sync_to_gpu()
+    dt = o.scalars()["dt"]
+    o.set_substep(2, 1)
+    s.set_substep(2, 1)
+    o.stage("lgrdistribution")
+    assert s.stage("lgrdistribution", 1) == 0
+    o.stage("forcing", 1)
+    assert s.stage("forcing", 1) == 0
+    rhs2 = p.of("rhs2") + p.of("fey") * dt
+    rhs3 = p.of("rhs3") + p.of("fez") * dt
+    np.testing.assert_array_equal(_sub(s.get("rhs2"), 1, n3m, 2, n2m), _sub(rhs2, 1, n3m, 2, n2m))
+    np.testing.assert_array_equal(_sub(s.get("rhs3"), 2, n3m, 1, n2m), _sub(rhs3, 2, n3m, 1, n2m))
+    for ns in range(2, 6):
+        p.sync_to_gpu()
+        assert o.step(ns) == 0
+        s.fluid_tsch(ns)
+        s.rigid(ns)
+        for f in ("q2", "q3"):
+            assert rel(_sub(s.get(f), 1, n3m, 1, n2m), _sub(p.of(f), 1, n3m, 1, n2m)) <= 1e-10, (f, ns)
+        assert rel(s.get("forces")[1:4], o.a("forces")[1:4]) <= 1e-10, ns
+    s.close()
+
+
 def test_marker_outside_domain_is_reported_not_faulted(tmp_path):
     """A marker pushed outside the grid on the host is caught by the device
     kernels' bounds checks (lgrdistribution.F90:217-221) and reported."""
