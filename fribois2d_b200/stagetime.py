@@ -1,11 +1,13 @@
 """Time one stage (or kernel) of the fluid step on a named workload.
 
-    python -m fribois2d_b200.stagetime WORKLOAD STAGE [POISSON] [REPS]
+    python -m fribois2d_b200.stagetime WORKLOAD STAGE [POISSON] [REPS] [--no-tune]
 
 WORKLOAD is one of the benchmark cases (``case.WORKLOADS``), STAGE a name of
 ``fribois2d_b200.STAGES`` (``helsolve``, ``i8x8_gemm``, ``poisson_tri`` ...) or
 ``step`` (full time steps), POISSON ``int8x8`` (default), ``fp64`` or
-``tf32x3``.  The case is set up, autotuned and advanced two steps; then the
+``tf32x3``.  The case is set up, autotuned (unless ``--no-tune``: the
+library's default tiles, and no tuning launches before the stage's own) and
+advanced two steps; then the
 stage runs once as a warm-up and REPS times (default 2) from a captured
 graph, and its mean device time is printed; with ``step``, REPS steps run
 from the step's captured graph and the time per step and the kernel launches
@@ -26,6 +28,8 @@ FORMS = {"int8x8": POISSON_INT8X8, "fp64": POISSON_FP64, "tf32x3": POISSON_TF32X
 
 
 def main(argv) -> int:
+    tune = "--no-tune" not in argv
+    argv = [a for a in argv if a != "--no-tune"]
     if len(argv) < 2:
         print(__doc__)
         return 2
@@ -35,7 +39,7 @@ def main(argv) -> int:
     c = cases.WORKLOADS[name]()
     s = Solver(c.write(os.path.join(tempfile.mkdtemp(prefix="fbstage_"), c.name)))
     s.set_poisson(FORMS[form])
-    tiles = s.autotune()
+    tiles = s.autotune() if tune else "library defaults"
     q2 = s.get("q2")
     q2[1:c.n3m + 1] += c.v_perturbation()
     s.set("q2", q2)

@@ -204,6 +204,14 @@ def test_dense_markers_spread_in_marker_order(tmp_path):
     dt = o.scalars()["dt"]
     o.set_substep(2, 1)
     s.set_substep(2, 1)
+    o.stage("cfl")
+    assert s.stage("cfl") == 0
+    o.stage("boucdq")
+    assert s.stage("boucdq", 1) == 0
+    for x in ("hdnl2", "hdnl3", "invtr2", "invtr3"):   # q2f, q3f: what the forcing interpolates
+        o.stage(x, 1)
+    assert s.stage("nl_rhs", 1) == 0
+    p.sync_to_gpu()
     o.stage("lgrdistribution")
     assert s.stage("lgrdistribution", 1) == 0
     o.stage("forcing", 1)
