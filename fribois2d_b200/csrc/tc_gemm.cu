@@ -62,11 +62,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+// has the phase with the given parity completed?  (never suspends the thread)
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
         : "r"(bar), "r"(parity)
@@ -80,13 +81,18 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// wait for the phase with the given parity; false after one second
+// wait for the phase with the given parity; false after one second.  The
+// waits poll with test_wait: a try_wait that suspends the thread resumes
+// late (a pipeline with its loads and MMAs removed took 2-2.5 us per
+// k-block of producer/consumer hand-offs with suspending waits), and each
+// waiting thread here is alone on its warp scheduler
 __device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_test_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
-    while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > 1000000000ull) return false;
-    return true;
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_test_wait(bar, parity)) return true;
+        if ((i & 255u) == 0 && global_ns() - t0 > 1000000000ull) return false;
+    }
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
