@@ -156,6 +156,36 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16 columns of 32 lanes without waiting; tmem_wait16 waits for every load
+// issued so far and ties the registers to the wait (their uses follow it),
+// tmem_after16 ties further registers to the same point
+__device__ __forceinline__ void tmem_load16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_after16(uint32_t (&r)[16]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y, int z) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
@@ -936,27 +966,31 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     const int row = m0 + warp * 32 + lane;
     const bool rok = ok && row < o.M;
     const double rs = rok ? o.rowscale[row] : 0.0;
-    // 32 columns at a time; with BN = 48 the second load also reads the next
-    // class's first 16 columns (inside the allocation), which are not used
+    // 16 columns at a time: the kI8S classes' loads in flight together, one wait
 #pragma unroll 1
-    for (int c = 0; c < (BN + 31) / 32; ++c) {
-        double acc[32];
+    for (int c = 0; c < BN / 16; ++c) {
+        uint32_t v[kS][16];
 #pragma unroll
-        for (int q = 0; q < 32; ++q) acc[q] = 0.0;
-#pragma unroll 1
+        for (int t = 0; t < kS; ++t)
+            tmem_load16_async(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * BN + c * 16),
+                              v[t]);
+        tmem_wait16(v[0]);
+#pragma unroll
+        for (int t = 1; t < kS; ++t) tmem_after16(v[t]);
+        double acc[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+#pragma unroll
         for (int t = kS - 1; t >= 0; --t) {
-            uint32_t v[32];
-            tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * BN + c * 32), v);
             const double wgt = ldexp(1.0, -7 * (t + 2));
 #pragma unroll
-            for (int q = 0; q < 32; ++q) acc[q] = acc[q] + static_cast<double>(static_cast<int32_t>(v[q])) * wgt;
+            for (int q = 0; q < 16; ++q) acc[q] = acc[q] + static_cast<double>(static_cast<int32_t>(v[t][q])) * wgt;
         }
         if (rok) {
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                const int col = n0 + c * 32 + q;
-                if (c * 32 + q < BN && col < o.N)
-                    o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
+            for (int q = 0; q < 16; ++q) {
+                const int col = n0 + c * 16 + q;
+                if (col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
             }
         }
     }
