@@ -749,7 +749,7 @@ def device_arm(args, rank, world, local):
             roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": hbm_src}
         accuracy = None
-        if args.poisson == "tf32x3":
+        if args.poisson == "tf32x3" and args.accuracy_steps > 0:
             accuracy = precision_error(fb, path, c, steps=args.accuracy_steps, sweeps=args.sweeps)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:

@@ -832,7 +832,7 @@ struct I8Cfg {
     // D s32 (2), A and B signed 8-bit (1), both K-major, M = 128; N set per MMA
     static constexpr uint32_t kIdescBase = (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(128 >> 4) << 24);
     static_assert(kI8S * BN <= 512, "TMEM columns");
-    static_assert(BN % 16 == 0 && 4 * BN <= 256, "MMA N of four slices: a multiple of 16, at most 256");
+    static_assert(BN % 16 == 0 && BN <= 256, "MMA N: a multiple of 16, at most 256");
     static_assert(kASlots >= 2 && kSmem <= 227 * 1024, "shared memory per CTA");
 };
 
@@ -889,7 +889,8 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
         if (kGlobalMaps) acquire_maps(ma, ma, mb, mb);
-        int ia = 0, nb = 0;
+        int ia = 0, nb = 0, slot = 0;
+        uint32_t aph = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
             if (!mbar_wait(bempty0 + 8 * sb, (static_cast<uint32_t>(kb >> 1) & 1u) ^ 1u)) {
@@ -900,15 +901,19 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
             for (int j = 0; j < kS; ++j)
                 tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
             nb = kb + 1;
+#pragma unroll
             for (int i = 0; i < kS; ++i) {
-                const int slot = ia % kAS;
-                if (!mbar_wait(aempty0 + 8 * slot, (static_cast<uint32_t>(ia / kAS) & 1u) ^ 1u)) {
+                if (!mbar_wait(aempty0 + 8 * slot, aph ^ 1u)) {
                     ok = false;
                     break;
                 }
                 mbar_expect_tx(afull0 + 8 * slot, Cfg::kATile);
                 tma_load_3d(sA + slot * Cfg::kATile, ma, afull0 + 8 * slot, kb * kI8BK, m0, i);
                 ++ia;
+                if (++slot == kAS) {
+                    slot = 0;
+                    aph ^= 1u;
+                }
             }
         }
         // every copy issued has landed before the CTA may finish
@@ -917,8 +922,14 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
         for (int q = (nb > 2 ? nb - 2 : 0); q < nb; ++q)
             if (!mbar_wait(bfull0 + 8 * (q & 1), static_cast<uint32_t>(q >> 1) & 1u)) ok = false;
     } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer
-        int ia = 0;
+        // ---- MMA issuer.  One thread issues every MMA, so its loop is kept
+        // lean: descriptors advance by constants (the 14-bit address field
+        // holds byte address / 16), the digit loops are unrolled, and one MMA
+        // covers up to 256 / BN B slices (N <= 256).
+        constexpr int kG = 256 / BN;
+        const uint64_t adesc = sw128_desc(sA), bdesc = sw128_desc(sB);
+        int slot = 0;
+        uint32_t aph = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
             if (!mbar_wait(bfull0 + 8 * sb, static_cast<uint32_t>(kb >> 1) & 1u)) {
@@ -926,31 +937,32 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
                 break;
             }
             tc_fence_after();
-            const uint32_t bst = sB + sb * Cfg::kBStage;
+            const uint64_t bst = bdesc + static_cast<uint64_t>((sb * Cfg::kBStage) >> 4);
+#pragma unroll
             for (int i = 0; i < kS; ++i) {
-                const int slot = ia % kAS;
-                if (!mbar_wait(afull0 + 8 * slot, static_cast<uint32_t>(ia / kAS) & 1u)) {
+                if (!mbar_wait(afull0 + 8 * slot, aph)) {
                     ok = false;
                     break;
                 }
-                tc_fence_after();
-                const uint32_t ast = sA + slot * Cfg::kATile;
+                const uint64_t ast = adesc + static_cast<uint64_t>((slot * Cfg::kATile) >> 4);
                 // B slices j0 .. j0+nsl-1 are consecutive rows in shared memory and
                 // their classes i+j0 .. consecutive TMEM column blocks: one MMA of
-                // N = nsl * BN covers up to four digit pairs
-                for (int j0 = 0; j0 < kS - i; j0 += 4) {
-                    const int nsl = min(4, kS - i - j0);
+                // N = nsl * BN covers nsl digit pairs
+#pragma unroll
+                for (int j0 = 0; j0 < kS - i; j0 += kG) {
+                    const int nsl = (kS - i - j0 < kG) ? kS - i - j0 : kG;
                     const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * BN) >> 3) << 17);
                     const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * BN);
+                    const uint64_t bj = bst + static_cast<uint64_t>((j0 * Cfg::kBSlice) >> 4);
 #pragma unroll
-                    for (int kk = 0; kk < kI8BK / 32; ++kk) {   // K = 32 bytes per MMA
-                        const uint64_t a = sw128_desc(ast + 32 * kk);
-                        const uint64_t b = sw128_desc(bst + j0 * Cfg::kBSlice + 32 * kk);
-                        mma_i8(acc_t, a, b, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
-                    }
+                    for (int kk = 0; kk < kI8BK / 32; ++kk)   // K = 32 bytes per MMA: +2 in the address field
+                        mma_i8(acc_t, ast + 2 * kk, bj + 2 * kk, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
                 }
                 mma_commit(aempty0 + 8 * slot);   // frees the A slot once these MMAs have read it
-                ++ia;
+                if (++slot == kAS) {
+                    slot = 0;
+                    aph ^= 1u;
+                }
             }
             if (!ok) break;
             mma_commit(bempty0 + 8 * sb);
