@@ -156,6 +156,13 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// the int32 in v as an FP64 value, exactly, with one FP64 subtraction instead
+// of a conversion: 2^52 + 2^31 + v has v + 2^31 (v with its sign bit
+// flipped) as the low 32 bits of its mantissa
+__device__ __forceinline__ double i32_as_f64(uint32_t v) {
+    return __hiloint2double(0x43300000, static_cast<int>(v ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 // 16 columns of 32 lanes without waiting; tmem_wait16 waits for every load
 // issued so far and ties the registers to the wait (their uses follow it),
 // tmem_after16 ties further registers to the same point
@@ -996,7 +1003,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
         for (int t = kS - 1; t >= 0; --t) {
             const double wgt = ldexp(1.0, -7 * (t + 2));
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[q] = acc[q] + static_cast<double>(static_cast<int32_t>(v[t][q])) * wgt;
+            for (int q = 0; q < 16; ++q) acc[q] = acc[q] + i32_as_f64(v[t][q]) * wgt;
         }
         if (rok) {
 #pragma unroll
