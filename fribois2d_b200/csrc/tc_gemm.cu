@@ -723,6 +723,7 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     constexpr int kP = V / 4, kRow = 2 * V + 1;   // words per row of the slice buffer (odd)
+    static_assert(V % 4 == 0, "four columns to a word");
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
@@ -822,7 +823,9 @@ __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
 // columns per thread: the CTA's share of ldk over its 8 warps
 inline int cut_values(long ldk) {
     const long per = (ldk + 8 * kCutCl - 1) / (8 * kCutCl);
-    return per <= 4 ? 4 : per <= 8 ? 8 : per <= 16 ? 16 : per <= 32 ? 32 : 64;
+    for (int v : {4, 8, 12, 16, 24, 32, 48})
+        if (per <= v) return v;
+    return 64;
 }
 
 // BN: output tile width, 64 or 48 (a 128 x 48 tile puts 132 CTAs on a
@@ -1216,10 +1219,10 @@ int i8_configure() {
 void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st) {
     const dim3 grid(rep.rows_pad / 32 * kCutCl, 1, n);
     switch (cut_values(rep.ldk)) {
-    case 4: pdl(kg_i8_cut<4>, grid, dim3(256), 0, st, tasks, R, K); break;
-    case 8: pdl(kg_i8_cut<8>, grid, dim3(256), 0, st, tasks, R, K); break;
-    case 16: pdl(kg_i8_cut<16>, grid, dim3(256), 0, st, tasks, R, K); break;
-    case 32: pdl(kg_i8_cut<32>, grid, dim3(256), 0, st, tasks, R, K); break;
+#define FB_CUT_CASE(V) \
+    case V: pdl(kg_i8_cut<V>, grid, dim3(256), 0, st, tasks, R, K); break;
+        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(12) FB_CUT_CASE(16) FB_CUT_CASE(24) FB_CUT_CASE(32) FB_CUT_CASE(48)
+#undef FB_CUT_CASE
     default: pdl(kg_i8_cut<64>, grid, dim3(256), 0, st, tasks, R, K); break;
     }
 }
@@ -1234,10 +1237,10 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
     const dim3 grid(p.rows_pad / 32 * kCutCl);
     const long plane = p.ldk * static_cast<long>(p.rows_pad);
     switch (cut_values(p.ldk)) {
-    case 4: pdl(k_i8_cut<4>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
-    case 8: pdl(k_i8_cut<8>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
-    case 16: pdl(k_i8_cut<16>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
-    case 32: pdl(k_i8_cut<32>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+#define FB_CUT_CASE(V) \
+    case V: pdl(k_i8_cut<V>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
+        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(12) FB_CUT_CASE(16) FB_CUT_CASE(24) FB_CUT_CASE(32) FB_CUT_CASE(48)
+#undef FB_CUT_CASE
     default: pdl(k_i8_cut<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
     }
 }
