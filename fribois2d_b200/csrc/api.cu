@@ -40,6 +40,10 @@ struct fb_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;              // marker set-up branch
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // fb_set_markers: pinned staging of the four marker arrays, free again once
+    // stage_ev (recorded after their copies) has completed
+    double *stage_h = nullptr;
+    cudaEvent_t stage_ev = nullptr;
     cublasHandle_t blas = nullptr;
     void *blas_ws = nullptr;                  // 32 MB workspace of cuBLAS / cuBLASLt
     // FP64 transforms through cuBLASLt with an algorithm timed per grid size
@@ -1211,6 +1215,8 @@ int fb_destroy(fb_ctx *c) {
         if (p) cudaFree(p);
     if (c->coef_pin) cudaFreeHost(c->coef_pin);
     if (c->coef_pini) cudaFreeHost(c->coef_pini);
+    if (c->stage_h) cudaFreeHost(c->stage_h);
+    if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->blas) cublasDestroy(c->blas);
     for (cublasLtMatrixLayout_t l : c->lt_l)
         if (l) cublasLtMatrixLayoutDestroy(l);
@@ -1713,14 +1719,28 @@ int fb_get_loads(fb_ctx *c, double *press, double *tau) {
     return FB_OK;
 }
 
+// The arrays are copied into pinned staging memory before the call returns
+// (the caller may reuse its buffers at once); the host-to-device copies are
+// ordered on the context stream ahead of the next step, without a wait here.
 int fb_set_markers(fb_ctx *c, const double *lmcc, const double *lmvel, const double *lmacc, const double *lmnor) {
     if (!c) return FB_ERR_STATE;
-    const size_t b = 2 * static_cast<size_t>(c->d.nlm) * sizeof(double);
-    if (lmcc) CK(cudaMemcpyAsync(c->d.lmcc, lmcc, b, cudaMemcpyHostToDevice, c->stream));
-    if (lmvel) CK(cudaMemcpyAsync(c->d.lmvel, lmvel, b, cudaMemcpyHostToDevice, c->stream));
-    if (lmacc) CK(cudaMemcpyAsync(c->d.lmacc, lmacc, b, cudaMemcpyHostToDevice, c->stream));
-    if (lmnor) CK(cudaMemcpyAsync(c->d.lmnor, lmnor, b, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    const size_t n = 2 * static_cast<size_t>(c->d.nlm), b = n * sizeof(double);
+    if (!n) return FB_OK;
+    CK(cudaSetDevice(c->device));
+    if (!c->stage_h) {
+        CK(cudaMallocHost(&c->stage_h, 4 * b));
+        CK(cudaEventCreateWithFlags(&c->stage_ev, cudaEventDisableTiming));
+    } else {
+        CK(cudaEventSynchronize(c->stage_ev));   // the previous call's copies have left the staging
+    }
+    const double *src[4] = {lmcc, lmvel, lmacc, lmnor};
+    double *dst[4] = {c->d.lmcc, c->d.lmvel, c->d.lmacc, c->d.lmnor};
+    for (int i = 0; i < 4; ++i) {
+        if (!src[i]) continue;
+        std::memcpy(c->stage_h + i * n, src[i], b);
+        CK(cudaMemcpyAsync(dst[i], c->stage_h + i * n, b, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaEventRecord(c->stage_ev, c->stream));
     return FB_OK;
 }
 
@@ -1741,7 +1761,8 @@ int fb_get_array(fb_ctx *c, int id, double *host, int64_t n) {
     if (!c || !host) return FB_ERR_STATE;
     Dev &d = c->d;
     double *p = nullptr;
-    CK(cudaStreamSynchronize(c->stream));
+    // every copy below is ordered on the context stream after the work that
+    // writes the array, and waited for before returning
     if (field_ptr(c, id, &p) == FB_OK) {
         if (n != static_cast<int64_t>(d.NK) * d.n2) return FB_ERR_STATE;
         CK(cudaMemcpy2DAsync(host, d.n2 * sizeof(double), p, d.P * sizeof(double), d.n2 * sizeof(double), d.NK,
@@ -2741,6 +2762,8 @@ int fb_batch_info(fb_batch *b, int32_t info[3]) {
 int fb_batch_advance(fb_batch *b, int nsteps) {
     if (!b || nsteps < 0) return FB_ERR_STATE;
     CK(cudaSetDevice(b->device));
+    // work the contexts queued on their own streams (marker uploads) comes first
+    for (fb_ctx *x : b->ctx) CK(cudaStreamSynchronize(x->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
     if (b->coupled && !b->cond_graph) {   // the fluid solves driven from the host
         for (int i = 0; i < nsteps; ++i) {

@@ -727,8 +727,7 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
-    constexpr int kPP = (V <= 32) ? 2 : 1;   // planes written per barrier
-    __shared__ uint32_t buf[2 * kPP * 32 * kRow];
+    __shared__ uint32_t buf[2 * 32 * kRow];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int rank = static_cast<int>(cl.block_rank());
     const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
@@ -761,10 +760,7 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
         sc[lane] = ldexp(1.0, -e);
         if (rank == 0 && r < R) rowscale[r] = ldexp(1.0, e);
     }
-    __syncthreads();
-    // no CTA may leave while another still reads its maxima: arrive now, wait
-    // at the end, so the digit work runs while the slowest CTA catches up
-    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    cl.sync();   // no CTA leaves while another still reads its maxima
     const double s = sc[lane];
     // |a s| < 1, so a s 2^(7 kI8S) (exact: powers of two) truncated toward
     // zero is an integer below 2^(7 kI8S) whose base-128 digits, carrying the
@@ -784,37 +780,26 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     static_assert(kI8S == 8, "2^56 = 128^kI8S");
     // this CTA's words that lie inside ldk, per row
     const int nwords = static_cast<int>(max(0L, min(static_cast<long>(2 * V), (ldk - c0) / 4)));
-    // kPP slices per phase; two sets of buffers, so one barrier per phase
-#pragma unroll 1
-    for (int ph = 0; ph < kI8S / kPP; ++ph) {
-        uint32_t *bset = buf + (ph & 1) * (kPP * 32 * kRow);
+    for (int i = 0; i < kI8S; ++i) {
+        uint32_t *bi = buf + (i & 1) * (32 * kRow);   // two buffers: one barrier per slice
+        const int sh = 7 * (kI8S - 1 - i);
 #pragma unroll
-        for (int e = 0; e < kPP; ++e) {
-            const int sh = 7 * (kI8S - 1 - (ph * kPP + e));
+        for (int p = 0; p < kP; ++p) {
+            uint32_t mag = 0;
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
-                uint32_t mag = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
-                // the negative values' bytes negated (bytewise, no carries between bytes)
-                const uint32_t m = neg[p];
-                bset[e * 32 * kRow + lane * kRow + 8 * p + w] = (mag & ~m) | (__vsub4(0u, mag) & m);
-            }
+            for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
+            // the negative values' bytes negated (bytewise, no carries between bytes)
+            const uint32_t m = neg[p];
+            bi[lane * kRow + 8 * p + w] = (mag & ~m) | (__vsub4(0u, mag) & m);
         }
         __syncthreads();
-#pragma unroll
-        for (int e = 0; e < kPP; ++e) {
-            const int i = ph * kPP + e;
-            for (int t = threadIdx.x; t < 32 * 2 * V; t += blockDim.x) {
-                const int row = t / (2 * V), wd = t - row * (2 * V);
-                if (wd < nwords)
-                    *reinterpret_cast<uint32_t *>(dig + static_cast<size_t>(i) * plane +
-                                                  static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) =
-                        bset[e * 32 * kRow + row * kRow + wd];
-            }
+        for (int t = threadIdx.x; t < 32 * 2 * V; t += blockDim.x) {
+            const int row = t / (2 * V), wd = t - row * (2 * V);
+            if (wd < nwords)
+                *reinterpret_cast<uint32_t *>(dig + static_cast<size_t>(i) * plane +
+                                              static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) = bi[row * kRow + wd];
         }
     }
-    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 template <int V>
