@@ -1301,9 +1301,35 @@ __device__ __forceinline__ void loads_probe_body(const Dev &d) {
     for (int i = 0; i < 7; ++i) pb[7 * (idir - 1) + i] = res[i];
 }
 
-__global__ void k_loads_probe(Dev d) {
-    FB_GRID_WAIT();
+// the probes of kLoadMk markers per block (their three threads in one block),
+// then each probed marker's own tangent (loads_transfer.F90:177-185) from its
+// first two probes
+constexpr int kLoadMk = 32;
+__device__ __forceinline__ void loads_probe_tan_body(const Dev &d) {
     loads_probe_body(d);
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * d.nlm || t % 3 != 0 || *d.status) return;
+    const int n = t / 3;
+    double *pb = d.probe + static_cast<size_t>(n) * 24;
+    if (pb[23] < 0.0) return;
+    const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
+    const double vel0 = pb[0], vel1 = pb[7];
+    const double veln_md = vel0 * nory + vel1 * norz;
+    const double velt0 = vel0 - veln_md * nory, velt1 = vel1 - veln_md * norz;
+    const double velt_md = sqrt(velt0 * velt0 + velt1 * velt1);
+    if (velt_md != 0.0) {
+        pb[21] = velt0 / sqrt(velt0 * velt0 + velt1 * velt1);
+        pb[22] = velt1 / sqrt(velt0 * velt0 + velt1 * velt1);
+        pb[23] = 1.0;
+    } else {
+        pb[23] = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(3 * kLoadMk) k_loads_probe(Dev d) {
+    FB_GRID_WAIT();
+    loads_probe_tan_body(d);
 }
 
 // loads_transfer_c (loads_transfer.F90:187-214): the tangent carries over
@@ -1312,76 +1338,79 @@ __global__ void k_loads_probe(Dev d) {
 // Also the L2 norms of checkbcs (ckbcs.F90:76-81).  Single block.
 __device__ __forceinline__ void loads_finish_body(const Dev &d) {
     __shared__ double sh[32];
+    __shared__ bool last;
     const double hpr = d.ddmin * d.kprobe, visc = d.visc;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double sv = 0.0, sw = 0.0;
-    const bool ok = (*d.status == 0);
-    if (ok) {   // the probe's own tangent (loads_transfer.F90:177-185)
-        for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
-            double *pb = d.probe + static_cast<size_t>(n) * 24;
-            if (pb[23] < 0.0) continue;
-            const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
-            const double vel0 = pb[0], vel1 = pb[7];
-            const double veln_md = vel0 * nory + vel1 * norz;
-            const double velt0 = vel0 - veln_md * nory, velt1 = vel1 - veln_md * norz;
-            const double velt_md = sqrt(velt0 * velt0 + velt1 * velt1);
-            if (velt_md != 0.0) {
-                pb[21] = velt0 / sqrt(velt0 * velt0 + velt1 * velt1);
-                pb[22] = velt1 / sqrt(velt0 * velt0 + velt1 * velt1);
-                pb[23] = 1.0;
-            } else {
-                pb[23] = 0.0;
-            }
-        }
-    }
-    __syncthreads();
-    if (ok) {
-        for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
-            const double *pb = d.probe + static_cast<size_t>(n) * 24;
+    if (n < d.nlm) {
+        const double *pb = d.probe + static_cast<size_t>(n) * 24;
+        if (*d.status == 0) {
             d.press[n] = 0.0;
             d.tau[2 * n] = 0.0;
             d.tau[2 * n + 1] = 0.0;
-            if (pb[23] < 0.0) continue;
-            double tany = 0.0, tanz = 0.0;
-            for (int m = n; m >= 0; --m) {
-                const double *pm = d.probe + static_cast<size_t>(m) * 24;
-                if (pm[23] > 0.5) {
-                    tany = pm[21];
-                    tanz = pm[22];
-                    break;
+            if (pb[23] >= 0.0) {
+                double tany = 0.0, tanz = 0.0;
+                for (int m = n; m >= 0; --m) {   // the last marker up to n with a tangent of its own
+                    const double *pm = d.probe + static_cast<size_t>(m) * 24;
+                    if (pm[23] > 0.5) {
+                        tany = pm[21];
+                        tanz = pm[22];
+                        break;
+                    }
                 }
+                const double *ucy = pb, *ucz = pb + 7, *pc = pb + 14;
+                const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
+                double dpdnw = d.lmacc[2 * n] * nory + d.lmacc[2 * n + 1] * norz;
+                dpdnw = -1.0 * dpdnw;
+                const double dpdne = pc[1] * nory + pc[2] * norz;
+                d.press[n] = pc[0] - 0.5 * (dpdnw + dpdne) * hpr;
+                const double ducdn = (ucy[1] * tany * nory + ucy[2] * tany * norz + ucz[1] * tanz * nory +
+                                      ucz[2] * tanz * norz);
+                const double d3ucdn3 = (pc[3] * nory * nory + pc[4] * nory * norz + pc[5] * norz * nory +
+                                        pc[6] * norz * norz) * 1.0 / visc;
+                const double d2ucdn2 = (ucy[3] * tany * nory * nory + ucy[4] * tany * nory * norz +
+                                        ucy[5] * tany * norz * nory + ucy[6] * tany * norz * norz +
+                                        ucz[3] * tanz * nory * nory + ucz[4] * tanz * nory * norz +
+                                        ucz[5] * tanz * norz * nory + ucz[6] * tanz * norz * norz);
+                const double ducdnm = ducdn - d2ucdn2 * hpr - 0.5 * d3ucdn3 * (hpr * hpr);
+                d.tau[2 * n] = visc * ducdnm * tany;
+                d.tau[2 * n + 1] = visc * ducdnm * tanz;
             }
-            const double *ucy = pb, *ucz = pb + 7, *pc = pb + 14;
-            const double nory = d.lmnor[2 * n], norz = d.lmnor[2 * n + 1];
-            double dpdnw = d.lmacc[2 * n] * nory + d.lmacc[2 * n + 1] * norz;
-            dpdnw = -1.0 * dpdnw;
-            const double dpdne = pc[1] * nory + pc[2] * norz;
-            d.press[n] = pc[0] - 0.5 * (dpdnw + dpdne) * hpr;
-            const double ducdn = (ucy[1] * tany * nory + ucy[2] * tany * norz + ucz[1] * tanz * nory +
-                                  ucz[2] * tanz * norz);
-            const double d3ucdn3 = (pc[3] * nory * nory + pc[4] * nory * norz + pc[5] * norz * nory +
-                                    pc[6] * norz * norz) * 1.0 / visc;
-            const double d2ucdn2 = (ucy[3] * tany * nory * nory + ucy[4] * tany * nory * norz +
-                                    ucy[5] * tany * norz * nory + ucy[6] * tany * norz * norz +
-                                    ucz[3] * tanz * nory * nory + ucz[4] * tanz * nory * norz +
-                                    ucz[5] * tanz * norz * nory + ucz[6] * tanz * norz * norz);
-            const double ducdnm = ducdn - d2ucdn2 * hpr - 0.5 * d3ucdn3 * (hpr * hpr);
-            d.tau[2 * n] = visc * ducdnm * tany;
-            d.tau[2 * n + 1] = visc * ducdnm * tanz;
         }
+        sv = d.bcerrv[n] * d.bcerrv[n];
+        sw = d.bcerrw[n] * d.bcerrw[n];
     }
-    for (int n = threadIdx.x; n < d.nlm; n += blockDim.x) {
-        sv = sv + d.bcerrv[n] * d.bcerrv[n];
-        sw = sw + d.bcerrw[n] * d.bcerrw[n];
-    }
+    // the L2 norms of checkbcs (ckbcs.F90:76-81): block partials, summed in
+    // block order by the last block
     const double tv = block_reduce_fast<false>(sv, sh);
     const double tw = block_reduce_fast<false>(sw, sh);
+    const int b = blockIdx.x, nb = gridDim.x;
+    double *rv = d.red, *rw = d.red + kRedSlot;
     if (threadIdx.x == 0) {
-        d.scal[S_NBCV] = sqrt(tv) / static_cast<double>(d.nlm);
-        d.scal[S_NBCW] = sqrt(tw) / static_cast<double>(d.nlm);
+        rv[b] = tv;
+        rw[b] = tw;
+        __threadfence();
+        last = (atomicAdd(d.count + 1, 1u) == static_cast<unsigned>(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double av = 0.0, aw = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        av = av + __ldcg(rv + i);
+        aw = aw + __ldcg(rw + i);
+    }
+    av = block_reduce_fast<false>(av, sh);
+    aw = block_reduce_fast<false>(aw, sh);
+    if (threadIdx.x == 0) {
+        d.count[1] = 0u;
+        d.scal[S_NBCV] = sqrt(av) / static_cast<double>(d.nlm);
+        d.scal[S_NBCW] = sqrt(aw) / static_cast<double>(d.nlm);
     }
 }
 
-__global__ void __launch_bounds__(1024) k_loads_finish(Dev d) {
+constexpr int kLoadFin = 128;   // markers per block of the finish
+__global__ void __launch_bounds__(kLoadFin) k_loads_finish(Dev d) {
     FB_GRID_WAIT();
     loads_finish_body(d);
 }
@@ -1740,13 +1769,13 @@ __global__ void __launch_bounds__(1024) kg_substep_mid(const GroupCase *__restri
     substep_mid_body(d, slot, s.ga, s.ro);
 }
 
-__global__ void kg_loads_probe(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(3 * kLoadMk) kg_loads_probe(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     if (!stage_case(g, &d)) return;
-    loads_probe_body(d);
+    loads_probe_tan_body(d);
 }
 
-__global__ void __launch_bounds__(1024) kg_loads_finish(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(kLoadFin) kg_loads_finish(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     if (!stage_case(g, &d)) return;
     loads_finish_body(d);
@@ -1832,8 +1861,8 @@ void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream
 }
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
-    pdl(k_loads_probe, dim3((3 * d.nlm + 63) / 64), dim3(64), 0, s, d);
-    pdl(k_loads_finish, dim3(1), dim3(1024), 0, s, d);
+    pdl(k_loads_probe, dim3((d.nlm + kLoadMk - 1) / kLoadMk), dim3(3 * kLoadMk), 0, s, d);
+    pdl(k_loads_finish, dim3((d.nlm + kLoadFin - 1) / kLoadFin), dim3(kLoadFin), 0, s, d);
 }
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
     pdl(k_diag, dim3(std::min(stride_blocks(d), 2048)), dim3(256), 0, s, d, hist_rows);
@@ -1905,8 +1934,8 @@ void glaunch_substep_mid(const Group &g, int n_next, int slot, cudaStream_t s) {
 void glaunch_loads(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
     if (!d.nlm) return;
-    pdl(kg_loads_probe, zgrid(dim3((3 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
-    pdl(kg_loads_finish, zgrid(dim3(1), g), dim3(1024), 0, s, g.cases);
+    pdl(kg_loads_probe, zgrid(dim3((d.nlm + kLoadMk - 1) / kLoadMk), g), dim3(3 * kLoadMk), 0, s, g.cases);
+    pdl(kg_loads_finish, zgrid(dim3((d.nlm + kLoadFin - 1) / kLoadFin), g), dim3(kLoadFin), 0, s, g.cases);
 }
 void glaunch_rigid(const Group &g, cudaStream_t s, int mode) {
     if (g.rep.nlm) pdl(kg_rigid, zgrid(dim3(1), g), dim3(512), 0, s, g.cases, mode);

@@ -158,7 +158,10 @@ int fb_advance(fb_ctx *ctx, int ns0, int nsteps, double *hist);
 /* Marker-side coupling for a host rigid-body solver (the reference's own
  * rigid.F90 kept on the host): fb_get_loads copies press (nlm) and tau
  * (nlm x 2) to the host; fb_set_markers uploads lmcc, lmvel, lmacc, lmnor
- * (each nlm x 2, any may be NULL to keep the device copy). */
+ * (each nlm x 2, any may be NULL to keep the device copy).  fb_set_markers
+ * copies the arrays into the context's pinned staging memory before it
+ * returns (the caller's buffers are free again at once) and orders the
+ * device copies ahead of the context's next step without waiting for them. */
 int fb_get_loads(fb_ctx *ctx, double *press, double *tau);
 int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const double *lmacc,
                    const double *lmnor);
