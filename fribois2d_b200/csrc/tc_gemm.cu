@@ -31,6 +31,7 @@ namespace fb {
 namespace {
 
 constexpr int kBM = 128, kBK = 32, kThreads = 128;
+constexpr int kI8Threads = 256;   // the INT8 product: producer and MMA warps, eight epilogue warps
 
 // tile width BN (64 or 128) sets the B tiles, the stage count (192 KB ring),
 // the TMEM columns and the instruction descriptor
@@ -93,6 +94,17 @@ __device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         if (mbar_test_wait(bar, parity)) return true;
         if ((i & 255u) == 0 && global_ns() - t0 > 1000000000ull) return false;
     }
+}
+
+// the same wait for threads that only wait (the epilogue's): they sleep
+// between polls and leave the issue slots to the producer and MMA threads
+__device__ bool mbar_wait_idle(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    while (!mbar_test_wait(bar, parity)) {
+        __nanosleep(128);
+        if (global_ns() - t0 > 1000000000ull) return false;
+    }
+    return true;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
@@ -163,32 +175,25 @@ __device__ __forceinline__ double i32_as_f64(uint32_t v) {
     return __hiloint2double(0x43300000, static_cast<int>(v ^ 0x80000000u)) - 4503601774854144.0;
 }
 
-// 16 columns of 32 lanes without waiting; tmem_wait16 waits for every load
+// 8 columns of 32 lanes without waiting; tmem_wait8 waits for every load
 // issued so far and ties the registers to the wait (their uses follow it),
-// tmem_after16 ties further registers to the same point
-__device__ __forceinline__ void tmem_load16_async(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+// tmem_after8 ties further registers to the same point
+__device__ __forceinline__ void tmem_load8_async(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+__device__ __forceinline__ void tmem_wait8(uint32_t (&r)[8]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
-                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
-                   "+r"(r[15])
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])
                  :
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_after16(uint32_t (&r)[16]) {
+__device__ __forceinline__ void tmem_after8(uint32_t (&r)[8]) {
     asm volatile(""
-                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
-                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
-                   "+r"(r[15])
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])
                  :
                  : "memory");
 }
@@ -981,37 +986,39 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     }
     __syncwarp();
 
-    // ---- epilogue: TMEM lane = tile row; accumulators summed in FP64 from the smallest weight up
-    if (!mbar_wait(done, 0)) ok = false;
+    // ---- epilogue: TMEM lane = tile row; accumulators summed in FP64 from the
+    // smallest weight up.  Eight warps: warp w reads TMEM lanes 32 (w % 4) ..
+    // (its rows) and every other 8-column chunk, starting at chunk w / 4.
+    if (!mbar_wait_idle(done, 0)) ok = false;
     __syncwarp();
     tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
+    const int quarter = warp & 3;
+    const int row = m0 + quarter * 32 + lane;
     const bool rok = ok && row < o.M;
     const double rs = rok ? o.rowscale[row] : 0.0;
-    // 16 columns at a time: the kI8S classes' loads in flight together, one wait
 #pragma unroll 1
-    for (int c = 0; c < BN / 16; ++c) {
-        uint32_t v[kS][16];
+    for (int c = warp >> 2; c < BN / 8; c += kI8Threads / 128) {
+        uint32_t v[kS][8];
 #pragma unroll
         for (int t = 0; t < kS; ++t)
-            tmem_load16_async(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(t * BN + c * 16),
-                              v[t]);
-        tmem_wait16(v[0]);
+            tmem_load8_async(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(t * BN + c * 8),
+                             v[t]);
+        tmem_wait8(v[0]);
 #pragma unroll
-        for (int t = 1; t < kS; ++t) tmem_after16(v[t]);
-        double acc[16];
+        for (int t = 1; t < kS; ++t) tmem_after8(v[t]);
+        double acc[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+        for (int q = 0; q < 8; ++q) acc[q] = 0.0;
 #pragma unroll
         for (int t = kS - 1; t >= 0; --t) {
             const double wgt = ldexp(1.0, -7 * (t + 2));
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[q] = acc[q] + i32_as_f64(v[t][q]) * wgt;
+            for (int q = 0; q < 8; ++q) acc[q] = acc[q] + i32_as_f64(v[t][q]) * wgt;
         }
         if (rok) {
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int col = n0 + c * 16 + q;
+            for (int q = 0; q < 8; ++q) {
+                const int col = n0 + c * 8 + q;
                 if (col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
             }
         }
@@ -1026,7 +1033,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
 }
 
 template <int BN>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kI8Threads, 1)
     k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
                 int *status) {
     FB_GRID_WAIT();
@@ -1035,7 +1042,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // grouped: blockIdx.z selects the product
 template <int BN>
-__global__ void __launch_bounds__(kThreads, 1) kg_i8x8_gemm(const I8Task *__restrict__ t) {
+__global__ void __launch_bounds__(kI8Threads, 1) kg_i8x8_gemm(const I8Task *__restrict__ t) {
     FB_GRID_WAIT();
     const I8Task &tk = t[blockIdx.z];
     if (tk.gate && !*tk.gate) return;
@@ -1229,8 +1236,8 @@ void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, i
 
 void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st) {
     const dim3 grid((M + 127) / 128, (N + bn - 1) / bn, n);
-    if (bn == 48) pdl(kg_i8x8_gemm<48>, grid, dim3(kThreads), I8Cfg<48>::kSmem, st, tasks);
-    else pdl(kg_i8x8_gemm<64>, grid, dim3(kThreads), I8Cfg<64>::kSmem, st, tasks);
+    if (bn == 48) pdl(kg_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, tasks);
+    else pdl(kg_i8x8_gemm<64>, grid, dim3(kI8Threads), I8Cfg<64>::kSmem, st, tasks);
 }
 
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {
@@ -1249,8 +1256,8 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
 void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st) {
     I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows};
     const dim3 grid((a.rows + 127) / 128, (b.rows + b.box - 1) / b.box);
-    if (b.box == 48) pdl(k_i8x8_gemm<48>, grid, dim3(kThreads), I8Cfg<48>::kSmem, st, a.map, b.map, o, a.K, status);
-    else pdl(k_i8x8_gemm<64>, grid, dim3(kThreads), I8Cfg<64>::kSmem, st, a.map, b.map, o, a.K, status);
+    if (b.box == 48) pdl(k_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, a.map, b.map, o, a.K, status);
+    else pdl(k_i8x8_gemm<64>, grid, dim3(kI8Threads), I8Cfg<64>::kSmem, st, a.map, b.map, o, a.K, status);
 }
 
 }  // namespace fb
