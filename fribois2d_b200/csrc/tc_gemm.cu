@@ -785,6 +785,8 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     static_assert(kI8S == 8, "2^56 = 128^kI8S");
     // this CTA's words that lie inside ldk, per row
     const int nwords = static_cast<int>(max(0L, min(static_cast<long>(2 * V), (ldk - c0) / 4)));
+    constexpr int kUnroll = (V <= 32) ? kI8S : 1;   // constant shifts where registers allow
+#pragma unroll kUnroll
     for (int i = 0; i < kI8S; ++i) {
         uint32_t *bi = buf + (i & 1) * (32 * kRow);   // two buffers: one barrier per slice
         const int sh = 7 * (kI8S - 1 - i);
@@ -798,11 +800,16 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
             bi[lane * kRow + 8 * p + w] = (mag & ~m) | (__vsub4(0u, mag) & m);
         }
         __syncthreads();
-        for (int t = threadIdx.x; t < 32 * 2 * V; t += blockDim.x) {
-            const int row = t / (2 * V), wd = t - row * (2 * V);
-            if (wd < nwords)
-                *reinterpret_cast<uint32_t *>(dig + static_cast<size_t>(i) * plane +
-                                              static_cast<size_t>(r0 + row) * ldk + c0 + 4 * wd) = bi[row * kRow + wd];
+        // 16-byte stores: four words of a row at a time (c0 and ldk are
+        // multiples of 16 bytes, so every chunk is aligned)
+        constexpr int kQ = V / 2;   // 16-byte chunks per row
+        for (int t = threadIdx.x; t < 32 * kQ; t += blockDim.x) {
+            const int row = t / kQ, qd = t - row * kQ;
+            if (4 * qd < nwords) {
+                const uint32_t *w4 = bi + row * kRow + 4 * qd;
+                *reinterpret_cast<uint4 *>(dig + static_cast<size_t>(i) * plane + static_cast<size_t>(r0 + row) * ldk +
+                                           c0 + 16 * qd) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+            }
         }
     }
 }
