@@ -677,7 +677,6 @@ def device_arm(args, rank, world, local):
         L = fb.lib()
         ptr = [ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_double)) for b in pin]
         fptr = ctypes.cast(fc.data_ptr(), ctypes.POINTER(ctypes.c_double))
-        ids = (fb.IDS["lmcc"], fb.IDS["lmvel"], fb.IDS["lmacc"], fb.IDS["lmnor"])
         ns0 = W + K
         Ke = max(3, min(K, 20))
         barrier()
@@ -687,8 +686,7 @@ def device_arm(args, rank, world, local):
             assert L.fb_set_markers(s.ctx, *ptr) == 0
             assert L.fb_fluid_tsch(s.ctx, ns) == 0
             assert L.fb_rigid(s.ctx, ns, fptr) == 0
-            for b, idx in zip(ptr, ids):
-                assert L.fb_get_array(s.ctx, idx, b, 2 * nlm) == 0
+            assert L.fb_get_markers(s.ctx, *ptr) == 0
         barrier()
         te = time.perf_counter() - te0
         te_max = max_over_ranks(dist, te, dev)

@@ -90,6 +90,7 @@ def lib() -> ctypes.CDLL:
         "fb_advance": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
         "fb_get_loads": ([vp, dp, dp], ctypes.c_int),
         "fb_set_markers": ([vp, dp, dp, dp, dp], ctypes.c_int),
+        "fb_get_markers": ([vp, dp, dp, dp, dp], ctypes.c_int),
         "fb_get_dims": ([vp, ip], ctypes.c_int),
         "fb_get_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
         "fb_set_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
@@ -399,6 +400,12 @@ class Solver:
                 for a in (lmcc, lmvel, lmacc, lmnor)]
         ptrs = [ctypes.POINTER(ctypes.c_double)() if a is None else _dp(a) for a in arrs]
         _check(self._lib.fb_set_markers(self.ctx, *ptrs), "fb_set_markers")
+
+    def get_markers(self):
+        """lmcc, lmvel, lmacc, lmnor, each (nlm, 2), read with one wait."""
+        out = [np.empty(2 * self.nlm) for _ in range(4)]
+        _check(self._lib.fb_get_markers(self.ctx, *[_dp(a) for a in out]), "fb_get_markers")
+        return [a.reshape(self.nlm, 2) for a in out]
 
     # ---- stages (one reference subroutine each)
     def set_substep(self, ns: int, n: int) -> None:

@@ -1744,6 +1744,19 @@ int fb_set_markers(fb_ctx *c, const double *lmcc, const double *lmvel, const dou
     return FB_OK;
 }
 
+int fb_get_markers(fb_ctx *c, double *lmcc, double *lmvel, double *lmacc, double *lmnor) {
+    if (!c) return FB_ERR_STATE;
+    const size_t b = 2 * static_cast<size_t>(c->d.nlm) * sizeof(double);
+    if (!b) return FB_OK;
+    CK(cudaSetDevice(c->device));
+    double *dst[4] = {lmcc, lmvel, lmacc, lmnor};
+    const double *src[4] = {c->d.lmcc, c->d.lmvel, c->d.lmacc, c->d.lmnor};
+    for (int i = 0; i < 4; ++i)
+        if (dst[i]) CK(cudaMemcpyAsync(dst[i], src[i], b, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FB_OK;
+}
+
 int fb_get_dims(fb_ctx *c, int32_t dims[8]) {
     if (!c || !dims) return FB_ERR_STATE;
     dims[0] = c->d.n2;

@@ -709,16 +709,14 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // 2^-55 of its largest entry.
 
 // The digit cut in one launch: a cluster of kCutCl CTAs per 32 rows, each
-// CTA over its own range of 8 V columns.  Thread (lane, warp w) holds row
-// lane's columns c0 + 32 p + 4 w + q (p < V / 4, q < 4) in registers, all
-// its loads in flight at once (each load coalesced over the 32 rows); the
-// CTA's row maxima go to the cluster through distributed shared memory, so
-// every CTA derives each row's exponent from the whole row; then each CTA
-// turns its values into 56-bit integers (one conversion each), takes the
-// digits from them with shifts, four columns to a 32-bit word, and writes
-// one slice at a time through two alternating shared-memory buffers (rows
-// of 2 V + 1 words: conflict-free) with coalesced stores along k.  The
-// operand is read once.
+// CTA over its own range of 8 V columns.  Thread (lane, warp w) holds V
+// consecutive columns of row lane in registers, all its loads in flight at
+// once (each load coalesced over the 32 rows); the CTA's row maxima go to the
+// cluster through distributed shared memory, so every CTA derives each row's
+// exponent from the whole row; then each thread turns its values into 56-bit
+// integers (one conversion each), takes the digits from them with shifts,
+// four columns to a 32-bit word, and stores each slice's V digit bytes of its
+// row with one 16-byte (or 8- or 4-byte) store.  The operand is read once.
 // Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
@@ -727,23 +725,22 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
                                             long ldk, long plane, double *rowscale) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
-    constexpr int kP = V / 4, kRow = 2 * V + 1;   // words per row of the slice buffer (odd)
-    static_assert(V % 4 == 0, "four columns to a word");
+    constexpr int kP = V / 4;   // 32-bit words (four columns) per thread and slice
+    static_assert(V == 4 || V == 8 || V % 16 == 0, "a thread's run of columns is one 4-, 8- or 16-byte store");
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
-    __shared__ uint32_t buf[2 * 32 * kRow];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int rank = static_cast<int>(cl.block_rank());
     const int r0 = (blockIdx.x / kCutCl) * 32, r = r0 + lane;
-    const int c0 = rank * 8 * V;
+    const int c0 = rank * 8 * V + V * w;   // this thread's V consecutive columns of row r
     double a[kP][4];
     double m = 0.0;
 #pragma unroll
     for (int p = 0; p < kP; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int k = c0 + 32 * p + 4 * w + q;
+            const int k = c0 + 4 * p + q;   // each load coalesced over the warp's 32 rows
             a[p][q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
         }
 #pragma unroll
@@ -783,32 +780,36 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
         }
     }
     static_assert(kI8S == 8, "2^56 = 128^kI8S");
-    // this CTA's words that lie inside ldk, per row
-    const int nwords = static_cast<int>(max(0L, min(static_cast<long>(2 * V), (ldk - c0) / 4)));
+    // each slice's V digits of row r are V consecutive bytes: the thread
+    // stores them itself (a whole 32-byte sector between neighbouring warps),
+    // no shared-memory transpose; rows up to rows_pad get digits (zero past R)
+    const bool live = c0 < ldk;   // ldk is a multiple of 128, so a run is inside or wholly past it
+    int8_t *out = dig + static_cast<size_t>(r) * ldk + c0;
     constexpr int kUnroll = (V <= 32) ? kI8S : 1;   // constant shifts where registers allow
 #pragma unroll kUnroll
     for (int i = 0; i < kI8S; ++i) {
-        uint32_t *bi = buf + (i & 1) * (32 * kRow);   // two buffers: one barrier per slice
         const int sh = 7 * (kI8S - 1 - i);
+        uint32_t word[kP];
 #pragma unroll
         for (int p = 0; p < kP; ++p) {
             uint32_t mag = 0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
             // the negative values' bytes negated (bytewise, no carries between bytes)
-            const uint32_t m = neg[p];
-            bi[lane * kRow + 8 * p + w] = (mag & ~m) | (__vsub4(0u, mag) & m);
+            const uint32_t mk = neg[p];
+            word[p] = (mag & ~mk) | (__vsub4(0u, mag) & mk);
         }
-        __syncthreads();
-        // 16-byte stores: four words of a row at a time (c0 and ldk are
-        // multiples of 16 bytes, so every chunk is aligned)
-        constexpr int kQ = V / 2;   // 16-byte chunks per row
-        for (int t = threadIdx.x; t < 32 * kQ; t += blockDim.x) {
-            const int row = t / kQ, qd = t - row * kQ;
-            if (4 * qd < nwords) {
-                const uint32_t *w4 = bi + row * kRow + 4 * qd;
-                *reinterpret_cast<uint4 *>(dig + static_cast<size_t>(i) * plane + static_cast<size_t>(r0 + row) * ldk +
-                                           c0 + 16 * qd) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        if (live) {
+            int8_t *o = out + static_cast<size_t>(i) * plane;
+            if constexpr (V >= 16) {
+#pragma unroll
+                for (int v4 = 0; v4 < V / 16; ++v4)
+                    reinterpret_cast<uint4 *>(o)[v4] =
+                        make_uint4(word[4 * v4], word[4 * v4 + 1], word[4 * v4 + 2], word[4 * v4 + 3]);
+            } else if constexpr (V == 8) {
+                *reinterpret_cast<uint2 *>(o) = make_uint2(word[0], word[1]);
+            } else {
+                *reinterpret_cast<uint32_t *>(o) = word[0];
             }
         }
     }
@@ -835,7 +836,7 @@ __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
 // columns per thread: the CTA's share of ldk over its 8 warps
 inline int cut_values(long ldk) {
     const long per = (ldk + 8 * kCutCl - 1) / (8 * kCutCl);
-    for (int v : {4, 8, 12, 16, 24, 32, 48})
+    for (int v : {4, 8, 16, 32})
         if (per <= v) return v;
     return 64;
 }
@@ -1235,7 +1236,7 @@ void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, i
     switch (cut_values(rep.ldk)) {
 #define FB_CUT_CASE(V) \
     case V: pdl(kg_i8_cut<V>, grid, dim3(256), 0, st, tasks, R, K); break;
-        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(12) FB_CUT_CASE(16) FB_CUT_CASE(24) FB_CUT_CASE(32) FB_CUT_CASE(48)
+        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(16) FB_CUT_CASE(32)
 #undef FB_CUT_CASE
     default: pdl(kg_i8_cut<64>, grid, dim3(256), 0, st, tasks, R, K); break;
     }
@@ -1253,7 +1254,7 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
     switch (cut_values(p.ldk)) {
 #define FB_CUT_CASE(V) \
     case V: pdl(k_i8_cut<V>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
-        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(12) FB_CUT_CASE(16) FB_CUT_CASE(24) FB_CUT_CASE(32) FB_CUT_CASE(48)
+        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(16) FB_CUT_CASE(32)
 #undef FB_CUT_CASE
     default: pdl(k_i8_cut<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
     }

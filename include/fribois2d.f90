@@ -79,6 +79,11 @@ module fribois2d_gpu
       type(c_ptr), value :: ctx
       real(c_double), dimension(*), intent(in) :: lmcc, lmvel, lmacc, lmnor
     end function
+    integer(c_int) function fb_get_markers(ctx, lmcc, lmvel, lmacc, lmnor) bind(C, name="fb_get_markers")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), dimension(*), intent(out) :: lmcc, lmvel, lmacc, lmnor
+    end function
     integer(c_int) function fb_last_history(ctx, row) bind(C, name="fb_last_history")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx

@@ -165,6 +165,10 @@ int fb_advance(fb_ctx *ctx, int ns0, int nsteps, double *hist);
 int fb_get_loads(fb_ctx *ctx, double *press, double *tau);
 int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const double *lmacc,
                    const double *lmnor);
+/* The same four marker arrays back to the host (any may be NULL), with one
+ * wait for all of them: the per-step read of a host that keeps its own
+ * marker state (fb_get_array per array waits once per array). */
+int fb_get_markers(fb_ctx *ctx, double *lmcc, double *lmvel, double *lmacc, double *lmnor);
 
 /* Last history row written (FB_HIST_COLS doubles), for per-step callers. */
 int fb_last_history(fb_ctx *ctx, double *row);

@@ -85,3 +85,35 @@ def test_report_diagnostics_match_the_fields(tmp_path):
     lines = (tmp_path / "out" / "fluid_rep.out").read_text().splitlines()
     assert len(lines) == 3 and float(lines[2][25:41]) == pytest.approx(c.params.dt, rel=1e-8)
     s.close()
+
+
+def test_marker_round_trip_through_the_host(tmp_path):
+    """fb_set_markers returns before its device copies finish (staged in pinned
+    memory) and fb_get_markers reads all four arrays with one wait: a host
+    that keeps its own marker state, stepping per call, gets exactly the
+    stepping of the device-side state, and the caller's buffers may be reused
+    at once."""
+    c = cases.tiny_cylinder()
+    path = c.write(str(tmp_path / c.name))
+    a, b = _solver(c, path), _solver(c, path)
+    a.advance(0, 5)
+    b.advance(0, 5)
+    names = ("lmcc", "lmvel", "lmacc", "lmnor")
+    for ns in range(5, 15):
+        got = b.get_markers()
+        for g, n in zip(got, names):
+            np.testing.assert_array_equal(g.reshape(-1), b.get(n).reshape(-1))
+        bufs = [g.copy() for g in got]
+        b.set_markers(*bufs)
+        for buf in bufs:
+            buf[:] = np.nan   # reused at once: the staged copy is what the device receives
+        a.fluid_tsch(ns)
+        a.rigid(ns)
+        b.fluid_tsch(ns)
+        b.rigid(ns)
+    for f in ("q2", "q3", "pr"):
+        np.testing.assert_array_equal(a.get(f), b.get(f))
+    for g, n in zip(b.get_markers(), names):
+        np.testing.assert_array_equal(g.reshape(-1), a.get(n).reshape(-1))
+    a.close()
+    b.close()
