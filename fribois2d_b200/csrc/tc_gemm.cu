@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // exponent from the whole row; then each thread turns its values into 56-bit
 // integers (one conversion each), takes the digits from them with shifts,
 // four columns to a 32-bit word, and stores each slice's V digit bytes of its
-// row with one 16-byte (or 8- or 4-byte) store.  The operand is read once.
+// row with 16-byte stores.  The operand is read once.
 // Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
@@ -726,7 +726,7 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     constexpr int kP = V / 4;   // 32-bit words (four columns) per thread and slice
-    static_assert(V == 4 || V == 8 || V % 16 == 0, "a thread's run of columns is one 4-, 8- or 16-byte store");
+    static_assert(V % 16 == 0, "a thread's run of columns is whole 16-byte stores");
     __shared__ double part[32];
     __shared__ double mx[8][32];
     __shared__ double sc[32];
@@ -801,16 +801,10 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
         }
         if (live) {
             int8_t *o = out + static_cast<size_t>(i) * plane;
-            if constexpr (V >= 16) {
 #pragma unroll
-                for (int v4 = 0; v4 < V / 16; ++v4)
-                    reinterpret_cast<uint4 *>(o)[v4] =
-                        make_uint4(word[4 * v4], word[4 * v4 + 1], word[4 * v4 + 2], word[4 * v4 + 3]);
-            } else if constexpr (V == 8) {
-                *reinterpret_cast<uint2 *>(o) = make_uint2(word[0], word[1]);
-            } else {
-                *reinterpret_cast<uint32_t *>(o) = word[0];
-            }
+            for (int v4 = 0; v4 < V / 16; ++v4)
+                reinterpret_cast<uint4 *>(o)[v4] =
+                    make_uint4(word[4 * v4], word[4 * v4 + 1], word[4 * v4 + 2], word[4 * v4 + 3]);
         }
     }
 }
@@ -836,9 +830,8 @@ __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
 // columns per thread: the CTA's share of ldk over its 8 warps
 inline int cut_values(long ldk) {
     const long per = (ldk + 8 * kCutCl - 1) / (8 * kCutCl);
-    for (int v : {4, 8, 16, 32})
-        if (per <= v) return v;
-    return 64;
+    // at least 16: whole 16-byte stores per slice and thread
+    return per <= 16 ? 16 : per <= 32 ? 32 : 64;
 }
 
 // BN: output tile width, 64 or 48 (a 128 x 48 tile puts 132 CTAs on a
@@ -1236,7 +1229,7 @@ void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, i
     switch (cut_values(rep.ldk)) {
 #define FB_CUT_CASE(V) \
     case V: pdl(kg_i8_cut<V>, grid, dim3(256), 0, st, tasks, R, K); break;
-        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(16) FB_CUT_CASE(32)
+        FB_CUT_CASE(16) FB_CUT_CASE(32)
 #undef FB_CUT_CASE
     default: pdl(kg_i8_cut<64>, grid, dim3(256), 0, st, tasks, R, K); break;
     }
@@ -1254,7 +1247,7 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
     switch (cut_values(p.ldk)) {
 #define FB_CUT_CASE(V) \
     case V: pdl(k_i8_cut<V>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
-        FB_CUT_CASE(4) FB_CUT_CASE(8) FB_CUT_CASE(16) FB_CUT_CASE(32)
+        FB_CUT_CASE(16) FB_CUT_CASE(32)
 #undef FB_CUT_CASE
     default: pdl(k_i8_cut<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
     }

@@ -403,9 +403,10 @@ __global__ void __launch_bounds__(kYLines * W * 32) k_ylines(Dev d, ScanSys s2, 
 // ---------------------------------------------------------------- Poisson modes
 
 // The per-mode y solves of phcalc (phcalc_outflow.F90:34-56): one warp per
-// mode.  The block loads the y off-diagonals once; each warp copies its
-// mode's right-hand side (a row of hmn) and reciprocal pivots to its own
-// shared-memory rows with coalesced loads, then solves with lane chunks of
+// mode.  The block copies the y off-diagonals once and each warp its mode's
+// right-hand side (a row of hmn) and reciprocal pivots to its own
+// shared-memory rows, all with cp.async in flight together (one wait instead
+// of a round trip per element group), then solves with lane chunks of
 // an odd length m (conflict-free 8-byte shared accesses): each lane composes
 // its chunk of the forward recurrence y(i) = a(i) y(i-1) + b(i),
 // a(i) = -amphj(i+1) g(i-1), the warp scans the composites, the lanes apply
@@ -418,9 +419,10 @@ __device__ __forceinline__ void ymodes_body(const Dev &d, int nw) {
     double *am = sm, *ap = sm + (n + 2);                       // 1-based off-diagonals
     double *line = sm + 2 * (n + 2) + static_cast<size_t>(w) * 2 * (n + 1);
     double *piv = line + (n + 1);
+    // every copy of the block in flight at once (cp.async), one wait
     for (int i = threadIdx.x; i <= n + 1; i += blockDim.x) {
-        am[i] = d.amphj[i];
-        ap[i] = d.apphj[i];
+        cp8(am + i, d.amphj + i);
+        cp8(ap + i, d.apphj + i);
     }
     const int r = blockIdx.x * nw + w;
     const bool live = (w < nw) && (r < d.n3m);
@@ -428,10 +430,11 @@ __device__ __forceinline__ void ymodes_body(const Dev &d, int nw) {
     if (live) {
         const double *pgr = d.pg + static_cast<size_t>(r) * d.ldh;
         for (int i = lane; i < n; i += 32) {
-            line[i] = __ldcg(row + i);
-            piv[i] = __ldg(pgr + i);
+            cp8(line + i, row + i);
+            cp8(piv + i, pgr + i);
         }
     }
+    cp_wait();
     __syncthreads();   // the off-diagonals (and every line) are staged
     if (!live) return;
     const int m = ((n + 31) / 32) | 1;
