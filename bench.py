@@ -277,9 +277,7 @@ def kernel_table(fb, path, c, poisson="int8x8", sweeps=2):
         # reads the FP64 operand and writes 8 int8 planes (16 B per cell)
         transform = [
             ("i8x8 GEMM (tcgen05 kind::i8, 36 digit pairs)", "i8x8_gemm", 6, 36 * gemm, "tensor_i8"),
-            # the cut of dph computes the divergence from q2, q3 (divg is not launched)
-            ("i8 digit cut with divg fused (dph from q2, q3)", "i8_split_div", 3, 4.0 * B, "hbm"),
-            ("i8 digit cut (hmn)", "i8_split", 3, 2.0 * B, "hbm"),
+            ("i8 digit cut (one cluster launch)", "i8_split", 6, 2.0 * B, "hbm"),
             ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
         ] + dgemm_rows
     elif poisson == "fp64":
@@ -298,7 +296,7 @@ def kernel_table(fb, path, c, poisson="int8x8", sweeps=2):
         ("boucdq", "boucdq", 3, 8.0 * 8 * n2m, "hbm"),
         ("nl_rhs", "nl_rhs", 3, 9 * B, "hbm"),
         ("helsolve (windowed, one launch)", "helsolve", 3, 10 * B, "hbm"),
-        ("divg", "divg", 0 if poisson == "int8x8" else 3, 3 * B, "hbm"),
+        ("divg", "divg", 3, 3 * B, "hbm"),
     ] + transform + [
         ("updvp_prcalc", "updvp", 3, 7 * B, "hbm"),
         ("submean_boucqt", "pr_submean", 3, 2 * B, "hbm"),

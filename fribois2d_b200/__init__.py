@@ -47,7 +47,7 @@ BOUNDARY = ("qb2s", "qb2n", "dqb2s", "dqb2n", "qb3s", "qb3n", "dqb3s", "dqb3n", 
 STAGES = dict(cfl=0, boucdq=1, nl_rhs=2, lgrdistribution=6, forcing=7, helsolve=8, divg=9,
               phcalc=10, updvp=11, pr_submean=13, checkbcs=15, loads=16, rigid=17,
               gemm_fwd=100, poisson_tri=101, gemm_bwd=102, tf32x3_gemm=103, i8_split=104,
-              i8x8_gemm=105, i8_split_div=106)
+              i8x8_gemm=105)
 HIST_COLS = 31
 HIST_NAMES = ("time", "Fy", "Fz", "M", "Fyp", "Fzp", "Fyv", "Fzv", "time_end", "py", "pz", "pa",
               "vy", "vz", "va", "ay", "az", "aa", "nbcv", "nbcw", "cflm", "dt",

@@ -860,21 +860,6 @@ int setup_i8(fb_ctx *c) {
 
 // phcalc with the transforms on the INT8 tensor cores (phcalc_outflow.F90:31,
 // 61-69): hmn = dph zmmt^T, per-mode y solves, dph = hmn zmm^T
-// divg + phcalc of the fused step: the cut of the first transform's operand
-// computes the divergence itself, so dph is first written by the second
-// transform (the stored-dph path below gives the same digits)
-int phcalc_i8_div(fb_ctx *c, double usdtal) {
-    const Dev &d = c->d;
-    cudaStream_t st = c->stream;
-    fb::launch_i8_split_div(d, usdtal, c->i8a, st);
-    fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
-    fb::launch_scan_poisson(d, st);
-    fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
-    fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st);
-    c->own_launches += 5;
-    return FB_OK;
-}
-
 int phcalc_i8(fb_ctx *c) {
     const Dev &d = c->d;
     cudaStream_t st = c->stream;
@@ -926,15 +911,11 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         break;
     case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
     case FB_ST_PHCALC:
-        // kOwn counts the mode solves of the DGEMM form; the tensor-core forms
-        // count all of their own launches themselves
         if (c->poisson_mode == FB_POISSON_TF32X3) {
-            c->own_launches -= 1;
             if ((r = phcalc_tf32(c))) return r;
             break;
         }
         if (c->poisson_mode == FB_POISSON_INT8X8) {
-            c->own_launches -= 1;
             if ((r = phcalc_i8(c))) return r;
             break;
         }
@@ -961,10 +942,6 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_TK_I8X8_GEMM:
         if (!c->i8_ready) return FB_ERR_STATE;
         fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
-        break;
-    case FB_TK_I8_SPLIT_DIV:
-        if (!c->i8_ready) return FB_ERR_STATE;
-        fb::launch_i8_split_div(d, c->usdtal[n - 1], c->i8a, st);
         break;
     default: return FB_ERR_STATE;
     }
@@ -1037,12 +1014,8 @@ int enqueue_fluid(fb_ctx *c, int ns) {
             if ((r = stage_impl(c, FB_ST_FORCING, ns, n == 1 ? 2 : n))) return r;
         }
         if ((r = stage_impl(c, FB_ST_HELSOLVE, ns, n))) return r;
-        if (c->poisson_mode == FB_POISSON_INT8X8) {
-            if ((r = phcalc_i8_div(c, c->usdtal[n - 1]))) return r;
-        } else {
-            if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
-            if ((r = stage_impl(c, FB_ST_PHCALC, ns, n))) return r;
-        }
+        if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
+        if ((r = stage_impl(c, FB_ST_PHCALC, ns, n))) return r;
         if (pend) {
             fb::launch_updvp_prcalc(d, al, al * c->beta, c->stream, true);
             c->own_launches += 1;

@@ -720,16 +720,9 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
-// value (row r, column k) of a cut operand stored column-major
-struct ColMajor {
-    const double *src;
-    long lds;
-    __device__ __forceinline__ double operator()(int r, int k) const { return src[static_cast<size_t>(k) * lds + r]; }
-};
-
-template <int V, class Load>
-__device__ __forceinline__ void i8_cut_body(const Load &load, int R, int K, int8_t *dig, long ldk, long plane,
-                                            double *rowscale) {
+template <int V>
+__device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long lds, int R, int K, int8_t *dig,
+                                            long ldk, long plane, double *rowscale) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     constexpr int kP = V / 4;   // 32-bit words (four columns) per thread and slice
@@ -748,7 +741,7 @@ __device__ __forceinline__ void i8_cut_body(const Load &load, int R, int K, int8
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int k = c0 + 4 * p + q;   // each load coalesced over the warp's 32 rows
-            a[p][q] = (r < R && k < K) ? load(r, k) : 0.0;
+            a[p][q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
         }
 #pragma unroll
     for (int p = 0; p < kP; ++p)
@@ -821,31 +814,7 @@ __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
     k_i8_cut(const double *__restrict__ src, long lds, int R, int K, int8_t *dig, long ldk, long plane,
              double *rowscale) {
     FB_GRID_WAIT();
-    i8_cut_body<V>(ColMajor{src, lds}, R, K, dig, ldk, plane, rowscale);
-}
-
-// the cut of divg's output computed from the velocities: row r is j = r + 1,
-// column k is z row k + 1, and the value is divergence.F90's
-// (q2(j+1,k) - q2(j,k)) udx2m(j) + (q3(j,k+1) - q3(j,k)) udx3m(k), times
-// usdtal, rounded operation by operation as k_divg computes it (no
-// contraction), so the digits equal the cut of the stored dph
-struct DivOfQ {
-    const double *q2, *q3, *udx2m, *udx3m;
-    long P;
-    double usdtal;
-    __device__ __forceinline__ double operator()(int r, int k) const {
-        const size_t c = static_cast<size_t>(k + 1) * P + r;   // (j, k+1) with j = r + 1
-        const double dv = __dmul_rn(__dsub_rn(q2[c + 1], q2[c]), udx2m[r + 1]);
-        const double dw = __dmul_rn(__dsub_rn(q3[c + P], q3[c]), udx3m[k + 1]);
-        return __dmul_rn(__dadd_rn(dv, dw), usdtal);
-    }
-};
-
-template <int V>
-__global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
-    k_i8_cut_div(DivOfQ dq, int R, int K, int8_t *dig, long ldk, long plane, double *rowscale) {
-    FB_GRID_WAIT();
-    i8_cut_body<V>(dq, R, K, dig, ldk, plane, rowscale);
+    i8_cut_body<V>(src, lds, R, K, dig, ldk, plane, rowscale);
 }
 
 // grouped (blockIdx.z = case; a cluster never spans two cases)
@@ -855,7 +824,7 @@ __global__ void __cluster_dims__(kCutCl, 1, 1) __launch_bounds__(256)
     const I8SplitTask t = tk[blockIdx.z];
     FB_GRID_WAIT();
     if (t.gate && !*t.gate) return;   // the whole cluster: one case
-    i8_cut_body<V>(ColMajor{t.src, t.lds}, R, K, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale);
+    i8_cut_body<V>(t.src, t.lds, R, K, t.dig, t.ldk, t.ldk * static_cast<long>(t.rows_pad), t.scale);
 }
 
 // columns per thread: the CTA's share of ldk over its 8 warps
@@ -1270,18 +1239,6 @@ void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStr
     const dim3 grid((M + 127) / 128, (N + bn - 1) / bn, n);
     if (bn == 48) pdl(kg_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, tasks);
     else pdl(kg_i8x8_gemm<64>, grid, dim3(kI8Threads), I8Cfg<64>::kSmem, st, tasks);
-}
-
-void launch_i8_split_div(const Dev &d, double usdtal, const I8Plan &p, cudaStream_t st) {
-    const dim3 grid(p.rows_pad / 32 * kCutCl);
-    const long plane = p.ldk * static_cast<long>(p.rows_pad);
-    const DivOfQ dq{d.q2, d.q3, d.udx2m, d.udx3m, static_cast<long>(d.P), usdtal};
-    const int R = d.n2m, K = d.n3m;
-    switch (cut_values(p.ldk)) {
-    case 16: pdl(k_i8_cut_div<16>, grid, dim3(256), 0, st, dq, R, K, p.dig, p.ldk, plane, p.scale); break;
-    case 32: pdl(k_i8_cut_div<32>, grid, dim3(256), 0, st, dq, R, K, p.dig, p.ldk, plane, p.scale); break;
-    default: pdl(k_i8_cut_div<64>, grid, dim3(256), 0, st, dq, R, K, p.dig, p.ldk, plane, p.scale); break;
-    }
 }
 
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st) {

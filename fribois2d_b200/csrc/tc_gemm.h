@@ -102,9 +102,6 @@ int i8_configure();
 int i8_plan(I8Plan &p, int rows, int K, int box_rows);
 // digits of the column-major source A(r, k) = src[k * lds + r], r < R, k < K
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
-// the cut of divg's output (dph rows 1..n3m) computed from q2, q3 on the fly,
-// digit for digit what launch_i8_split of the stored dph produces
-void launch_i8_split_div(const Dev &d, double usdtal, const I8Plan &p, cudaStream_t st);
 // out[c * ldo + r] = sum_k A(r, k) B(c, k)
 void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st);
 // the same over n cases of one shape (rep: geometry of the split)

@@ -33,7 +33,7 @@ module fribois2d_gpu
        FB_ST_FORCING = 7, FB_ST_HELSOLVE = 8, FB_ST_DIVG = 9, FB_ST_PHCALC = 10, FB_ST_UPDVP = 11, &
        FB_ST_PRSUBMEAN = 13, FB_ST_CHECKBCS = 15, FB_ST_LOADS = 16, FB_ST_RIGID = 17
   integer(c_int), parameter :: FB_TK_GEMM_FWD = 100, FB_TK_POISSON_TRI = 101, FB_TK_GEMM_BWD = 102, &
-       FB_TK_TF32X3_GEMM = 103, FB_TK_I8_SPLIT = 104, FB_TK_I8X8_GEMM = 105, FB_TK_I8_SPLIT_DIV = 106
+       FB_TK_TF32X3_GEMM = 103, FB_TK_I8_SPLIT = 104, FB_TK_I8X8_GEMM = 105
   ! options without a counterpart in the reference
   integer(c_int), parameter :: FB_BATCH_GROUPED = 0, FB_BATCH_GRAPH = 1
   integer(c_int), parameter :: FB_COUPLING_LOOSE = 0, FB_COUPLING_STRONG = 1, FB_COUPLING_LEARNED = 2

@@ -277,7 +277,6 @@ int fb_last_advance_ms(fb_ctx *ctx, double *ms);
 #define FB_TK_TF32X3_GEMM 103 /* one 3xTF32 tensor-core transform (precision form) */
 #define FB_TK_I8_SPLIT 104    /* digit cut of dph for the INT8 transform */
 #define FB_TK_I8X8_GEMM 105   /* one INT8 digit-slice transform, hmn = dph zmmt^T */
-#define FB_TK_I8_SPLIT_DIV 106 /* digit cut of the divergence computed from q2, q3 (the step's fused divg) */
 int fb_time_stage(fb_ctx *ctx, int stage, int n, int reps, double *ms);
 /* Number of this library's own kernels one captured time step launches
  * (library kernels of cuBLAS and CUB are not counted). */
