@@ -911,11 +911,15 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         break;
     case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
     case FB_ST_PHCALC:
+        // kOwn counts the mode solves of the DGEMM form; the tensor-core forms
+        // count all of their own launches themselves
         if (c->poisson_mode == FB_POISSON_TF32X3) {
+            c->own_launches -= 1;
             if ((r = phcalc_tf32(c))) return r;
             break;
         }
         if (c->poisson_mode == FB_POISSON_INT8X8) {
+            c->own_launches -= 1;
             if ((r = phcalc_i8(c))) return r;
             break;
         }
