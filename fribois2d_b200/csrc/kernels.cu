@@ -69,19 +69,35 @@ __device__ __forceinline__ void cfl_body(const Dev &d) {
     const int t = threadIdx.x, nt = blockDim.x;
     const int b = blockIdx.x, nb = gridDim.x;
     double qcf = 1.0e-8, q3a = 0.0;
-    // rows k over the blocks, columns j over the threads (no index division)
+    // rows k over the blocks, columns j over the threads (no index division);
+    // kU columns of a thread per pass, their loads all issued before the
+    // first use (the same per-thread order of the sum as one at a time)
+    constexpr int kU = 4;
     for (int k = b + 1; k <= d.n3m; k += nb) {
         const int kp = k + 1;
         const double udx3 = d.udx3m[k], dz = d.zz[kp] - d.zz[k];
-        for (int j = t + 1; j <= d.n2m; j += nt) {
-            const int jp = j + 1;
-            const double udx2 = d.udx2m[j];
-            const double q = (fabs((Fv(d.q2, j, k) + Fv(d.q2, jp, k)) * 0.5 * udx2) +
-                              fabs((Fv(d.q3, j, k) + Fv(d.q3, j, kp)) * 0.5 * udx3));
-            // fmax drops a NaN: a non-finite velocity turns into +inf, which
-            // every later fmax keeps, so the CFL test below catches it
-            qcf = fmax(qcf, (q == q) ? q : INFINITY);
-            q3a = q3a + Fv(d.q3, j, k) * dz * (d.rc[jp] - d.rc[j]);
+        for (int j0 = t + 1; j0 <= d.n2m; j0 += kU * nt) {
+            double a2[kU], b2[kU], a3[kU], b3[kU], u2[kU], rj[kU], rjp[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int j = min(j0 + u * nt, d.n2m), jp = j + 1;
+                a2[u] = Fv(d.q2, j, k);
+                b2[u] = Fv(d.q2, jp, k);
+                a3[u] = Fv(d.q3, j, k);
+                b3[u] = Fv(d.q3, j, kp);
+                u2[u] = d.udx2m[j];
+                rj[u] = d.rc[j];
+                rjp[u] = d.rc[jp];
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (j0 + u * nt > d.n2m) break;
+                const double q = (fabs((a2[u] + b2[u]) * 0.5 * u2[u]) + fabs((a3[u] + b3[u]) * 0.5 * udx3));
+                // fmax drops a NaN: a non-finite velocity turns into +inf, which
+                // every later fmax keeps, so the CFL test below catches it
+                qcf = fmax(qcf, (q == q) ? q : INFINITY);
+                q3a = q3a + a3[u] * dz * (rjp[u] - rj[u]);
+            }
         }
     }
     const double pm = block_reduce_fast<true>(qcf, sh);

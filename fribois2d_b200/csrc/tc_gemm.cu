@@ -861,7 +861,8 @@ template <int BN, bool kGlobalMaps>
 __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorMap *mb, const I8Out &o, int K,
                                           int *status) {
     using Cfg = I8Cfg<BN>;
-    constexpr int kS = kI8S, kAS = Cfg::kASlots;
+    constexpr int kS = kI8S, kAS = Cfg::kASlots, kAP = kAS / 2;   // A slots, in pairs of slices
+    static_assert(kAS % 2 == 0 && kS % 2 == 0, "A slices move in pairs");
     extern __shared__ uint8_t smraw[];
     const uint32_t raw = smem_u32(smraw);
     const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
@@ -882,7 +883,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
             mbar_init(bfull0 + 8 * q, 1);
             mbar_init(bempty0 + 8 * q, 1);
         }
-        for (int q = 0; q < kAS; ++q) {
+        for (int q = 0; q < kAP; ++q) {
             mbar_init(afull0 + 8 * q, 1);
             mbar_init(aempty0 + 8 * q, 1);
         }
@@ -905,7 +906,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
         if (kGlobalMaps) acquire_maps(ma, ma, mb, mb);
-        int ia = 0, nb = 0, slot = 0;
+        int ip = 0, nb = 0, ps = 0;   // A slice pairs issued, B stages issued, pair slot
         uint32_t aph = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
@@ -918,23 +919,24 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
                 tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
             nb = kb + 1;
 #pragma unroll
-            for (int i = 0; i < kS; ++i) {
-                if (!mbar_wait(aempty0 + 8 * slot, aph ^ 1u)) {
+            for (int i = 0; i < kS; i += 2) {   // slices i, i + 1 on one barrier
+                if (!mbar_wait(aempty0 + 8 * ps, aph ^ 1u)) {
                     ok = false;
                     break;
                 }
-                mbar_expect_tx(afull0 + 8 * slot, Cfg::kATile);
-                tma_load_3d(sA + slot * Cfg::kATile, ma, afull0 + 8 * slot, kb * kI8BK, m0, i);
-                ++ia;
-                if (++slot == kAS) {
-                    slot = 0;
+                mbar_expect_tx(afull0 + 8 * ps, 2 * Cfg::kATile);
+                tma_load_3d(sA + (2 * ps) * Cfg::kATile, ma, afull0 + 8 * ps, kb * kI8BK, m0, i);
+                tma_load_3d(sA + (2 * ps + 1) * Cfg::kATile, ma, afull0 + 8 * ps, kb * kI8BK, m0, i + 1);
+                ++ip;
+                if (++ps == kAP) {
+                    ps = 0;
                     aph ^= 1u;
                 }
             }
         }
         // every copy issued has landed before the CTA may finish
-        for (int q = (ia > kAS ? ia - kAS : 0); q < ia; ++q)
-            if (!mbar_wait(afull0 + 8 * (q % kAS), static_cast<uint32_t>(q / kAS) & 1u)) ok = false;
+        for (int q = (ip > kAP ? ip - kAP : 0); q < ip; ++q)
+            if (!mbar_wait(afull0 + 8 * (q % kAP), static_cast<uint32_t>(q / kAP) & 1u)) ok = false;
         for (int q = (nb > 2 ? nb - 2 : 0); q < nb; ++q)
             if (!mbar_wait(bfull0 + 8 * (q & 1), static_cast<uint32_t>(q >> 1) & 1u)) ok = false;
     } else if (warp == 1 && lane == 0) {
@@ -944,7 +946,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
         // covers up to 256 / BN B slices (N <= 256).
         constexpr int kG = 256 / BN;
         const uint64_t adesc = sw128_desc(sA), bdesc = sw128_desc(sB);
-        int slot = 0;
+        int ps = 0;
         uint32_t aph = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
@@ -955,28 +957,32 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
             tc_fence_after();
             const uint64_t bst = bdesc + static_cast<uint64_t>((sb * Cfg::kBStage) >> 4);
 #pragma unroll
-            for (int i = 0; i < kS; ++i) {
-                if (!mbar_wait(afull0 + 8 * slot, aph)) {
+            for (int i2 = 0; i2 < kS; i2 += 2) {   // A slices i2, i2 + 1: one wait, one commit
+                if (!mbar_wait(afull0 + 8 * ps, aph)) {
                     ok = false;
                     break;
                 }
-                const uint64_t ast = adesc + static_cast<uint64_t>((slot * Cfg::kATile) >> 4);
-                // B slices j0 .. j0+nsl-1 are consecutive rows in shared memory and
-                // their classes i+j0 .. consecutive TMEM column blocks: one MMA of
-                // N = nsl * BN covers nsl digit pairs
 #pragma unroll
-                for (int j0 = 0; j0 < kS - i; j0 += kG) {
-                    const int nsl = (kS - i - j0 < kG) ? kS - i - j0 : kG;
-                    const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * BN) >> 3) << 17);
-                    const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * BN);
-                    const uint64_t bj = bst + static_cast<uint64_t>((j0 * Cfg::kBSlice) >> 4);
+                for (int e = 0; e < 2; ++e) {
+                    const int i = i2 + e;
+                    const uint64_t ast = adesc + static_cast<uint64_t>(((2 * ps + e) * Cfg::kATile) >> 4);
+                    // B slices j0 .. j0+nsl-1 are consecutive rows in shared memory and
+                    // their classes i+j0 .. consecutive TMEM column blocks: one MMA of
+                    // N = nsl * BN covers nsl digit pairs
 #pragma unroll
-                    for (int kk = 0; kk < kI8BK / 32; ++kk)   // K = 32 bytes per MMA: +2 in the address field
-                        mma_i8(acc_t, ast + 2 * kk, bj + 2 * kk, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
+                    for (int j0 = 0; j0 < kS - i; j0 += kG) {
+                        const int nsl = (kS - i - j0 < kG) ? kS - i - j0 : kG;
+                        const uint32_t idesc = Cfg::kIdescBase | (static_cast<uint32_t>((nsl * BN) >> 3) << 17);
+                        const uint32_t acc_t = tmem + static_cast<uint32_t>((i + j0) * BN);
+                        const uint64_t bj = bst + static_cast<uint64_t>((j0 * Cfg::kBSlice) >> 4);
+#pragma unroll
+                        for (int kk = 0; kk < kI8BK / 32; ++kk)   // K = 32 bytes per MMA: +2 in the address field
+                            mma_i8(acc_t, ast + 2 * kk, bj + 2 * kk, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
+                    }
                 }
-                mma_commit(aempty0 + 8 * slot);   // frees the A slot once these MMAs have read it
-                if (++slot == kAS) {
-                    slot = 0;
+                mma_commit(aempty0 + 8 * ps);   // frees the two A slots once these MMAs have read them
+                if (++ps == kAP) {
+                    ps = 0;
                     aph ^= 1u;
                 }
             }
