@@ -551,6 +551,8 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         if ((st = dnew(c, &d.hslot, nlm * 2))) return st;
         if ((st = dnew(c, &d.chain, nlm * 2 * fb::kSD))) return st;
         if ((st = dnew(c, &d.chead, nlm * 2 * fb::kSD))) return st;
+        if ((st = dnew(c, &d.hlist, nlm * 2 * fb::kSD * fb::kHeadList))) return st;
+        if ((st = dnew(c, &d.hlen, nlm * 2 * fb::kSD))) return st;
     }
     if ((st = dnew(c, &d.probe, nlm * 24))) return st;
     if ((st = dnew(c, &d.press, nlm))) return st;

@@ -12,6 +12,7 @@ namespace fb {
 constexpr int kSD = 9;  // MLS support nodes per marker and direction (dimSD)
 constexpr int kBucket = 16;        // marker slots per spreading-table entry
 constexpr int kBucketLevels = 16;  // entries per start cell at most (256 boxes)
+constexpr int kHeadList = 8;       // chain members a head keeps in line (read with two 16-byte loads)
 
 struct TriDev {          // factors of one tridiagonal system (DGTTRF output)
     int n;
@@ -69,6 +70,8 @@ struct Dev {
     int *chain;              // per contribution slot: next slot of the same cell in marker
                              // order (>= 0) or -1 at the end, written by the cell's head
     int *chead;              // per contribution slot: 1 if it heads its cell's chain
+    int *hlist;              // per head slot: the chain's next kHeadList slots in order (then chain[])
+    int *hlen;               // per head slot: the chain's length after the head
     double *probe;           // [marker][24]: ucy(7), ucz(7), pc(7), tan(2), flag
     double *press, *tau, *bcerrv, *bcerrw;
     // rigid body

@@ -707,23 +707,25 @@ __global__ void k_mls_setup(Dev d) {
 // interp_spread (forcing_MLS.F90:135-182), interpolation half: the
 // provisional velocity q* = q + rhs (INVTR.F90:147,275) at the support,
 // direct forcing F = (V - u*)/dt and the per-node contributions cl*phi*F.
+// One (marker, direction) per 16 lanes, node m on lane m < kSD: the nine
+// support loads are independent, and each lane forms the sum of the nine
+// products in node order from the group's shuffles (the sequential sum).
+constexpr int kInterpLanes = 16;
 __device__ __forceinline__ void mls_interp_body(const Dev &d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * d.nlm) return;
-    if (*d.status) return;
-    const int n = t >> 1, idir = (t & 1) + 1;
+    const int T = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = T / kInterpLanes, m = T % kInterpLanes, lane = threadIdx.x & 31;
+    const bool have = t < 2 * d.nlm;
+    const bool stopped = (*d.status != 0);
+    const int tt = have ? t : 0;
+    const int n = tt >> 1, idir = (tt & 1) + 1;
     const double pos2 = d.lmcc[2 * n + 1];
-    double *c = d.contrib + static_cast<size_t>(t) * kSD;
-    if (!(d.zz[1] < pos2 && pos2 < d.zz[d.n3])) {
-        for (int m = 0; m < kSD; ++m) c[m] = 0.0;
-        return;
-    }
-    const double *phi = d.phi + static_cast<size_t>(t) * kSD;
-    const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
-    const double *q = (idir == 1) ? d.q2 : d.q3;
-    const double *r = (idir == 1) ? d.rhs2 : d.rhs3;
-    double u = 0.0;
-    for (int m = 0; m < kSD; ++m) {
+    const bool inside = (d.zz[1] < pos2 && pos2 < d.zz[d.n3]);
+    double phim = 0.0, prod = 0.0;
+    if (have && inside && m < kSD) {
+        const int *eu = d.eulins + static_cast<size_t>(tt) * 2 * kSD;
+        const double *q = (idir == 1) ? d.q2 : d.q3;
+        const double *r = (idir == 1) ? d.rhs2 : d.rhs3;
+        phim = d.phi[static_cast<size_t>(tt) * kSD + m];
         const int j = eu[m], k = eu[kSD + m];
         // q2f/q3f are written only where invtr2/invtr3 write them; elsewhere
         // the reference reads storage that was never set (zero here)
@@ -734,11 +736,19 @@ __device__ __forceinline__ void mls_interp_body(const Dev &d) {
             const size_t i = fidx(d, j, k);
             qf = q[i] + r[i];
         }
-        u = u + phi[m] * qf;
+        prod = phim * qf;
+    }
+    double u = 0.0;
+#pragma unroll
+    for (int mm = 0; mm < kSD; ++mm) u = u + __shfl_sync(0xffffffffu, prod, (lane & ~(kInterpLanes - 1)) + mm);
+    if (!have || stopped || m >= kSD) return;
+    double *c = d.contrib + static_cast<size_t>(tt) * kSD;
+    if (!inside) {
+        c[m] = 0.0;
+        return;
     }
     const double f = (d.lmvel[2 * n + idir - 1] - u) / d.dt;
-    const double clv = d.cl[t];
-    for (int m = 0; m < kSD; ++m) c[m] = clv * phi[m] * f;
+    c[m] = d.cl[tt] * phim * f;
 }
 
 __global__ void k_mls_interp(Dev d) {
@@ -815,7 +825,8 @@ __device__ __forceinline__ void spread_chains_body(const Dev &d) {
         raise_status(d, FB_ERR_UNSUPPORTED);
         return;
     }
-    // this slot heads the cell's chain: link the touchers in marker order
+    // this slot heads the cell's chain: link the touchers in marker order;
+    // the head also keeps the first kHeadList of them in line
     d.chead[g] = 1;
     int prev_slot = g;
     for (int p = 0; p < L; ++p) {
@@ -823,6 +834,9 @@ __device__ __forceinline__ void spread_chains_body(const Dev &d) {
         prev_slot = ls[p];
     }
     d.chain[prev_slot] = -1;
+    d.hlen[g] = L;
+    int *hl = d.hlist + static_cast<size_t>(g) * kHeadList;
+    for (int p = 0; p < kHeadList; ++p) hl[p] = (p < L) ? ls[p] : g;
 }
 
 __global__ void k_spread_chains(Dev d) {
@@ -838,8 +852,23 @@ __device__ __forceinline__ void mls_spread_body(const Dev &d) {
     const int t = g / kSD, dir = t & 1;
     const int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
     const int m = g % kSD;
+    // the head's in-line list gives the first kHeadList members at once
+    // (independent loads); a longer chain continues along chain[]; the sum
+    // runs in chain order
+    const int L = d.hlen[g];
+    const int4 *hl = reinterpret_cast<const int4 *>(d.hlist + static_cast<size_t>(g) * kHeadList);
+    const int4 h0 = hl[0], h1 = hl[1];
+    const int idx[kHeadList] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+    double cv[kHeadList];
+#pragma unroll
+    for (int p = 0; p < kHeadList; ++p) cv[p] = d.contrib[idx[p]];   // the head's own slot past the end
     double fe = 0.0;
-    for (int s = g; s >= 0; s = d.chain[s]) fe = fe + d.contrib[s];
+    fe = fe + d.contrib[g];
+#pragma unroll
+    for (int p = 0; p < kHeadList; ++p)
+        if (p < L) fe = fe + cv[p];
+    if (L > kHeadList)
+        for (int s = d.chain[idx[kHeadList - 1]]; s >= 0; s = d.chain[s]) fe = fe + d.contrib[s];
     double *r = (dir == 0) ? d.rhs2 : d.rhs3;
     const size_t i = fidx(d, eu[m], eu[kSD + m]);
     r[i] = r[i] + fe * d.dt;
@@ -1844,7 +1873,7 @@ void launch_mls_setup(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_mls_setup, dim3((2 * d.nlm + 63) / 64), dim3(64), 0, s, d);
 }
 void launch_mls_interp(const Dev &d, cudaStream_t s) {
-    if (d.nlm) pdl(k_mls_interp, dim3((2 * d.nlm + 63) / 64), dim3(64), 0, s, d);
+    if (d.nlm) pdl(k_mls_interp, dim3((2 * d.nlm * kInterpLanes + 255) / 256), dim3(256), 0, s, d);
 }
 void launch_spread_chains(const Dev &d, cudaStream_t s) {
     const int n = 2 * d.nlm * kSD;
@@ -1929,7 +1958,7 @@ void glaunch_marker_setup(const Group &g, cudaStream_t s) {
 void glaunch_forcing(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
     if (!d.nlm) return;
-    pdl(kg_mls_interp, zgrid(dim3((2 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
+    pdl(kg_mls_interp, zgrid(dim3((2 * d.nlm * kInterpLanes + 255) / 256), g), dim3(256), 0, s, g.cases);
     pdl(kg_mls_spread, zgrid(dim3((2 * d.nlm * kSD + 127) / 128), g), dim3(128), 0, s, g.cases);
 }
 void glaunch_divg(const Group &g, int n, cudaStream_t s) {
