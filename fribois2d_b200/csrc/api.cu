@@ -96,7 +96,7 @@ struct fb_ctx {
     bool cond_graph = true;                    // coupled step as a graph WHILE node (else a host loop)
     int tune_tk = 64;         // windowed helsolve tile height (autotuned per grid size)
     int tune_bn = 128;        // 3xTF32 GEMM tile width (autotuned per grid size)
-    int tune_i8bn = fb::kI8BN;  // INT8 digit-product tile width, 48 or 64 (autotuned per grid size)
+    int tune_i8bn = fb::kI8BN;  // INT8 digit-product tile width, 32, 48 or 64 (autotuned per grid size)
     bool i8_fixed = false;      // the width set by FRIBOIS2D_I8_TILE: not tuned
     // precision form of the Poisson solve (3xTF32 tensor-core transforms + one
     // FP64 refinement sweep); planes of TF32 splits, tensor maps, FP64 scratch
@@ -421,9 +421,9 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     }
     c->device = device;
     if (const char *hv = std::getenv("FRIBOIS2D_HELSOLVE")) c->allow_win = std::strcmp(hv, "scan") != 0;
-    if (const char *tw = std::getenv("FRIBOIS2D_I8_TILE")) {   // fixed INT8 product tile width (48 or 64)
+    if (const char *tw = std::getenv("FRIBOIS2D_I8_TILE")) {   // fixed INT8 product tile width (32, 48 or 64)
         const int w = std::atoi(tw);
-        if (w == 48 || w == 64) {
+        if (w == 32 || w == 48 || w == 64) {
             c->tune_i8bn = w;
             c->i8_fixed = true;
         }
@@ -2879,10 +2879,10 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
         }
         if (!r && want_ibn && !ibn) {
             double best = 1e30;
-            for (int cand : {64, 48}) {
+            for (int cand : {64, 48, 32}) {
                 double ms = 0.0;
                 if ((r = i8_tile(cand)) || (r = fb_time_stage(c, FB_TK_I8X8_GEMM, 1, 10, &ms))) break;
-                if (ms < best * 0.98) {   // 48 must win clearly
+                if (ms < best * 0.98) {   // a narrower tile must win clearly
                     best = ms;
                     ibn = cand;
                 }

@@ -834,8 +834,9 @@ inline int cut_values(long ldk) {
     return per <= 16 ? 16 : per <= 32 ? 32 : 64;
 }
 
-// BN: output tile width, 64 or 48 (a 128 x 48 tile puts 132 CTAs on a
-// 768 x 1024 product where 128 x 64 tiles leave a third of the 148 SMs idle)
+// BN: output tile width, 64, 48 or 32 (a 128 x 48 tile puts 132 CTAs on a
+// 768 x 1024 product where 128 x 64 tiles leave a third of the 148 SMs idle;
+// 32 spreads small products over more SMs, one MMA of N = 32 (8 - i) per A slice)
 template <int BN>
 struct I8Cfg {
     static constexpr uint32_t kATile = 128 * kI8BK;                 // one A digit slice: 128 rows x 128 B
@@ -1192,7 +1193,7 @@ void launch_split_t(const double *src, long lds, int R, int C, const SplitPlane 
 // ---- INT8 FP64 products: buffers, maps, launches
 int i8_plan(I8Plan &p, int rows, int K, int box_rows) {
     if (K > kI8MaxK) return FB_ERR_UNSUPPORTED;   // the int32 class sums would overflow
-    if (box_rows != 128 && box_rows != 64 && box_rows != 48) return FB_ERR_STATE;
+    if (box_rows != 128 && box_rows != 64 && box_rows != 48 && box_rows != 32) return FB_ERR_STATE;
     if (!p.dig || (p.ldk % 128) || p.rows_pad < rows) return FB_ERR_STATE;
     if (!g_encode) {
         void *fn = nullptr;
@@ -1226,7 +1227,11 @@ int i8_configure() {
                     cudaFuncSetAttribute(k_i8x8_gemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(I8Cfg<48>::kSmem)) == cudaSuccess &&
                     cudaFuncSetAttribute(kg_i8x8_gemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(I8Cfg<48>::kSmem)) == cudaSuccess;
+                                         static_cast<int>(I8Cfg<48>::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(k_i8x8_gemm<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<32>::kSmem)) == cudaSuccess &&
+                    cudaFuncSetAttribute(kg_i8x8_gemm<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(I8Cfg<32>::kSmem)) == cudaSuccess;
     return ok ? FB_OK : FB_ERR_CUDA;
 }
 
@@ -1244,6 +1249,7 @@ void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, i
 void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st) {
     const dim3 grid((M + 127) / 128, (N + bn - 1) / bn, n);
     if (bn == 48) pdl(kg_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, tasks);
+    else if (bn == 32) pdl(kg_i8x8_gemm<32>, grid, dim3(kI8Threads), I8Cfg<32>::kSmem, st, tasks);
     else pdl(kg_i8x8_gemm<64>, grid, dim3(kI8Threads), I8Cfg<64>::kSmem, st, tasks);
 }
 
@@ -1264,6 +1270,7 @@ void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *s
     I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows};
     const dim3 grid((a.rows + 127) / 128, (b.rows + b.box - 1) / b.box);
     if (b.box == 48) pdl(k_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, a.map, b.map, o, a.K, status);
+    else if (b.box == 32) pdl(k_i8x8_gemm<32>, grid, dim3(kI8Threads), I8Cfg<32>::kSmem, st, a.map, b.map, o, a.K, status);
     else pdl(k_i8x8_gemm<64>, grid, dim3(kI8Threads), I8Cfg<64>::kSmem, st, a.map, b.map, o, a.K, status);
 }
 
