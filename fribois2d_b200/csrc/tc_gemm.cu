@@ -855,9 +855,10 @@ struct I8Cfg {
 
 // One CTA per 128 x BN tile of C.  Per k-block of 128: the producer
 // thread loads all B slices (one barrier) and streams the A slices through
-// a ring; the MMA thread multiplies A slice i with B slices j < kI8S - i into
-// accumulators i + j (MMAs of K = 32 over up to four slices at once).  Every wait gives up after one
-// second with FB_ERR_TIMEOUT.
+// a ring, two slices per barrier; the MMA thread multiplies A slice i with B
+// slices j < kI8S - i into accumulators i + j (MMAs of K = 32 over up to
+// 256 / BN slices at once); eight warps drain the accumulators.  Every wait
+// gives up after one second with FB_ERR_TIMEOUT.
 template <int BN, bool kGlobalMaps>
 __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorMap *mb, const I8Out &o, int K,
                                           int *status) {
