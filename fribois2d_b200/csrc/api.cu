@@ -529,10 +529,22 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
         if ((st = h2d(c, d.qb3n, v.data(), v.size() * sizeof(double)))) return st;
     }
     const size_t nlm = static_cast<size_t>(std::max(d.nlm, 1));
-    if ((st = dup(c, &d.lmcc, c->hc.lmcc))) return st;
-    if ((st = dup(c, &d.lmvel, c->hc.lmvel))) return st;
-    if ((st = dup(c, &d.lmacc, c->hc.lmacc))) return st;
-    if ((st = dup(c, &d.lmnor, c->hc.lmnor))) return st;
+    {   // the four marker arrays in one allocation, in this order, so that a
+        // host's per-step marker exchange is one copy each way
+        const size_t m = c->hc.lmcc.size();
+        if (c->hc.lmvel.size() != m || c->hc.lmacc.size() != m || c->hc.lmnor.size() != m) return FB_ERR_STATE;
+        double *mk = nullptr;
+        if ((st = dnew(c, &mk, 4 * std::max<size_t>(m, 1)))) return st;
+        d.lmcc = mk;
+        d.lmvel = mk + m;
+        d.lmacc = mk + 2 * m;
+        d.lmnor = mk + 3 * m;
+        if ((st = h2d(c, d.lmcc, c->hc.lmcc.data(), m * sizeof(double))) ||
+            (st = h2d(c, d.lmvel, c->hc.lmvel.data(), m * sizeof(double))) ||
+            (st = h2d(c, d.lmacc, c->hc.lmacc.data(), m * sizeof(double))) ||
+            (st = h2d(c, d.lmnor, c->hc.lmnor.data(), m * sizeof(double))))
+            return st;
+    }
     if ((st = dup(c, &d.lmA, c->hc.lmA))) return st;
     if ((st = dup(c, &d.vert, c->hc.vert))) return st;
     if ((st = dnew(c, &d.lmind, nlm * 4))) return st;
@@ -1741,25 +1753,34 @@ int fb_set_markers(fb_ctx *c, const double *lmcc, const double *lmvel, const dou
     }
     const double *src[4] = {lmcc, lmvel, lmacc, lmnor};
     double *dst[4] = {c->d.lmcc, c->d.lmvel, c->d.lmacc, c->d.lmnor};
+    const bool all = lmcc && lmvel && lmacc && lmnor;   // the device arrays are contiguous: one copy
     for (int i = 0; i < 4; ++i) {
         if (!src[i]) continue;
         std::memcpy(c->stage_h + i * n, src[i], b);
-        CK(cudaMemcpyAsync(dst[i], c->stage_h + i * n, b, cudaMemcpyHostToDevice, c->stream));
+        if (!all) CK(cudaMemcpyAsync(dst[i], c->stage_h + i * n, b, cudaMemcpyHostToDevice, c->stream));
     }
+    if (all) CK(cudaMemcpyAsync(c->d.lmcc, c->stage_h, 4 * b, cudaMemcpyHostToDevice, c->stream));
     CK(cudaEventRecord(c->stage_ev, c->stream));
     return FB_OK;
 }
 
 int fb_get_markers(fb_ctx *c, double *lmcc, double *lmvel, double *lmacc, double *lmnor) {
     if (!c) return FB_ERR_STATE;
-    const size_t b = 2 * static_cast<size_t>(c->d.nlm) * sizeof(double);
+    const size_t n = 2 * static_cast<size_t>(c->d.nlm), b = n * sizeof(double);
     if (!b) return FB_OK;
     CK(cudaSetDevice(c->device));
     double *dst[4] = {lmcc, lmvel, lmacc, lmnor};
-    const double *src[4] = {c->d.lmcc, c->d.lmvel, c->d.lmacc, c->d.lmnor};
-    for (int i = 0; i < 4; ++i)
-        if (dst[i]) CK(cudaMemcpyAsync(dst[i], src[i], b, cudaMemcpyDeviceToHost, c->stream));
+    if (!c->stage_h) {
+        CK(cudaMallocHost(&c->stage_h, 4 * b));
+        CK(cudaEventCreateWithFlags(&c->stage_ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(c->stage_ev, c->stream));
+    }
+    // the contiguous device arrays in one copy through the pinned staging,
+    // once fb_set_markers' copies out of it are done (stream order)
+    CK(cudaMemcpyAsync(c->stage_h, c->d.lmcc, 4 * b, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < 4; ++i)
+        if (dst[i]) std::memcpy(dst[i], c->stage_h + i * n, b);
     return FB_OK;
 }
 
