@@ -664,7 +664,7 @@ struct WinShape {            // shared-memory layout of one tile of kWTk rows (i
         a_size = a1 > a2 ? a1 : a2;
         const int b1 = rows * ypitch, b2 = nzf * kWSeg * kWTj;
         b_size = b1 > b2 ? b1 : b2;
-        c_size = 3 * ncy + 3 * ncz;
+        c_size = 4 * ncy + 3 * ncz;   // y: a e g and the row normalisers; z: a e g
     }
 };
 
@@ -693,13 +693,13 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
     const int rows = sh.rows, cols = sh.cols;
     const int iy0 = j0 - 1 - Ky;          // y line index of tile column 0
     const int iz0 = k0 - 1 - Kz;          // z line index of tile row 0
-    double *cya = C, *cye = C + sh.ncy, *cyg = C + 2 * sh.ncy;
-    double *cza = C + 3 * sh.ncy, *cze = cza + sh.ncz, *czg = cza + 2 * sh.ncz;
+    double *cya = C, *cye = C + sh.ncy, *cyg = C + 2 * sh.ncy, *cys = C + 3 * sh.ncy;
+    double *cza = C + 4 * sh.ncy, *cze = cza + sh.ncz, *czg = cza + 2 * sh.ncz;
 
-    // 1. coefficients and the right-hand side tile scaled by the y row
-    //    normalisers; A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r)
-    // all of the tile's copies are issued at once (cp.async); each thread then
-    // scales the rhs values it copied by the y row normalisers
+    // 1. coefficients, the y row normalisers of the tile's columns (cys) and
+    //    the right-hand side tile; A[r * pitch + c] holds (j0 - Ky + c, k0 - Kz + r).
+    //    All of the tile's copies are issued at once (cp.async); the forward
+    //    y recurrences scale the right-hand side as they read it
     for (int c = threadIdx.x; c < sh.ncy; c += kWThreads) {
         const int i = iy0 + c;
         if (i >= 0 && i < ny) {
@@ -709,6 +709,9 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
         } else {
             cya[c] = cye[c] = cyg[c] = 0.0;
         }
+        const int jc = j0 - Ky + c;
+        if (c < cols && jc >= jlo && jc <= d.n2m) cp8(cys + c, by + jc);
+        else cys[c] = 0.0;
     }
     for (int c = threadIdx.x; c < sh.ncz; c += kWThreads) {
         const int i = iz0 + c;
@@ -724,13 +727,11 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
         constexpr int kCC = 3;   // column chunks of 32 (cols <= 96)
         int jc[kCC];
         bool okc[kCC];
-        double sc[kCC];
 #pragma unroll
         for (int cc = 0; cc < kCC; ++cc) {
             const int c = lane + 32 * cc;
             jc[cc] = j0 - Ky + c;
             okc[cc] = (c < cols) && (jc[cc] >= jlo && jc[cc] <= d.n2m);
-            sc[cc] = okc[cc] ? __ldg(by + jc[cc]) : 0.0;
         }
         for (int r = w; r < rows; r += kWarps) {
             const int k = k0 - Kz + r;
@@ -744,16 +745,6 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
             }
         }
         cp_wait();
-        for (int r = w; r < rows; r += kWarps) {
-            const int k = k0 - Kz + r;
-            const bool kok = (k >= klo && k <= d.n3m);
-#pragma unroll
-            for (int cc = 0; cc < kCC; ++cc) {
-                if (lane + 32 * cc >= cols || !(kok && okc[cc])) continue;
-                double *dst = A + r * sh.pitch + lane + 32 * cc;
-                *dst = *dst * sc[cc];
-            }
-        }
     }
     __syncthreads();
 
@@ -767,8 +758,8 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
         const double *arow = A + rr * sh.pitch + c0;
         const int lo = -(j0 - 1 + sg * kWSegY);  // line index 0 relative to the segment start
         double y[kWSegY];
-        seg_fwd<kWSegY, KM>([&](int u) { return cya[c0 + u]; }, [&](int u) { return arow[u]; }, Ky, lo,
-                           ny - (j0 - 1 + sg * kWSegY), y);
+        seg_fwd<kWSegY, KM>([&](int u) { return cya[c0 + u]; }, [&](int u) { return arow[u] * cys[c0 + u]; }, Ky,
+                           lo, ny - (j0 - 1 + sg * kWSegY), y);
         if (r < rows) {
 #pragma unroll
             for (int t = 0; t < kWSegY; ++t) B[r * sh.ypitch + sg * kWSegY + t] = y[t];
