@@ -783,19 +783,25 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
                            [&](int u) { return brow[u]; }, Ky, ny - (j0 - 1 + sg * kWSeg), x);
         if (r < rows) {
             const double bzk = (k >= 1 && k <= nz) ? __ldg(bz + k) : 0.0;
+            double *arow = A + r * kWXp + sg * kWSeg;
+            if (k != 1 && k != nz) {   // interior rows: no inflow/outflow term
 #pragma unroll
-            for (int t = 0; t < kWSeg; ++t) {
-                const int j = j0 + sg * kWSeg + t;
-                const int jj = min(max(j, 1), d.n2m);
-                double f = live ? x[t] * bzk : 0.0;
-                if (fld == 0) {
-                    if (k == 1) f = f + d.dqb2s[jj] * sd.ugkks;
-                    if (k == nz) f = f + d.dqb2n[jj] * sd.ugkkn;
-                } else {
-                    if (k == 1) f = d.dqb3s[jj];
-                    if (k == nz) f = d.dqb3n[jj];
+                for (int t = 0; t < kWSeg; ++t) arow[t] = live ? x[t] * bzk : 0.0;
+            } else {
+#pragma unroll
+                for (int t = 0; t < kWSeg; ++t) {
+                    const int j = j0 + sg * kWSeg + t;
+                    const int jj = min(max(j, 1), d.n2m);
+                    double f = live ? x[t] * bzk : 0.0;
+                    if (fld == 0) {
+                        if (k == 1) f = f + d.dqb2s[jj] * sd.ugkks;
+                        if (k == nz) f = f + d.dqb2n[jj] * sd.ugkkn;
+                    } else {
+                        if (k == 1) f = d.dqb3s[jj];
+                        if (k == nz) f = d.dqb3n[jj];
+                    }
+                    arow[t] = f;
                 }
-                A[r * kWXp + sg * kWSeg + t] = f;
             }
         }
     }
@@ -809,8 +815,11 @@ __device__ __forceinline__ void helsolve_win_body(const Dev &d, const SubDev &sd
     for (int sg = w; sg < sh.nzf; sg += kWarps) {
         const int c0 = Kz + sg * kWSeg;  // tile row and coefficient index of the segment start
         double y[kWSeg];
-        seg_fwd<kWSeg, KM>([&](int u) { return cza[c0 + u]; },
-                           [&](int u) { return acol[min(c0 + u, rows - 1) * kWXp]; }, Kz,
+        // rows past the tile's halo (c0 + u >= rows, last segment only) read
+        // whatever region A holds there, inside its allocation ((rows + 15) x
+        // kWXp < rows x pitch): they feed only positions past the halo, which
+        // the backward z phase never reads
+        seg_fwd<kWSeg, KM>([&](int u) { return cza[c0 + u]; }, [&](int u) { return acol[(c0 + u) * kWXp]; }, Kz,
                            -(k0 - 1 + sg * kWSeg), nz - (k0 - 1 + sg * kWSeg), y);
 #pragma unroll
         for (int t = 0; t < kWSeg; ++t) B[(sg * kWSeg + t) * kWTj + lane] = y[t];
