@@ -931,9 +931,13 @@ cudaError_t scan_configure() {
 #define AL(K)                                  \
     if ((e = allow_smem(K)) != cudaSuccess) return e;
     AL((k_ylines<9, 0>)) AL((k_ylines<17, 0>)) AL((k_ylines<33, 0>))
+    AL((k_helsolve_win<9, 32>)) AL((k_helsolve_win<9, 64>))
     AL((k_helsolve_win<12, 32>)) AL((k_helsolve_win<12, 64>))
+    AL((k_helsolve_win<16, 32>)) AL((k_helsolve_win<16, 64>))
     AL((k_helsolve_win<kWinMax, 32>)) AL((k_helsolve_win<kWinMax, 64>))
+    AL((kg_helsolve_win<9, 32>)) AL((kg_helsolve_win<9, 64>))
     AL((kg_helsolve_win<12, 32>)) AL((kg_helsolve_win<12, 64>))
+    AL((kg_helsolve_win<16, 32>)) AL((kg_helsolve_win<16, 64>))
     AL((kg_helsolve_win<kWinMax, 32>)) AL((kg_helsolve_win<kWinMax, 64>))
     if ((e = cudaFuncSetAttribute(k_ymodes, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(kg_ymodes, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024)) != cudaSuccess)
@@ -948,8 +952,15 @@ void win_launch(const Dev &d, const SubDev &s, cudaStream_t st) {
     const dim3 grid(ntj * ntk, 2);
     const WinShape<TK> sh(s.win_y, s.win_z);
     const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
-    if (s.win_y <= 12 && s.win_z <= 12)
+    // the warm-up of every segment runs KM predicated steps: the smallest
+    // instantiated KM that covers both windows
+    const int km = std::max(s.win_y, s.win_z);
+    if (km <= 9)
+        pdl(k_helsolve_win<9, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
+    else if (km <= 12)
         pdl(k_helsolve_win<12, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
+    else if (km <= 16)
+        pdl(k_helsolve_win<16, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
     else
         pdl(k_helsolve_win<kWinMax, TK>, dim3(grid), dim3(kWThreads), smem, st, d, s, ntj, s.win_y, s.win_z);
 }
@@ -991,8 +1002,13 @@ void gwin_launch(const Group &g, int n, cudaStream_t st) {
     const int ky = g.win_ky[n], kz = g.win_kz[n];
     const WinShape<TK> sh(ky, kz);   // sizes grow with the windows: fits every case
     const size_t smem = static_cast<size_t>(sh.a_size + sh.b_size + sh.c_size) * sizeof(double);
-    if (ky <= 12 && kz <= 12)
+    const int km = std::max(ky, kz);
+    if (km <= 9)
+        pdl(kg_helsolve_win<9, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
+    else if (km <= 12)
         pdl(kg_helsolve_win<12, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
+    else if (km <= 16)
+        pdl(kg_helsolve_win<16, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
     else
         pdl(kg_helsolve_win<kWinMax, TK>, grid, dim3(kWThreads), smem, st, g.cases, n, ntj);
 }
