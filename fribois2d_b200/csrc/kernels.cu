@@ -495,51 +495,28 @@ __global__ void k_lgrdist(Dev d) {
     lgrdist_body(d);
 }
 
-// MLSint.F90:4-104 (MLS_SD_ind): 3x3 support moved inside the field.
-// Returns false when a support node lacks its right neighbour on an axis.
-__device__ bool sd_ind(const Dev &d, int idir, int i0, int k0, double sdc[2][kSD], double sdd[2][kSD],
-                       int eul[2][kSD]) {
-    const double *y, *z;
-    int dimy, dimz;
-    if (idir == 1) {
-        y = d.rc; dimy = d.n2; z = d.zm; dimz = d.n3m;
-    } else if (idir == 2) {
-        y = d.rm; dimy = d.n2m; z = d.zz; dimz = d.n3;
-    } else {
-        y = d.rm; dimy = d.n2m; z = d.zm; dimz = d.n3m;
-    }
-    const int sj = (i0 == 1) ? 1 : (i0 == d.n2m ? -1 : 0);
-    const int sk = (k0 == 1) ? 1 : (k0 == d.n3m ? -1 : 0);
-    int m = 0;
-    for (int j = 1; j <= 3; ++j)
-        for (int k = 1; k <= 3; ++k) {
-            const int ej = i0 + (j + sj) - 2, ek = k0 + (k + sk) - 2;
-            if (ej < 1 || ej + 1 > dimy || ek < 1 || ek + 1 > dimz) return false;
-            sdc[0][m] = y[ej];
-            sdd[0][m] = y[ej + 1] - y[ej];
-            sdc[1][m] = z[ek];
-            sdd[1][m] = z[ek + 1] - z[ek];
-            eul[0][m] = ej;
-            eul[1][m] = ek;
-            ++m;
-        }
-    return true;
-}
-
 // utils_math.f90:637-725 (GEsolve), n = 3, scaled partial pivoting
-__device__ bool gesolve3(const double ai[3][3], const double bi[3], double x[3]) {
+__device__ __forceinline__ bool gesolve3(const double ai[3][3], const double bi[3], double x[3]) {
+    // every loop unrolled and the row exchange written per candidate row, so
+    // that the matrix stays in registers
     double a[3][3], b[3], s[3];
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         b[i] = bi[i];
+#pragma unroll
         for (int j = 0; j < 3; ++j) a[i][j] = ai[i][j];
     }
+#pragma unroll
     for (int k = 0; k < 2; ++k) {
+#pragma unroll
         for (int i = k; i < 3; ++i) {
             s[i] = 0.0;
+#pragma unroll
             for (int j = k; j < 3; ++j) s[i] = fmax(s[i], fabs(a[i][j]));
         }
         double pivot = fabs(a[k][k] / s[k]);
         int l = k;
+#pragma unroll
         for (int j = k + 1; j < 3; ++j) {
             double q = fabs(a[j][k] / s[j]);
             if (q > pivot) {
@@ -548,26 +525,33 @@ __device__ bool gesolve3(const double ai[3][3], const double bi[3], double x[3])
             }
         }
         if (pivot == 0.0) return false;
-        if (l != k) {
+#pragma unroll
+        for (int r = k + 1; r < 3; ++r) {
+            if (l != r) continue;
+#pragma unroll
             for (int j = k; j < 3; ++j) {
                 double t = a[k][j];
-                a[k][j] = a[l][j];
-                a[l][j] = t;
+                a[k][j] = a[r][j];
+                a[r][j] = t;
             }
             double t = b[k];
-            b[k] = b[l];
-            b[l] = t;
+            b[k] = b[r];
+            b[r] = t;
         }
+#pragma unroll
         for (int i = k + 1; i < 3; ++i) {
             double c = a[i][k] / a[k][k];
             a[i][k] = 0.0;
             b[i] = b[i] - c * b[k];
+#pragma unroll
             for (int j = k + 1; j < 3; ++j) a[i][j] = a[i][j] - c * a[k][j];
         }
     }
     x[2] = b[2] / a[2][2];
+#pragma unroll
     for (int i = 1; i >= 0; --i) {
         double c = 0.0;
+#pragma unroll
         for (int j = i + 1; j < 3; ++j) c = c + a[i][j] * x[j];
         x[i] = (b[i] - c) / a[i][i];
     }
@@ -614,68 +598,128 @@ __device__ void wkernel(int wfun, double difc, double sdds, double &wc, double &
     }
 }
 
+// Groups of kNodeLanes lanes work on one (marker, direction) each, support
+// node m on lane m < kSD; a sum over the support is formed in node order from
+// the group's shuffles (the sequential loop's sum).  Every lane of a warp
+// reaches every shuffle: a group that stops (outside the channel, an error)
+// carries on with its loads and stores switched off.
+constexpr int kNodeLanes = 16;
+
+// x summed over the group's first kSD lanes in lane order, on every lane
+__device__ __forceinline__ double group_sum_nodes(double x, int base) {
+    double s = 0.0;
+#pragma unroll
+    for (int mm = 0; mm < kSD; ++mm) s = s + __shfl_sync(0xffffffffu, x, base + mm);
+    return s;
+}
+
+// the group's lane index of the least v, the first of equal values (as a
+// sequential search with a strict comparison finds it); lanes past the
+// searched range hold +inf
+__device__ __forceinline__ int group_argmin(double v, int m) {
+    int i = m;
+#pragma unroll
+    for (int o = kNodeLanes / 2; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (ov < v || (ov == v && oi < i)) {
+            v = ov;
+            i = oi;
+        }
+    }
+    return i;
+}
+
+// true when no lane of the group (base .. base + kNodeLanes - 1) has flag set
+__device__ __forceinline__ bool group_none(bool flag, int base) {
+    return (__ballot_sync(0xffffffffu, flag) & (((1u << kNodeLanes) - 1u) << base)) == 0u;
+}
+
+// the support arrays of MLS_SD_ind (MLSint.F90:4-104) for direction idir
+__device__ __forceinline__ void sd_axes(const Dev &d, int idir, const double *&y, int &dimy, const double *&z,
+                                        int &dimz) {
+    if (idir == 1) {
+        y = d.rc; dimy = d.n2; z = d.zm; dimz = d.n3m;
+    } else if (idir == 2) {
+        y = d.rm; dimy = d.n2m; z = d.zz; dimz = d.n3;
+    } else {
+        y = d.rm; dimy = d.n2m; z = d.zm; dimz = d.n3m;
+    }
+}
+
 // Marker set-up at substep 1: MLS_SD_ind + MLS_SF + momentum coefficient cl
 // (forcing_MLS.F90:57-94, MLSint.F90:115-166, compute_AB :284-338), and the
-// spreading keys.  One thread per (marker, direction).
+// spreading keys.  One (marker, direction) per group of kNodeLanes lanes.
 __device__ __forceinline__ void mls_setup_body(const Dev &d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * d.nlm) return;
-    const int n = t >> 1, idir = (t & 1) + 1;
-    double *phi = d.phi + static_cast<size_t>(t) * kSD;
-    int *eu = d.eulins + static_cast<size_t>(t) * 2 * kSD;
-    for (int m = 0; m < kSD; ++m) phi[m] = 0.0;
-    d.cl[t] = 0.0;
-    if (*d.status) return;
+    if (!d.nlm) return;
+    const int T = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = T / kNodeLanes, m = T % kNodeLanes;
+    const int base = (threadIdx.x & 31) & ~(kNodeLanes - 1);
+    const bool have = t < 2 * d.nlm;
+    const int tt = have ? t : 0;
+    const int n = tt >> 1, idir = (tt & 1) + 1;
+    const bool node = m < kSD;
+    double *phi = d.phi + static_cast<size_t>(tt) * kSD;
+    int *eu = d.eulins + static_cast<size_t>(tt) * 2 * kSD;
+    if (have && node) phi[m] = 0.0;
+    if (have && m == 0) d.cl[tt] = 0.0;
+    const bool stopped = __shfl_sync(0xffffffffu, static_cast<int>(*d.status != 0), base) != 0;
     const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
-    if (!(d.zz[1] < pos[1] && pos[1] < d.zz[d.n3])) return;
+    const bool ok = have && !stopped && (d.zz[1] < pos[1] && pos[1] < d.zz[d.n3]);
     const int i0 = d.lmind[4 * n + 2 * (idir - 1)], k0 = d.lmind[4 * n + 2 * (idir - 1) + 1];
-    double sdc[2][kSD], sdd[2][kSD];
-    int eul[2][kSD];
-    if (i0 < 1 || k0 < 1 || !sd_ind(d, idir, i0, k0, sdc, sdd, eul)) {
-        raise_status(d, FB_ERR_MARKER_OUT);
-        return;
-    }
-    double w[kSD];
-    for (int i = 0; i < kSD; ++i) {
+    // MLS_SD_ind: node m = 3 (j - 1) + (k - 1) of the 3 x 3 support, moved
+    // inside the field
+    const double *y, *z;
+    int dimy, dimz;
+    sd_axes(d, idir, y, dimy, z, dimz);
+    const int sj = (i0 == 1) ? 1 : (i0 == d.n2m ? -1 : 0);
+    const int sk = (k0 == 1) ? 1 : (k0 == d.n3m ? -1 : 0);
+    const int mm = node ? m : 0;
+    const int ej = i0 + (mm / 3 + 1 + sj) - 2, ek = k0 + (mm % 3 + 1 + sk) - 2;
+    const bool bad = ok && node && (ej < 1 || ej + 1 > dimy || ek < 1 || ek + 1 > dimz);
+    const bool good = group_none(bad, base) && ok && i0 >= 1 && k0 >= 1;
+    if (ok && !good && m == 0) raise_status(d, FB_ERR_MARKER_OUT);
+    double sc0 = 0.0, sc1 = 0.0, sd0 = 0.0, sd1 = 0.0, w = 0.0;
+    if (good && node) {
+        sc0 = y[ej];
+        sd0 = y[ej + 1] - y[ej];
+        sc1 = z[ek];
+        sd1 = z[ek + 1] - z[ek];
         double wc0, wc1, dw;
-        wkernel(d.wfun, pos[0] - sdc[0][i], d.radiusSD * sdd[0][i], wc0, dw);
-        wkernel(d.wfun, pos[1] - sdc[1][i], d.radiusSD * sdd[1][i], wc1, dw);
-        w[i] = wc0 * wc1;
+        wkernel(d.wfun, pos[0] - sc0, d.radiusSD * sd0, wc0, dw);
+        wkernel(d.wfun, pos[1] - sc1, d.radiusSD * sd1, wc1, dw);
+        w = wc0 * wc1;
     }
-    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int i = 0; i < kSD; ++i) {
-        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) A[a][b] = A[a][b] + w[i] * (pk[a] * pk[b]);
-    }
+    const double pk[3] = {1.0, sc0, sc1};
+    double A[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)   // pk[a] pk[b] = pk[b] pk[a]: the same terms, the same sums
+            A[a][b] = (b < a) ? A[b][a] : group_sum_nodes(w * (pk[a] * pk[b]), base);
     const double gps[3] = {1.0, pos[0], pos[1]};
     double ptA[3];
     gesolve3(A, gps, ptA);
-    double ph[kSD], sumphi = 0.0;
-    for (int m = 0; m < kSD; ++m) {
-        const double B0 = 1.0 * w[m], B1 = sdc[0][m] * w[m], B2 = sdc[1][m] * w[m];
-        double acc = 0.0;
-        acc = acc + ptA[0] * B0;
-        acc = acc + ptA[1] * B1;
-        acc = acc + ptA[2] * B2;
-        ph[m] = acc;
+    const double B0 = 1.0 * w, B1 = sc0 * w, B2 = sc1 * w;
+    double ph = 0.0;
+    ph = ph + ptA[0] * B0;
+    ph = ph + ptA[1] * B1;
+    ph = ph + ptA[2] * B2;
+    const double sumphi = group_sum_nodes(ph, base);
+    if (good && m == 0 && !(fabs(1.0 - fabs(sumphi)) <= 1.0e-10)) raise_status(d, FB_ERR_MLS);
+    const double vol = sd0 * sd1;
+    const double dvel = group_sum_nodes(ph * vol, base);
+    const double lgr_h = group_sum_nodes(1.0 / 2.0 * ph * (sd0 + sd1), base);
+    if (!good) return;   // (after the group's last shuffle)
+    if (node) {
+        phi[m] = ph;
+        eu[m] = ej;
+        eu[kSD + m] = ek;
     }
-    for (int m = 0; m < kSD; ++m) sumphi = sumphi + ph[m];
-    if (!(fabs(1.0 - fabs(sumphi)) <= 1.0e-10)) raise_status(d, FB_ERR_MLS);
-    double dvel = 0.0, lgr_h = 0.0;
-    for (int m = 0; m < kSD; ++m) {
-        const double vol = sdd[0][m] * sdd[1][m];
-        dvel = dvel + ph[m] * vol;
-        lgr_h = lgr_h + 1.0 / 2.0 * ph[m] * (sdd[0][m] + sdd[1][m]);
-    }
-    d.cl[t] = d.lmA[n] * lgr_h / dvel;
-    for (int m = 0; m < kSD; ++m) {
-        phi[m] = ph[m];
-        eu[m] = eul[0][m];
-        eu[kSD + m] = eul[1][m];
-    }
-    // register the support box (start cell = node m = 0) for the spreading
-    const unsigned long long cell = static_cast<unsigned long long>(idir - 1) * d.NK * d.P + fidx(d, eul[0][0], eul[1][0]);
+    if (m != 0) return;
+    d.cl[tt] = d.lmA[n] * lgr_h / dvel;
+    // register the support box (start cell = node m = 0, this lane's) for the spreading
+    const unsigned long long cell = static_cast<unsigned long long>(idir - 1) * d.NK * d.P + fidx(d, ej, ek);
     const unsigned mask = (1u << d.hlog) - 1u;
     for (int lev = 0; lev < kBucketLevels; ++lev) {
         const unsigned long long key = cell * kBucketLevels + lev + 1;
@@ -692,7 +736,7 @@ __device__ __forceinline__ void mls_setup_body(const Dev &d) {
         const int slot = atomicAdd(d.hcnt + h, 1);
         if (slot < kBucket) {
             d.hval[static_cast<size_t>(h) * kBucket + slot] = n;
-            d.hslot[t] = static_cast<int>(h) + 1;
+            d.hslot[tt] = static_cast<int>(h) + 1;
             return;
         }
     }
@@ -1195,134 +1239,56 @@ __global__ void __launch_bounds__(1024) k_substep_mid(Dev d, int slot, double ga
 
 // ------------------------------------------------------------ loads
 
-// loads_transfer.F90:238-281 (probeind)
-__device__ bool probeind(const Dev &d, int idir, int mj, int mk, const double pp[2], int &ij, int &ik) {
-    const int off = 5;
-    const int js = mj - off, je = mj + off, ks = mk - off, ke = mk + off;
-    if (js < 1 || je > d.n2 || ks < 1 || ke > d.n3) return false;
-    const double *ya = (idir == 1) ? d.rc : d.rm;
-    const double *za = (idir == 2) ? d.zz : d.zm;
-    int b = js;
-    double bv = fabs(ya[js] - pp[0]);
-    for (int i = js + 1; i <= je; ++i) {
-        double v = fabs(ya[i] - pp[0]);
-        if (v < bv) bv = v, b = i;
-    }
-    ij = b;
-    b = ks;
-    bv = fabs(za[ks] - pp[1]);
-    for (int i = ks + 1; i <= ke; ++i) {
-        double v = fabs(za[i] - pp[1]);
-        if (v < bv) bv = v, b = i;
-    }
-    ik = b;
-    return true;
-}
+// loads_transfer_c (loads_transfer.F90:143-185), per-marker part: the probe
+// interpolation of v, w or p with first and second derivatives; the v and w
+// groups also form checkbcs (ckbcs.F90:29-60) with the substep-1 weights.
+// One (marker, quantity) per group of kLoadLanes lanes, support node m on
+// lane m < kSD: the nodes' weights, moment terms and field reads are
+// independent, and every sum over the nodes is formed in node order from the
+// group's shuffles, so each result is that of the sequential loops.  Every
+// lane of a warp reaches every shuffle: a group that stops (outside the
+// channel, an error) carries on with its loads and stores switched off.
+constexpr int kLoadLanes = kNodeLanes;
+constexpr int kLoadMk = 2;   // markers per block: the three groups of a marker in one block
+constexpr int kLoadThreads = 3 * kLoadMk * kLoadLanes;
 
-// MLSint.F90:173-258 (MLS_SF_d) with compute_AB_d :342-402
-__device__ bool mls_sf_d(const Dev &d, const double pos[2], const double sdc[2][kSD],
-                         const double sdd[2][kSD], double phid[3][kSD]) {
-    double w[kSD][3];
-    for (int i = 0; i < kSD; ++i) {
-        double wc[2], dw[2];
-        for (int k = 0; k < 2; ++k) wkernel(d.wfun, pos[k] - sdc[k][i], d.radiusSD * sdd[k][i], wc[k], dw[k]);
-        w[i][0] = wc[0] * wc[1];
-        w[i][1] = wc[1] * dw[0];
-        w[i][2] = wc[0] * dw[1];
-    }
-    double A[3][3][3];
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-            for (int l = 0; l < 3; ++l) A[a][b][l] = 0.0;
-    for (int i = 0; i < kSD; ++i) {
-        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) {
-                const double pp = pk[a] * pk[b];
-                for (int l = 0; l < 3; ++l) A[a][b][l] = A[a][b][l] + w[i][l] * pp;
-            }
-    }
-    double Aa[3][3];
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) Aa[a][b] = A[a][b][0];
-    double gam[3][3];
-    const double gps[3] = {1.0, pos[0], pos[1]};
-    double g0[3];
-    gesolve3(Aa, gps, g0);
-    for (int l = 1; l <= 2; ++l) {
-        double C[3], gx[3];
-        for (int a = 0; a < 3; ++a) {
-            double acc = 0.0;
-            for (int b = 0; b < 3; ++b) acc = acc + A[a][b][l] * g0[b];
-            const double gpl = (a == l) ? 1.0 : 0.0;
-            C[a] = gpl - acc;
-        }
-        gesolve3(Aa, C, gx);
-        for (int a = 0; a < 3; ++a) gam[a][l] = gx[a];
-    }
-    for (int a = 0; a < 3; ++a) gam[a][0] = g0[a];
-    double sumphi = 0.0;
-    for (int i = 0; i < kSD; ++i) {
-        const double pk[3] = {1.0, sdc[0][i], sdc[1][i]};
-        double p0 = 0.0, p1 = 0.0, p2 = 0.0;
-        for (int a = 0; a < 3; ++a) {
-            const double B0 = pk[a] * w[i][0], B1 = pk[a] * w[i][1], B2 = pk[a] * w[i][2];
-            p0 = p0 + gam[a][0] * B0;
-            p1 = p1 + gam[a][1] * B0 + gam[a][0] * B1;
-            p2 = p2 + gam[a][2] * B0 + gam[a][0] * B2;
-        }
-        phid[0][i] = p0;
-        phid[1][i] = p1;
-        phid[2][i] = p2;
-        sumphi = sumphi + p0;
-    }
-    return fabs(1.0 - fabs(sumphi)) <= 1.0e-10;
-}
-
-// getpbup (loads_transfer.F90:285-357) for one quantity
-__device__ void getpbup_one(const Dev &d, const double *f, const int eul[2][kSD], const double ph[3][kSD],
-                            double out[7]) {
-    for (int i = 0; i < 7; ++i) out[i] = 0.0;
-    for (int n = 0; n < kSD; ++n) {
-        const int cyk = eul[0][n], czk = eul[1][n];
-        const double f0 = Fv(f, cyk, czk);
-        const double uk1 = (f0 - Fv(f, cyk - 1, czk)) * d.dx2 / d.g2rc[cyk];
-        const double uk2 = (f0 - Fv(f, cyk, czk - 1)) * d.dx3 / d.g3rc[czk];
-        for (int i = 0; i < 3; ++i) out[i] = out[i] + ph[i][n] * f0;
-        out[3] = out[3] + ph[1][n] * uk1;
-        out[4] = out[4] + ph[1][n] * uk2;
-        out[5] = out[5] + ph[2][n] * uk1;
-        out[6] = out[6] + ph[2][n] * uk2;
-    }
-}
-
-// loads_transfer_c (loads_transfer.F90:143-185), per-marker part: the
-// probe interpolation of v, w or p with first and second derivatives (one
-// thread per marker and quantity); the v and w threads also form checkbcs
-// (ckbcs.F90:29-60) with the substep-1 weights.
 __device__ __forceinline__ void loads_probe_body(const Dev &d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * d.nlm) return;
-    const int n = t / 3, idir = t % 3 + 1;
+    constexpr unsigned kAll = 0xffffffffu;
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    const int T = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = T / kLoadLanes, m = T % kLoadLanes;
+    const int base = (threadIdx.x & 31) & ~(kLoadLanes - 1);
+    const bool have = t < 3 * d.nlm;
+    const int tt = have ? t : 0;
+    const int n = tt / 3, idir = tt % 3 + 1;
+    const bool node = m < kSD;
     double *pb = d.probe + static_cast<size_t>(n) * 24;
     const double pos[2] = {d.lmcc[2 * n], d.lmcc[2 * n + 1]};
     const bool inside = (d.zz[1] < pos[1] && pos[1] < d.zz[d.n3]);
-    if (idir == 1) {
-        pb[23] = inside ? 0.0 : -1.0;
-        d.bcerrv[n] = 0.0;
+    if (have && m == 0) {
+        if (idir == 1) {
+            pb[23] = inside ? 0.0 : -1.0;
+            d.bcerrv[n] = 0.0;
+        }
+        if (idir == 2) d.bcerrw[n] = 0.0;
     }
-    if (idir == 2) d.bcerrw[n] = 0.0;
-    if (*d.status || !inside) return;
-    if (idir <= 2) {
-        const int tt = 2 * n + idir - 1;
-        const double *phi = d.phi + static_cast<size_t>(tt) * kSD;
-        const int *eu = d.eulins + static_cast<size_t>(tt) * 2 * kSD;
+    const bool stopped = __shfl_sync(kAll, static_cast<int>(*d.status != 0), base) != 0;
+    const bool ok = have && !stopped && inside;
+
+    // checkbcs: the velocity at the marker from the substep-1 weights
+    double prod = 0.0;
+    if (ok && idir <= 2 && node) {
+        const int t2 = 2 * n + idir - 1;
+        const int *eu = d.eulins + static_cast<size_t>(t2) * 2 * kSD;
         const double *q = (idir == 1) ? d.q2 : d.q3;
-        double u = 0.0;
-        for (int m = 0; m < kSD; ++m) u = u + phi[m] * q[fidx(d, eu[m], eu[kSD + m])];
+        prod = d.phi[static_cast<size_t>(t2) * kSD + m] * q[fidx(d, eu[m], eu[kSD + m])];
+    }
+    const double u = group_sum_nodes(prod, base);
+    if (ok && idir <= 2 && m == 0) {
         if (idir == 1) d.bcerrv[n] = d.lmvel[2 * n] - u;
         else d.bcerrw[n] = d.lmvel[2 * n + 1] - u;
     }
+
     const double hpr = d.ddmin * d.kprobe;
     const double probe[2] = {pos[0] + d.lmnor[2 * n] * hpr, pos[1] + d.lmnor[2 * n + 1] * hpr};
     int mj, mk;
@@ -1333,28 +1299,151 @@ __device__ __forceinline__ void loads_probe_body(const Dev &d) {
         mj = d.lmind[4 * n + 2 * (idir - 1)];
         mk = d.lmind[4 * n + 2 * (idir - 1) + 1];
     }
-    int ij, ik;
-    double sdc[2][kSD], sdd[2][kSD], ph[3][kSD], res[7];
-    int eul[2][kSD];
-    if (!probeind(d, idir, mj, mk, probe, ij, ik) || !sd_ind(d, idir, ij, ik, sdc, sdd, eul) || eul[0][0] < 2) {
-        raise_status(d, FB_ERR_MARKER_OUT);
-        return;
+
+    // probeind (loads_transfer.F90:238-281): the nearest y and z lines to the
+    // probe within 5 lines of the marker's own; lane i holds lines js + i, ks + i
+    constexpr int off = 5;
+    const int js = mj - off, ks = mk - off;
+    const bool inrange = ok && js >= 1 && mj + off <= d.n2 && ks >= 1 && mk + off <= d.n3;
+    const double *ya = (idir == 1) ? d.rc : d.rm;
+    const double *za = (idir == 2) ? d.zz : d.zm;
+    double vy = inf, vz = inf;
+    if (inrange && m <= 2 * off) {
+        vy = fabs(ya[js + m] - probe[0]);
+        vz = fabs(za[ks + m] - probe[1]);
     }
-    if (!mls_sf_d(d, probe, sdc, sdd, ph)) raise_status(d, FB_ERR_MLS);
-    const double *f = (idir == 1) ? d.q2 : (idir == 2 ? d.q3 : d.pr);
-    getpbup_one(d, f, eul, ph, res);
-    for (int i = 0; i < 7; ++i) pb[7 * (idir - 1) + i] = res[i];
+    // a NaN distance never wins the strict comparison; one at the first line
+    // keeps the first line
+    const bool y0nan = isnan(__shfl_sync(kAll, vy, base)), z0nan = isnan(__shfl_sync(kAll, vz, base));
+    const int iy = group_argmin(isnan(vy) ? inf : vy, m);
+    const int iz = group_argmin(isnan(vz) ? inf : vz, m);
+    const int ij = js + (y0nan ? 0 : iy), ik = ks + (z0nan ? 0 : iz);
+
+    // MLS_SD_ind (MLSint.F90:4-104): node m = 3 (j - 1) + (k - 1) of the 3 x 3
+    // support, moved inside the field
+    const double *y, *z;
+    int dimy, dimz;
+    sd_axes(d, idir, y, dimy, z, dimz);
+    const int sj = (ij == 1) ? 1 : (ij == d.n2m ? -1 : 0);
+    const int sk = (ik == 1) ? 1 : (ik == d.n3m ? -1 : 0);
+    const int mm = node ? m : 0;
+    const int ej = ij + (mm / 3 + 1 + sj) - 2, ek = ik + (mm % 3 + 1 + sk) - 2;
+    const bool bad = inrange && node && (ej < 1 || ej + 1 > dimy || ek < 1 || ek + 1 > dimz);
+    const bool supported = group_none(bad, base) && inrange;
+    const int ej0 = __shfl_sync(kAll, ej, base);
+    const bool good = supported && ej0 >= 2;
+    if (ok && !good && m == 0) raise_status(d, FB_ERR_MARKER_OUT);
+    const bool act = good && node;
+
+    // the field values that getpbup reads, requested before the MLS algebra
+    // so that their latency overlaps it
+    double f0 = 0.0, fym = 0.0, fzm = 0.0, g2r = 1.0, g3r = 1.0;
+    if (act) {
+        const double *f = (idir == 1) ? d.q2 : (idir == 2 ? d.q3 : d.pr);
+        f0 = Fv(f, ej, ek);
+        fym = Fv(f, ej - 1, ek);
+        fzm = Fv(f, ej, ek - 1);
+        g2r = d.g2rc[ej];
+        g3r = d.g3rc[ek];
+    }
+
+    // MLS_SF_d (MLSint.F90:173-258) with compute_AB_d (:342-402)
+    double sc0 = 0.0, sc1 = 0.0, w0 = 0.0, w1 = 0.0, w2 = 0.0;
+    if (act) {
+        sc0 = y[ej];
+        sc1 = z[ek];
+        const double sd0 = y[ej + 1] - y[ej], sd1 = z[ek + 1] - z[ek];
+        double wc[2], dw[2];
+        wkernel(d.wfun, probe[0] - sc0, d.radiusSD * sd0, wc[0], dw[0]);
+        wkernel(d.wfun, probe[1] - sc1, d.radiusSD * sd1, wc[1], dw[1]);
+        w0 = wc[0] * wc[1];
+        w1 = wc[1] * dw[0];
+        w2 = wc[0] * dw[1];
+    }
+    const double pk[3] = {1.0, sc0, sc1};
+    double A[3][3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            if (b < a) {   // pk[a] pk[b] = pk[b] pk[a]: the same terms, the same sums
+#pragma unroll
+                for (int l = 0; l < 3; ++l) A[a][b][l] = A[b][a][l];
+                continue;
+            }
+            const double pp = pk[a] * pk[b];
+            A[a][b][0] = group_sum_nodes(w0 * pp, base);
+            A[a][b][1] = group_sum_nodes(w1 * pp, base);
+            A[a][b][2] = group_sum_nodes(w2 * pp, base);
+        }
+    double Aa[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) Aa[a][b] = A[a][b][0];
+    double gam[3][3];
+    const double gps[3] = {1.0, probe[0], probe[1]};
+    double g0[3];
+    gesolve3(Aa, gps, g0);
+#pragma unroll
+    for (int l = 1; l <= 2; ++l) {
+        double C[3], gx[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double acc = 0.0;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc = acc + A[a][b][l] * g0[b];
+            const double gpl = (a == l) ? 1.0 : 0.0;
+            C[a] = gpl - acc;
+        }
+        gesolve3(Aa, C, gx);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gam[a][l] = gx[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) gam[a][0] = g0[a];
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double B0 = pk[a] * w0, B1 = pk[a] * w1, B2 = pk[a] * w2;
+        p0 = p0 + gam[a][0] * B0;
+        p1 = p1 + gam[a][1] * B0 + gam[a][0] * B1;
+        p2 = p2 + gam[a][2] * B0 + gam[a][0] * B2;
+    }
+    const double sumphi = group_sum_nodes(p0, base);
+    if (good && m == 0 && !(fabs(1.0 - fabs(sumphi)) <= 1.0e-10)) raise_status(d, FB_ERR_MLS);
+
+    // getpbup (loads_transfer.F90:285-357) for this quantity
+    double o[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (act) {
+        const double uk1 = (f0 - fym) * d.dx2 / g2r;
+        const double uk2 = (f0 - fzm) * d.dx3 / g3r;
+        o[0] = p0 * f0;
+        o[1] = p1 * f0;
+        o[2] = p2 * f0;
+        o[3] = p1 * uk1;
+        o[4] = p1 * uk2;
+        o[5] = p2 * uk1;
+        o[6] = p2 * uk2;
+    }
+    double res = 0.0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const double s = group_sum_nodes(o[i], base);
+        if (m == i) res = s;
+    }
+    if (good && m < 7) pb[7 * (idir - 1) + m] = res;
 }
 
-// the probes of kLoadMk markers per block (their three threads in one block),
-// then each probed marker's own tangent (loads_transfer.F90:177-185) from its
-// first two probes
-constexpr int kLoadMk = 32;
+// the probes of kLoadMk markers per block, then each probed marker's own
+// tangent (loads_transfer.F90:177-185) from its first two probes
 __device__ __forceinline__ void loads_probe_tan_body(const Dev &d) {
+    if (!d.nlm) return;
     loads_probe_body(d);
     __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * d.nlm || t % 3 != 0 || *d.status) return;
+    const int T = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = T / kLoadLanes;
+    if (t >= 3 * d.nlm || t % 3 != 0 || T % kLoadLanes != 0 || *d.status) return;
     const int n = t / 3;
     double *pb = d.probe + static_cast<size_t>(n) * 24;
     if (pb[23] < 0.0) return;
@@ -1372,7 +1461,7 @@ __device__ __forceinline__ void loads_probe_tan_body(const Dev &d) {
     }
 }
 
-__global__ void __launch_bounds__(3 * kLoadMk) k_loads_probe(Dev d) {
+__global__ void __launch_bounds__(kLoadThreads, 5) k_loads_probe(Dev d) {
     FB_GRID_WAIT();
     loads_probe_tan_body(d);
 }
@@ -1814,7 +1903,7 @@ __global__ void __launch_bounds__(1024) kg_substep_mid(const GroupCase *__restri
     substep_mid_body(d, slot, s.ga, s.ro);
 }
 
-__global__ void __launch_bounds__(3 * kLoadMk) kg_loads_probe(const GroupCase *__restrict__ g) {
+__global__ void __launch_bounds__(kLoadThreads, 5) kg_loads_probe(const GroupCase *__restrict__ g) {
     __shared__ Dev d;
     if (!stage_case(g, &d)) return;
     loads_probe_tan_body(d);
@@ -1870,7 +1959,7 @@ void launch_lgrdist(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_lgrdist, dim3((d.nlm + 127) / 128), dim3(128), 0, s, d);
 }
 void launch_mls_setup(const Dev &d, cudaStream_t s) {
-    if (d.nlm) pdl(k_mls_setup, dim3((2 * d.nlm + 63) / 64), dim3(64), 0, s, d);
+    if (d.nlm) pdl(k_mls_setup, dim3((2 * d.nlm * kNodeLanes + 255) / 256), dim3(256), 0, s, d);
 }
 void launch_mls_interp(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_mls_interp, dim3((2 * d.nlm * kInterpLanes + 255) / 256), dim3(256), 0, s, d);
@@ -1906,7 +1995,7 @@ void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream
 }
 void launch_loads(const Dev &d, cudaStream_t s) {
     if (!d.nlm) return;
-    pdl(k_loads_probe, dim3((d.nlm + kLoadMk - 1) / kLoadMk), dim3(3 * kLoadMk), 0, s, d);
+    pdl(k_loads_probe, dim3((d.nlm + kLoadMk - 1) / kLoadMk), dim3(kLoadThreads), 0, s, d);
     pdl(k_loads_finish, dim3((d.nlm + kLoadFin - 1) / kLoadFin), dim3(kLoadFin), 0, s, d);
 }
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
@@ -1952,7 +2041,7 @@ void glaunch_marker_setup(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
     if (!d.nlm) return;
     pdl(kg_lgrdist, zgrid(dim3((d.nlm + 127) / 128), g), dim3(128), 0, s, g.cases);
-    pdl(kg_mls_setup, zgrid(dim3((2 * d.nlm + 63) / 64), g), dim3(64), 0, s, g.cases);
+    pdl(kg_mls_setup, zgrid(dim3((2 * d.nlm * kNodeLanes + 255) / 256), g), dim3(256), 0, s, g.cases);
     pdl(kg_spread_chains, zgrid(dim3((2 * d.nlm * kSD + 127) / 128), g), dim3(128), 0, s, g.cases);
 }
 void glaunch_forcing(const Group &g, cudaStream_t s) {
@@ -1979,7 +2068,7 @@ void glaunch_substep_mid(const Group &g, int n_next, int slot, cudaStream_t s) {
 void glaunch_loads(const Group &g, cudaStream_t s) {
     const Dev &d = g.rep;
     if (!d.nlm) return;
-    pdl(kg_loads_probe, zgrid(dim3((d.nlm + kLoadMk - 1) / kLoadMk), g), dim3(3 * kLoadMk), 0, s, g.cases);
+    pdl(kg_loads_probe, zgrid(dim3((d.nlm + kLoadMk - 1) / kLoadMk), g), dim3(kLoadThreads), 0, s, g.cases);
     pdl(kg_loads_finish, zgrid(dim3((d.nlm + kLoadFin - 1) / kLoadFin), g), dim3(kLoadFin), 0, s, g.cases);
 }
 void glaunch_rigid(const Group &g, cudaStream_t s, int mode) {
