@@ -878,10 +878,10 @@ int phcalc_i8(fb_ctx *c) {
     const Dev &d = c->d;
     cudaStream_t st = c->stream;
     fb::launch_i8_split(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, st);
-    fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
+    fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st, true);   // i8f, i8b: cut once at set-up
     fb::launch_scan_poisson(d, st);
     fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
-    fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st);
+    fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st, true);
     c->own_launches += 5;   // two digit cuts, two products, the mode solves
     return FB_OK;
 }
@@ -959,7 +959,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         break;
     case FB_TK_I8X8_GEMM:
         if (!c->i8_ready) return FB_ERR_STATE;
-        fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st);
+        fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st, true);
         break;
     default: return FB_ERR_STATE;
     }

@@ -903,23 +903,52 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // The set-up above touches no global memory: under programmatic dependent
+    // launch it overlaps the previous kernel's tail.  Every thread but the
+    // producer waits for that kernel here; the producer first issues the copies
+    // of a B operand that was in place before it (the eigenvector planes), so
+    // that they are in flight while the previous kernel drains.
+    const bool producer = (warp == 0 && lane == 0);
+    if (!kGlobalMaps && !producer) FB_GRID_WAIT();
+    // the epilogue's scales: this row's, and columns n0 + lane, n0 + 32 + lane
+    const int quarter = warp & 3;
+    const int row = m0 + quarter * 32 + lane;
+    double rs = 0.0, cs0 = 0.0, cs1 = 0.0;
+    auto load_scales = [&]() {
+        if (row < o.M) rs = o.rowscale[row];
+        if (n0 + lane < o.N) cs0 = o.colscale[n0 + lane];
+        if (BN > 32 && lane + 32 < BN && n0 + 32 + lane < o.N) cs1 = o.colscale[n0 + 32 + lane];
+    };
+    if (!producer) load_scales();
 
     bool ok = true;
-    if (warp == 0 && lane == 0) {
+    if (producer) {
         // ---- TMA producer
         if (kGlobalMaps) acquire_maps(ma, ma, mb, mb);
-        int ip = 0, nb = 0, ps = 0;   // A slice pairs issued, B stages issued, pair slot
+        int pre = 0;   // B stages issued before the wait (both buffers start empty)
+        if (!kGlobalMaps && o.b_const) {
+            for (; pre < 2 && pre < nk; ++pre) {
+                mbar_expect_tx(bfull0 + 8 * pre, Cfg::kBStage);
+                for (int j = 0; j < kS; ++j)
+                    tma_load_3d(sB + pre * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * pre, pre * kI8BK, n0, j);
+            }
+        }
+        if (!kGlobalMaps) FB_GRID_WAIT();
+        load_scales();
+        int ip = 0, nb = pre, ps = 0;   // A slice pairs issued, B stages issued, pair slot
         uint32_t aph = 0;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int sb = kb & 1;
-            if (!mbar_wait(bempty0 + 8 * sb, (static_cast<uint32_t>(kb >> 1) & 1u) ^ 1u)) {
-                ok = false;
-                break;
+            if (kb >= pre) {
+                if (!mbar_wait(bempty0 + 8 * sb, (static_cast<uint32_t>(kb >> 1) & 1u) ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(bfull0 + 8 * sb, Cfg::kBStage);
+                for (int j = 0; j < kS; ++j)
+                    tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
+                nb = kb + 1;
             }
-            mbar_expect_tx(bfull0 + 8 * sb, Cfg::kBStage);
-            for (int j = 0; j < kS; ++j)
-                tma_load_3d(sB + sb * Cfg::kBStage + j * Cfg::kBSlice, mb, bfull0 + 8 * sb, kb * kI8BK, n0, j);
-            nb = kb + 1;
 #pragma unroll
             for (int i = 0; i < kS; i += 2) {   // slices i, i + 1 on one barrier
                 if (!mbar_wait(aempty0 + 8 * ps, aph ^ 1u)) {
@@ -1001,10 +1030,7 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
     if (!mbar_wait_idle(done, 0)) ok = false;
     __syncwarp();
     tc_fence_after();
-    const int quarter = warp & 3;
-    const int row = m0 + quarter * 32 + lane;
     const bool rok = ok && row < o.M;
-    const double rs = rok ? o.rowscale[row] : 0.0;
 #pragma unroll 1
     for (int c = warp >> 2; c < BN / 8; c += kI8Threads / 128) {
         uint32_t v[kS][8];
@@ -1024,12 +1050,11 @@ __device__ __forceinline__ void i8x8_body(const CUtensorMap *ma, const CUtensorM
 #pragma unroll
             for (int q = 0; q < 8; ++q) acc[q] = acc[q] + i32_as_f64(v[t][q]) * wgt;
         }
-        if (rok) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int col = n0 + c * 8 + q;
-                if (col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * o.colscale[col];
-            }
+        for (int q = 0; q < 8; ++q) {
+            const int cc = c * 8 + q, col = n0 + cc;   // cc is the same on every lane
+            const double cs = __shfl_sync(0xffffffffu, cc < 32 ? cs0 : cs1, cc & 31);
+            if (rok && col < o.N) o.out[static_cast<size_t>(col) * o.ldo + row] = acc[q] * rs * cs;
         }
     }
     if (!ok) atomicCAS(status, 0, FB_ERR_TIMEOUT);
@@ -1045,8 +1070,7 @@ template <int BN>
 __global__ void __launch_bounds__(kI8Threads, 1)
     k_i8x8_gemm(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb, I8Out o, int K,
                 int *status) {
-    FB_GRID_WAIT();
-    i8x8_body<BN, false>(&ma, &mb, o, K, status);
+    i8x8_body<BN, false>(&ma, &mb, o, K, status);   // waits for the previous kernel after its set-up
 }
 
 // grouped: blockIdx.z selects the product
@@ -1267,8 +1291,9 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
 }
 
 // the tile width is the B operand's box height (i8_plan)
-void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st) {
-    I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows};
+void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st,
+                 bool b_const) {
+    I8Out o{out, ldo, a.scale, b.scale, a.rows, b.rows, b_const ? 1 : 0};
     const dim3 grid((a.rows + 127) / 128, (b.rows + b.box - 1) / b.box);
     if (b.box == 48) pdl(k_i8x8_gemm<48>, grid, dim3(kI8Threads), I8Cfg<48>::kSmem, st, a.map, b.map, o, a.K, status);
     else if (b.box == 32) pdl(k_i8x8_gemm<32>, grid, dim3(kI8Threads), I8Cfg<32>::kSmem, st, a.map, b.map, o, a.K, status);

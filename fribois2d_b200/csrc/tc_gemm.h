@@ -79,6 +79,7 @@ struct I8Out {
     long ldo;
     const double *rowscale, *colscale;
     int M, N;
+    int b_const = 0;   // B's digit planes and scales were written before the previous kernel ran
 };
 // grouped launches (blockIdx.z = case): per-case split sources and products
 struct I8SplitTask {
@@ -103,7 +104,11 @@ int i8_plan(I8Plan &p, int rows, int K, int box_rows);
 // digits of the column-major source A(r, k) = src[k * lds + r], r < R, k < K
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
 // out[c * ldo + r] = sum_k A(r, k) B(c, k)
-void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st);
+// b_const: b's planes and scales were written before the previous kernel in
+// the stream started (the constant eigenvector operand), so its first copies
+// may be issued before waiting for that kernel
+void launch_i8x8(const I8Plan &a, const I8Plan &b, double *out, long ldo, int *status, cudaStream_t st,
+                 bool b_const = false);
 // the same over n cases of one shape (rep: geometry of the split)
 void launch_i8_split_group(const I8SplitTask *tasks, const I8Plan &rep, int R, int K, int n, cudaStream_t st);
 void launch_i8x8_group(const I8Task *tasks, int M, int N, int n, int bn, cudaStream_t st);
