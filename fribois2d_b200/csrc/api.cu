@@ -54,6 +54,7 @@ struct fb_ctx {
     cublasLtMatmulAlgo_t lt_algo[2] = {};
     bool lt_on[2] = {false, false};
     Dev d{};
+    fb::NlMaps nlmaps{};                      // TMA descriptors of q2, q3, pr for the k_nl_rhs tiles
     SubDev sub[3]{};
     double usdtal[3] = {0, 0, 0};
     std::vector<void *> allocs;
@@ -513,6 +514,7 @@ int create_impl(const char *dir, int device, fb_ctx *c) {
     for (double **f : fields)
         if ((st = dnew(c, f, nf))) return st;
     if ((st = dnew(c, &d.hmn, static_cast<size_t>(d.n3m) * d.ldh))) return st;
+    if ((st = fb::encode_nl_maps(&c->nlmaps, d))) return st;
     {   // inqpr (initial_sol.F90:268-296): q2 = 0, q3 = velin = 1, pr = 0
         std::vector<double> one(nf, 0.0);
         for (int k = 0; k <= g.n3; ++k)
@@ -901,7 +903,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     switch (stage) {
     case FB_ST_CFL: fb::launch_cfl(d, st); break;
     case FB_ST_BOUCDQ: fb::launch_boucdq(d, ga, ro, st); break;
-    case FB_ST_NL_RHS: fb::launch_nl_rhs(d, al, ga, ro, st); break;
+    case FB_ST_NL_RHS: fb::launch_nl_rhs(d, al, ga, ro, st, false, &c->nlmaps); break;
     case FB_ST_LGRDIST: fb::launch_lgrdist(d, st); break;
     case FB_ST_FORCING:
         if (!d.nlm) break;
@@ -1021,7 +1023,7 @@ int enqueue_fluid(fb_ctx *c, int ns) {
         coefs(c, ns, n, al, ga, ro);
         if (!pend && (r = stage_impl(c, FB_ST_BOUCDQ, ns, n))) return r;
         if (pend) {
-            fb::launch_nl_rhs(d, al, ga, ro, c->stream, true);
+            fb::launch_nl_rhs(d, al, ga, ro, c->stream, true, &c->nlmaps);
             c->own_launches += 1;
         } else if ((r = stage_impl(c, FB_ST_NL_RHS, ns, n))) {
             return r;

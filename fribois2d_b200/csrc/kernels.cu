@@ -10,9 +10,12 @@
 #include <cmath>
 #include <cstdint>
 
+#include <cudaTypedefs.h>
+
 #include "device.cuh"
 #include "kernels.h"
 #include "pdl.h"
+#include "tma.cuh"
 #include "../../include/fribois2d.h"
 
 namespace fb {
@@ -194,13 +197,34 @@ struct NlTile {
 };
 constexpr size_t kNlSmem = 2 * sizeof(NlTile);
 
+// The TMA-staged tile: one box per field of kNlTH rows (k0 - 1 .. k0 + 32) by
+// kNlTW columns.  A box must start on a 16-byte boundary, so it starts one
+// column left of the halo: column c holds j = j0 - 2 + c, and the stencil
+// reads columns 1 .. 34.  Each field array starts on a 128-byte boundary.
+constexpr int kNlTW = kNlJ + 4, kNlTH = kNlK + 2;
+struct alignas(128) NlTileT {
+    alignas(128) double q2[kNlTH][kNlTW];
+    alignas(128) double q3[kNlTH][kNlTW];
+    alignas(128) double pr[kNlTH][kNlTW];
+    double udx3m[kNlK], ap3sk[kNlK], ac3sk[kNlK], am3sk[kNlK];
+    double udx3c[kNlK], ap3ck[kNlK], ac3ck[kNlK], am3ck[kNlK];
+    double udx2c[kNlJ], am2j[kNlJ], ac2j[kNlJ], ap2j[kNlJ];
+    double udx2m[kNlJ], am3j[kNlJ], ac3j[kNlJ], ap3j[kNlJ];
+};
+constexpr uint32_t kNlBoxBytes = kNlTH * kNlTW * 8;
+static_assert(kNlBoxBytes % 16 == 0 && (kNlTW * 8) % 16 == 0, "TMA box rows in 16-byte units");
+// two tiles, their two mbarriers, and the slack to align the tiles to 128 bytes
+constexpr size_t kNlSmemT = 2 * sizeof(NlTileT) + 128 + 128;
+
 // ru2v, ru3v: ru2/ru3 at the cell, read before any cell of the thread is
 // stored (0 when ro = 0)
-__device__ __forceinline__ void nl_cell(const Dev &d, const NlTile &t, int j0, int k0, int jc, int kc, double al,
+// kC0: the tile column of j = j0 (1 for the cp.async tile, 2 for the TMA tile)
+template <int kC0, class Tile>
+__device__ __forceinline__ void nl_cell(const Dev &d, const Tile &t, int j0, int k0, int jc, int kc, double al,
                                         double ga, double ro, double ru2v, double ru3v) {
-#define S2(j, k) t.q2[(k) - k0 + 1][(j) - j0 + 1]
-#define S3(j, k) t.q3[(k) - k0 + 1][(j) - j0 + 1]
-#define SP(j, k) t.pr[(k) - k0 + 1][(j) - j0 + 1]
+#define S2(j, k) t.q2[(k) - k0 + 1][(j) - j0 + kC0]
+#define S3(j, k) t.q3[(k) - k0 + 1][(j) - j0 + kC0]
+#define SP(j, k) t.pr[(k) - k0 + 1][(j) - j0 + kC0]
     const int n2m = d.n2m, n3m = d.n3m;
     const double dt = d.dt, alre = al / d.ren;
 
@@ -302,26 +326,10 @@ __device__ __forceinline__ void nl_cell(const Dev &d, const NlTile &t, int j0, i
 #undef S3
 #undef SP
 
-// issues the copies of one tile into t (one cp.async group per thread)
-__device__ __forceinline__ void nl_prefetch(const Dev &d, NlTile &t, int tile, int ntj, int tid) {
-    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
-    // tile + halo: j = j0-1 .. j0+kNlJ, k = k0-1 .. k0+kNlK (entries outside
-    // the stored arrays, j < 1, j > n2, k > n3, are never read by a cell)
-    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
-    for (int e = tid; e < kW * kH; e += 256) {
-        const int r = e / kW, c = e % kW;
-        const int j = j0 - 1 + c, k = k0 - 1 + r;
-        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) {
-            const size_t i = fidx(d, j, k);
-            cp8(&t.q2[r][c], d.q2 + i);
-            cp8(&t.q3[r][c], d.q3 + i);
-            cp8(&t.pr[r][c], d.pr + i);
-        } else {
-            t.q2[r][c] = 0.0;
-            t.q3[r][c] = 0.0;
-            t.pr[r][c] = 0.0;
-        }
-    }
+// the tile's coefficient vectors (cp.async), and the commit of the thread's
+// cp.async group
+template <class Tile>
+__device__ __forceinline__ void nl_prefetch_coef(const Dev &d, Tile &t, int j0, int k0, int tid) {
     if (tid < kNlK) {
         const int k = min(k0 + tid, d.n3m);
         cp8(&t.udx3m[tid], d.udx3m + k);
@@ -344,6 +352,29 @@ __device__ __forceinline__ void nl_prefetch(const Dev &d, NlTile &t, int tile, i
         cp8(&t.ap3j[c], d.ap3j + j);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// issues the copies of one tile into t (one cp.async group per thread)
+__device__ __forceinline__ void nl_prefetch(const Dev &d, NlTile &t, int tile, int ntj, int tid) {
+    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+    // tile + halo: j = j0-1 .. j0+kNlJ, k = k0-1 .. k0+kNlK (entries outside
+    // the stored arrays, j < 1, j > n2, k > n3, are never read by a cell)
+    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
+    for (int e = tid; e < kW * kH; e += 256) {
+        const int r = e / kW, c = e % kW;
+        const int j = j0 - 1 + c, k = k0 - 1 + r;
+        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) {
+            const size_t i = fidx(d, j, k);
+            cp8(&t.q2[r][c], d.q2 + i);
+            cp8(&t.q3[r][c], d.q3 + i);
+            cp8(&t.pr[r][c], d.pr + i);
+        } else {
+            t.q2[r][c] = 0.0;
+            t.q3[r][c] = 0.0;
+            t.pr[r][c] = 0.0;
+        }
+    }
+    nl_prefetch_coef(d, t, j0, k0, tid);
 }
 
 // ru2/ru3 at this thread's cells of a tile (0 when ro = 0)
@@ -406,7 +437,7 @@ __device__ __forceinline__ void nl_rhs_body(const Dev &d, double al, double ga, 
             for (int i = 0; i < kNlK / 8; ++i) {
                 const int kc = k0 + (kNlK / 8) * threadIdx.y + i;
                 if (kc > d.n3m) break;
-                nl_cell(d, t, j0, k0, jc, kc, al, ga, ro, r2[i], r3[i]);
+                nl_cell<1>(d, t, j0, k0, jc, kc, al, ga, ro, r2[i], r3[i]);
             }
         }
         __syncthreads();   // this buffer is refilled two tiles on
@@ -417,6 +448,101 @@ __global__ void __launch_bounds__(256, kNlBlocksPerSM) k_nl_rhs(Dev d, double al
     extern __shared__ __align__(16) unsigned char nl_smem[];
     FB_GRID_WAIT();
     nl_rhs_body(d, al, ga, ro, reinterpret_cast<NlTile *>(nl_smem), pend != 0);
+}
+
+// the three field boxes of a tile, issued by one thread on the buffer's
+// mbarrier.  The proxy fence orders the threads' earlier reads (and the pend
+// pass's writes) of this buffer before the copies overwrite it.  Boxes that
+// reach past the fields (j < 1, j > n2, k > n3) are zero-filled there; no cell
+// reads those entries.
+__device__ __forceinline__ void nl_issue_tma(const NlMaps &m, NlTileT &t, uint32_t bar, int tile, int ntj) {
+    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+    const int x = j0 - 3, y = k0 - 1;   // x: element j - 1 of the column j = j0 - 2 (even: 16-byte aligned)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, 3u * kNlBoxBytes);
+    tma_load_2d(smem_u32(&t.q2[0][0]), &m.q2, bar, x, y);
+    tma_load_2d(smem_u32(&t.q3[0][0]), &m.q3, bar, x, y);
+    tma_load_2d(smem_u32(&t.pr[0][0]), &m.pr, bar, x, y);
+}
+
+// nl_rhs_body with the field tiles staged by TMA: tile it waits on phase
+// it / 2 of its buffer's mbarrier; the coefficient vectors stay cp.async.  A
+// wait that gives up (one second) records FB_ERR_TIMEOUT and ends the block's
+// tiles.
+__device__ __forceinline__ void nl_rhs_tma_body(const Dev &d, const NlMaps &m, double al, double ga, double ro,
+                                                NlTileT *buf, uint64_t *bars, bool pend) {
+    const double pravg = pend ? d.scal[S_PRAVG] : 0.0;
+    const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    const uint32_t bar0 = smem_u32(bars), bar1 = smem_u32(bars + 1);
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        nl_issue_tma(m, buf[0], bar0, tile, ntj);
+    }
+    {
+        const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+        nl_prefetch_coef(d, buf[0], j0, k0, tid);
+    }
+    double r2n[kNlK / 8], r3n[kNlK / 8];
+    nl_ru(d, tile, ntj, ro, r2n, r3n);
+    __syncthreads();   // the barriers are initialised before any thread waits on them
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        NlTileT &t = buf[it & 1];
+        double r2[kNlK / 8], r3[kNlK / 8];
+#pragma unroll
+        for (int i = 0; i < kNlK / 8; ++i) {
+            r2[i] = r2n[i];
+            r3[i] = r3n[i];
+        }
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) {
+            if (tid == 0) nl_issue_tma(m, buf[(it + 1) & 1], (it & 1) ? bar0 : bar1, nxt, ntj);
+            nl_prefetch_coef(d, buf[(it + 1) & 1], 1 + (nxt % ntj) * kNlJ, 1 + (nxt / ntj) * kNlK, tid);
+            nl_ru(d, nxt, ntj, ro, r2n, r3n);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        const bool landed = mbar_wait((it & 1) ? bar1 : bar0, static_cast<uint32_t>(it >> 1) & 1u);
+        if (__syncthreads_or(!landed)) {
+            if (tid == 0) atomicCAS(d.status, 0, FB_ERR_TIMEOUT);
+            return;
+        }
+        if (pend) {
+            for (int e = tid; e < kNlTH * kNlTW; e += 256) {
+                double &x = t.pr[e / kNlTW][e % kNlTW];
+                x = x - pravg;
+            }
+            __syncthreads();
+        }
+        const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+        const int jc = j0 + threadIdx.x;
+        if (jc <= d.n2m) {
+#pragma unroll
+            for (int i = 0; i < kNlK / 8; ++i) {
+                const int kc = k0 + (kNlK / 8) * threadIdx.y + i;
+                if (kc > d.n3m) break;
+                nl_cell<2>(d, t, j0, k0, jc, kc, al, ga, ro, r2[i], r3[i]);
+            }
+        }
+        __syncthreads();   // this buffer is refilled two tiles on
+    }
+}
+
+__global__ void __launch_bounds__(256, kNlBlocksPerSM)
+    k_nl_rhs_tma(const __grid_constant__ Dev d, const __grid_constant__ NlMaps m, double al, double ga, double ro,
+                 int pend) {
+    extern __shared__ __align__(16) unsigned char nl_smem[];
+    const uint32_t raw = smem_u32(nl_smem);
+    unsigned char *base = nl_smem + ((128u - (raw & 127u)) & 127u);   // the tiles on 128-byte boundaries
+    NlTileT *buf = reinterpret_cast<NlTileT *>(base);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(base + 2 * sizeof(NlTileT));
+    FB_GRID_WAIT();
+    nl_rhs_tma_body(d, m, al, ga, ro, buf, bars, pend != 0);
 }
 
 // ------------------------------------------------------------ MLS forcing
@@ -1951,9 +2077,39 @@ void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(std::min(d.n3m, 
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
 int nl_tiles(const Dev &d) { return ((d.n2m + kNlJ - 1) / kNlJ) * ((d.n3m + kNlK - 1) / kNlK); }
 
-void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s, bool pend) {
+void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s, bool pend, const NlMaps *maps) {
     const int blocks = std::min(nl_tiles(d), 148 * kNlBlocksPerSM);
-    pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro, pend ? 1 : 0);
+    if (maps) pdl(k_nl_rhs_tma, dim3(blocks), dim3(32, 8), kNlSmemT, s, d, *maps, al, ga, ro, pend ? 1 : 0);
+    else pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro, pend ? 1 : 0);
+}
+
+// q2, q3, pr as 2-D FP64 tensors: x = j - 1 (j = 1 .. n2), y = k (0 .. n3),
+// rows P doubles apart; a box is one tile with its halo (kNlTW x kNlTH)
+int encode_nl_maps(NlMaps *m, const Dev &d) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return FB_ERR_CUDA;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const double *f[3] = {d.q2, d.q3, d.pr};
+    CUtensorMap *dst[3] = {&m->q2, &m->q3, &m->pr};
+    for (int i = 0; i < 3; ++i) {
+        if ((reinterpret_cast<uintptr_t>(f[i]) & 15u) || (static_cast<long>(d.P) * 8) % 16 || d.P < d.n2)
+            return FB_ERR_STATE;
+        const cuuint64_t dims[2] = {static_cast<cuuint64_t>(d.n2), static_cast<cuuint64_t>(d.n3) + 1u};
+        const cuuint64_t strides[1] = {static_cast<cuuint64_t>(d.P) * 8u};
+        const cuuint32_t box[2] = {static_cast<cuuint32_t>(kNlTW), static_cast<cuuint32_t>(kNlTH)};
+        const cuuint32_t es[2] = {1, 1};
+        const CUresult r = encode(dst[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(f[i]), dims,
+                                  strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return FB_ERR_CUDA;
+    }
+    return FB_OK;
 }
 void launch_lgrdist(const Dev &d, cudaStream_t s) {
     if (d.nlm) pdl(k_lgrdist, dim3((d.nlm + 127) / 128), dim3(128), 0, s, d);
@@ -2027,6 +2183,9 @@ void glaunch_nl_rhs(const Group &g, int n, cudaStream_t s, bool pend) {
 cudaError_t kernels_configure() {
     cudaError_t e = cudaFuncSetAttribute(k_nl_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kNlSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_nl_rhs_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kNlSmemT));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kg_nl_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kNlSmem));
     if (e == cudaSuccess)

@@ -1,6 +1,7 @@
 // Kernel launchers of the fluid time step (definitions in kernels.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -12,8 +13,16 @@ constexpr int kRedSlot = 65536;  // block partials per reduction slot
 cudaError_t kernels_configure();   // shared-memory limits (once per device)
 void launch_cfl(const Dev &d, cudaStream_t s);
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s);
-// pend / deferred: the fused step's deferred pr_submean of RK3 substeps 1 and 2
-void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s, bool pend = false);
+// TMA descriptors of q2, q3 and pr for the tiles of k_nl_rhs: the fields as
+// 2-D arrays (j - 1 fastest, row k, k = 0 .. n3), one box per tile and field
+struct alignas(64) NlMaps {
+    CUtensorMap q2, q3, pr;
+};
+int encode_nl_maps(NlMaps *m, const Dev &d);   // FB_OK, or an error (no maps)
+// pend / deferred: the fused step's deferred pr_submean of RK3 substeps 1 and 2.
+// maps: stage the tiles with TMA (the single-case step); null: cp.async
+void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s, bool pend = false,
+                   const NlMaps *maps = nullptr);
 void launch_lgrdist(const Dev &d, cudaStream_t s);
 void launch_mls_setup(const Dev &d, cudaStream_t s);
 void launch_mls_interp(const Dev &d, cudaStream_t s);
