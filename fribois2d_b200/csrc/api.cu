@@ -54,7 +54,7 @@ struct fb_ctx {
     cublasLtMatmulAlgo_t lt_algo[2] = {};
     bool lt_on[2] = {false, false};
     Dev d{};
-    fb::NlMaps nlmaps{};                      // TMA descriptors of q2, q3, pr for the k_nl_rhs tiles
+    fb::NlMaps nlmaps{};                      // TMA descriptors of the stencil tiles' fields
     SubDev sub[3]{};
     double usdtal[3] = {0, 0, 0};
     std::vector<void *> allocs;
@@ -943,7 +943,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         fb::launch_scan_poisson(d, st);
         if ((r = gemm_bwd(c))) return r;
         break;
-    case FB_ST_UPDVP: fb::launch_updvp_prcalc(d, al, al * c->beta, st); break;
+    case FB_ST_UPDVP: fb::launch_updvp_prcalc(d, al, al * c->beta, st, false, &c->nlmaps); break;
     case FB_ST_PRSUBMEAN: fb::launch_submean_boucqt(d, st); break;
     case FB_ST_CHECKBCS:
     case FB_ST_LOADS: fb::launch_loads(d, st); break;
@@ -1037,7 +1037,7 @@ int enqueue_fluid(fb_ctx *c, int ns) {
         if ((r = stage_impl(c, FB_ST_DIVG, ns, n))) return r;
         if ((r = stage_impl(c, FB_ST_PHCALC, ns, n))) return r;
         if (pend) {
-            fb::launch_updvp_prcalc(d, al, al * c->beta, c->stream, true);
+            fb::launch_updvp_prcalc(d, al, al * c->beta, c->stream, true, &c->nlmaps);
             c->own_launches += 1;
         } else if ((r = stage_impl(c, FB_ST_UPDVP, ns, n))) {
             return r;

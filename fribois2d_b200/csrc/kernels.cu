@@ -1178,15 +1178,25 @@ struct UpTile {
 constexpr size_t kUpSmem = 2 * sizeof(UpTile);
 constexpr int kUpBlocksPerSM = 3;
 
-__device__ __forceinline__ void up_prefetch(const Dev &d, UpTile &t, int tile, int ntj, int tid) {
+// the TMA-staged form: the dph box of kNlTH x kNlTW (column c holds j = j0 - 2 + c)
+struct alignas(128) UpTileT {
+    alignas(128) double dph[kNlTH][kNlTW];
+    double kc[6][kNlK];
+    double jc[6][kNlJ];
+};
+constexpr size_t kUpSmemT = 2 * sizeof(UpTileT) + 128 + 128;   // tiles, two mbarriers, alignment slack
+
+// the dph box of a tile, issued by one thread (see nl_issue_tma)
+__device__ __forceinline__ void up_issue_tma(const NlMaps &m, UpTileT &t, uint32_t bar, int tile, int ntj) {
     const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
-    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
-    for (int e = tid; e < kW * kH; e += 256) {
-        const int r = e / kW, c = e % kW;
-        const int j = j0 - 1 + c, k = k0 - 1 + r;
-        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) cp8(&t.dph[r][c], d.dph + fidx(d, j, k));
-        else t.dph[r][c] = 0.0;
-    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, kNlBoxBytes);
+    tma_load_2d(smem_u32(&t.dph[0][0]), &m.dph, bar, j0 - 3, k0 - 1);
+}
+
+// the tile's coefficient vectors (cp.async) and the commit of the thread's group
+template <class Tile>
+__device__ __forceinline__ void up_prefetch_coef(const Dev &d, Tile &t, int j0, int k0, int tid) {
     if (tid < kNlK) {
         const int k = min(k0 + tid, d.n3m);
         cp8(&t.kc[0][tid], d.udx3c + k);
@@ -1207,6 +1217,18 @@ __device__ __forceinline__ void up_prefetch(const Dev &d, UpTile &t, int tile, i
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+__device__ __forceinline__ void up_prefetch(const Dev &d, UpTile &t, int tile, int ntj, int tid) {
+    const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
+    constexpr int kW = kNlJ + 2, kH = kNlK + 2;
+    for (int e = tid; e < kW * kH; e += 256) {
+        const int r = e / kW, c = e % kW;
+        const int j = j0 - 1 + c, k = k0 - 1 + r;
+        if (j >= 1 && j <= d.n2 && k >= 0 && k <= d.n3) cp8(&t.dph[r][c], d.dph + fidx(d, j, k));
+        else t.dph[r][c] = 0.0;
+    }
+    up_prefetch_coef(d, t, j0, k0, tid);
+}
+
 // q2, q3, pr at this thread's cells of a tile, read before any is written
 __device__ __forceinline__ void up_own(const Dev &d, int tile, int ntj, double (&q2)[kNlK / 8], double (&q3)[kNlK / 8],
                                        double (&pr)[kNlK / 8]) {
@@ -1224,11 +1246,15 @@ __device__ __forceinline__ void up_own(const Dev &d, int tile, int ntj, double (
 
 // pend: as for nl_rhs, pr - pravg of the previous substep is the pressure
 // this update starts from (read before this grid's last block stores the new
-// mean)
-__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be, UpTile *buf,
-                                                  bool pend = false) {
+// mean).  kTma: the dph tiles are TMA boxes on the mbarriers bars (maps m);
+// a wait that gives up records FB_ERR_TIMEOUT and ends the block's tiles (the
+// block still takes part in the mean)
+template <bool kTma, class Tile>
+__device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, double be, Tile *buf, bool pend = false,
+                                                  const NlMaps *m = nullptr, uint64_t *bars = nullptr) {
     __shared__ double sh[32];
     __shared__ bool last;
+    constexpr int kC0 = kTma ? 2 : 1;   // the tile column of j = j0
     const double pravg = pend ? d.scal[S_PRAVG] : 0.0;
     const int ntj = (d.n2m + kNlJ - 1) / kNlJ, ntk = (d.n3m + kNlK - 1) / kNlK, ntiles = ntj * ntk;
     const int t = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
@@ -1237,12 +1263,28 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
     double part = 0.0;
     int tile = blockIdx.x;
     double q2n[kC], q3n[kC], prn[kC];
+    uint32_t bar0 = 0, bar1 = 0;
+    if constexpr (kTma) {
+        bar0 = smem_u32(bars);
+        bar1 = smem_u32(bars + 1);
+    }
     if (tile < ntiles) {
-        up_prefetch(d, buf[0], tile, ntj, t);
+        if constexpr (kTma) {
+            if (t == 0) {
+                mbar_init(bar0, 1);
+                mbar_init(bar1, 1);
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+                up_issue_tma(*m, buf[0], bar0, tile, ntj);
+            }
+            up_prefetch_coef(d, buf[0], 1 + (tile % ntj) * kNlJ, 1 + (tile / ntj) * kNlK, t);
+            __syncthreads();   // the barriers are initialised before any thread waits on them
+        } else {
+            up_prefetch(d, buf[0], tile, ntj, t);
+        }
         up_own(d, tile, ntj, q2n, q3n, prn);
     }
     for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-        const UpTile &u = buf[it & 1];
+        const Tile &u = buf[it & 1];
         double q2v[kC], q3v[kC], prv[kC];
 #pragma unroll
         for (int i = 0; i < kC; ++i) {
@@ -1252,16 +1294,29 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
         }
         const int nxt = tile + gridDim.x;
         if (nxt < ntiles) {
-            up_prefetch(d, buf[(it + 1) & 1], nxt, ntj, t);
+            if constexpr (kTma) {
+                if (t == 0) up_issue_tma(*m, buf[(it + 1) & 1], (it & 1) ? bar0 : bar1, nxt, ntj);
+                up_prefetch_coef(d, buf[(it + 1) & 1], 1 + (nxt % ntj) * kNlJ, 1 + (nxt / ntj) * kNlK, t);
+            } else {
+                up_prefetch(d, buf[(it + 1) & 1], nxt, ntj, t);
+            }
             up_own(d, nxt, ntj, q2n, q3n, prn);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
-        __syncthreads();
+        if constexpr (kTma) {
+            const bool landed = mbar_wait((it & 1) ? bar1 : bar0, static_cast<uint32_t>(it >> 1) & 1u);
+            if (__syncthreads_or(!landed)) {
+                if (t == 0) atomicCAS(d.status, 0, FB_ERR_TIMEOUT);
+                break;
+            }
+        } else {
+            __syncthreads();
+        }
         const int j0 = 1 + (tile % ntj) * kNlJ, k0 = 1 + (tile / ntj) * kNlK;
         const int jc = j0 + threadIdx.x;
-#define TD(j, k) u.dph[(k) - k0 + 1][(j) - j0 + 1]
+#define TD(j, k) u.dph[(k) - k0 + 1][(j) - j0 + kC0]
         if (jc <= d.n2m) {
             const int cj = jc - j0;
             const int jm = jmv_(jc), jp = jpv_(d, jc);
@@ -1313,7 +1368,18 @@ __device__ __forceinline__ void updvp_prcalc_body(const Dev &d, double al, doubl
 __global__ void __launch_bounds__(256, kUpBlocksPerSM) k_updvp_prcalc(Dev d, double al, double be, int pend) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     FB_GRID_WAIT();
-    updvp_prcalc_body(d, al, be, reinterpret_cast<UpTile *>(up_smem), pend != 0);
+    updvp_prcalc_body<false>(d, al, be, reinterpret_cast<UpTile *>(up_smem), pend != 0);
+}
+
+__global__ void __launch_bounds__(256, kUpBlocksPerSM)
+    k_updvp_prcalc_tma(const __grid_constant__ Dev d, const __grid_constant__ NlMaps m, double al, double be,
+                       int pend) {
+    extern __shared__ __align__(16) unsigned char up_smem[];
+    const uint32_t raw = smem_u32(up_smem);
+    unsigned char *base = up_smem + ((128u - (raw & 127u)) & 127u);   // the tiles on 128-byte boundaries
+    FB_GRID_WAIT();
+    updvp_prcalc_body<true>(d, al, be, reinterpret_cast<UpTileT *>(base), pend != 0, &m,
+                            reinterpret_cast<uint64_t *>(base + 2 * sizeof(UpTileT)));
 }
 
 // pr_submean (updvp.F90:336: the whole array) and boucqt (iobcs.F90:97-105)
@@ -2012,7 +2078,7 @@ __global__ void __launch_bounds__(256, kUpBlocksPerSM) kg_updvp_prcalc(const Gro
     __shared__ Dev d;
     __shared__ SubDev s;
     if (!stage_case(g, &d, &s, n)) return;
-    updvp_prcalc_body(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem), pend != 0);
+    updvp_prcalc_body<false>(d, s.al, s.al * s.beta, reinterpret_cast<UpTile *>(up_smem), pend != 0);
 }
 
 __global__ void kg_submean_boucqt(const GroupCase *__restrict__ g, int deferred) {
@@ -2083,7 +2149,7 @@ void launch_nl_rhs(const Dev &d, double al, double ga, double ro, cudaStream_t s
     else pdl(k_nl_rhs, dim3(blocks), dim3(32, 8), kNlSmem, s, d, al, ga, ro, pend ? 1 : 0);
 }
 
-// q2, q3, pr as 2-D FP64 tensors: x = j - 1 (j = 1 .. n2), y = k (0 .. n3),
+// q2, q3, pr, dph as 2-D FP64 tensors: x = j - 1 (j = 1 .. n2), y = k (0 .. n3),
 // rows P doubles apart; a box is one tile with its halo (kNlTW x kNlTH)
 int encode_nl_maps(NlMaps *m, const Dev &d) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -2095,9 +2161,9 @@ int encode_nl_maps(NlMaps *m, const Dev &d) {
             return FB_ERR_CUDA;
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
-    const double *f[3] = {d.q2, d.q3, d.pr};
-    CUtensorMap *dst[3] = {&m->q2, &m->q3, &m->pr};
-    for (int i = 0; i < 3; ++i) {
+    const double *f[4] = {d.q2, d.q3, d.pr, d.dph};
+    CUtensorMap *dst[4] = {&m->q2, &m->q3, &m->pr, &m->dph};
+    for (int i = 0; i < 4; ++i) {
         if ((reinterpret_cast<uintptr_t>(f[i]) & 15u) || (static_cast<long>(d.P) * 8) % 16 || d.P < d.n2)
             return FB_ERR_STATE;
         const cuuint64_t dims[2] = {static_cast<cuuint64_t>(d.n2), static_cast<cuuint64_t>(d.n3) + 1u};
@@ -2138,9 +2204,10 @@ void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
     dim3 b(32, 8);
     pdl(k_divg, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, usdtal);
 }
-void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend) {
+void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend, const NlMaps *maps) {
     const int blocks = std::min(nl_tiles(d), 148 * kUpBlocksPerSM);
-    pdl(k_updvp_prcalc, dim3(blocks), dim3(32, 8), kUpSmem, s, d, al, be, pend ? 1 : 0);
+    if (maps) pdl(k_updvp_prcalc_tma, dim3(blocks), dim3(32, 8), kUpSmemT, s, d, *maps, al, be, pend ? 1 : 0);
+    else pdl(k_updvp_prcalc, dim3(blocks), dim3(32, 8), kUpSmem, s, d, al, be, pend ? 1 : 0);
 }
 void launch_submean_boucqt(const Dev &d, cudaStream_t s, bool deferred) {
     dim3 b(32, 8);
@@ -2186,6 +2253,9 @@ cudaError_t kernels_configure() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_nl_rhs_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kNlSmemT));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_updvp_prcalc_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kUpSmemT));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kg_nl_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kNlSmem));
     if (e == cudaSuccess)

@@ -13,10 +13,11 @@ constexpr int kRedSlot = 65536;  // block partials per reduction slot
 cudaError_t kernels_configure();   // shared-memory limits (once per device)
 void launch_cfl(const Dev &d, cudaStream_t s);
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s);
-// TMA descriptors of q2, q3 and pr for the tiles of k_nl_rhs: the fields as
-// 2-D arrays (j - 1 fastest, row k, k = 0 .. n3), one box per tile and field
+// TMA descriptors of the fields that the stencil tiles stage (q2, q3, pr for
+// k_nl_rhs, dph for k_updvp_prcalc): 2-D arrays (j - 1 fastest, row k,
+// k = 0 .. n3), one box per tile and field
 struct alignas(64) NlMaps {
-    CUtensorMap q2, q3, pr;
+    CUtensorMap q2, q3, pr, dph;
 };
 int encode_nl_maps(NlMaps *m, const Dev &d);   // FB_OK, or an error (no maps)
 // pend / deferred: the fused step's deferred pr_submean of RK3 substeps 1 and 2.
@@ -30,7 +31,8 @@ void launch_mls_spread(const Dev &d, cudaStream_t s);
 void launch_spread_chains(const Dev &d, cudaStream_t s);
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
 void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
-void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend = false);
+void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend = false,
+                         const NlMaps *maps = nullptr);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s, bool deferred = false);
 void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream_t s);  // boucqt + next boucdq
 void launch_loads(const Dev &d, cudaStream_t s);
