@@ -73,33 +73,49 @@ __device__ __forceinline__ void cfl_body(const Dev &d) {
     const int b = blockIdx.x, nb = gridDim.x;
     double qcf = 1.0e-8, q3a = 0.0;
     // rows k over the blocks, columns j over the threads (no index division);
-    // kU columns of a thread per pass, their loads all issued before the
-    // first use (the same per-thread order of the sum as one at a time)
-    constexpr int kU = 4;
-    for (int k = b + 1; k <= d.n3m; k += nb) {
-        const int kp = k + 1;
-        const double udx3 = d.udx3m[k], dz = d.zz[kp] - d.zz[k];
+    // kR rows (k, k + nb, ...) by kU columns of a thread per pass, their loads
+    // all issued before the first use; a row's terms are summed before the
+    // next row's (for rows of up to kU x blockDim columns, the per-thread
+    // order of the sum is that of one value at a time)
+    constexpr int kU = 4, kR = 2;
+    for (int k0 = b + 1; k0 <= d.n3m; k0 += kR * nb) {
+        double udx3[kR], dz[kR];
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+            const int k = min(k0 + r * nb, d.n3m);
+            udx3[r] = d.udx3m[k];
+            dz[r] = d.zz[k + 1] - d.zz[k];
+        }
         for (int j0 = t + 1; j0 <= d.n2m; j0 += kU * nt) {
-            double a2[kU], b2[kU], a3[kU], b3[kU], u2[kU], rj[kU], rjp[kU];
+            double a2[kR][kU], b2[kR][kU], a3[kR][kU], b3[kR][kU], u2[kU], rj[kU], rjp[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int j = min(j0 + u * nt, d.n2m), jp = j + 1;
-                a2[u] = Fv(d.q2, j, k);
-                b2[u] = Fv(d.q2, jp, k);
-                a3[u] = Fv(d.q3, j, k);
-                b3[u] = Fv(d.q3, j, kp);
                 u2[u] = d.udx2m[j];
                 rj[u] = d.rc[j];
                 rjp[u] = d.rc[jp];
+#pragma unroll
+                for (int r = 0; r < kR; ++r) {
+                    const int k = min(k0 + r * nb, d.n3m);
+                    a2[r][u] = Fv(d.q2, j, k);
+                    b2[r][u] = Fv(d.q2, jp, k);
+                    a3[r][u] = Fv(d.q3, j, k);
+                    b3[r][u] = Fv(d.q3, j, k + 1);
+                }
             }
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                if (j0 + u * nt > d.n2m) break;
-                const double q = (fabs((a2[u] + b2[u]) * 0.5 * u2[u]) + fabs((a3[u] + b3[u]) * 0.5 * udx3));
-                // fmax drops a NaN: a non-finite velocity turns into +inf, which
-                // every later fmax keeps, so the CFL test below catches it
-                qcf = fmax(qcf, (q == q) ? q : INFINITY);
-                q3a = q3a + a3[u] * dz * (rjp[u] - rj[u]);
+            for (int r = 0; r < kR; ++r) {
+                if (k0 + r * nb > d.n3m) break;
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    if (j0 + u * nt > d.n2m) break;
+                    const double q = (fabs((a2[r][u] + b2[r][u]) * 0.5 * u2[u]) +
+                                      fabs((a3[r][u] + b3[r][u]) * 0.5 * udx3[r]));
+                    // fmax drops a NaN: a non-finite velocity turns into +inf, which
+                    // every later fmax keeps, so the CFL test below catches it
+                    qcf = fmax(qcf, (q == q) ? q : INFINITY);
+                    q3a = q3a + a3[r][u] * dz[r] * (rjp[u] - rj[u]);
+                }
             }
         }
     }
@@ -2139,7 +2155,9 @@ int group_stride_blocks(const Dev &d) {
     const long cells = static_cast<long>(d.n2m) * d.n3m;
     return static_cast<int>(std::max<long>(1, std::min<long>((cells + 2047) / 2048, 148L * 8)));
 }
-void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(std::min(d.n3m, 148 * 8)), dim3(256), 0, s, d); }
+// two blocks per SM, each on pairs of rows: few partials for the last block
+// to gather, and few arrivals on the grid's counter
+void launch_cfl(const Dev &d, cudaStream_t s) { pdl(k_cfl, dim3(std::min(d.n3m, 148 * 2)), dim3(256), 0, s, d); }
 void launch_boucdq(const Dev &d, double ga, double ro, cudaStream_t s) { pdl(k_boucdq, dim3(1), dim3(1024), 0, s, d, ga, ro); }
 int nl_tiles(const Dev &d) { return ((d.n2m + kNlJ - 1) / kNlJ) * ((d.n3m + kNlK - 1) / kNlK); }
 
