@@ -277,7 +277,7 @@ def kernel_table(fb, path, c, poisson="int8x8", sweeps=2):
         # reads the FP64 operand and writes 8 int8 planes (16 B per cell)
         transform = [
             ("i8x8 GEMM (tcgen05 kind::i8, 36 digit pairs)", "i8x8_gemm", 6, 36 * gemm, "tensor_i8"),
-            ("i8 digit cut (one cluster launch)", "i8_split", 6, 2.0 * B, "hbm"),
+            ("i8 digit cut (row maxima from the producers)", "i8_split", 6, 2.0 * B, "hbm"),
             ("poisson_tri", "poisson_tri", 3, 3 * B, "hbm"),
         ] + dgemm_rows
     elif poisson == "fp64":

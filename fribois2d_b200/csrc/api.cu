@@ -110,6 +110,10 @@ struct fb_ctx {
     // FP64 transforms on the INT8 tensor cores: digit planes of the data
     // operand (dph, then hmn) and of the two eigenvector matrices
     fb::I8Plan i8a{}, i8f{}, i8b{};
+    // row maxima of the data operand for the digit cut, accumulated by its
+    // producer: [0, ldh) dph's (divg), [ldh, 2 ldh) hmn's (the mode solves);
+    // each cut clears the other half for the next producer
+    double *i8max = nullptr;
     bool i8_ready = false;
     int own_launches = 0;     // own kernels enqueued (counted while capturing)
     int step_kernels = 0;     // own kernels per captured step (coupled: with one fluid solve)
@@ -865,6 +869,7 @@ int setup_i8(fb_ctx *c) {
     if ((st = make(c->i8a, d.n2m, 128)) || (st = make(c->i8f, d.n3m, c->tune_i8bn)) ||
         (st = make(c->i8b, d.n3m, c->tune_i8bn)))
         return st;
+    if ((st = dnew(c, &c->i8max, 2 * static_cast<size_t>(d.ldh)))) return st;   // zeroed
     // forward B(m, k) = zmmt(m, k); backward B(k, m) = zmm(k, m): both column-major
     fb::launch_i8_split(c->zmmt, d.n3m, d.n3m, d.n3m, c->i8f, c->stream);
     fb::launch_i8_split(c->zmm, d.n3m, d.n3m, d.n3m, c->i8b, c->stream);
@@ -879,10 +884,12 @@ int setup_i8(fb_ctx *c) {
 int phcalc_i8(fb_ctx *c) {
     const Dev &d = c->d;
     cudaStream_t st = c->stream;
-    fb::launch_i8_split(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, st);
+    // dph's row maxima come from divg, hmn's from the mode solves
+    double *mx_dph = c->i8max, *mx_hmn = c->i8max + d.ldh;
+    fb::launch_i8_cut_rows(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, mx_dph, mx_hmn, st);
     fb::launch_i8x8(c->i8a, c->i8f, d.hmn, d.ldh, d.status, st, true);   // i8f, i8b: cut once at set-up
-    fb::launch_scan_poisson(d, st);
-    fb::launch_i8_split(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, st);
+    fb::launch_scan_poisson(d, st, mx_hmn);
+    fb::launch_i8_cut_rows(d.hmn, d.ldh, d.n2m, d.n3m, c->i8a, mx_hmn, mx_dph, st);
     fb::launch_i8x8(c->i8a, c->i8b, d.dph + d.P, d.P, d.status, st, true);
     c->own_launches += 5;   // two digit cuts, two products, the mode solves
     return FB_OK;
@@ -925,7 +932,9 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
             fb::launch_helsolve(d, s, st);
         }
         break;
-    case FB_ST_DIVG: fb::launch_divg(d, c->usdtal[n - 1], st); break;
+    case FB_ST_DIVG:   // with the INT8 transforms: dph's row maxima for their digit cut
+        fb::launch_divg(d, c->usdtal[n - 1], st, c->poisson_mode == FB_POISSON_INT8X8 ? c->i8max : nullptr);
+        break;
     case FB_ST_PHCALC:
         // kOwn counts the mode solves of the DGEMM form; the tensor-core forms
         // count all of their own launches themselves
@@ -955,9 +964,9 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
         if (!c->pw) return FB_ERR_STATE;
         fb::launch_tf32x3(c->plan_fwd, d.hmn, d.ldh, nullptr, 0, d.status, st);
         break;
-    case FB_TK_I8_SPLIT:
+    case FB_TK_I8_SPLIT:   // the step's form: dph's row maxima from the last divg (kept)
         if (!c->i8_ready) return FB_ERR_STATE;
-        fb::launch_i8_split(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, st);
+        fb::launch_i8_cut_rows(d.dph + d.P, d.P, d.n2m, d.n3m, c->i8a, c->i8max, nullptr, st);
         break;
     case FB_TK_I8X8_GEMM:
         if (!c->i8_ready) return FB_ERR_STATE;
@@ -3179,18 +3188,25 @@ int fb_gemm_i8x8(int device, int M, int N, int K, const double *A, const double 
     pa.scale = static_cast<double *>(alloc(sizeof(double) * pa.rows_pad));
     pb.scale = static_cast<double *>(alloc(sizeof(double) * pb.rows_pad));
     int *status = static_cast<int *>(alloc(sizeof(int)));
+    double *mxA = static_cast<double *>(alloc(sizeof(double) * M));
+    double *mxB = static_cast<double *>(alloc(sizeof(double) * N));
     st = FB_OK;
-    if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !status)
+    if (!dA || !dB || !dC || !pa.dig || !pb.dig || !pa.scale || !pb.scale || !status || !mxA || !mxB)
         st = FB_ERR_CUDA;
     if (!st && (cudaMemcpy(dA, A, sizeof(double) * M * K, cudaMemcpyHostToDevice) != cudaSuccess ||
                 cudaMemcpy(dB, B, sizeof(double) * N * K, cudaMemcpyHostToDevice) != cudaSuccess ||
-                cudaMemset(status, 0, sizeof(int)) != cudaSuccess))
+                cudaMemset(status, 0, sizeof(int)) != cudaSuccess ||
+                cudaMemset(mxA, 0, sizeof(double) * M) != cudaSuccess ||
+                cudaMemset(mxB, 0, sizeof(double) * N) != cudaSuccess))
         st = FB_ERR_CUDA;
     if (!st) st = fb::i8_plan(pa, M, K, 128);
     if (!st) st = fb::i8_plan(pb, N, K, fb::kI8BN);
     if (!st) {
-        fb::launch_i8_split(dA, M, M, K, pa, nullptr);
-        fb::launch_i8_split(dB, N, N, K, pb, nullptr);
+        // row maxima, then the cut of each operand (the step's kernels)
+        fb::launch_i8_rowmax(dA, M, M, K, mxA, nullptr);
+        fb::launch_i8_rowmax(dB, N, N, K, mxB, nullptr);
+        fb::launch_i8_cut_rows(dA, M, M, K, pa, mxA, nullptr, nullptr);
+        fb::launch_i8_cut_rows(dB, N, N, K, pb, mxB, nullptr, nullptr);
         fb::launch_i8x8(pa, pb, dC, M, status, nullptr);
         if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = FB_ERR_CUDA;
     }

@@ -112,6 +112,12 @@ __device__ __forceinline__ void cp8(double *dst, const double *src) {
 }
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// *addr = max(*addr, v) for non-negative, non-NaN doubles: their bit
+// patterns order as their values
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long *>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
 // copies case blockIdx.z's view of a group (and the constants of substep n
 // when ss is given) to shared memory, then waits for the preceding kernel
 // (programmatic dependent launch) and the block.  The group array is written

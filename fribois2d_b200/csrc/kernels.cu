@@ -1168,18 +1168,40 @@ __global__ void k_tri_z3(Dev d, SubDev s) {
 // ------------------------------------------------------------ Poisson
 
 // divergence.F90:88-115 (divg)
-__device__ __forceinline__ void divg_body(const Dev &d, double usdtal) {
+// Blocks of 32 x 8 threads over 32 x (8 kDivK) cells: thread (x, y) takes j0 + x
+// and the rows k0 + y + 8 i.  rmax (may be null): the maxima of |dph| over
+// each row j (the rows of the INT8 transform's data operand) are accumulated
+// into rmax[j - 1], one atomic per block and row, for the digit cut that follows
+constexpr int kDivK = 4;
+__device__ __forceinline__ void divg_body(const Dev &d, double usdtal, double *rmax = nullptr) {
     const int jc = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int kc = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    if (jc > d.n2m || kc > d.n3m) return;
-    const double dqcap = (Fv(d.q2, jc + 1, kc) - Fv(d.q2, jc, kc)) * d.udx2m[jc] +
-                         (Fv(d.q3, jc, kc + 1) - Fv(d.q3, jc, kc)) * d.udx3m[kc];
-    Fv(d.dph, jc, kc) = dqcap * usdtal;
+    const int kb = blockIdx.y * blockDim.y * kDivK + threadIdx.y + 1;
+    double m = 0.0;
+    if (jc <= d.n2m) {
+#pragma unroll
+        for (int i = 0; i < kDivK; ++i) {
+            const int kc = kb + static_cast<int>(blockDim.y) * i;
+            if (kc > d.n3m) break;
+            const double dqcap = (Fv(d.q2, jc + 1, kc) - Fv(d.q2, jc, kc)) * d.udx2m[jc] +
+                                 (Fv(d.q3, jc, kc + 1) - Fv(d.q3, jc, kc)) * d.udx3m[kc];
+            const double v = dqcap * usdtal;
+            Fv(d.dph, jc, kc) = v;
+            m = fmax(m, fabs(v));   // fmax drops a NaN, as the cut's maximum does
+        }
+    }
+    if (!rmax) return;
+    __shared__ double part[8][32];
+    part[threadIdx.y][threadIdx.x] = m;
+    __syncthreads();
+    if (threadIdx.y == 0 && jc <= d.n2m) {
+        for (int q = 1; q < 8; ++q) m = fmax(m, part[q][threadIdx.x]);
+        if (m > 0.0) atomic_max_nonneg(rmax + jc - 1, m);
+    }
 }
 
-__global__ void k_divg(Dev d, double usdtal) {
+__global__ void k_divg(Dev d, double usdtal, double *rmax) {
     FB_GRID_WAIT();
-    divg_body(d, usdtal);
+    divg_body(d, usdtal, rmax);
 }
 
 // updvp.F90:5-59 (updvp) fused with updvp.F90:68-105 (prcalc) and the
@@ -2218,9 +2240,9 @@ void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s) {
     pdl(k_tri_y3, dim3((d.n3m + 63) / 64), dim3(64), 0, s, d, sd);
     pdl(k_tri_z3, dim3((d.n2m + 63) / 64), dim3(64), 0, s, d, sd);
 }
-void launch_divg(const Dev &d, double usdtal, cudaStream_t s) {
-    dim3 b(32, 8);
-    pdl(k_divg, dim3(grid2(d.n2m, d.n3m, b)), dim3(b), 0, s, d, usdtal);
+void launch_divg(const Dev &d, double usdtal, cudaStream_t s, double *rmax) {
+    dim3 b(32, 8);   // the row maxima's reduction assumes these blocks
+    pdl(k_divg, dim3(grid2(d.n2m, (d.n3m + kDivK - 1) / kDivK, b)), dim3(b), 0, s, d, usdtal, rmax);
 }
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend, const NlMaps *maps) {
     const int blocks = std::min(nl_tiles(d), 148 * kUpBlocksPerSM);
@@ -2299,7 +2321,7 @@ void glaunch_forcing(const Group &g, cudaStream_t s) {
 }
 void glaunch_divg(const Group &g, int n, cudaStream_t s) {
     dim3 b(32, 8);
-    pdl(kg_divg, zgrid(grid2(g.rep.n2m, g.rep.n3m, b), g), dim3(b), 0, s, g.cases, n);
+    pdl(kg_divg, zgrid(grid2(g.rep.n2m, (g.rep.n3m + kDivK - 1) / kDivK, b), g), dim3(b), 0, s, g.cases, n);
 }
 void glaunch_updvp_prcalc(const Group &g, int n, cudaStream_t s, bool pend) {
     const int per_case = std::max(1, std::min(nl_tiles(g.rep), (2 * 148 * kUpBlocksPerSM + g.n - 1) / g.n));

@@ -30,7 +30,8 @@ void launch_mls_interp(const Dev &d, cudaStream_t s);
 void launch_mls_spread(const Dev &d, cudaStream_t s);
 void launch_spread_chains(const Dev &d, cudaStream_t s);
 void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
-void launch_divg(const Dev &d, double usdtal, cudaStream_t s);
+// rmax (may be null): n2m row maxima of |dph| accumulated for the INT8 digit cut
+void launch_divg(const Dev &d, double usdtal, cudaStream_t s, double *rmax = nullptr);
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend = false,
                          const NlMaps *maps = nullptr);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s, bool deferred = false);

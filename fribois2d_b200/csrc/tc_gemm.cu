@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -658,6 +659,57 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // Columns past K and rows past R get zero digits, up to ldk and rows_pad.
 constexpr int kCutCl = 8;
 
+// the digits of a thread's V values a of row r (columns c0 ..) at the row's
+// scale s = 2^-e into the kI8S slices
+template <int V>
+__device__ __forceinline__ void i8_cut_emit(const double (&a)[V / 4][4], double s, int r, int c0, int8_t *dig,
+                                            long ldk, long plane) {
+    constexpr int kP = V / 4;   // 32-bit words (four columns) per thread and slice
+    // |a s| < 1, so a s 2^(7 kI8S) (exact: powers of two) truncated toward
+    // zero is an integer below 2^(7 kI8S) whose base-128 digits, carrying the
+    // sign of a, are the kI8S digits: d_i = sign(a) floor(|a s| 128^(i+1)) mod 128
+    unsigned long long u[kP][4];
+    uint32_t neg[kP];
+#pragma unroll
+    for (int p = 0; p < kP; ++p) {
+        neg[p] = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long long v = __double2ll_rz((a[p][q] * s) * 72057594037927936.0);   // 2^56
+            u[p][q] = static_cast<unsigned long long>(v < 0 ? -v : v);
+            neg[p] |= (v < 0 ? 0xFFu : 0u) << (8 * q);
+        }
+    }
+    static_assert(kI8S == 8, "2^56 = 128^kI8S");
+    // each slice's V digits of row r are V consecutive bytes: the thread
+    // stores them itself (a whole 32-byte sector between neighbouring warps),
+    // no shared-memory transpose; rows up to rows_pad get digits (zero past R)
+    const bool live = c0 < ldk;   // ldk is a multiple of 128, so a run is inside or wholly past it
+    int8_t *out = dig + static_cast<size_t>(r) * ldk + c0;
+    constexpr int kUnroll = (V <= 32) ? kI8S : 1;   // constant shifts where registers allow
+#pragma unroll kUnroll
+    for (int i = 0; i < kI8S; ++i) {
+        const int sh = 7 * (kI8S - 1 - i);
+        uint32_t word[kP];
+#pragma unroll
+        for (int p = 0; p < kP; ++p) {
+            uint32_t mag = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
+            // the negative values' bytes negated (bytewise, no carries between bytes)
+            const uint32_t mk = neg[p];
+            word[p] = (mag & ~mk) | (__vsub4(0u, mag) & mk);
+        }
+        if (live) {
+            int8_t *o = out + static_cast<size_t>(i) * plane;
+#pragma unroll
+            for (int v4 = 0; v4 < V / 16; ++v4)
+                reinterpret_cast<uint4 *>(o)[v4] =
+                    make_uint4(word[4 * v4], word[4 * v4 + 1], word[4 * v4 + 2], word[4 * v4 + 3]);
+        }
+    }
+}
+
 template <int V>
 __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long lds, int R, int K, int8_t *dig,
                                             long ldk, long plane, double *rowscale) {
@@ -701,49 +753,57 @@ __device__ __forceinline__ void i8_cut_body(const double *__restrict__ src, long
         if (rank == 0 && r < R) rowscale[r] = ldexp(1.0, e);
     }
     cl.sync();   // no CTA leaves while another still reads its maxima
-    const double s = sc[lane];
-    // |a s| < 1, so a s 2^(7 kI8S) (exact: powers of two) truncated toward
-    // zero is an integer below 2^(7 kI8S) whose base-128 digits, carrying the
-    // sign of a, are the kI8S digits: d_i = sign(a) floor(|a s| 128^(i+1)) mod 128
-    unsigned long long u[kP][4];
-    uint32_t neg[kP];
+    i8_cut_emit<V>(a, sc[lane], r, c0, dig, ldk, plane);
+}
+
+// The cut with the rows' maxima of |a| given (accumulated by the operand's
+// producer, or by k_i8_rowmax): no exchange between blocks.  Block (x, y):
+// rows 32 x .. 32 x + 31 (lane = row), columns 8 V y + V w .. (warp w), the
+// layout of the cluster form.  Column group 0 stores the row scales and, for
+// the next producer, clears its maxima (clear, may be null).
+template <int V>
+__global__ void __launch_bounds__(256)
+    k_i8_cut_rows(const double *__restrict__ src, long lds, int R, int K, int8_t *dig, long ldk, long plane,
+                  double *rowscale, const double *__restrict__ rmax, double *clear) {
+    FB_GRID_WAIT();
+    constexpr int kP = V / 4;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r = blockIdx.x * 32 + lane;
+    const int c0 = blockIdx.y * 8 * V + V * w;
+    double a[kP][4];
 #pragma unroll
-    for (int p = 0; p < kP; ++p) {
-        neg[p] = 0;
+    for (int p = 0; p < kP; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const long long v = __double2ll_rz((a[p][q] * s) * 72057594037927936.0);   // 2^56
-            u[p][q] = static_cast<unsigned long long>(v < 0 ? -v : v);
-            neg[p] |= (v < 0 ? 0xFFu : 0u) << (8 * q);
+            const int k = c0 + 4 * p + q;   // each load coalesced over the warp's 32 rows
+            a[p][q] = (r < R && k < K) ? src[static_cast<size_t>(k) * lds + r] : 0.0;
         }
+    const double mm = (r < R) ? rmax[r] : 0.0;
+    int e = 0;
+    if (mm > 0.0) frexp(mm, &e);   // mm < 2^e
+    if (blockIdx.y == 0 && w == 0 && r < R) {
+        rowscale[r] = ldexp(1.0, e);
+        if (clear) clear[r] = 0.0;
     }
-    static_assert(kI8S == 8, "2^56 = 128^kI8S");
-    // each slice's V digits of row r are V consecutive bytes: the thread
-    // stores them itself (a whole 32-byte sector between neighbouring warps),
-    // no shared-memory transpose; rows up to rows_pad get digits (zero past R)
-    const bool live = c0 < ldk;   // ldk is a multiple of 128, so a run is inside or wholly past it
-    int8_t *out = dig + static_cast<size_t>(r) * ldk + c0;
-    constexpr int kUnroll = (V <= 32) ? kI8S : 1;   // constant shifts where registers allow
-#pragma unroll kUnroll
-    for (int i = 0; i < kI8S; ++i) {
-        const int sh = 7 * (kI8S - 1 - i);
-        uint32_t word[kP];
-#pragma unroll
-        for (int p = 0; p < kP; ++p) {
-            uint32_t mag = 0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) mag |= static_cast<uint32_t>((u[p][q] >> sh) & 127u) << (8 * q);
-            // the negative values' bytes negated (bytewise, no carries between bytes)
-            const uint32_t mk = neg[p];
-            word[p] = (mag & ~mk) | (__vsub4(0u, mag) & mk);
-        }
-        if (live) {
-            int8_t *o = out + static_cast<size_t>(i) * plane;
-#pragma unroll
-            for (int v4 = 0; v4 < V / 16; ++v4)
-                reinterpret_cast<uint4 *>(o)[v4] =
-                    make_uint4(word[4 * v4], word[4 * v4 + 1], word[4 * v4 + 2], word[4 * v4 + 3]);
-        }
+    i8_cut_emit<V>(a, ldexp(1.0, -e), r, c0, dig, ldk, plane);
+}
+
+// rmax[r] = max(rmax[r], max_k |src[k lds + r]|) for rows r < R, columns k < K
+// (NaN dropped, as fmax does); blocks of 32 rows x 8 column strides
+__global__ void __launch_bounds__(256) k_i8_rowmax(const double *__restrict__ src, long lds, int R, int K,
+                                                   double *rmax) {
+    __shared__ double part[8][32];
+    FB_GRID_WAIT();
+    const int r = blockIdx.x * 32 + threadIdx.x;
+    double m = 0.0;
+    if (r < R)
+        for (int k = blockIdx.y * 8 + threadIdx.y; k < K; k += gridDim.y * 8)
+            m = fmax(m, fabs(src[static_cast<size_t>(k) * lds + r]));
+    part[threadIdx.y][threadIdx.x] = m;
+    __syncthreads();
+    if (threadIdx.y == 0 && r < R) {
+        for (int q = 1; q < 8; ++q) m = fmax(m, part[q][threadIdx.x]);
+        atomic_max_nonneg(rmax + r, m);
     }
 }
 
@@ -1226,6 +1286,28 @@ void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p,
 #undef FB_CUT_CASE
     default: pdl(k_i8_cut<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale); break;
     }
+}
+
+void launch_i8_cut_rows(const double *src, long lds, int R, int K, const I8Plan &p, const double *rmax,
+                        double *clear, cudaStream_t st) {
+    const dim3 grid(p.rows_pad / 32, kCutCl);
+    const long plane = p.ldk * static_cast<long>(p.rows_pad);
+    switch (cut_values(p.ldk)) {
+#define FB_CUT_CASE(V)                                                                                           \
+    case V:                                                                                                      \
+        pdl(k_i8_cut_rows<V>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale, rmax, clear); \
+        break;
+        FB_CUT_CASE(16) FB_CUT_CASE(32)
+#undef FB_CUT_CASE
+    default:
+        pdl(k_i8_cut_rows<64>, grid, dim3(256), 0, st, src, lds, R, K, p.dig, p.ldk, plane, p.scale, rmax, clear);
+        break;
+    }
+}
+
+void launch_i8_rowmax(const double *src, long lds, int R, int K, double *rmax, cudaStream_t st) {
+    const dim3 grid((R + 31) / 32, std::max(1, std::min((K + 7) / 8, 16)));
+    pdl(k_i8_rowmax, grid, dim3(32, 8), 0, st, src, lds, R, K, rmax);
 }
 
 // the tile width is the B operand's box height (i8_plan)

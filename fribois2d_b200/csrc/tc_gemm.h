@@ -103,6 +103,12 @@ int i8_configure();
 int i8_plan(I8Plan &p, int rows, int K, int box_rows);
 // digits of the column-major source A(r, k) = src[k * lds + r], r < R, k < K
 void launch_i8_split(const double *src, long lds, int R, int K, const I8Plan &p, cudaStream_t st);
+// the cut with the rows' maxima of |src| given in rmax (R entries); clear
+// (R entries, may be null) is zeroed for the next producer's maxima
+void launch_i8_cut_rows(const double *src, long lds, int R, int K, const I8Plan &p, const double *rmax,
+                        double *clear, cudaStream_t st);
+// rmax[r] = max(rmax[r], max_k |src(r, k)|); rmax must start at zero
+void launch_i8_rowmax(const double *src, long lds, int R, int K, double *rmax, cudaStream_t st);
 // out[c * ldo + r] = sum_k A(r, k) B(c, k)
 // b_const: b's planes and scales were written before the previous kernel in
 // the stream started (the constant eigenvector operand), so its first copies

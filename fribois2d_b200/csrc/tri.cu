@@ -413,30 +413,10 @@ __global__ void __launch_bounds__(kYLines * W * 32) k_ylines(Dev d, ScanSys s2, 
 // them, scale by g(i), and do the same backward with
 // e(i) = -apphj(i+1) g(i); only warp-level synchronisation inside the
 // solve.  nw warps (modes) per block, as many as the shared memory holds.
-__device__ __forceinline__ void ymodes_body(const Dev &d, int nw) {
-    extern __shared__ double sm[];
-    const int n = d.n2m, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double *am = sm, *ap = sm + (n + 2);                       // 1-based off-diagonals
-    double *line = sm + 2 * (n + 2) + static_cast<size_t>(w) * 2 * (n + 1);
-    double *piv = line + (n + 1);
-    // every copy of the block in flight at once (cp.async), one wait
-    for (int i = threadIdx.x; i <= n + 1; i += blockDim.x) {
-        cp8(am + i, d.amphj + i);
-        cp8(ap + i, d.apphj + i);
-    }
-    const int r = blockIdx.x * nw + w;
-    const bool live = (w < nw) && (r < d.n3m);
-    double *row = live ? d.hmn + static_cast<size_t>(r) * d.ldh : nullptr;
-    if (live) {
-        const double *pgr = d.pg + static_cast<size_t>(r) * d.ldh;
-        for (int i = lane; i < n; i += 32) {
-            cp8(line + i, row + i);
-            cp8(piv + i, pgr + i);
-        }
-    }
-    cp_wait();
-    __syncthreads();   // the off-diagonals (and every line) are staged
-    if (!live) return;
+// one warp's mode: the forward and backward recurrences of the staged line
+// (in place), then the line stored to its row of hmn
+__device__ __forceinline__ void ymodes_solve(int n, int lane, const double *am, const double *ap, double *line,
+                                             const double *piv, double *row) {
     const int m = ((n + 31) / 32) | 1;
     const int i0 = min(lane * m, n), cnt = min(m, n - i0);
     // forward: composite of the chunk, y_out = A y_in + C
@@ -492,9 +472,47 @@ __device__ __forceinline__ void ymodes_body(const Dev &d, int nw) {
     for (int i = lane; i < n; i += 32) row[i] = line[i];
 }
 
-__global__ void __launch_bounds__(256) k_ymodes(Dev d, int nw) {
+// rmax (may be null): the maxima of |hmn| over each row j (over the modes:
+// the rows of the INT8 transform's data operand) are accumulated into rmax[j]
+// from the block's modes, for the digit cut that follows
+__device__ __forceinline__ void ymodes_body(const Dev &d, int nw, double *rmax = nullptr) {
+    extern __shared__ double sm[];
+    const int n = d.n2m, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *am = sm, *ap = sm + (n + 2);                       // 1-based off-diagonals
+    double *line = sm + 2 * (n + 2) + static_cast<size_t>(w) * 2 * (n + 1);
+    double *piv = line + (n + 1);
+    // every copy of the block in flight at once (cp.async), one wait
+    for (int i = threadIdx.x; i <= n + 1; i += blockDim.x) {
+        cp8(am + i, d.amphj + i);
+        cp8(ap + i, d.apphj + i);
+    }
+    const int r = blockIdx.x * nw + w;
+    const bool live = (w < nw) && (r < d.n3m);
+    double *row = live ? d.hmn + static_cast<size_t>(r) * d.ldh : nullptr;
+    if (live) {
+        const double *pgr = d.pg + static_cast<size_t>(r) * d.ldh;
+        for (int i = lane; i < n; i += 32) {
+            cp8(line + i, row + i);
+            cp8(piv + i, pgr + i);
+        }
+    }
+    cp_wait();
+    __syncthreads();   // the off-diagonals (and every line) are staged
+    if (live) ymodes_solve(n, lane, am, ap, line, piv, row);
+    if (!rmax) return;
+    __syncthreads();   // every live warp's solved line is in shared memory
+    const int nlive = max(0, min(nw, d.n3m - blockIdx.x * nw));
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double mx = 0.0;
+        for (int q = 0; q < nlive; ++q)
+            mx = fmax(mx, fabs(sm[2 * (n + 2) + static_cast<size_t>(q) * 2 * (n + 1) + j]));
+        if (mx > 0.0) atomic_max_nonneg(rmax + j, mx);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_ymodes(Dev d, int nw, double *rmax) {
     FB_GRID_WAIT();
-    ymodes_body(d, nw);
+    ymodes_body(d, nw, rmax);
 }
 
 __global__ void __launch_bounds__(256) kg_ymodes(const GroupCase *__restrict__ g, int nw) {
@@ -988,10 +1006,10 @@ int ymodes_shape(const Dev &d, size_t *smem) {
 }
 }  // namespace
 
-void launch_scan_poisson(const Dev &d, cudaStream_t st) {
+void launch_scan_poisson(const Dev &d, cudaStream_t st, double *rmax) {
     size_t smem = 0;
     const int nw = ymodes_shape(d, &smem);
-    pdl(k_ymodes, dim3((d.n3m + nw - 1) / nw), dim3(32 * nw), smem, st, d, nw);
+    pdl(k_ymodes, dim3((d.n3m + nw - 1) / nw), dim3(32 * nw), smem, st, d, nw, rmax);
 }
 
 template <int TK>

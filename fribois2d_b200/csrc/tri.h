@@ -17,7 +17,9 @@ constexpr int kWinMax = 24;  // longest truncation window of the windowed helsol
 cudaError_t scan_configure();
 void launch_win_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
 void launch_scan_helsolve(const Dev &d, const SubDev &s, cudaStream_t st);
-void launch_scan_poisson(const Dev &d, cudaStream_t st);
+// rmax (may be null): n2m row maxima of |hmn| (over the modes) accumulated for
+// the INT8 digit cut
+void launch_scan_poisson(const Dev &d, cudaStream_t st, double *rmax = nullptr);
 void glaunch_win_helsolve(const Group &g, int n, cudaStream_t st);  // substep n (0-based)
 void glaunch_scan_poisson(const Group &g, cudaStream_t st);
 
