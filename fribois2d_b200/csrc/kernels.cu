@@ -61,6 +61,35 @@ __device__ double block_reduce_fast(double v, double *sh) {
     return r;
 }
 
+// block_reduce_fast<false> of N values at once (the same shuffle tree for
+// each, so the same sums), three barriers in all; sh holds 32 N doubles
+template <int N>
+__device__ void block_sum_n(double (&v)[N], double *sh) {
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = warp_reduce<false>(v[i]);
+    if ((t & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < N; ++i) sh[32 * i + (t >> 5)] = v[i];
+    __syncthreads();
+    if (t < 32) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double r = (t < nw) ? sh[32 * i + t] : 0.0;
+            r = warp_reduce<false>(r);
+            v[i] = r;
+        }
+    }
+    if (t == 0)   // (lane 0 read slot 32 i itself before; the other lanes read other slots)
+#pragma unroll
+        for (int i = 0; i < N; ++i) sh[32 * i] = v[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = sh[32 * i];
+    __syncthreads();
+}
+
 // ------------------------------------------------------------ cfl
 
 // cfl.F90 (fluid_tsch.F90:211-258) and the fixed-dt check fluid_tsch.F90:49-55.
@@ -1803,89 +1832,125 @@ __device__ void modfn(double K[6], const double t[6], const double FF[6], const 
 // RK4 update they give into rigid[9..17] only; RIGID_COMMIT is RIGID_STEP
 // with the load fin (markers restored to the start of the step first).
 __device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode, const double *fin) {
-    __shared__ double sh[32];
+    __shared__ double sh[32 * 5];
     __shared__ double cm[18];
     __shared__ double rot[4];
+    __shared__ double xns[6];
+    __shared__ double rs[18], kin[9];   // the body state and the prescribed kinematics, read once
+    __shared__ int mcon[3];
     const int tid = threadIdx.x, nt = blockDim.x, nlm = d.nlm;
     double *R = d.rigid;
     const bool from_loads = (mode == RIGID_STEP || mode == RIGID_FORCES);
+    if (tid < 18) rs[tid] = R[tid];
+    else if (tid >= 32 && tid < 41) kin[tid - 32] = d.kinori[tid - 32];
+    else if (tid >= 64 && tid < 67) mcon[tid - 64] = d.rbmcon[tid - 64];
+    if (!from_loads) __syncthreads();   // (otherwise the block sums' barriers order them)
     double fyp = 0.0, fzp = 0.0, fyv = 0.0, fzv = 0.0, mom = 0.0;
     if (from_loads) {
         const double c0 = (mode == RIGID_FORCES) ? R[9] : R[0], c1 = (mode == RIGID_FORCES) ? R[10] : R[1];
+        double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};   // fyp, fzp, fyv, fzv, mom
         for (int i = tid; i < nlm; i += nt) {
             const double p = d.press[i], A = d.lmA[i];
             const double Fp1 = -p * d.lmnor[2 * i] * A, Fp2 = -p * d.lmnor[2 * i + 1] * A;
             const double Fv1 = d.tau[2 * i] * A, Fv2 = d.tau[2 * i + 1] * A;
-            fyp = fyp + Fp1;
-            fzp = fzp + Fp2;
-            fyv = fyv + Fv1;
-            fzv = fzv + Fv2;
+            f[0] = f[0] + Fp1;
+            f[1] = f[1] + Fp2;
+            f[2] = f[2] + Fv1;
+            f[3] = f[3] + Fv2;
             const double r1 = d.lmcc[2 * i] - c0, r2 = d.lmcc[2 * i + 1] - c1;
-            mom = mom + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
+            f[4] = f[4] + (r1 * (Fp2 + Fv2) - r2 * (Fp1 + Fv1));
         }
-        fyp = block_reduce_fast<false>(fyp, sh);
-        fzp = block_reduce_fast<false>(fzp, sh);
-        fyv = block_reduce_fast<false>(fyv, sh);
-        fzv = block_reduce_fast<false>(fzv, sh);
-        mom = block_reduce_fast<false>(mom, sh);
+        block_sum_n<5>(f, sh);   // the five block sums (the same trees as one at a time)
+        fyp = f[0];
+        fzp = f[1];
+        fyv = f[2];
+        fzv = f[3];
+        mom = f[4];
     }
+    // the loads of the step (every thread forms the same values)
+    const double time = d.scal[S_TIME], dt = d.dt;
+    double Fy, Fz, M;
+    if (from_loads) {
+        const double fy = fyp + fyv, fz = fzp + fzv;
+        const double g0 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF0;
+        const double g1 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF1;
+        Fy = fy + g0;
+        Fz = fz + g1;
+        M = mom;
+    } else {
+        Fy = fin[0];
+        Fz = fin[1];
+        M = fin[2];
+    }
+    if (tid == 0 && from_loads) {
+        d.forces[0] = time;
+        d.forces[1] = Fy;
+        d.forces[2] = Fz;
+        d.forces[3] = M;
+        d.forces[4] = fyp;
+        d.forces[5] = fzp;
+        d.forces[6] = fyv;
+        d.forces[7] = fzv;
+    }
+    // explicit RK4 with loads frozen over the stages: the three degrees of
+    // freedom (y, z, rotation) are independent (modfn), one thread each
+    if (tid < 3) {
+        const int i = tid;
+        const double csp = (i == 0) ? d.cmposi0 : (i == 1 ? d.cmposi1 : d.cmroti);
+        double FFi, Mii;
+        if (i == 0) {
+            if (d.rtcoup) {
+                FFi = Fy + M / d.rrr;
+                Mii = 1.0 / ((d.rba1 / (d.rrr * d.rrr) + d.rba0) * d.rbden);
+            } else {
+                FFi = Fy;
+                Mii = 1.0 / (d.rba0 * d.rbden);
+            }
+        } else if (i == 1) {
+            FFi = Fz;
+            Mii = 1.0 / (d.rba0 * d.rbden);
+        } else {
+            FFi = M;
+            Mii = 1.0 / (d.rba1 * d.rbden);
+        }
+        const double kk = d.kk[i], cc = d.cc[i], kk3 = d.kk3[i];
+        // modfn (rigid.F90) for component i: K_x = v, K_v = Mi (-kk x + -cc v + -kk3 x^3 + F)
+        auto mod = [&](double x, double v, double &kx, double &kv) {
+            const double cube = x * x * x;
+            const double lin = -kk * x + -cc * v;
+            const double rhs = lin + -kk3 * cube + FFi;
+            kx = v;
+            kv = Mii * rhs;
+        };
+        const double xo = rs[i] - csp, vo = rs[3 + i];
+        double k1x, k1v, k2x, k2v, k3x, k3v, k4x, k4v;
+        mod(xo, vo, k1x, k1v);
+        mod(xo + k1x * dt / 2.0, vo + k1v * dt / 2.0, k2x, k2v);
+        mod(xo + k2x * dt / 2.0, vo + k2v * dt / 2.0, k3x, k3v);
+        mod(xo + k3x * dt, vo + k3v * dt, k4x, k4v);
+        xns[i] = xo + dt * (k1x / 6.0 + k2x / 3.0 + k3x / 3.0 + k4x / 6.0);
+        xns[3 + i] = vo + dt * (k1v / 6.0 + k2v / 3.0 + k3v / 3.0 + k4v / 6.0);
+    }
+    __syncthreads();
     if (tid == 0) {
-        const double time = d.scal[S_TIME], dt = d.dt;
-        double Fy, Fz, M;
-        if (from_loads) {
-            const double fy = fyp + fyv, fz = fzp + fzv;
-            const double g0 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF0;
-            const double g1 = (1.0 - 1.0 / d.rbden) * d.rba0 * d.rbgravF1;
-            Fy = fy + g0;
-            Fz = fz + g1;
-            M = mom;
-            d.forces[0] = time;
-            d.forces[1] = Fy;
-            d.forces[2] = Fz;
-            d.forces[3] = M;
-            d.forces[4] = fyp;
-            d.forces[5] = fzp;
-            d.forces[6] = fyv;
-            d.forces[7] = fzv;
-        } else {
-            Fy = fin[0];
-            Fz = fin[1];
-            M = fin[2];
-        }
-        // explicit RK4 with loads frozen over the stages
         const double csp[3] = {d.cmposi0, d.cmposi1, d.cmroti};
-        double xo[6], FF[6] = {0.0, 0.0, 0.0, 0.0, Fz, M}, Mi[3];
-        for (int i = 0; i < 3; ++i) xo[i] = R[i] - csp[i];
-        for (int i = 0; i < 3; ++i) xo[i + 3] = R[3 + i];
-        if (d.rtcoup) {
-            FF[3] = Fy + M / d.rrr;
-            Mi[0] = 1.0 / ((d.rba1 / (d.rrr * d.rrr) + d.rba0) * d.rbden);
-        } else {
-            FF[3] = Fy;
-            Mi[0] = 1.0 / (d.rba0 * d.rbden);
-        }
-        Mi[1] = 1.0 / (d.rba0 * d.rbden);
-        Mi[2] = 1.0 / (d.rba1 * d.rbden);
-        double K1[6], K2[6], K3[6], K4[6], t1[6], xn[6];
-        modfn(K1, xo, FF, Mi, d);
-        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K1[i] * dt / 2.0;
-        modfn(K2, t1, FF, Mi, d);
-        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K2[i] * dt / 2.0;
-        modfn(K3, t1, FF, Mi, d);
-        for (int i = 0; i < 6; ++i) t1[i] = xo[i] + K3[i] * dt;
-        modfn(K4, t1, FF, Mi, d);
-        for (int i = 0; i < 6; ++i) xn[i] = xo[i] + dt * (K1[i] / 6.0 + K2[i] / 3.0 + K3[i] / 3.0 + K4[i] / 6.0);
-        double *P1 = R + 9, *V1 = R + 12, *A1 = R + 15;
+        double xn[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) xn[i] = xns[i];
+        // P1, V1, A1 (rigid[9..17]) formed in shared memory (cm), then stored
+        for (int i = 0; i < 18; ++i) cm[i] = rs[i];
+        double *P1 = cm + 9, *V1 = cm + 12, *A1 = cm + 15;
         if (!d.rtcoup) {
+#pragma unroll
             for (int i = 0; i < 3; ++i) {
                 P1[i] = csp[i] + xn[i];
                 V1[i] = xn[3 + i];
-                A1[i] = (V1[i] - R[3 + i]) / dt;
+                A1[i] = (V1[i] - rs[3 + i]) / dt;
             }
         } else {
             P1[0] = csp[0] + xn[0];
             V1[0] = xn[3];
-            A1[0] = (V1[0] - R[3]) / dt;
+            A1[0] = (V1[0] - rs[3]) / dt;
             P1[1] = csp[1];
             V1[1] = 0.0;
             A1[1] = 0.0;
@@ -1893,70 +1958,118 @@ __device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode
             V1[2] = V1[0] / d.rrr;
             A1[2] = A1[2] / d.rrr;  // as rigid.F90:296 (incoming value / rr)
         }
+#pragma unroll
         for (int i = 0; i < 3; ++i)
-            if (d.rbmcon[i] == 1) {
-                P1[i] = d.kinori[i];
-                V1[i] = d.kinori[3 + i];
-                A1[i] = d.kinori[6 + i];
+            if (mcon[i] == 1) {
+                P1[i] = kin[i];
+                V1[i] = kin[3 + i];
+                A1[i] = kin[6 + i];
             }
-        const double cmrot = P1[2] - R[2];
+        const double cmrot = P1[2] - rs[2];
         rot[0] = cos(cmrot);
         rot[1] = -sin(cmrot);
         rot[2] = sin(cmrot);
         rot[3] = cos(cmrot);
-        for (int i = 0; i < 18; ++i) cm[i] = R[i];
+        for (int i = 9; i < 18; ++i) R[i] = cm[i];
     }
     __syncthreads();
     if (mode == RIGID_FORCES) return;   // the update the loads give, markers untouched
+    // Each loop reads all of a thread's kRgU entries before it stores any: the
+    // stores could alias the next loads, so a load after a store would wait
+    // for the store's round trip.
+    constexpr int kRgU = 4;
     const double *P0 = cm, *P1 = cm + 9, *V1 = cm + 12, *A1 = cm + 15;
-    for (int i = tid; i < nlm; i += nt) {
-        const double rho0 = d.lmcc[2 * i] - P0[0], rho1 = d.lmcc[2 * i + 1] - P0[1];
-        const double c10 = -V1[2] * rho1, c11 = V1[2] * rho0;
-        const double c20 = -A1[2] * rho1, c21 = A1[2] * rho0;
-        const double c30 = -V1[2] * c11, c31 = V1[2] * c10;
-        d.lmcc[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
-        d.lmcc[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
-        d.lmvel[2 * i] = V1[0] + c10;
-        d.lmvel[2 * i + 1] = V1[1] + c11;
-        d.lmacc[2 * i] = A1[0] + c20 + c30;
-        d.lmacc[2 * i + 1] = A1[1] + c21 + c31;
+    for (int i0 = tid; i0 < nlm; i0 += kRgU * nt) {
+        double y[kRgU], z[kRgU];
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = min(i0 + u * nt, nlm - 1);
+            y[u] = d.lmcc[2 * i];
+            z[u] = d.lmcc[2 * i + 1];
+        }
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = i0 + u * nt;
+            if (i >= nlm) break;
+            const double rho0 = y[u] - P0[0], rho1 = z[u] - P0[1];
+            const double c10 = -V1[2] * rho1, c11 = V1[2] * rho0;
+            const double c20 = -A1[2] * rho1, c21 = A1[2] * rho0;
+            const double c30 = -V1[2] * c11, c31 = V1[2] * c10;
+            d.lmcc[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
+            d.lmcc[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
+            d.lmvel[2 * i] = V1[0] + c10;
+            d.lmvel[2 * i + 1] = V1[1] + c11;
+            d.lmacc[2 * i] = A1[0] + c20 + c30;
+            d.lmacc[2 * i + 1] = A1[1] + c21 + c31;
+        }
     }
     // vertices rotate about the updated centre (rigid.F90:110-121)
-    for (int i = tid; i <= nlm; i += nt) {
-        const double rho0 = d.vert[2 * i] - P1[0], rho1 = d.vert[2 * i + 1] - P1[1];
-        d.vert[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
-        d.vert[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
+    for (int i0 = tid; i0 <= nlm; i0 += kRgU * nt) {
+        double y[kRgU], z[kRgU];
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = min(i0 + u * nt, nlm);
+            y[u] = d.vert[2 * i];
+            z[u] = d.vert[2 * i + 1];
+        }
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = i0 + u * nt;
+            if (i > nlm) break;
+            const double rho0 = y[u] - P1[0], rho1 = z[u] - P1[1];
+            d.vert[2 * i] = P1[0] + (rot[0] * rho0 + rot[1] * rho1);
+            d.vert[2 * i + 1] = P1[1] + (rot[2] * rho0 + rot[3] * rho1);
+        }
     }
     __syncthreads();
-    for (int i = tid; i < nlm; i += nt) {
-        const double *a = d.vert + 2 * i, *b = d.vert + 2 * i + 2;
-        const double v1[3] = {0.0 - 0.0, b[0] - a[0], b[1] - a[1]};
-        const double v2[3] = {-1.0 - 0.0, (a[0] + b[0]) * 0.5 - a[0], (a[1] + b[1]) * 0.5 - a[1]};
-        const double c0 = v1[1] * v2[2] - v1[2] * v2[1];
-        const double c1 = v1[2] * v2[0] - v1[0] * v2[2];
-        const double c2 = v1[0] * v2[1] - v1[1] * v2[0];
-        const double den = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
-        d.lmnor[2 * i] = c1 / den;
-        d.lmnor[2 * i + 1] = c2 / den;
+    for (int i0 = tid; i0 < nlm; i0 += kRgU * nt) {
+        double va[kRgU][4];   // vertices i and i + 1
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = min(i0 + u * nt, nlm - 1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) va[u][q] = d.vert[2 * i + q];
+        }
+#pragma unroll
+        for (int u = 0; u < kRgU; ++u) {
+            const int i = i0 + u * nt;
+            if (i >= nlm) break;
+            const double *a = va[u], *b = va[u] + 2;
+            const double v1[3] = {0.0 - 0.0, b[0] - a[0], b[1] - a[1]};
+            const double v2[3] = {-1.0 - 0.0, (a[0] + b[0]) * 0.5 - a[0], (a[1] + b[1]) * 0.5 - a[1]};
+            const double c0 = v1[1] * v2[2] - v1[2] * v2[1];
+            const double c1 = v1[2] * v2[0] - v1[0] * v2[2];
+            const double c2 = v1[0] * v2[1] - v1[1] * v2[0];
+            const double den = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+            d.lmnor[2 * i] = c1 / den;
+            d.lmnor[2 * i + 1] = c2 / den;
+        }
     }
     if (mode == RIGID_PLACE) return;     // markers at the trial state; nothing committed
     if (tid == 0) {
+        // every value read before the first store (see above)
+        const double t0 = d.scal[S_TIME], stepd = d.scal[S_STEP];
+        const double nbcv = d.scal[S_NBCV], nbcw = d.scal[S_NBCW], cflm = d.scal[S_CFLM];
+        double fv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) fv[i] = d.forces[i];
+        const double solves = (mode == RIGID_COMMIT) ? fin[3] : 1.0;   // fluid solves this step
         for (int i = 0; i < 9; ++i) R[i] = cm[9 + i];
-        const double t0 = d.scal[S_TIME];
         const double t1 = t0 + d.dt;
         d.scal[S_TIME] = t1;
-        const int row = static_cast<int>(d.scal[S_STEP]);
+        const int row = static_cast<int>(stepd);
         if (hist_rows > 0) {
             double *h = d.hist + static_cast<size_t>(row % hist_rows) * FB_HIST_COLS;
-            for (int i = 0; i < 8; ++i) h[i] = d.forces[i];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) h[i] = fv[i];
             h[8] = t1;
             for (int i = 0; i < 9; ++i) h[9 + i] = cm[9 + i];
-            h[18] = d.scal[S_NBCV];
-            h[19] = d.scal[S_NBCW];
-            h[20] = d.scal[S_CFLM];
+            h[18] = nbcv;
+            h[19] = nbcw;
+            h[20] = cflm;
             h[21] = d.dt;
             for (int i = 22; i < FB_HIST_COLS; ++i) h[i] = 0.0;  // diagnostics, when enabled
-            h[30] = (mode == RIGID_COMMIT) ? fin[3] : 1.0;        // fluid solves this step
+            h[30] = solves;
         }
         d.scal[S_STEP] = static_cast<double>(row + 1);
     }
