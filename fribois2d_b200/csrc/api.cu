@@ -2914,9 +2914,9 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
             // (148 SMs, one CTA each); ties go to the wider tile (fewer MMA
             // instructions per column).  Timed alone, back-to-back launches
             // overlap one launch's last wave with the next one's first, which
-            // favours narrow two-wave tiles that lose inside the time step
-            // (galloping rectangle: 480 us per step with 48 columns, ~490
-            // with the width such timing picked, 513 with 64).
+            // favours narrow two-wave tiles; inside the time step the next
+            // kernel is another stage (galloping rectangle, the same process:
+            // 480 us per step with 48 columns, 513 with 64).
             const int mt = (d.n2m + 127) / 128;
             double best = 1e30;
             for (int cand : {64, 48, 32}) {
