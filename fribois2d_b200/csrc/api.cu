@@ -44,6 +44,9 @@ struct fb_ctx {
     // stage_ev (recorded after their copies) has completed
     double *stage_h = nullptr;
     cudaEvent_t stage_ev = nullptr;
+    // fb_fluid_tsch / fb_rigid: status and forcecomp row written by the GPU
+    // into mapped host memory (k_publish), read after the stream sync
+    double *mbox_h = nullptr, *mbox_d = nullptr;
     cublasHandle_t blas = nullptr;
     void *blas_ws = nullptr;                  // 32 MB workspace of cuBLAS / cuBLASLt
     // FP64 transforms through cuBLASLt with an algorithm timed per grid size
@@ -1245,6 +1248,7 @@ int fb_destroy(fb_ctx *c) {
     if (c->coef_pin) cudaFreeHost(c->coef_pin);
     if (c->coef_pini) cudaFreeHost(c->coef_pini);
     if (c->stage_h) cudaFreeHost(c->stage_h);
+    if (c->mbox_h) cudaFreeHost(c->mbox_h);
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->blas) cublasDestroy(c->blas);
     for (cublasLtMatrixLayout_t l : c->lt_l)
@@ -1261,15 +1265,34 @@ int fb_destroy(fb_ctx *c) {
     return FB_OK;
 }
 
+// the mapped host words of k_publish (allocated once, outside any capture)
+int mbox_ready(fb_ctx *c) {
+    if (c->mbox_h) return FB_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaHostAlloc(&c->mbox_h, 16 * sizeof(double), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->mbox_d), c->mbox_h, 0));
+    return FB_OK;
+}
+
+int mbox_status(const fb_ctx *c) {
+    return static_cast<int>(static_cast<const volatile double *>(c->mbox_h)[0]);
+}
+
 int fb_fluid_tsch(fb_ctx *c, int ns) {
     if (!c) return FB_ERR_STATE;
     int r;
+    if ((r = mbox_ready(c))) return r;
     if (!c->vardt && ns >= 1) {
         // fixed dt after the first step: the same launches every step,
-        // replayed from a graph captured at the first such call
+        // replayed from a graph captured at the first such call (with the
+        // status published at its end)
         if (!c->fgraph_exec) {
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             r = enqueue_fluid(c, ns);
+            if (!r) {
+                fb::launch_publish(c->d, false, c->mbox_d, c->stream);
+                c->own_launches += 1;
+            }
             cudaGraph_t g = nullptr;
             const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
             if (r || e != cudaSuccess) {
@@ -1280,24 +1303,29 @@ int fb_fluid_tsch(fb_ctx *c, int ns) {
             CK(cudaGraphInstantiate(&c->fgraph_exec, g, 0));
         }
         CK(cudaGraphLaunch(c->fgraph_exec, c->stream));
-    } else if ((r = enqueue_fluid(c, ns))) {
-        return r;
+    } else {
+        if ((r = enqueue_fluid(c, ns))) return r;
+        fb::launch_publish(c->d, false, c->mbox_d, c->stream);
+        c->own_launches += 1;
     }
-    int status = 0;
-    if ((r = read_status(c, &status))) return r;
-    return status;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return mbox_status(c);
 }
 
 int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
     if (!c) return FB_ERR_STATE;
-    int r = stage_impl(c, FB_ST_RIGID, ns, 1);
-    if (r) return r;
+    int r;
+    if ((r = mbox_ready(c))) return r;
+    if ((r = stage_impl(c, FB_ST_RIGID, ns, 1))) return r;
     if ((r = enqueue_report(c))) return r;
-    if (forcecomp) CK(cudaMemcpyAsync(forcecomp, c->d.forces, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    int status = 0;
-    if ((r = read_status(c, &status))) return r;
+    fb::launch_publish(c->d, true, c->mbox_d, c->stream);   // status and the forcecomp row
+    c->own_launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    if (forcecomp) std::memcpy(forcecomp, c->mbox_h + 1, 8 * sizeof(double));
     host_clock(c, 1);
-    return status;
+    return mbox_status(c);
 }
 
 int fb_last_history(fb_ctx *c, double *row);

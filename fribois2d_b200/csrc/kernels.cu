@@ -2377,6 +2377,22 @@ void launch_loads(const Dev &d, cudaStream_t s) {
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s) {
     pdl(k_diag, dim3(std::min(stride_blocks(d), 2048)), dim3(256), 0, s, d, hist_rows);
 }
+// The end of a synchronous API call: the status word (and the forcecomp
+// row) written by the GPU into mapped host memory, so that the host reads them
+// after its stream synchronisation without a device-to-host copy
+__global__ void k_publish(const int *status, const double *forces, double *mbox) {
+    FB_GRID_WAIT();
+    volatile double *m = mbox;
+    m[0] = static_cast<double>(*status);
+    if (forces)
+        for (int i = 0; i < 8; ++i) m[1 + i] = forces[i];
+    __threadfence_system();
+}
+void launch_publish(const Dev &d, bool forces, double *mbox, cudaStream_t s) {
+    pdl(k_publish, dim3(1), dim3(1), 0, s, static_cast<const int *>(d.status),
+        forces ? static_cast<const double *>(d.forces) : nullptr, mbox);
+}
+
 void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin) {
     if (d.nlm) pdl(k_rigid, dim3(1), dim3(512), 0, s, d, hist_rows, mode, fin);
 }

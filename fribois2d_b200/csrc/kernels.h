@@ -34,6 +34,9 @@ void launch_helsolve(const Dev &d, const SubDev &sd, cudaStream_t s);
 void launch_divg(const Dev &d, double usdtal, cudaStream_t s, double *rmax = nullptr);
 void launch_updvp_prcalc(const Dev &d, double al, double be, cudaStream_t s, bool pend = false,
                          const NlMaps *maps = nullptr);
+// mbox[0] = *d.status, mbox[1..8] = d.forces[0..7] (when forces); mbox in
+// mapped host memory
+void launch_publish(const Dev &d, bool forces, double *mbox, cudaStream_t s);
 void launch_submean_boucqt(const Dev &d, cudaStream_t s, bool deferred = false);
 void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream_t s);  // boucqt + next boucdq
 void launch_loads(const Dev &d, cudaStream_t s);
