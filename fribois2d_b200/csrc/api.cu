@@ -1266,7 +1266,7 @@ int fb_destroy(fb_ctx *c) {
 }
 
 // the mapped host words of k_publish (allocated once, outside any capture)
-int mbox_ready(fb_ctx *c) {
+static int mbox_ready(fb_ctx *c) {
     if (c->mbox_h) return FB_OK;
     CK(cudaSetDevice(c->device));
     CK(cudaHostAlloc(&c->mbox_h, 16 * sizeof(double), cudaHostAllocMapped));
@@ -1274,7 +1274,7 @@ int mbox_ready(fb_ctx *c) {
     return FB_OK;
 }
 
-int mbox_status(const fb_ctx *c) {
+static int mbox_status(const fb_ctx *c) {
     return static_cast<int>(static_cast<const volatile double *>(c->mbox_h)[0]);
 }
 
