@@ -183,21 +183,24 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ CPU arm
 
-def cpu_run(case_name, seconds, max_steps):
+def cpu_run(case_name, seconds, max_steps, warmup=1):
     """The oracle (a C restatement of the reference's CPU path) on the host
-    cores with all threads; returns (cell-steps/s, steps timed, threads)."""
+    cores with all threads, after `warmup` untimed steps (the first touches
+    every array); returns (cell-steps/s, steps timed, threads, seconds)."""
     import oracle
     c = make_case(case_name)
     path = write_deck(c, 99)
     threads = os.cpu_count() or 1
     o = oracle.Oracle(oracle.parse_deck(path), threads=threads)
     o.add_v_perturbation(c.v_perturbation())
-    st = o.step(0)  # warm-up step (first touch of every array)
-    if st:
-        raise RuntimeError(f"oracle status {st}")
+    for w in range(max(1, warmup)):
+        st = o.step(w)
+        if st:
+            raise RuntimeError(f"oracle status {st}")
+    w0 = max(1, warmup)
     steps, t0 = 0, time.perf_counter()
     while steps < max_steps:
-        if o.step(steps + 1):
+        if o.step(w0 + steps):
             raise RuntimeError("oracle failed")
         steps += 1
         if time.perf_counter() - t0 > seconds:
@@ -212,15 +215,16 @@ def reference_arm(args, rank, world):
     try:
         import oracle
         oracle.build()
+        W = max(3, args.warmup)
         value, steps, threads, secs = cpu_run(args.config, seconds=max(30.0, 3.0 * args.cpu_seconds),
-                                              max_steps=max(1, args.steps))
+                                              max_steps=max(1, args.steps), warmup=W)
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle failed: {e}"}))
         return
     c = make_case(args.config)
     line = {
         "impl": "reference", "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+        "steps": steps, "warmup": W, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": c.name, "cells": c.cells, "markers": c.nlm, "host": "cpu"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
