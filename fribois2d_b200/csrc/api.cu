@@ -47,6 +47,7 @@ struct fb_ctx {
     // fb_fluid_tsch / fb_rigid: status and forcecomp row written by the GPU
     // into mapped host memory (k_publish), read after the stream sync
     double *mbox_h = nullptr, *mbox_d = nullptr;
+    double *rigid_mbox = nullptr;   // set by fb_rigid around its rigid stage: k_rigid publishes itself
     cublasHandle_t blas = nullptr;
     void *blas_ws = nullptr;                  // 32 MB workspace of cuBLAS / cuBLASLt
     // FP64 transforms through cuBLASLt with an algorithm timed per grid size
@@ -959,7 +960,7 @@ int stage_impl(fb_ctx *c, int stage, int ns, int n) {
     case FB_ST_PRSUBMEAN: fb::launch_submean_boucqt(d, st); break;
     case FB_ST_CHECKBCS:
     case FB_ST_LOADS: fb::launch_loads(d, st); break;
-    case FB_ST_RIGID: fb::launch_rigid(d, c->hist_cap, st); break;
+    case FB_ST_RIGID: fb::launch_rigid(d, c->hist_cap, st, fb::RIGID_STEP, nullptr, c->rigid_mbox); break;
     case FB_TK_GEMM_FWD: return gemm_fwd(c);
     case FB_TK_POISSON_TRI: fb::launch_scan_poisson(d, st); break;
     case FB_TK_GEMM_BWD: return gemm_bwd(c);
@@ -1317,10 +1318,21 @@ int fb_rigid(fb_ctx *c, int ns, double *forcecomp) {
     if (!c) return FB_ERR_STATE;
     int r;
     if ((r = mbox_ready(c))) return r;
-    if ((r = stage_impl(c, FB_ST_RIGID, ns, 1))) return r;
-    if ((r = enqueue_report(c))) return r;
-    fb::launch_publish(c->d, true, c->mbox_d, c->stream);   // status and the forcecomp row
-    c->own_launches += 1;
+    if (!c->report || !c->d.nlm) {   // k_rigid publishes the status and the forcecomp row itself
+        c->rigid_mbox = c->d.nlm ? c->mbox_d : nullptr;
+        r = stage_impl(c, FB_ST_RIGID, ns, 1);
+        c->rigid_mbox = nullptr;
+        if (r) return r;
+        if (!c->d.nlm) {   // no rigid launch without markers
+            fb::launch_publish(c->d, true, c->mbox_d, c->stream);
+            c->own_launches += 1;
+        }
+    } else {
+        if ((r = stage_impl(c, FB_ST_RIGID, ns, 1))) return r;
+        if ((r = enqueue_report(c))) return r;
+        fb::launch_publish(c->d, true, c->mbox_d, c->stream);   // status and the forcecomp row
+        c->own_launches += 1;
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
     if (forcecomp) std::memcpy(forcecomp, c->mbox_h + 1, 8 * sizeof(double));

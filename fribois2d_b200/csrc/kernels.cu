@@ -1831,7 +1831,8 @@ __device__ void modfn(double K[6], const double t[6], const double FF[6], const 
 // markers at that new state (moment about the new centre) and evaluates the
 // RK4 update they give into rigid[9..17] only; RIGID_COMMIT is RIGID_STEP
 // with the load fin (markers restored to the start of the step first).
-__device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode, const double *fin) {
+__device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode, const double *fin,
+                                           double *mbox = nullptr) {
     __shared__ double sh[32 * 5];
     __shared__ double cm[18];
     __shared__ double rot[4];
@@ -2072,12 +2073,19 @@ __device__ __forceinline__ void rigid_body(const Dev &d, int hist_rows, int mode
             h[30] = solves;
         }
         d.scal[S_STEP] = static_cast<double>(row + 1);
+        if (mbox) {   // the synchronous call's status and forcecomp row, into mapped host memory
+            volatile double *m = mbox;
+            m[0] = static_cast<double>(*d.status);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) m[1 + i] = fv[i];
+            __threadfence_system();
+        }
     }
 }
 
-__global__ void __launch_bounds__(512) k_rigid(Dev d, int hist_rows, int mode, const double *fin) {
+__global__ void __launch_bounds__(512) k_rigid(Dev d, int hist_rows, int mode, const double *fin, double *mbox) {
     FB_GRID_WAIT();
-    rigid_body(d, hist_rows, mode, fin);
+    rigid_body(d, hist_rows, mode, fin, mbox);
 }
 
 // ------------------------------------------------------------ diagnostics
@@ -2393,8 +2401,8 @@ void launch_publish(const Dev &d, bool forces, double *mbox, cudaStream_t s) {
         forces ? static_cast<const double *>(d.forces) : nullptr, mbox);
 }
 
-void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin) {
-    if (d.nlm) pdl(k_rigid, dim3(1), dim3(512), 0, s, d, hist_rows, mode, fin);
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode, const double *fin, double *mbox) {
+    if (d.nlm) pdl(k_rigid, dim3(1), dim3(512), 0, s, d, hist_rows, mode, fin, mbox);
 }
 
 

@@ -42,7 +42,10 @@ void launch_substep_mid(const Dev &d, int slot, double ga, double ro, cudaStream
 void launch_loads(const Dev &d, cudaStream_t s);
 void launch_diag(const Dev &d, int hist_rows, cudaStream_t s);
 enum RigidMode { RIGID_STEP = 0, RIGID_PLACE = 1, RIGID_FORCES = 2, RIGID_COMMIT = 3 };
-void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode = RIGID_STEP, const double *fin = nullptr);
+// mbox (mapped host memory, may be null; RIGID_STEP and RIGID_COMMIT): the status
+// word and the forcecomp row, written at the end as k_publish does
+void launch_rigid(const Dev &d, int hist_rows, cudaStream_t s, int mode = RIGID_STEP, const double *fin = nullptr,
+                  double *mbox = nullptr);
 
 // grouped forms (one launch over a group of cases; substep n 0-based)
 void glaunch_cfl(const Group &g, cudaStream_t s);
