@@ -647,8 +647,12 @@ __global__ void __launch_bounds__(256) kg_poisson_residual(const GroupCase *__re
 // DGEMM; a row whose entries span many decades is reproduced only to
 // 2^-55 of its largest entry.
 
-// The digit cut in one launch: a cluster of kCutCl CTAs per 32 rows, each
-// CTA over its own range of 8 V columns.  Thread (lane, warp w) holds V
+// Two forms of the digit cut.  k_i8_cut_rows (the time step, the public
+// product) takes each row's maximum from an array that the operand's producer
+// (or k_i8_rowmax) accumulated, so its blocks are independent.  k_i8_cut (the
+// eigenvector operands at set-up, the batched launches) finds the maxima
+// itself: a cluster of kCutCl CTAs per 32 rows, each CTA over its own range of
+// 8 V columns.  Thread (lane, warp w) holds V
 // consecutive columns of row lane in registers, all its loads in flight at
 // once (each load coalesced over the 32 rows); the CTA's row maxima go to the
 // cluster through distributed shared memory, so every CTA derives each row's
