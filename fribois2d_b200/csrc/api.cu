@@ -2957,16 +2957,7 @@ int fb_autotune(fb_ctx *c, int32_t choice[2]) {
             // favours narrow two-wave tiles; inside the time step the next
             // kernel is another stage (galloping rectangle, the same process:
             // 480 us per step with 48 columns, 513 with 64).
-            const int mt = (d.n2m + 127) / 128;
-            double best = 1e30;
-            for (int cand : {64, 48, 32}) {
-                const int ctas = mt * ((d.n3m + cand - 1) / cand);
-                const double cost = static_cast<double>((ctas + 147) / 148) * cand;
-                if (cost < best) {
-                    best = cost;
-                    ibn = cand;
-                }
-            }
+            ibn = fb::i8_tile_width(d.n2m, d.n3m);   // C = dph (n2m rows) x eigenvectors (n3m)
             r = i8_tile(ibn);
         }
         if (!r && want_bn && !bn) {

@@ -66,6 +66,25 @@ constexpr int kI8BN = 64;     // output tile width (the default; 48 is the other
 // of at most 127 * 127 per k into an int32 TMEM accumulator, so
 // K * kI8S * 127^2 must stay below 2^31 (K <= 16642); i8_plan rejects more.
 constexpr int kI8MaxK = 16384;
+
+// The INT8 product's tile width for C[rows x cols] (one CTA per 128 x width
+// tile): the width of 64, 48 or 32 that minimises (CTA waves on sms SMs) x
+// width, ties to the wider tile.  A CTA's time grows with its width, so this
+// is the product's time in units of one column of one wave.
+inline int i8_tile_width(int rows, int cols, int sms = 148) {
+    const int mt = (rows + 127) / 128;
+    int best_w = 64;
+    long best = -1;
+    for (int w : {64, 48, 32}) {
+        const long ctas = static_cast<long>(mt) * ((cols + w - 1) / w);
+        const long cost = ((ctas + sms - 1) / sms) * w;
+        if (best < 0 || cost < best) {
+            best = cost;
+            best_w = w;
+        }
+    }
+    return best_w;
+}
 struct I8Plan {
     CUtensorMap map;
     int8_t *dig;
