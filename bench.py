@@ -671,7 +671,7 @@ def device_arm(args, rank, world, local):
 
     # end to end through the C ABI with host buffers (loose FSI coupling as
     # the reference runs it: markers in, fluid step, rigid step, state out)
-    e2e = None
+    e2e = e2e_one_call = None
     if not args.no_e2e:
         nlm = c.nlm
         pin = [torch.empty(2 * nlm, dtype=torch.float64).pin_memory() for _ in range(4)]
@@ -705,6 +705,22 @@ def device_arm(args, rank, world, local):
         e2e = {"value": replica_throughput(world, c.cells, Ke, 1e3 * te_max), "unit": UNIT,
                "h2d_bytes_per_step": 4 * 2 * nlm * 8, "d2h_bytes_per_step": 4 * 2 * nlm * 8 + 8 * 8,
                "steps": Ke, "warmup": We, "timing": "host wall clock, per-step synchronous C-ABI calls"}
+        # the same step through the combined call (one wait per step)
+        ns0 += Ke
+        for i in range(We):
+            assert L.fb_step_markers(s.ctx, ns0 + i, *ptr, fptr) == 0
+        ns0 += We
+        barrier()
+        te0 = time.perf_counter()
+        for i in range(Ke):
+            assert L.fb_step_markers(s.ctx, ns0 + i, *ptr, fptr) == 0
+        barrier()
+        te1_max = max_over_ranks(dist, time.perf_counter() - te0, dev)
+        e2e_one_call = {"value": replica_throughput(world, c.cells, Ke, 1e3 * te1_max), "unit": UNIT,
+                        "h2d_bytes_per_step": 4 * 2 * nlm * 8, "d2h_bytes_per_step": 4 * 2 * nlm * 8 + 8 * 8,
+                        "steps": Ke, "warmup": We,
+                        "timing": "host wall clock, fb_step_markers: markers in, fluid step, rigid update, "
+                                  "markers and the forcecomp row out, one wait per step"}
 
     result = None
     if rank == 0:
@@ -774,7 +790,8 @@ def device_arm(args, rank, world, local):
                        "parallelism": f"replicas x{world}" if world > 1 else "single case",
                        "tiles": {"helsolve_rows": tiles[0], "gemm_cols": tiles[1] if args.poisson == "tf32x3" else None},
                        "l2": "flushed (256 MB write) between timed steps"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "accuracy": accuracy,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_one_call": e2e_one_call,
+            "accuracy": accuracy,
             "gpu_launches": per_step_kernels * K, "clocks": clk,
             "fp64_gemm_peak_tflops": peak_fp64,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()} for r in table],

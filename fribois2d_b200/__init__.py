@@ -91,6 +91,7 @@ def lib() -> ctypes.CDLL:
         "fb_get_loads": ([vp, dp, dp], ctypes.c_int),
         "fb_set_markers": ([vp, dp, dp, dp, dp], ctypes.c_int),
         "fb_get_markers": ([vp, dp, dp, dp, dp], ctypes.c_int),
+        "fb_step_markers": ([vp, ctypes.c_int, dp, dp, dp, dp, dp], ctypes.c_int),
         "fb_get_dims": ([vp, ip], ctypes.c_int),
         "fb_get_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),
         "fb_set_array": ([vp, ctypes.c_int, dp, i64], ctypes.c_int),

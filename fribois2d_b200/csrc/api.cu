@@ -1835,6 +1835,41 @@ int fb_get_markers(fb_ctx *c, double *lmcc, double *lmvel, double *lmacc, double
     return FB_OK;
 }
 
+int fb_step_markers(fb_ctx *c, int ns, double *lmcc, double *lmvel, double *lmacc, double *lmnor,
+                    double *forcecomp) {
+    if (!c) return FB_ERR_STATE;
+    int r;
+    if ((r = mbox_ready(c))) return r;
+    if ((r = fb_set_markers(c, lmcc, lmvel, lmacc, lmnor))) return r;
+    if (!c->vardt && ns >= 1 && c->fgraph_exec) {
+        CK(cudaGraphLaunch(c->fgraph_exec, c->stream));   // the fluid step (status into the mapped words)
+    } else {
+        // the first fixed-dt step captures the graph, a variable dt needs the host: as fb_fluid_tsch
+        const int st = fb_fluid_tsch(c, ns);
+        if (st) return st;
+    }
+    // the rigid update publishes the (sticky) status and the forcecomp row itself
+    c->rigid_mbox = c->d.nlm ? c->mbox_d : nullptr;
+    r = stage_impl(c, FB_ST_RIGID, ns, 1);
+    c->rigid_mbox = nullptr;
+    if (r) return r;
+    if (!c->d.nlm || c->report) {
+        if ((r = enqueue_report(c))) return r;
+        fb::launch_publish(c->d, true, c->mbox_d, c->stream);
+        c->own_launches += 1;
+    }
+    const size_t n = 2 * static_cast<size_t>(c->d.nlm), b = n * sizeof(double);
+    if (b) CK(cudaMemcpyAsync(c->stage_h, c->d.lmcc, 4 * b, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));   // the one wait
+    double *dst[4] = {lmcc, lmvel, lmacc, lmnor};
+    for (int i = 0; b && i < 4; ++i)
+        if (dst[i]) std::memcpy(dst[i], c->stage_h + i * n, b);
+    if (forcecomp) std::memcpy(forcecomp, c->mbox_h + 1, 8 * sizeof(double));
+    host_clock(c, 1);
+    return mbox_status(c);
+}
+
 int fb_get_dims(fb_ctx *c, int32_t dims[8]) {
     if (!c || !dims) return FB_ERR_STATE;
     dims[0] = c->d.n2;

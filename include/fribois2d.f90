@@ -84,6 +84,14 @@ module fribois2d_gpu
       type(c_ptr), value :: ctx
       real(c_double), dimension(*), intent(out) :: lmcc, lmvel, lmacc, lmnor
     end function
+    integer(c_int) function fb_step_markers(ctx, ns, lmcc, lmvel, lmacc, lmnor, forcecomp) &
+        bind(C, name="fb_step_markers")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: ns
+      real(c_double), dimension(*), intent(inout) :: lmcc, lmvel, lmacc, lmnor
+      real(c_double), dimension(8), intent(out) :: forcecomp
+    end function
     integer(c_int) function fb_last_history(ctx, row) bind(C, name="fb_last_history")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx

@@ -169,6 +169,16 @@ int fb_set_markers(fb_ctx *ctx, const double *lmcc, const double *lmvel, const d
  * wait for all of them: the per-step read of a host that keeps its own
  * marker state (fb_get_array per array waits once per array). */
 int fb_get_markers(fb_ctx *ctx, double *lmcc, double *lmvel, double *lmacc, double *lmnor);
+/* No reference counterpart: one loosely coupled step of main.F90:85-97 for a
+ * host that exchanges the markers every step, in one call with one wait:
+ * fb_set_markers(lmcc, lmvel, lmacc, lmnor), fb_fluid_tsch(ns), fb_rigid(ns,
+ * forcecomp), fb_get_markers(lmcc, lmvel, lmacc, lmnor).  The four arrays
+ * (nlm x 2 each) are read and then overwritten with the updated markers;
+ * forcecomp may be NULL.  Returns the step's status; unlike the separate
+ * calls, the rigid update of a replayed (fixed-dt) step runs even when the
+ * fluid step reported an error. */
+int fb_step_markers(fb_ctx *ctx, int ns, double *lmcc, double *lmvel, double *lmacc, double *lmnor,
+                    double *forcecomp);
 
 /* Last history row written (FB_HIST_COLS doubles), for per-step callers. */
 int fb_last_history(fb_ctx *ctx, double *row);

@@ -117,3 +117,36 @@ def test_marker_round_trip_through_the_host(tmp_path):
         np.testing.assert_array_equal(g.reshape(-1), a.get(n).reshape(-1))
     a.close()
     b.close()
+
+
+def test_step_markers_equals_the_four_calls(tmp_path):
+    """fb_step_markers (markers in, fluid step, rigid update, markers out, one
+    wait) leaves the same state, markers and forcecomp rows, bit for bit, as
+    fb_set_markers + fb_fluid_tsch + fb_rigid + fb_get_markers."""
+    import ctypes
+    c = cases.tiny_cylinder()
+    path = c.write(str(tmp_path / c.name))
+    a, b = _solver(c, path), _solver(c, path)
+    a.advance(0, 3)
+    b.advance(0, 3)
+    L = fb.lib()
+    dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))   # noqa: E731
+    names = ("lmcc", "lmvel", "lmacc", "lmnor")
+    ma = [np.zeros(2 * c.nlm) for _ in names]
+    assert L.fb_get_markers(a.ctx, *[dp(m) for m in ma]) == 0   # the device layout, as the host keeps it
+    mb = [m.copy() for m in ma]
+    fa, fb_ = np.zeros(8), np.zeros(8)
+    for ns in range(3, 12):
+        assert L.fb_set_markers(a.ctx, *[dp(m) for m in ma]) == 0
+        assert L.fb_fluid_tsch(a.ctx, ns) == 0
+        assert L.fb_rigid(a.ctx, ns, dp(fa)) == 0
+        assert L.fb_get_markers(a.ctx, *[dp(m) for m in ma]) == 0
+        assert L.fb_step_markers(b.ctx, ns, *[dp(m) for m in mb], dp(fb_)) == 0
+        np.testing.assert_array_equal(fa, fb_)
+        for x, y in zip(ma, mb):
+            np.testing.assert_array_equal(x, y)
+    for f in ("q2", "q3", "pr"):
+        np.testing.assert_array_equal(a.get(f), b.get(f))
+    np.testing.assert_array_equal(a.last_history(), b.last_history())
+    a.close()
+    b.close()
